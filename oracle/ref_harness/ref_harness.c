@@ -1,0 +1,306 @@
+/*
+ * Harness that runs SHOCK's own CPU implementation of the per-RK-stage
+ * right-hand side, compiled UNMODIFIED from the reference sources
+ * (src/Functions.c, src/WENO.c, src/ZD.c, src/BC.c,
+ * src/ManufacturedSolution.c), as a single block with no MPI.
+ *
+ * Test infrastructure only: it is the pin for the CPU restatement in
+ * oracle/shock_oracle.c and the timed CPU baseline of bench.py.  Nothing
+ * in the shipped library links it.
+ *
+ * What the harness supplies instead of the reference's I/O and MPI layer:
+ *   - set-up follows SHOCK.c:main (SHOCK.c:127-288): DefineParameters,
+ *     postprocessLoad (restart path, Functions.c:797-877, fed with the
+ *     same Fortran-order arrays loadFile would return), ExtrapolateGhostCells,
+ *     mesh transfer, CreateMetric, mesh transfer, check_Metric,
+ *     mirrorGhostCellsMetric, CreateViscidMetric, SetAllBoundaryConditions,
+ *     the MMS part of setOptions (SHOCK.c:858-878), WriteValuesFromU1ToU2.
+ *   - TransferFlowParameterWithGhosts (Functions.c:3580-3684) and
+ *     TransferMeshParameter (Functions.c:3481-3578) are replaced by the
+ *     single-block periodic equivalent: every ghost layer of a periodic
+ *     axis takes the values of its periodic image, over the ghost-inclusive
+ *     slab, axis after axis (the reference repeats the exchange 2x/3x for
+ *     the same effect on edges and corners, Functions.c:2117-2136).  Mesh
+ *     coordinates get the periodic Translation added as a float32, exactly
+ *     as Load.c:110 stores it and Functions.c:2657-2661 applies it.  The
+ *     reference definitions are weakened with objcopy so these win.
+ *   - the time loop is the core of startSimulation (SHOCK.c:557-663):
+ *     CalcRungeKutta then WriteValuesFromU1ToU2(U_RK -> U_lastStep).
+ */
+#include "mpi.h"
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+
+#include "SHOCK.h"
+#include "Functions.h"
+#include "WENO.h"
+#include "ZD.h"
+#include "BC.h"
+#include "ManufacturedSolution.h"
+
+FLT leftEigenvector[5][5];
+FLT rightEigenvector[5][5];
+
+typedef struct {
+    int ni, nj, nk;
+    int time_order;
+    double tau, mach, reynolds, prandtl, gamma, gas_r, t0, l0;
+    int inviscid;
+    int mms;
+    int mms_case;
+    int periodic[3];
+    double period[3];
+} ref_params;
+
+static struct strct_configuration cfg;
+static struct strct_mesh msh;
+static struct strct_U U_last, U_rk, U_b1, U_b2;
+static struct strct_Flux Qf, Qsum, Fl, Flh;
+static struct strct_Film film;
+static ref_params prm;
+static int live = 0;
+
+#define NG (cfg.int_iMeshPointsGhostCells * cfg.int_jMeshPointsGhostCells * cfg.int_kMeshPointsGhostCells)
+#define IDX(i, j, k) ((i) * cfg.int_jMeshPointsGhostCells * cfg.int_kMeshPointsGhostCells + (j) * cfg.int_kMeshPointsGhostCells + (k))
+
+static int lo_real(int a) { return a == 0 ? cfg.int_iStartReal : a == 1 ? cfg.int_jStartReal : cfg.int_kStartReal; }
+static int hi_real(int a) { return a == 0 ? cfg.int_iEndReal : a == 1 ? cfg.int_jEndReal : cfg.int_kEndReal; }
+static int hi_ghost(int a) { return a == 0 ? cfg.int_iEndGhosts : a == 1 ? cfg.int_jEndGhosts : cfg.int_kEndGhosts; }
+
+/* One pass of the periodic image copy along axis a over the ghost-inclusive
+ * slab.  fields: array of field pointers; ntr: how many leading fields get
+ * the float32 translation (coordinates). */
+static void periodic_pass(int a, FLT **fields, int nf, const float *trans)
+{
+    int n = hi_real(a) - lo_real(a) + 1;
+    int idx[3], lim[3];
+    lim[0] = cfg.int_iEndGhosts; lim[1] = cfg.int_jEndGhosts; lim[2] = cfg.int_kEndGhosts;
+    for (idx[0] = 0; idx[0] <= lim[0]; idx[0]++)
+        for (idx[1] = 0; idx[1] <= lim[1]; idx[1]++)
+            for (idx[2] = 0; idx[2] <= lim[2]; idx[2]++) {
+                int g = idx[a], src[3];
+                float t;
+                if (g >= lo_real(a) && g <= hi_real(a)) continue;
+                src[0] = idx[0]; src[1] = idx[1]; src[2] = idx[2];
+                if (g < lo_real(a)) { src[a] = g + n; t = -trans[a]; }
+                else { src[a] = g - n; t = trans[a]; }
+                for (int f = 0; f < nf; f++) {
+                    FLT v = fields[f][IDX(src[0], src[1], src[2])];
+                    if (trans && f < 3) v = v + (f == a ? t : 0.0f);
+                    fields[f][IDX(idx[0], idx[1], idx[2])] = v;
+                }
+            }
+}
+
+/* Replaces Functions.c:3481 for a single periodic block. */
+void TransferMeshParameter(struct strct_configuration *pc, struct strct_mesh *pm)
+{
+    (void)pc;
+    FLT *f[13] = {pm->x, pm->y, pm->z, pm->xi_x, pm->xi_y, pm->xi_z, pm->eta_x,
+                  pm->eta_y, pm->eta_z, pm->zeta_x, pm->zeta_y, pm->zeta_z, pm->jacobian};
+    float trans[3];
+    for (int a = 0; a < 3; a++) trans[a] = (float)prm.period[a];
+    for (int a = 0; a < MESHDIMENSIONS; a++)
+        if (prm.periodic[a]) periodic_pass(a, f, 13, trans);
+}
+
+/* Replaces Functions.c:3580 for a single periodic block (u,v,w,e,rho). */
+void TransferFlowParameterWithGhosts(struct strct_configuration *pc, struct strct_mesh *pm,
+                                     struct strct_U *pu)
+{
+    (void)pc; (void)pm;
+    FLT *f[5] = {pu->u, pu->v, pu->w, pu->e, pu->rho};
+    for (int a = 0; a < MESHDIMENSIONS; a++)
+        if (prm.periodic[a]) periodic_pass(a, f, 5, NULL);
+}
+
+void ref_free(void);
+
+int ref_init(const ref_params *p, const double *x, const double *y, const double *z,
+             const double *u, const double *v, const double *w, const double *pr,
+             const double *rho)
+{
+    vta vx, vy, vz, vu, vv, vw, vrho, vp;
+    if (live) ref_free();
+    memset(&cfg, 0, sizeof(cfg));
+    memset(&msh, 0, sizeof(msh));
+    prm = *p;
+
+    cfg.int_SpaceOrder = SPACEORDER;
+    cfg.int_TimeOrder = p->time_order;
+    cfg.numericalTau = p->tau;
+    cfg.numericalTauStart = p->tau;
+    cfg.machNumber = p->mach;
+    cfg.reynoldsNumber = p->reynolds;
+    cfg.prandtlNumber = p->prandtl;
+    cfg.gammaNumber = p->gamma;
+    cfg.gasConstantNumber = p->gas_r;
+    cfg.T0_dim = p->t0;
+    cfg.L0_dim = p->l0;
+    cfg.flag_Inviscid = p->inviscid;
+    cfg.flag_ManufacturedSolution = p->mms ? 1 : 0;
+    cfg.ManufacturedSolution_case = p->mms_case;
+    cfg.int_TotalIterations = 1;
+    cfg.int_Samples = 1;
+    cfg.IBC_MovingStepsize = 1;
+    cfg.int_initializeType = 1;
+    cfg.InitializeValues_rho0 = 1.0;
+    cfg.InitializeValues_p0 = 1.0;
+    cfg.MPI_rank = 0;
+    cfg.MPI_size = 1;
+    cfg.NumberInterfaces = 0;
+    cfg.zonesize[0] = p->ni;
+    cfg.zonesize[1] = p->nj;
+#if MESHDIMENSIONS == 3
+    cfg.zonesize[2] = p->nk;
+#endif
+    cfg.InterfaceNeighbourLeft = cfg.InterfaceNeighbourRight = p->periodic[0] ? 0 : NO_NEIGHBOUR;
+    cfg.InterfaceNeighbourBottom = cfg.InterfaceNeighbourTop = p->periodic[1] ? 0 : NO_NEIGHBOUR;
+    cfg.InterfaceNeighbourBehind = cfg.InterfaceNeighbourInFront = p->periodic[2] ? 0 : NO_NEIGHBOUR;
+
+    DefineParameters(&cfg);
+
+    vx.ptr = (void *)x; vx.dt = RealDouble;
+    vy.ptr = (void *)y; vy.dt = RealDouble;
+    vz.ptr = (void *)z; vz.dt = RealDouble;
+    vu.ptr = (void *)u; vu.dt = RealDouble;
+    vv.ptr = (void *)v; vv.dt = RealDouble;
+    vw.ptr = (void *)w; vw.dt = RealDouble;
+    vp.ptr = (void *)pr; vp.dt = RealDouble;
+    vrho.ptr = (void *)rho; vrho.dt = RealDouble;
+    postprocessLoad(&vx, &vy, &vz, &vu, &vv, &vw, &vrho, &vp, &cfg, &msh, &U_last, &U_rk,
+                    &Fl, &Flh, &Qf, &Qsum, &film, &U_b1, &U_b2);
+
+    ExtrapolateGhostCells(&cfg, &msh);
+    for (int r = 0; r < MESHDIMENSIONS; r++) TransferMeshParameter(&cfg, &msh);
+    CreateMetric(&cfg, &msh);
+    for (int r = 0; r < MESHDIMENSIONS; r++) TransferMeshParameter(&cfg, &msh);
+    check_Metric(&cfg, &msh);
+    mirrorGhostCellsMetric(&cfg, &msh);
+    CreateViscidMetric(&cfg, &msh);
+    SetAllBoundaryConditions(&cfg, &msh, &U_last, &U_last);
+    if (cfg.flag_ManufacturedSolution == 1) {
+        ConfigureManufacturedSolution(&cfg);
+        InitializeManufacturedSolution(&cfg, &msh, &U_last);
+        SetAllBoundaryConditions(&cfg, &msh, &U_last, &U_last);
+    }
+    WriteValuesFromU1ToU2(&cfg, &U_last, &U_rk);
+    live = 1;
+    return 0;
+}
+
+void ref_dims(int *out)
+{
+    out[0] = cfg.int_iMeshPointsGhostCells;
+    out[1] = cfg.int_jMeshPointsGhostCells;
+    out[2] = cfg.int_kMeshPointsGhostCells;
+    out[3] = cfg.int_iStartReal;
+    out[4] = cfg.int_jStartReal;
+    out[5] = cfg.int_kStartReal;
+}
+
+/* One right-hand side at U_RK, in CalcRungeKutta's stage order
+ * (Functions.c:2111-2293) without the RK update. q: 5*NG. */
+void ref_rhs(double *q)
+{
+    int n = NG;
+    DeleteQ(&cfg, &Qf);
+    TransferFlowParameterWithGhosts(&cfg, &msh, &U_rk);
+    CalcValues(&cfg, &msh, &U_rk);
+    SetAllBoundaryConditions(&cfg, &msh, &U_rk, &U_last);
+    CalcFluxesInXiDirection(&cfg, &msh, &U_rk, &Fl, &Flh, &Qf);
+    CalcFluxesInEtaDirection(&cfg, &msh, &U_rk, &Fl, &Flh, &Qf);
+#if MESHDIMENSIONS == 3
+    CalcFluxesInZetaDirection(&cfg, &msh, &U_rk, &Fl, &Flh, &Qf);
+#endif
+    if (cfg.flag_Inviscid != 1) {
+        CalcDeviationsForDirectViscidFluxes(&cfg, &msh, &U_rk);
+        CalcViscidFluxesInXiDirectionDirectly(&cfg, &msh, &U_rk, &Qf);
+        CalcViscidFluxesInEtaDirectionDirectly(&cfg, &msh, &U_rk, &Qf);
+#if MESHDIMENSIONS == 3
+        CalcViscidFluxesInZetaDirectionDirectly(&cfg, &msh, &U_rk, &Qf);
+#endif
+    }
+    if (cfg.flag_ManufacturedSolution == 1) AddManufacturedSolutionSource(&cfg, &msh, &Qf);
+    memcpy(q + 0 * (size_t)n, Qf.Mass, sizeof(double) * n);
+    memcpy(q + 1 * (size_t)n, Qf.xiMomentum, sizeof(double) * n);
+    memcpy(q + 2 * (size_t)n, Qf.etaMomentum, sizeof(double) * n);
+    memcpy(q + 3 * (size_t)n, Qf.zetaMomentum, sizeof(double) * n);
+    memcpy(q + 4 * (size_t)n, Qf.Energy, sizeof(double) * n);
+}
+
+/* n time steps, the core of startSimulation (SHOCK.c:557-663). */
+void ref_steps(int n)
+{
+    for (int s = 0; s < n; s++) {
+        CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh);
+        WriteValuesFromU1ToU2(&cfg, &U_rk, &U_last);
+    }
+}
+
+/* out: rho,u,v,w,e,p,T,c,mue (9*NG) of U_RK (which=0) or U_lastStep (1). */
+void ref_get_state(double *out, int which)
+{
+    struct strct_U *s = which ? &U_last : &U_rk;
+    FLT *f[9] = {s->rho, s->u, s->v, s->w, s->e, s->p, s->T, s->c, s->mue};
+    int n = NG;
+    for (int a = 0; a < 9; a++) memcpy(out + (size_t)a * n, f[a], sizeof(double) * n);
+}
+
+/* Overwrite rho,u,v,w,e (5*NG) of both U_RK and U_lastStep. */
+void ref_set_state(const double *in)
+{
+    int n = NG;
+    FLT *a[5] = {U_rk.rho, U_rk.u, U_rk.v, U_rk.w, U_rk.e};
+    FLT *b[5] = {U_last.rho, U_last.u, U_last.v, U_last.w, U_last.e};
+    for (int f = 0; f < 5; f++) {
+        memcpy(a[f], in + (size_t)f * n, sizeof(double) * n);
+        memcpy(b[f], in + (size_t)f * n, sizeof(double) * n);
+    }
+}
+
+/* out: x,y,z,J,xi_x,xi_y,xi_z,eta_x,eta_y,eta_z,zeta_x,zeta_y,zeta_z (13*NG). */
+void ref_get_geom(double *out)
+{
+    FLT *f[13] = {msh.x, msh.y, msh.z, msh.jacobian, msh.xi_x, msh.xi_y, msh.xi_z,
+                  msh.eta_x, msh.eta_y, msh.eta_z, msh.zeta_x, msh.zeta_y, msh.zeta_z};
+    int n = NG;
+    for (int a = 0; a < 13; a++) memcpy(out + (size_t)a * n, f[a], sizeof(double) * n);
+}
+
+/* Seconds of wall time for nstage RK stages: nstage/TimeOrder full steps
+ * through CalcRungeKutta (TimeOrder stages each). */
+double ref_time_steps(int nsteps)
+{
+    struct timespec a, b;
+    clock_gettime(CLOCK_MONOTONIC, &a);
+    ref_steps(nsteps);
+    clock_gettime(CLOCK_MONOTONIC, &b);
+    return (double)(b.tv_sec - a.tv_sec) + 1e-9 * (double)(b.tv_nsec - a.tv_nsec);
+}
+
+int ref_time_order(void) { return cfg.int_TimeOrder; }
+
+/* J*S of the manufactured-solution source as AddManufacturedSolutionSource
+ * adds it to a zeroed Q (src/ManufacturedSolution.c:25-175); 5*NG. */
+void ref_mms_source(double *js5)
+{
+    int n = NG;
+    DeleteQ(&cfg, &Qf);
+    AddManufacturedSolutionSource(&cfg, &msh, &Qf);
+    memcpy(js5 + 0 * (size_t)n, Qf.Mass, sizeof(double) * n);
+    memcpy(js5 + 1 * (size_t)n, Qf.xiMomentum, sizeof(double) * n);
+    memcpy(js5 + 2 * (size_t)n, Qf.etaMomentum, sizeof(double) * n);
+    memcpy(js5 + 3 * (size_t)n, Qf.zetaMomentum, sizeof(double) * n);
+    memcpy(js5 + 4 * (size_t)n, Qf.Energy, sizeof(double) * n);
+}
+
+void ref_free(void)
+{
+    if (!live) return;
+    FreeMemory(&cfg, &msh, &U_last, &U_rk, &Fl, &Flh, &Qf, &Qsum, &film);
+    live = 0;
+}

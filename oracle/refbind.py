@@ -1,0 +1,215 @@
+"""ctypes bindings for the oracle libraries (test infrastructure only).
+
+* ``RefSolver`` drives SHOCK's own CPU code (oracle/_ref/libshockref_*.so,
+  built by oracle/Makefile from the unmodified reference sources) through
+  ref_harness.c.
+* ``Oracle`` drives the CPU restatement (oracle/liboracle.so).
+
+Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg use
+this module, as the checker.  The shipped library never imports it.
+
+Array conventions (both bindings): ghosted SoA fields, C order with k
+fastest, index ijk = i*NJg*NKg + j*NKg + k (src/Functions.c:2306); 2D uses
+NKg = 1.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_dp = C.POINTER(C.c_double)
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+class RefParams(C.Structure):
+    _fields_ = [
+        ("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int),
+        ("time_order", C.c_int),
+        ("tau", C.c_double), ("mach", C.c_double), ("reynolds", C.c_double),
+        ("prandtl", C.c_double), ("gamma", C.c_double), ("gas_r", C.c_double),
+        ("t0", C.c_double), ("l0", C.c_double),
+        ("inviscid", C.c_int), ("mms", C.c_int), ("mms_case", C.c_int),
+        ("periodic", C.c_int * 3), ("period", C.c_double * 3),
+    ]
+
+
+def ref_available(order: int, dim: int) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", f"libshockref_w{order}_{dim}d.so"))
+
+
+class RefSolver:
+    """One block of SHOCK's reference solver (one library per order/dim)."""
+
+    _libs: dict = {}
+
+    def __init__(self, case):
+        self.case = case
+        key = (case.order, case.dim)
+        if key not in RefSolver._libs:
+            path = os.path.join(HERE, "_ref", f"libshockref_w{case.order}_{case.dim}d.so")
+            if not os.path.exists(path):
+                raise FileNotFoundError(path + " (run make -C oracle ref)")
+            lib = C.CDLL(path, mode=os.RTLD_LOCAL)
+            lib.ref_init.restype = C.c_int
+            lib.ref_time_steps.restype = C.c_double
+            RefSolver._libs[key] = lib
+        self.lib = RefSolver._libs[key]
+        p = RefParams()
+        p.ni, p.nj, p.nk = case.ni, case.nj, (case.nk if case.dim == 3 else 1)
+        p.time_order = case.time_order
+        p.tau, p.mach, p.reynolds = case.tau, case.mach, case.reynolds
+        p.prandtl, p.gamma, p.gas_r, p.t0, p.l0 = case.prandtl, case.gamma, case.gas_r, case.t0, case.l0
+        p.inviscid = int(case.inviscid)
+        p.mms = 1 if case.mms == "reference" else 0
+        p.mms_case = case.mms_case
+        for a in range(3):
+            p.periodic[a] = int(case.periodic[a])
+            p.period[a] = case.period[a]
+        self.params = p
+        f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
+        x, y, z, u, v, w, pr, rho = (f(a) for a in case.real_fields())
+        self._keep = (x, y, z, u, v, w, pr, rho)
+        rc = self.lib.ref_init(C.byref(p), _ptr(x), _ptr(y), _ptr(z), _ptr(u), _ptr(v),
+                               _ptr(w), _ptr(pr), _ptr(rho))
+        assert rc == 0
+        d = (C.c_int * 6)()
+        self.lib.ref_dims(d)
+        self.shape = (d[0], d[1], d[2])
+        self.start = (d[3], d[4], d[5])
+        self.n = d[0] * d[1] * d[2]
+
+    def rhs(self) -> np.ndarray:
+        q = np.zeros(5 * self.n)
+        self.lib.ref_rhs(_ptr(q))
+        return q.reshape((5,) + self.shape)
+
+    def steps(self, n: int):
+        self.lib.ref_steps(C.c_int(n))
+
+    def time_steps(self, n: int) -> float:
+        return self.lib.ref_time_steps(C.c_int(n))
+
+    def state(self, which: int = 0) -> np.ndarray:
+        """rho,u,v,w,e,p,T,c,mue of U_RK (0) or U_lastStep (1)."""
+        s = np.zeros(9 * self.n)
+        self.lib.ref_get_state(_ptr(s), C.c_int(which))
+        return s.reshape((9,) + self.shape)
+
+    def set_state(self, prim5: np.ndarray):
+        a = np.ascontiguousarray(prim5, dtype=np.float64).ravel()
+        assert a.size == 5 * self.n
+        self.lib.ref_set_state(_ptr(a))
+
+    def geometry(self) -> np.ndarray:
+        """x,y,z,J,xi_x,xi_y,xi_z,eta_x,eta_y,eta_z,zeta_x,zeta_y,zeta_z."""
+        g = np.zeros(13 * self.n)
+        self.lib.ref_get_geom(_ptr(g))
+        return g.reshape((13,) + self.shape)
+
+    def mms_source(self) -> np.ndarray:
+        """J*S of the reference manufactured-solution source (5 fields)."""
+        q = np.zeros(5 * self.n)
+        self.lib.ref_mms_source(_ptr(q))
+        return q.reshape((5,) + self.shape)
+
+    def mms_exact(self) -> np.ndarray:
+        """Exact solution at every ghosted point after set-up (9 fields)."""
+        return self.state(1)
+
+
+class OcParams(C.Structure):
+    _fields_ = [
+        ("dim", C.c_int), ("order", C.c_int),
+        ("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int),
+        ("time_order", C.c_int),
+        ("tau", C.c_double), ("mach", C.c_double), ("reynolds", C.c_double),
+        ("prandtl", C.c_double), ("gamma", C.c_double), ("gas_r", C.c_double),
+        ("t0", C.c_double), ("l0", C.c_double),
+        ("inviscid", C.c_int), ("mms", C.c_int),
+        ("periodic", C.c_int * 3), ("period", C.c_double * 3),
+    ]
+
+
+_oclib = None
+
+
+def _oracle_lib():
+    global _oclib
+    if _oclib is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise FileNotFoundError(path + " (run make -C oracle)")
+        lib = C.CDLL(path)
+        lib.oc_create.restype = C.c_void_p
+        for name in ("oc_dims", "oc_set_dirichlet", "oc_set_source", "oc_set_state",
+                     "oc_get_state", "oc_get_geom", "oc_rhs", "oc_steps", "oc_free"):
+            getattr(lib, name).argtypes = None
+        _oclib = lib
+    return _oclib
+
+
+class Oracle:
+    """The CPU restatement, same calling convention as RefSolver."""
+
+    def __init__(self, case, dirichlet9=None, source5=None):
+        lib = self.lib = _oracle_lib()
+        p = OcParams()
+        p.dim, p.order = case.dim, case.order
+        p.ni, p.nj, p.nk = case.ni, case.nj, (case.nk if case.dim == 3 else 1)
+        p.time_order = case.time_order
+        p.tau, p.mach, p.reynolds = case.tau, case.mach, case.reynolds
+        p.prandtl, p.gamma, p.gas_r, p.t0, p.l0 = case.prandtl, case.gamma, case.gas_r, case.t0, case.l0
+        p.inviscid = int(case.inviscid)
+        p.mms = 0 if case.mms == "none" else 1
+        for a in range(3):
+            p.periodic[a] = int(case.periodic[a])
+            p.period[a] = case.period[a]
+        f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
+        arrs = [f(a) for a in case.real_fields()]
+        self.h = C.c_void_p(lib.oc_create(C.byref(p), *[_ptr(a) for a in arrs]))
+        d = (C.c_int * 6)()
+        lib.oc_dims(self.h, d)
+        self.shape = (d[0], d[1], d[2])
+        self.start = (d[3], d[4], d[5])
+        self.n = d[0] * d[1] * d[2]
+        if dirichlet9 is not None:
+            a = np.ascontiguousarray(dirichlet9, np.float64).ravel()
+            lib.oc_set_dirichlet(self.h, _ptr(a))
+        if source5 is not None:
+            a = np.ascontiguousarray(source5, np.float64).ravel()
+            lib.oc_set_source(self.h, _ptr(a))
+
+    def __del__(self):
+        try:
+            self.lib.oc_free(self.h)
+        except Exception:
+            pass
+
+    def rhs(self):
+        q = np.zeros(5 * self.n)
+        self.lib.oc_rhs(self.h, _ptr(q))
+        return q.reshape((5,) + self.shape)
+
+    def steps(self, n):
+        self.lib.oc_steps(self.h, C.c_int(n))
+
+    def state(self, which=0):
+        s = np.zeros(9 * self.n)
+        self.lib.oc_get_state(self.h, _ptr(s), C.c_int(which))
+        return s.reshape((9,) + self.shape)
+
+    def set_state(self, prim5):
+        a = np.ascontiguousarray(prim5, np.float64).ravel()
+        self.lib.oc_set_state(self.h, _ptr(a))
+
+    def geometry(self):
+        g = np.zeros(13 * self.n)
+        self.lib.oc_get_geom(self.h, _ptr(g))
+        return g.reshape((13,) + self.shape)

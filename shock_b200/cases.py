@@ -1,0 +1,290 @@
+"""Problem set-ups: grids, initial states and SHOCK parameters.
+
+A ``Case`` carries everything SHOCK reads from its CGNS grid/solution and
+``config.ini`` for one run of the per-RK-stage path: the real-point
+coordinates and primitive fields (the arrays ``loadFile`` returns,
+src/Load.c:252-744), the ``[Numerics]``/``[FluidProperties]``/``[Options]``
+keys the hot path consumes (src/Import.c:36-238), and which faces are
+periodic (SHOCK encodes periodicity as self-interfaces in the ``.sddc``
+division file, src/Load.c:191-250).
+
+Non-dimensionalisation follows SHOCK (src/Functions.c:2012-2013,
+docs/goveq.tex:158-162): Upsilon = 1/(gamma Ma^2), p = rho T,
+e = |u|^2/2 + Upsilon/(gamma-1) p/rho, velocities in units of
+u_ref = Ma c_0.  States given with rho_0 = 1, c_0 = 1 map to SHOCK units
+at Ma = 1 as rho_S = rho, u_S = u, p_S = gamma p.
+
+The generators here build the benchmark workloads from their definitions
+with seeded synthetic data (no dataset is involved):
+  * ``mms_square``       -- 2D manufactured solution on the unit square
+  * ``taylor_green``     -- 3D Taylor-Green vortex on a perturbed periodic cube
+  * ``decaying_turbulence`` -- random-phase solenoidal field, periodic cube
+  * ``isentropic_vortex``-- 2D periodic isentropic vortex (ensemble members)
+  * ``smooth_random``    -- smooth random periodic states for parity tests
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+from typing import Optional, Tuple
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Case:
+    dim: int
+    order: int                      # WENO order: 5 or 9 (SPACEORDER)
+    ni: int
+    nj: int
+    nk: int
+    x: np.ndarray                   # real-point coordinates, shape (ni,nj,nk)
+    y: np.ndarray
+    z: np.ndarray
+    rho: np.ndarray                 # real-point primitives, shape (ni,nj,nk)
+    u: np.ndarray
+    v: np.ndarray
+    w: np.ndarray
+    p: np.ndarray
+    time_order: int = 4             # [Numerics] TimeOrder: 3 (RK3-TVD) or 4 (RK4)
+    tau: float = 1e-3               # [Numerics] Tau
+    mach: float = 1.0               # [FluidProperties] Mach
+    reynolds: float = 1000.0        # Reynolds
+    prandtl: float = 0.72           # Prandtl
+    gamma: float = 1.4              # Gamma
+    gas_r: float = 287.0            # R
+    t0: float = 300.0               # T
+    l0: float = 1.0                 # L
+    inviscid: bool = False          # [Options] Inviscid
+    mms: str = "none"               # "none" | "reference" (ManufacturedSolution.c family) | "baseline"
+    mms_case: int = 0               # [ManufacturedSolution] case
+    periodic: Tuple[bool, bool, bool] = (True, True, True)
+    period: Tuple[float, float, float] = (1.0, 1.0, 1.0)
+    name: str = "case"
+
+    @property
+    def ghosts(self) -> int:
+        return (self.order + 1) // 2
+
+    @property
+    def real_points(self) -> int:
+        return self.ni * self.nj * (self.nk if self.dim == 3 else 1)
+
+    def real_fields(self):
+        return (self.x, self.y, self.z, self.u, self.v, self.w, self.p, self.rho)
+
+    def replace(self, **kw) -> "Case":
+        return dataclasses.replace(self, **kw)
+
+    def energy(self) -> np.ndarray:
+        """e from (rho,u,v,w,p) exactly as src/Functions.c:872-874 forms it."""
+        ups = 1.0 / (self.gamma * (self.mach * self.mach))
+        return (0.5 * ((self.u * self.u) + (self.v * self.v) + (self.w * self.w))
+                + self.p / self.rho / (self.gamma - 1.0) * ups)
+
+
+def _mesh(dim, n, lo, length, endpoint):
+    axes = []
+    for a in range(3):
+        if a < dim:
+            if endpoint:
+                axes.append(lo[a] + length[a] * np.arange(n[a]) / (n[a] - 1))
+            else:
+                axes.append(lo[a] + length[a] * np.arange(n[a]) / n[a])
+        else:
+            axes.append(np.zeros(1))
+    return np.meshgrid(*axes, indexing="ij")
+
+
+def cfl_tau(case: Case, cfl: float = 0.5) -> float:
+    """tau = cfl / max over cells of sum_d (|theta_d| + c |grad xi_d|) on the
+    initial state, with |grad xi_d| = 1/spacing of the Cartesian skeleton."""
+    ups = 1.0 / (case.gamma * case.mach ** 2)
+    c = np.sqrt(ups * case.gamma * case.p / case.rho)
+    vel = (case.u, case.v, case.w)
+    n = (case.ni, case.nj, case.nk)
+    s = np.zeros_like(case.rho)
+    for a in range(case.dim):
+        h = case.period[a] / n[a] if case.periodic[a] else case.period[a] / (n[a] - 1)
+        s = s + (np.abs(vel[a]) + c) / h
+    return float(cfl / s.max())
+
+
+def smooth_random(dim: int, order: int, n: Tuple[int, int, int], seed: int = 0,
+                  amp: float = 0.05, mach: float = 1.0, inviscid: bool = False,
+                  reynolds: float = 200.0, time_order: int = 4, stretch: float = 0.0,
+                  length: float = 1.0) -> Case:
+    """Smooth random periodic state: a few low Fourier modes per field on a
+    periodic box, optionally with a smooth coordinate stretch per axis."""
+    rng = np.random.default_rng(seed)
+    ni, nj, nk = n[0], n[1], (n[2] if dim == 3 else 1)
+    L = (length, length, length if dim == 3 else 1.0)
+    x, y, z = _mesh(dim, (ni, nj, nk), (0.0, 0.0, 0.0), L, endpoint=False)
+    if stretch:
+        x = x + stretch * L[0] / (2 * math.pi) * np.sin(2 * math.pi * x / L[0])
+        y = y + stretch * L[1] / (2 * math.pi) * np.sin(2 * math.pi * y / L[1])
+        if dim == 3:
+            z = z + stretch * L[2] / (2 * math.pi) * np.sin(2 * math.pi * z / L[2])
+    X = [2 * math.pi * x / L[0], 2 * math.pi * y / L[1], 2 * math.pi * z / L[2]]
+
+    def field():
+        f = np.zeros_like(x)
+        for _ in range(3):
+            kv = rng.integers(0, 3, size=3)
+            if dim == 2:
+                kv[2] = 0
+            ph = rng.uniform(0, 2 * math.pi)
+            f = f + rng.normal() * np.sin(kv[0] * X[0] + kv[1] * X[1] + kv[2] * X[2] + ph)
+        return f
+
+    rho = 1.0 + amp * field()
+    u = 0.3 + amp * field()
+    v = -0.2 + amp * field()
+    w = (0.1 + amp * field()) if dim == 3 else np.zeros_like(x)
+    p = 1.0 + amp * field()
+    c = Case(dim=dim, order=order, ni=ni, nj=nj, nk=nk, x=x, y=y, z=z, rho=rho, u=u, v=v,
+             w=w, p=p, time_order=time_order, mach=mach, reynolds=reynolds,
+             inviscid=inviscid, periodic=(True, True, dim == 3), period=L,
+             name=f"smooth{dim}d_w{order}")
+    c.tau = cfl_tau(c)
+    return c
+
+
+def taylor_green(n: int = 64, order: int = 5, mach: float = 0.1, reynolds: float = 1600.0,
+                 perturb: float = 0.05, time_order: int = 4) -> Case:
+    """3D Taylor-Green vortex on [0,2pi)^3 with every coordinate perturbed by
+    x_i += perturb*sin(x_j)*sin(x_k).  u = sin x cos y cos z,
+    v = -cos x sin y cos z, w = 0, p = p0 + (cos2x+cos2y)(cos2z+2)/16 at Ma,
+    isothermal rho (T = 1).  In SHOCK units p_S = 1 + gamma Ma^2 (...)/16."""
+    L = 2 * math.pi
+    X, Y, Z = _mesh(3, (n, n, n), (0.0, 0.0, 0.0), (L, L, L), endpoint=False)
+    x = X + perturb * np.sin(Y) * np.sin(Z)
+    y = Y + perturb * np.sin(X) * np.sin(Z)
+    z = Z + perturb * np.sin(X) * np.sin(Y)
+    gamma = 1.4
+    u = np.sin(X) * np.cos(Y) * np.cos(Z)
+    v = -np.cos(X) * np.sin(Y) * np.cos(Z)
+    w = np.zeros_like(X)
+    p = 1.0 + gamma * mach ** 2 * (np.cos(2 * X) + np.cos(2 * Y)) * (np.cos(2 * Z) + 2.0) / 16.0
+    rho = p.copy()
+    c = Case(dim=3, order=order, ni=n, nj=n, nk=n, x=x, y=y, z=z, rho=rho, u=u, v=v, w=w,
+             p=p, time_order=time_order, mach=mach, reynolds=reynolds, gamma=gamma,
+             periodic=(True, True, True), period=(L, L, L), name=f"tgv{n}_w{order}")
+    c.tau = cfl_tau(c)
+    return c
+
+
+def mms_square(n: int = 64, order: int = 5, family: str = "baseline", reynolds: float = 100.0,
+               mms_case: int = 0, inviscid: bool = False, time_order: int = 4) -> Case:
+    """2D unit square with n x n points on [0,1]^2 (x_i = i/(n-1), the
+    2d_cube layout), manufactured-solution mode: every face is a Dirichlet
+    ghost face holding the exact solution (src/ManufacturedSolution.c:340-388).
+
+    family "baseline": rho = 1+0.1 sin(2pi x)sin(2pi y), u = 0.3 cos(2pi x)sin(2pi y),
+      v = 0.3 sin(2pi x)cos(2pi y), p = 1/gamma + 0.05 cos(2pi x)cos(2pi y), at
+      Ma = 1 (so p_S = gamma p), Re = 100, Pr = 0.72.
+    family "reference": SHOCK's own sum-of-separable family; the initial state
+      is overwritten by InitializeManufacturedSolution, so the fields here are
+      placeholders."""
+    X, Y, Z = _mesh(2, (n, n, 1), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), endpoint=True)
+    gamma = 1.4
+    tp = 2 * math.pi
+    rho = 1.0 + 0.1 * np.sin(tp * X) * np.sin(tp * Y)
+    u = 0.3 * np.cos(tp * X) * np.sin(tp * Y)
+    v = 0.3 * np.sin(tp * X) * np.cos(tp * Y)
+    w = np.zeros_like(X)
+    p = gamma * (1.0 / gamma + 0.05 * np.cos(tp * X) * np.cos(tp * Y))
+    mach = 1.0
+    if family == "reference":
+        mach = 0.5
+        rho = np.ones_like(X)
+        u = np.zeros_like(X)
+        v = np.zeros_like(X)
+        p = np.ones_like(X)
+    c = Case(dim=2, order=order, ni=n, nj=n, nk=1, x=X, y=Y, z=Z, rho=rho, u=u, v=v, w=w, p=p,
+             time_order=time_order, mach=mach, reynolds=reynolds, gamma=gamma,
+             inviscid=inviscid, mms=family, mms_case=mms_case,
+             periodic=(False, False, False), period=(1.0, 1.0, 1.0),
+             name=f"mms_{family}{n}_w{order}")
+    c.tau = cfl_tau(c)
+    return c
+
+
+def isentropic_vortex(n: int, beta: float, mach_inf: float, order: int = 5,
+                      length: float = 10.0, inviscid: bool = True, reynolds: float = 1e4,
+                      time_order: int = 4) -> Case:
+    """2D isentropic vortex (Shu's form) centred in a periodic [0,L)^2 box,
+    free stream along x at Mach mach_inf, with rho_0 = 1, c_0 = 1, p_0 = 1/gamma:
+      du = -beta/(2pi) (y-yc) e^{(1-r^2)/2}, dv = beta/(2pi) (x-xc) e^{(1-r^2)/2},
+      T = 1 - (gamma-1) beta^2/(8 gamma pi^2) e^{1-r^2}, rho = T^{1/(gamma-1)},
+      p = rho T / gamma.  Mapped to SHOCK units at Ma = 1."""
+    gamma = 1.4
+    X, Y, Z = _mesh(2, (n, n, 1), (0.0, 0.0, 0.0), (length, length, 1.0), endpoint=False)
+    xc = yc = length / 2
+    r2 = (X - xc) ** 2 + (Y - yc) ** 2
+    ex = np.exp(0.5 * (1.0 - r2))
+    u = mach_inf + (-beta / (2 * math.pi)) * (Y - yc) * ex
+    v = (beta / (2 * math.pi)) * (X - xc) * ex
+    T = 1.0 - (gamma - 1.0) * beta ** 2 / (8 * gamma * math.pi ** 2) * ex * ex
+    rho = T ** (1.0 / (gamma - 1.0))
+    p_b = rho * T / gamma
+    c = Case(dim=2, order=order, ni=n, nj=n, nk=1, x=X, y=Y, z=Z, rho=rho, u=u, v=v,
+             w=np.zeros_like(X), p=gamma * p_b, time_order=time_order, mach=1.0,
+             reynolds=reynolds, gamma=gamma, inviscid=inviscid,
+             periodic=(True, True, False), period=(length, length, 1.0),
+             name=f"vortex{n}")
+    c.tau = cfl_tau(c)
+    return c
+
+
+def decaying_turbulence(n: int = 512, order: int = 9, seed: int = 3, mach_t: float = 0.6,
+                        re_lambda: float = 100.0, k0: float = 4.0,
+                        time_order: int = 4) -> Case:
+    """Random-phase solenoidal velocity on [0,2pi)^3 with E(k) ~ k^4 exp(-2(k/k0)^2),
+    scaled to turbulent Mach sqrt(<u.u>)/c = mach_t; rho = 1, p = 1/gamma
+    (p_S = 1 at Ma = 1).  Re chosen so Re_lambda = u' lambda / nu = re_lambda
+    with lambda^2 = 15 u'^2 / <omega^2> and u' = sqrt(<u.u>/3)."""
+    L = 2 * math.pi
+    rng = np.random.default_rng(seed)
+    kk = np.fft.fftfreq(n, d=1.0 / n)
+    kz = np.fft.rfftfreq(n, d=1.0 / n)
+    KX, KY, KZ = np.meshgrid(kk, kk, kz, indexing="ij")
+    K2 = KX ** 2 + KY ** 2 + KZ ** 2
+    K = np.sqrt(K2)
+    Ksafe = np.where(K == 0, 1.0, K)
+    E = Ksafe ** 4 * np.exp(-2.0 * (Ksafe / k0) ** 2)
+    amp = np.sqrt(E / (4 * math.pi * Ksafe ** 2))
+    amp[K == 0] = 0.0
+    uh = []
+    for _ in range(3):
+        ph = rng.uniform(0, 2 * math.pi, size=K.shape)
+        uh.append(amp * np.exp(1j * ph))
+    # project onto divergence-free
+    dot = (KX * uh[0] + KY * uh[1] + KZ * uh[2]) / np.where(K2 == 0, 1.0, K2)
+    uh = [uh[0] - KX * dot, uh[1] - KY * dot, uh[2] - KZ * dot]
+    vel = [np.fft.irfftn(h, s=(n, n, n), axes=(0, 1, 2)) for h in uh]
+    gamma = 1.4
+    c0 = 1.0  # rho = 1, p = 1/gamma
+    urms = math.sqrt(float(np.mean(vel[0] ** 2 + vel[1] ** 2 + vel[2] ** 2)))
+    scale = mach_t * c0 / urms
+    vel = [v * scale for v in vel]
+    # vorticity magnitude from spectral derivatives
+    om2 = 0.0
+    wh = [np.fft.rfftn(v) for v in vel]
+    cx = 1j * KY * wh[2] - 1j * KZ * wh[1]
+    cy = 1j * KZ * wh[0] - 1j * KX * wh[2]
+    cz = 1j * KX * wh[1] - 1j * KY * wh[0]
+    for cc in (cx, cy, cz):
+        om2 += float(np.mean(np.fft.irfftn(cc, s=(n, n, n)) ** 2))
+    uprime = math.sqrt(float(np.mean(vel[0] ** 2 + vel[1] ** 2 + vel[2] ** 2)) / 3.0)
+    lam = math.sqrt(15.0 * uprime ** 2 / om2)
+    nu = uprime * lam / re_lambda
+    reynolds = 1.0 / nu        # rho = 1, u_ref = c_0 = 1, L_ref = 1
+    X, Y, Z = _mesh(3, (n, n, n), (0.0, 0.0, 0.0), (L, L, L), endpoint=False)
+    rho = np.ones_like(X)
+    p = np.ones_like(X)  # p_S = gamma * (1/gamma)
+    c = Case(dim=3, order=order, ni=n, nj=n, nk=n, x=X, y=Y, z=Z, rho=rho, u=vel[0], v=vel[1],
+             w=vel[2], p=p, time_order=time_order, mach=1.0, reynolds=reynolds, gamma=gamma,
+             periodic=(True, True, True), period=(L, L, L), name=f"turb{n}_w{order}")
+    c.tau = cfl_tau(c)
+    return c
