@@ -1,0 +1,134 @@
+/*
+ * shock_b200 -- B200 implementation of SHOCK's per-RK-stage right-hand
+ * side (WENO5/9 characteristic flux splitting, central viscous fluxes,
+ * RK stage update, ghost-cell fills), behind a plain C ABI.
+ *
+ * Conventions
+ *   - every entry point returns 0 on success or a negative SHOCK_E* code;
+ *     nothing calls exit().  shock_last_error() gives a message.
+ *   - field arrays on the host are SHOCK's ghosted SoA layout: C order
+ *     with k fastest, ijk = i*NJg*NKg + j*NKg + k (src/Functions.c:2306),
+ *     NKg = 1 in 2D, (order+1)/2 ghost layers per side
+ *     (src/Functions.c:58-85).  "Fortran order" arrays are real points
+ *     only, i fastest, as src/Load.c hands them to postprocessLoad.
+ *   - state variables are SHOCK's strct_U members rho,u,v,w,e
+ *     (src/SHOCK.h:590-620); fluxes are strct_Flux Mass, xiMomentum,
+ *     etaMomentum, zetaMomentum, Energy (src/SHOCK.h:634-641).
+ *   - one context owns its device buffers, stream and CUDA graphs; calls
+ *     on different contexts may run from different host threads, calls on
+ *     one context must not.
+ */
+#ifndef SHOCK_B200_H
+#define SHOCK_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SHOCK_OK 0
+#define SHOCK_EINVAL (-1)   /* bad argument or unsupported configuration */
+#define SHOCK_ENOMEM (-2)   /* device allocation or HBM budget exceeded */
+#define SHOCK_ECUDA (-3)    /* CUDA runtime error */
+#define SHOCK_ENAN (-4)     /* non-finite density detected (checkNAN) */
+#define SHOCK_ETIMEOUT (-5) /* a bounded wait ran out */
+#define SHOCK_EBUSY (-6)    /* no free slot (serving) */
+
+#define SHOCK_FP64 0        /* everything in FP64 (reference precision) */
+#define SHOCK_MIXED 1       /* FP32 WENO/viscous stencils, FP64 state/RK/metric/p-T recovery */
+
+/* The config.ini keys the hot path consumes (src/Import.c:36-238) plus the
+ * grid description src/Load.c takes from the CGNS file and .sddc division. */
+typedef struct shock_params {
+    int dim;            /* MESHDIMENSIONS: 2 or 3 */
+    int order;          /* SPACEORDER: 5 or 9 */
+    int ni, nj, nk;     /* real points per axis (nk = 1 in 2D) */
+    int time_order;     /* [Numerics] TimeOrder: 3 (RK3-TVD) or 4 (RK4) */
+    double tau;         /* [Numerics] Tau */
+    double mach;        /* [FluidProperties] Mach */
+    double reynolds;    /* Reynolds */
+    double prandtl;     /* Prandtl */
+    double gamma;       /* Gamma */
+    double gas_r;       /* R */
+    double t0;          /* T */
+    double l0;          /* L */
+    int inviscid;       /* [Options] Inviscid */
+    int mms;            /* [Options] ManufacturedSolution: mu = 1, Dirichlet faces, source term */
+    int periodic[3];    /* periodic self-interface per axis (.sddc) */
+    double period[3];   /* periodic Translation per axis (stored as float32 like src/Load.c:110) */
+    int precision;      /* SHOCK_FP64 or SHOCK_MIXED */
+    int zeta_fix;       /* 0: reproduce src/ZD.c:547-548 (zeta viscous stencil centred on j); 1: centred on k */
+} shock_params;
+
+typedef struct shock_ctx shock_ctx;
+
+const char *shock_last_error(void);
+int shock_device_count(int *n);
+
+/* Create a solver for one block.  x,y,z and the primitives u,v,w,p,rho are
+ * real points in Fortran order (what loadFile returns, src/Load.c:252-744);
+ * e is formed from p as src/Functions.c:872-874 does.  Replaces SHOCK's
+ * set-up chain postprocessLoad -> ExtrapolateGhostCells -> TransferMesh ->
+ * CreateMetric -> TransferMesh -> CreateViscidMetric (src/SHOCK.c:138-223). */
+int shock_create(const shock_params *p, const double *x, const double *y, const double *z,
+                 const double *u, const double *v, const double *w, const double *pr,
+                 const double *rho, int device, shock_ctx **out);
+int shock_destroy(shock_ctx *ctx);
+
+/* Ghosted sizes NIg,NJg,NKg and first real index per axis. */
+int shock_dims(const shock_ctx *ctx, int out6[6]);
+
+/* Manufactured-solution Dirichlet faces: the exact rho,u,v,w,e on every
+ * ghosted point (9*NG doubles: rho,u,v,w,e,p,T,c,mue; only the first five
+ * are used).  Replaces InitializeManufacturedSolution /
+ * WriteBCManufacturedSolution* (src/ManufacturedSolution.c:177-338). */
+int shock_set_dirichlet(shock_ctx *ctx, const double *exact9);
+
+/* Time-independent source J*S added to Q each stage, 5*NG doubles (real
+ * points used).  Replaces AddManufacturedSolutionSource
+ * (src/ManufacturedSolution.c:25-175); the caller evaluates S once. */
+int shock_set_source(shock_ctx *ctx, const double *js5);
+
+/* Host <-> device state (rho,u,v,w,e; 5*NG doubles, ghosted).
+ * which = 0: U_RK (the running state), 1: U_lastStep. */
+int shock_upload_state(shock_ctx *ctx, const double *prim5);
+int shock_download_state(shock_ctx *ctx, double *prim5, int which);
+
+/* One right-hand side at the current state, in CalcRungeKutta's stage
+ * order without the RK update (src/Functions.c:2111-2293); q5 = 5*NG
+ * doubles (real points written, ghosts zero). */
+int shock_rhs(shock_ctx *ctx, double *q5);
+
+/* nsteps full time steps on the device (src/Functions.c:2034-2390 called
+ * by startSimulation, src/SHOCK.c:557-663).  The state stays resident. */
+int shock_step(shock_ctx *ctx, int nsteps);
+
+/* Same as shock_step, asynchronous on the context's stream (captured as a
+ * CUDA graph after the first call). */
+int shock_step_async(shock_ctx *ctx, int nsteps);
+int shock_sync(shock_ctx *ctx);
+
+/* NaN/Inf scan of rho over the real points (src/Functions.c:5419-5467);
+ * *bad receives the count.  Returns SHOCK_ENAN when bad > 0. */
+int shock_check_nan(shock_ctx *ctx, int *bad);
+
+/* Geometry after set-up: x,y,z,J,xi_x..zeta_z (13*NG doubles). */
+int shock_geometry(shock_ctx *ctx, double *out13);
+
+/* Device bytes held by the context. */
+int shock_device_bytes(const shock_ctx *ctx, size_t *bytes);
+
+/* Time (ms, CUDA events on the context stream) of the last shock_step /
+ * shock_step_async batch. */
+int shock_last_step_ms(shock_ctx *ctx, float *ms);
+
+/* The launch list of one stage: number of kernels per stage and the
+ * kernel that dominates (name written to buf). */
+int shock_kernels_per_step(const shock_ctx *ctx, int *n);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

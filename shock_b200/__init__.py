@@ -1,0 +1,208 @@
+"""shock_b200: SHOCK's per-RK-stage right-hand side on a B200.
+
+Python host side over the C ABI in include/shock_b200.h
+(shock_b200/libshock_b200.so, built from shock_b200/csrc for sm_100a).
+
+``Solver`` mirrors SHOCK's solver entry points for one block:
+set-up from a grid and initial state (SHOCK.c:main up to startSimulation),
+``rhs()`` (one stage right-hand side, the pieces CalcRungeKutta calls),
+``steps(n)`` (n calls of CalcRungeKutta, src/Functions.c:2034-2390, with
+the state kept on the device) and state download (the U_RK arrays).
+
+There is no CPU fallback: constructing a Solver without the compiled
+library or without a CUDA device raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+from . import cases  # noqa: F401
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libshock_b200.so")
+
+SHOCK_FP64 = 0
+SHOCK_MIXED = 1
+
+_lib = None
+_lock = threading.Lock()
+
+_dp = C.POINTER(C.c_double)
+
+
+class ShockError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"shock_b200 error {code}: {msg}")
+        self.code = code
+
+
+class Params(C.Structure):
+    """Mirror of struct shock_params (include/shock_b200.h)."""
+    _fields_ = [
+        ("dim", C.c_int), ("order", C.c_int),
+        ("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int),
+        ("time_order", C.c_int),
+        ("tau", C.c_double), ("mach", C.c_double), ("reynolds", C.c_double),
+        ("prandtl", C.c_double), ("gamma", C.c_double), ("gas_r", C.c_double),
+        ("t0", C.c_double), ("l0", C.c_double),
+        ("inviscid", C.c_int), ("mms", C.c_int),
+        ("periodic", C.c_int * 3), ("period", C.c_double * 3),
+        ("precision", C.c_int), ("zeta_fix", C.c_int),
+    ]
+
+
+def build_library(force: bool = False) -> str:
+    """Compile shock_b200/csrc into libshock_b200.so (nvcc, sm_100a)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "csrc")], check=True)
+    return LIB_PATH
+
+
+def lib():
+    """Load the compiled library (building it if it is missing)."""
+    global _lib
+    with _lock:
+        if _lib is None:
+            if not os.path.exists(LIB_PATH):
+                build_library()
+            L = C.CDLL(LIB_PATH)
+            L.shock_last_error.restype = C.c_char_p
+            L.shock_create.argtypes = [C.POINTER(Params)] + [_dp] * 8 + [C.c_int, C.POINTER(C.c_void_p)]
+            for name in ("shock_destroy", "shock_dims", "shock_set_dirichlet", "shock_set_source",
+                         "shock_upload_state", "shock_download_state", "shock_rhs", "shock_step",
+                         "shock_step_async", "shock_sync", "shock_check_nan", "shock_geometry",
+                         "shock_device_bytes", "shock_last_step_ms", "shock_kernels_per_step"):
+                getattr(L, name).restype = C.c_int
+            _lib = L
+        return _lib
+
+
+def _check(rc):
+    if rc != 0:
+        raise ShockError(rc, lib().shock_last_error().decode())
+
+
+def _ptr(a):
+    assert a.dtype == np.float64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_dp)
+
+
+def params_from_case(case, precision=SHOCK_FP64, zeta_fix=False) -> Params:
+    p = Params()
+    p.dim, p.order = case.dim, case.order
+    p.ni, p.nj, p.nk = case.ni, case.nj, (case.nk if case.dim == 3 else 1)
+    p.time_order = case.time_order
+    p.tau, p.mach, p.reynolds = case.tau, case.mach, case.reynolds
+    p.prandtl, p.gamma, p.gas_r, p.t0, p.l0 = case.prandtl, case.gamma, case.gas_r, case.t0, case.l0
+    p.inviscid = int(case.inviscid)
+    p.mms = 0 if case.mms == "none" else 1
+    for a in range(3):
+        p.periodic[a] = int(case.periodic[a])
+        p.period[a] = float(case.period[a])
+    p.precision = int(precision)
+    p.zeta_fix = int(bool(zeta_fix))
+    return p
+
+
+class Solver:
+    """One block of SHOCK's stage right-hand side on a CUDA device."""
+
+    def __init__(self, case, precision=SHOCK_FP64, device: int = 0, zeta_fix: bool = False,
+                 dirichlet9=None, source5=None):
+        self.case = case
+        self.lib = lib()
+        self.params = params_from_case(case, precision, zeta_fix)
+        f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
+        arrs = [f(a) for a in case.real_fields()]
+        h = C.c_void_p()
+        _check(self.lib.shock_create(C.byref(self.params), *[_ptr(a) for a in arrs], int(device), C.byref(h)))
+        self.h = h
+        d = (C.c_int * 6)()
+        _check(self.lib.shock_dims(self.h, d))
+        self.shape = (d[0], d[1], d[2])
+        self.start = (d[3], d[4], d[5])
+        self.n = d[0] * d[1] * d[2]
+        if dirichlet9 is not None:
+            a = np.ascontiguousarray(dirichlet9, np.float64).ravel()
+            assert a.size == 9 * self.n
+            _check(self.lib.shock_set_dirichlet(self.h, _ptr(a)))
+        if source5 is not None:
+            a = np.ascontiguousarray(source5, np.float64).ravel()
+            assert a.size == 5 * self.n
+            _check(self.lib.shock_set_source(self.h, _ptr(a)))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.shock_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def rhs(self) -> np.ndarray:
+        q = np.zeros(5 * self.n)
+        _check(self.lib.shock_rhs(self.h, _ptr(q)))
+        return q.reshape((5,) + self.shape)
+
+    def steps(self, n: int):
+        _check(self.lib.shock_step(self.h, C.c_int(n)))
+
+    def steps_async(self, n: int):
+        _check(self.lib.shock_step_async(self.h, C.c_int(n)))
+
+    def sync(self):
+        _check(self.lib.shock_sync(self.h))
+
+    def last_ms(self) -> float:
+        v = C.c_float()
+        _check(self.lib.shock_last_step_ms(self.h, C.byref(v)))
+        return v.value
+
+    def state(self) -> np.ndarray:
+        """rho,u,v,w,e (ghosted)."""
+        s = np.zeros(5 * self.n)
+        _check(self.lib.shock_download_state(self.h, _ptr(s), 0))
+        return s.reshape((5,) + self.shape)
+
+    def set_state(self, prim5):
+        a = np.ascontiguousarray(prim5, np.float64).ravel()
+        assert a.size == 5 * self.n
+        _check(self.lib.shock_upload_state(self.h, _ptr(a)))
+
+    def geometry(self) -> np.ndarray:
+        g = np.zeros(13 * self.n)
+        _check(self.lib.shock_geometry(self.h, _ptr(g)))
+        return g.reshape((13,) + self.shape)
+
+    def check_nan(self) -> int:
+        bad = C.c_int()
+        rc = self.lib.shock_check_nan(self.h, C.byref(bad))
+        if rc not in (0, -4):
+            _check(rc)
+        return bad.value
+
+    def device_bytes(self) -> int:
+        b = C.c_size_t()
+        _check(self.lib.shock_device_bytes(self.h, C.byref(b)))
+        return b.value
+
+    def kernels_per_step(self) -> int:
+        n = C.c_int()
+        _check(self.lib.shock_kernels_per_step(self.h, C.byref(n)))
+        return n.value
+
+    def real(self, a: np.ndarray) -> np.ndarray:
+        """Real-point view of a ghosted field array (..., NIg, NJg, NKg)."""
+        g = self.start
+        c = self.case
+        if c.dim == 3:
+            return a[..., g[0]:g[0] + c.ni, g[1]:g[1] + c.nj, g[2]:g[2] + c.nk]
+        return a[..., g[0]:g[0] + c.ni, g[1]:g[1] + c.nj, :]

@@ -1,0 +1,409 @@
+// C ABI of shock_b200 (declared in include/shock_b200.h).
+//
+// One shock_ctx holds one block's device state: three rotating buffers of
+// rho,u,v,w,e (U_lastStep and the two running stage states of
+// CalcRungeKutta, src/Functions.c:2034-2390, without the state copy that
+// startSimulation does at src/SHOCK.c:663), Q_sum, Q, the primitive
+// fields, the geometry and the nodal derivatives.  A time step is one
+// CUDA graph of TimeOrder stages; the graph is captured once per buffer
+// rotation and replayed.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "internal.h"
+
+using namespace shock;
+
+namespace {
+
+thread_local std::string g_err;
+
+int fail(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+
+#define CK(call)                                                                                  \
+    do {                                                                                          \
+        cudaError_t e_ = (call);                                                                  \
+        if (e_ != cudaSuccess) return fail(SHOCK_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+    } while (0)
+
+}  // namespace
+
+struct shock_ctx {
+    shock_params p{};
+    Layout L;
+    Grid G{};
+    Phys P{};
+    Fields F{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    double *pool = nullptr;
+    size_t pool_bytes = 0;
+    double *buf[3][5] = {};
+    int un = 0;          // buffer holding U_lastStep (== running state between steps)
+    bool has_source = false;
+    RKCoef rk[4]{};
+    cudaGraphExec_t step_graph[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.f;
+    int kernels_per_step = 0;
+    std::vector<std::vector<double>> geo_host;
+};
+
+static void set_rk(shock_ctx *c)
+{
+    if (c->p.time_order == 4) {
+        const double a[4] = {1., 1., 1., 1.}, b[4] = {0., 0., 0., 0.}, q[4] = {0.5, 0.5, 1., 1. / 6.};
+        const double d[4] = {0., 0., 0., 1. / 6.}, s[4] = {1., 2., 2., 0.};
+        for (int i = 0; i < 4; i++) c->rk[i] = RKCoef{a[i], b[i], q[i], d[i], s[i]};
+    } else {
+        const double a[3] = {1., 3. / 4., 1. / 3.}, b[3] = {0., 1. / 4., 2. / 3.}, q[3] = {1., 1. / 4., 2. / 3.};
+        for (int i = 0; i < 3; i++) c->rk[i] = RKCoef{a[i], b[i], q[i], 0., 0.};
+    }
+}
+
+// Launch the right-hand side of one stage on state `in`.
+static void enqueue_rhs(shock_ctx *c, double *const in[5], int &nk)
+{
+    cudaStream_t s = c->stream;
+    const double *cin[5] = {in[0], in[1], in[2], in[3], in[4]};
+    launch_ghosts(c->G, in, s);
+    nk += (c->G.periodic[0] || c->G.periodic[1] || c->G.periodic[2]) ? 1 : 0;
+    launch_prim(c->G, c->P, cin, c->F, s);
+    nk++;
+    if (!c->p.inviscid) {
+        launch_nodal(c->G, cin, c->F, s);
+        nk++;
+    }
+    for (int d = 0; d < c->p.dim; d++) {
+        launch_weno(c->G, c->P, c->p.precision, d, d == 0, cin, c->F, s);
+        nk++;
+    }
+    if (!c->p.inviscid)
+        for (int d = 0; d < c->p.dim; d++) {
+            launch_viscous(c->G, c->P, c->p.precision, d, cin, c->F, s);
+            nk++;
+        }
+}
+
+static void enqueue_step(shock_ctx *c, int un, int &nk)
+{
+    int cur = un;
+    for (int st = 0; st < c->p.time_order; st++) {
+        int out = 0;
+        while (out == un || out == cur) out++;
+        enqueue_rhs(c, c->buf[cur], nk);
+        const double *cin[5] = {c->buf[cur][0], c->buf[cur][1], c->buf[cur][2], c->buf[cur][3], c->buf[cur][4]};
+        Fields F = c->F;
+        for (int q = 0; q < 5; q++) F.Un[q] = c->buf[un][q];
+        launch_rk(c->G, c->rk[st], c->p.tau, cin, c->buf[out], F, c->has_source, c->stream);
+        nk++;
+        cur = out;
+    }
+}
+
+static int final_buffer(const shock_ctx *c, int un)
+{
+    int cur = un;
+    for (int st = 0; st < c->p.time_order; st++) {
+        int out = 0;
+        while (out == un || out == cur) out++;
+        cur = out;
+    }
+    return cur;
+}
+
+extern "C" {
+
+const char *shock_last_error(void) { return g_err.c_str(); }
+
+int shock_device_count(int *n)
+{
+    CK(cudaGetDeviceCount(n));
+    return SHOCK_OK;
+}
+
+int shock_create(const shock_params *p, const double *x, const double *y, const double *z, const double *u,
+                 const double *v, const double *w, const double *pr, const double *rho, int device, shock_ctx **out)
+{
+    if (!p || !out || !x || !y || !u || !v || !w || !pr || !rho) return fail(SHOCK_EINVAL, "null argument");
+    if (p->dim != 2 && p->dim != 3) return fail(SHOCK_EINVAL, "dim must be 2 or 3");
+    if (p->order != 5 && p->order != 9) return fail(SHOCK_EINVAL, "order must be 5 or 9");
+    if (p->time_order != 3 && p->time_order != 4) return fail(SHOCK_EINVAL, "time_order must be 3 or 4");
+    if (p->precision != SHOCK_FP64 && p->precision != SHOCK_MIXED) return fail(SHOCK_EINVAL, "bad precision");
+    int g = (p->order + 1) / 2;
+    if (p->ni < g + 1 || p->nj < g + 1 || (p->dim == 3 && p->nk < g + 1))
+        return fail(SHOCK_EINVAL, "block smaller than the stencil (%d points per axis needed)", g + 1);
+    if (p->dim == 3 && !z) return fail(SHOCK_EINVAL, "z coordinates missing");
+    if (p->dim == 3 && !p->inviscid && !p->zeta_fix && p->nj > p->nk)
+        return fail(SHOCK_EINVAL, "zeta viscous stencil centred on j needs nj <= nk (src/ZD.c:547-548)");
+    for (int a = 0; a < p->dim; a++)
+        if (!p->periodic[a] && !p->mms)
+            return fail(SHOCK_EINVAL, "axis %d: only periodic or manufactured-solution faces are supported", a);
+    if (p->mach <= 0 || p->reynolds <= 0 || p->gamma <= 1.0 || p->tau <= 0) return fail(SHOCK_EINVAL, "bad physics");
+
+    shock_ctx *c = new shock_ctx();
+    c->p = *p;
+    c->device = device;
+    HostBlock hb;
+    build_block(*p, x, y, z, u, v, w, pr, rho, hb);
+    c->L = hb.L;
+    Grid &G = c->G;
+    G.dim = p->dim; G.order = p->order; G.g = c->L.g;
+    for (int a = 0; a < 3; a++) {
+        G.n[a] = c->L.n[a]; G.N[a] = c->L.N[a]; G.st[a] = c->L.st[a];
+        G.periodic[a] = a < p->dim ? p->periodic[a] : 0;
+    }
+    G.NG = c->L.NG;
+    Phys &P = c->P;
+    P.gamma = p->gamma;
+    P.ups = 1.0 / (p->gamma * (p->mach * p->mach));
+    P.psi = 1.0 / p->reynolds;
+    P.suth = 100.4 / p->t0;
+    P.gam = 1.0 / ((p->gamma - 1.0) * (p->mach * p->mach) * p->reynolds * p->prandtl);
+    P.eps64 = 10. * sqrt(2.2250738585072014e-308);   // 10*sqrt(DBL_MIN), src/Functions.c:1829
+    P.eps32 = 10.f * sqrtf(1.17549435e-38f);          // 10*sqrt(FLT_MIN), the float build's value
+    P.mms = p->mms ? 1 : 0;
+    P.zeta_fix = p->zeta_fix;
+    set_rk(c);
+
+    if (cudaSetDevice(device) != cudaSuccess) { delete c; return fail(SHOCK_ECUDA, "cudaSetDevice(%d)", device); }
+    // field count: 3x5 state, 5 Qs, 5 Q, 4 prim, 10 geometry, 12 nodal
+    const int nfield = 15 + 5 + 5 + 4 + 10 + (p->inviscid ? 0 : 12);
+    c->pool_bytes = sizeof(double) * (size_t)nfield * (size_t)G.NG;
+    if (cudaMalloc(&c->pool, c->pool_bytes) != cudaSuccess) {
+        delete c;
+        return fail(SHOCK_ENOMEM, "cudaMalloc of %zu bytes failed", (size_t)nfield * G.NG * 8);
+    }
+    cudaMemset(c->pool, 0, c->pool_bytes);
+    double *q = c->pool;
+    auto take = [&]() { double *r = q; q += G.NG; return r; };
+    for (int b = 0; b < 3; b++)
+        for (int f = 0; f < 5; f++) c->buf[b][f] = take();
+    for (int f = 0; f < 5; f++) c->F.Qs[f] = take();
+    for (int f = 0; f < 5; f++) c->F.Q[f] = take();
+    c->F.p = take(); c->F.T = take(); c->F.c = take(); c->F.mu = take();
+    c->F.J = take();
+    for (int f = 0; f < 9; f++) c->F.m[f] = take();
+    for (int f = 0; f < 12; f++) c->F.Nd[f] = p->inviscid ? nullptr : take();
+    for (int f = 0; f < 5; f++) c->F.js[f] = nullptr;
+    if (cudaMalloc(&c->F.flag, 64) != cudaSuccess) {
+        cudaFree(c->pool);
+        delete c;
+        return fail(SHOCK_ENOMEM, "flag allocation");
+    }
+    prepare_kernels();
+    cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    cudaEventCreate(&c->ev0);
+    cudaEventCreate(&c->ev1);
+
+    size_t nb = sizeof(double) * G.NG;
+    cudaMemcpy(c->F.J, hb.geo[3].data(), nb, cudaMemcpyHostToDevice);
+    for (int f = 0; f < 9; f++) cudaMemcpy(c->F.m[f], hb.geo[4 + f].data(), nb, cudaMemcpyHostToDevice);
+    for (int b = 0; b < 3; b++)
+        for (int f = 0; f < 5; f++) cudaMemcpy(c->buf[b][f], hb.prim[f].data(), nb, cudaMemcpyHostToDevice);
+    c->geo_host = std::move(hb.geo);
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) {
+        shock_destroy(c);
+        return fail(SHOCK_ECUDA, "set-up upload: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return SHOCK_OK;
+}
+
+int shock_destroy(shock_ctx *c)
+{
+    if (!c) return SHOCK_OK;
+    cudaSetDevice(c->device);
+    for (int i = 0; i < 3; i++)
+        if (c->step_graph[i]) cudaGraphExecDestroy(c->step_graph[i]);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->F.js[0]) cudaFree(c->F.js[0]);
+    if (c->pool) cudaFree(c->pool);
+    if (c->F.flag) cudaFree(c->F.flag);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return SHOCK_OK;
+}
+
+int shock_dims(const shock_ctx *c, int out6[6])
+{
+    if (!c || !out6) return fail(SHOCK_EINVAL, "null argument");
+    for (int a = 0; a < 3; a++) {
+        out6[a] = c->L.N[a];
+        out6[3 + a] = a < c->p.dim ? c->L.g : 0;
+    }
+    return SHOCK_OK;
+}
+
+int shock_set_dirichlet(shock_ctx *c, const double *exact9)
+{
+    if (!c || !exact9) return fail(SHOCK_EINVAL, "null argument");
+    CK(cudaSetDevice(c->device));
+    size_t nb = sizeof(double) * c->G.NG;
+    for (int b = 0; b < 3; b++)
+        for (int f = 0; f < 5; f++)
+            CK(cudaMemcpy(c->buf[b][f], exact9 + (size_t)f * c->G.NG, nb, cudaMemcpyHostToDevice));
+    c->un = 0;
+    return SHOCK_OK;
+}
+
+int shock_set_source(shock_ctx *c, const double *js5)
+{
+    if (!c || !js5) return fail(SHOCK_EINVAL, "null argument");
+    CK(cudaSetDevice(c->device));
+    size_t nb = sizeof(double) * c->G.NG;
+    if (!c->F.js[0]) {
+        double *b;
+        if (cudaMalloc(&b, 5 * nb) != cudaSuccess) return fail(SHOCK_ENOMEM, "source allocation");
+        for (int f = 0; f < 5; f++) c->F.js[f] = b + (size_t)f * c->G.NG;
+        for (int i = 0; i < 3; i++)
+            if (c->step_graph[i]) { cudaGraphExecDestroy(c->step_graph[i]); c->step_graph[i] = nullptr; }
+    }
+    for (int f = 0; f < 5; f++) CK(cudaMemcpy(c->F.js[f], js5 + (size_t)f * c->G.NG, nb, cudaMemcpyHostToDevice));
+    c->has_source = true;
+    return SHOCK_OK;
+}
+
+int shock_upload_state(shock_ctx *c, const double *prim5)
+{
+    if (!c || !prim5) return fail(SHOCK_EINVAL, "null argument");
+    CK(cudaSetDevice(c->device));
+    size_t nb = sizeof(double) * c->G.NG;
+    for (int b = 0; b < 3; b++)
+        for (int f = 0; f < 5; f++)
+            CK(cudaMemcpyAsync(c->buf[b][f], prim5 + (size_t)f * c->G.NG, nb, cudaMemcpyHostToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    c->un = 0;
+    return SHOCK_OK;
+}
+
+int shock_download_state(shock_ctx *c, double *prim5, int which)
+{
+    (void)which;   // between steps U_RK and U_lastStep are the same buffer
+    if (!c || !prim5) return fail(SHOCK_EINVAL, "null argument");
+    CK(cudaSetDevice(c->device));
+    size_t nb = sizeof(double) * c->G.NG;
+    for (int f = 0; f < 5; f++)
+        CK(cudaMemcpyAsync(prim5 + (size_t)f * c->G.NG, c->buf[c->un][f], nb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SHOCK_OK;
+}
+
+int shock_rhs(shock_ctx *c, double *q5)
+{
+    if (!c || !q5) return fail(SHOCK_EINVAL, "null argument");
+    CK(cudaSetDevice(c->device));
+    int nk = 0;
+    enqueue_rhs(c, c->buf[c->un], nk);
+    if (c->has_source) launch_add_source(c->G, c->F, c->stream);
+    CK(cudaGetLastError());
+    size_t nb = sizeof(double) * c->G.NG;
+    for (int f = 0; f < 5; f++)
+        CK(cudaMemcpyAsync(q5 + (size_t)f * c->G.NG, c->F.Q[f], nb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SHOCK_OK;
+}
+
+int shock_step_async(shock_ctx *c, int nsteps)
+{
+    if (!c || nsteps < 0) return fail(SHOCK_EINVAL, "bad argument");
+    CK(cudaSetDevice(c->device));
+    CK(cudaEventRecord(c->ev0, c->stream));
+    for (int it = 0; it < nsteps; it++) {
+        int un = c->un;
+        if (!c->step_graph[un]) {
+            cudaGraph_t gr;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            int nk = 0;
+            for (int q = 0; q < 5; q++) CK(cudaMemsetAsync(c->F.Qs[q], 0, sizeof(double) * c->G.NG, c->stream));
+            enqueue_step(c, un, nk);
+            CK(cudaStreamEndCapture(c->stream, &gr));
+            CK(cudaGraphInstantiate(&c->step_graph[un], gr, 0));
+            cudaGraphDestroy(gr);
+            c->kernels_per_step = nk;
+        }
+        CK(cudaGraphLaunch(c->step_graph[un], c->stream));
+        c->un = final_buffer(c, un);
+    }
+    CK(cudaEventRecord(c->ev1, c->stream));
+    return SHOCK_OK;
+}
+
+int shock_sync(shock_ctx *c)
+{
+    if (!c) return fail(SHOCK_EINVAL, "null argument");
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaGetLastError());
+    cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1);
+    return SHOCK_OK;
+}
+
+int shock_step(shock_ctx *c, int nsteps)
+{
+    int rc = shock_step_async(c, nsteps);
+    if (rc) return rc;
+    return shock_sync(c);
+}
+
+int shock_check_nan(shock_ctx *c, int *bad)
+{
+    if (!c || !bad) return fail(SHOCK_EINVAL, "null argument");
+    CK(cudaSetDevice(c->device));
+    CK(cudaMemsetAsync(c->F.flag, 0, sizeof(unsigned), c->stream));
+    launch_nan_check(c->G, c->buf[c->un][0], c->F.flag, c->stream);
+    unsigned h = 0;
+    CK(cudaMemcpyAsync(&h, c->F.flag, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *bad = (int)h;
+    return h ? fail(SHOCK_ENAN, "%u non-finite densities", h) : SHOCK_OK;
+}
+
+int shock_geometry(shock_ctx *c, double *out13)
+{
+    if (!c || !out13) return fail(SHOCK_EINVAL, "null argument");
+    for (int f = 0; f < 13; f++)
+        memcpy(out13 + (size_t)f * c->G.NG, c->geo_host[f].data(), sizeof(double) * c->G.NG);
+    return SHOCK_OK;
+}
+
+int shock_device_bytes(const shock_ctx *c, size_t *bytes)
+{
+    if (!c || !bytes) return fail(SHOCK_EINVAL, "null argument");
+    *bytes = c->pool_bytes + (c->F.js[0] ? 5 * sizeof(double) * c->G.NG : 0);
+    return SHOCK_OK;
+}
+
+int shock_last_step_ms(shock_ctx *c, float *ms)
+{
+    if (!c || !ms) return fail(SHOCK_EINVAL, "null argument");
+    *ms = c->last_ms;
+    return SHOCK_OK;
+}
+
+int shock_kernels_per_step(const shock_ctx *c, int *n)
+{
+    if (!c || !n) return fail(SHOCK_EINVAL, "null argument");
+    *n = c->kernels_per_step;
+    return SHOCK_OK;
+}
+
+}  // extern "C"

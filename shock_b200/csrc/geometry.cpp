@@ -1,0 +1,217 @@
+// Host-side block set-up: ghost coordinates, metric, Jacobian, initial state.
+//
+// Runs once per block in FP64 on the CPU and must reproduce SHOCK's set-up
+// chain value for value, because the stage kernels consume its output and
+// parity is judged against SHOCK's own results:
+//   postprocessLoad        src/Functions.c:26-898   (ranges, initial state)
+//   ExtrapolateGhostCells  src/Functions.c:6511-6848
+//   TransferMeshParameter  src/Functions.c:3481-3578 (periodic images,
+//                          Translation as float32, src/Load.c:110)
+//   CreateMetric           src/Functions.c:6388-6509 (3D cross terms zeroed)
+// This file is compiled without FMA contraction (see the Makefile).
+#include "internal.h"
+
+#include <cstring>
+
+namespace shock {
+
+namespace {
+
+struct Box {
+    int sr[3], er[3], eg[3];
+    long long st[3];
+    long long at(int i, int j, int k) const { return i * st[0] + j * st[1] + k; }
+};
+
+// Six face loops in SHOCK's order (Left, Right, Bottom, Top, Behind,
+// InFront): each ghost layer is the neighbour layer plus the mirrored
+// spacing of the interior, x[g] = x[g+1] + x[s] - x[s+1].
+void extrapolate(std::vector<double> &f, const Box &b, int dim)
+{
+    auto E = [&](int i, int j, int k) -> double & { return f[b.at(i, j, k)]; };
+    int s = b.sr[0];
+    for (int i = b.sr[0] - 1; i >= 0; i--, s++)
+        for (int j = b.sr[1]; j <= b.er[1]; j++)
+            for (int k = b.sr[2]; k <= b.er[2]; k++) E(i, j, k) = E(i + 1, j, k) + E(s, j, k) - E(s + 1, j, k);
+    s = b.er[0];
+    for (int i = b.er[0] + 1; i <= b.eg[0]; i++, s--)
+        for (int j = b.sr[1]; j <= b.er[1]; j++)
+            for (int k = b.sr[2]; k <= b.er[2]; k++) E(i, j, k) = E(i - 1, j, k) + E(s, j, k) - E(s - 1, j, k);
+    for (int i = 0; i <= b.eg[0]; i++) {
+        s = b.sr[1];
+        for (int j = b.sr[1] - 1; j >= 0; j--, s++)
+            for (int k = b.sr[2]; k <= b.er[2]; k++) E(i, j, k) = E(i, j + 1, k) + E(i, s, k) - E(i, s + 1, k);
+    }
+    for (int i = 0; i <= b.eg[0]; i++) {
+        s = b.er[1];
+        for (int j = b.er[1] + 1; j <= b.eg[1]; j++, s--)
+            for (int k = b.sr[2]; k <= b.er[2]; k++) E(i, j, k) = E(i, j - 1, k) + E(i, s, k) - E(i, s - 1, k);
+    }
+    if (dim == 3) {
+        for (int i = 0; i <= b.eg[0]; i++)
+            for (int j = 0; j <= b.eg[1]; j++) {
+                s = b.sr[2];
+                for (int k = b.sr[2] - 1; k >= 0; k--, s++) E(i, j, k) = E(i, j, k + 1) + E(i, j, s) - E(i, j, s + 1);
+                s = b.er[2];
+                for (int k = b.er[2] + 1; k <= b.eg[2]; k++, s--) E(i, j, k) = E(i, j, k - 1) + E(i, j, s) - E(i, j, s - 1);
+            }
+    }
+}
+
+}  // namespace
+
+// Periodic image copy over the ghost-inclusive slab of every periodic axis;
+// the first ncoord fields are coordinates and receive the axis Translation
+// rounded to float32.
+void periodic_images(const Layout &L, const shock_params &p, double **f, int nf, int ncoord)
+{
+    int idx[3], src[3];
+    for (int a = 0; a < p.dim; a++) {
+        if (!p.periodic[a]) continue;
+        int n = L.n[a];
+        float tr = (float)p.period[a];
+        for (idx[0] = 0; idx[0] < L.N[0]; idx[0]++)
+            for (idx[1] = 0; idx[1] < L.N[1]; idx[1]++)
+                for (idx[2] = 0; idx[2] < L.N[2]; idx[2]++) {
+                    int gi = idx[a];
+                    if (gi >= L.g && gi < L.g + n) continue;
+                    float t;
+                    src[0] = idx[0]; src[1] = idx[1]; src[2] = idx[2];
+                    if (gi < L.g) { src[a] = gi + n; t = -tr; }
+                    else { src[a] = gi - n; t = tr; }
+                    long long d = L.at(idx[0], idx[1], idx[2]), o = L.at(src[0], src[1], src[2]);
+                    for (int q = 0; q < nf; q++) {
+                        double v = f[q][o];
+                        if (q < ncoord) v = v + (q == a ? t : 0.0f);
+                        f[q][d] = v;
+                    }
+                }
+    }
+}
+
+int build_block(const shock_params &p, const double *x, const double *y, const double *z,
+                const double *u, const double *v, const double *w, const double *pr,
+                const double *rho, HostBlock &hb)
+{
+    const int dim = p.dim;
+    Layout &L = hb.L;
+    L.init(p);
+    const long long NG = L.NG;
+    hb.geo.assign(13, std::vector<double>(NG, 0.0));
+    hb.prim.assign(5, std::vector<double>(NG, 0.0));
+    std::vector<double> &X = hb.geo[0], &Y = hb.geo[1], &Z = hb.geo[2];
+    const double ups = 1.0 / (p.gamma * (p.mach * p.mach));
+    const double gm = p.gamma;
+
+    // Initialize (src/Functions.c:1327-1353): rho0 = 1, u = v = w = 0, p0 = 1 on every point.
+    for (long long o = 0; o < NG; o++) {
+        hb.prim[0][o] = 1.0;
+        hb.prim[4][o] = (0.5 * ((0.0 * 0.0) + (0.0 * 0.0) + (0.0 * 0.0)) + 1.0 / 1.0 / (gm - 1.0) * ups);
+    }
+    // Real points from Fortran order (src/Functions.c:746-877).
+    for (int k = 0; k < (dim == 3 ? p.nk : 1); k++)
+        for (int j = 0; j < p.nj; j++)
+            for (int i = 0; i < p.ni; i++) {
+                size_t f = ((size_t)k * p.nj + j) * p.ni + i;
+                long long o = L.at(i + L.g, j + L.g, dim == 3 ? k + L.g : 0);
+                X[o] = x[f];
+                Y[o] = y[f];
+                Z[o] = dim == 3 ? z[f] : 0.0;
+                hb.prim[0][o] = rho[f];
+                hb.prim[1][o] = u[f];
+                hb.prim[2][o] = v[f];
+                hb.prim[3][o] = w[f];
+                hb.prim[4][o] = (0.5 * ((u[f] * u[f]) + (v[f] * v[f]) + (w[f] * w[f])) + pr[f] / rho[f] / (gm - 1.0) * ups);
+            }
+
+    Box b;
+    for (int a = 0; a < 3; a++) {
+        b.sr[a] = a < dim ? L.g : 0;
+        b.er[a] = a < dim ? L.g + L.n[a] - 1 : 0;
+        b.eg[a] = L.N[a] - 1;
+        b.st[a] = L.st[a];
+    }
+    extrapolate(X, b, dim);
+    extrapolate(Y, b, dim);
+    if (dim == 3) extrapolate(Z, b, dim);
+
+    // +1 extended grid (the *_extrapolate arrays, src/Functions.c:6690-6848).
+    Box e;
+    int NE[3];
+    for (int a = 0; a < 3; a++) NE[a] = a < dim ? L.N[a] + 2 : 1;
+    e.st[0] = (long long)NE[1] * NE[2]; e.st[1] = NE[2]; e.st[2] = 1;
+    for (int a = 0; a < 3; a++) {
+        e.sr[a] = a < dim ? b.sr[a] + 1 : 0;
+        e.er[a] = a < dim ? b.er[a] + 1 : 0;
+        e.eg[a] = a < dim ? b.eg[a] + 2 : 0;
+    }
+    const long long NEtot = (long long)NE[0] * NE[1] * NE[2];
+    std::vector<double> xe(NEtot, 0.0), ye(NEtot, 0.0), ze(NEtot, 0.0);
+    auto copy_ext = [&]() {
+        for (int i = 0; i < L.N[0]; i++)
+            for (int j = 0; j < L.N[1]; j++)
+                for (int k = 0; k < L.N[2]; k++) {
+                    long long ee = e.at(i + 1, j + 1, dim == 3 ? k + 1 : 0), o = L.at(i, j, k);
+                    xe[ee] = X[o]; ye[ee] = Y[o]; ze[ee] = Z[o];
+                }
+    };
+    copy_ext();
+    extrapolate(xe, e, dim);
+    extrapolate(ye, e, dim);
+    if (dim == 3) extrapolate(ze, e, dim);
+
+    double *gf[13] = {X.data(), Y.data(), Z.data(), hb.geo[4].data(), hb.geo[5].data(), hb.geo[6].data(),
+                      hb.geo[7].data(), hb.geo[8].data(), hb.geo[9].data(), hb.geo[10].data(),
+                      hb.geo[11].data(), hb.geo[12].data(), hb.geo[3].data()};
+    for (int r = 0; r < dim; r++) periodic_images(L, p, gf, 13, 3);
+
+    // CreateMetric on the extended grid.
+    copy_ext();
+    std::vector<double> &J = hb.geo[3];
+    for (int i = 0; i < L.N[0]; i++)
+        for (int j = 0; j < L.N[1]; j++)
+            for (int k = 0; k < L.N[2]; k++) {
+                int ie = i + 1, je = j + 1, ke = dim == 3 ? k + 1 : 0;
+                double x_xi = (-0.5 * xe[e.at(ie - 1, je, ke)] + 0.5 * xe[e.at(ie + 1, je, ke)]);
+                double y_xi = (-0.5 * ye[e.at(ie - 1, je, ke)] + 0.5 * ye[e.at(ie + 1, je, ke)]);
+                double x_eta = (-0.5 * xe[e.at(ie, je - 1, ke)] + 0.5 * xe[e.at(ie, je + 1, ke)]);
+                double y_eta = (-0.5 * ye[e.at(ie, je - 1, ke)] + 0.5 * ye[e.at(ie, je + 1, ke)]);
+                double z_xi, z_eta, x_zeta, y_zeta, z_zeta;
+                if (dim == 2) {
+                    z_xi = 0.0; z_eta = 0.0; x_zeta = 0.0; y_zeta = 0.0; z_zeta = 1.0;
+                } else {
+                    z_zeta = (-0.5 * ze[e.at(ie, je, ke - 1)] + 0.5 * ze[e.at(ie, je, ke + 1)]);
+                    y_xi = 0.0; z_xi = 0.0; x_eta = 0.0; z_eta = 0.0; x_zeta = 0.0; y_zeta = 0.0;
+                }
+                long long o = L.at(i, j, k);
+                double Jv = x_xi * y_eta * z_zeta + x_eta * y_zeta * z_xi + x_zeta * y_xi * z_eta
+                            - x_zeta * y_eta * z_xi - x_eta * y_xi * z_zeta - x_xi * y_zeta * z_eta;
+                J[o] = Jv;
+                hb.geo[4][o] = (y_eta * z_zeta - y_zeta * z_eta) / Jv;
+                hb.geo[5][o] = (x_zeta * z_eta - x_eta * z_zeta) / Jv;
+                hb.geo[6][o] = (x_eta * y_zeta - x_zeta * y_eta) / Jv;
+                hb.geo[7][o] = (y_zeta * z_xi - y_xi * z_zeta) / Jv;
+                hb.geo[8][o] = (x_xi * z_zeta - x_zeta * z_xi) / Jv;
+                hb.geo[9][o] = (x_zeta * y_xi - x_xi * y_zeta) / Jv;
+                hb.geo[10][o] = (y_xi * z_eta - y_eta * z_xi) / Jv;
+                hb.geo[11][o] = (x_eta * z_xi - x_xi * z_eta) / Jv;
+                hb.geo[12][o] = (x_xi * y_eta - x_eta * y_xi) / Jv;
+            }
+    for (int r = 0; r < dim; r++) periodic_images(L, p, gf, 13, 3);
+    return 0;
+}
+
+void Layout::init(const shock_params &p)
+{
+    dim = p.dim;
+    order = p.order;
+    g = (p.order + 1) / 2;
+    n[0] = p.ni; n[1] = p.nj; n[2] = p.dim == 3 ? p.nk : 1;
+    for (int a = 0; a < 3; a++) N[a] = a < p.dim ? n[a] + p.order + 1 : 1;
+    st[0] = (long long)N[1] * N[2];
+    st[1] = N[2];
+    st[2] = 1;
+    NG = (long long)N[0] * N[1] * N[2];
+}
+
+}  // namespace shock

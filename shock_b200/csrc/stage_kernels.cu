@@ -1,0 +1,941 @@
+// sm_100a kernels for one RK stage of SHOCK's right-hand side.
+//
+// Stage pipeline (one launch each, captured in a CUDA graph per step):
+//   ghosts   periodic image copy of rho,u,v,w,e     src/Functions.c:3580-3684
+//   prim     p, T, c, mu on every ghosted point       src/Functions.c:2392-2481
+//   nodal    nodal velocity/temperature derivatives   src/ZD.c:697-810
+//   weno_d   inviscid WENO flux difference, d=xi,eta,zeta  src/WENO.c:206-1083
+//   visc_d   central viscous flux difference, d=xi,eta,zeta src/ZD.c:47-694
+//   rk       RK stage update of the real points       src/Functions.c:2300-2365
+//
+// The sweep kernels (weno_d, visc_d) stage one tile of line segments in
+// shared memory: 32 lines side by side along the fastest non-sweep axis
+// (coalesced loads), TL cells along the sweep axis plus the stencil halo.
+// One thread computes one face flux; the face fluxes of the tile are then
+// differenced per cell, so every face is evaluated once per tile and the
+// characteristic 5x5 projections stay in registers.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+
+#include "internal.h"
+
+namespace shock {
+
+#define SHOCK_CHECK_LAUNCH() (void)0
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+struct Idx3 {
+    int v[3];
+};
+
+__device__ __forceinline__ Idx3 unflatten(const Grid &G, long long o)
+{
+    Idx3 r;
+    r.v[0] = (int)(o / G.st[0]);
+    long long rem = o - (long long)r.v[0] * G.st[0];
+    r.v[1] = (int)(rem / G.st[1]);
+    r.v[2] = (int)(rem - (long long)r.v[1] * G.st[1]);
+    return r;
+}
+
+__device__ __forceinline__ bool is_real(const Grid &G, int a, int i) { return i >= G.g && i < G.g + G.n[a]; }
+
+// ---------------------------------------------------------------------------
+// ghosts: periodic images over the ghost shell (all periodic axes at once;
+// equivalent to SHOCK's repeated slab exchange).
+// ---------------------------------------------------------------------------
+__global__ void k_ghosts(Grid G, double *r, double *u, double *v, double *w, double *e)
+{
+    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (o >= G.NG) return;
+    Idx3 p = unflatten(G, o);
+    Idx3 s = p;
+    bool ghost = false;
+    for (int a = 0; a < G.dim; a++) {
+        if (!G.periodic[a]) continue;
+        int i = p.v[a];
+        if (i < G.g) { s.v[a] = i + G.n[a]; ghost = true; }
+        else if (i >= G.g + G.n[a]) { s.v[a] = i - G.n[a]; ghost = true; }
+    }
+    if (!ghost) return;
+    long long q = s.v[0] * G.st[0] + s.v[1] * G.st[1] + s.v[2];
+    r[o] = r[q];
+    u[o] = u[q];
+    v[o] = v[q];
+    w[o] = w[q];
+    e[o] = e[q];
+}
+
+// ---------------------------------------------------------------------------
+// prim: CalcValues (p with fabs, T = |p/rho|, c, Sutherland mu or mu = 1).
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void k_prim(Grid G, Phys P, const double *__restrict__ R, const double *__restrict__ U,
+                       const double *__restrict__ V, const double *__restrict__ W,
+                       const double *__restrict__ E, double *p, double *T, double *c, double *mu)
+{
+    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (o >= G.NG) return;
+    double rho = R[o], u = U[o], v = V[o], e = E[o];
+    double q2 = (u * u) + (v * v);
+    if (DIM == 3) {
+        double w = W[o];
+        q2 = q2 + (w * w);
+    }
+    double pp = fabs(rho * (P.gamma - 1.0) / P.ups * (e - 0.5 * q2));
+    double pr = pp / rho;
+    p[o] = pp;
+    T[o] = fabs(pr);
+    c[o] = sqrt(P.ups * P.gamma * pp / rho);
+    mu[o] = P.mms ? 1.0 : ((1.0 + P.suth) * pow(pr, 1.5) / (pr + P.suth));
+}
+
+// ---------------------------------------------------------------------------
+// nodal derivatives (6th / 10th order central, src/Functions.c:1936-1942 /
+// :1884-1894), each direction on the points that are real along it.
+// 3D needs u,v,w; 2D u,v,T (its metric has cross terms).
+// ---------------------------------------------------------------------------
+template <int ORDER>
+struct ZD;
+template <>
+struct ZD<5> {
+    static constexpr int H = 3;
+    __device__ static double node(int l)
+    {
+        const double c[7] = {-1. / 60., 3. / 20., -3. / 4., 0., 3. / 4., -3. / 20., 1. / 60.};
+        return c[l];
+    }
+    __device__ static double half(int l)
+    {
+        const double c[6] = {-1. / 90., 25. / 180., -245. / 180., 245. / 180., -25. / 180., 1. / 90.};
+        return c[l];
+    }
+    __device__ static double interp(int l)
+    {
+        const double c[6] = {1. / 60., -8. / 60., 37. / 60., 37. / 60., -8. / 60., 1. / 60.};
+        return c[l];
+    }
+};
+template <>
+struct ZD<9> {
+    static constexpr int H = 5;
+    __device__ static double node(int l)
+    {
+        const double c[11] = {-1. / 1260., 25. / 2520., -150. / 2520., 600. / 2520., -2100. / 2520., 0.,
+                              2100. / 2520., -600. / 2520., 150. / 2520., -25. / 2520., 1. / 1260.};
+        return c[l];
+    }
+    __device__ static double half(int l)
+    {
+        const double c[10] = {-3. / 9450., 351. / 75600., -2649. / 75600., 15351. / 75600., -110649. / 75600.,
+                              110649. / 75600., -15351. / 75600., 2649. / 75600., -351. / 75600., 3. / 9450.};
+        return c[l];
+    }
+    __device__ static double interp(int l)
+    {
+        const double c[10] = {1. / 1260., -23. / 2520., 127. / 2520., -473. / 2520., 1627. / 2520.,
+                              1627. / 2520., -473. / 2520., 127. / 2520., -23. / 2520., 1. / 1260.};
+        return c[l];
+    }
+};
+
+template <int DIM, int ORDER>
+__global__ void k_nodal(Grid G, const double *__restrict__ U, const double *__restrict__ V,
+                        const double *__restrict__ W, const double *__restrict__ T, Fields F)
+{
+    constexpr int H = ZD<ORDER>::H;
+    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (o >= G.NG) return;
+    Idx3 p = unflatten(G, o);
+    const double *var[4] = {U, V, W, T};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        if (!is_real(G, d, p.v[d])) continue;
+        long long sd = G.st[d];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (DIM == 3 && q == 3) continue;   // T derivatives unused with the diagonal 3D metric
+            if (DIM == 2 && q == 2) continue;   // no w in 2D
+            double acc = 0.0;
+#pragma unroll
+            for (int l = 0; l <= 2 * H; l++) acc += ZD<ORDER>::node(l) * var[q][o + (l - H) * sd];
+            F.Nd[3 * q + d][o] = acc;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// WENO reconstruction weights (src/WENO.c:11-204).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T phi_w5(const T *d, T eps)
+{
+    T is0 = T(13.) * (d[0] - d[1]) * (d[0] - d[1]) + T(3.) * (d[0] - T(3.) * d[1]) * (d[0] - T(3.) * d[1]);
+    T is1 = T(13.) * (d[1] - d[2]) * (d[1] - d[2]) + T(3.) * (d[1] + d[2]) * (d[1] + d[2]);
+    T is2 = T(13.) * (d[2] - d[3]) * (d[2] - d[3]) + T(3.) * (T(3.) * d[2] - d[3]) * (T(3.) * d[2] - d[3]);
+    T a0 = (is0 + eps) * (is0 + eps), a1 = (is1 + eps) * (is1 + eps), a2 = (is2 + eps) * (is2 + eps);
+    T o0t = T(1.) / a0, o1t = T(6.) / a1, o2t = T(3.) / a2;
+    T s = o0t + o1t + o2t;
+    T o0 = o0t / s, o2 = o2t / s;
+    T q1 = d[0] - T(2.) * d[1] + d[2];
+    T q2 = d[1] - T(2.) * d[2] + d[3];
+    return T(1. / 3.) * o0 * q1 + T(1. / 6.) * (o2 - T(0.5)) * q2;
+}
+
+// WENO9 smoothness-indicator quadratic forms (src/WENO.c:25-53), stored
+// as the upper triangle per sub-stencil.
+__constant__ double c_w9is[5][15] = {
+    {22658., -208501., 364863., -288007., 86329., 482963., -1704396., 1358458., -411487., 1521393., -2462076., 758823., 1020563., -649501., 107918.},
+    {6908., -60871., 99213., -70237., 18079., 138563., -464976., 337018., -88297., 406293., -611976., 165153., 242723., -140251., 22658.},
+    {6908., -51001., 67923., -38947., 8209., 104963., -299076., 179098., -38947., 231153., -299076., 67923., 104963., -51001., 6908.},
+    {22658., -140251., 165153., -88297., 18079., 242723., -611976., 337018., -70237., 406293., -464976., 99213., 138563., -60871., 6908.},
+    {107918., -649501., 758823., -411487., 86329., 1020563., -2462076., 1358458., -288007., 1521393., -1704396., 364863., 482963., -208501., 22658.},
+};
+__constant__ float c_w9is_f[5][15] = {
+    {22658.f, -208501.f, 364863.f, -288007.f, 86329.f, 482963.f, -1704396.f, 1358458.f, -411487.f, 1521393.f, -2462076.f, 758823.f, 1020563.f, -649501.f, 107918.f},
+    {6908.f, -60871.f, 99213.f, -70237.f, 18079.f, 138563.f, -464976.f, 337018.f, -88297.f, 406293.f, -611976.f, 165153.f, 242723.f, -140251.f, 22658.f},
+    {6908.f, -51001.f, 67923.f, -38947.f, 8209.f, 104963.f, -299076.f, 179098.f, -38947.f, 231153.f, -299076.f, 67923.f, 104963.f, -51001.f, 6908.f},
+    {22658.f, -140251.f, 165153.f, -88297.f, 18079.f, 242723.f, -611976.f, 337018.f, -70237.f, 406293.f, -464976.f, 99213.f, 138563.f, -60871.f, 6908.f},
+    {107918.f, -649501.f, 758823.f, -411487.f, 86329.f, 1020563.f, -2462076.f, 1358458.f, -288007.f, 1521393.f, -1704396.f, 364863.f, 482963.f, -208501.f, 22658.f},
+};
+
+template <typename T>
+__device__ __forceinline__ T w9c(int k, int i);
+template <>
+__device__ __forceinline__ double w9c<double>(int k, int i) { return c_w9is[k][i]; }
+template <>
+__device__ __forceinline__ float w9c<float>(int k, int i) { return c_w9is_f[k][i]; }
+
+// f: 9 stencil values, d: 8 differences.
+template <typename T>
+__device__ __forceinline__ T phi_w9(const T *f, const T *d, T eps)
+{
+    const T dk[5] = {T(1. / 126.), T(10. / 63.), T(10. / 21.), T(20. / 63.), T(5. / 126.)};
+    T ot[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        T acc = T(0);
+        int c = 0;
+#pragma unroll
+        for (int a = 0; a < 5; a++) {
+            T in = w9c<T>(k, c++) * f[k + a];
+#pragma unroll
+            for (int b = a + 1; b < 5; b++) in = in + w9c<T>(k, c++) * f[k + b];
+            acc = (a == 0) ? f[k] * in : acc + f[k + a] * in;
+        }
+        T t = acc + eps;
+        ot[k] = dk[k] / (t * t);
+    }
+    T s = ot[0] + ot[1] + ot[2] + ot[3] + ot[4];
+    T o0 = ot[0] / s, o2 = ot[2] / s, o3 = ot[3] / s, o4 = ot[4] / s;
+    T q1 = d[0] - T(4.) * d[1] + T(6.) * d[2] - T(4.) * d[3] + d[4];
+    T q2 = d[1] - T(4.) * d[2] + T(6.) * d[3] - T(4.) * d[4] + d[5];
+    T q3 = d[2] - T(4.) * d[3] + T(6.) * d[4] - T(4.) * d[5] + d[6];
+    T q4 = d[3] - T(4.) * d[4] + T(6.) * d[5] - T(4.) * d[6] + d[7];
+    return T(1. / 5.) * o0 * q1 + T(1. / 20.) * o2 * q2 + T(1. / 60.) * o3 * (T(3.) * q2 - T(2.) * q3)
+           + T(1. / 60.) * o4 * (T(3.) * q2 - T(2.) * q3 + T(3.) * q4)
+           - T(1. / 840.) * (T(39.) * q2 - T(14.) * q3 + T(3.) * q4);
+}
+
+// ---------------------------------------------------------------------------
+// Sweep geometry: sweep axis D, lateral axis (32 lines, the fastest
+// non-sweep axis), other axis (3D).
+// ---------------------------------------------------------------------------
+template <int DIM, int D>
+struct Axes {
+    static constexpr int LAT = (D != DIM - 1) ? DIM - 1 : DIM - 2;
+    static constexpr int OTH = (DIM == 3) ? (3 - D - LAT) : 2;
+    static constexpr bool CONTIG = (D == DIM - 1);   // sweep along the contiguous axis
+};
+
+constexpr int TL = 15;       // cells per tile along the sweep
+constexpr int NROW = TL + 1; // face rows (threadIdx.y)
+constexpr int NLANE = 32;    // lines per tile
+
+// Per-point values staged for the WENO face computation.
+enum { WF0 = 0, WU0 = 5, WVU = 10, WVV, WVW, WC, WLAM, WJ, WN0 };
+
+template <int DIM>
+struct WenoNV {
+    static constexpr int NN = DIM == 3 ? 1 : 2;   // stored components of the unit normal
+    static constexpr int NV = WN0 + NN;
+};
+
+// ---------------------------------------------------------------------------
+// weno_d (FP64): thread-per-face characteristic WENO (src/WENO.c:206-494).
+// ---------------------------------------------------------------------------
+template <int DIM, int ORDER, int D>
+__global__ void __launch_bounds__(NLANE *NROW, 1)
+    k_weno(Grid G, Phys P, bool first, const double *__restrict__ R, const double *__restrict__ Uu,
+           const double *__restrict__ Vv, const double *__restrict__ Ww, const double *__restrict__ Ee,
+           Fields F)
+{
+    using A = Axes<DIM, D>;
+    constexpr int r = (ORDER - 1) / 2;
+    constexpr int NP = TL + 2 * r + 2;
+    constexpr int NV = WenoNV<DIM>::NV;
+    constexpr int NN = WenoNV<DIM>::NN;
+    extern __shared__ double smem[];
+    double *sh = smem;                         // [NV][NP][NLANE]
+    double *fh = smem + NV * NP * NLANE;       // [5][NROW][NLANE]
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+#define FH(c, f, l) fh[((c) * NROW + (f)) * NLANE + (l)]
+
+    const int lane = threadIdx.x, row = threadIdx.y;
+    const int c0 = G.g + blockIdx.x * TL;              // first cell of the tile (ghosted index)
+    const int l0 = G.g + blockIdx.y * NLANE;
+    const int oth = (DIM == 3) ? G.g + blockIdx.z : 0;
+    const int nD = G.n[D], nL = G.n[A::LAT];
+    const long long sD = G.st[D], sL = G.st[A::LAT], sO = (DIM == 3) ? G.st[A::OTH] : 0;
+    const long long base = (long long)l0 * sL + (long long)oth * sO;
+
+    // ---- stage point quantities ------------------------------------------
+    const int tid = row * NLANE + lane;
+    for (int it = tid; it < NP * NLANE; it += NLANE * NROW) {
+        int t, l;
+        if (A::CONTIG) { t = it % NP; l = it / NP; }
+        else { l = it % NLANE; t = it / NLANE; }
+        int pd = c0 - 1 - r + t;
+        if (l0 + l >= G.g + nL || pd >= G.N[D]) continue;
+        long long o = base + (long long)l * sL + (long long)pd * sD;
+        double rho = R[o], u = Uu[o], v = Vv[o], w = (DIM == 3) ? Ww[o] : 0.0, e = Ee[o];
+        double p = F.p[o], c = F.c[o], J = F.J[o];
+        double mx, my, mz, th, nrm;
+        if (DIM == 3) {
+            double mm = F.m[3 * D + D][o];
+            mx = D == 0 ? mm : 0.0;
+            my = D == 1 ? mm : 0.0;
+            mz = D == 2 ? mm : 0.0;
+            th = (D == 0 ? u : D == 1 ? v : w) * mm;
+            nrm = fabs(mm);
+        } else {
+            mx = F.m[3 * D + 0][o];
+            my = F.m[3 * D + 1][o];
+            mz = 0.0;
+            th = u * mx + v * my;
+            nrm = sqrt(mx * mx + my * my);
+        }
+        double rt = rho * th;
+        SH(WF0 + 0, t, l) = J * rt;
+        SH(WF0 + 1, t, l) = J * (rt * u + mx * p * P.ups);
+        SH(WF0 + 2, t, l) = J * (rt * v + my * p * P.ups);
+        SH(WF0 + 3, t, l) = J * (rt * w + mz * p * P.ups);
+        SH(WF0 + 4, t, l) = J * (rt * (e + p / rho * P.ups));
+        SH(WU0 + 0, t, l) = rho;
+        SH(WU0 + 1, t, l) = rho * u;
+        SH(WU0 + 2, t, l) = rho * v;
+        SH(WU0 + 3, t, l) = rho * w;
+        SH(WU0 + 4, t, l) = rho * e;
+        SH(WVU, t, l) = u;
+        SH(WVV, t, l) = v;
+        SH(WVW, t, l) = w;
+        SH(WC, t, l) = c;
+        SH(WLAM, t, l) = fabs(th) + c * nrm;
+        SH(WJ, t, l) = J;
+        if (DIM == 3) {
+            SH(WN0, t, l) = (D == 0 ? mx : D == 1 ? my : mz) / nrm;
+        } else {
+            SH(WN0, t, l) = mx / nrm;
+            SH(WN0 + 1, t, l) = my / nrm;
+        }
+    }
+    __syncthreads();
+
+    // ---- one face per thread ----------------------------------------------
+    const bool lane_ok = (l0 + lane) < G.g + nL;
+    const int f = row;                 // face between points ta = r+f and ta+1
+    const int ta = r + f;
+    if (lane_ok && (c0 - 1 + f) <= G.g + nD - 1) {
+        const double gm = P.gamma;
+        double u = 0.5 * (SH(WVU, ta, lane) + SH(WVU, ta + 1, lane));
+        double v = 0.5 * (SH(WVV, ta, lane) + SH(WVV, ta + 1, lane));
+        double w = 0.5 * (SH(WVW, ta, lane) + SH(WVW, ta + 1, lane));
+        double rho = 0.5 * (SH(WU0, ta, lane) + SH(WU0, ta + 1, lane));
+        double c = 0.5 * (SH(WC, ta, lane) + SH(WC, ta + 1, lane));
+        double nx, ny, nz;
+        if (DIM == 3) {
+            double nd = 0.5 * (SH(WN0, ta, lane) + SH(WN0, ta + 1, lane));
+            nx = D == 0 ? nd : 0.0;
+            ny = D == 1 ? nd : 0.0;
+            nz = D == 2 ? nd : 0.0;
+        } else {
+            nx = 0.5 * (SH(WN0, ta, lane) + SH(WN0, ta + 1, lane));
+            ny = 0.5 * (SH(WN0 + 1, ta, lane) + SH(WN0 + 1, ta + 1, lane));
+            nz = 0.0;
+        }
+        (void)NN;
+        const double q2 = u * u + v * v + w * w;
+        const double M2 = q2 / (c * c);      // M*M with M = sqrt(q2)/c
+        const double un = u * nx + v * ny + w * nz;
+        const double sq2 = 1.4142135623730951;
+        const double gc = (gm - 1.0) / (c * c);
+        const double irho = 1.0 / rho;
+        const double isc = 1.0 / (c * sq2);
+        const double kin = 1.0 - 0.5 * (gm - 1.0) * M2;
+        const double jh = (SH(WJ, ta, lane) + SH(WJ, ta + 1, lane)) / 2.0;
+        double lam = 0.0;
+#pragma unroll
+        for (int s = 0; s <= 2 * r + 1; s++) {
+            double lm = SH(WLAM, f + s, lane);
+            lam = lam < lm ? lm : lam;
+        }
+        const double a = lam * jh;
+        double out[5] = {0., 0., 0., 0., 0.};
+#pragma unroll 1
+        for (int ch = 0; ch < 5; ch++) {
+            double L0, L1, L2, L3, L4;
+            switch (ch) {
+            case 0:
+                L0 = nx * kin - irho * (v * nz - w * ny); L1 = gc * u * nx; L2 = gc * v * nx + nz * irho;
+                L3 = gc * w * nx - ny * irho; L4 = -gc * nx; break;
+            case 1:
+                L0 = ny * kin - irho * (w * nx - u * nz); L1 = gc * u * ny - nz * irho; L2 = gc * v * ny;
+                L3 = gc * w * ny + nx * irho; L4 = -gc * ny; break;
+            case 2:
+                L0 = nz * kin - irho * (u * ny - v * nx); L1 = gc * u * nz + ny * irho; L2 = gc * v * nz - nx * irho;
+                L3 = gc * w * nz; L4 = -gc * nz; break;
+            case 3:
+                L0 = isc * ((gm - 1.0) * q2 / 2. - c * un); L1 = (-(gm - 1.0) * u / c + nx) / sq2;
+                L2 = (-(gm - 1.0) * v / c + ny) / sq2; L3 = (-(gm - 1.0) * w / c + nz) / sq2; L4 = (gm - 1.) * isc; break;
+            default:
+                L0 = isc * ((gm - 1.0) * q2 / 2. + c * un); L1 = (-(gm - 1.0) * u / c - nx) / sq2;
+                L2 = (-(gm - 1.0) * v / c - ny) / sq2; L3 = (-(gm - 1.0) * w / c - nz) / sq2; L4 = (gm - 1.) * isc; break;
+            }
+            double Pp[2 * r + 2], Pm[2 * r + 2];
+#pragma unroll
+            for (int s = 0; s <= 2 * r + 1; s++) {
+                int t = f + s;
+                double lf = L0 * SH(WF0 + 0, t, lane) + L1 * SH(WF0 + 1, t, lane) + L2 * SH(WF0 + 2, t, lane)
+                            + L3 * SH(WF0 + 3, t, lane) + L4 * SH(WF0 + 4, t, lane);
+                double lu = L0 * SH(WU0 + 0, t, lane) + L1 * SH(WU0 + 1, t, lane) + L2 * SH(WU0 + 2, t, lane)
+                            + L3 * SH(WU0 + 3, t, lane) + L4 * SH(WU0 + 4, t, lane);
+                Pp[s] = 0.5 * (lf + a * lu);
+                Pm[s] = 0.5 * (lf - a * lu);
+            }
+            double phi;
+            if (ORDER == 5) {
+                double dp[4], dm[4];
+#pragma unroll
+                for (int s = 0; s < 4; s++) {
+                    dp[s] = Pp[s + 1] - Pp[s];
+                    dm[s] = Pm[2 * r + 1 - s] - Pm[2 * r - s];
+                }
+                phi = -phi_w5<double>(dp, P.eps64) + phi_w5<double>(dm, P.eps64);
+            } else {
+                double fp[9], fm[9], dp[8], dm[8];
+#pragma unroll
+                for (int s = 0; s < 9; s++) { fp[s] = Pp[s]; fm[s] = Pm[2 * r + 1 - s]; }
+#pragma unroll
+                for (int s = 0; s < 8; s++) { dp[s] = fp[s + 1] - fp[s]; dm[s] = fm[s] - fm[s + 1]; }
+                phi = -phi_w9<double>(fp, dp, P.eps64) + phi_w9<double>(fm, dm, P.eps64);
+            }
+            // right eigenvector column ch
+            switch (ch) {
+            case 0:
+                out[0] += nx * phi; out[1] += u * nx * phi; out[2] += (v * nx + rho * nz) * phi;
+                out[3] += (w * nx - rho * ny) * phi; out[4] += (q2 / 2. * nx + rho * (v * nz - w * ny)) * phi; break;
+            case 1:
+                out[0] += ny * phi; out[1] += (u * ny - rho * nz) * phi; out[2] += v * ny * phi;
+                out[3] += (w * ny + rho * nx) * phi; out[4] += (q2 / 2. * ny + rho * (w * nx - u * nz)) * phi; break;
+            case 2:
+                out[0] += nz * phi; out[1] += (u * nz + rho * ny) * phi; out[2] += (v * nz - rho * nx) * phi;
+                out[3] += w * nz * phi; out[4] += (q2 / 2. * nz + rho * (u * ny - v * nx)) * phi; break;
+            case 3: {
+                double s = isc * phi;
+                out[0] += s; out[1] += (u + nx * c) * s; out[2] += (v + ny * c) * s; out[3] += (w + nz * c) * s;
+                out[4] += (q2 / 2. + c * c / (gm - 1.) + c * un) * s; break;
+            }
+            default: {
+                double s = isc * phi;
+                out[0] += s; out[1] += (u - nx * c) * s; out[2] += (v - ny * c) * s; out[3] += (w - nz * c) * s;
+                out[4] += (q2 / 2. + c * c / (gm - 1.) - c * un) * s; break;
+            }
+            }
+        }
+        // central part (src/WENO.c:1754-1816)
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            double th;
+            if (ORDER == 9)
+                th = 1. / 840. * (533. * (SH(WF0 + q, ta + 1, lane) + SH(WF0 + q, ta, lane))
+                                  - 139. * (SH(WF0 + q, ta + 2, lane) + SH(WF0 + q, ta - 1, lane))
+                                  + 29. * (SH(WF0 + q, ta + 3, lane) + SH(WF0 + q, ta - 2, lane))
+                                  - 3. * (SH(WF0 + q, ta + 4, lane) + SH(WF0 + q, ta - 3, lane)));
+            else
+                th = 1. / 12. * (-1. * (SH(WF0 + q, ta - 1, lane) + SH(WF0 + q, ta + 2, lane))
+                                 + 7. * (SH(WF0 + q, ta, lane) + SH(WF0 + q, ta + 1, lane)));
+            FH(q, f, lane) = out[q] + th;
+        }
+    }
+    __syncthreads();
+
+    // ---- flux difference into Q ---------------------------------------------
+    if (lane_ok && row < TL && c0 + row <= G.g + nD - 1) {
+        long long o = base + (long long)lane * sL + (long long)(c0 + row) * sD;
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            if (DIM == 2 && q == 3) {
+                // zetaMomentum stays untouched in 2D except for the flux difference of zeros
+            }
+            double prev = first ? 0.0 : F.Q[q][o];
+            F.Q[q][o] = prev - (FH(q, row + 1, lane) - FH(q, row, lane));
+        }
+    }
+#undef SH
+#undef FH
+}
+
+// ---------------------------------------------------------------------------
+// visc_d: central viscous flux difference (src/ZD.c:47-694).
+//
+// Viscous factors are recomputed from the metric instead of streaming the
+// 90 Fluss_Faktor arrays (src/Functions.c:6245-6386):
+//   K[i][k][m] = J ( delta_ik a.grad(xi_m) + a_k dxi_m/dx_i - 2/3 a_i dxi_m/dx_k ),
+//   heat      = J a.grad(xi_m),     a = grad(xi_d),
+// each multiplied by mu and averaged over the two points of the face.
+// 3D uses SHOCK's diagonal metric, so only 8 of the 30 factors are non-zero.
+// ---------------------------------------------------------------------------
+enum { V3U = 0, V3V, V3W, V3T, V3X0, V3X1, V3X2, V3X3, V3F1, V3FA, V3FB, V3NV };
+enum { V2U = 0, V2V, V2T, V2XU, V2XV, V2XT, V2MJ, V2AX, V2AY, V2BX, V2BY, V2NV };
+
+template <int DIM, int ORDER, int D>
+__global__ void __launch_bounds__(NLANE *NROW, 1)
+    k_visc(Grid G, Phys P, const double *__restrict__ Uu, const double *__restrict__ Vv,
+           const double *__restrict__ Ww, Fields F)
+{
+    using A = Axes<DIM, D>;
+    constexpr int H = ZD<ORDER>::H;          // half stencil: l = 0..2H-1 around the face
+    constexpr int NP = TL + 2 * H;
+    constexpr int NV = DIM == 3 ? V3NV : V2NV;
+    constexpr int NG_OUT = DIM == 3 ? 4 : 3; // face outputs: momentum (DIM) + heat
+    // 3D: the two non-sweep axes
+    constexpr int MA = (D == 0) ? 1 : 0;
+    constexpr int MB = (D == 2) ? 1 : 2;
+    const bool quirk = (DIM == 3 && D == 2 && !P.zeta_fix);
+
+    extern __shared__ double smem[];
+    double *sh = smem;                       // [NV][NP][NLANE]
+    double *fo = smem + NV * NP * NLANE;     // [NG_OUT or 3 K][NROW][NLANE]
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+#define FO(c, f, l) fo[((c) * NROW + (f)) * NLANE + (l)]
+
+    const int lane = threadIdx.x, row = threadIdx.y;
+    const int c0 = G.g + blockIdx.x * TL;
+    const int l0 = G.g + blockIdx.y * NLANE;
+    const int oth = (DIM == 3) ? G.g + blockIdx.z : 0;
+    const int nD = G.n[D], nL = G.n[A::LAT];
+    const long long sD = G.st[D], sL = G.st[A::LAT], sO = (DIM == 3) ? G.st[A::OTH] : 0;
+    const long long base = (long long)l0 * sL + (long long)oth * sO;
+
+    // ---- stage: points c0-H .. c0+TL+H-1 along the sweep ----------------------
+    const int tid = row * NLANE + lane;
+    for (int it = tid; it < NP * NLANE; it += NLANE * NROW) {
+        int t, l;
+        if (A::CONTIG) { t = it % NP; l = it / NP; }
+        else { l = it % NLANE; t = it / NLANE; }
+        int pd = c0 - H + t;
+        if (l0 + l >= G.g + nL || pd >= G.N[D]) continue;
+        long long o = base + (long long)l * sL + (long long)pd * sD;
+        double mu = F.mu[o], J = F.J[o];
+        if (DIM == 3) {
+            double cd = F.m[4 * D][o], ca = F.m[4 * MA][o], cb = F.m[4 * MB][o];
+            SH(V3U, t, l) = Uu[o];
+            SH(V3V, t, l) = Vv[o];
+            SH(V3W, t, l) = Ww[o];
+            SH(V3T, t, l) = F.T[o];
+            SH(V3X0, t, l) = F.Nd[3 * MA + MA][o];   // d vel_MA / d xi_MA
+            SH(V3X1, t, l) = F.Nd[3 * MB + MB][o];   // d vel_MB / d xi_MB
+            SH(V3X2, t, l) = F.Nd[3 * D + MA][o];    // d vel_D / d xi_MA
+            SH(V3X3, t, l) = F.Nd[3 * D + MB][o];    // d vel_D / d xi_MB
+            double mj = mu * J;
+            SH(V3F1, t, l) = mj * (cd * cd);
+            SH(V3FA, t, l) = mj * (cd * ca);
+            SH(V3FB, t, l) = mj * (cd * cb);
+        } else {
+            constexpr int E = 1 - D;
+            SH(V2U, t, l) = Uu[o];
+            SH(V2V, t, l) = Vv[o];
+            SH(V2T, t, l) = F.T[o];
+            SH(V2XU, t, l) = F.Nd[3 * 0 + E][o];
+            SH(V2XV, t, l) = F.Nd[3 * 1 + E][o];
+            SH(V2XT, t, l) = F.Nd[3 * 3 + E][o];
+            SH(V2MJ, t, l) = mu * J;
+            SH(V2AX, t, l) = F.m[3 * D + 0][o];
+            SH(V2AY, t, l) = F.m[3 * D + 1][o];
+            SH(V2BX, t, l) = F.m[3 * E + 0][o];
+            SH(V2BY, t, l) = F.m[3 * E + 1][o];
+        }
+    }
+    __syncthreads();
+
+    const bool lane_ok = (l0 + lane) < G.g + nL;
+    const int f = row;                       // face (c0-1+f)+1/2: points c0-1+f-H+1 .. c0-1+f+H
+    const double t23 = 2.0 / 3.0, t43 = 4.0 / 3.0;
+    if (lane_ok && (c0 - 1 + f) <= G.g + nD - 1) {
+        const int ta = f + H - 1;            // staged index of the left point
+        if (DIM == 3) {
+            double K1 = 0.5 * (SH(V3F1, ta, lane) + SH(V3F1, ta + 1, lane));
+            double KA = 0.5 * (SH(V3FA, ta, lane) + SH(V3FA, ta + 1, lane));
+            double KB = 0.5 * (SH(V3FB, ta, lane) + SH(V3FB, ta + 1, lane));
+            if (quirk) {
+                FO(0, f, lane) = K1; FO(1, f, lane) = KA; FO(2, f, lane) = KB;
+            } else {
+                double dU = 0, dV = 0, dW = 0, dT = 0, x0 = 0, x1 = 0, x2 = 0, x3 = 0;
+#pragma unroll
+                for (int l = 0; l < 2 * H; l++) {
+                    int t = f + l;
+                    double ch = ZD<ORDER>::half(l), ci = ZD<ORDER>::interp(l);
+                    dU += ch * SH(V3U, t, lane); dV += ch * SH(V3V, t, lane);
+                    dW += ch * SH(V3W, t, lane); dT += ch * SH(V3T, t, lane);
+                    x0 += ci * SH(V3X0, t, lane); x1 += ci * SH(V3X1, t, lane);
+                    x2 += ci * SH(V3X2, t, lane); x3 += ci * SH(V3X3, t, lane);
+                }
+                double dvel[3] = {dU, dV, dW};
+                // momentum along D: d vel_D/d xi_D * 4/3 K1 - 2/3 (d vel_MA/d xi_MA KA + d vel_MB/d xi_MB KB)
+                double gD = dvel[D] * (t43 * K1) + x0 * (-t23 * KA) + x1 * (-t23 * KB);
+                double gA = dvel[MA] * K1 + x2 * KA;    // momentum MA: d vel_MA/d xi_D K1 + d vel_D/d xi_MA KA
+                double gB = dvel[MB] * K1 + x3 * KB;
+                double g3[3];
+                g3[D] = gD; g3[MA] = gA; g3[MB] = gB;
+                FO(0, f, lane) = g3[0]; FO(1, f, lane) = g3[1]; FO(2, f, lane) = g3[2];
+                FO(3, f, lane) = dT * K1;
+            }
+        } else {
+            constexpr int E = 1 - D;
+            double dU = 0, dV = 0, dT = 0, xU = 0, xV = 0, xT = 0;
+#pragma unroll
+            for (int l = 0; l < 2 * H; l++) {
+                int t = f + l;
+                double ch = ZD<ORDER>::half(l), ci = ZD<ORDER>::interp(l);
+                dU += ch * SH(V2U, t, lane); dV += ch * SH(V2V, t, lane); dT += ch * SH(V2T, t, lane);
+                xU += ci * SH(V2XU, t, lane); xV += ci * SH(V2XV, t, lane); xT += ci * SH(V2XT, t, lane);
+            }
+            // derivatives at the face indexed [var][dir]
+            double Dk[2][2], DT[2];
+            Dk[0][D] = dU; Dk[1][D] = dV; DT[D] = dT;
+            Dk[0][E] = xU; Dk[1][E] = xV; DT[E] = xT;
+            double gx = 0, gy = 0, hh = 0;
+#pragma unroll
+            for (int side = 0; side < 2; side++) {
+                int t = ta + side;
+                double mj = SH(V2MJ, t, lane);
+                double ax = SH(V2AX, t, lane), ay = SH(V2AY, t, lane);
+                double bx = SH(V2BX, t, lane), by = SH(V2BY, t, lane);
+                double gm[2][2];   // grad xi_m, m = xi, eta
+                gm[D][0] = ax; gm[D][1] = ay; gm[E][0] = bx; gm[E][1] = by;
+                double av[2] = {ax, ay};
+                double s0 = 0, s1 = 0, sh0 = 0;
+#pragma unroll
+                for (int m = 0; m < 2; m++) {
+                    double adot = ax * gm[m][0] + ay * gm[m][1];
+#pragma unroll
+                    for (int k = 0; k < 2; k++) {
+                        double K0 = (k == 0 ? adot : 0.0) + av[k] * gm[m][0] - t23 * av[0] * gm[m][k];
+                        double Kk1 = (k == 1 ? adot : 0.0) + av[k] * gm[m][1] - t23 * av[1] * gm[m][k];
+                        s0 += Dk[k][m] * K0;
+                        s1 += Dk[k][m] * Kk1;
+                    }
+                    sh0 += DT[m] * adot;
+                }
+                gx += 0.5 * mj * s0;
+                gy += 0.5 * mj * s1;
+                hh += 0.5 * mj * sh0;
+            }
+            FO(0, f, lane) = gx; FO(1, f, lane) = gy; FO(2, f, lane) = hh;
+        }
+    }
+    __syncthreads();
+
+    // ---- cell update ----------------------------------------------------------
+    if (lane_ok && row < TL && c0 + row <= G.g + nD - 1) {
+        const int cell = c0 + row;
+        long long o = base + (long long)lane * sL + (long long)cell * sD;
+        double mu = F.mu[o], J = F.J[o];
+        double vel[3] = {Uu[o], Vv[o], DIM == 3 ? Ww[o] : 0.0};
+        double gp[3] = {0, 0, 0}, gmn[3] = {0, 0, 0}, hp = 0, hm = 0;
+        double nodeB = 0;
+        if (DIM == 3) {
+            double cd = F.m[4 * D][o], ca = F.m[4 * MA][o], cb = F.m[4 * MB][o];
+            if (quirk) {
+                // half-point stencils along k centred on the j index (src/ZD.c:547-548)
+                const int jj = (int)((o / G.st[1]) % G.N[1]);
+                long long lb = o - (o % G.st[1]);            // (i, j, 0)
+                double Dm[8] = {0, 0, 0, 0, 0, 0, 0, 0}, Dp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+                const double *vs[4] = {Uu, Vv, Ww, F.T};
+                const double *xs[4] = {F.Nd[3 * MA + MA], F.Nd[3 * MB + MB], F.Nd[3 * D + MA], F.Nd[3 * D + MB]};
+#pragma unroll
+                for (int l = 0; l < 2 * H; l++) {
+                    long long im = lb + (jj + l - H), ip = im + 1;
+                    double ch = ZD<ORDER>::half(l), ci = ZD<ORDER>::interp(l);
+#pragma unroll
+                    for (int q = 0; q < 4; q++) {
+                        Dm[q] += ch * vs[q][im]; Dp[q] += ch * vs[q][ip];
+                        Dm[4 + q] += ci * xs[q][im]; Dp[4 + q] += ci * xs[q][ip];
+                    }
+                }
+                double K1p = FO(0, row + 1, lane), KAp = FO(1, row + 1, lane), KBp = FO(2, row + 1, lane);
+                double K1m = FO(0, row, lane), KAm = FO(1, row, lane), KBm = FO(2, row, lane);
+                gp[D] = Dp[D] * (t43 * K1p) + Dp[4] * (-t23 * KAp) + Dp[5] * (-t23 * KBp);
+                gp[MA] = Dp[MA] * K1p + Dp[6] * KAp;
+                gp[MB] = Dp[MB] * K1p + Dp[7] * KBp;
+                hp = Dp[3] * K1p;
+                gmn[D] = Dm[D] * (t43 * K1m) + Dm[4] * (-t23 * KAm) + Dm[5] * (-t23 * KBm);
+                gmn[MA] = Dm[MA] * K1m + Dm[6] * KAm;
+                gmn[MB] = Dm[MB] * K1m + Dm[7] * KBm;
+                hm = Dm[3] * K1m;
+            } else {
+#pragma unroll
+                for (int q = 0; q < 3; q++) { gp[q] = FO(q, row + 1, lane); gmn[q] = FO(q, row, lane); }
+                hp = FO(3, row + 1, lane);
+                hm = FO(3, row, lane);
+            }
+            // node term: mu * sum_i N[i][D] * sum_{k,m} N[k][m] Fac[i][k][m] at the cell
+            double F1 = J * (cd * cd), FA = J * (cd * ca), FB = J * (cd * cb);
+            double nDD = F.Nd[3 * D + D][o], nAA = F.Nd[3 * MA + MA][o], nBB = F.Nd[3 * MB + MB][o];
+            double nAD = F.Nd[3 * MA + D][o], nBD = F.Nd[3 * MB + D][o];
+            double nDA = F.Nd[3 * D + MA][o], nDB = F.Nd[3 * D + MB][o];
+            double hD = nDD * (t43 * F1) + nAA * (-t23 * FA) + nBB * (-t23 * FB);
+            double hA = nAD * F1 + nDA * FA;
+            double hB = nBD * F1 + nDB * FB;
+            nodeB = mu * (nDD * hD + nAD * hA + nBD * hB);
+        } else {
+            constexpr int E = 1 - D;
+#pragma unroll
+            for (int q = 0; q < 2; q++) { gp[q] = FO(q, row + 1, lane); gmn[q] = FO(q, row, lane); }
+            hp = FO(2, row + 1, lane);
+            hm = FO(2, row, lane);
+            double ax = F.m[3 * D + 0][o], ay = F.m[3 * D + 1][o];
+            double gmv[2][2];
+            gmv[D][0] = ax; gmv[D][1] = ay; gmv[E][0] = F.m[3 * E + 0][o]; gmv[E][1] = F.m[3 * E + 1][o];
+            double av[2] = {ax, ay};
+            double N[2][2];   // N[var][dir]
+            N[0][0] = F.Nd[0][o]; N[0][1] = F.Nd[1][o]; N[1][0] = F.Nd[3][o]; N[1][1] = F.Nd[4][o];
+            double hsum[2] = {0, 0};
+#pragma unroll
+            for (int m = 0; m < 2; m++) {
+                double adot = ax * gmv[m][0] + ay * gmv[m][1];
+#pragma unroll
+                for (int k = 0; k < 2; k++) {
+#pragma unroll
+                    for (int i = 0; i < 2; i++) {
+                        double K = (i == k ? adot : 0.0) + av[k] * gmv[m][i] - t23 * av[i] * gmv[m][k];
+                        hsum[i] += N[k][m] * K;
+                    }
+                }
+            }
+            nodeB = mu * J * (N[0][D] * hsum[0] + N[1][D] * hsum[1]);
+        }
+        const double psi = P.psi;
+        F.Q[1][o] = F.Q[1][o] + psi * (gp[0] - gmn[0]);
+        F.Q[2][o] = F.Q[2][o] + psi * (gp[1] - gmn[1]);
+        if (DIM == 3) F.Q[3][o] = F.Q[3][o] + psi * (gp[2] - gmn[2]);
+        double Aterm = vel[0] * (gp[0] - gmn[0]) + vel[1] * (gp[1] - gmn[1]);
+        if (DIM == 3) Aterm += vel[2] * (gp[2] - gmn[2]);
+        F.Q[4][o] = F.Q[4][o] + 0.5 * (P.gam + P.gam) * (hp - hm) + psi * (Aterm + nodeB);
+    }
+#undef SH
+#undef FO
+}
+
+// ---------------------------------------------------------------------------
+// RK stage update of the real points (src/Functions.c:2300-2365), with the
+// time-independent source J*S added to Q first.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__global__ void k_rk(Grid G, RKCoef K, double tau, StageIn in, Fields F, double *o0, double *o1,
+                     double *o2, double *o3, double *o4, int has_source, int nreal)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nreal) return;
+    int i, j, k;
+    if (DIM == 3) {
+        k = t % G.n[2];
+        int r = t / G.n[2];
+        j = r % G.n[1];
+        i = r / G.n[1];
+    } else {
+        k = 0;
+        j = t % G.n[1];
+        i = t / G.n[1];
+    }
+    long long o = (long long)(i + G.g) * G.st[0] + (long long)(j + G.g) * G.st[1] + (DIM == 3 ? k + G.g : 0);
+    double Q[5], Qs[5];
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+        Q[c] = F.Q[c][o];
+        if (has_source) Q[c] += F.js[c][o];
+        Qs[c] = F.Qs[c][o] + K.s * Q[c];
+        F.Qs[c][o] = Qs[c];
+    }
+    double ro = in.U[0][o];
+    double tj = tau / F.J[o];
+    double rn = K.a * F.Un[0][o] + K.b * ro + tj * (K.c * Q[0] + K.d * Qs[0]);
+    double *outs[5] = {o0, o1, o2, o3, o4};
+    outs[0][o] = rn;
+#pragma unroll
+    for (int c = 1; c < 5; c++) {
+        if (DIM == 2 && c == 3) { outs[3][o] = 0.0; continue; }
+        outs[c][o] = (K.a * F.Un[c][o] * F.Un[0][o] + K.b * in.U[c][o] * ro + tj * (K.c * Q[c] + K.d * Qs[c])) / rn;
+    }
+}
+
+__global__ void k_add_source(Grid G, Fields F)
+{
+    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (o >= G.NG) return;
+    Idx3 p = unflatten(G, o);
+    for (int a = 0; a < G.dim; a++)
+        if (!is_real(G, a, p.v[a])) return;
+    for (int c = 0; c < 5; c++) F.Q[c][o] += F.js[c][o];
+}
+
+__global__ void k_nan(Grid G, const double *rho, unsigned int *flag)
+{
+    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (o >= G.NG) return;
+    Idx3 p = unflatten(G, o);
+    for (int a = 0; a < G.dim; a++)
+        if (!is_real(G, a, p.v[a])) return;
+    double r = rho[o];
+    if (!isfinite(r)) atomicAdd(flag, 1u);
+}
+
+// ---------------------------------------------------------------------------
+// launchers
+// ---------------------------------------------------------------------------
+static inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + bs - 1) / bs); }
+
+void launch_ghosts(const Grid &G, double *const U[5], cudaStream_t s)
+{
+    if (!(G.periodic[0] || G.periodic[1] || G.periodic[2])) return;
+    k_ghosts<<<blocks_for(G.NG, 256), 256, 0, s>>>(G, U[0], U[1], U[2], U[3], U[4]);
+}
+
+void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s)
+{
+    if (G.dim == 3)
+        k_prim<3><<<blocks_for(G.NG, 256), 256, 0, s>>>(G, P, U[0], U[1], U[2], U[3], U[4], F.p, F.T, F.c, F.mu);
+    else
+        k_prim<2><<<blocks_for(G.NG, 256), 256, 0, s>>>(G, P, U[0], U[1], U[2], U[3], U[4], F.p, F.T, F.c, F.mu);
+}
+
+void launch_nodal(const Grid &G, const double *const U[5], const Fields &F, cudaStream_t s)
+{
+    unsigned nb = blocks_for(G.NG, 256);
+    if (G.dim == 3 && G.order == 5) k_nodal<3, 5><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F);
+    else if (G.dim == 3) k_nodal<3, 9><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F);
+    else if (G.order == 5) k_nodal<2, 5><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F);
+    else k_nodal<2, 9><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F);
+}
+
+template <int DIM, int D>
+static dim3 sweep_grid(const Grid &G)
+{
+    using A = Axes<DIM, D>;
+    return dim3((G.n[D] + TL - 1) / TL, (G.n[A::LAT] + NLANE - 1) / NLANE, DIM == 3 ? G.n[A::OTH] : 1);
+}
+
+template <int DIM, int ORDER, int D>
+static void weno_one(const Grid &G, const Phys &P, bool first, const double *const U[5], const Fields &F,
+                     cudaStream_t s)
+{
+    constexpr int r = (ORDER - 1) / 2;
+    constexpr int NP = TL + 2 * r + 2;
+    size_t smem = sizeof(double) * ((size_t)WenoNV<DIM>::NV * NP * NLANE + 5 * NROW * NLANE);
+    if (!G.order) {   // attribute pass (called once per device before any capture)
+        cudaFuncSetAttribute(k_weno<DIM, ORDER, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        return;
+    }
+    k_weno<DIM, ORDER, D><<<sweep_grid<DIM, D>(G), dim3(NLANE, NROW), smem, s>>>(G, P, first, U[0], U[1], U[2],
+                                                                                U[3], U[4], F);
+}
+
+template <int DIM, int ORDER, int D>
+static void visc_one(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s)
+{
+    constexpr int H = ZD<ORDER>::H;
+    constexpr int NP = TL + 2 * H;
+    constexpr int NV = DIM == 3 ? V3NV : V2NV;
+    size_t smem = sizeof(double) * ((size_t)NV * NP * NLANE + 4 * NROW * NLANE);
+    if (!G.order) {
+        cudaFuncSetAttribute(k_visc<DIM, ORDER, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        return;
+    }
+    k_visc<DIM, ORDER, D><<<sweep_grid<DIM, D>(G), dim3(NLANE, NROW), smem, s>>>(G, P, U[1], U[2], U[3], F);
+}
+
+void launch_weno(const Grid &G, const Phys &P, int precision, int d, bool first, const double *const U[5],
+                 const Fields &F, cudaStream_t s)
+{
+    (void)precision;
+#define W(DIM, ORD, D) \
+    if (G.dim == DIM && G.order == ORD && d == D) { weno_one<DIM, ORD, D>(G, P, first, U, F, s); return; }
+    W(3, 5, 0) W(3, 5, 1) W(3, 5, 2) W(3, 9, 0) W(3, 9, 1) W(3, 9, 2)
+    W(2, 5, 0) W(2, 5, 1) W(2, 9, 0) W(2, 9, 1)
+#undef W
+}
+
+void launch_viscous(const Grid &G, const Phys &P, int precision, int d, const double *const U[5],
+                    const Fields &F, cudaStream_t s)
+{
+    (void)precision;
+#define V(DIM, ORD, D) \
+    if (G.dim == DIM && G.order == ORD && d == D) { visc_one<DIM, ORD, D>(G, P, U, F, s); return; }
+    V(3, 5, 0) V(3, 5, 1) V(3, 5, 2) V(3, 9, 0) V(3, 9, 1) V(3, 9, 2)
+    V(2, 5, 0) V(2, 5, 1) V(2, 9, 0) V(2, 9, 1)
+#undef V
+}
+
+void launch_rk(const Grid &G, const RKCoef &rk, double tau, const double *const Uin[5], double *const Uout[5],
+               const Fields &F, bool has_source, cudaStream_t s)
+{
+    StageIn in;
+    for (int c = 0; c < 5; c++) in.U[c] = Uin[c];
+    int nreal = G.n[0] * G.n[1] * (G.dim == 3 ? G.n[2] : 1);
+    if (G.dim == 3)
+        k_rk<3><<<blocks_for(nreal, 256), 256, 0, s>>>(G, rk, tau, in, F, Uout[0], Uout[1], Uout[2], Uout[3], Uout[4],
+                                                       has_source ? 1 : 0, nreal);
+    else
+        k_rk<2><<<blocks_for(nreal, 256), 256, 0, s>>>(G, rk, tau, in, F, Uout[0], Uout[1], Uout[2], Uout[3], Uout[4],
+                                                       has_source ? 1 : 0, nreal);
+}
+
+void launch_add_source(const Grid &G, const Fields &F, cudaStream_t s)
+{
+    k_add_source<<<blocks_for(G.NG, 256), 256, 0, s>>>(G, F);
+}
+
+void launch_nan_check(const Grid &G, const double *rho, unsigned int *flag, cudaStream_t s)
+{
+    k_nan<<<blocks_for(G.NG, 256), 256, 0, s>>>(G, rho, flag);
+}
+
+// Raise the dynamic shared-memory limit of every sweep kernel on the
+// current device.  Called at context creation, outside any graph capture.
+void prepare_kernels()
+{
+    Grid G{};
+    Phys P{};
+    Fields F{};
+    const double *U[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    G.order = 0;
+    weno_one<3, 5, 0>(G, P, true, U, F, 0); weno_one<3, 5, 1>(G, P, true, U, F, 0); weno_one<3, 5, 2>(G, P, true, U, F, 0);
+    weno_one<3, 9, 0>(G, P, true, U, F, 0); weno_one<3, 9, 1>(G, P, true, U, F, 0); weno_one<3, 9, 2>(G, P, true, U, F, 0);
+    weno_one<2, 5, 0>(G, P, true, U, F, 0); weno_one<2, 5, 1>(G, P, true, U, F, 0);
+    weno_one<2, 9, 0>(G, P, true, U, F, 0); weno_one<2, 9, 1>(G, P, true, U, F, 0);
+    visc_one<3, 5, 0>(G, P, U, F, 0); visc_one<3, 5, 1>(G, P, U, F, 0); visc_one<3, 5, 2>(G, P, U, F, 0);
+    visc_one<3, 9, 0>(G, P, U, F, 0); visc_one<3, 9, 1>(G, P, U, F, 0); visc_one<3, 9, 2>(G, P, U, F, 0);
+    visc_one<2, 5, 0>(G, P, U, F, 0); visc_one<2, 5, 1>(G, P, U, F, 0);
+    visc_one<2, 9, 0>(G, P, U, F, 0); visc_one<2, 9, 1>(G, P, U, F, 0);
+}
+
+void launch_copy_state(const Grid &G, const double *const src[5], double *const dst[5], cudaStream_t s)
+{
+    for (int c = 0; c < 5; c++) cudaMemcpyAsync(dst[c], src[c], sizeof(double) * G.NG, cudaMemcpyDeviceToDevice, s);
+}
+
+}  // namespace shock

@@ -1,0 +1,121 @@
+"""GPU (sm_100a kernels through the C ABI) against SHOCK's results.
+
+Tolerances (FP64 form): one right-hand side within 1e-12 of the reference,
+normwise per conserved variable (max|Q_gpu - Q_ref| / max|Q_ref|); the state
+after 100 full RK4 steps within 1e-10 relative L2 per variable.  The GPU
+contracts multiply-adds into FMAs, so agreement is not bitwise.
+"""
+import numpy as np
+import pytest
+
+import shock_b200
+from _util import golden_names, l2_rel, load_golden, real, rel_err
+from refbind import Oracle
+from shock_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+RHS_TOL = 1e-12
+L2_TOL_100 = 1e-10
+
+
+def _solver(case, d=None, **kw):
+    d = d or {}
+    return shock_b200.Solver(case, dirichlet9=d.get("dirichlet9"), source5=d.get("source5"), **kw)
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_rhs_matches_reference_golden(name):
+    case, d = load_golden(name)
+    s = _solver(case, d)
+    q = real(case, s.rhs())
+    ref = real(case, d["rhs"])
+    if case.mms != "none":
+        scale = np.abs(real(case, d["source5"])).max()
+        err = np.abs(q - ref).max() / scale
+        assert err <= RHS_TOL, err
+    else:
+        err = rel_err(q, ref)
+        assert (err <= RHS_TOL).all(), err
+
+
+@pytest.mark.parametrize("name", golden_names())
+def test_steps_match_reference_golden(name):
+    case, d = load_golden(name)
+    s = _solver(case, d)
+    s.steps(int(d["nsteps"]))
+    err = rel_err(real(case, s.state()), real(case, d["state"]))
+    assert (err <= 1e-12).all(), err
+
+
+@pytest.mark.parametrize("dim,order,inviscid,n", [
+    (2, 5, False, (64, 64, 1)), (2, 9, False, (40, 36, 1)), (3, 5, False, (24, 20, 22)),
+    (3, 9, False, (20, 18, 18)), (3, 5, True, (17, 19, 23)), (2, 5, True, (13, 17, 1)),
+])
+def test_rhs_matches_oracle_sizes(dim, order, inviscid, n):
+    """Ragged and odd sizes (tile remainders along every axis)."""
+    c = cases.smooth_random(dim, order, n, seed=5, inviscid=inviscid, stretch=0.08)
+    o = Oracle(c)
+    s = _solver(c)
+    assert np.array_equal(s.geometry(), o.geometry())
+    err = rel_err(real(c, s.rhs()), real(c, o.rhs()))
+    assert (err <= RHS_TOL).all(), err
+
+
+def test_tgv_100_steps_l2():
+    """Curvilinear Taylor-Green (perturbed grid), 100 RK4 steps vs the oracle."""
+    c = cases.taylor_green(16, order=5)
+    o = Oracle(c)
+    s = _solver(c)
+    o.steps(100)
+    s.steps(100)
+    err = l2_rel(real(c, s.state()), real(c, o.state()[:5]))
+    assert (err <= L2_TOL_100).all(), err
+
+
+def test_mms_100_steps_l2():
+    """2D manufactured solution on the unit square (64^2, WENO5, viscous), 100 steps."""
+    c = cases.mms_square(64, 5, family="reference", mms_case=0)
+    from refbind import RefSolver, ref_available
+    if ref_available(5, 2):
+        r = RefSolver(c)
+        dir9, src = r.mms_exact(), r.mms_source()
+    else:
+        d = load_golden("w5_2d_mms_reference")[1]
+        pytest.skip("reference build not present for 64^2 manufactured data")
+    o = Oracle(c, dirichlet9=dir9, source5=src)
+    s = _solver(c, {"dirichlet9": dir9, "source5": src})
+    o.steps(100)
+    s.steps(100)
+    err = l2_rel(real(c, s.state()), real(c, o.state()[:5]))
+    assert (err <= L2_TOL_100).all(), err
+
+
+def test_rk3_and_w9_steps():
+    c = cases.smooth_random(3, 9, (16, 14, 15), seed=9, time_order=3)
+    o = Oracle(c)
+    s = _solver(c)
+    o.steps(10)
+    s.steps(10)
+    err = l2_rel(real(c, s.state()), real(c, o.state()[:5]))
+    assert (err <= 1e-11).all(), err
+
+
+def test_deterministic():
+    c = cases.smooth_random(3, 5, (20, 18, 19), seed=3)
+    a = _solver(c)
+    b = _solver(c)
+    a.steps(5)
+    b.steps(5)
+    assert np.array_equal(a.state(), b.state())
+
+
+def test_nan_flag():
+    """Fault injected on the host: a NaN density in the uploaded state."""
+    c = cases.smooth_random(2, 5, (16, 16, 1), seed=1)
+    s = _solver(c)
+    st = s.state()
+    g = c.ghosts
+    st[0, g + 3, g + 4, 0] = np.nan
+    s.set_state(st)
+    assert s.check_nan() == 1
