@@ -124,9 +124,18 @@ int shock_device_bytes(const shock_ctx *ctx, size_t *bytes);
  * shock_step_async batch. */
 int shock_last_step_ms(shock_ctx *ctx, float *ms);
 
-/* The launch list of one stage: number of kernels per stage and the
- * kernel that dominates (name written to buf). */
+/* Number of kernel launches in one captured time step. */
 int shock_kernels_per_step(const shock_ctx *ctx, int *n);
+
+/* Time every kernel of one stage right-hand side plus the RK update
+ * separately (CUDA events between launches, outside any graph).  names
+ * receives up to max entries of 48 characters each, ms the times in
+ * milliseconds; *count the number of kernels. */
+int shock_profile_stage(shock_ctx *ctx, int max, char *names, float *ms, int *count);
+
+/* FP64 and FP32 fused multiply-add throughput of a device in TFLOP/s,
+ * measured with a register-only FMA loop (roofline denominators). */
+int shock_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 
 #ifdef __cplusplus
 }

@@ -119,6 +119,13 @@ void TransferFlowParameterWithGhosts(struct strct_configuration *pc, struct strc
 
 void ref_free(void);
 
+static void copy_out(double *q, const struct strct_Flux *F, int n)
+{
+    const FLT *f[5] = {F->Mass, F->xiMomentum, F->etaMomentum, F->zetaMomentum, F->Energy};
+    for (int c = 0; c < 5; c++)
+        for (int o = 0; o < n; o++) q[(size_t)c * n + o] = (double)f[c][o];
+}
+
 int ref_init(const ref_params *p, const double *x, const double *y, const double *z,
              const double *u, const double *v, const double *w, const double *pr,
              const double *rho)
@@ -225,11 +232,7 @@ void ref_rhs(double *q)
 #endif
     }
     if (cfg.flag_ManufacturedSolution == 1) AddManufacturedSolutionSource(&cfg, &msh, &Qf);
-    memcpy(q + 0 * (size_t)n, Qf.Mass, sizeof(double) * n);
-    memcpy(q + 1 * (size_t)n, Qf.xiMomentum, sizeof(double) * n);
-    memcpy(q + 2 * (size_t)n, Qf.etaMomentum, sizeof(double) * n);
-    memcpy(q + 3 * (size_t)n, Qf.zetaMomentum, sizeof(double) * n);
-    memcpy(q + 4 * (size_t)n, Qf.Energy, sizeof(double) * n);
+    copy_out(q, &Qf, n);
 }
 
 /* n time steps, the core of startSimulation (SHOCK.c:557-663). */
@@ -247,7 +250,8 @@ void ref_get_state(double *out, int which)
     struct strct_U *s = which ? &U_last : &U_rk;
     FLT *f[9] = {s->rho, s->u, s->v, s->w, s->e, s->p, s->T, s->c, s->mue};
     int n = NG;
-    for (int a = 0; a < 9; a++) memcpy(out + (size_t)a * n, f[a], sizeof(double) * n);
+    for (int a = 0; a < 9; a++)
+        for (int o = 0; o < n; o++) out[(size_t)a * n + o] = (double)f[a][o];
 }
 
 /* Overwrite rho,u,v,w,e (5*NG) of both U_RK and U_lastStep. */
@@ -256,10 +260,8 @@ void ref_set_state(const double *in)
     int n = NG;
     FLT *a[5] = {U_rk.rho, U_rk.u, U_rk.v, U_rk.w, U_rk.e};
     FLT *b[5] = {U_last.rho, U_last.u, U_last.v, U_last.w, U_last.e};
-    for (int f = 0; f < 5; f++) {
-        memcpy(a[f], in + (size_t)f * n, sizeof(double) * n);
-        memcpy(b[f], in + (size_t)f * n, sizeof(double) * n);
-    }
+    for (int f = 0; f < 5; f++)
+        for (int o = 0; o < n; o++) { a[f][o] = (FLT)in[(size_t)f * n + o]; b[f][o] = (FLT)in[(size_t)f * n + o]; }
 }
 
 /* out: x,y,z,J,xi_x,xi_y,xi_z,eta_x,eta_y,eta_z,zeta_x,zeta_y,zeta_z (13*NG). */
@@ -268,7 +270,8 @@ void ref_get_geom(double *out)
     FLT *f[13] = {msh.x, msh.y, msh.z, msh.jacobian, msh.xi_x, msh.xi_y, msh.xi_z,
                   msh.eta_x, msh.eta_y, msh.eta_z, msh.zeta_x, msh.zeta_y, msh.zeta_z};
     int n = NG;
-    for (int a = 0; a < 13; a++) memcpy(out + (size_t)a * n, f[a], sizeof(double) * n);
+    for (int a = 0; a < 13; a++)
+        for (int o = 0; o < n; o++) out[(size_t)a * n + o] = (double)f[a][o];
 }
 
 /* Seconds of wall time for nstage RK stages: nstage/TimeOrder full steps
@@ -291,11 +294,7 @@ void ref_mms_source(double *js5)
     int n = NG;
     DeleteQ(&cfg, &Qf);
     AddManufacturedSolutionSource(&cfg, &msh, &Qf);
-    memcpy(js5 + 0 * (size_t)n, Qf.Mass, sizeof(double) * n);
-    memcpy(js5 + 1 * (size_t)n, Qf.xiMomentum, sizeof(double) * n);
-    memcpy(js5 + 2 * (size_t)n, Qf.etaMomentum, sizeof(double) * n);
-    memcpy(js5 + 3 * (size_t)n, Qf.zetaMomentum, sizeof(double) * n);
-    memcpy(js5 + 4 * (size_t)n, Qf.Energy, sizeof(double) * n);
+    copy_out(js5, &Qf, n);
 }
 
 void ref_free(void)

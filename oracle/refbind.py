@@ -40,8 +40,9 @@ class RefParams(C.Structure):
     ]
 
 
-def ref_available(order: int, dim: int) -> bool:
-    return os.path.exists(os.path.join(HERE, "_ref", f"libshockref_w{order}_{dim}d.so"))
+def ref_available(order: int, dim: int, extended: bool = False) -> bool:
+    tag = "80" if extended else ""
+    return os.path.exists(os.path.join(HERE, "_ref", f"libshockref{tag}_w{order}_{dim}d.so"))
 
 
 class RefSolver:
@@ -49,11 +50,13 @@ class RefSolver:
 
     _libs: dict = {}
 
-    def __init__(self, case):
+    def __init__(self, case, extended=False):
+        """extended=True loads the PRECISION=3 (80-bit long double) build."""
         self.case = case
-        key = (case.order, case.dim)
+        tag = "80" if extended else ""
+        key = (case.order, case.dim, tag)
         if key not in RefSolver._libs:
-            path = os.path.join(HERE, "_ref", f"libshockref_w{case.order}_{case.dim}d.so")
+            path = os.path.join(HERE, "_ref", f"libshockref{tag}_w{case.order}_{case.dim}d.so")
             if not os.path.exists(path):
                 raise FileNotFoundError(path + " (run make -C oracle ref)")
             lib = C.CDLL(path, mode=os.RTLD_LOCAL)

@@ -21,6 +21,7 @@ typedef double real;
 #define R_SQRT sqrt
 #define R_FABS fabs
 #define R_POW pow
+#define ORACLE_PHASE(name) ((void)0)
 #else
 #include ORACLE_REAL
 #endif
@@ -736,14 +737,19 @@ static void viscous_direction(oc_solver *s, int d, int clean)
  * ------------------------------------------------------------------------- */
 static void stage_rhs(oc_solver *s)
 {
+    static const char *wn[3] = {"weno_xi", "weno_eta", "weno_zeta"};
+    static const char *vn[3] = {"visc_xi", "visc_eta", "visc_zeta"};
     for (int c = 0; c < 5; c++) memset(s->Q[c], 0, sizeof(real) * s->NG);
     periodic_fill(s, (double **)s->Ur, 5, 0);
+    ORACLE_PHASE("ghosts");
     calc_values(s);
     dirichlet_faces(s, s->Ur, 1);
-    for (int d = 0; d < s->p.dim; d++) weno_direction(s, d);
+    ORACLE_PHASE("prim");
+    for (int d = 0; d < s->p.dim; d++) { weno_direction(s, d); ORACLE_PHASE(wn[d]); }
     if (!s->p.inviscid) {
         nodal_derivatives(s);
-        for (int d = 0; d < s->p.dim; d++) viscous_direction(s, d, 0);
+        ORACLE_PHASE("nodal");
+        for (int d = 0; d < s->p.dim; d++) { viscous_direction(s, d, 0); ORACLE_PHASE(vn[d]); }
     }
     if (s->js)
         for (int i = s->sr[0]; i <= s->er[0]; i++)
@@ -780,7 +786,9 @@ void oc_steps(oc_solver *s, int n)
         for (int c = 0; c < 5; c++) memset(s->Qs[c], 0, sizeof(real) * s->NG);
         for (int st = 0; st < s->p.time_order; st++) {
             stage_rhs(s);
+            ORACLE_PHASE("source");
             rk_update(s, st);
+            ORACLE_PHASE("rk");
         }
         for (int c = 0; c < 5; c++) memcpy(s->Un[c], s->Ur[c], sizeof(real) * s->NG);
     }

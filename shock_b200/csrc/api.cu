@@ -145,6 +145,7 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
     if (p->order != 5 && p->order != 9) return fail(SHOCK_EINVAL, "order must be 5 or 9");
     if (p->time_order != 3 && p->time_order != 4) return fail(SHOCK_EINVAL, "time_order must be 3 or 4");
     if (p->precision != SHOCK_FP64 && p->precision != SHOCK_MIXED) return fail(SHOCK_EINVAL, "bad precision");
+    if (p->precision == SHOCK_MIXED) return fail(SHOCK_EINVAL, "mixed precision kernels are not built yet");
     int g = (p->order + 1) / 2;
     if (p->ni < g + 1 || p->nj < g + 1 || (p->dim == 3 && p->nk < g + 1))
         return fail(SHOCK_EINVAL, "block smaller than the stencil (%d points per axis needed)", g + 1);
@@ -287,11 +288,18 @@ int shock_upload_state(shock_ctx *c, const double *prim5)
     if (!c || !prim5) return fail(SHOCK_EINVAL, "null argument");
     CK(cudaSetDevice(c->device));
     size_t nb = sizeof(double) * c->G.NG;
-    for (int b = 0; b < 3; b++)
-        for (int f = 0; f < 5; f++)
-            CK(cudaMemcpyAsync(c->buf[b][f], prim5 + (size_t)f * c->G.NG, nb, cudaMemcpyHostToDevice, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
     c->un = 0;
+    for (int f = 0; f < 5; f++)
+        CK(cudaMemcpyAsync(c->buf[0][f], prim5 + (size_t)f * c->G.NG, nb, cudaMemcpyHostToDevice, c->stream));
+    // The stage buffers are written before they are read except for the
+    // ghost layers of non-periodic (Dirichlet) faces, which never change.
+    bool dirichlet = false;
+    for (int a = 0; a < c->p.dim; a++) dirichlet |= !c->p.periodic[a];
+    if (dirichlet)
+        for (int b = 1; b < 3; b++)
+            for (int f = 0; f < 5; f++)
+                CK(cudaMemcpyAsync(c->buf[b][f], c->buf[0][f], nb, cudaMemcpyDeviceToDevice, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
     return SHOCK_OK;
 }
 
@@ -403,6 +411,74 @@ int shock_kernels_per_step(const shock_ctx *c, int *n)
 {
     if (!c || !n) return fail(SHOCK_EINVAL, "null argument");
     *n = c->kernels_per_step;
+    return SHOCK_OK;
+}
+
+int shock_profile_stage(shock_ctx *c, int max, char *names, float *ms, int *count)
+{
+    if (!c || !names || !ms || !count) return fail(SHOCK_EINVAL, "null argument");
+    CK(cudaSetDevice(c->device));
+    std::vector<cudaEvent_t> ev;
+    std::vector<std::string> nm;
+    auto mark = [&](const char *name) {
+        cudaEvent_t e;
+        cudaEventCreate(&e);
+        cudaEventRecord(e, c->stream);
+        ev.push_back(e);
+        if (name) nm.push_back(name);
+    };
+    double *const *in = c->buf[c->un];
+    const double *cin[5] = {in[0], in[1], in[2], in[3], in[4]};
+    static const char *dn[3] = {"xi", "eta", "zeta"};
+    mark(nullptr);
+    launch_ghosts(c->G, in, c->stream); mark("ghosts");
+    launch_prim(c->G, c->P, cin, c->F, c->stream); mark("prim");
+    if (!c->p.inviscid) { launch_nodal(c->G, cin, c->F, c->stream); mark("nodal"); }
+    for (int d = 0; d < c->p.dim; d++) {
+        launch_weno(c->G, c->P, c->p.precision, d, d == 0, cin, c->F, c->stream);
+        nm.push_back(std::string("weno_") + dn[d]);
+        cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, c->stream); ev.push_back(e);
+    }
+    if (!c->p.inviscid)
+        for (int d = 0; d < c->p.dim; d++) {
+            launch_viscous(c->G, c->P, c->p.precision, d, cin, c->F, c->stream);
+            nm.push_back(std::string("visc_") + dn[d]);
+            cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, c->stream); ev.push_back(e);
+        }
+    // RK update into a scratch buffer (the running state is left untouched)
+    int out = (c->un + 1) % 3;
+    Fields F = c->F;
+    for (int q = 0; q < 5; q++) F.Un[q] = c->buf[c->un][q];
+    launch_rk(c->G, c->rk[0], c->p.tau, cin, c->buf[out], F, c->has_source, c->stream); mark("rk");
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaGetLastError());
+    int n = (int)nm.size();
+    for (int i = 0; i < n && i < max; i++) {
+        float t = 0;
+        cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
+        ms[i] = t;
+        strncpy(names + 48 * i, nm[i].c_str(), 47);
+        names[48 * i + 47] = 0;
+    }
+    for (auto e : ev) cudaEventDestroy(e);
+    for (int q = 0; q < 5; q++) CK(cudaMemsetAsync(c->F.Qs[q], 0, sizeof(double) * c->G.NG, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *count = n < max ? n : max;
+    return SHOCK_OK;
+}
+
+int shock_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops)
+{
+    if (!fp64_tflops || !fp32_tflops) return fail(SHOCK_EINVAL, "null argument");
+    CK(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CK(cudaGetDeviceProperties(&prop, device));
+    cudaStream_t s;
+    CK(cudaStreamCreate(&s));
+    *fp64_tflops = fma_probe(1, prop.multiProcessorCount, s);
+    *fp32_tflops = fma_probe(0, prop.multiProcessorCount, s);
+    cudaStreamDestroy(s);
+    CK(cudaGetLastError());
     return SHOCK_OK;
 }
 

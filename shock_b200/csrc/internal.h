@@ -86,5 +86,6 @@ void launch_copy_state(const Grid &G, const double *const src[5], double *const 
 void launch_nan_check(const Grid &G, const double *rho, unsigned int *flag, cudaStream_t s);
 void launch_add_source(const Grid &G, const Fields &F, cudaStream_t s);
 void prepare_kernels();
+double fma_probe(int fp64, int sms, cudaStream_t s);
 
 }  // namespace shock

@@ -939,3 +939,58 @@ void launch_copy_state(const Grid &G, const double *const src[5], double *const 
 }
 
 }  // namespace shock
+
+namespace shock {
+
+// ---------------------------------------------------------------------------
+// FMA throughput probe: every thread runs independent chains of fused
+// multiply-adds on registers (no memory traffic), giving the device's
+// FP64 / FP32 pipe peak for the roofline denominators.
+// ---------------------------------------------------------------------------
+template <typename T, int CHAINS, int ITERS>
+__global__ void k_fma_probe(T *out, T seed)
+{
+    T a[CHAINS];
+#pragma unroll
+    for (int c = 0; c < CHAINS; c++) a[c] = seed + T(threadIdx.x + c);
+    const T m = T(0.999999), b = T(1e-7);
+#pragma unroll 4
+    for (int it = 0; it < ITERS; it++) {
+#pragma unroll
+        for (int c = 0; c < CHAINS; c++) a[c] = fma(a[c], m, b);
+    }
+    T s = T(0);
+#pragma unroll
+    for (int c = 0; c < CHAINS; c++) s += a[c];
+    if (s == T(-12345.678)) out[threadIdx.x] = s;   // keeps the chains alive
+}
+
+double fma_probe(int fp64, int sms, cudaStream_t s)
+{
+    constexpr int CH = 8, IT = 4096;
+    void *buf = nullptr;
+    cudaMalloc(&buf, 4096 * sizeof(double));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    dim3 grid(sms * 8), block(256);
+    double best = 0;
+    for (int rep = 0; rep < 4; rep++) {
+        cudaEventRecord(e0, s);
+        if (fp64) k_fma_probe<double, CH, IT><<<grid, block, 0, s>>>((double *)buf, 1.0);
+        else k_fma_probe<float, CH, IT><<<grid, block, 0, s>>>((float *)buf, 1.0f);
+        cudaEventRecord(e1, s);
+        cudaEventSynchronize(e1);
+        float ms = 0;
+        cudaEventElapsedTime(&ms, e0, e1);
+        double flops = 2.0 * CH * IT * (double)grid.x * block.x;
+        double tf = flops / (ms * 1e-3) / 1e12;
+        if (tf > best) best = tf;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(buf);
+    return best;
+}
+
+}  // namespace shock

@@ -6,7 +6,10 @@ on small seeded cases and stores, per case, the inputs (grid, initial
 primitives, parameters, manufactured-solution data) and the outputs
 (geometry, one right-hand side, the state after a few full RK steps).
 The fixtures pin the CPU restatement in oracle/ (tests/test_oracle_pin.py)
-and, through it, the GPU kernels.
+and, through it, the GPU kernels.  The same reference sources built at
+PRECISION=3 (80-bit long double) give rhs80/state80: the distance between
+the FP64 and the 80-bit results is SHOCK's own FP64 rounding floor, which
+sets the parity tolerance on ill-conditioned cases (low Mach, WENO9).
 
 Usage: python tests/golden/make_golden.py
 """
@@ -59,6 +62,10 @@ def main():
         r.steps(nsteps)
         d["nsteps"] = nsteps
         d["state"] = r.state(0)[:5]
+        r80 = RefSolver(c, extended=True)
+        d["rhs80"] = r80.rhs()
+        r80.steps(nsteps)
+        d["state80"] = r80.state(0)[:5]
         np.savez_compressed(os.path.join(OUT, name + ".npz"), **d)
         print("wrote", name)
 
