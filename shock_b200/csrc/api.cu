@@ -145,7 +145,6 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
     if (p->order != 5 && p->order != 9) return fail(SHOCK_EINVAL, "order must be 5 or 9");
     if (p->time_order != 3 && p->time_order != 4) return fail(SHOCK_EINVAL, "time_order must be 3 or 4");
     if (p->precision != SHOCK_FP64 && p->precision != SHOCK_MIXED) return fail(SHOCK_EINVAL, "bad precision");
-    if (p->precision == SHOCK_MIXED) return fail(SHOCK_EINVAL, "mixed precision kernels are not built yet");
     int g = (p->order + 1) / 2;
     if (p->ni < g + 1 || p->nj < g + 1 || (p->dim == 3 && p->nk < g + 1))
         return fail(SHOCK_EINVAL, "block smaller than the stencil (%d points per axis needed)", g + 1);

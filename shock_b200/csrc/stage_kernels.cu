@@ -18,6 +18,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <type_traits>
 
 #include "internal.h"
 
@@ -252,9 +253,11 @@ struct Axes {
     static constexpr bool CONTIG = (D == DIM - 1);   // sweep along the contiguous axis
 };
 
-constexpr int TL = 15;       // cells per tile along the sweep
-constexpr int NROW = TL + 1; // face rows (threadIdx.y)
-constexpr int NLANE = 32;    // lines per tile
+constexpr int TL = 15;         // cells per tile along the sweep
+constexpr int NFACE = TL + 1;  // faces per tile line
+constexpr int NLANE = 32;      // lines per tile
+constexpr int NROWT = 8;       // thread rows; each handles faces row and row + 8
+constexpr int NTHR = NLANE * NROWT;
 
 // Per-point values staged for the WENO face computation.
 enum { WF0 = 0, WU0 = 5, WVU = 10, WVV, WVW, WC, WLAM, WJ, WN0 };
@@ -265,43 +268,50 @@ struct WenoNV {
     static constexpr int NV = WN0 + NN;
 };
 
-// ---------------------------------------------------------------------------
-// weno_d (FP64): thread-per-face characteristic WENO (src/WENO.c:206-494).
-// ---------------------------------------------------------------------------
+struct Tile {
+    int c0, l0, nD, nL;
+    long long sD, sL, base;
+    bool lane_ok;
+};
+
+template <int DIM, int D>
+__device__ __forceinline__ Tile make_tile(const Grid &G, int lane)
+{
+    using A = Axes<DIM, D>;
+    Tile t;
+    t.c0 = G.g + blockIdx.x * TL;
+    t.l0 = G.g + blockIdx.y * NLANE;
+    const int oth = (DIM == 3) ? G.g + blockIdx.z : 0;
+    t.nD = G.n[D];
+    t.nL = G.n[A::LAT];
+    t.sD = G.st[D];
+    t.sL = G.st[A::LAT];
+    const long long sO = (DIM == 3) ? G.st[A::OTH] : 0;
+    t.base = (long long)t.l0 * t.sL + (long long)oth * sO;
+    t.lane_ok = (t.l0 + lane) < G.g + t.nL;
+    return t;
+}
+
+// Stage point fluxes, conserved variables, face-state inputs and the local
+// spectral radius of NP points per lane: points c0-1-r .. c0+TL+r.
 template <int DIM, int ORDER, int D>
-__global__ void __launch_bounds__(NLANE *NROW, 1)
-    k_weno(Grid G, Phys P, bool first, const double *__restrict__ R, const double *__restrict__ Uu,
-           const double *__restrict__ Vv, const double *__restrict__ Ww, const double *__restrict__ Ee,
-           Fields F)
+__device__ __forceinline__ void stage_weno(const Grid &G, const Phys &P, const Tile &T, double *sh,
+                                           const double *__restrict__ R, const double *__restrict__ Uu,
+                                           const double *__restrict__ Vv, const double *__restrict__ Ww,
+                                           const double *__restrict__ Ee, const Fields &F)
 {
     using A = Axes<DIM, D>;
     constexpr int r = (ORDER - 1) / 2;
     constexpr int NP = TL + 2 * r + 2;
-    constexpr int NV = WenoNV<DIM>::NV;
-    constexpr int NN = WenoNV<DIM>::NN;
-    extern __shared__ double smem[];
-    double *sh = smem;                         // [NV][NP][NLANE]
-    double *fh = smem + NV * NP * NLANE;       // [5][NROW][NLANE]
 #define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
-#define FH(c, f, l) fh[((c) * NROW + (f)) * NLANE + (l)]
-
-    const int lane = threadIdx.x, row = threadIdx.y;
-    const int c0 = G.g + blockIdx.x * TL;              // first cell of the tile (ghosted index)
-    const int l0 = G.g + blockIdx.y * NLANE;
-    const int oth = (DIM == 3) ? G.g + blockIdx.z : 0;
-    const int nD = G.n[D], nL = G.n[A::LAT];
-    const long long sD = G.st[D], sL = G.st[A::LAT], sO = (DIM == 3) ? G.st[A::OTH] : 0;
-    const long long base = (long long)l0 * sL + (long long)oth * sO;
-
-    // ---- stage point quantities ------------------------------------------
-    const int tid = row * NLANE + lane;
-    for (int it = tid; it < NP * NLANE; it += NLANE * NROW) {
+    const int tid = threadIdx.y * NLANE + threadIdx.x;
+    for (int it = tid; it < NP * NLANE; it += NTHR) {
         int t, l;
         if (A::CONTIG) { t = it % NP; l = it / NP; }
         else { l = it % NLANE; t = it / NLANE; }
-        int pd = c0 - 1 - r + t;
-        if (l0 + l >= G.g + nL || pd >= G.N[D]) continue;
-        long long o = base + (long long)l * sL + (long long)pd * sD;
+        int pd = T.c0 - 1 - r + t;
+        if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
+        long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
         double rho = R[o], u = Uu[o], v = Vv[o], w = (DIM == 3) ? Ww[o] : 0.0, e = Ee[o];
         double p = F.p[o], c = F.c[o], J = F.J[o];
         double mx, my, mz, th, nrm;
@@ -343,150 +353,309 @@ __global__ void __launch_bounds__(NLANE *NROW, 1)
             SH(WN0 + 1, t, l) = my / nrm;
         }
     }
-    __syncthreads();
+#undef SH
+}
 
-    // ---- one face per thread ----------------------------------------------
-    const bool lane_ok = (l0 + lane) < G.g + nL;
-    const int f = row;                 // face between points ta = r+f and ta+1
-    const int ta = r + f;
-    if (lane_ok && (c0 - 1 + f) <= G.g + nD - 1) {
-        const double gm = P.gamma;
-        double u = 0.5 * (SH(WVU, ta, lane) + SH(WVU, ta + 1, lane));
-        double v = 0.5 * (SH(WVV, ta, lane) + SH(WVV, ta + 1, lane));
-        double w = 0.5 * (SH(WVW, ta, lane) + SH(WVW, ta + 1, lane));
-        double rho = 0.5 * (SH(WU0, ta, lane) + SH(WU0, ta + 1, lane));
-        double c = 0.5 * (SH(WC, ta, lane) + SH(WC, ta + 1, lane));
-        double nx, ny, nz;
-        if (DIM == 3) {
-            double nd = 0.5 * (SH(WN0, ta, lane) + SH(WN0, ta + 1, lane));
-            nx = D == 0 ? nd : 0.0;
-            ny = D == 1 ? nd : 0.0;
-            nz = D == 2 ? nd : 0.0;
-        } else {
-            nx = 0.5 * (SH(WN0, ta, lane) + SH(WN0, ta + 1, lane));
-            ny = 0.5 * (SH(WN0 + 1, ta, lane) + SH(WN0 + 1, ta + 1, lane));
-            nz = 0.0;
-        }
-        (void)NN;
-        const double q2 = u * u + v * v + w * w;
-        const double M2 = q2 / (c * c);      // M*M with M = sqrt(q2)/c
-        const double un = u * nx + v * ny + w * nz;
-        const double sq2 = 1.4142135623730951;
-        const double gc = (gm - 1.0) / (c * c);
-        const double irho = 1.0 / rho;
-        const double isc = 1.0 / (c * sq2);
-        const double kin = 1.0 - 0.5 * (gm - 1.0) * M2;
-        const double jh = (SH(WJ, ta, lane) + SH(WJ, ta + 1, lane)) / 2.0;
-        double lam = 0.0;
-#pragma unroll
-        for (int s = 0; s <= 2 * r + 1; s++) {
-            double lm = SH(WLAM, f + s, lane);
-            lam = lam < lm ? lm : lam;
-        }
-        const double a = lam * jh;
-        double out[5] = {0., 0., 0., 0., 0.};
-#pragma unroll 1
-        for (int ch = 0; ch < 5; ch++) {
-            double L0, L1, L2, L3, L4;
-            switch (ch) {
-            case 0:
-                L0 = nx * kin - irho * (v * nz - w * ny); L1 = gc * u * nx; L2 = gc * v * nx + nz * irho;
-                L3 = gc * w * nx - ny * irho; L4 = -gc * nx; break;
-            case 1:
-                L0 = ny * kin - irho * (w * nx - u * nz); L1 = gc * u * ny - nz * irho; L2 = gc * v * ny;
-                L3 = gc * w * ny + nx * irho; L4 = -gc * ny; break;
-            case 2:
-                L0 = nz * kin - irho * (u * ny - v * nx); L1 = gc * u * nz + ny * irho; L2 = gc * v * nz - nx * irho;
-                L3 = gc * w * nz; L4 = -gc * nz; break;
-            case 3:
-                L0 = isc * ((gm - 1.0) * q2 / 2. - c * un); L1 = (-(gm - 1.0) * u / c + nx) / sq2;
-                L2 = (-(gm - 1.0) * v / c + ny) / sq2; L3 = (-(gm - 1.0) * w / c + nz) / sq2; L4 = (gm - 1.) * isc; break;
-            default:
-                L0 = isc * ((gm - 1.0) * q2 / 2. + c * un); L1 = (-(gm - 1.0) * u / c - nx) / sq2;
-                L2 = (-(gm - 1.0) * v / c - ny) / sq2; L3 = (-(gm - 1.0) * w / c - nz) / sq2; L4 = (gm - 1.) * isc; break;
-            }
-            double Pp[2 * r + 2], Pm[2 * r + 2];
-#pragma unroll
-            for (int s = 0; s <= 2 * r + 1; s++) {
-                int t = f + s;
-                double lf = L0 * SH(WF0 + 0, t, lane) + L1 * SH(WF0 + 1, t, lane) + L2 * SH(WF0 + 2, t, lane)
-                            + L3 * SH(WF0 + 3, t, lane) + L4 * SH(WF0 + 4, t, lane);
-                double lu = L0 * SH(WU0 + 0, t, lane) + L1 * SH(WU0 + 1, t, lane) + L2 * SH(WU0 + 2, t, lane)
-                            + L3 * SH(WU0 + 3, t, lane) + L4 * SH(WU0 + 4, t, lane);
-                Pp[s] = 0.5 * (lf + a * lu);
-                Pm[s] = 0.5 * (lf - a * lu);
-            }
-            double phi;
-            if (ORDER == 5) {
-                double dp[4], dm[4];
-#pragma unroll
-                for (int s = 0; s < 4; s++) {
-                    dp[s] = Pp[s + 1] - Pp[s];
-                    dm[s] = Pm[2 * r + 1 - s] - Pm[2 * r - s];
-                }
-                phi = -phi_w5<double>(dp, P.eps64) + phi_w5<double>(dm, P.eps64);
-            } else {
-                double fp[9], fm[9], dp[8], dm[8];
-#pragma unroll
-                for (int s = 0; s < 9; s++) { fp[s] = Pp[s]; fm[s] = Pm[2 * r + 1 - s]; }
-#pragma unroll
-                for (int s = 0; s < 8; s++) { dp[s] = fp[s + 1] - fp[s]; dm[s] = fm[s] - fm[s + 1]; }
-                phi = -phi_w9<double>(fp, dp, P.eps64) + phi_w9<double>(fm, dm, P.eps64);
-            }
-            // right eigenvector column ch
-            switch (ch) {
-            case 0:
-                out[0] += nx * phi; out[1] += u * nx * phi; out[2] += (v * nx + rho * nz) * phi;
-                out[3] += (w * nx - rho * ny) * phi; out[4] += (q2 / 2. * nx + rho * (v * nz - w * ny)) * phi; break;
-            case 1:
-                out[0] += ny * phi; out[1] += (u * ny - rho * nz) * phi; out[2] += v * ny * phi;
-                out[3] += (w * ny + rho * nx) * phi; out[4] += (q2 / 2. * ny + rho * (w * nx - u * nz)) * phi; break;
-            case 2:
-                out[0] += nz * phi; out[1] += (u * nz + rho * ny) * phi; out[2] += (v * nz - rho * nx) * phi;
-                out[3] += w * nz * phi; out[4] += (q2 / 2. * nz + rho * (u * ny - v * nx)) * phi; break;
-            case 3: {
-                double s = isc * phi;
-                out[0] += s; out[1] += (u + nx * c) * s; out[2] += (v + ny * c) * s; out[3] += (w + nz * c) * s;
-                out[4] += (q2 / 2. + c * c / (gm - 1.) + c * un) * s; break;
-            }
-            default: {
-                double s = isc * phi;
-                out[0] += s; out[1] += (u - nx * c) * s; out[2] += (v - ny * c) * s; out[3] += (w - nz * c) * s;
-                out[4] += (q2 / 2. + c * c / (gm - 1.) - c * un) * s; break;
-            }
-            }
-        }
-        // central part (src/WENO.c:1754-1816)
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-            double th;
-            if (ORDER == 9)
-                th = 1. / 840. * (533. * (SH(WF0 + q, ta + 1, lane) + SH(WF0 + q, ta, lane))
-                                  - 139. * (SH(WF0 + q, ta + 2, lane) + SH(WF0 + q, ta - 1, lane))
-                                  + 29. * (SH(WF0 + q, ta + 3, lane) + SH(WF0 + q, ta - 2, lane))
-                                  - 3. * (SH(WF0 + q, ta + 4, lane) + SH(WF0 + q, ta - 3, lane)));
-            else
-                th = 1. / 12. * (-1. * (SH(WF0 + q, ta - 1, lane) + SH(WF0 + q, ta + 2, lane))
-                                 + 7. * (SH(WF0 + q, ta, lane) + SH(WF0 + q, ta + 1, lane)));
-            FH(q, f, lane) = out[q] + th;
-        }
-    }
-    __syncthreads();
+// Face state (arithmetic means, src/WENO.c:1104-1139) and derived scalars.
+template <typename T>
+struct FaceState {
+    T u, v, w, rho, c, nx, ny, nz, q2, un, gc, irho, isc, kin, gm;
+};
 
-    // ---- flux difference into Q ---------------------------------------------
-    if (lane_ok && row < TL && c0 + row <= G.g + nD - 1) {
-        long long o = base + (long long)lane * sL + (long long)(c0 + row) * sD;
-#pragma unroll
-        for (int q = 0; q < 5; q++) {
-            if (DIM == 2 && q == 3) {
-                // zetaMomentum stays untouched in 2D except for the flux difference of zeros
-            }
-            double prev = first ? 0.0 : F.Q[q][o];
-            F.Q[q][o] = prev - (FH(q, row + 1, lane) - FH(q, row, lane));
-        }
+template <int DIM, int ORDER, int D, typename T>
+__device__ __forceinline__ FaceState<T> face_state(const Phys &P, const double *sh, int ta, int lane)
+{
+    constexpr int r = (ORDER - 1) / 2;
+    constexpr int NP = TL + 2 * r + 2;
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+    FaceState<T> s;
+    s.gm = (T)P.gamma;
+    s.u = T(0.5) * (T)(SH(WVU, ta, lane) + SH(WVU, ta + 1, lane));
+    s.v = T(0.5) * (T)(SH(WVV, ta, lane) + SH(WVV, ta + 1, lane));
+    s.w = T(0.5) * (T)(SH(WVW, ta, lane) + SH(WVW, ta + 1, lane));
+    s.rho = T(0.5) * (T)(SH(WU0, ta, lane) + SH(WU0, ta + 1, lane));
+    s.c = T(0.5) * (T)(SH(WC, ta, lane) + SH(WC, ta + 1, lane));
+    if (DIM == 3) {
+        T nd = T(0.5) * (T)(SH(WN0, ta, lane) + SH(WN0, ta + 1, lane));
+        s.nx = D == 0 ? nd : T(0);
+        s.ny = D == 1 ? nd : T(0);
+        s.nz = D == 2 ? nd : T(0);
+    } else {
+        s.nx = T(0.5) * (T)(SH(WN0, ta, lane) + SH(WN0, ta + 1, lane));
+        s.ny = T(0.5) * (T)(SH(WN0 + 1, ta, lane) + SH(WN0 + 1, ta + 1, lane));
+        s.nz = T(0);
     }
 #undef SH
-#undef FH
+    s.q2 = s.u * s.u + s.v * s.v + s.w * s.w;
+    T M2 = s.q2 / (s.c * s.c);
+    s.un = s.u * s.nx + s.v * s.ny + s.w * s.nz;
+    s.gc = (s.gm - T(1)) / (s.c * s.c);
+    s.irho = T(1) / s.rho;
+    s.isc = T(1) / (s.c * T(1.4142135623730951));
+    s.kin = T(1) - T(0.5) * (s.gm - T(1)) * M2;
+    return s;
+}
+
+// Row ch of the left eigenvector matrix (src/WENO.c:1202-1236).
+template <typename T>
+__device__ __forceinline__ void left_row(const FaceState<T> &s, int ch, T &L0, T &L1, T &L2, T &L3, T &L4)
+{
+    const T sq2 = T(1.4142135623730951), g1 = s.gm - T(1);
+    switch (ch) {
+    case 0:
+        L0 = s.nx * s.kin - s.irho * (s.v * s.nz - s.w * s.ny); L1 = s.gc * s.u * s.nx;
+        L2 = s.gc * s.v * s.nx + s.nz * s.irho; L3 = s.gc * s.w * s.nx - s.ny * s.irho; L4 = -s.gc * s.nx; break;
+    case 1:
+        L0 = s.ny * s.kin - s.irho * (s.w * s.nx - s.u * s.nz); L1 = s.gc * s.u * s.ny - s.nz * s.irho;
+        L2 = s.gc * s.v * s.ny; L3 = s.gc * s.w * s.ny + s.nx * s.irho; L4 = -s.gc * s.ny; break;
+    case 2:
+        L0 = s.nz * s.kin - s.irho * (s.u * s.ny - s.v * s.nx); L1 = s.gc * s.u * s.nz + s.ny * s.irho;
+        L2 = s.gc * s.v * s.nz - s.nx * s.irho; L3 = s.gc * s.w * s.nz; L4 = -s.gc * s.nz; break;
+    case 3:
+        L0 = s.isc * (g1 * s.q2 / T(2) - s.c * s.un); L1 = (-g1 * s.u / s.c + s.nx) / sq2;
+        L2 = (-g1 * s.v / s.c + s.ny) / sq2; L3 = (-g1 * s.w / s.c + s.nz) / sq2; L4 = g1 * s.isc; break;
+    default:
+        L0 = s.isc * (g1 * s.q2 / T(2) + s.c * s.un); L1 = (-g1 * s.u / s.c - s.nx) / sq2;
+        L2 = (-g1 * s.v / s.c - s.ny) / sq2; L3 = (-g1 * s.w / s.c - s.nz) / sq2; L4 = g1 * s.isc; break;
+    }
+}
+
+// out += (column ch of the right eigenvector matrix) * phi (src/WENO.c:1176-1200).
+template <typename T>
+__device__ __forceinline__ void add_right_col(const FaceState<T> &s, int ch, T phi, T *out)
+{
+    switch (ch) {
+    case 0:
+        out[0] += s.nx * phi; out[1] += s.u * s.nx * phi; out[2] += (s.v * s.nx + s.rho * s.nz) * phi;
+        out[3] += (s.w * s.nx - s.rho * s.ny) * phi;
+        out[4] += (s.q2 / T(2) * s.nx + s.rho * (s.v * s.nz - s.w * s.ny)) * phi; break;
+    case 1:
+        out[0] += s.ny * phi; out[1] += (s.u * s.ny - s.rho * s.nz) * phi; out[2] += s.v * s.ny * phi;
+        out[3] += (s.w * s.ny + s.rho * s.nx) * phi;
+        out[4] += (s.q2 / T(2) * s.ny + s.rho * (s.w * s.nx - s.u * s.nz)) * phi; break;
+    case 2:
+        out[0] += s.nz * phi; out[1] += (s.u * s.nz + s.rho * s.ny) * phi; out[2] += (s.v * s.nz - s.rho * s.nx) * phi;
+        out[3] += s.w * s.nz * phi;
+        out[4] += (s.q2 / T(2) * s.nz + s.rho * (s.u * s.ny - s.v * s.nx)) * phi; break;
+    case 3: {
+        T sc = s.isc * phi;
+        out[0] += sc; out[1] += (s.u + s.nx * s.c) * sc; out[2] += (s.v + s.ny * s.c) * sc;
+        out[3] += (s.w + s.nz * s.c) * sc; out[4] += (s.q2 / T(2) + s.c * s.c / (s.gm - T(1)) + s.c * s.un) * sc; break;
+    }
+    default: {
+        T sc = s.isc * phi;
+        out[0] += sc; out[1] += (s.u - s.nx * s.c) * sc; out[2] += (s.v - s.ny * s.c) * sc;
+        out[3] += (s.w - s.nz * s.c) * sc; out[4] += (s.q2 / T(2) + s.c * s.c / (s.gm - T(1)) - s.c * s.un) * sc; break;
+    }
+    }
+}
+
+// WENO part of the face flux in FP64 (src/WENO.c:296-430): split fluxes
+// F +/- lambda J_{i+1/2} U projected on the characteristic fields, Phi+,
+// Phi-, back-projection.  f: face index in the tile (points f..f+2r+1).
+template <int DIM, int ORDER, int D>
+__device__ __forceinline__ void face_weno_fp64(const Phys &P, const double *sh, int f, int lane, double *out)
+{
+    constexpr int r = (ORDER - 1) / 2;
+    constexpr int NP = TL + 2 * r + 2;
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+    const int ta = r + f;
+    const FaceState<double> s = face_state<DIM, ORDER, D, double>(P, sh, ta, lane);
+    const double jh = (SH(WJ, ta, lane) + SH(WJ, ta + 1, lane)) / 2.0;
+    double lam = 0.0;
+#pragma unroll
+    for (int q = 0; q <= 2 * r + 1; q++) {
+        double lm = SH(WLAM, f + q, lane);
+        lam = lam < lm ? lm : lam;
+    }
+    const double a = lam * jh;
+#pragma unroll
+    for (int q = 0; q < 5; q++) out[q] = 0.0;
+#pragma unroll 1
+    for (int ch = 0; ch < 5; ch++) {
+        double L0, L1, L2, L3, L4;
+        left_row<double>(s, ch, L0, L1, L2, L3, L4);
+        double Pp[2 * r + 2], Pm[2 * r + 2];
+#pragma unroll
+        for (int q = 0; q <= 2 * r + 1; q++) {
+            int t = f + q;
+            double lf = L0 * SH(WF0 + 0, t, lane) + L1 * SH(WF0 + 1, t, lane) + L2 * SH(WF0 + 2, t, lane)
+                        + L3 * SH(WF0 + 3, t, lane) + L4 * SH(WF0 + 4, t, lane);
+            double lu = L0 * SH(WU0 + 0, t, lane) + L1 * SH(WU0 + 1, t, lane) + L2 * SH(WU0 + 2, t, lane)
+                        + L3 * SH(WU0 + 3, t, lane) + L4 * SH(WU0 + 4, t, lane);
+            Pp[q] = 0.5 * (lf + a * lu);
+            Pm[q] = 0.5 * (lf - a * lu);
+        }
+        double phi;
+        if (ORDER == 5) {
+            double dp[4], dm[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                dp[q] = Pp[q + 1] - Pp[q];
+                dm[q] = Pm[2 * r + 1 - q] - Pm[2 * r - q];
+            }
+            phi = -phi_w5<double>(dp, P.eps64) + phi_w5<double>(dm, P.eps64);
+        } else {
+            double fp[9], fm[9], dp[8], dm[8];
+#pragma unroll
+            for (int q = 0; q < 9; q++) { fp[q] = Pp[q]; fm[q] = Pm[2 * r + 1 - q]; }
+#pragma unroll
+            for (int q = 0; q < 8; q++) { dp[q] = fp[q + 1] - fp[q]; dm[q] = fm[q] - fm[q + 1]; }
+            phi = -phi_w9<double>(fp, dp, P.eps64) + phi_w9<double>(fm, dm, P.eps64);
+        }
+        add_right_col<double>(s, ch, phi, out);
+    }
+#undef SH
+}
+
+// Mixed form of the same: the projection, indicators, weights and
+// back-projection in FP32 on FP64-formed point-to-point differences dl.
+template <int DIM, int ORDER, int D>
+__device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh, const float *dl, int f, int lane,
+                                                double *outd)
+{
+    constexpr int r = (ORDER - 1) / 2;
+    constexpr int NP = TL + 2 * r + 2;
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+#define DL(v, t, l) dl[((v) * (NP - 1) + (t)) * NLANE + (l)]
+    const int ta = r + f;
+    const FaceState<float> s = face_state<DIM, ORDER, D, float>(P, sh, ta, lane);
+    const double jh = (SH(WJ, ta, lane) + SH(WJ, ta + 1, lane)) / 2.0;
+    double lam = 0.0;
+#pragma unroll
+    for (int q = 0; q <= 2 * r + 1; q++) {
+        double lm = SH(WLAM, f + q, lane);
+        lam = lam < lm ? lm : lam;
+    }
+    const float a = (float)(lam * jh);
+    const float eps = P.eps32;
+    float out[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll 1
+    for (int ch = 0; ch < 5; ch++) {
+        float L0, L1, L2, L3, L4;
+        left_row<float>(s, ch, L0, L1, L2, L3, L4);
+        float dp[2 * r + 1], dmv[2 * r + 1];
+#pragma unroll
+        for (int q = 0; q <= 2 * r; q++) {
+            int t = f + q;
+            float lf = L0 * DL(0, t, lane) + L1 * DL(1, t, lane) + L2 * DL(2, t, lane) + L3 * DL(3, t, lane)
+                       + L4 * DL(4, t, lane);
+            float lu = L0 * DL(5, t, lane) + L1 * DL(6, t, lane) + L2 * DL(7, t, lane) + L3 * DL(8, t, lane)
+                       + L4 * DL(9, t, lane);
+            dp[q] = 0.5f * (lf + a * lu);
+            dmv[q] = 0.5f * (lf - a * lu);
+        }
+        float phi;
+        if (ORDER == 5) {
+            float dP[4], dM[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) { dP[q] = dp[q]; dM[q] = dmv[2 * r - q]; }
+            phi = -phi_w5<float>(dP, eps) + phi_w5<float>(dM, eps);
+        } else {
+            float dP[8], dM[8], fp[9], fm[9];
+#pragma unroll
+            for (int q = 0; q < 8; q++) { dP[q] = dp[q]; dM[q] = dmv[2 * r - q]; }
+            fp[0] = 0.f;
+            fm[0] = 0.f;
+#pragma unroll
+            for (int q = 0; q < 8; q++) { fp[q + 1] = fp[q] + dP[q]; fm[q + 1] = fm[q] - dM[q]; }
+            phi = -phi_w9<float>(fp, dP, eps) + phi_w9<float>(fm, dM, eps);
+        }
+        add_right_col<float>(s, ch, phi, out);
+    }
+#pragma unroll
+    for (int q = 0; q < 5; q++) outd[q] = (double)out[q];
+#undef SH
+#undef DL
+}
+
+// Central part of the face flux (src/WENO.c:1754-1816), FP64.
+template <int ORDER>
+__device__ __forceinline__ double central(const double *sh, int NP, int q, int ta, int lane)
+{
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+    if (ORDER == 9)
+        return 1. / 840. * (533. * (SH(WF0 + q, ta + 1, lane) + SH(WF0 + q, ta, lane))
+                            - 139. * (SH(WF0 + q, ta + 2, lane) + SH(WF0 + q, ta - 1, lane))
+                            + 29. * (SH(WF0 + q, ta + 3, lane) + SH(WF0 + q, ta - 2, lane))
+                            - 3. * (SH(WF0 + q, ta + 4, lane) + SH(WF0 + q, ta - 3, lane)));
+    return 1. / 12. * (-1. * (SH(WF0 + q, ta - 1, lane) + SH(WF0 + q, ta + 2, lane))
+                       + 7. * (SH(WF0 + q, ta, lane) + SH(WF0 + q, ta + 1, lane)));
+#undef SH
+}
+
+// ---------------------------------------------------------------------------
+// weno_d: thread-per-face characteristic WENO, flux difference into Q
+// (src/WENO.c:206-494 and its eta/zeta twins).  256 threads, 2 faces each;
+// the face fluxes reuse the staging buffer so two tiles fit on an SM.
+// ---------------------------------------------------------------------------
+template <int DIM, int ORDER, int D, bool MIXED>
+__global__ void __launch_bounds__(NTHR, 2)
+    k_weno(Grid G, Phys P, bool first, const double *__restrict__ R, const double *__restrict__ Uu,
+           const double *__restrict__ Vv, const double *__restrict__ Ww, const double *__restrict__ Ee, Fields F)
+{
+    constexpr int r = (ORDER - 1) / 2;
+    constexpr int NP = TL + 2 * r + 2;
+    constexpr int NV = WenoNV<DIM>::NV;
+    extern __shared__ double smem[];
+    double *sh = smem;                                  // [NV][NP][NLANE]
+    float *dl = (float *)(smem + NV * NP * NLANE);      // mixed: [10][NP-1][NLANE]
+    double *fh = smem;                                  // [5][NFACE][NLANE], aliases sh after the faces
+    const int lane = threadIdx.x, row = threadIdx.y;
+    const Tile T = make_tile<DIM, D>(G, lane);
+
+    stage_weno<DIM, ORDER, D>(G, P, T, sh, R, Uu, Vv, Ww, Ee, F);
+    __syncthreads();
+    if (MIXED) {
+        const int tid = row * NLANE + lane;
+        for (int it = tid; it < (NP - 1) * NLANE; it += NTHR) {
+            int l = it % NLANE, t = it / NLANE;
+            if (T.l0 + l >= G.g + T.nL || T.c0 - r + t >= G.N[D]) continue;
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                dl[((q) * (NP - 1) + t) * NLANE + l] =
+                    (float)(sh[((WF0 + q) * NP + t + 1) * NLANE + l] - sh[((WF0 + q) * NP + t) * NLANE + l]);
+                dl[((5 + q) * (NP - 1) + t) * NLANE + l] =
+                    (float)(sh[((WU0 + q) * NP + t + 1) * NLANE + l] - sh[((WU0 + q) * NP + t) * NLANE + l]);
+            }
+        }
+        __syncthreads();
+    }
+    double res[2][5];
+    bool ok[2];
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const int f = row + k * NROWT;
+        ok[k] = T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1;
+        if (ok[k]) {
+            double w5[5];
+            if (MIXED) face_weno_mixed<DIM, ORDER, D>(P, sh, dl, f, lane, w5);
+            else face_weno_fp64<DIM, ORDER, D>(P, sh, f, lane, w5);
+#pragma unroll
+            for (int q = 0; q < 5; q++) res[k][q] = w5[q] + central<ORDER>(sh, NP, q, r + f, lane);
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const int f = row + k * NROWT;
+        if (ok[k])
+#pragma unroll
+            for (int q = 0; q < 5; q++) fh[(q * NFACE + f) * NLANE + lane] = res[k][q];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const int cr = row + k * NROWT;      // cell row in the tile
+        if (cr < TL && T.lane_ok && T.c0 + cr <= G.g + T.nD - 1) {
+            long long o = T.base + (long long)lane * T.sL + (long long)(T.c0 + cr) * T.sD;
+#pragma unroll
+            for (int q = 0; q < 5; q++) {
+                double prev = first ? 0.0 : F.Q[q][o];
+                F.Q[q][o] = prev - (fh[(q * NFACE + cr + 1) * NLANE + lane] - fh[(q * NFACE + cr) * NLANE + lane]);
+            }
+        }
+    }
 }
 
 // ---------------------------------------------------------------------------
@@ -502,44 +671,40 @@ __global__ void __launch_bounds__(NLANE *NROW, 1)
 enum { V3U = 0, V3V, V3W, V3T, V3X0, V3X1, V3X2, V3X3, V3F1, V3FA, V3FB, V3NV };
 enum { V2U = 0, V2V, V2T, V2XU, V2XV, V2XT, V2MJ, V2AX, V2AY, V2BX, V2BY, V2NV };
 
-template <int DIM, int ORDER, int D>
-__global__ void __launch_bounds__(NLANE *NROW, 1)
+template <int DIM, int ORDER, int D, bool MIXED>
+__global__ void __launch_bounds__(NTHR, 2)
     k_visc(Grid G, Phys P, const double *__restrict__ Uu, const double *__restrict__ Vv,
            const double *__restrict__ Ww, Fields F)
 {
     using A = Axes<DIM, D>;
+    using TS = typename std::conditional<MIXED, float, double>::type;   // stencil arithmetic
     constexpr int H = ZD<ORDER>::H;          // half stencil: l = 0..2H-1 around the face
     constexpr int NP = TL + 2 * H;
     constexpr int NV = DIM == 3 ? V3NV : V2NV;
-    constexpr int NG_OUT = DIM == 3 ? 4 : 3; // face outputs: momentum (DIM) + heat
-    // 3D: the two non-sweep axes
-    constexpr int MA = (D == 0) ? 1 : 0;
+    constexpr int MA = (D == 0) ? 1 : 0;     // 3D: the two non-sweep axes
     constexpr int MB = (D == 2) ? 1 : 2;
     const bool quirk = (DIM == 3 && D == 2 && !P.zeta_fix);
 
     extern __shared__ double smem[];
     double *sh = smem;                       // [NV][NP][NLANE]
-    double *fo = smem + NV * NP * NLANE;     // [NG_OUT or 3 K][NROW][NLANE]
+    double *fo = smem + NV * NP * NLANE;     // [4][NFACE][NLANE]
+    double *qd = fo + 4 * NFACE * NLANE;     // quirk: [16][NLANE] per-line half-point values
 #define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
-#define FO(c, f, l) fo[((c) * NROW + (f)) * NLANE + (l)]
+#define FO(c, f, l) fo[((c) * NFACE + (f)) * NLANE + (l)]
+#define QD(c, l) qd[(c) * NLANE + (l)]
 
     const int lane = threadIdx.x, row = threadIdx.y;
-    const int c0 = G.g + blockIdx.x * TL;
-    const int l0 = G.g + blockIdx.y * NLANE;
-    const int oth = (DIM == 3) ? G.g + blockIdx.z : 0;
-    const int nD = G.n[D], nL = G.n[A::LAT];
-    const long long sD = G.st[D], sL = G.st[A::LAT], sO = (DIM == 3) ? G.st[A::OTH] : 0;
-    const long long base = (long long)l0 * sL + (long long)oth * sO;
+    const Tile T = make_tile<DIM, D>(G, lane);
 
     // ---- stage: points c0-H .. c0+TL+H-1 along the sweep ----------------------
     const int tid = row * NLANE + lane;
-    for (int it = tid; it < NP * NLANE; it += NLANE * NROW) {
+    for (int it = tid; it < NP * NLANE; it += NTHR) {
         int t, l;
         if (A::CONTIG) { t = it % NP; l = it / NP; }
         else { l = it % NLANE; t = it / NLANE; }
-        int pd = c0 - H + t;
-        if (l0 + l >= G.g + nL || pd >= G.N[D]) continue;
-        long long o = base + (long long)l * sL + (long long)pd * sD;
+        int pd = T.c0 - H + t;
+        if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
+        long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
         double mu = F.mu[o], J = F.J[o];
         if (DIM == 3) {
             double cd = F.m[4 * D][o], ca = F.m[4 * MA][o], cb = F.m[4 * MB][o];
@@ -570,13 +735,41 @@ __global__ void __launch_bounds__(NLANE *NROW, 1)
             SH(V2BY, t, l) = F.m[3 * E + 1][o];
         }
     }
+    if (DIM == 3 && D == 2) {
+        if (quirk && T.lane_ok) {
+            // half-point stencils along k centred on the j index (src/ZD.c:547-548),
+            // the same for every cell of the line: 16 values per lane, 2 per row
+            const int jj = T.l0 + lane;                     // lateral axis of the zeta sweep is j
+            const long long lb = T.base + (long long)lane * T.sL;   // (i, j, 0)
+            const double *vs[4] = {Uu, Vv, Ww, F.T};
+            const double *xs[4] = {F.Nd[3 * MA + MA], F.Nd[3 * MB + MB], F.Nd[3 * D + MA], F.Nd[3 * D + MB]};
+#pragma unroll
+            for (int k2 = 0; k2 < 2; k2++) {
+                int idx = row * 2 + k2;                     // 0..15: side*8 + quantity
+                int side = idx >> 3, qn = idx & 7;
+                const double *src = qn < 4 ? vs[qn] : xs[qn - 4];
+                TS acc = 0;
+                if (qn < 4) {
+                    double ref = src[lb + jj];              // value near the stencil centre
+#pragma unroll
+                    for (int l = 0; l < 2 * H; l++)
+                        acc += (TS)ZD<ORDER>::half(l) * (TS)(src[lb + (jj + l - H + side)] - (MIXED ? ref : 0.0));
+                } else {
+#pragma unroll
+                    for (int l = 0; l < 2 * H; l++) acc += (TS)ZD<ORDER>::interp(l) * (TS)src[lb + (jj + l - H + side)];
+                }
+                QD(idx, lane) = (double)acc;
+            }
+        }
+    }
     __syncthreads();
 
-    const bool lane_ok = (l0 + lane) < G.g + nL;
-    const int f = row;                       // face (c0-1+f)+1/2: points c0-1+f-H+1 .. c0-1+f+H
     const double t23 = 2.0 / 3.0, t43 = 4.0 / 3.0;
-    if (lane_ok && (c0 - 1 + f) <= G.g + nD - 1) {
-        const int ta = f + H - 1;            // staged index of the left point
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const int f = row + k * NROWT;   // face (c0-1+f)+1/2: staged points f .. f+2H-1
+        if (!(T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1)) continue;
+        const int ta = f + H - 1;        // staged index of the left point
         if (DIM == 3) {
             double K1 = 0.5 * (SH(V3F1, ta, lane) + SH(V3F1, ta + 1, lane));
             double KA = 0.5 * (SH(V3FA, ta, lane) + SH(V3FA, ta + 1, lane));
@@ -584,37 +777,40 @@ __global__ void __launch_bounds__(NLANE *NROW, 1)
             if (quirk) {
                 FO(0, f, lane) = K1; FO(1, f, lane) = KA; FO(2, f, lane) = KB;
             } else {
-                double dU = 0, dV = 0, dW = 0, dT = 0, x0 = 0, x1 = 0, x2 = 0, x3 = 0;
+                TS dU = 0, dV = 0, dW = 0, dT = 0, x0 = 0, x1 = 0, x2 = 0, x3 = 0;
+                const double ru = MIXED ? SH(V3U, ta, lane) : 0.0, rv = MIXED ? SH(V3V, ta, lane) : 0.0;
+                const double rw = MIXED ? SH(V3W, ta, lane) : 0.0, rT = MIXED ? SH(V3T, ta, lane) : 0.0;
 #pragma unroll
                 for (int l = 0; l < 2 * H; l++) {
                     int t = f + l;
-                    double ch = ZD<ORDER>::half(l), ci = ZD<ORDER>::interp(l);
-                    dU += ch * SH(V3U, t, lane); dV += ch * SH(V3V, t, lane);
-                    dW += ch * SH(V3W, t, lane); dT += ch * SH(V3T, t, lane);
-                    x0 += ci * SH(V3X0, t, lane); x1 += ci * SH(V3X1, t, lane);
-                    x2 += ci * SH(V3X2, t, lane); x3 += ci * SH(V3X3, t, lane);
+                    TS ch = (TS)ZD<ORDER>::half(l), ci = (TS)ZD<ORDER>::interp(l);
+                    dU += ch * (TS)(SH(V3U, t, lane) - ru); dV += ch * (TS)(SH(V3V, t, lane) - rv);
+                    dW += ch * (TS)(SH(V3W, t, lane) - rw); dT += ch * (TS)(SH(V3T, t, lane) - rT);
+                    x0 += ci * (TS)SH(V3X0, t, lane); x1 += ci * (TS)SH(V3X1, t, lane);
+                    x2 += ci * (TS)SH(V3X2, t, lane); x3 += ci * (TS)SH(V3X3, t, lane);
                 }
-                double dvel[3] = {dU, dV, dW};
-                // momentum along D: d vel_D/d xi_D * 4/3 K1 - 2/3 (d vel_MA/d xi_MA KA + d vel_MB/d xi_MB KB)
-                double gD = dvel[D] * (t43 * K1) + x0 * (-t23 * KA) + x1 * (-t23 * KB);
-                double gA = dvel[MA] * K1 + x2 * KA;    // momentum MA: d vel_MA/d xi_D K1 + d vel_D/d xi_MA KA
-                double gB = dvel[MB] * K1 + x3 * KB;
+                double dvel[3] = {(double)dU, (double)dV, (double)dW};
+                double gD = dvel[D] * (t43 * K1) + (double)x0 * (-t23 * KA) + (double)x1 * (-t23 * KB);
+                double gA = dvel[MA] * K1 + (double)x2 * KA;
+                double gB = dvel[MB] * K1 + (double)x3 * KB;
                 double g3[3];
                 g3[D] = gD; g3[MA] = gA; g3[MB] = gB;
                 FO(0, f, lane) = g3[0]; FO(1, f, lane) = g3[1]; FO(2, f, lane) = g3[2];
-                FO(3, f, lane) = dT * K1;
+                FO(3, f, lane) = (double)dT * K1;
             }
         } else {
             constexpr int E = 1 - D;
-            double dU = 0, dV = 0, dT = 0, xU = 0, xV = 0, xT = 0;
+            TS dU = 0, dV = 0, dT = 0, xU = 0, xV = 0, xT = 0;
+            const double ru = MIXED ? SH(V2U, ta, lane) : 0.0, rv = MIXED ? SH(V2V, ta, lane) : 0.0;
+            const double rT = MIXED ? SH(V2T, ta, lane) : 0.0;
 #pragma unroll
             for (int l = 0; l < 2 * H; l++) {
                 int t = f + l;
-                double ch = ZD<ORDER>::half(l), ci = ZD<ORDER>::interp(l);
-                dU += ch * SH(V2U, t, lane); dV += ch * SH(V2V, t, lane); dT += ch * SH(V2T, t, lane);
-                xU += ci * SH(V2XU, t, lane); xV += ci * SH(V2XV, t, lane); xT += ci * SH(V2XT, t, lane);
+                TS ch = (TS)ZD<ORDER>::half(l), ci = (TS)ZD<ORDER>::interp(l);
+                dU += ch * (TS)(SH(V2U, t, lane) - ru); dV += ch * (TS)(SH(V2V, t, lane) - rv);
+                dT += ch * (TS)(SH(V2T, t, lane) - rT);
+                xU += ci * (TS)SH(V2XU, t, lane); xV += ci * (TS)SH(V2XV, t, lane); xT += ci * (TS)SH(V2XT, t, lane);
             }
-            // derivatives at the face indexed [var][dir]
             double Dk[2][2], DT[2];
             Dk[0][D] = dU; Dk[1][D] = dV; DT[D] = dT;
             Dk[0][E] = xU; Dk[1][E] = xV; DT[E] = xT;
@@ -625,7 +821,7 @@ __global__ void __launch_bounds__(NLANE *NROW, 1)
                 double mj = SH(V2MJ, t, lane);
                 double ax = SH(V2AX, t, lane), ay = SH(V2AY, t, lane);
                 double bx = SH(V2BX, t, lane), by = SH(V2BY, t, lane);
-                double gm[2][2];   // grad xi_m, m = xi, eta
+                double gm[2][2];
                 gm[D][0] = ax; gm[D][1] = ay; gm[E][0] = bx; gm[E][1] = by;
                 double av[2] = {ax, ay};
                 double s0 = 0, s1 = 0, sh0 = 0;
@@ -633,11 +829,11 @@ __global__ void __launch_bounds__(NLANE *NROW, 1)
                 for (int m = 0; m < 2; m++) {
                     double adot = ax * gm[m][0] + ay * gm[m][1];
 #pragma unroll
-                    for (int k = 0; k < 2; k++) {
-                        double K0 = (k == 0 ? adot : 0.0) + av[k] * gm[m][0] - t23 * av[0] * gm[m][k];
-                        double Kk1 = (k == 1 ? adot : 0.0) + av[k] * gm[m][1] - t23 * av[1] * gm[m][k];
-                        s0 += Dk[k][m] * K0;
-                        s1 += Dk[k][m] * Kk1;
+                    for (int kk = 0; kk < 2; kk++) {
+                        double K0 = (kk == 0 ? adot : 0.0) + av[kk] * gm[m][0] - t23 * av[0] * gm[m][kk];
+                        double Kk1 = (kk == 1 ? adot : 0.0) + av[kk] * gm[m][1] - t23 * av[1] * gm[m][kk];
+                        s0 += Dk[kk][m] * K0;
+                        s1 += Dk[kk][m] * Kk1;
                     }
                     sh0 += DT[m] * adot;
                 }
@@ -651,9 +847,11 @@ __global__ void __launch_bounds__(NLANE *NROW, 1)
     __syncthreads();
 
     // ---- cell update ----------------------------------------------------------
-    if (lane_ok && row < TL && c0 + row <= G.g + nD - 1) {
-        const int cell = c0 + row;
-        long long o = base + (long long)lane * sL + (long long)cell * sD;
+#pragma unroll
+    for (int k = 0; k < 2; k++) {
+        const int cr = row + k * NROWT;
+        if (!(cr < TL && T.lane_ok && T.c0 + cr <= G.g + T.nD - 1)) continue;
+        long long o = T.base + (long long)lane * T.sL + (long long)(T.c0 + cr) * T.sD;
         double mu = F.mu[o], J = F.J[o];
         double vel[3] = {Uu[o], Vv[o], DIM == 3 ? Ww[o] : 0.0};
         double gp[3] = {0, 0, 0}, gmn[3] = {0, 0, 0}, hp = 0, hm = 0;
@@ -661,24 +859,12 @@ __global__ void __launch_bounds__(NLANE *NROW, 1)
         if (DIM == 3) {
             double cd = F.m[4 * D][o], ca = F.m[4 * MA][o], cb = F.m[4 * MB][o];
             if (quirk) {
-                // half-point stencils along k centred on the j index (src/ZD.c:547-548)
-                const int jj = (int)((o / G.st[1]) % G.N[1]);
-                long long lb = o - (o % G.st[1]);            // (i, j, 0)
-                double Dm[8] = {0, 0, 0, 0, 0, 0, 0, 0}, Dp[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-                const double *vs[4] = {Uu, Vv, Ww, F.T};
-                const double *xs[4] = {F.Nd[3 * MA + MA], F.Nd[3 * MB + MB], F.Nd[3 * D + MA], F.Nd[3 * D + MB]};
+                double K1p = FO(0, cr + 1, lane), KAp = FO(1, cr + 1, lane), KBp = FO(2, cr + 1, lane);
+                double K1m = FO(0, cr, lane), KAm = FO(1, cr, lane), KBm = FO(2, cr, lane);
+                // QD: side 0 = minus (j-1/2), side 1 = plus; quantities u,v,w,T along, then x0..x3
+                double Dm[8], Dp[8];
 #pragma unroll
-                for (int l = 0; l < 2 * H; l++) {
-                    long long im = lb + (jj + l - H), ip = im + 1;
-                    double ch = ZD<ORDER>::half(l), ci = ZD<ORDER>::interp(l);
-#pragma unroll
-                    for (int q = 0; q < 4; q++) {
-                        Dm[q] += ch * vs[q][im]; Dp[q] += ch * vs[q][ip];
-                        Dm[4 + q] += ci * xs[q][im]; Dp[4 + q] += ci * xs[q][ip];
-                    }
-                }
-                double K1p = FO(0, row + 1, lane), KAp = FO(1, row + 1, lane), KBp = FO(2, row + 1, lane);
-                double K1m = FO(0, row, lane), KAm = FO(1, row, lane), KBm = FO(2, row, lane);
+                for (int q = 0; q < 8; q++) { Dm[q] = QD(q, lane); Dp[q] = QD(8 + q, lane); }
                 gp[D] = Dp[D] * (t43 * K1p) + Dp[4] * (-t23 * KAp) + Dp[5] * (-t23 * KBp);
                 gp[MA] = Dp[MA] * K1p + Dp[6] * KAp;
                 gp[MB] = Dp[MB] * K1p + Dp[7] * KBp;
@@ -689,9 +875,9 @@ __global__ void __launch_bounds__(NLANE *NROW, 1)
                 hm = Dm[3] * K1m;
             } else {
 #pragma unroll
-                for (int q = 0; q < 3; q++) { gp[q] = FO(q, row + 1, lane); gmn[q] = FO(q, row, lane); }
-                hp = FO(3, row + 1, lane);
-                hm = FO(3, row, lane);
+                for (int q = 0; q < 3; q++) { gp[q] = FO(q, cr + 1, lane); gmn[q] = FO(q, cr, lane); }
+                hp = FO(3, cr + 1, lane);
+                hm = FO(3, cr, lane);
             }
             // node term: mu * sum_i N[i][D] * sum_{k,m} N[k][m] Fac[i][k][m] at the cell
             double F1 = J * (cd * cd), FA = J * (cd * ca), FB = J * (cd * cb);
@@ -705,25 +891,25 @@ __global__ void __launch_bounds__(NLANE *NROW, 1)
         } else {
             constexpr int E = 1 - D;
 #pragma unroll
-            for (int q = 0; q < 2; q++) { gp[q] = FO(q, row + 1, lane); gmn[q] = FO(q, row, lane); }
-            hp = FO(2, row + 1, lane);
-            hm = FO(2, row, lane);
+            for (int q = 0; q < 2; q++) { gp[q] = FO(q, cr + 1, lane); gmn[q] = FO(q, cr, lane); }
+            hp = FO(2, cr + 1, lane);
+            hm = FO(2, cr, lane);
             double ax = F.m[3 * D + 0][o], ay = F.m[3 * D + 1][o];
             double gmv[2][2];
             gmv[D][0] = ax; gmv[D][1] = ay; gmv[E][0] = F.m[3 * E + 0][o]; gmv[E][1] = F.m[3 * E + 1][o];
             double av[2] = {ax, ay};
-            double N[2][2];   // N[var][dir]
+            double N[2][2];
             N[0][0] = F.Nd[0][o]; N[0][1] = F.Nd[1][o]; N[1][0] = F.Nd[3][o]; N[1][1] = F.Nd[4][o];
             double hsum[2] = {0, 0};
 #pragma unroll
             for (int m = 0; m < 2; m++) {
                 double adot = ax * gmv[m][0] + ay * gmv[m][1];
 #pragma unroll
-                for (int k = 0; k < 2; k++) {
+                for (int kk = 0; kk < 2; kk++) {
 #pragma unroll
                     for (int i = 0; i < 2; i++) {
-                        double K = (i == k ? adot : 0.0) + av[k] * gmv[m][i] - t23 * av[i] * gmv[m][k];
-                        hsum[i] += N[k][m] * K;
+                        double K = (i == kk ? adot : 0.0) + av[kk] * gmv[m][i] - t23 * av[i] * gmv[m][kk];
+                        hsum[i] += N[kk][m] * K;
                     }
                 }
             }
@@ -739,6 +925,7 @@ __global__ void __launch_bounds__(NLANE *NROW, 1)
     }
 #undef SH
 #undef FO
+#undef QD
 }
 
 // ---------------------------------------------------------------------------
@@ -839,54 +1026,65 @@ static dim3 sweep_grid(const Grid &G)
     return dim3((G.n[D] + TL - 1) / TL, (G.n[A::LAT] + NLANE - 1) / NLANE, DIM == 3 ? G.n[A::OTH] : 1);
 }
 
-template <int DIM, int ORDER, int D>
+// G.order == 0 is the attribute pass: raise the dynamic shared-memory limit
+// of the instantiation (done once per device, before any graph capture).
+template <int DIM, int ORDER, int D, bool MIXED>
 static void weno_one(const Grid &G, const Phys &P, bool first, const double *const U[5], const Fields &F,
                      cudaStream_t s)
 {
     constexpr int r = (ORDER - 1) / 2;
     constexpr int NP = TL + 2 * r + 2;
-    size_t smem = sizeof(double) * ((size_t)WenoNV<DIM>::NV * NP * NLANE + 5 * NROW * NLANE);
-    if (!G.order) {   // attribute pass (called once per device before any capture)
-        cudaFuncSetAttribute(k_weno<DIM, ORDER, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    size_t smem = sizeof(double) * (size_t)WenoNV<DIM>::NV * NP * NLANE
+                  + (MIXED ? sizeof(float) * (size_t)10 * (NP - 1) * NLANE : 0);
+    if (!G.order) {
+        cudaFuncSetAttribute(k_weno<DIM, ORDER, D, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         return;
     }
-    k_weno<DIM, ORDER, D><<<sweep_grid<DIM, D>(G), dim3(NLANE, NROW), smem, s>>>(G, P, first, U[0], U[1], U[2],
-                                                                                U[3], U[4], F);
+    k_weno<DIM, ORDER, D, MIXED><<<sweep_grid<DIM, D>(G), dim3(NLANE, NROWT), smem, s>>>(G, P, first, U[0], U[1],
+                                                                                        U[2], U[3], U[4], F);
 }
 
-template <int DIM, int ORDER, int D>
+template <int DIM, int ORDER, int D, bool MIXED>
 static void visc_one(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s)
 {
     constexpr int H = ZD<ORDER>::H;
     constexpr int NP = TL + 2 * H;
     constexpr int NV = DIM == 3 ? V3NV : V2NV;
-    size_t smem = sizeof(double) * ((size_t)NV * NP * NLANE + 4 * NROW * NLANE);
+    size_t smem = sizeof(double) * ((size_t)NV * NP * NLANE + 4 * NFACE * NLANE + 16 * NLANE);
     if (!G.order) {
-        cudaFuncSetAttribute(k_visc<DIM, ORDER, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_visc<DIM, ORDER, D, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         return;
     }
-    k_visc<DIM, ORDER, D><<<sweep_grid<DIM, D>(G), dim3(NLANE, NROW), smem, s>>>(G, P, U[1], U[2], U[3], F);
+    k_visc<DIM, ORDER, D, MIXED><<<sweep_grid<DIM, D>(G), dim3(NLANE, NROWT), smem, s>>>(G, P, U[1], U[2], U[3], F);
 }
+
+#define SHOCK_SWEEP_CASES(X)                                                           \
+    X(3, 5, 0) X(3, 5, 1) X(3, 5, 2) X(3, 9, 0) X(3, 9, 1) X(3, 9, 2) X(2, 5, 0) X(2, 5, 1) \
+    X(2, 9, 0) X(2, 9, 1)
 
 void launch_weno(const Grid &G, const Phys &P, int precision, int d, bool first, const double *const U[5],
                  const Fields &F, cudaStream_t s)
 {
-    (void)precision;
-#define W(DIM, ORD, D) \
-    if (G.dim == DIM && G.order == ORD && d == D) { weno_one<DIM, ORD, D>(G, P, first, U, F, s); return; }
-    W(3, 5, 0) W(3, 5, 1) W(3, 5, 2) W(3, 9, 0) W(3, 9, 1) W(3, 9, 2)
-    W(2, 5, 0) W(2, 5, 1) W(2, 9, 0) W(2, 9, 1)
+#define W(DIM, ORD, D)                                                                  \
+    if (G.dim == DIM && G.order == ORD && d == D) {                                      \
+        if (precision == SHOCK_MIXED) weno_one<DIM, ORD, D, true>(G, P, first, U, F, s); \
+        else weno_one<DIM, ORD, D, false>(G, P, first, U, F, s);                         \
+        return;                                                                          \
+    }
+    SHOCK_SWEEP_CASES(W)
 #undef W
 }
 
 void launch_viscous(const Grid &G, const Phys &P, int precision, int d, const double *const U[5],
                     const Fields &F, cudaStream_t s)
 {
-    (void)precision;
-#define V(DIM, ORD, D) \
-    if (G.dim == DIM && G.order == ORD && d == D) { visc_one<DIM, ORD, D>(G, P, U, F, s); return; }
-    V(3, 5, 0) V(3, 5, 1) V(3, 5, 2) V(3, 9, 0) V(3, 9, 1) V(3, 9, 2)
-    V(2, 5, 0) V(2, 5, 1) V(2, 9, 0) V(2, 9, 1)
+#define V(DIM, ORD, D)                                                               \
+    if (G.dim == DIM && G.order == ORD && d == D) {                                   \
+        if (precision == SHOCK_MIXED) visc_one<DIM, ORD, D, true>(G, P, U, F, s);     \
+        else visc_one<DIM, ORD, D, false>(G, P, U, F, s);                             \
+        return;                                                                       \
+    }
+    SHOCK_SWEEP_CASES(V)
 #undef V
 }
 
@@ -923,14 +1121,11 @@ void prepare_kernels()
     Fields F{};
     const double *U[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     G.order = 0;
-    weno_one<3, 5, 0>(G, P, true, U, F, 0); weno_one<3, 5, 1>(G, P, true, U, F, 0); weno_one<3, 5, 2>(G, P, true, U, F, 0);
-    weno_one<3, 9, 0>(G, P, true, U, F, 0); weno_one<3, 9, 1>(G, P, true, U, F, 0); weno_one<3, 9, 2>(G, P, true, U, F, 0);
-    weno_one<2, 5, 0>(G, P, true, U, F, 0); weno_one<2, 5, 1>(G, P, true, U, F, 0);
-    weno_one<2, 9, 0>(G, P, true, U, F, 0); weno_one<2, 9, 1>(G, P, true, U, F, 0);
-    visc_one<3, 5, 0>(G, P, U, F, 0); visc_one<3, 5, 1>(G, P, U, F, 0); visc_one<3, 5, 2>(G, P, U, F, 0);
-    visc_one<3, 9, 0>(G, P, U, F, 0); visc_one<3, 9, 1>(G, P, U, F, 0); visc_one<3, 9, 2>(G, P, U, F, 0);
-    visc_one<2, 5, 0>(G, P, U, F, 0); visc_one<2, 5, 1>(G, P, U, F, 0);
-    visc_one<2, 9, 0>(G, P, U, F, 0); visc_one<2, 9, 1>(G, P, U, F, 0);
+#define A(DIM, ORD, D)                                                                         \
+    weno_one<DIM, ORD, D, false>(G, P, true, U, F, 0); weno_one<DIM, ORD, D, true>(G, P, true, U, F, 0); \
+    visc_one<DIM, ORD, D, false>(G, P, U, F, 0); visc_one<DIM, ORD, D, true>(G, P, U, F, 0);
+    SHOCK_SWEEP_CASES(A)
+#undef A
 }
 
 void launch_copy_state(const Grid &G, const double *const src[5], double *const dst[5], cudaStream_t s)
