@@ -91,6 +91,24 @@ int shock_set_dirichlet(shock_ctx *ctx, const double *exact9);
  * (src/ManufacturedSolution.c:25-175); the caller evaluates S once. */
 int shock_set_source(shock_ctx *ctx, const double *js5);
 
+/* Exact solution (9*NG: rho,u,v,w,e,p,T,c,mue on every ghosted point) and
+ * source J*S (5*NG, real points) of the built-in 2D product-form
+ * manufactured solution rho = 1+0.1 sin(2 pi x)sin(2 pi y),
+ * u = 0.3 cos(2 pi x)sin(2 pi y), v = 0.3 sin(2 pi x)cos(2 pi y),
+ * p = 1/gamma + 0.05 cos(2 pi x)cos(2 pi y) (rho_0 = c_0 = 1, Ma = 1),
+ * evaluated in long double on this block's coordinates, the way
+ * src/ManufacturedSolution.c evaluates SHOCK's own family.  Feed the
+ * results to shock_set_dirichlet / shock_set_source. */
+int shock_mms_baseline(const shock_ctx *ctx, double *exact9, double *js5);
+
+/* Host-only set-up without a device: the block geometry (13*NG, as
+ * shock_geometry) and the built-in manufactured solution (as
+ * shock_mms_baseline) for the grid x,y,z (real points, Fortran order). */
+int shock_host_geometry(const shock_params *p, const double *x, const double *y, const double *z,
+                        double *out13);
+int shock_host_mms_baseline(const shock_params *p, const double *x, const double *y, const double *z,
+                            double *exact9, double *js5);
+
 /* Host <-> device state (rho,u,v,w,e; 5*NG doubles, ghosted).
  * which = 0: U_RK (the running state), 1: U_lastStep. */
 int shock_upload_state(shock_ctx *ctx, const double *prim5);

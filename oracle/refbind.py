@@ -50,10 +50,12 @@ class RefSolver:
 
     _libs: dict = {}
 
-    def __init__(self, case, extended=False):
-        """extended=True loads the PRECISION=3 (80-bit long double) build."""
+    def __init__(self, case, extended=False, external=None):
+        """extended=True loads the PRECISION=3 (80-bit long double) build.
+        external=(exact9, js5): manufactured solution given as arrays on the
+        ghosted block (the build with ref_harness/mms_external.c)."""
         self.case = case
-        tag = "80" if extended else ""
+        tag = "80" if extended else ("x" if external is not None else "")
         key = (case.order, case.dim, tag)
         if key not in RefSolver._libs:
             path = os.path.join(HERE, "_ref", f"libshockref{tag}_w{case.order}_{case.dim}d.so")
@@ -70,7 +72,7 @@ class RefSolver:
         p.tau, p.mach, p.reynolds = case.tau, case.mach, case.reynolds
         p.prandtl, p.gamma, p.gas_r, p.t0, p.l0 = case.prandtl, case.gamma, case.gas_r, case.t0, case.l0
         p.inviscid = int(case.inviscid)
-        p.mms = 1 if case.mms == "reference" else 0
+        p.mms = 1 if (case.mms == "reference" or external is not None) else 0
         p.mms_case = case.mms_case
         for a in range(3):
             p.periodic[a] = int(case.periodic[a])
@@ -79,6 +81,10 @@ class RefSolver:
         f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
         x, y, z, u, v, w, pr, rho = (f(a) for a in case.real_fields())
         self._keep = (x, y, z, u, v, w, pr, rho)
+        if external is not None:
+            ex = np.ascontiguousarray(external[0], np.float64).ravel()
+            js = np.ascontiguousarray(external[1], np.float64).ravel()
+            self.lib.ref_set_external(_ptr(ex), _ptr(js), C.c_size_t(ex.size // 9))
         rc = self.lib.ref_init(C.byref(p), _ptr(x), _ptr(y), _ptr(z), _ptr(u), _ptr(v),
                                _ptr(w), _ptr(pr), _ptr(rho))
         assert rc == 0

@@ -24,7 +24,7 @@ import numpy as np
 from . import cases  # noqa: F401
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libshock_b200.so")
+LIB_PATH = os.environ.get("SHOCK_B200_LIB", os.path.join(HERE, "libshock_b200.so"))
 
 SHOCK_FP64 = 0
 SHOCK_MIXED = 1
@@ -76,7 +76,9 @@ def lib():
             for name in ("shock_destroy", "shock_dims", "shock_set_dirichlet", "shock_set_source",
                          "shock_upload_state", "shock_download_state", "shock_rhs", "shock_step",
                          "shock_step_async", "shock_sync", "shock_check_nan", "shock_geometry",
-                         "shock_device_bytes", "shock_last_step_ms", "shock_kernels_per_step"):
+                         "shock_device_bytes", "shock_last_step_ms", "shock_kernels_per_step",
+                         "shock_mms_baseline", "shock_profile_stage", "shock_measure_fma_peak",
+                         "shock_host_geometry", "shock_host_mms_baseline"):
                 getattr(L, name).restype = C.c_int
             _lib = L
         return _lib
@@ -109,6 +111,37 @@ def params_from_case(case, precision=SHOCK_FP64, zeta_fix=False) -> Params:
     return p
 
 
+def _ghosted_shape(case):
+    g = case.order + 1
+    return (case.ni + g, case.nj + g, (case.nk + g) if case.dim == 3 else 1)
+
+
+def _fortran_coords(case):
+    f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
+    return f(case.x), f(case.y), f(case.z)
+
+
+def host_geometry(case) -> np.ndarray:
+    """Block geometry (x,y,z,J, 9 metrics; ghosted) built on the host, no device."""
+    shp = _ghosted_shape(case)
+    out = np.zeros((13,) + shp)
+    x, y, z = _fortran_coords(case)
+    p = params_from_case(case)
+    _check(lib().shock_host_geometry(C.byref(p), _ptr(x), _ptr(y), _ptr(z), _ptr(out)))
+    return out
+
+
+def host_mms_baseline(case):
+    """(exact9, js5) of the built-in 2D manufactured solution, computed on the host."""
+    shp = _ghosted_shape(case)
+    ex = np.zeros((9,) + shp)
+    js = np.zeros((5,) + shp)
+    x, y, z = _fortran_coords(case)
+    p = params_from_case(case)
+    _check(lib().shock_host_mms_baseline(C.byref(p), _ptr(x), _ptr(y), _ptr(z), _ptr(ex), _ptr(js)))
+    return ex, js
+
+
 class Solver:
     """One block of SHOCK's stage right-hand side on a CUDA device."""
 
@@ -127,6 +160,8 @@ class Solver:
         self.shape = (d[0], d[1], d[2])
         self.start = (d[3], d[4], d[5])
         self.n = d[0] * d[1] * d[2]
+        if case.mms == "baseline" and dirichlet9 is None and source5 is None:
+            dirichlet9, source5 = self.mms_baseline()
         if dirichlet9 is not None:
             a = np.ascontiguousarray(dirichlet9, np.float64).ravel()
             assert a.size == 9 * self.n
@@ -135,6 +170,13 @@ class Solver:
             a = np.ascontiguousarray(source5, np.float64).ravel()
             assert a.size == 5 * self.n
             _check(self.lib.shock_set_source(self.h, _ptr(a)))
+
+    def mms_baseline(self):
+        """(exact9, js5) of the built-in 2D manufactured solution on this block."""
+        ex = np.zeros(9 * self.n)
+        js = np.zeros(5 * self.n)
+        _check(self.lib.shock_mms_baseline(self.h, _ptr(ex), _ptr(js)))
+        return ex.reshape((9,) + self.shape), js.reshape((5,) + self.shape)
 
     def close(self):
         if getattr(self, "h", None):

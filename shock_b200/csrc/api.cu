@@ -171,6 +171,7 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
     G.NG = c->L.NG;
     Phys &P = c->P;
     P.gamma = p->gamma;
+    P.igm1 = 1.0 / (p->gamma - 1.0);
     P.ups = 1.0 / (p->gamma * (p->mach * p->mach));
     P.psi = 1.0 / p->reynolds;
     P.suth = 100.4 / p->t0;
@@ -262,6 +263,47 @@ int shock_set_dirichlet(shock_ctx *c, const double *exact9)
         for (int f = 0; f < 5; f++)
             CK(cudaMemcpy(c->buf[b][f], exact9 + (size_t)f * c->G.NG, nb, cudaMemcpyHostToDevice));
     c->un = 0;
+    return SHOCK_OK;
+}
+
+int shock_mms_baseline(const shock_ctx *c, double *exact9, double *js5)
+{
+    if (!c || !exact9 || !js5) return fail(SHOCK_EINVAL, "null argument");
+    if (c->p.dim != 2) return fail(SHOCK_EINVAL, "the built-in manufactured solution is 2D");
+    mms_baseline_fields(c->L, c->p, c->geo_host, exact9, js5);
+    return SHOCK_OK;
+}
+
+static int host_block(const shock_params *p, const double *x, const double *y, const double *z, HostBlock &hb)
+{
+    if (!p || !x || !y || (p->dim == 3 && !z)) return fail(SHOCK_EINVAL, "null argument");
+    if (p->dim != 2 && p->dim != 3) return fail(SHOCK_EINVAL, "dim must be 2 or 3");
+    if (p->order != 5 && p->order != 9) return fail(SHOCK_EINVAL, "order must be 5 or 9");
+    size_t nr = (size_t)p->ni * p->nj * (p->dim == 3 ? p->nk : 1);
+    std::vector<double> zero(nr, 0.0), one(nr, 1.0);
+    build_block(*p, x, y, z ? z : zero.data(), zero.data(), zero.data(), zero.data(), one.data(), one.data(), hb);
+    return SHOCK_OK;
+}
+
+int shock_host_geometry(const shock_params *p, const double *x, const double *y, const double *z, double *out13)
+{
+    HostBlock hb;
+    int rc = host_block(p, x, y, z, hb);
+    if (rc) return rc;
+    if (!out13) return fail(SHOCK_EINVAL, "null argument");
+    for (int f = 0; f < 13; f++) memcpy(out13 + (size_t)f * hb.L.NG, hb.geo[f].data(), sizeof(double) * hb.L.NG);
+    return SHOCK_OK;
+}
+
+int shock_host_mms_baseline(const shock_params *p, const double *x, const double *y, const double *z,
+                            double *exact9, double *js5)
+{
+    HostBlock hb;
+    int rc = host_block(p, x, y, z, hb);
+    if (rc) return rc;
+    if (!exact9 || !js5) return fail(SHOCK_EINVAL, "null argument");
+    if (p->dim != 2) return fail(SHOCK_EINVAL, "the built-in manufactured solution is 2D");
+    mms_baseline_fields(hb.L, *p, hb.geo, exact9, js5);
     return SHOCK_OK;
 }
 

@@ -33,6 +33,8 @@ int build_block(const shock_params &p, const double *x, const double *y, const d
                 const double *u, const double *v, const double *w, const double *pr,
                 const double *rho, HostBlock &hb);
 void periodic_images(const Layout &L, const shock_params &p, double **f, int nf, int ncoord);
+void mms_baseline_fields(const Layout &L, const shock_params &p, const std::vector<std::vector<double>> &geo,
+                         double *exact9, double *js5);
 
 // ---------------------------------------------------------------------------
 // Device-side views.  All pointers are device pointers into one allocation.
@@ -46,7 +48,7 @@ struct Grid {
 };
 
 struct Phys {
-    double gamma, ups, psi, gam, suth, eps64;
+    double gamma, ups, psi, gam, suth, eps64, igm1;
     float eps32;
     int mms;
     int zeta_fix;

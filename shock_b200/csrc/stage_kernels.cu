@@ -179,9 +179,9 @@ __device__ __forceinline__ T phi_w5(const T *d, T eps)
     T is1 = T(13.) * (d[1] - d[2]) * (d[1] - d[2]) + T(3.) * (d[1] + d[2]) * (d[1] + d[2]);
     T is2 = T(13.) * (d[2] - d[3]) * (d[2] - d[3]) + T(3.) * (T(3.) * d[2] - d[3]) * (T(3.) * d[2] - d[3]);
     T a0 = (is0 + eps) * (is0 + eps), a1 = (is1 + eps) * (is1 + eps), a2 = (is2 + eps) * (is2 + eps);
-    T o0t = T(1.) / a0, o1t = T(6.) / a1, o2t = T(3.) / a2;
-    T s = o0t + o1t + o2t;
-    T o0 = o0t / s, o2 = o2t / s;
+    T o0t = T(1.) / a0, o1t = T(6.) * (T(1.) / a1), o2t = T(3.) * (T(1.) / a2);
+    T rs = T(1.) / (o0t + o1t + o2t);
+    T o0 = o0t * rs, o2 = o2t * rs;
     T q1 = d[0] - T(2.) * d[1] + d[2];
     T q2 = d[1] - T(2.) * d[2] + d[3];
     return T(1. / 3.) * o0 * q1 + T(1. / 6.) * (o2 - T(0.5)) * q2;
@@ -229,10 +229,10 @@ __device__ __forceinline__ T phi_w9(const T *f, const T *d, T eps)
             acc = (a == 0) ? f[k] * in : acc + f[k + a] * in;
         }
         T t = acc + eps;
-        ot[k] = dk[k] / (t * t);
+        ot[k] = dk[k] * (T(1.) / (t * t));
     }
-    T s = ot[0] + ot[1] + ot[2] + ot[3] + ot[4];
-    T o0 = ot[0] / s, o2 = ot[2] / s, o3 = ot[3] / s, o4 = ot[4] / s;
+    T rs = T(1.) / (ot[0] + ot[1] + ot[2] + ot[3] + ot[4]);
+    T o0 = ot[0] * rs, o2 = ot[2] * rs, o3 = ot[3] * rs, o4 = ot[4] * rs;
     T q1 = d[0] - T(4.) * d[1] + T(6.) * d[2] - T(4.) * d[3] + d[4];
     T q2 = d[1] - T(4.) * d[2] + T(6.) * d[3] - T(4.) * d[4] + d[5];
     T q3 = d[2] - T(4.) * d[3] + T(6.) * d[4] - T(4.) * d[5] + d[6];
@@ -359,7 +359,7 @@ __device__ __forceinline__ void stage_weno(const Grid &G, const Phys &P, const T
 // Face state (arithmetic means, src/WENO.c:1104-1139) and derived scalars.
 template <typename T>
 struct FaceState {
-    T u, v, w, rho, c, nx, ny, nz, q2, un, gc, irho, isc, kin, gm;
+    T u, v, w, rho, c, nx, ny, nz, q2, un, gc, irho, isc, kin, gm, ic, g1c, hc;
 };
 
 template <int DIM, int ORDER, int D, typename T>
@@ -387,12 +387,15 @@ __device__ __forceinline__ FaceState<T> face_state(const Phys &P, const double *
     }
 #undef SH
     s.q2 = s.u * s.u + s.v * s.v + s.w * s.w;
-    T M2 = s.q2 / (s.c * s.c);
+    s.ic = T(1) / s.c;
+    const T ic2 = s.ic * s.ic;
     s.un = s.u * s.nx + s.v * s.ny + s.w * s.nz;
-    s.gc = (s.gm - T(1)) / (s.c * s.c);
+    s.gc = (s.gm - T(1)) * ic2;
+    s.g1c = (s.gm - T(1)) * s.ic;                        // (gamma-1)/c
     s.irho = T(1) / s.rho;
-    s.isc = T(1) / (s.c * T(1.4142135623730951));
-    s.kin = T(1) - T(0.5) * (s.gm - T(1)) * M2;
+    s.isc = s.ic * T(0.70710678118654752440);            // 1/(c sqrt 2)
+    s.kin = T(1) - T(0.5) * (s.gm - T(1)) * (s.q2 * ic2);
+    s.hc = s.q2 / T(2) + s.c * s.c * (T)P.igm1;          // q^2/2 + c^2/(gamma-1)
     return s;
 }
 
@@ -400,7 +403,7 @@ __device__ __forceinline__ FaceState<T> face_state(const Phys &P, const double *
 template <typename T>
 __device__ __forceinline__ void left_row(const FaceState<T> &s, int ch, T &L0, T &L1, T &L2, T &L3, T &L4)
 {
-    const T sq2 = T(1.4142135623730951), g1 = s.gm - T(1);
+    const T isq2 = T(0.70710678118654752440), g1 = s.gm - T(1);
     switch (ch) {
     case 0:
         L0 = s.nx * s.kin - s.irho * (s.v * s.nz - s.w * s.ny); L1 = s.gc * s.u * s.nx;
@@ -412,11 +415,11 @@ __device__ __forceinline__ void left_row(const FaceState<T> &s, int ch, T &L0, T
         L0 = s.nz * s.kin - s.irho * (s.u * s.ny - s.v * s.nx); L1 = s.gc * s.u * s.nz + s.ny * s.irho;
         L2 = s.gc * s.v * s.nz - s.nx * s.irho; L3 = s.gc * s.w * s.nz; L4 = -s.gc * s.nz; break;
     case 3:
-        L0 = s.isc * (g1 * s.q2 / T(2) - s.c * s.un); L1 = (-g1 * s.u / s.c + s.nx) / sq2;
-        L2 = (-g1 * s.v / s.c + s.ny) / sq2; L3 = (-g1 * s.w / s.c + s.nz) / sq2; L4 = g1 * s.isc; break;
+        L0 = s.isc * (g1 * s.q2 / T(2) - s.c * s.un); L1 = (-s.g1c * s.u + s.nx) * isq2;
+        L2 = (-s.g1c * s.v + s.ny) * isq2; L3 = (-s.g1c * s.w + s.nz) * isq2; L4 = g1 * s.isc; break;
     default:
-        L0 = s.isc * (g1 * s.q2 / T(2) + s.c * s.un); L1 = (-g1 * s.u / s.c - s.nx) / sq2;
-        L2 = (-g1 * s.v / s.c - s.ny) / sq2; L3 = (-g1 * s.w / s.c - s.nz) / sq2; L4 = g1 * s.isc; break;
+        L0 = s.isc * (g1 * s.q2 / T(2) + s.c * s.un); L1 = (-s.g1c * s.u - s.nx) * isq2;
+        L2 = (-s.g1c * s.v - s.ny) * isq2; L3 = (-s.g1c * s.w - s.nz) * isq2; L4 = g1 * s.isc; break;
     }
 }
 
@@ -440,12 +443,12 @@ __device__ __forceinline__ void add_right_col(const FaceState<T> &s, int ch, T p
     case 3: {
         T sc = s.isc * phi;
         out[0] += sc; out[1] += (s.u + s.nx * s.c) * sc; out[2] += (s.v + s.ny * s.c) * sc;
-        out[3] += (s.w + s.nz * s.c) * sc; out[4] += (s.q2 / T(2) + s.c * s.c / (s.gm - T(1)) + s.c * s.un) * sc; break;
+        out[3] += (s.w + s.nz * s.c) * sc; out[4] += (s.hc + s.c * s.un) * sc; break;
     }
     default: {
         T sc = s.isc * phi;
         out[0] += sc; out[1] += (s.u - s.nx * s.c) * sc; out[2] += (s.v - s.ny * s.c) * sc;
-        out[3] += (s.w - s.nz * s.c) * sc; out[4] += (s.q2 / T(2) + s.c * s.c / (s.gm - T(1)) - s.c * s.un) * sc; break;
+        out[3] += (s.w - s.nz * s.c) * sc; out[4] += (s.hc - s.c * s.un) * sc; break;
     }
     }
 }
@@ -473,12 +476,16 @@ __device__ __forceinline__ void face_weno_fp64(const Phys &P, const double *sh, 
     for (int q = 0; q < 5; q++) out[q] = 0.0;
 #pragma unroll 1
     for (int ch = 0; ch < 5; ch++) {
+        // reload the window from shared memory in every iteration instead of
+        // holding 2r+2 points x 10 values in registers (keeps two tiles per SM)
+        asm volatile("" ::: "memory");
         double L0, L1, L2, L3, L4;
         left_row<double>(s, ch, L0, L1, L2, L3, L4);
         double Pp[2 * r + 2], Pm[2 * r + 2];
 #pragma unroll
         for (int q = 0; q <= 2 * r + 1; q++) {
             int t = f + q;
+            asm volatile("" ::: "memory");   // issue this point's loads here, not all up front
             double lf = L0 * SH(WF0 + 0, t, lane) + L1 * SH(WF0 + 1, t, lane) + L2 * SH(WF0 + 2, t, lane)
                         + L3 * SH(WF0 + 3, t, lane) + L4 * SH(WF0 + 4, t, lane);
             double lu = L0 * SH(WU0 + 0, t, lane) + L1 * SH(WU0 + 1, t, lane) + L2 * SH(WU0 + 2, t, lane)
@@ -532,6 +539,7 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
     float out[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
 #pragma unroll 1
     for (int ch = 0; ch < 5; ch++) {
+        asm volatile("" ::: "memory");
         float L0, L1, L2, L3, L4;
         left_row<float>(s, ch, L0, L1, L2, L3, L4);
         float dp[2 * r + 1], dmv[2 * r + 1];
@@ -589,8 +597,11 @@ __device__ __forceinline__ double central(const double *sh, int NP, int q, int t
 // (src/WENO.c:206-494 and its eta/zeta twins).  256 threads, 2 faces each;
 // the face fluxes reuse the staging buffer so two tiles fit on an SM.
 // ---------------------------------------------------------------------------
+#ifndef SHOCK_WENO_MINB
+#define SHOCK_WENO_MINB 2
+#endif
 template <int DIM, int ORDER, int D, bool MIXED>
-__global__ void __launch_bounds__(NTHR, 2)
+__global__ void __launch_bounds__(NTHR, SHOCK_WENO_MINB)
     k_weno(Grid G, Phys P, bool first, const double *__restrict__ R, const double *__restrict__ Uu,
            const double *__restrict__ Vv, const double *__restrict__ Ww, const double *__restrict__ Ee, Fields F)
 {
@@ -621,27 +632,40 @@ __global__ void __launch_bounds__(NTHR, 2)
         }
         __syncthreads();
     }
-    double res[2][5];
-    bool ok[2];
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-        const int f = row + k * NROWT;
-        ok[k] = T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1;
-        if (ok[k]) {
+    // face fluxes: faces 0..7 go to a dedicated buffer as soon as they are
+    // computed, faces 8..15 stay in registers until the staging buffer is free
+    double *f0 = smem + NV * NP * NLANE + (MIXED ? (10 * (NP - 1) * NLANE + 1) / 2 : 0);   // [5][NROWT][NLANE]
+    double res[5];
+    bool ok1;
+    {
+        const int f = row;
+        if (T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1) {
             double w5[5];
             if (MIXED) face_weno_mixed<DIM, ORDER, D>(P, sh, dl, f, lane, w5);
             else face_weno_fp64<DIM, ORDER, D>(P, sh, f, lane, w5);
 #pragma unroll
-            for (int q = 0; q < 5; q++) res[k][q] = w5[q] + central<ORDER>(sh, NP, q, r + f, lane);
+            for (int q = 0; q < 5; q++) f0[(q * NROWT + row) * NLANE + lane] = w5[q] + central<ORDER>(sh, NP, q, r + f, lane);
+        }
+    }
+    asm volatile("" ::: "memory");
+    {
+        const int f = row + NROWT;
+        ok1 = T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1;
+        if (ok1) {
+            double w5[5];
+            if (MIXED) face_weno_mixed<DIM, ORDER, D>(P, sh, dl, f, lane, w5);
+            else face_weno_fp64<DIM, ORDER, D>(P, sh, f, lane, w5);
+#pragma unroll
+            for (int q = 0; q < 5; q++) res[q] = w5[q] + central<ORDER>(sh, NP, q, r + f, lane);
         }
     }
     __syncthreads();
+    if (T.lane_ok) {
 #pragma unroll
-    for (int k = 0; k < 2; k++) {
-        const int f = row + k * NROWT;
-        if (ok[k])
+        for (int q = 0; q < 5; q++) fh[(q * NFACE + row) * NLANE + lane] = f0[(q * NROWT + row) * NLANE + lane];
+        if (ok1)
 #pragma unroll
-            for (int q = 0; q < 5; q++) fh[(q * NFACE + f) * NLANE + lane] = res[k][q];
+            for (int q = 0; q < 5; q++) fh[(q * NFACE + row + NROWT) * NLANE + lane] = res[q];
     }
     __syncthreads();
 #pragma unroll
@@ -1034,8 +1058,8 @@ static void weno_one(const Grid &G, const Phys &P, bool first, const double *con
 {
     constexpr int r = (ORDER - 1) / 2;
     constexpr int NP = TL + 2 * r + 2;
-    size_t smem = sizeof(double) * (size_t)WenoNV<DIM>::NV * NP * NLANE
-                  + (MIXED ? sizeof(float) * (size_t)10 * (NP - 1) * NLANE : 0);
+    size_t smem = sizeof(double) * ((size_t)WenoNV<DIM>::NV * NP * NLANE + 5 * NROWT * NLANE)
+                  + (MIXED ? sizeof(double) * (size_t)((10 * (NP - 1) * NLANE + 1) / 2) : 0);
     if (!G.order) {
         cudaFuncSetAttribute(k_weno<DIM, ORDER, D, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         return;
