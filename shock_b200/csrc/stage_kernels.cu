@@ -597,11 +597,10 @@ __device__ __forceinline__ double central(const double *sh, int NP, int q, int t
 // (src/WENO.c:206-494 and its eta/zeta twins).  256 threads, 2 faces each;
 // the face fluxes reuse the staging buffer so two tiles fit on an SM.
 // ---------------------------------------------------------------------------
-#ifndef SHOCK_WENO_MINB
-#define SHOCK_WENO_MINB 2
-#endif
+// WENO5 fits 128 registers (two tiles per SM); the WENO9 face needs more,
+// so it runs one tile per SM without spilling.
 template <int DIM, int ORDER, int D, bool MIXED>
-__global__ void __launch_bounds__(NTHR, SHOCK_WENO_MINB)
+__global__ void __launch_bounds__(NTHR, ORDER == 5 ? 2 : 1)
     k_weno(Grid G, Phys P, bool first, const double *__restrict__ R, const double *__restrict__ Uu,
            const double *__restrict__ Vv, const double *__restrict__ Ww, const double *__restrict__ Ee, Fields F)
 {
@@ -610,7 +609,6 @@ __global__ void __launch_bounds__(NTHR, SHOCK_WENO_MINB)
     constexpr int NV = WenoNV<DIM>::NV;
     extern __shared__ double smem[];
     double *sh = smem;                                  // [NV][NP][NLANE]
-    float *dl = (float *)(smem + NV * NP * NLANE);      // mixed: [10][NP-1][NLANE]
     double *fh = smem;                                  // [5][NFACE][NLANE], aliases sh after the faces
     const int lane = threadIdx.x, row = threadIdx.y;
     const Tile T = make_tile<DIM, D>(G, lane);
@@ -618,31 +616,66 @@ __global__ void __launch_bounds__(NTHR, SHOCK_WENO_MINB)
     stage_weno<DIM, ORDER, D>(G, P, T, sh, R, Uu, Vv, Ww, Ee, F);
     __syncthreads();
     if (MIXED) {
-        const int tid = row * NLANE + lane;
-        for (int it = tid; it < (NP - 1) * NLANE; it += NTHR) {
-            int l = it % NLANE, t = it / NLANE;
-            if (T.l0 + l >= G.g + T.nL || T.c0 - r + t >= G.N[D]) continue;
+        // fb: the 16 face fluxes of every line.  Central parts first (they need
+        // the FP64 point fluxes), then the FP32 differences overwrite the
+        // point-flux region, then the WENO parts are added.
+        double *fb = smem + NV * NP * NLANE;           // [5][NFACE][NLANE]
+        float *dl = (float *)(smem + WF0 * NP * NLANE); // [10][NP-1][NLANE] over the F region
 #pragma unroll
-            for (int q = 0; q < 5; q++) {
-                dl[((q) * (NP - 1) + t) * NLANE + l] =
-                    (float)(sh[((WF0 + q) * NP + t + 1) * NLANE + l] - sh[((WF0 + q) * NP + t) * NLANE + l]);
-                dl[((5 + q) * (NP - 1) + t) * NLANE + l] =
-                    (float)(sh[((WU0 + q) * NP + t + 1) * NLANE + l] - sh[((WU0 + q) * NP + t) * NLANE + l]);
+        for (int k = 0; k < 2; k++) {
+            const int f = row + k * NROWT;
+            if (T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1)
+#pragma unroll
+                for (int q = 0; q < 5; q++) fb[(q * NFACE + f) * NLANE + lane] = central<ORDER>(sh, NP, q, r + f, lane);
+        }
+        constexpr int NIT = ((NP - 1) * NLANE + NTHR - 1) / NTHR;
+        float dv[NIT][10];
+#pragma unroll
+        for (int m = 0; m < NIT; m++) {
+            int it = row * NLANE + lane + m * NTHR;
+            int l = it % NLANE, t = it / NLANE;
+            if (it < (NP - 1) * NLANE && T.l0 + l < G.g + T.nL && T.c0 - r + t < G.N[D]) {
+#pragma unroll
+                for (int q = 0; q < 5; q++) {
+                    dv[m][q] = (float)(sh[((WF0 + q) * NP + t + 1) * NLANE + l] - sh[((WF0 + q) * NP + t) * NLANE + l]);
+                    dv[m][5 + q] = (float)(sh[((WU0 + q) * NP + t + 1) * NLANE + l] - sh[((WU0 + q) * NP + t) * NLANE + l]);
+                }
             }
         }
         __syncthreads();
-    }
+#pragma unroll
+        for (int m = 0; m < NIT; m++) {
+            int it = row * NLANE + lane + m * NTHR;
+            int l = it % NLANE, t = it / NLANE;
+            if (it < (NP - 1) * NLANE && T.l0 + l < G.g + T.nL && T.c0 - r + t < G.N[D])
+#pragma unroll
+                for (int q = 0; q < 10; q++) dl[(q * (NP - 1) + t) * NLANE + l] = dv[m][q];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < 2; k++) {
+            const int f = row + k * NROWT;
+            asm volatile("" ::: "memory");
+            if (T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1) {
+                double w5[5];
+                face_weno_mixed<DIM, ORDER, D>(P, sh, dl, f, lane, w5);
+#pragma unroll
+                for (int q = 0; q < 5; q++) fb[(q * NFACE + f) * NLANE + lane] += w5[q];
+            }
+        }
+        __syncthreads();
+        fh = fb;
+    } else {
     // face fluxes: faces 0..7 go to a dedicated buffer as soon as they are
     // computed, faces 8..15 stay in registers until the staging buffer is free
-    double *f0 = smem + NV * NP * NLANE + (MIXED ? (10 * (NP - 1) * NLANE + 1) / 2 : 0);   // [5][NROWT][NLANE]
+    double *f0 = smem + NV * NP * NLANE;   // [5][NROWT][NLANE]
     double res[5];
     bool ok1;
     {
         const int f = row;
         if (T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1) {
             double w5[5];
-            if (MIXED) face_weno_mixed<DIM, ORDER, D>(P, sh, dl, f, lane, w5);
-            else face_weno_fp64<DIM, ORDER, D>(P, sh, f, lane, w5);
+            face_weno_fp64<DIM, ORDER, D>(P, sh, f, lane, w5);
 #pragma unroll
             for (int q = 0; q < 5; q++) f0[(q * NROWT + row) * NLANE + lane] = w5[q] + central<ORDER>(sh, NP, q, r + f, lane);
         }
@@ -653,8 +686,7 @@ __global__ void __launch_bounds__(NTHR, SHOCK_WENO_MINB)
         ok1 = T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1;
         if (ok1) {
             double w5[5];
-            if (MIXED) face_weno_mixed<DIM, ORDER, D>(P, sh, dl, f, lane, w5);
-            else face_weno_fp64<DIM, ORDER, D>(P, sh, f, lane, w5);
+            face_weno_fp64<DIM, ORDER, D>(P, sh, f, lane, w5);
 #pragma unroll
             for (int q = 0; q < 5; q++) res[q] = w5[q] + central<ORDER>(sh, NP, q, r + f, lane);
         }
@@ -668,16 +700,19 @@ __global__ void __launch_bounds__(NTHR, SHOCK_WENO_MINB)
             for (int q = 0; q < 5; q++) fh[(q * NFACE + row + NROWT) * NLANE + lane] = res[q];
     }
     __syncthreads();
+    }
+    // flux difference into Q; along a contiguous axis the threads walk the
+    // cells of one line (coalesced), otherwise one line per lane
+    for (int it = row * NLANE + lane; it < TL * NLANE; it += NTHR) {
+        int cr, ln;
+        if (Axes<DIM, D>::CONTIG) { cr = it % TL; ln = it / TL; }
+        else { ln = it % NLANE; cr = it / NLANE; }
+        if (T.l0 + ln >= G.g + T.nL || T.c0 + cr > G.g + T.nD - 1) continue;
+        long long o = T.base + (long long)ln * T.sL + (long long)(T.c0 + cr) * T.sD;
 #pragma unroll
-    for (int k = 0; k < 2; k++) {
-        const int cr = row + k * NROWT;      // cell row in the tile
-        if (cr < TL && T.lane_ok && T.c0 + cr <= G.g + T.nD - 1) {
-            long long o = T.base + (long long)lane * T.sL + (long long)(T.c0 + cr) * T.sD;
-#pragma unroll
-            for (int q = 0; q < 5; q++) {
-                double prev = first ? 0.0 : F.Q[q][o];
-                F.Q[q][o] = prev - (fh[(q * NFACE + cr + 1) * NLANE + lane] - fh[(q * NFACE + cr) * NLANE + lane]);
-            }
+        for (int q = 0; q < 5; q++) {
+            double prev = first ? 0.0 : F.Q[q][o];
+            F.Q[q][o] = prev - (fh[(q * NFACE + cr + 1) * NLANE + ln] - fh[(q * NFACE + cr) * NLANE + ln]);
         }
     }
 }
@@ -870,12 +905,14 @@ __global__ void __launch_bounds__(NTHR, 2)
     }
     __syncthreads();
 
-    // ---- cell update ----------------------------------------------------------
-#pragma unroll
-    for (int k = 0; k < 2; k++) {
-        const int cr = row + k * NROWT;
-        if (!(cr < TL && T.lane_ok && T.c0 + cr <= G.g + T.nD - 1)) continue;
-        long long o = T.base + (long long)lane * T.sL + (long long)(T.c0 + cr) * T.sD;
+    // ---- cell update: along a contiguous axis the threads walk the cells of
+    // one line (coalesced), otherwise one line per thread lane ----------------
+    for (int it = row * NLANE + threadIdx.x; it < TL * NLANE; it += NTHR) {
+        int cr, ln;
+        if (A::CONTIG) { cr = it % TL; ln = it / TL; }
+        else { ln = it % NLANE; cr = it / NLANE; }
+        if (T.l0 + ln >= G.g + T.nL || T.c0 + cr > G.g + T.nD - 1) continue;
+        long long o = T.base + (long long)ln * T.sL + (long long)(T.c0 + cr) * T.sD;
         double mu = F.mu[o], J = F.J[o];
         double vel[3] = {Uu[o], Vv[o], DIM == 3 ? Ww[o] : 0.0};
         double gp[3] = {0, 0, 0}, gmn[3] = {0, 0, 0}, hp = 0, hm = 0;
@@ -883,12 +920,12 @@ __global__ void __launch_bounds__(NTHR, 2)
         if (DIM == 3) {
             double cd = F.m[4 * D][o], ca = F.m[4 * MA][o], cb = F.m[4 * MB][o];
             if (quirk) {
-                double K1p = FO(0, cr + 1, lane), KAp = FO(1, cr + 1, lane), KBp = FO(2, cr + 1, lane);
-                double K1m = FO(0, cr, lane), KAm = FO(1, cr, lane), KBm = FO(2, cr, lane);
+                double K1p = FO(0, cr + 1, ln), KAp = FO(1, cr + 1, ln), KBp = FO(2, cr + 1, ln);
+                double K1m = FO(0, cr, ln), KAm = FO(1, cr, ln), KBm = FO(2, cr, ln);
                 // QD: side 0 = minus (j-1/2), side 1 = plus; quantities u,v,w,T along, then x0..x3
                 double Dm[8], Dp[8];
 #pragma unroll
-                for (int q = 0; q < 8; q++) { Dm[q] = QD(q, lane); Dp[q] = QD(8 + q, lane); }
+                for (int q = 0; q < 8; q++) { Dm[q] = QD(q, ln); Dp[q] = QD(8 + q, ln); }
                 gp[D] = Dp[D] * (t43 * K1p) + Dp[4] * (-t23 * KAp) + Dp[5] * (-t23 * KBp);
                 gp[MA] = Dp[MA] * K1p + Dp[6] * KAp;
                 gp[MB] = Dp[MB] * K1p + Dp[7] * KBp;
@@ -899,9 +936,9 @@ __global__ void __launch_bounds__(NTHR, 2)
                 hm = Dm[3] * K1m;
             } else {
 #pragma unroll
-                for (int q = 0; q < 3; q++) { gp[q] = FO(q, cr + 1, lane); gmn[q] = FO(q, cr, lane); }
-                hp = FO(3, cr + 1, lane);
-                hm = FO(3, cr, lane);
+                for (int q = 0; q < 3; q++) { gp[q] = FO(q, cr + 1, ln); gmn[q] = FO(q, cr, ln); }
+                hp = FO(3, cr + 1, ln);
+                hm = FO(3, cr, ln);
             }
             // node term: mu * sum_i N[i][D] * sum_{k,m} N[k][m] Fac[i][k][m] at the cell
             double F1 = J * (cd * cd), FA = J * (cd * ca), FB = J * (cd * cb);
@@ -915,9 +952,9 @@ __global__ void __launch_bounds__(NTHR, 2)
         } else {
             constexpr int E = 1 - D;
 #pragma unroll
-            for (int q = 0; q < 2; q++) { gp[q] = FO(q, cr + 1, lane); gmn[q] = FO(q, cr, lane); }
-            hp = FO(2, cr + 1, lane);
-            hm = FO(2, cr, lane);
+            for (int q = 0; q < 2; q++) { gp[q] = FO(q, cr + 1, ln); gmn[q] = FO(q, cr, ln); }
+            hp = FO(2, cr + 1, ln);
+            hm = FO(2, cr, ln);
             double ax = F.m[3 * D + 0][o], ay = F.m[3 * D + 1][o];
             double gmv[2][2];
             gmv[D][0] = ax; gmv[D][1] = ay; gmv[E][0] = F.m[3 * E + 0][o]; gmv[E][1] = F.m[3 * E + 1][o];
@@ -1058,8 +1095,7 @@ static void weno_one(const Grid &G, const Phys &P, bool first, const double *con
 {
     constexpr int r = (ORDER - 1) / 2;
     constexpr int NP = TL + 2 * r + 2;
-    size_t smem = sizeof(double) * ((size_t)WenoNV<DIM>::NV * NP * NLANE + 5 * NROWT * NLANE)
-                  + (MIXED ? sizeof(double) * (size_t)((10 * (NP - 1) * NLANE + 1) / 2) : 0);
+    size_t smem = sizeof(double) * ((size_t)WenoNV<DIM>::NV * NP * NLANE + 5 * (MIXED ? NFACE : NROWT) * NLANE);
     if (!G.order) {
         cudaFuncSetAttribute(k_weno<DIM, ORDER, D, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         return;
