@@ -49,10 +49,9 @@ __device__ __forceinline__ bool is_real(const Grid &G, int a, int i) { return i 
 // ghosts: periodic images over the ghost shell (all periodic axes at once;
 // equivalent to SHOCK's repeated slab exchange).
 // ---------------------------------------------------------------------------
-__global__ void k_ghosts(Grid G, double *r, double *u, double *v, double *w, double *e)
+__device__ __forceinline__ void ghost_body(const Grid &G, long long o, double *r, double *u, double *v, double *w,
+                                           double *e)
 {
-    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (o >= G.NG) return;
     Idx3 p = unflatten(G, o);
     Idx3 s = p;
     bool ghost = false;
@@ -71,16 +70,22 @@ __global__ void k_ghosts(Grid G, double *r, double *u, double *v, double *w, dou
     e[o] = e[q];
 }
 
+__global__ void k_ghosts(Grid G, double *r, double *u, double *v, double *w, double *e)
+{
+    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (o < G.NG) ghost_body(G, o, r, u, v, w, e);
+}
+
 // ---------------------------------------------------------------------------
 // prim: CalcValues (p with fabs, T = |p/rho|, c, Sutherland mu or mu = 1).
 // ---------------------------------------------------------------------------
 template <int DIM>
-__global__ void k_prim(Grid G, Phys P, const double *__restrict__ R, const double *__restrict__ U,
-                       const double *__restrict__ V, const double *__restrict__ W,
-                       const double *__restrict__ E, double *p, double *T, double *c, double *mu)
+__device__ __forceinline__ void prim_body(const Grid &G, const Phys &P, long long o, const double *__restrict__ R,
+                                          const double *__restrict__ U, const double *__restrict__ V,
+                                          const double *__restrict__ W, const double *__restrict__ E, double *p,
+                                          double *T, double *c, double *mu)
 {
-    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (o >= G.NG) return;
+    (void)G;
     double rho = R[o], u = U[o], v = V[o], e = E[o];
     double q2 = (u * u) + (v * v);
     if (DIM == 3) {
@@ -93,6 +98,15 @@ __global__ void k_prim(Grid G, Phys P, const double *__restrict__ R, const doubl
     T[o] = fabs(pr);
     c[o] = sqrt(P.ups * P.gamma * pp / rho);
     mu[o] = P.mms ? 1.0 : ((1.0 + P.suth) * pow(pr, 1.5) / (pr + P.suth));
+}
+
+template <int DIM>
+__global__ void k_prim(Grid G, Phys P, const double *__restrict__ R, const double *__restrict__ U,
+                       const double *__restrict__ V, const double *__restrict__ W,
+                       const double *__restrict__ E, double *p, double *T, double *c, double *mu)
+{
+    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (o < G.NG) prim_body<DIM>(G, P, o, R, U, V, W, E, p, T, c, mu);
 }
 
 // ---------------------------------------------------------------------------
@@ -145,12 +159,11 @@ struct ZD<9> {
 };
 
 template <int DIM, int ORDER>
-__global__ void k_nodal(Grid G, const double *__restrict__ U, const double *__restrict__ V,
-                        const double *__restrict__ W, const double *__restrict__ T, Fields F)
+__device__ __forceinline__ void nodal_body(const Grid &G, long long o, const double *__restrict__ U,
+                                           const double *__restrict__ V, const double *__restrict__ W,
+                                           const double *__restrict__ T, const Fields &F)
 {
     constexpr int H = ZD<ORDER>::H;
-    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (o >= G.NG) return;
     Idx3 p = unflatten(G, o);
     const double *var[4] = {U, V, W, T};
 #pragma unroll
@@ -167,6 +180,14 @@ __global__ void k_nodal(Grid G, const double *__restrict__ U, const double *__re
             F.Nd[3 * q + d][o] = acc;
         }
     }
+}
+
+template <int DIM, int ORDER>
+__global__ void k_nodal(Grid G, const double *__restrict__ U, const double *__restrict__ V,
+                        const double *__restrict__ W, const double *__restrict__ T, Fields F)
+{
+    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (o < G.NG) nodal_body<DIM, ORDER>(G, o, U, V, W, T, F);
 }
 
 // ---------------------------------------------------------------------------
@@ -275,13 +296,13 @@ struct Tile {
 };
 
 template <int DIM, int D>
-__device__ __forceinline__ Tile make_tile(const Grid &G, int lane)
+__device__ __forceinline__ Tile make_tile(const Grid &G, int lane, int bx, int by, int bz)
 {
     using A = Axes<DIM, D>;
     Tile t;
-    t.c0 = G.g + blockIdx.x * TL;
-    t.l0 = G.g + blockIdx.y * NLANE;
-    const int oth = (DIM == 3) ? G.g + blockIdx.z : 0;
+    t.c0 = G.g + bx * TL;
+    t.l0 = G.g + by * NLANE;
+    const int oth = (DIM == 3) ? G.g + bz : 0;
     t.nD = G.n[D];
     t.nL = G.n[A::LAT];
     t.sD = G.st[D];
@@ -306,9 +327,10 @@ __device__ __forceinline__ void stage_weno(const Grid &G, const Phys &P, const T
 #define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
     const int tid = threadIdx.y * NLANE + threadIdx.x;
     for (int it = tid; it < NP * NLANE; it += NTHR) {
-        int t, l;
-        if (A::CONTIG) { t = it % NP; l = it / NP; }
-        else { l = it % NLANE; t = it / NLANE; }
+        // lane-fastest: conflict-free shared-memory stores; along a
+        // contiguous axis the 32 lines are 32 strided rows whose sectors the
+        // following points of the loop reuse from L1
+        const int l = it % NLANE, t = it / NLANE;
         int pd = T.c0 - 1 - r + t;
         if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
         long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
@@ -600,9 +622,10 @@ __device__ __forceinline__ double central(const double *sh, int NP, int q, int t
 // WENO5 fits 128 registers (two tiles per SM); the WENO9 face needs more,
 // so it runs one tile per SM without spilling.
 template <int DIM, int ORDER, int D, bool MIXED>
-__global__ void __launch_bounds__(NTHR, ORDER == 5 ? 2 : 1)
-    k_weno(Grid G, Phys P, bool first, const double *__restrict__ R, const double *__restrict__ Uu,
-           const double *__restrict__ Vv, const double *__restrict__ Ww, const double *__restrict__ Ee, Fields F)
+__device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool first, const double *__restrict__ R,
+                                          const double *__restrict__ Uu, const double *__restrict__ Vv,
+                                          const double *__restrict__ Ww, const double *__restrict__ Ee,
+                                          const Fields &F, int bx, int by, int bz)
 {
     constexpr int r = (ORDER - 1) / 2;
     constexpr int NP = TL + 2 * r + 2;
@@ -611,7 +634,7 @@ __global__ void __launch_bounds__(NTHR, ORDER == 5 ? 2 : 1)
     double *sh = smem;                                  // [NV][NP][NLANE]
     double *fh = smem;                                  // [5][NFACE][NLANE], aliases sh after the faces
     const int lane = threadIdx.x, row = threadIdx.y;
-    const Tile T = make_tile<DIM, D>(G, lane);
+    const Tile T = make_tile<DIM, D>(G, lane, bx, by, bz);
 
     stage_weno<DIM, ORDER, D>(G, P, T, sh, R, Uu, Vv, Ww, Ee, F);
     __syncthreads();
@@ -717,6 +740,14 @@ __global__ void __launch_bounds__(NTHR, ORDER == 5 ? 2 : 1)
     }
 }
 
+template <int DIM, int ORDER, int D, bool MIXED>
+__global__ void __launch_bounds__(NTHR, ORDER == 5 ? 2 : 1)
+    k_weno(Grid G, Phys P, bool first, const double *__restrict__ R, const double *__restrict__ Uu,
+           const double *__restrict__ Vv, const double *__restrict__ Ww, const double *__restrict__ Ee, Fields F)
+{
+    weno_body<DIM, ORDER, D, MIXED>(G, P, first, R, Uu, Vv, Ww, Ee, F, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 // ---------------------------------------------------------------------------
 // visc_d: central viscous flux difference (src/ZD.c:47-694).
 //
@@ -731,9 +762,9 @@ enum { V3U = 0, V3V, V3W, V3T, V3X0, V3X1, V3X2, V3X3, V3F1, V3FA, V3FB, V3NV };
 enum { V2U = 0, V2V, V2T, V2XU, V2XV, V2XT, V2MJ, V2AX, V2AY, V2BX, V2BY, V2NV };
 
 template <int DIM, int ORDER, int D, bool MIXED>
-__global__ void __launch_bounds__(NTHR, 2)
-    k_visc(Grid G, Phys P, const double *__restrict__ Uu, const double *__restrict__ Vv,
-           const double *__restrict__ Ww, Fields F)
+__device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const double *__restrict__ Uu,
+                                          const double *__restrict__ Vv, const double *__restrict__ Ww,
+                                          const Fields &F, int bx, int by, int bz)
 {
     using A = Axes<DIM, D>;
     using TS = typename std::conditional<MIXED, float, double>::type;   // stencil arithmetic
@@ -753,14 +784,15 @@ __global__ void __launch_bounds__(NTHR, 2)
 #define QD(c, l) qd[(c) * NLANE + (l)]
 
     const int lane = threadIdx.x, row = threadIdx.y;
-    const Tile T = make_tile<DIM, D>(G, lane);
+    const Tile T = make_tile<DIM, D>(G, lane, bx, by, bz);
 
     // ---- stage: points c0-H .. c0+TL+H-1 along the sweep ----------------------
     const int tid = row * NLANE + lane;
     for (int it = tid; it < NP * NLANE; it += NTHR) {
-        int t, l;
-        if (A::CONTIG) { t = it % NP; l = it / NP; }
-        else { l = it % NLANE; t = it / NLANE; }
+        // lane-fastest: conflict-free shared-memory stores; along a
+        // contiguous axis the 32 lines are 32 strided rows whose sectors the
+        // following points of the loop reuse from L1
+        const int l = it % NLANE, t = it / NLANE;
         int pd = T.c0 - H + t;
         if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
         long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
@@ -913,12 +945,11 @@ __global__ void __launch_bounds__(NTHR, 2)
         else { ln = it % NLANE; cr = it / NLANE; }
         if (T.l0 + ln >= G.g + T.nL || T.c0 + cr > G.g + T.nD - 1) continue;
         long long o = T.base + (long long)ln * T.sL + (long long)(T.c0 + cr) * T.sD;
-        double mu = F.mu[o], J = F.J[o];
-        double vel[3] = {Uu[o], Vv[o], DIM == 3 ? Ww[o] : 0.0};
+        const int ts = cr + H;        // staged index of the cell
         double gp[3] = {0, 0, 0}, gmn[3] = {0, 0, 0}, hp = 0, hm = 0;
-        double nodeB = 0;
+        double nodeB = 0, vel[3];
         if (DIM == 3) {
-            double cd = F.m[4 * D][o], ca = F.m[4 * MA][o], cb = F.m[4 * MB][o];
+            vel[0] = SH(V3U, ts, ln); vel[1] = SH(V3V, ts, ln); vel[2] = SH(V3W, ts, ln);
             if (quirk) {
                 double K1p = FO(0, cr + 1, ln), KAp = FO(1, cr + 1, ln), KBp = FO(2, cr + 1, ln);
                 double K1m = FO(0, cr, ln), KAm = FO(1, cr, ln), KBm = FO(2, cr, ln);
@@ -940,27 +971,30 @@ __global__ void __launch_bounds__(NTHR, 2)
                 hp = FO(3, cr + 1, ln);
                 hm = FO(3, cr, ln);
             }
-            // node term: mu * sum_i N[i][D] * sum_{k,m} N[k][m] Fac[i][k][m] at the cell
-            double F1 = J * (cd * cd), FA = J * (cd * ca), FB = J * (cd * cb);
-            double nDD = F.Nd[3 * D + D][o], nAA = F.Nd[3 * MA + MA][o], nBB = F.Nd[3 * MB + MB][o];
-            double nAD = F.Nd[3 * MA + D][o], nBD = F.Nd[3 * MB + D][o];
-            double nDA = F.Nd[3 * D + MA][o], nDB = F.Nd[3 * D + MB][o];
+            // node term: mu * sum_i N[i][D] * sum_{k,m} N[k][m] Fac[i][k][m] at the cell;
+            // the staged factors already carry mu*J
+            const double F1 = SH(V3F1, ts, ln), FA = SH(V3FA, ts, ln), FB = SH(V3FB, ts, ln);
+            const double nAA = SH(V3X0, ts, ln), nBB = SH(V3X1, ts, ln);
+            const double nDA = SH(V3X2, ts, ln), nDB = SH(V3X3, ts, ln);
+            const double nDD = F.Nd[3 * D + D][o], nAD = F.Nd[3 * MA + D][o], nBD = F.Nd[3 * MB + D][o];
             double hD = nDD * (t43 * F1) + nAA * (-t23 * FA) + nBB * (-t23 * FB);
             double hA = nAD * F1 + nDA * FA;
             double hB = nBD * F1 + nDB * FB;
-            nodeB = mu * (nDD * hD + nAD * hA + nBD * hB);
+            nodeB = nDD * hD + nAD * hA + nBD * hB;
         } else {
             constexpr int E = 1 - D;
+            vel[0] = SH(V2U, ts, ln); vel[1] = SH(V2V, ts, ln); vel[2] = 0.0;
 #pragma unroll
             for (int q = 0; q < 2; q++) { gp[q] = FO(q, cr + 1, ln); gmn[q] = FO(q, cr, ln); }
             hp = FO(2, cr + 1, ln);
             hm = FO(2, cr, ln);
-            double ax = F.m[3 * D + 0][o], ay = F.m[3 * D + 1][o];
+            double ax = SH(V2AX, ts, ln), ay = SH(V2AY, ts, ln);
             double gmv[2][2];
-            gmv[D][0] = ax; gmv[D][1] = ay; gmv[E][0] = F.m[3 * E + 0][o]; gmv[E][1] = F.m[3 * E + 1][o];
+            gmv[D][0] = ax; gmv[D][1] = ay; gmv[E][0] = SH(V2BX, ts, ln); gmv[E][1] = SH(V2BY, ts, ln);
             double av[2] = {ax, ay};
-            double N[2][2];
-            N[0][0] = F.Nd[0][o]; N[0][1] = F.Nd[1][o]; N[1][0] = F.Nd[3][o]; N[1][1] = F.Nd[4][o];
+            double N[2][2];   // N[var][dir]
+            N[0][E] = SH(V2XU, ts, ln); N[1][E] = SH(V2XV, ts, ln);
+            N[0][D] = F.Nd[3 * 0 + D][o]; N[1][D] = F.Nd[3 * 1 + D][o];
             double hsum[2] = {0, 0};
 #pragma unroll
             for (int m = 0; m < 2; m++) {
@@ -974,7 +1008,7 @@ __global__ void __launch_bounds__(NTHR, 2)
                     }
                 }
             }
-            nodeB = mu * J * (N[0][D] * hsum[0] + N[1][D] * hsum[1]);
+            nodeB = SH(V2MJ, ts, ln) * (N[0][D] * hsum[0] + N[1][D] * hsum[1]);
         }
         const double psi = P.psi;
         F.Q[1][o] = F.Q[1][o] + psi * (gp[0] - gmn[0]);
@@ -989,16 +1023,23 @@ __global__ void __launch_bounds__(NTHR, 2)
 #undef QD
 }
 
+template <int DIM, int ORDER, int D, bool MIXED>
+__global__ void __launch_bounds__(NTHR, 2)
+    k_visc(Grid G, Phys P, const double *__restrict__ Uu, const double *__restrict__ Vv,
+           const double *__restrict__ Ww, Fields F)
+{
+    visc_body<DIM, ORDER, D, MIXED>(G, P, Uu, Vv, Ww, F, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
 // ---------------------------------------------------------------------------
 // RK stage update of the real points (src/Functions.c:2300-2365), with the
 // time-independent source J*S added to Q first.
 // ---------------------------------------------------------------------------
 template <int DIM>
-__global__ void k_rk(Grid G, RKCoef K, double tau, StageIn in, Fields F, double *o0, double *o1,
-                     double *o2, double *o3, double *o4, int has_source, int nreal)
+__device__ __forceinline__ void rk_body(const Grid &G, const RKCoef &K, double tau, const StageIn &in,
+                                        const Fields &F, double *o0, double *o1, double *o2, double *o3, double *o4,
+                                        int has_source, int t)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nreal) return;
     int i, j, k;
     if (DIM == 3) {
         k = t % G.n[2];
@@ -1029,6 +1070,14 @@ __global__ void k_rk(Grid G, RKCoef K, double tau, StageIn in, Fields F, double 
         if (DIM == 2 && c == 3) { outs[3][o] = 0.0; continue; }
         outs[c][o] = (K.a * F.Un[c][o] * F.Un[0][o] + K.b * in.U[c][o] * ro + tj * (K.c * Q[c] + K.d * Qs[c])) / rn;
     }
+}
+
+template <int DIM>
+__global__ void k_rk(Grid G, RKCoef K, double tau, StageIn in, Fields F, double *o0, double *o1,
+                     double *o2, double *o3, double *o4, int has_source, int nreal)
+{
+    int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < nreal) rk_body<DIM>(G, K, tau, in, F, o0, o1, o2, o3, o4, has_source, t);
 }
 
 __global__ void k_add_source(Grid G, Fields F)
