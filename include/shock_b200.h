@@ -155,6 +155,44 @@ int shock_profile_stage(shock_ctx *ctx, int max, char *names, float *ms, int *co
  * measured with a register-only FMA loop (roofline denominators). */
 int shock_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 
+/* Largest block (ghosted points NIg*NJg*NKg) shock_rhs_static accepts. */
+#define SHOCK_STATIC_MAX_POINTS 524288
+
+/* One stage right-hand side (the same kernels as shock_rhs) on device
+ * buffers that the caller owns, allocating nothing on the device or the
+ * host.  No counterpart in the reference: SHOCK's RHS functions always run
+ * on its own calloc'd arrays.  It is for callers that cannot let a library
+ * allocate, because they have already split the GPU's memory among their
+ * own objects (a loop admitting work against a fixed HBM budget, a solver
+ * with its own arena), and that do not want a shock_ctx's 16 scratch
+ * fields kept per block.
+ *
+ *   p       block description as for shock_create; all axes periodic
+ *           (mms = 0); at most SHOCK_STATIC_MAX_POINTS ghosted points,
+ *           larger blocks return SHOCK_EINVAL.  tau is not used.
+ *   geom13  device pointer, 13*NG doubles: x,y,z,J and the nine metric
+ *           terms as shock_host_geometry writes them (read only).
+ *   state5  device pointer, 5*NG doubles rho,u,v,w,e; its periodic ghost
+ *           points are overwritten with their images, as SHOCK's halo
+ *           exchange does to U_RK.
+ *   q5      device pointer, 5*NG doubles; the right-hand side is written
+ *           on the real points, ghost points are left as they were.
+ *   stream  a cudaStream_t (NULL: the default stream); the work is queued
+ *           there and the call returns without waiting.
+ *
+ * The intermediate fields (p, T, c, mu, 12 nodal derivatives) live in one
+ * fixed 64 MiB array per device inside the library.  The first call on a
+ * device sets up that device (finds the array's address and raises the
+ * kernels' shared-memory limits), so make one call on each device before
+ * any stream capture.  The array is shared by all calls on a device and
+ * keeps what the last call left in it: calls that may overlap in time (on
+ * different streams, or from different host threads) race and give wrong
+ * results; serialise them, e.g. on one stream.  Part of the array is
+ * cleared on the stream at the start of each viscous call (the nodal
+ * derivatives must read as zero where they are not computed); nothing
+ * else needs to start at zero. */
+int shock_rhs_static(const shock_params *p, const double *geom13, double *state5, double *q5, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -43,6 +43,20 @@ int fail(int code, const char *fmt, ...)
 
 }  // namespace
 
+namespace shock {
+// Record an error message for shock_last_error from another translation unit.
+int report_error(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_err = buf;
+    return code;
+}
+}  // namespace shock
+
 struct shock_ctx {
     shock_params p{};
     Layout L;

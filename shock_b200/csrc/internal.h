@@ -88,6 +88,7 @@ void launch_copy_state(const Grid &G, const double *const src[5], double *const 
 void launch_nan_check(const Grid &G, const double *rho, unsigned int *flag, cudaStream_t s);
 void launch_add_source(const Grid &G, const Fields &F, cudaStream_t s);
 void prepare_kernels();
+int report_error(int code, const char *fmt, ...);   // sets shock_last_error, returns code
 double fma_probe(int fp64, int sms, cudaStream_t s);
 
 }  // namespace shock
