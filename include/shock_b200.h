@@ -155,6 +155,115 @@ int shock_profile_stage(shock_ctx *ctx, int max, char *names, float *ms, int *co
  * measured with a register-only FMA loop (roofline denominators). */
 int shock_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops);
 
+/* ------------------------------------------------------------------------
+ * Batched execution (no counterpart in the reference, which runs one block
+ * per MPI rank): many independent periodic blocks ("members") of one class
+ * (dim, order, precision, time_order) advanced together on one device, each
+ * with its own size, physics, tau and number of steps.  Every RK stage of
+ * all members is one persistent launch (or one launch per phase, see
+ * shock_batch_tuning); a time step is one CUDA graph.  A member's results
+ * are the same as a shock_ctx running that block alone.
+ * ------------------------------------------------------------------------ */
+typedef struct shock_batch shock_batch;
+
+typedef struct shock_batch_tuning {
+    int persistent;          /* 1: one cooperative launch per stage (grid barriers between phases);
+                                0: one launch per phase */
+    int blocks_per_sm;       /* resident tiles per SM of the persistent / sweep launches */
+    int chunk;               /* points per item of the point-wise phases (multiple of 256) */
+    int small_tile_max;      /* members whose longest axis has at most this many points use
+                                7-cell sweep tiles (one face per thread) instead of 15-cell ones */
+    int max_blocks_per_sm;   /* out: occupancy limit of the chosen form */
+} shock_batch_tuning;
+
+/* arena_bytes of device memory are allocated once and are the batch's HBM
+ * budget: members are placed in it without further allocation. */
+int shock_batch_create(int dim, int order, int precision, int time_order, size_t arena_bytes, int device,
+                       shock_batch **out);
+int shock_batch_destroy(shock_batch *b);
+/* Device bytes one member described by p takes from the arena. */
+int shock_batch_member_bytes(const shock_params *p, size_t *bytes);
+/* Add a member (arguments as shock_create) that will run nsteps time steps;
+ * *member receives its handle.  SHOCK_ENOMEM when it does not fit in the
+ * arena.  Takes effect at the next step call. */
+int shock_batch_add(shock_batch *b, const shock_params *p, const double *x, const double *y, const double *z,
+                    const double *u, const double *v, const double *w, const double *pr, const double *rho,
+                    int nsteps, int *member);
+/* Remove a member and return its memory to the arena (waits for the
+ * batch's queued work). */
+int shock_batch_remove(shock_batch *b, int member);
+/* nsteps time steps of every member that still has steps to run; members
+ * whose count reaches zero stay frozen at their final state. */
+int shock_batch_step(shock_batch *b, int nsteps);
+int shock_batch_step_async(shock_batch *b, int nsteps);
+/* Wait for queued steps; SHOCK_ETIMEOUT if a grid-barrier wait ran out. */
+int shock_batch_sync(shock_batch *b);
+/* Device time (ms) of the last shock_batch_step(_async) call's steps. */
+int shock_batch_last_ms(const shock_batch *b, float *ms);
+int shock_batch_steps_left(const shock_batch *b, int member, int *left);
+/* Ghosted sizes and first real index of a member (as shock_dims). */
+int shock_batch_dims(const shock_batch *b, int member, int out6[6]);
+/* A member's current rho,u,v,w,e (5*NG doubles, ghosted). */
+int shock_batch_download_state(shock_batch *b, int member, double *prim5);
+int shock_batch_set_tuning(shock_batch *b, const shock_batch_tuning *t);
+int shock_batch_get_tuning(const shock_batch *b, shock_batch_tuning *t);
+/* Active members, arena bytes in use / total, kernel launches per step. */
+int shock_batch_info(const shock_batch *b, int *members, size_t *arena_used, size_t *arena_total,
+                     int *kernels_per_step);
+
+/* ------------------------------------------------------------------------
+ * Serving (no counterpart in the reference): a request loop that takes
+ * solve requests (one periodic block, its initial state and a number of
+ * time steps) as they arrive, keeps their state on the device, admits them
+ * against an HBM budget and advances every admitted request with continuous
+ * batching (one batch per class; classes run on their own streams).  A
+ * request's result is the same alone and in any mix.
+ * ------------------------------------------------------------------------ */
+typedef struct shock_server shock_server;
+
+typedef struct shock_server_config {
+    int device;
+    size_t hbm_budget;       /* device bytes for request state; reserved once at creation */
+    int max_requests;        /* requests on the device at once (0: limited by memory only) */
+    int setup_threads;       /* host threads building grids and metrics ahead of admission (0: 4) */
+    double round_ms;         /* device time per round of steps between admissions (0: 10 ms) */
+} shock_server_config;
+
+typedef struct shock_request_info {
+    double submit_s, admit_s, done_s;   /* server clock (s since creation): time to solution = done - submit */
+    double cell_stages;                 /* real points x stages x steps */
+    int status;                         /* SHOCK_OK or the error that failed the request */
+    int dims[6];                        /* ghosted sizes and first real index (as shock_dims) */
+} shock_request_info;
+
+typedef struct shock_server_stats {
+    long long queued, running, completed, failed, rounds, steps_launched;
+    double cell_stages;      /* of completed requests */
+    double busy_ms;          /* device time of all rounds */
+    size_t arena_used, arena_total;
+    double uptime_s;
+    int loop_error;
+} shock_server_stats;
+
+int shock_server_create(const shock_server_config *cfg, shock_server **out);
+/* Launch configuration of one request class; before its first request. */
+int shock_server_set_tuning(shock_server *s, int dim, int order, int precision, int time_order,
+                            const shock_batch_tuning *t);
+/* Queue a request (arguments as shock_create; p->precision selects the
+ * form).  The inputs are copied; *id identifies the request.  SHOCK_ENOMEM
+ * if it could never fit in the budget. */
+int shock_server_submit(shock_server *s, const shock_params *p, const double *x, const double *y, const double *z,
+                        const double *u, const double *v, const double *w, const double *pr, const double *rho,
+                        int nsteps, long long *id);
+/* Wait until request id has finished (SHOCK_ETIMEOUT after timeout_s). */
+int shock_server_wait(shock_server *s, long long id, double timeout_s);
+/* Final rho,u,v,w,e of a finished request (5*NG doubles, ghosted; prim5 may
+ * be NULL) and its timings; releases the request. */
+int shock_server_result(shock_server *s, long long id, double *prim5, size_t n, shock_request_info *info);
+int shock_server_get_stats(shock_server *s, shock_server_stats *st);
+/* Stop the loop (requests not finished are dropped) and free everything. */
+int shock_server_destroy(shock_server *s);
+
 /* Largest block (ghosted points NIg*NJg*NKg) shock_rhs_static accepts. */
 #define SHOCK_STATIC_MAX_POINTS 524288
 

@@ -78,8 +78,23 @@ def lib():
                          "shock_step_async", "shock_sync", "shock_check_nan", "shock_geometry",
                          "shock_device_bytes", "shock_last_step_ms", "shock_kernels_per_step",
                          "shock_mms_baseline", "shock_profile_stage", "shock_measure_fma_peak",
-                         "shock_host_geometry", "shock_host_mms_baseline"):
+                         "shock_host_geometry", "shock_host_mms_baseline", "shock_rhs_static",
+                         "shock_batch_create", "shock_batch_destroy", "shock_batch_member_bytes",
+                         "shock_batch_add", "shock_batch_remove", "shock_batch_step", "shock_batch_step_async",
+                         "shock_batch_sync", "shock_batch_last_ms", "shock_batch_steps_left",
+                         "shock_batch_dims", "shock_batch_download_state", "shock_batch_set_tuning",
+                         "shock_batch_get_tuning", "shock_batch_info", "shock_server_create",
+                         "shock_server_set_tuning", "shock_server_submit", "shock_server_wait",
+                         "shock_server_result", "shock_server_get_stats", "shock_server_destroy"):
                 getattr(L, name).restype = C.c_int
+            L.shock_batch_create.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int, C.c_size_t, C.c_int,
+                                             C.POINTER(C.c_void_p)]
+            L.shock_batch_add.argtypes = [C.c_void_p, C.POINTER(Params)] + [_dp] * 8 + [C.c_int,
+                                                                                      C.POINTER(C.c_int)]
+            L.shock_server_submit.argtypes = [C.c_void_p, C.POINTER(Params)] + [_dp] * 8 + [
+                C.c_int, C.POINTER(C.c_longlong)]
+            L.shock_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_double]
+            L.shock_server_result.argtypes = [C.c_void_p, C.c_longlong, _dp, C.c_size_t, C.c_void_p]
             _lib = L
         return _lib
 
@@ -248,3 +263,194 @@ class Solver:
         if c.dim == 3:
             return a[..., g[0]:g[0] + c.ni, g[1]:g[1] + c.nj, g[2]:g[2] + c.nk]
         return a[..., g[0]:g[0] + c.ni, g[1]:g[1] + c.nj, :]
+
+
+class BatchTuning(C.Structure):
+    """Mirror of struct shock_batch_tuning (include/shock_b200.h)."""
+    _fields_ = [("persistent", C.c_int), ("blocks_per_sm", C.c_int), ("chunk", C.c_int),
+                ("small_tile_max", C.c_int), ("max_blocks_per_sm", C.c_int)]
+
+
+def member_bytes(case, precision=SHOCK_FP64) -> int:
+    """Device bytes one batch member for this case takes from a batch arena."""
+    b = C.c_size_t()
+    p = params_from_case(case, precision)
+    _check(lib().shock_batch_member_bytes(C.byref(p), C.byref(b)))
+    return b.value
+
+
+class Batch:
+    """Many periodic blocks of one class (dim, order, precision, RK order)
+    advanced together on one device (shock_batch_* in the C ABI).  Each
+    member keeps its own size, physics, tau and step count; members can be
+    added and removed between steps."""
+
+    def __init__(self, dim: int, order: int, precision=SHOCK_FP64, time_order: int = 4,
+                 arena_bytes: int = 1 << 30, device: int = 0):
+        self.lib = lib()
+        self.dim, self.order, self.precision, self.time_order = dim, order, precision, time_order
+        h = C.c_void_p()
+        _check(self.lib.shock_batch_create(dim, order, int(precision), time_order, int(arena_bytes),
+                                           int(device), C.byref(h)))
+        self.h = h
+        self.cases = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.shock_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add(self, case, nsteps: int) -> int:
+        p = params_from_case(case, self.precision)
+        f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
+        arrs = [f(a) for a in case.real_fields()]
+        m = C.c_int()
+        _check(self.lib.shock_batch_add(self.h, C.byref(p), *[_ptr(a) for a in arrs], int(nsteps),
+                                        C.byref(m)))
+        self.cases[m.value] = case
+        return m.value
+
+    def remove(self, m: int):
+        _check(self.lib.shock_batch_remove(self.h, int(m)))
+        self.cases.pop(m, None)
+
+    def step(self, n: int = 1):
+        _check(self.lib.shock_batch_step(self.h, int(n)))
+
+    def step_async(self, n: int = 1):
+        _check(self.lib.shock_batch_step_async(self.h, int(n)))
+
+    def sync(self):
+        _check(self.lib.shock_batch_sync(self.h))
+
+    def last_ms(self) -> float:
+        v = C.c_float()
+        _check(self.lib.shock_batch_last_ms(self.h, C.byref(v)))
+        return v.value
+
+    def steps_left(self, m: int) -> int:
+        v = C.c_int()
+        _check(self.lib.shock_batch_steps_left(self.h, int(m), C.byref(v)))
+        return v.value
+
+    def shape(self, m: int):
+        d = (C.c_int * 6)()
+        _check(self.lib.shock_batch_dims(self.h, int(m), d))
+        return (d[0], d[1], d[2])
+
+    def state(self, m: int) -> np.ndarray:
+        shp = self.shape(m)
+        s = np.zeros(5 * shp[0] * shp[1] * shp[2])
+        _check(self.lib.shock_batch_download_state(self.h, int(m), _ptr(s)))
+        return s.reshape((5,) + shp)
+
+    def tuning(self) -> BatchTuning:
+        t = BatchTuning()
+        _check(self.lib.shock_batch_get_tuning(self.h, C.byref(t)))
+        return t
+
+    def set_tuning(self, persistent=None, blocks_per_sm=None, chunk=None, small_tile_max=None):
+        t = self.tuning()
+        if small_tile_max is not None:
+            t.small_tile_max = int(small_tile_max)
+        if persistent is not None:
+            t.persistent = int(persistent)
+        if blocks_per_sm is not None:
+            t.blocks_per_sm = int(blocks_per_sm)
+        if chunk is not None:
+            t.chunk = int(chunk)
+        _check(self.lib.shock_batch_set_tuning(self.h, C.byref(t)))
+
+    def info(self) -> dict:
+        n, k = C.c_int(), C.c_int()
+        used, total = C.c_size_t(), C.c_size_t()
+        _check(self.lib.shock_batch_info(self.h, C.byref(n), C.byref(used), C.byref(total), C.byref(k)))
+        return {"members": n.value, "arena_used": used.value, "arena_total": total.value,
+                "kernels_per_step": k.value}
+
+
+class ServerConfig(C.Structure):
+    """Mirror of struct shock_server_config."""
+    _fields_ = [("device", C.c_int), ("hbm_budget", C.c_size_t), ("max_requests", C.c_int),
+                ("setup_threads", C.c_int), ("round_ms", C.c_double)]
+
+
+class RequestInfo(C.Structure):
+    """Mirror of struct shock_request_info."""
+    _fields_ = [("submit_s", C.c_double), ("admit_s", C.c_double), ("done_s", C.c_double),
+                ("cell_stages", C.c_double), ("status", C.c_int), ("dims", C.c_int * 6)]
+
+
+class ServerStats(C.Structure):
+    """Mirror of struct shock_server_stats."""
+    _fields_ = [("queued", C.c_longlong), ("running", C.c_longlong), ("completed", C.c_longlong),
+                ("failed", C.c_longlong), ("rounds", C.c_longlong), ("steps_launched", C.c_longlong),
+                ("cell_stages", C.c_double), ("busy_ms", C.c_double), ("arena_used", C.c_size_t),
+                ("arena_total", C.c_size_t), ("uptime_s", C.c_double), ("loop_error", C.c_int)]
+
+
+class Server:
+    """The C request loop (shock_server_*): submit solve requests as they
+    arrive; each runs on the device with continuous batching inside an HBM
+    budget and is collected with wait()/result()."""
+
+    def __init__(self, hbm_budget: int = 150 * 10 ** 9, device: int = 0, max_requests: int = 0,
+                 setup_threads: int = 0, round_ms: float = 0.0):
+        self.lib = lib()
+        cfg = ServerConfig(int(device), int(hbm_budget), int(max_requests), int(setup_threads), float(round_ms))
+        h = C.c_void_p()
+        _check(self.lib.shock_server_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        self.cases = {}
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.shock_server_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_tuning(self, dim, order, precision, time_order=4, **kw):
+        t = BatchTuning(kw.get("persistent", 1), kw.get("blocks_per_sm", 1), kw.get("chunk", 2048),
+                        kw.get("small_tile_max", 0), 0)
+        _check(self.lib.shock_server_set_tuning(self.h, int(dim), int(order), int(precision), int(time_order),
+                                                C.byref(t)))
+
+    def submit(self, case, nsteps: int, precision=SHOCK_FP64) -> int:
+        p = params_from_case(case, precision)
+        f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
+        arrs = [f(a) for a in case.real_fields()]
+        rid = C.c_longlong()
+        _check(self.lib.shock_server_submit(self.h, C.byref(p), *[_ptr(a) for a in arrs], int(nsteps),
+                                            C.byref(rid)))
+        self.cases[rid.value] = case
+        return rid.value
+
+    def wait(self, rid: int, timeout: float = 600.0):
+        _check(self.lib.shock_server_wait(self.h, C.c_longlong(rid), C.c_double(timeout)))
+
+    def result(self, rid: int):
+        """(rho,u,v,w,e ghosted, info dict) of a finished request; releases it."""
+        case = self.cases.pop(rid)
+        shp = _ghosted_shape(case)
+        out = np.zeros(5 * shp[0] * shp[1] * shp[2])
+        info = RequestInfo()
+        _check(self.lib.shock_server_result(self.h, C.c_longlong(rid), _ptr(out), out.size, C.byref(info)))
+        d = {"submit_s": info.submit_s, "admit_s": info.admit_s, "done_s": info.done_s,
+             "tts_s": info.done_s - info.submit_s, "cell_stages": info.cell_stages, "status": info.status}
+        return out.reshape((5,) + shp), d
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        _check(self.lib.shock_server_get_stats(self.h, C.byref(st)))
+        return {k: getattr(st, k) for k, _ in ServerStats._fields_}

@@ -288,3 +288,69 @@ def decaying_turbulence(n: int = 512, order: int = 9, seed: int = 3, mach_t: flo
              periodic=(True, True, True), period=(L, L, L), name=f"turb{n}_w{order}")
     c.tau = cfl_tau(c)
     return c
+
+
+def taylor_green_2d(n: int = 64, order: int = 5, mach: float = 0.1, reynolds: float = 1600.0,
+                    time_order: int = 4) -> Case:
+    """2D Taylor-Green vortex on the uniform periodic [0,2pi)^2: u = sin x cos y,
+    v = -cos x sin y, p_S = 1 + gamma Ma^2 (cos 2x + cos 2y)/4, isothermal rho."""
+    L = 2 * math.pi
+    X, Y, Z = _mesh(2, (n, n, 1), (0.0, 0.0, 0.0), (L, L, 1.0), endpoint=False)
+    gamma = 1.4
+    u = np.sin(X) * np.cos(Y)
+    v = -np.cos(X) * np.sin(Y)
+    p = 1.0 + gamma * mach ** 2 * (np.cos(2 * X) + np.cos(2 * Y)) / 4.0
+    c = Case(dim=2, order=order, ni=n, nj=n, nk=1, x=X, y=Y, z=Z, rho=p.copy(), u=u, v=v,
+             w=np.zeros_like(X), p=p, time_order=time_order, mach=mach, reynolds=reynolds, gamma=gamma,
+             periodic=(True, True, False), period=(L, L, 1.0), name=f"tgv2d{n}_w{order}")
+    c.tau = cfl_tau(c)
+    return c
+
+
+def vortex_column(n: int, nz: int, beta: float, mach_inf: float, order: int = 5, length: float = 10.0,
+                  inviscid: bool = False, reynolds: float = 1e4, time_order: int = 4) -> Case:
+    """The 2D isentropic vortex extruded along z (w = 0) on a periodic
+    [0,L)^2 x [0,L nz/n) box with n x n x nz points."""
+    v2 = isentropic_vortex(n, beta, mach_inf, order=order, length=length, inviscid=inviscid,
+                           reynolds=reynolds, time_order=time_order)
+    h = length / n
+    X, Y, Z = _mesh(3, (n, n, nz), (0.0, 0.0, 0.0), (length, length, h * nz), endpoint=False)
+    rep = lambda a: np.repeat(a[:, :, :1], nz, axis=2)
+    c = Case(dim=3, order=order, ni=n, nj=n, nk=nz, x=X, y=Y, z=Z, rho=rep(v2.rho), u=rep(v2.u),
+             v=rep(v2.v), w=np.zeros_like(X), p=rep(v2.p), time_order=time_order, mach=1.0,
+             reynolds=reynolds, gamma=v2.gamma, inviscid=inviscid, periodic=(True, True, True),
+             period=(length, length, h * nz), name=f"vcol{n}x{nz}")
+    c.tau = cfl_tau(c)
+    return c
+
+
+def serving_stream(count: int, seed: int = 5, rate: float = 200.0, min_points: int = 32 ** 2,
+                   max_points: int = 128 ** 3):
+    """Seeded solve requests for the serving workload: Poisson arrivals at
+    `rate` per second; total points log-uniform in [min_points, max_points],
+    half 2D (n x n) and half 3D (n^3); Taylor-Green or isentropic vortex;
+    Mach U[0.1, 0.6], Re U[100, 5000], WENO5 or WENO9, 20..500 steps.
+    Returns a list of (arrival time s, case, nsteps)."""
+    rng = np.random.default_rng(seed)
+    t = 0.0
+    out = []
+    for _ in range(count):
+        t += float(rng.exponential(1.0 / rate))
+        pts = math.exp(rng.uniform(math.log(min_points), math.log(max_points)))
+        dim = 2 if rng.uniform() < 0.5 else 3
+        order = 5 if rng.uniform() < 0.5 else 9
+        tgv = rng.uniform() < 0.5
+        mach = float(rng.uniform(0.1, 0.6))
+        re = float(rng.uniform(100.0, 5000.0))
+        nsteps = int(rng.integers(20, 501))
+        beta = float(rng.uniform(1.0, 5.0))
+        if dim == 2:
+            n = max(order + 3, int(round(math.sqrt(pts))))
+            case = taylor_green_2d(n, order, mach, re) if tgv else \
+                isentropic_vortex(n, beta, mach, order=order, inviscid=False, reynolds=re)
+        else:
+            n = max(order + 3, int(round(pts ** (1.0 / 3.0))))
+            case = taylor_green(n, order, mach, re, perturb=0.0) if tgv else \
+                vortex_column(n, n, beta, mach, order=order, reynolds=re)
+        out.append((t, case, nsteps))
+    return out

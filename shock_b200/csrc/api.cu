@@ -78,17 +78,43 @@ struct shock_ctx {
     std::vector<std::vector<double>> geo_host;
 };
 
-static void set_rk(shock_ctx *c)
+namespace shock {
+
+// RK coefficients of src/Functions.c:1961-2009 (a, b, c, d and the Q_sum
+// factor s of each stage).
+void rk_coefficients(int time_order, RKCoef out[4])
 {
-    if (c->p.time_order == 4) {
+    if (time_order == 4) {
         const double a[4] = {1., 1., 1., 1.}, b[4] = {0., 0., 0., 0.}, q[4] = {0.5, 0.5, 1., 1. / 6.};
         const double d[4] = {0., 0., 0., 1. / 6.}, s[4] = {1., 2., 2., 0.};
-        for (int i = 0; i < 4; i++) c->rk[i] = RKCoef{a[i], b[i], q[i], d[i], s[i]};
+        for (int i = 0; i < 4; i++) out[i] = RKCoef{a[i], b[i], q[i], d[i], s[i]};
     } else {
         const double a[3] = {1., 3. / 4., 1. / 3.}, b[3] = {0., 1. / 4., 2. / 3.}, q[3] = {1., 1. / 4., 2. / 3.};
-        for (int i = 0; i < 3; i++) c->rk[i] = RKCoef{a[i], b[i], q[i], 0., 0.};
+        for (int i = 0; i < 3; i++) out[i] = RKCoef{a[i], b[i], q[i], 0., 0.};
+        out[3] = RKCoef{0., 0., 0., 0., 0.};
     }
 }
+
+// Non-dimensional constants of the path (src/Functions.c:1758-2032).
+Phys make_phys(const shock_params &p)
+{
+    Phys P{};
+    P.gamma = p.gamma;
+    P.igm1 = 1.0 / (p.gamma - 1.0);
+    P.ups = 1.0 / (p.gamma * (p.mach * p.mach));
+    P.psi = 1.0 / p.reynolds;
+    P.suth = 100.4 / p.t0;
+    P.gam = 1.0 / ((p.gamma - 1.0) * (p.mach * p.mach) * p.reynolds * p.prandtl);
+    P.eps64 = 10. * sqrt(2.2250738585072014e-308);   // 10*sqrt(DBL_MIN), src/Functions.c:1829
+    P.eps32 = 10.f * sqrtf(1.17549435e-38f);          // 10*sqrt(FLT_MIN), the float build's value
+    P.mms = p.mms ? 1 : 0;
+    P.zeta_fix = p.zeta_fix;
+    return P;
+}
+
+}  // namespace shock
+
+static void set_rk(shock_ctx *c) { rk_coefficients(c->p.time_order, c->rk); }
 
 // Launch the right-hand side of one stage on state `in`.
 static void enqueue_rhs(shock_ctx *c, double *const in[5], int &nk)
@@ -176,24 +202,9 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
     HostBlock hb;
     build_block(*p, x, y, z, u, v, w, pr, rho, hb);
     c->L = hb.L;
+    c->G = make_grid(c->L, *p);
     Grid &G = c->G;
-    G.dim = p->dim; G.order = p->order; G.g = c->L.g;
-    for (int a = 0; a < 3; a++) {
-        G.n[a] = c->L.n[a]; G.N[a] = c->L.N[a]; G.st[a] = c->L.st[a];
-        G.periodic[a] = a < p->dim ? p->periodic[a] : 0;
-    }
-    G.NG = c->L.NG;
-    Phys &P = c->P;
-    P.gamma = p->gamma;
-    P.igm1 = 1.0 / (p->gamma - 1.0);
-    P.ups = 1.0 / (p->gamma * (p->mach * p->mach));
-    P.psi = 1.0 / p->reynolds;
-    P.suth = 100.4 / p->t0;
-    P.gam = 1.0 / ((p->gamma - 1.0) * (p->mach * p->mach) * p->reynolds * p->prandtl);
-    P.eps64 = 10. * sqrt(2.2250738585072014e-308);   // 10*sqrt(DBL_MIN), src/Functions.c:1829
-    P.eps32 = 10.f * sqrtf(1.17549435e-38f);          // 10*sqrt(FLT_MIN), the float build's value
-    P.mms = p->mms ? 1 : 0;
-    P.zeta_fix = p->zeta_fix;
+    c->P = make_phys(*p);
     set_rk(c);
 
     if (cudaSetDevice(device) != cudaSuccess) { delete c; return fail(SHOCK_ECUDA, "cudaSetDevice(%d)", device); }

@@ -74,6 +74,90 @@ struct RKCoef {
     double a, b, c, d, s;
 };
 
+// ---------------------------------------------------------------------------
+// Batched execution: many blocks (members) advanced by the same kernels.
+// ---------------------------------------------------------------------------
+constexpr int TL_HOST = 15;     // cells per sweep tile along the sweep (stage_bodies.cuh: TL)
+constexpr int TILE_SHORT = 7;   // the short sweep tile of batched members (one face per thread)
+constexpr int NTHR_HOST = 256;  // threads per sweep tile (stage_bodies.cuh: NTHR)
+
+enum BatchPhase {
+    PH_GHOST = 0, PH_PRIM, PH_NODAL, PH_WENO0, PH_WENO1, PH_WENO2, PH_VISC0, PH_VISC1, PH_VISC2, PH_RK,
+    NPHASE
+};
+
+struct Member {            // one block of a batch (device copy; host keeps the same struct)
+    Grid G;
+    Phys P;
+    Fields F;              // Q, Q_sum, p, T, c, mu, J, metric, nodal derivatives of this block
+    double *buf[3][5];     // three rotating rho,u,v,w,e buffers
+    double tau;
+    int inviscid;
+    int un;                // buffer holding U_lastStep; advanced on the device after each step
+    int steps_left;        // steps still to run; 0 = frozen (its items are skipped)
+    int tile;              // sweep tile length along the sweep: TL_HOST or TILE_SHORT cells
+};
+
+struct BatchItem {         // one unit of work: a sweep tile (a,b,c) or a chunk a of points
+    int m, a, b, c;
+};
+
+struct BatchPlan {         // device-resident: where each phase's items start
+    int off[NPHASE + 1];
+    int chunk;             // points per elementwise item
+    int nmember;
+};
+
+struct BatchSync {         // device counters; zeroed by the step's last kernel
+    unsigned next[4][NPHASE];   // dynamic item counters (stage, phase)
+    unsigned bar[4];            // grid-barrier arrivals per stage
+    unsigned err;               // 1: a barrier wait ran out (sticky until the host clears it)
+    unsigned pad[3];
+};
+
+struct BatchLaunch {       // launch configuration chosen by the tuner
+    int persistent;        // 1: one launch per stage with grid barriers; 0: one launch per phase
+    int blocks_per_sm;
+    int sms;
+};
+
+// Device views of a block described by p with layout L (host helpers).
+inline Grid make_grid(const Layout &L, const shock_params &p)
+{
+    Grid G{};
+    G.dim = p.dim; G.order = p.order; G.g = L.g;
+    for (int a = 0; a < 3; a++) {
+        G.n[a] = L.n[a]; G.N[a] = L.N[a]; G.st[a] = L.st[a];
+        G.periodic[a] = a < p.dim ? p.periodic[a] : 0;
+    }
+    G.NG = L.NG;
+    return G;
+}
+
+Phys make_phys(const shock_params &p);            // api.cu
+void rk_coefficients(int time_order, RKCoef out[4]);   // api.cu
+
+// Device arena shared by batches (batch.cu) and the batch entry points the
+// serving loop uses (serve.cu).
+struct DeviceArena;
+DeviceArena *arena_create(int device, size_t bytes);   // nullptr if the allocation fails
+void arena_destroy(DeviceArena *a);
+size_t arena_used(DeviceArena *a);
+size_t arena_total(DeviceArena *a);
+int batch_create_in(int dim, int order, int precision, int time_order, DeviceArena *arena, int device,
+                    shock_batch **out);
+int batch_add_block(shock_batch *b, const shock_params &p, const HostBlock &hb, int nsteps, int *member);
+
+// Batched launchers (batch_kernels.cu).
+int batch_smem_bytes(int dim, int order, int precision);
+int batch_max_blocks_per_sm(int dim, int order, int precision, int persistent);
+void batch_prepare_kernels();
+cudaError_t launch_batch_stage(int dim, int order, int precision, const BatchLaunch &L, const Member *mem,
+                               const BatchItem *items, const BatchPlan *plan, BatchSync *sync, int stage,
+                               const RKCoef &K, const int *phase_has_items, cudaStream_t s);
+void launch_batch_advance(Member *mem, const BatchPlan *plan, int capacity, int time_order, BatchSync *sync,
+                          cudaStream_t s);
+
 // Kernel launchers (stage_kernels.cu).
 void launch_ghosts(const Grid &G, double *const U[5], cudaStream_t s);
 void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s);

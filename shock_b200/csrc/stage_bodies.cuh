@@ -1,0 +1,1057 @@
+// Device bodies of the stage kernels, shared by the single-block kernels
+// (stage_kernels.cu) and the batched kernels (batch_kernels.cu).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <type_traits>
+
+#include "internal.h"
+
+namespace shock {
+
+// ---------------------------------------------------------------------------
+// small helpers
+// ---------------------------------------------------------------------------
+struct Idx3 {
+    int v[3];
+};
+
+__device__ __forceinline__ Idx3 unflatten(const Grid &G, long long o)
+{
+    Idx3 r;
+    r.v[0] = (int)(o / G.st[0]);
+    long long rem = o - (long long)r.v[0] * G.st[0];
+    r.v[1] = (int)(rem / G.st[1]);
+    r.v[2] = (int)(rem - (long long)r.v[1] * G.st[1]);
+    return r;
+}
+
+__device__ __forceinline__ bool is_real(const Grid &G, int a, int i) { return i >= G.g && i < G.g + G.n[a]; }
+
+// ---------------------------------------------------------------------------
+// ghosts: periodic images over the ghost shell (all periodic axes at once;
+// equivalent to SHOCK's repeated slab exchange).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ void ghost_body(const Grid &G, long long o, double *r, double *u, double *v, double *w,
+                                           double *e)
+{
+    Idx3 p = unflatten(G, o);
+    Idx3 s = p;
+    bool ghost = false;
+    for (int a = 0; a < G.dim; a++) {
+        if (!G.periodic[a]) continue;
+        int i = p.v[a];
+        if (i < G.g) { s.v[a] = i + G.n[a]; ghost = true; }
+        else if (i >= G.g + G.n[a]) { s.v[a] = i - G.n[a]; ghost = true; }
+    }
+    if (!ghost) return;
+    long long q = s.v[0] * G.st[0] + s.v[1] * G.st[1] + s.v[2];
+    r[o] = r[q];
+    u[o] = u[q];
+    v[o] = v[q];
+    w[o] = w[q];
+    e[o] = e[q];
+}
+
+// ---------------------------------------------------------------------------
+// prim: CalcValues (p with fabs, T = |p/rho|, c, Sutherland mu or mu = 1).
+// ---------------------------------------------------------------------------
+template <int DIM>
+__device__ __forceinline__ void prim_body(const Grid &G, const Phys &P, long long o, const double *__restrict__ R,
+                                          const double *__restrict__ U, const double *__restrict__ V,
+                                          const double *__restrict__ W, const double *__restrict__ E, double *p,
+                                          double *T, double *c, double *mu)
+{
+    (void)G;
+    double rho = R[o], u = U[o], v = V[o], e = E[o];
+    double q2 = (u * u) + (v * v);
+    if (DIM == 3) {
+        double w = W[o];
+        q2 = q2 + (w * w);
+    }
+    double pp = fabs(rho * (P.gamma - 1.0) / P.ups * (e - 0.5 * q2));
+    double pr = pp / rho;
+    p[o] = pp;
+    T[o] = fabs(pr);
+    c[o] = sqrt(P.ups * P.gamma * pp / rho);
+    mu[o] = P.mms ? 1.0 : ((1.0 + P.suth) * pow(pr, 1.5) / (pr + P.suth));
+}
+
+// ---------------------------------------------------------------------------
+// nodal derivatives (6th / 10th order central, src/Functions.c:1936-1942 /
+// :1884-1894), each direction on the points that are real along it.
+// 3D needs u,v,w; 2D u,v,T (its metric has cross terms).
+// ---------------------------------------------------------------------------
+template <int ORDER>
+struct ZD;
+template <>
+struct ZD<5> {
+    static constexpr int H = 3;
+    __device__ static double node(int l)
+    {
+        const double c[7] = {-1. / 60., 3. / 20., -3. / 4., 0., 3. / 4., -3. / 20., 1. / 60.};
+        return c[l];
+    }
+    __device__ static double half(int l)
+    {
+        const double c[6] = {-1. / 90., 25. / 180., -245. / 180., 245. / 180., -25. / 180., 1. / 90.};
+        return c[l];
+    }
+    __device__ static double interp(int l)
+    {
+        const double c[6] = {1. / 60., -8. / 60., 37. / 60., 37. / 60., -8. / 60., 1. / 60.};
+        return c[l];
+    }
+};
+template <>
+struct ZD<9> {
+    static constexpr int H = 5;
+    __device__ static double node(int l)
+    {
+        const double c[11] = {-1. / 1260., 25. / 2520., -150. / 2520., 600. / 2520., -2100. / 2520., 0.,
+                              2100. / 2520., -600. / 2520., 150. / 2520., -25. / 2520., 1. / 1260.};
+        return c[l];
+    }
+    __device__ static double half(int l)
+    {
+        const double c[10] = {-3. / 9450., 351. / 75600., -2649. / 75600., 15351. / 75600., -110649. / 75600.,
+                              110649. / 75600., -15351. / 75600., 2649. / 75600., -351. / 75600., 3. / 9450.};
+        return c[l];
+    }
+    __device__ static double interp(int l)
+    {
+        const double c[10] = {1. / 1260., -23. / 2520., 127. / 2520., -473. / 2520., 1627. / 2520.,
+                              1627. / 2520., -473. / 2520., 127. / 2520., -23. / 2520., 1. / 1260.};
+        return c[l];
+    }
+};
+
+template <int DIM, int ORDER>
+__device__ __forceinline__ void nodal_body(const Grid &G, long long o, const double *__restrict__ U,
+                                           const double *__restrict__ V, const double *__restrict__ W,
+                                           const double *__restrict__ T, const Fields &F)
+{
+    constexpr int H = ZD<ORDER>::H;
+    Idx3 p = unflatten(G, o);
+    const double *var[4] = {U, V, W, T};
+#pragma unroll
+    for (int d = 0; d < DIM; d++) {
+        if (!is_real(G, d, p.v[d])) continue;
+        long long sd = G.st[d];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            if (DIM == 3 && q == 3) continue;   // T derivatives unused with the diagonal 3D metric
+            if (DIM == 2 && q == 2) continue;   // no w in 2D
+            double acc = 0.0;
+#pragma unroll
+            for (int l = 0; l <= 2 * H; l++) acc += ZD<ORDER>::node(l) * var[q][o + (l - H) * sd];
+            F.Nd[3 * q + d][o] = acc;
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// WENO reconstruction weights (src/WENO.c:11-204).
+// ---------------------------------------------------------------------------
+template <typename T>
+__device__ __forceinline__ T phi_w5(const T *d, T eps)
+{
+    T is0 = T(13.) * (d[0] - d[1]) * (d[0] - d[1]) + T(3.) * (d[0] - T(3.) * d[1]) * (d[0] - T(3.) * d[1]);
+    T is1 = T(13.) * (d[1] - d[2]) * (d[1] - d[2]) + T(3.) * (d[1] + d[2]) * (d[1] + d[2]);
+    T is2 = T(13.) * (d[2] - d[3]) * (d[2] - d[3]) + T(3.) * (T(3.) * d[2] - d[3]) * (T(3.) * d[2] - d[3]);
+    T a0 = (is0 + eps) * (is0 + eps), a1 = (is1 + eps) * (is1 + eps), a2 = (is2 + eps) * (is2 + eps);
+    T o0t = T(1.) / a0, o1t = T(6.) * (T(1.) / a1), o2t = T(3.) * (T(1.) / a2);
+    T rs = T(1.) / (o0t + o1t + o2t);
+    T o0 = o0t * rs, o2 = o2t * rs;
+    T q1 = d[0] - T(2.) * d[1] + d[2];
+    T q2 = d[1] - T(2.) * d[2] + d[3];
+    return T(1. / 3.) * o0 * q1 + T(1. / 6.) * (o2 - T(0.5)) * q2;
+}
+
+// WENO9 smoothness-indicator quadratic forms (src/WENO.c:25-53), stored
+// as the upper triangle per sub-stencil.
+static __constant__ double c_w9is[5][15] = {
+    {22658., -208501., 364863., -288007., 86329., 482963., -1704396., 1358458., -411487., 1521393., -2462076., 758823., 1020563., -649501., 107918.},
+    {6908., -60871., 99213., -70237., 18079., 138563., -464976., 337018., -88297., 406293., -611976., 165153., 242723., -140251., 22658.},
+    {6908., -51001., 67923., -38947., 8209., 104963., -299076., 179098., -38947., 231153., -299076., 67923., 104963., -51001., 6908.},
+    {22658., -140251., 165153., -88297., 18079., 242723., -611976., 337018., -70237., 406293., -464976., 99213., 138563., -60871., 6908.},
+    {107918., -649501., 758823., -411487., 86329., 1020563., -2462076., 1358458., -288007., 1521393., -1704396., 364863., 482963., -208501., 22658.},
+};
+static __constant__ float c_w9is_f[5][15] = {
+    {22658.f, -208501.f, 364863.f, -288007.f, 86329.f, 482963.f, -1704396.f, 1358458.f, -411487.f, 1521393.f, -2462076.f, 758823.f, 1020563.f, -649501.f, 107918.f},
+    {6908.f, -60871.f, 99213.f, -70237.f, 18079.f, 138563.f, -464976.f, 337018.f, -88297.f, 406293.f, -611976.f, 165153.f, 242723.f, -140251.f, 22658.f},
+    {6908.f, -51001.f, 67923.f, -38947.f, 8209.f, 104963.f, -299076.f, 179098.f, -38947.f, 231153.f, -299076.f, 67923.f, 104963.f, -51001.f, 6908.f},
+    {22658.f, -140251.f, 165153.f, -88297.f, 18079.f, 242723.f, -611976.f, 337018.f, -70237.f, 406293.f, -464976.f, 99213.f, 138563.f, -60871.f, 6908.f},
+    {107918.f, -649501.f, 758823.f, -411487.f, 86329.f, 1020563.f, -2462076.f, 1358458.f, -288007.f, 1521393.f, -1704396.f, 364863.f, 482963.f, -208501.f, 22658.f},
+};
+
+template <typename T>
+__device__ __forceinline__ T w9c(int k, int i);
+template <>
+__device__ __forceinline__ double w9c<double>(int k, int i) { return c_w9is[k][i]; }
+template <>
+__device__ __forceinline__ float w9c<float>(int k, int i) { return c_w9is_f[k][i]; }
+
+// f: 9 stencil values, d: 8 differences.
+template <typename T>
+__device__ __forceinline__ T phi_w9(const T *f, const T *d, T eps)
+{
+    const T dk[5] = {T(1. / 126.), T(10. / 63.), T(10. / 21.), T(20. / 63.), T(5. / 126.)};
+    T ot[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        T acc = T(0);
+        int c = 0;
+#pragma unroll
+        for (int a = 0; a < 5; a++) {
+            T in = w9c<T>(k, c++) * f[k + a];
+#pragma unroll
+            for (int b = a + 1; b < 5; b++) in = in + w9c<T>(k, c++) * f[k + b];
+            acc = (a == 0) ? f[k] * in : acc + f[k + a] * in;
+        }
+        T t = acc + eps;
+        ot[k] = dk[k] * (T(1.) / (t * t));
+    }
+    T rs = T(1.) / (ot[0] + ot[1] + ot[2] + ot[3] + ot[4]);
+    T o0 = ot[0] * rs, o2 = ot[2] * rs, o3 = ot[3] * rs, o4 = ot[4] * rs;
+    T q1 = d[0] - T(4.) * d[1] + T(6.) * d[2] - T(4.) * d[3] + d[4];
+    T q2 = d[1] - T(4.) * d[2] + T(6.) * d[3] - T(4.) * d[4] + d[5];
+    T q3 = d[2] - T(4.) * d[3] + T(6.) * d[4] - T(4.) * d[5] + d[6];
+    T q4 = d[3] - T(4.) * d[4] + T(6.) * d[5] - T(4.) * d[6] + d[7];
+    return T(1. / 5.) * o0 * q1 + T(1. / 20.) * o2 * q2 + T(1. / 60.) * o3 * (T(3.) * q2 - T(2.) * q3)
+           + T(1. / 60.) * o4 * (T(3.) * q2 - T(2.) * q3 + T(3.) * q4)
+           - T(1. / 840.) * (T(39.) * q2 - T(14.) * q3 + T(3.) * q4);
+}
+
+// ---------------------------------------------------------------------------
+// Sweep geometry: sweep axis D, lateral axis (32 lines, the fastest
+// non-sweep axis), other axis (3D).
+// ---------------------------------------------------------------------------
+template <int DIM, int D>
+struct Axes {
+    static constexpr int LAT = (D != DIM - 1) ? DIM - 1 : DIM - 2;
+    static constexpr int OTH = (DIM == 3) ? (3 - D - LAT) : 2;
+    static constexpr bool CONTIG = (D == DIM - 1);   // sweep along the contiguous axis
+};
+
+constexpr int TL = 15;         // cells per tile along the sweep
+constexpr int NFACE = TL + 1;  // faces per tile line
+constexpr int NLANE = 32;      // lines per tile
+constexpr int NROWT = 8;       // thread rows; each handles faces row and row + 8
+constexpr int NTHR = NLANE * NROWT;
+static_assert(TL == TL_HOST && NTHR == NTHR_HOST, "host copies of the tile constants");
+
+// Per-point values staged for the WENO face computation.
+enum { WF0 = 0, WU0 = 5, WVU = 10, WVV, WVW, WC, WLAM, WJ, WN0 };
+
+template <int DIM>
+struct WenoNV {
+    static constexpr int NN = DIM == 3 ? 1 : 2;   // stored components of the unit normal
+    static constexpr int NV = WN0 + NN;
+};
+
+struct Tile {
+    int c0, l0, nD, nL;
+    long long sD, sL, base;
+    bool lane_ok;
+};
+
+template <int DIM, int D, int TLN = TL>
+__device__ __forceinline__ Tile make_tile(const Grid &G, int lane, int bx, int by, int bz)
+{
+    using A = Axes<DIM, D>;
+    Tile t;
+    t.c0 = G.g + bx * TLN;
+    t.l0 = G.g + by * NLANE;
+    const int oth = (DIM == 3) ? G.g + bz : 0;
+    t.nD = G.n[D];
+    t.nL = G.n[A::LAT];
+    t.sD = G.st[D];
+    t.sL = G.st[A::LAT];
+    const long long sO = (DIM == 3) ? G.st[A::OTH] : 0;
+    t.base = (long long)t.l0 * t.sL + (long long)oth * sO;
+    t.lane_ok = (t.l0 + lane) < G.g + t.nL;
+    return t;
+}
+
+// Stage point fluxes, conserved variables, face-state inputs and the local
+// spectral radius of NP points per lane: points c0-1-r .. c0+TLN+r.
+template <int DIM, int ORDER, int D, int TLN = TL>
+__device__ __forceinline__ void stage_weno(const Grid &G, const Phys &P, const Tile &T, double *sh,
+                                           const double *__restrict__ R, const double *__restrict__ Uu,
+                                           const double *__restrict__ Vv, const double *__restrict__ Ww,
+                                           const double *__restrict__ Ee, const Fields &F)
+{
+    using A = Axes<DIM, D>;
+    constexpr int r = (ORDER - 1) / 2;
+    constexpr int NP = TLN + 2 * r + 2;
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+    const int tid = threadIdx.y * NLANE + threadIdx.x;
+    for (int it = tid; it < NP * NLANE; it += NTHR) {
+        // lane-fastest: conflict-free shared-memory stores; along a
+        // contiguous axis the 32 lines are 32 strided rows whose sectors the
+        // following points of the loop reuse from L1
+        const int l = it % NLANE, t = it / NLANE;
+        int pd = T.c0 - 1 - r + t;
+        if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
+        long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
+        double rho = R[o], u = Uu[o], v = Vv[o], w = (DIM == 3) ? Ww[o] : 0.0, e = Ee[o];
+        double p = F.p[o], c = F.c[o], J = F.J[o];
+        double mx, my, mz, th, nrm;
+        if (DIM == 3) {
+            double mm = F.m[3 * D + D][o];
+            mx = D == 0 ? mm : 0.0;
+            my = D == 1 ? mm : 0.0;
+            mz = D == 2 ? mm : 0.0;
+            th = (D == 0 ? u : D == 1 ? v : w) * mm;
+            nrm = fabs(mm);
+        } else {
+            mx = F.m[3 * D + 0][o];
+            my = F.m[3 * D + 1][o];
+            mz = 0.0;
+            th = u * mx + v * my;
+            nrm = sqrt(mx * mx + my * my);
+        }
+        double rt = rho * th;
+        SH(WF0 + 0, t, l) = J * rt;
+        SH(WF0 + 1, t, l) = J * (rt * u + mx * p * P.ups);
+        SH(WF0 + 2, t, l) = J * (rt * v + my * p * P.ups);
+        SH(WF0 + 3, t, l) = J * (rt * w + mz * p * P.ups);
+        SH(WF0 + 4, t, l) = J * (rt * (e + p / rho * P.ups));
+        SH(WU0 + 0, t, l) = rho;
+        SH(WU0 + 1, t, l) = rho * u;
+        SH(WU0 + 2, t, l) = rho * v;
+        SH(WU0 + 3, t, l) = rho * w;
+        SH(WU0 + 4, t, l) = rho * e;
+        SH(WVU, t, l) = u;
+        SH(WVV, t, l) = v;
+        SH(WVW, t, l) = w;
+        SH(WC, t, l) = c;
+        SH(WLAM, t, l) = fabs(th) + c * nrm;
+        SH(WJ, t, l) = J;
+        if (DIM == 3) {
+            SH(WN0, t, l) = (D == 0 ? mx : D == 1 ? my : mz) / nrm;
+        } else {
+            SH(WN0, t, l) = mx / nrm;
+            SH(WN0 + 1, t, l) = my / nrm;
+        }
+    }
+#undef SH
+}
+
+// Face state (arithmetic means, src/WENO.c:1104-1139) and derived scalars.
+template <typename T>
+struct FaceState {
+    T u, v, w, rho, c, nx, ny, nz, q2, un, gc, irho, isc, kin, gm, ic, g1c, hc;
+};
+
+template <int DIM, int ORDER, int D, typename T, int TLN = TL>
+__device__ __forceinline__ FaceState<T> face_state(const Phys &P, const double *sh, int ta, int lane)
+{
+    constexpr int r = (ORDER - 1) / 2;
+    constexpr int NP = TLN + 2 * r + 2;
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+    FaceState<T> s;
+    s.gm = (T)P.gamma;
+    s.u = T(0.5) * (T)(SH(WVU, ta, lane) + SH(WVU, ta + 1, lane));
+    s.v = T(0.5) * (T)(SH(WVV, ta, lane) + SH(WVV, ta + 1, lane));
+    s.w = T(0.5) * (T)(SH(WVW, ta, lane) + SH(WVW, ta + 1, lane));
+    s.rho = T(0.5) * (T)(SH(WU0, ta, lane) + SH(WU0, ta + 1, lane));
+    s.c = T(0.5) * (T)(SH(WC, ta, lane) + SH(WC, ta + 1, lane));
+    if (DIM == 3) {
+        T nd = T(0.5) * (T)(SH(WN0, ta, lane) + SH(WN0, ta + 1, lane));
+        s.nx = D == 0 ? nd : T(0);
+        s.ny = D == 1 ? nd : T(0);
+        s.nz = D == 2 ? nd : T(0);
+    } else {
+        s.nx = T(0.5) * (T)(SH(WN0, ta, lane) + SH(WN0, ta + 1, lane));
+        s.ny = T(0.5) * (T)(SH(WN0 + 1, ta, lane) + SH(WN0 + 1, ta + 1, lane));
+        s.nz = T(0);
+    }
+#undef SH
+    s.q2 = s.u * s.u + s.v * s.v + s.w * s.w;
+    s.ic = T(1) / s.c;
+    const T ic2 = s.ic * s.ic;
+    s.un = s.u * s.nx + s.v * s.ny + s.w * s.nz;
+    s.gc = (s.gm - T(1)) * ic2;
+    s.g1c = (s.gm - T(1)) * s.ic;                        // (gamma-1)/c
+    s.irho = T(1) / s.rho;
+    s.isc = s.ic * T(0.70710678118654752440);            // 1/(c sqrt 2)
+    s.kin = T(1) - T(0.5) * (s.gm - T(1)) * (s.q2 * ic2);
+    s.hc = s.q2 / T(2) + s.c * s.c * (T)P.igm1;          // q^2/2 + c^2/(gamma-1)
+    return s;
+}
+
+// Row ch of the left eigenvector matrix (src/WENO.c:1202-1236).
+template <typename T>
+__device__ __forceinline__ void left_row(const FaceState<T> &s, int ch, T &L0, T &L1, T &L2, T &L3, T &L4)
+{
+    const T isq2 = T(0.70710678118654752440), g1 = s.gm - T(1);
+    switch (ch) {
+    case 0:
+        L0 = s.nx * s.kin - s.irho * (s.v * s.nz - s.w * s.ny); L1 = s.gc * s.u * s.nx;
+        L2 = s.gc * s.v * s.nx + s.nz * s.irho; L3 = s.gc * s.w * s.nx - s.ny * s.irho; L4 = -s.gc * s.nx; break;
+    case 1:
+        L0 = s.ny * s.kin - s.irho * (s.w * s.nx - s.u * s.nz); L1 = s.gc * s.u * s.ny - s.nz * s.irho;
+        L2 = s.gc * s.v * s.ny; L3 = s.gc * s.w * s.ny + s.nx * s.irho; L4 = -s.gc * s.ny; break;
+    case 2:
+        L0 = s.nz * s.kin - s.irho * (s.u * s.ny - s.v * s.nx); L1 = s.gc * s.u * s.nz + s.ny * s.irho;
+        L2 = s.gc * s.v * s.nz - s.nx * s.irho; L3 = s.gc * s.w * s.nz; L4 = -s.gc * s.nz; break;
+    case 3:
+        L0 = s.isc * (g1 * s.q2 / T(2) - s.c * s.un); L1 = (-s.g1c * s.u + s.nx) * isq2;
+        L2 = (-s.g1c * s.v + s.ny) * isq2; L3 = (-s.g1c * s.w + s.nz) * isq2; L4 = g1 * s.isc; break;
+    default:
+        L0 = s.isc * (g1 * s.q2 / T(2) + s.c * s.un); L1 = (-s.g1c * s.u - s.nx) * isq2;
+        L2 = (-s.g1c * s.v - s.ny) * isq2; L3 = (-s.g1c * s.w - s.nz) * isq2; L4 = g1 * s.isc; break;
+    }
+}
+
+// out += (column ch of the right eigenvector matrix) * phi (src/WENO.c:1176-1200).
+template <typename T>
+__device__ __forceinline__ void add_right_col(const FaceState<T> &s, int ch, T phi, T *out)
+{
+    switch (ch) {
+    case 0:
+        out[0] += s.nx * phi; out[1] += s.u * s.nx * phi; out[2] += (s.v * s.nx + s.rho * s.nz) * phi;
+        out[3] += (s.w * s.nx - s.rho * s.ny) * phi;
+        out[4] += (s.q2 / T(2) * s.nx + s.rho * (s.v * s.nz - s.w * s.ny)) * phi; break;
+    case 1:
+        out[0] += s.ny * phi; out[1] += (s.u * s.ny - s.rho * s.nz) * phi; out[2] += s.v * s.ny * phi;
+        out[3] += (s.w * s.ny + s.rho * s.nx) * phi;
+        out[4] += (s.q2 / T(2) * s.ny + s.rho * (s.w * s.nx - s.u * s.nz)) * phi; break;
+    case 2:
+        out[0] += s.nz * phi; out[1] += (s.u * s.nz + s.rho * s.ny) * phi; out[2] += (s.v * s.nz - s.rho * s.nx) * phi;
+        out[3] += s.w * s.nz * phi;
+        out[4] += (s.q2 / T(2) * s.nz + s.rho * (s.u * s.ny - s.v * s.nx)) * phi; break;
+    case 3: {
+        T sc = s.isc * phi;
+        out[0] += sc; out[1] += (s.u + s.nx * s.c) * sc; out[2] += (s.v + s.ny * s.c) * sc;
+        out[3] += (s.w + s.nz * s.c) * sc; out[4] += (s.hc + s.c * s.un) * sc; break;
+    }
+    default: {
+        T sc = s.isc * phi;
+        out[0] += sc; out[1] += (s.u - s.nx * s.c) * sc; out[2] += (s.v - s.ny * s.c) * sc;
+        out[3] += (s.w - s.nz * s.c) * sc; out[4] += (s.hc - s.c * s.un) * sc; break;
+    }
+    }
+}
+
+// WENO part of the face flux in FP64 (src/WENO.c:296-430): split fluxes
+// F +/- lambda J_{i+1/2} U projected on the characteristic fields, Phi+,
+// Phi-, back-projection.  f: face index in the tile (points f..f+2r+1).
+template <int DIM, int ORDER, int D, int TLN = TL>
+__device__ __forceinline__ void face_weno_fp64(const Phys &P, const double *sh, int f, int lane, double *out)
+{
+    constexpr int r = (ORDER - 1) / 2;
+    constexpr int NP = TLN + 2 * r + 2;
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+    const int ta = r + f;
+    const FaceState<double> s = face_state<DIM, ORDER, D, double, TLN>(P, sh, ta, lane);
+    const double jh = (SH(WJ, ta, lane) + SH(WJ, ta + 1, lane)) / 2.0;
+    double lam = 0.0;
+#pragma unroll
+    for (int q = 0; q <= 2 * r + 1; q++) {
+        double lm = SH(WLAM, f + q, lane);
+        lam = lam < lm ? lm : lam;
+    }
+    const double a = lam * jh;
+#pragma unroll
+    for (int q = 0; q < 5; q++) out[q] = 0.0;
+#pragma unroll 1
+    for (int ch = 0; ch < 5; ch++) {
+        // reload the window from shared memory in every iteration instead of
+        // holding 2r+2 points x 10 values in registers (keeps two tiles per SM)
+        asm volatile("" ::: "memory");
+        double L0, L1, L2, L3, L4;
+        left_row<double>(s, ch, L0, L1, L2, L3, L4);
+        double Pp[2 * r + 2], Pm[2 * r + 2];
+#pragma unroll
+        for (int q = 0; q <= 2 * r + 1; q++) {
+            int t = f + q;
+            asm volatile("" ::: "memory");   // issue this point's loads here, not all up front
+            double lf = L0 * SH(WF0 + 0, t, lane) + L1 * SH(WF0 + 1, t, lane) + L2 * SH(WF0 + 2, t, lane)
+                        + L3 * SH(WF0 + 3, t, lane) + L4 * SH(WF0 + 4, t, lane);
+            double lu = L0 * SH(WU0 + 0, t, lane) + L1 * SH(WU0 + 1, t, lane) + L2 * SH(WU0 + 2, t, lane)
+                        + L3 * SH(WU0 + 3, t, lane) + L4 * SH(WU0 + 4, t, lane);
+            Pp[q] = 0.5 * (lf + a * lu);
+            Pm[q] = 0.5 * (lf - a * lu);
+        }
+        double phi;
+        if (ORDER == 5) {
+            double dp[4], dm[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) {
+                dp[q] = Pp[q + 1] - Pp[q];
+                dm[q] = Pm[2 * r + 1 - q] - Pm[2 * r - q];
+            }
+            phi = -phi_w5<double>(dp, P.eps64) + phi_w5<double>(dm, P.eps64);
+        } else {
+            double fp[9], fm[9], dp[8], dm[8];
+#pragma unroll
+            for (int q = 0; q < 9; q++) { fp[q] = Pp[q]; fm[q] = Pm[2 * r + 1 - q]; }
+#pragma unroll
+            for (int q = 0; q < 8; q++) { dp[q] = fp[q + 1] - fp[q]; dm[q] = fm[q] - fm[q + 1]; }
+            phi = -phi_w9<double>(fp, dp, P.eps64) + phi_w9<double>(fm, dm, P.eps64);
+        }
+        add_right_col<double>(s, ch, phi, out);
+    }
+#undef SH
+}
+
+// Mixed form of the same: the projection, indicators, weights and
+// back-projection in FP32 on FP64-formed point-to-point differences dl.
+template <int DIM, int ORDER, int D, int TLN = TL>
+__device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh, const float *dl, int f, int lane,
+                                                double *outd)
+{
+    constexpr int r = (ORDER - 1) / 2;
+    constexpr int NP = TLN + 2 * r + 2;
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+#define DL(v, t, l) dl[((v) * (NP - 1) + (t)) * NLANE + (l)]
+    const int ta = r + f;
+    const FaceState<float> s = face_state<DIM, ORDER, D, float, TLN>(P, sh, ta, lane);
+    const double jh = (SH(WJ, ta, lane) + SH(WJ, ta + 1, lane)) / 2.0;
+    double lam = 0.0;
+#pragma unroll
+    for (int q = 0; q <= 2 * r + 1; q++) {
+        double lm = SH(WLAM, f + q, lane);
+        lam = lam < lm ? lm : lam;
+    }
+    const float a = (float)(lam * jh);
+    const float eps = P.eps32;
+    float out[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
+#pragma unroll 1
+    for (int ch = 0; ch < 5; ch++) {
+        asm volatile("" ::: "memory");
+        float L0, L1, L2, L3, L4;
+        left_row<float>(s, ch, L0, L1, L2, L3, L4);
+        float dp[2 * r + 1], dmv[2 * r + 1];
+#pragma unroll
+        for (int q = 0; q <= 2 * r; q++) {
+            int t = f + q;
+            float lf = L0 * DL(0, t, lane) + L1 * DL(1, t, lane) + L2 * DL(2, t, lane) + L3 * DL(3, t, lane)
+                       + L4 * DL(4, t, lane);
+            float lu = L0 * DL(5, t, lane) + L1 * DL(6, t, lane) + L2 * DL(7, t, lane) + L3 * DL(8, t, lane)
+                       + L4 * DL(9, t, lane);
+            dp[q] = 0.5f * (lf + a * lu);
+            dmv[q] = 0.5f * (lf - a * lu);
+        }
+        float phi;
+        if (ORDER == 5) {
+            float dP[4], dM[4];
+#pragma unroll
+            for (int q = 0; q < 4; q++) { dP[q] = dp[q]; dM[q] = dmv[2 * r - q]; }
+            phi = -phi_w5<float>(dP, eps) + phi_w5<float>(dM, eps);
+        } else {
+            float dP[8], dM[8], fp[9], fm[9];
+#pragma unroll
+            for (int q = 0; q < 8; q++) { dP[q] = dp[q]; dM[q] = dmv[2 * r - q]; }
+            fp[0] = 0.f;
+            fm[0] = 0.f;
+#pragma unroll
+            for (int q = 0; q < 8; q++) { fp[q + 1] = fp[q] + dP[q]; fm[q + 1] = fm[q] - dM[q]; }
+            phi = -phi_w9<float>(fp, dP, eps) + phi_w9<float>(fm, dM, eps);
+        }
+        add_right_col<float>(s, ch, phi, out);
+    }
+#pragma unroll
+    for (int q = 0; q < 5; q++) outd[q] = (double)out[q];
+#undef SH
+#undef DL
+}
+
+// Central part of the face flux (src/WENO.c:1754-1816), FP64.
+template <int ORDER>
+__device__ __forceinline__ double central(const double *sh, int NP, int q, int ta, int lane)
+{
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+    if (ORDER == 9)
+        return 1. / 840. * (533. * (SH(WF0 + q, ta + 1, lane) + SH(WF0 + q, ta, lane))
+                            - 139. * (SH(WF0 + q, ta + 2, lane) + SH(WF0 + q, ta - 1, lane))
+                            + 29. * (SH(WF0 + q, ta + 3, lane) + SH(WF0 + q, ta - 2, lane))
+                            - 3. * (SH(WF0 + q, ta + 4, lane) + SH(WF0 + q, ta - 3, lane)));
+    return 1. / 12. * (-1. * (SH(WF0 + q, ta - 1, lane) + SH(WF0 + q, ta + 2, lane))
+                       + 7. * (SH(WF0 + q, ta, lane) + SH(WF0 + q, ta + 1, lane)));
+#undef SH
+}
+
+// ---------------------------------------------------------------------------
+// weno_d: thread-per-face characteristic WENO, flux difference into Q
+// (src/WENO.c:206-494 and its eta/zeta twins).  256 threads, 2 faces each;
+// the face fluxes reuse the staging buffer so two tiles fit on an SM.
+// ---------------------------------------------------------------------------
+// WENO5 fits 128 registers (two tiles per SM); the WENO9 face needs more,
+// so it runs one tile per SM without spilling.
+template <int DIM, int ORDER, int D, bool MIXED, int TLN = TL>
+__device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool first, const double *__restrict__ R,
+                                          const double *__restrict__ Uu, const double *__restrict__ Vv,
+                                          const double *__restrict__ Ww, const double *__restrict__ Ee,
+                                          const Fields &F, int bx, int by, int bz)
+{
+    constexpr int r = (ORDER - 1) / 2;
+    constexpr int NP = TLN + 2 * r + 2;
+    constexpr int NV = WenoNV<DIM>::NV;
+    constexpr int NFT = TLN + 1;                        // faces per line
+    constexpr int FPT = NFT / NROWT;                    // faces per thread
+    static_assert(NFT % NROWT == 0 && (FPT == 1 || FPT == 2), "tile length");
+    extern __shared__ double smem[];
+    double *sh = smem;                                  // [NV][NP][NLANE]
+    double *fh = smem;                                  // [5][NFT][NLANE], aliases sh after the faces
+    const int lane = threadIdx.x, row = threadIdx.y;
+    const Tile T = make_tile<DIM, D, TLN>(G, lane, bx, by, bz);
+
+    stage_weno<DIM, ORDER, D, TLN>(G, P, T, sh, R, Uu, Vv, Ww, Ee, F);
+    __syncthreads();
+    if (MIXED) {
+        // fb: the 16 face fluxes of every line.  Central parts first (they need
+        // the FP64 point fluxes), then the FP32 differences overwrite the
+        // point-flux region, then the WENO parts are added.
+        double *fb = smem + NV * NP * NLANE;           // [5][NFT][NLANE]
+        float *dl = (float *)(smem + WF0 * NP * NLANE); // [10][NP-1][NLANE] over the F region
+#pragma unroll
+        for (int k = 0; k < FPT; k++) {
+            const int f = row + k * NROWT;
+            if (T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1)
+#pragma unroll
+                for (int q = 0; q < 5; q++) fb[(q * NFT + f) * NLANE + lane] = central<ORDER>(sh, NP, q, r + f, lane);
+        }
+        constexpr int NIT = ((NP - 1) * NLANE + NTHR - 1) / NTHR;
+        float dv[NIT][10];
+#pragma unroll
+        for (int m = 0; m < NIT; m++) {
+            int it = row * NLANE + lane + m * NTHR;
+            int l = it % NLANE, t = it / NLANE;
+            if (it < (NP - 1) * NLANE && T.l0 + l < G.g + T.nL && T.c0 - r + t < G.N[D]) {
+#pragma unroll
+                for (int q = 0; q < 5; q++) {
+                    dv[m][q] = (float)(sh[((WF0 + q) * NP + t + 1) * NLANE + l] - sh[((WF0 + q) * NP + t) * NLANE + l]);
+                    dv[m][5 + q] = (float)(sh[((WU0 + q) * NP + t + 1) * NLANE + l] - sh[((WU0 + q) * NP + t) * NLANE + l]);
+                }
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int m = 0; m < NIT; m++) {
+            int it = row * NLANE + lane + m * NTHR;
+            int l = it % NLANE, t = it / NLANE;
+            if (it < (NP - 1) * NLANE && T.l0 + l < G.g + T.nL && T.c0 - r + t < G.N[D])
+#pragma unroll
+                for (int q = 0; q < 10; q++) dl[(q * (NP - 1) + t) * NLANE + l] = dv[m][q];
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < FPT; k++) {
+            const int f = row + k * NROWT;
+            asm volatile("" ::: "memory");
+            if (T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1) {
+                double w5[5];
+                face_weno_mixed<DIM, ORDER, D, TLN>(P, sh, dl, f, lane, w5);
+#pragma unroll
+                for (int q = 0; q < 5; q++) fb[(q * NFT + f) * NLANE + lane] += w5[q];
+            }
+        }
+        __syncthreads();
+        fh = fb;
+    } else if (FPT == 1) {
+    // one face per thread: into registers, then over the staging buffer
+    double res[5];
+    const bool ok0 = T.lane_ok && (T.c0 - 1 + row) <= G.g + T.nD - 1;
+    if (ok0) {
+        double w5[5];
+        face_weno_fp64<DIM, ORDER, D, TLN>(P, sh, row, lane, w5);
+#pragma unroll
+        for (int q = 0; q < 5; q++) res[q] = w5[q] + central<ORDER>(sh, NP, q, r + row, lane);
+    }
+    __syncthreads();
+    if (ok0)
+#pragma unroll
+        for (int q = 0; q < 5; q++) fh[(q * NFT + row) * NLANE + lane] = res[q];
+    __syncthreads();
+    } else {
+    // face fluxes: faces 0..7 go to a dedicated buffer as soon as they are
+    // computed, faces 8..15 stay in registers until the staging buffer is free
+    double *f0 = smem + NV * NP * NLANE;   // [5][NROWT][NLANE]
+    double res[5];
+    bool ok1;
+    {
+        const int f = row;
+        if (T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1) {
+            double w5[5];
+            face_weno_fp64<DIM, ORDER, D, TLN>(P, sh, f, lane, w5);
+#pragma unroll
+            for (int q = 0; q < 5; q++) f0[(q * NROWT + row) * NLANE + lane] = w5[q] + central<ORDER>(sh, NP, q, r + f, lane);
+        }
+    }
+    asm volatile("" ::: "memory");
+    {
+        const int f = row + NROWT;
+        ok1 = T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1;
+        if (ok1) {
+            double w5[5];
+            face_weno_fp64<DIM, ORDER, D, TLN>(P, sh, f, lane, w5);
+#pragma unroll
+            for (int q = 0; q < 5; q++) res[q] = w5[q] + central<ORDER>(sh, NP, q, r + f, lane);
+        }
+    }
+    __syncthreads();
+    if (T.lane_ok) {
+#pragma unroll
+        for (int q = 0; q < 5; q++) fh[(q * NFT + row) * NLANE + lane] = f0[(q * NROWT + row) * NLANE + lane];
+        if (ok1)
+#pragma unroll
+            for (int q = 0; q < 5; q++) fh[(q * NFT + row + NROWT) * NLANE + lane] = res[q];
+    }
+    __syncthreads();
+    }
+    // flux difference into Q; along a contiguous axis the threads walk the
+    // cells of one line (coalesced), otherwise one line per lane
+    for (int it = row * NLANE + lane; it < TLN * NLANE; it += NTHR) {
+        int cr, ln;
+        if (Axes<DIM, D>::CONTIG) { cr = it % TLN; ln = it / TLN; }
+        else { ln = it % NLANE; cr = it / NLANE; }
+        if (T.l0 + ln >= G.g + T.nL || T.c0 + cr > G.g + T.nD - 1) continue;
+        long long o = T.base + (long long)ln * T.sL + (long long)(T.c0 + cr) * T.sD;
+#pragma unroll
+        for (int q = 0; q < 5; q++) {
+            double prev = first ? 0.0 : F.Q[q][o];
+            F.Q[q][o] = prev - (fh[(q * NFT + cr + 1) * NLANE + ln] - fh[(q * NFT + cr) * NLANE + ln]);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// visc_d: central viscous flux difference (src/ZD.c:47-694).
+//
+// Viscous factors are recomputed from the metric instead of streaming the
+// 90 Fluss_Faktor arrays (src/Functions.c:6245-6386):
+//   K[i][k][m] = J ( delta_ik a.grad(xi_m) + a_k dxi_m/dx_i - 2/3 a_i dxi_m/dx_k ),
+//   heat      = J a.grad(xi_m),     a = grad(xi_d),
+// each multiplied by mu and averaged over the two points of the face.
+// 3D uses SHOCK's diagonal metric, so only 8 of the 30 factors are non-zero.
+// ---------------------------------------------------------------------------
+enum { V3U = 0, V3V, V3W, V3T, V3X0, V3X1, V3X2, V3X3, V3F1, V3FA, V3FB, V3NV };
+enum { V2U = 0, V2V, V2T, V2XU, V2XV, V2XT, V2MJ, V2AX, V2AY, V2BX, V2BY, V2NV };
+
+template <int DIM, int ORDER, int D, bool MIXED, int TLN = TL>
+__device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const double *__restrict__ Uu,
+                                          const double *__restrict__ Vv, const double *__restrict__ Ww,
+                                          const Fields &F, int bx, int by, int bz)
+{
+    using A = Axes<DIM, D>;
+    using TS = typename std::conditional<MIXED, float, double>::type;   // stencil arithmetic
+    constexpr int H = ZD<ORDER>::H;          // half stencil: l = 0..2H-1 around the face
+    constexpr int NP = TLN + 2 * H;
+    constexpr int NV = DIM == 3 ? V3NV : V2NV;
+    constexpr int MA = (D == 0) ? 1 : 0;     // 3D: the two non-sweep axes
+    constexpr int MB = (D == 2) ? 1 : 2;
+    const bool quirk = (DIM == 3 && D == 2 && !P.zeta_fix);
+
+    extern __shared__ double smem[];
+    double *sh = smem;                       // [NV][NP][NLANE]
+    constexpr int NFT = TLN + 1;             // faces per line
+    constexpr int FPT = NFT / NROWT;         // faces per thread
+    static_assert(NFT % NROWT == 0 && (FPT == 1 || FPT == 2), "tile length");
+    double *fo = smem + NV * NP * NLANE;     // [4][NFT][NLANE]
+    double *qd = fo + 4 * NFT * NLANE;       // quirk: [16][NLANE] per-line half-point values
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+#define FO(c, f, l) fo[((c) * NFT + (f)) * NLANE + (l)]
+#define QD(c, l) qd[(c) * NLANE + (l)]
+
+    const int lane = threadIdx.x, row = threadIdx.y;
+    const Tile T = make_tile<DIM, D, TLN>(G, lane, bx, by, bz);
+
+    // ---- stage: points c0-H .. c0+TLN+H-1 along the sweep ----------------------
+    const int tid = row * NLANE + lane;
+    for (int it = tid; it < NP * NLANE; it += NTHR) {
+        // lane-fastest: conflict-free shared-memory stores; along a
+        // contiguous axis the 32 lines are 32 strided rows whose sectors the
+        // following points of the loop reuse from L1
+        const int l = it % NLANE, t = it / NLANE;
+        int pd = T.c0 - H + t;
+        if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
+        long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
+        double mu = F.mu[o], J = F.J[o];
+        if (DIM == 3) {
+            double cd = F.m[4 * D][o], ca = F.m[4 * MA][o], cb = F.m[4 * MB][o];
+            SH(V3U, t, l) = Uu[o];
+            SH(V3V, t, l) = Vv[o];
+            SH(V3W, t, l) = Ww[o];
+            SH(V3T, t, l) = F.T[o];
+            SH(V3X0, t, l) = F.Nd[3 * MA + MA][o];   // d vel_MA / d xi_MA
+            SH(V3X1, t, l) = F.Nd[3 * MB + MB][o];   // d vel_MB / d xi_MB
+            SH(V3X2, t, l) = F.Nd[3 * D + MA][o];    // d vel_D / d xi_MA
+            SH(V3X3, t, l) = F.Nd[3 * D + MB][o];    // d vel_D / d xi_MB
+            double mj = mu * J;
+            SH(V3F1, t, l) = mj * (cd * cd);
+            SH(V3FA, t, l) = mj * (cd * ca);
+            SH(V3FB, t, l) = mj * (cd * cb);
+        } else {
+            constexpr int E = 1 - D;
+            SH(V2U, t, l) = Uu[o];
+            SH(V2V, t, l) = Vv[o];
+            SH(V2T, t, l) = F.T[o];
+            SH(V2XU, t, l) = F.Nd[3 * 0 + E][o];
+            SH(V2XV, t, l) = F.Nd[3 * 1 + E][o];
+            SH(V2XT, t, l) = F.Nd[3 * 3 + E][o];
+            SH(V2MJ, t, l) = mu * J;
+            SH(V2AX, t, l) = F.m[3 * D + 0][o];
+            SH(V2AY, t, l) = F.m[3 * D + 1][o];
+            SH(V2BX, t, l) = F.m[3 * E + 0][o];
+            SH(V2BY, t, l) = F.m[3 * E + 1][o];
+        }
+    }
+    if (DIM == 3 && D == 2) {
+        if (quirk && T.lane_ok) {
+            // half-point stencils along k centred on the j index (src/ZD.c:547-548),
+            // the same for every cell of the line: 16 values per lane, 2 per row
+            const int jj = T.l0 + lane;                     // lateral axis of the zeta sweep is j
+            const long long lb = T.base + (long long)lane * T.sL;   // (i, j, 0)
+            const double *vs[4] = {Uu, Vv, Ww, F.T};
+            const double *xs[4] = {F.Nd[3 * MA + MA], F.Nd[3 * MB + MB], F.Nd[3 * D + MA], F.Nd[3 * D + MB]};
+#pragma unroll
+            for (int k2 = 0; k2 < 2; k2++) {
+                int idx = row * 2 + k2;                     // 0..15: side*8 + quantity
+                int side = idx >> 3, qn = idx & 7;
+                const double *src = qn < 4 ? vs[qn] : xs[qn - 4];
+                TS acc = 0;
+                if (qn < 4) {
+                    double ref = src[lb + jj];              // value near the stencil centre
+#pragma unroll
+                    for (int l = 0; l < 2 * H; l++)
+                        acc += (TS)ZD<ORDER>::half(l) * (TS)(src[lb + (jj + l - H + side)] - (MIXED ? ref : 0.0));
+                } else {
+#pragma unroll
+                    for (int l = 0; l < 2 * H; l++) acc += (TS)ZD<ORDER>::interp(l) * (TS)src[lb + (jj + l - H + side)];
+                }
+                QD(idx, lane) = (double)acc;
+            }
+        }
+    }
+    __syncthreads();
+
+    const double t23 = 2.0 / 3.0, t43 = 4.0 / 3.0;
+#pragma unroll
+    for (int k = 0; k < FPT; k++) {
+        const int f = row + k * NROWT;   // face (c0-1+f)+1/2: staged points f .. f+2H-1
+        if (!(T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1)) continue;
+        const int ta = f + H - 1;        // staged index of the left point
+        if (DIM == 3) {
+            double K1 = 0.5 * (SH(V3F1, ta, lane) + SH(V3F1, ta + 1, lane));
+            double KA = 0.5 * (SH(V3FA, ta, lane) + SH(V3FA, ta + 1, lane));
+            double KB = 0.5 * (SH(V3FB, ta, lane) + SH(V3FB, ta + 1, lane));
+            if (quirk) {
+                FO(0, f, lane) = K1; FO(1, f, lane) = KA; FO(2, f, lane) = KB;
+            } else {
+                TS dU = 0, dV = 0, dW = 0, dT = 0, x0 = 0, x1 = 0, x2 = 0, x3 = 0;
+                const double ru = MIXED ? SH(V3U, ta, lane) : 0.0, rv = MIXED ? SH(V3V, ta, lane) : 0.0;
+                const double rw = MIXED ? SH(V3W, ta, lane) : 0.0, rT = MIXED ? SH(V3T, ta, lane) : 0.0;
+#pragma unroll
+                for (int l = 0; l < 2 * H; l++) {
+                    int t = f + l;
+                    TS ch = (TS)ZD<ORDER>::half(l), ci = (TS)ZD<ORDER>::interp(l);
+                    dU += ch * (TS)(SH(V3U, t, lane) - ru); dV += ch * (TS)(SH(V3V, t, lane) - rv);
+                    dW += ch * (TS)(SH(V3W, t, lane) - rw); dT += ch * (TS)(SH(V3T, t, lane) - rT);
+                    x0 += ci * (TS)SH(V3X0, t, lane); x1 += ci * (TS)SH(V3X1, t, lane);
+                    x2 += ci * (TS)SH(V3X2, t, lane); x3 += ci * (TS)SH(V3X3, t, lane);
+                }
+                double dvel[3] = {(double)dU, (double)dV, (double)dW};
+                double gD = dvel[D] * (t43 * K1) + (double)x0 * (-t23 * KA) + (double)x1 * (-t23 * KB);
+                double gA = dvel[MA] * K1 + (double)x2 * KA;
+                double gB = dvel[MB] * K1 + (double)x3 * KB;
+                double g3[3];
+                g3[D] = gD; g3[MA] = gA; g3[MB] = gB;
+                FO(0, f, lane) = g3[0]; FO(1, f, lane) = g3[1]; FO(2, f, lane) = g3[2];
+                FO(3, f, lane) = (double)dT * K1;
+            }
+        } else {
+            constexpr int E = 1 - D;
+            TS dU = 0, dV = 0, dT = 0, xU = 0, xV = 0, xT = 0;
+            const double ru = MIXED ? SH(V2U, ta, lane) : 0.0, rv = MIXED ? SH(V2V, ta, lane) : 0.0;
+            const double rT = MIXED ? SH(V2T, ta, lane) : 0.0;
+#pragma unroll
+            for (int l = 0; l < 2 * H; l++) {
+                int t = f + l;
+                TS ch = (TS)ZD<ORDER>::half(l), ci = (TS)ZD<ORDER>::interp(l);
+                dU += ch * (TS)(SH(V2U, t, lane) - ru); dV += ch * (TS)(SH(V2V, t, lane) - rv);
+                dT += ch * (TS)(SH(V2T, t, lane) - rT);
+                xU += ci * (TS)SH(V2XU, t, lane); xV += ci * (TS)SH(V2XV, t, lane); xT += ci * (TS)SH(V2XT, t, lane);
+            }
+            double Dk[2][2], DT[2];
+            Dk[0][D] = dU; Dk[1][D] = dV; DT[D] = dT;
+            Dk[0][E] = xU; Dk[1][E] = xV; DT[E] = xT;
+            double gx = 0, gy = 0, hh = 0;
+#pragma unroll
+            for (int side = 0; side < 2; side++) {
+                int t = ta + side;
+                double mj = SH(V2MJ, t, lane);
+                double ax = SH(V2AX, t, lane), ay = SH(V2AY, t, lane);
+                double bx = SH(V2BX, t, lane), by = SH(V2BY, t, lane);
+                double gm[2][2];
+                gm[D][0] = ax; gm[D][1] = ay; gm[E][0] = bx; gm[E][1] = by;
+                double av[2] = {ax, ay};
+                double s0 = 0, s1 = 0, sh0 = 0;
+#pragma unroll
+                for (int m = 0; m < 2; m++) {
+                    double adot = ax * gm[m][0] + ay * gm[m][1];
+#pragma unroll
+                    for (int kk = 0; kk < 2; kk++) {
+                        double K0 = (kk == 0 ? adot : 0.0) + av[kk] * gm[m][0] - t23 * av[0] * gm[m][kk];
+                        double Kk1 = (kk == 1 ? adot : 0.0) + av[kk] * gm[m][1] - t23 * av[1] * gm[m][kk];
+                        s0 += Dk[kk][m] * K0;
+                        s1 += Dk[kk][m] * Kk1;
+                    }
+                    sh0 += DT[m] * adot;
+                }
+                gx += 0.5 * mj * s0;
+                gy += 0.5 * mj * s1;
+                hh += 0.5 * mj * sh0;
+            }
+            FO(0, f, lane) = gx; FO(1, f, lane) = gy; FO(2, f, lane) = hh;
+        }
+    }
+    __syncthreads();
+
+    // ---- cell update: along a contiguous axis the threads walk the cells of
+    // one line (coalesced), otherwise one line per thread lane ----------------
+    for (int it = row * NLANE + threadIdx.x; it < TLN * NLANE; it += NTHR) {
+        int cr, ln;
+        if (A::CONTIG) { cr = it % TLN; ln = it / TLN; }
+        else { ln = it % NLANE; cr = it / NLANE; }
+        if (T.l0 + ln >= G.g + T.nL || T.c0 + cr > G.g + T.nD - 1) continue;
+        long long o = T.base + (long long)ln * T.sL + (long long)(T.c0 + cr) * T.sD;
+        const int ts = cr + H;        // staged index of the cell
+        double gp[3] = {0, 0, 0}, gmn[3] = {0, 0, 0}, hp = 0, hm = 0;
+        double nodeB = 0, vel[3];
+        if (DIM == 3) {
+            vel[0] = SH(V3U, ts, ln); vel[1] = SH(V3V, ts, ln); vel[2] = SH(V3W, ts, ln);
+            if (quirk) {
+                double K1p = FO(0, cr + 1, ln), KAp = FO(1, cr + 1, ln), KBp = FO(2, cr + 1, ln);
+                double K1m = FO(0, cr, ln), KAm = FO(1, cr, ln), KBm = FO(2, cr, ln);
+                // QD: side 0 = minus (j-1/2), side 1 = plus; quantities u,v,w,T along, then x0..x3
+                double Dm[8], Dp[8];
+#pragma unroll
+                for (int q = 0; q < 8; q++) { Dm[q] = QD(q, ln); Dp[q] = QD(8 + q, ln); }
+                gp[D] = Dp[D] * (t43 * K1p) + Dp[4] * (-t23 * KAp) + Dp[5] * (-t23 * KBp);
+                gp[MA] = Dp[MA] * K1p + Dp[6] * KAp;
+                gp[MB] = Dp[MB] * K1p + Dp[7] * KBp;
+                hp = Dp[3] * K1p;
+                gmn[D] = Dm[D] * (t43 * K1m) + Dm[4] * (-t23 * KAm) + Dm[5] * (-t23 * KBm);
+                gmn[MA] = Dm[MA] * K1m + Dm[6] * KAm;
+                gmn[MB] = Dm[MB] * K1m + Dm[7] * KBm;
+                hm = Dm[3] * K1m;
+            } else {
+#pragma unroll
+                for (int q = 0; q < 3; q++) { gp[q] = FO(q, cr + 1, ln); gmn[q] = FO(q, cr, ln); }
+                hp = FO(3, cr + 1, ln);
+                hm = FO(3, cr, ln);
+            }
+            // node term: mu * sum_i N[i][D] * sum_{k,m} N[k][m] Fac[i][k][m] at the cell;
+            // the staged factors already carry mu*J
+            const double F1 = SH(V3F1, ts, ln), FA = SH(V3FA, ts, ln), FB = SH(V3FB, ts, ln);
+            const double nAA = SH(V3X0, ts, ln), nBB = SH(V3X1, ts, ln);
+            const double nDA = SH(V3X2, ts, ln), nDB = SH(V3X3, ts, ln);
+            const double nDD = F.Nd[3 * D + D][o], nAD = F.Nd[3 * MA + D][o], nBD = F.Nd[3 * MB + D][o];
+            double hD = nDD * (t43 * F1) + nAA * (-t23 * FA) + nBB * (-t23 * FB);
+            double hA = nAD * F1 + nDA * FA;
+            double hB = nBD * F1 + nDB * FB;
+            nodeB = nDD * hD + nAD * hA + nBD * hB;
+        } else {
+            constexpr int E = 1 - D;
+            vel[0] = SH(V2U, ts, ln); vel[1] = SH(V2V, ts, ln); vel[2] = 0.0;
+#pragma unroll
+            for (int q = 0; q < 2; q++) { gp[q] = FO(q, cr + 1, ln); gmn[q] = FO(q, cr, ln); }
+            hp = FO(2, cr + 1, ln);
+            hm = FO(2, cr, ln);
+            double ax = SH(V2AX, ts, ln), ay = SH(V2AY, ts, ln);
+            double gmv[2][2];
+            gmv[D][0] = ax; gmv[D][1] = ay; gmv[E][0] = SH(V2BX, ts, ln); gmv[E][1] = SH(V2BY, ts, ln);
+            double av[2] = {ax, ay};
+            double N[2][2];   // N[var][dir]
+            N[0][E] = SH(V2XU, ts, ln); N[1][E] = SH(V2XV, ts, ln);
+            N[0][D] = F.Nd[3 * 0 + D][o]; N[1][D] = F.Nd[3 * 1 + D][o];
+            double hsum[2] = {0, 0};
+#pragma unroll
+            for (int m = 0; m < 2; m++) {
+                double adot = ax * gmv[m][0] + ay * gmv[m][1];
+#pragma unroll
+                for (int kk = 0; kk < 2; kk++) {
+#pragma unroll
+                    for (int i = 0; i < 2; i++) {
+                        double K = (i == kk ? adot : 0.0) + av[kk] * gmv[m][i] - t23 * av[i] * gmv[m][kk];
+                        hsum[i] += N[kk][m] * K;
+                    }
+                }
+            }
+            nodeB = SH(V2MJ, ts, ln) * (N[0][D] * hsum[0] + N[1][D] * hsum[1]);
+        }
+        const double psi = P.psi;
+        F.Q[1][o] = F.Q[1][o] + psi * (gp[0] - gmn[0]);
+        F.Q[2][o] = F.Q[2][o] + psi * (gp[1] - gmn[1]);
+        if (DIM == 3) F.Q[3][o] = F.Q[3][o] + psi * (gp[2] - gmn[2]);
+        double Aterm = vel[0] * (gp[0] - gmn[0]) + vel[1] * (gp[1] - gmn[1]);
+        if (DIM == 3) Aterm += vel[2] * (gp[2] - gmn[2]);
+        F.Q[4][o] = F.Q[4][o] + 0.5 * (P.gam + P.gam) * (hp - hm) + psi * (Aterm + nodeB);
+    }
+#undef SH
+#undef FO
+#undef QD
+}
+
+// ---------------------------------------------------------------------------
+// RK stage update of the real points (src/Functions.c:2300-2365), with the
+// time-independent source J*S added to Q first.
+// ---------------------------------------------------------------------------
+template <int DIM>
+__device__ __forceinline__ void rk_body(const Grid &G, const RKCoef &K, double tau, const StageIn &in,
+                                        const Fields &F, double *o0, double *o1, double *o2, double *o3, double *o4,
+                                        int has_source, int t, bool zero_qs = false)
+{
+    int i, j, k;
+    if (DIM == 3) {
+        k = t % G.n[2];
+        int r = t / G.n[2];
+        j = r % G.n[1];
+        i = r / G.n[1];
+    } else {
+        k = 0;
+        j = t % G.n[1];
+        i = t / G.n[1];
+    }
+    long long o = (long long)(i + G.g) * G.st[0] + (long long)(j + G.g) * G.st[1] + (DIM == 3 ? k + G.g : 0);
+    double Q[5], Qs[5];
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+        Q[c] = F.Q[c][o];
+        if (has_source) Q[c] += F.js[c][o];
+        Qs[c] = (zero_qs ? 0.0 : F.Qs[c][o]) + K.s * Q[c];   // zero_qs: Q_sum starts this step
+        F.Qs[c][o] = Qs[c];
+    }
+    double ro = in.U[0][o];
+    double tj = tau / F.J[o];
+    double rn = K.a * F.Un[0][o] + K.b * ro + tj * (K.c * Q[0] + K.d * Qs[0]);
+    double *outs[5] = {o0, o1, o2, o3, o4};
+    outs[0][o] = rn;
+#pragma unroll
+    for (int c = 1; c < 5; c++) {
+        if (DIM == 2 && c == 3) { outs[3][o] = 0.0; continue; }
+        outs[c][o] = (K.a * F.Un[c][o] * F.Un[0][o] + K.b * in.U[c][o] * ro + tj * (K.c * Q[c] + K.d * Qs[c])) / rn;
+    }
+}
+
+
+// Dynamic shared memory of the sweep bodies.
+template <int DIM, int ORDER, bool MIXED, int TLN = TL>
+constexpr size_t weno_smem_bytes()
+{
+    return sizeof(double) * ((size_t)WenoNV<DIM>::NV * (TLN + ORDER + 1) * NLANE + 5 * (MIXED ? TLN + 1 : NROWT) * NLANE);
+}
+
+template <int DIM, int ORDER, int TLN = TL>
+constexpr size_t visc_smem_bytes()
+{
+    return sizeof(double) * ((size_t)(DIM == 3 ? V3NV : V2NV) * (TLN + ORDER + 1) * NLANE + 4 * (TLN + 1) * NLANE + 16 * NLANE);
+}
+
+}  // namespace shock

@@ -96,24 +96,8 @@ extern "C" int shock_rhs_static(const shock_params *p, const double *geom13, dou
     int rc = scratch_for_current_device(&scratch);
     if (rc) return rc;
 
-    Grid G{};
-    G.dim = p->dim; G.order = p->order; G.g = L.g;
-    for (int a = 0; a < 3; a++) {
-        G.n[a] = L.n[a]; G.N[a] = L.N[a]; G.st[a] = L.st[a];
-        G.periodic[a] = a < p->dim ? p->periodic[a] : 0;
-    }
-    G.NG = L.NG;
-    Phys P{};
-    P.gamma = p->gamma;
-    P.igm1 = 1.0 / (p->gamma - 1.0);
-    P.ups = 1.0 / (p->gamma * (p->mach * p->mach));
-    P.psi = 1.0 / p->reynolds;
-    P.suth = 100.4 / p->t0;
-    P.gam = 1.0 / ((p->gamma - 1.0) * (p->mach * p->mach) * p->reynolds * p->prandtl);
-    P.eps64 = 10. * sqrt(2.2250738585072014e-308);   // 10*sqrt(DBL_MIN), src/Functions.c:1829
-    P.eps32 = 10.f * sqrtf(1.17549435e-38f);          // 10*sqrt(FLT_MIN)
-    P.mms = 0;
-    P.zeta_fix = p->zeta_fix;
+    const Grid G = make_grid(L, *p);
+    const Phys P = make_phys(*p);
 
     // Field views: caller's geometry (J and the nine metric terms follow
     // x, y, z), caller's state and output, library scratch.

@@ -1,0 +1,139 @@
+"""Batched execution (shock_batch_*) against single-block solves.
+
+Every member of a batch runs the device bodies of the single-block kernels
+with the same operation order; compiled into other kernels, the compiler may
+contract a few multiply-adds differently, so a member agrees with its solo
+solve (shock_ctx) to rounding level, checked at the parity tolerance of one
+RHS (1e-12 relative per variable).  Within the batched path a member's
+result does not depend on what else is in the batch: alone and in a mix,
+joining or leaving at any step, it is bitwise the same.  The mixed-precision
+batch is checked against the FP64 solve of every instance (relative L2
+<= 1e-6 per conserved variable).
+"""
+import numpy as np
+import pytest
+
+import shock_b200
+from _util import conserved, l2_rel, real, rel_err
+from shock_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-12
+
+
+def _close(got, ref):
+    err = rel_err(got, ref)
+    return (err <= TOL).all(), err
+
+
+def _alone(case, nsteps, precision=shock_b200.SHOCK_FP64, persistent=1, dim=2, order=5):
+    b = shock_b200.Batch(dim, order, precision)
+    b.set_tuning(persistent=persistent)
+    m = b.add(case, nsteps)
+    b.step(nsteps)
+    st = b.state(m)
+    b.close()
+    return st
+
+
+def _solo(case, nsteps, precision=shock_b200.SHOCK_FP64):
+    s = shock_b200.Solver(case, precision=precision)
+    s.steps(nsteps)
+    st = s.state()
+    s.close()
+    return st
+
+
+def _vortices(ns, seed=4):
+    rng = np.random.default_rng(seed)
+    out = []
+    for n in ns:
+        out.append(cases.isentropic_vortex(int(n), beta=float(rng.uniform(1, 5)),
+                                           mach_inf=float(rng.uniform(0.2, 0.8))))
+    return out
+
+
+@pytest.mark.parametrize("persistent", [1, 0])
+def test_batch_2d_vortices_match_solo(persistent):
+    cs = _vortices([32, 48, 40, 64, 33])
+    b = shock_b200.Batch(2, 5, shock_b200.SHOCK_FP64)
+    b.set_tuning(persistent=persistent)
+    ms = [b.add(c, 6) for c in cs]
+    b.step(6)
+    for m, c in zip(ms, cs):
+        got = real(c, b.state(m))
+        ok, err = _close(got, real(c, _solo(c, 6)))
+        assert ok, (c.name, err)
+        assert np.array_equal(got, real(c, _alone(c, 6, persistent=persistent))), c.name
+    b.close()
+
+
+def test_batch_3d_viscous_uneven_members():
+    cs = [cases.taylor_green(16, order=5), cases.smooth_random(3, 5, (20, 12, 18), seed=3),
+          cases.smooth_random(3, 5, (12, 16, 16), seed=5)]
+    b = shock_b200.Batch(3, 5, shock_b200.SHOCK_FP64)
+    ms = [b.add(c, 3) for c in cs]
+    b.step(3)
+    for m, c in zip(ms, cs):
+        ok, err = _close(real(c, b.state(m)), real(c, _solo(c, 3)))
+        assert ok, (c.name, err)
+
+
+def test_batch_w9_2d_viscous():
+    cs = [cases.smooth_random(2, 9, (24, 30, 1), seed=11), cases.smooth_random(2, 9, (40, 20, 1), seed=12)]
+    b = shock_b200.Batch(2, 9, shock_b200.SHOCK_FP64)
+    ms = [b.add(c, 2) for c in cs]
+    b.step(2)
+    for m, c in zip(ms, cs):
+        ok, err = _close(real(c, b.state(m)), real(c, _solo(c, 2)))
+        assert ok, (c.name, err)
+
+
+def test_batch_members_join_finish_and_leave():
+    """Continuous batching: members with different step counts, one added
+    after two steps and one removed early; each result is bitwise the same
+    as the member alone in a batch."""
+    a, bcase, c, d = _vortices([32, 48, 36, 40], seed=9)
+    b = shock_b200.Batch(2, 5, shock_b200.SHOCK_FP64)
+    ma = b.add(a, 3)
+    mb = b.add(bcase, 5)
+    md = b.add(d, 50)
+    b.step(2)
+    mc = b.add(c, 4)
+    b.remove(md)
+    b.step(4)                       # a stops after 3, b after 5, c runs 4
+    assert b.steps_left(ma) == 0 and b.steps_left(mb) == 0 and b.steps_left(mc) == 0
+    for m, case, n in ((ma, a, 3), (mb, bcase, 5), (mc, c, 4)):
+        got = real(case, b.state(m))
+        assert np.array_equal(got, real(case, _alone(case, n))), case.name
+        ok, err = _close(got, real(case, _solo(case, n)))
+        assert ok, (case.name, err)
+
+
+def test_batch_arena_budget():
+    cs = _vortices([64, 64, 64])
+    need = shock_b200.member_bytes(cs[0])
+    b = shock_b200.Batch(2, 5, shock_b200.SHOCK_FP64, arena_bytes=2 * need)
+    m0 = b.add(cs[0], 1)
+    b.add(cs[1], 1)
+    with pytest.raises(shock_b200.ShockError) as e:
+        b.add(cs[2], 1)
+    assert e.value.code == -2
+    b.remove(m0)
+    b.add(cs[2], 1)
+    assert b.info()["members"] == 2
+
+
+def test_batch_mixed_vs_fp64_solo():
+    cs = _vortices([32, 64, 48])
+    b = shock_b200.Batch(2, 5, shock_b200.SHOCK_MIXED)
+    ms = [b.add(c, 20) for c in cs]
+    b.step(20)
+    for m, c in zip(ms, cs):
+        got = conserved(real(c, b.state(m)))
+        ref = conserved(real(c, _solo(c, 20)))
+        err = l2_rel(got, ref)
+        assert (err[[0, 1, 2, 4]] <= 1e-6).all(), (c.name, err)
+        # and the same as the instance alone in a mixed batch
+        assert np.array_equal(real(c, b.state(m)), real(c, _alone(c, 20, shock_b200.SHOCK_MIXED)))
