@@ -59,7 +59,7 @@ class Params(C.Structure):
 def build_library(force: bool = False) -> str:
     """Compile shock_b200/csrc into libshock_b200.so (nvcc, sm_100a)."""
     if force or not os.path.exists(LIB_PATH):
-        subprocess.run(["make", "-s", "-C", os.path.join(HERE, "csrc")], check=True)
+        subprocess.run(["make", "-s", "-j8", "-C", os.path.join(HERE, "csrc")], check=True)
     return LIB_PATH
 
 

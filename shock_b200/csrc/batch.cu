@@ -270,7 +270,12 @@ int rebuild_plan(shock_batch *b)
             const bool visc = !h.p.inviscid;
             const long long nreal = (long long)G.n[0] * G.n[1] * (G.dim == 3 ? G.n[2] : 1);
             switch (ph) {
-            case PH_GHOST:
+            case PH_GHOST: {
+                const long long ns = 2LL * G.g * G.N[1] * G.N[2] + (long long)G.n[0] * 2 * G.g * G.N[2] +
+                                     (G.dim == 3 ? (long long)G.n[0] * G.n[1] * 2 * G.g : 0);   // shell_points
+                for (long long a = 0; a * b->chunk < ns; a++) items.push_back(BatchItem{m, (int)a, 0, 0});
+                break;
+            }
             case PH_PRIM:
                 for (long long a = 0; a * b->chunk < G.NG; a++) items.push_back(BatchItem{m, (int)a, 0, 0});
                 break;

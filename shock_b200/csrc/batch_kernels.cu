@@ -138,15 +138,22 @@ __device__ __forceinline__ void run_item(int ph, const Member &M, const BatchIte
     stage_buffers(M.un, stage, cur, out);
     double *const *U = M.buf[cur];
     switch (ph) {
-    case PH_GHOST:
+    case PH_GHOST: {
+        const long long t0 = (long long)it.a * chunk, ns = shell_points(M.G);
+        for (int j = tid; j < chunk; j += NTHR) {
+            const long long t = t0 + j;
+            if (t >= ns) break;
+            ghost_body(M.G, shell_index(M.G, t), U[0], U[1], U[2], U[3], U[4]);
+        }
+        break;
+    }
     case PH_PRIM:
     case PH_NODAL: {
         const long long o0 = (long long)it.a * chunk;
         for (int j = tid; j < chunk; j += NTHR) {
             const long long o = o0 + j;
             if (o >= M.G.NG) break;
-            if (ph == PH_GHOST) ghost_body(M.G, o, U[0], U[1], U[2], U[3], U[4]);
-            else if (ph == PH_PRIM)
+            if (ph == PH_PRIM)
                 prim_body<DIM>(M.G, M.P, o, U[0], U[1], U[2], U[3], U[4], M.F.p, M.F.T, M.F.c, M.F.mu);
             else nodal_body<DIM, ORDER>(M.G, o, U[1], U[2], U[3], M.F.T, M.F);
         }

@@ -34,6 +34,50 @@ __device__ __forceinline__ bool is_real(const Grid &G, int a, int i) { return i 
 // ghosts: periodic images over the ghost shell (all periodic axes at once;
 // equivalent to SHOCK's repeated slab exchange).
 // ---------------------------------------------------------------------------
+// The ghost shell of a block, enumerated without the real core: points
+// whose i is a ghost (any j, k), then i real and j a ghost (any k), then
+// (3D) i, j real and k a ghost; k fastest within each part.
+__host__ __device__ __forceinline__ long long shell_points(const Grid &G)
+{
+    const long long g2 = 2 * G.g, N1 = G.N[1], N2 = G.N[2];
+    long long n = g2 * N1 * N2 + (long long)G.n[0] * g2 * N2;
+    if (G.dim == 3) n += (long long)G.n[0] * G.n[1] * g2;
+    return n;
+}
+
+__device__ __forceinline__ long long shell_index(const Grid &G, long long t)
+{
+    const int g = G.g, g2 = 2 * G.g;
+    const long long N1 = G.N[1], N2 = G.N[2];
+    int i, j, k;
+    const long long A = g2 * N1 * N2;
+    if (t < A) {
+        const int ii = (int)(t / (N1 * N2));
+        const long long rem = t - (long long)ii * N1 * N2;
+        i = ii < g ? ii : ii + G.n[0];
+        j = (int)(rem / N2);
+        k = (int)(rem - (long long)j * N2);
+    } else {
+        t -= A;
+        const long long B = (long long)G.n[0] * g2 * N2;
+        if (t < B) {
+            i = g + (int)(t / (g2 * N2));
+            const long long rem = t - (long long)(i - g) * g2 * N2;
+            const int jj = (int)(rem / N2);
+            j = jj < g ? jj : jj + G.n[1];
+            k = (int)(rem - (long long)jj * N2);
+        } else {
+            t -= B;
+            i = g + (int)(t / ((long long)G.n[1] * g2));
+            const long long rem = t - (long long)(i - g) * G.n[1] * g2;
+            j = g + (int)(rem / g2);
+            const int kk = (int)(rem - (long long)(j - g) * g2);
+            k = kk < g ? kk : kk + G.n[2];
+        }
+    }
+    return (long long)i * G.st[0] + (long long)j * G.st[1] + k;
+}
+
 __device__ __forceinline__ void ghost_body(const Grid &G, long long o, double *r, double *u, double *v, double *w,
                                            double *e)
 {
@@ -241,6 +285,8 @@ constexpr int NFACE = TL + 1;  // faces per tile line
 constexpr int NLANE = 32;      // lines per tile
 constexpr int NROWT = 8;       // thread rows; each handles faces row and row + 8
 constexpr int NTHR = NLANE * NROWT;
+constexpr int NLS = NLANE + 1;   // lane stride of the shared-memory tiles: padded so a warp walking
+                                 // along a line (consecutive points) hits distinct banks
 static_assert(TL == TL_HOST && NTHR == NTHR_HOST, "host copies of the tile constants");
 
 // Per-point values staged for the WENO face computation.
@@ -287,13 +333,13 @@ __device__ __forceinline__ void stage_weno(const Grid &G, const Phys &P, const T
     using A = Axes<DIM, D>;
     constexpr int r = (ORDER - 1) / 2;
     constexpr int NP = TLN + 2 * r + 2;
-#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
     const int tid = threadIdx.y * NLANE + threadIdx.x;
     for (int it = tid; it < NP * NLANE; it += NTHR) {
-        // lane-fastest: conflict-free shared-memory stores; along a
-        // contiguous axis the 32 lines are 32 strided rows whose sectors the
-        // following points of the loop reuse from L1
-        const int l = it % NLANE, t = it / NLANE;
+        // along the contiguous axis consecutive threads take consecutive
+        // points of a line (coalesced loads; the padded lane stride keeps the
+        // shared-memory stores conflict-free), otherwise consecutive lines
+        const int l = A::CONTIG ? it / NP : it % NLANE, t = A::CONTIG ? it % NP : it / NLANE;
         int pd = T.c0 - 1 - r + t;
         if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
         long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
@@ -352,7 +398,7 @@ __device__ __forceinline__ FaceState<T> face_state(const Phys &P, const double *
 {
     constexpr int r = (ORDER - 1) / 2;
     constexpr int NP = TLN + 2 * r + 2;
-#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
     FaceState<T> s;
     s.gm = (T)P.gamma;
     s.u = T(0.5) * (T)(SH(WVU, ta, lane) + SH(WVU, ta + 1, lane));
@@ -446,7 +492,7 @@ __device__ __forceinline__ void face_weno_fp64(const Phys &P, const double *sh, 
 {
     constexpr int r = (ORDER - 1) / 2;
     constexpr int NP = TLN + 2 * r + 2;
-#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
     const int ta = r + f;
     const FaceState<double> s = face_state<DIM, ORDER, D, double, TLN>(P, sh, ta, lane);
     const double jh = (SH(WJ, ta, lane) + SH(WJ, ta + 1, lane)) / 2.0;
@@ -508,7 +554,7 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
 {
     constexpr int r = (ORDER - 1) / 2;
     constexpr int NP = TLN + 2 * r + 2;
-#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
 #define DL(v, t, l) dl[((v) * (NP - 1) + (t)) * NLANE + (l)]
     const int ta = r + f;
     const FaceState<float> s = face_state<DIM, ORDER, D, float, TLN>(P, sh, ta, lane);
@@ -566,7 +612,7 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
 template <int ORDER>
 __device__ __forceinline__ double central(const double *sh, int NP, int q, int ta, int lane)
 {
-#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
     if (ORDER == 9)
         return 1. / 840. * (533. * (SH(WF0 + q, ta + 1, lane) + SH(WF0 + q, ta, lane))
                             - 139. * (SH(WF0 + q, ta + 2, lane) + SH(WF0 + q, ta - 1, lane))
@@ -597,25 +643,30 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
     constexpr int FPT = NFT / NROWT;                    // faces per thread
     static_assert(NFT % NROWT == 0 && (FPT == 1 || FPT == 2), "tile length");
     extern __shared__ double smem[];
-    double *sh = smem;                                  // [NV][NP][NLANE]
-    double *fh = smem;                                  // [5][NFT][NLANE], aliases sh after the faces
+    double *sh = smem;                                  // [NV][NP][NLS]
+    double *fh = smem;                                  // [5][NFT][NLS], aliases sh after the faces
     const int lane = threadIdx.x, row = threadIdx.y;
     const Tile T = make_tile<DIM, D, TLN>(G, lane, bx, by, bz);
 
     stage_weno<DIM, ORDER, D, TLN>(G, P, T, sh, R, Uu, Vv, Ww, Ee, F);
     __syncthreads();
     if (MIXED) {
-        // fb: the 16 face fluxes of every line.  Central parts first (they need
-        // the FP64 point fluxes), then the FP32 differences overwrite the
-        // point-flux region, then the WENO parts are added.
-        double *fb = smem + NV * NP * NLANE;           // [5][NFT][NLANE]
-        float *dl = (float *)(smem + WF0 * NP * NLANE); // [10][NP-1][NLANE] over the F region
+        // Central parts first, into registers (they need the FP64 point
+        // fluxes); then the FP32 point-to-point differences overwrite the
+        // point-flux region; the face fluxes fb then take the momentum and
+        // energy rows of the conserved-variable region (density stays: the
+        // face state reads it), and the WENO parts are added.  Everything fits
+        // in the staging buffer, so two tiles share an SM.
+        static_assert(5 * NFT <= 4 * NP, "face fluxes fit over four staged rows");
+        double *fb = smem + (WU0 + 1) * NP * NLS;      // [5][NFT][NLS]
+        float *dl = (float *)(smem + WF0 * NP * NLS);   // [10][NP-1][NLANE] over the F region
+        double cen[FPT][5];
 #pragma unroll
         for (int k = 0; k < FPT; k++) {
             const int f = row + k * NROWT;
             if (T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1)
 #pragma unroll
-                for (int q = 0; q < 5; q++) fb[(q * NFT + f) * NLANE + lane] = central<ORDER>(sh, NP, q, r + f, lane);
+                for (int q = 0; q < 5; q++) cen[k][q] = central<ORDER>(sh, NP, q, r + f, lane);
         }
         constexpr int NIT = ((NP - 1) * NLANE + NTHR - 1) / NTHR;
         float dv[NIT][10];
@@ -626,8 +677,8 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
             if (it < (NP - 1) * NLANE && T.l0 + l < G.g + T.nL && T.c0 - r + t < G.N[D]) {
 #pragma unroll
                 for (int q = 0; q < 5; q++) {
-                    dv[m][q] = (float)(sh[((WF0 + q) * NP + t + 1) * NLANE + l] - sh[((WF0 + q) * NP + t) * NLANE + l]);
-                    dv[m][5 + q] = (float)(sh[((WU0 + q) * NP + t + 1) * NLANE + l] - sh[((WU0 + q) * NP + t) * NLANE + l]);
+                    dv[m][q] = (float)(sh[((WF0 + q) * NP + t + 1) * NLS + l] - sh[((WF0 + q) * NP + t) * NLS + l]);
+                    dv[m][5 + q] = (float)(sh[((WU0 + q) * NP + t + 1) * NLS + l] - sh[((WU0 + q) * NP + t) * NLS + l]);
                 }
             }
         }
@@ -640,6 +691,13 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
 #pragma unroll
                 for (int q = 0; q < 10; q++) dl[(q * (NP - 1) + t) * NLANE + l] = dv[m][q];
         }
+#pragma unroll
+        for (int k = 0; k < FPT; k++) {
+            const int f = row + k * NROWT;
+            if (T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1)
+#pragma unroll
+                for (int q = 0; q < 5; q++) fb[(q * NFT + f) * NLS + lane] = cen[k][q];
+        }
         __syncthreads();
 #pragma unroll
         for (int k = 0; k < FPT; k++) {
@@ -649,7 +707,7 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
                 double w5[5];
                 face_weno_mixed<DIM, ORDER, D, TLN>(P, sh, dl, f, lane, w5);
 #pragma unroll
-                for (int q = 0; q < 5; q++) fb[(q * NFT + f) * NLANE + lane] += w5[q];
+                for (int q = 0; q < 5; q++) fb[(q * NFT + f) * NLS + lane] += w5[q];
             }
         }
         __syncthreads();
@@ -667,12 +725,12 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
     __syncthreads();
     if (ok0)
 #pragma unroll
-        for (int q = 0; q < 5; q++) fh[(q * NFT + row) * NLANE + lane] = res[q];
+        for (int q = 0; q < 5; q++) fh[(q * NFT + row) * NLS + lane] = res[q];
     __syncthreads();
     } else {
     // face fluxes: faces 0..7 go to a dedicated buffer as soon as they are
     // computed, faces 8..15 stay in registers until the staging buffer is free
-    double *f0 = smem + NV * NP * NLANE;   // [5][NROWT][NLANE]
+    double *f0 = smem + NV * NP * NLS;     // [5][NROWT][NLANE]
     double res[5];
     bool ok1;
     {
@@ -698,10 +756,10 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
     __syncthreads();
     if (T.lane_ok) {
 #pragma unroll
-        for (int q = 0; q < 5; q++) fh[(q * NFT + row) * NLANE + lane] = f0[(q * NROWT + row) * NLANE + lane];
+        for (int q = 0; q < 5; q++) fh[(q * NFT + row) * NLS + lane] = f0[(q * NROWT + row) * NLANE + lane];
         if (ok1)
 #pragma unroll
-            for (int q = 0; q < 5; q++) fh[(q * NFT + row + NROWT) * NLANE + lane] = res[q];
+            for (int q = 0; q < 5; q++) fh[(q * NFT + row + NROWT) * NLS + lane] = res[q];
     }
     __syncthreads();
     }
@@ -716,7 +774,7 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
 #pragma unroll
         for (int q = 0; q < 5; q++) {
             double prev = first ? 0.0 : F.Q[q][o];
-            F.Q[q][o] = prev - (fh[(q * NFT + cr + 1) * NLANE + ln] - fh[(q * NFT + cr) * NLANE + ln]);
+            F.Q[q][o] = prev - (fh[(q * NFT + cr + 1) * NLS + ln] - fh[(q * NFT + cr) * NLS + ln]);
         }
     }
 }
@@ -753,10 +811,10 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
     constexpr int NFT = TLN + 1;             // faces per line
     constexpr int FPT = NFT / NROWT;         // faces per thread
     static_assert(NFT % NROWT == 0 && (FPT == 1 || FPT == 2), "tile length");
-    double *fo = smem + NV * NP * NLANE;     // [4][NFT][NLANE]
-    double *qd = fo + 4 * NFT * NLANE;       // quirk: [16][NLANE] per-line half-point values
-#define SH(v, t, l) sh[((v) * NP + (t)) * NLANE + (l)]
-#define FO(c, f, l) fo[((c) * NFT + (f)) * NLANE + (l)]
+    double *fo = smem + NV * NP * NLS;       // [4][NFT][NLS]
+    double *qd = fo + 4 * NFT * NLS;         // quirk: [16][NLANE] per-line half-point values
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
+#define FO(c, f, l) fo[((c) * NFT + (f)) * NLS + (l)]
 #define QD(c, l) qd[(c) * NLANE + (l)]
 
     const int lane = threadIdx.x, row = threadIdx.y;
@@ -765,10 +823,9 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
     // ---- stage: points c0-H .. c0+TLN+H-1 along the sweep ----------------------
     const int tid = row * NLANE + lane;
     for (int it = tid; it < NP * NLANE; it += NTHR) {
-        // lane-fastest: conflict-free shared-memory stores; along a
-        // contiguous axis the 32 lines are 32 strided rows whose sectors the
-        // following points of the loop reuse from L1
-        const int l = it % NLANE, t = it / NLANE;
+        // along the contiguous axis consecutive threads take consecutive
+        // points of a line (coalesced), otherwise consecutive lines
+        const int l = A::CONTIG ? it / NP : it % NLANE, t = A::CONTIG ? it % NP : it / NLANE;
         int pd = T.c0 - H + t;
         if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
         long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
@@ -1045,13 +1102,13 @@ __device__ __forceinline__ void rk_body(const Grid &G, const RKCoef &K, double t
 template <int DIM, int ORDER, bool MIXED, int TLN = TL>
 constexpr size_t weno_smem_bytes()
 {
-    return sizeof(double) * ((size_t)WenoNV<DIM>::NV * (TLN + ORDER + 1) * NLANE + 5 * (MIXED ? TLN + 1 : NROWT) * NLANE);
+    return sizeof(double) * ((size_t)WenoNV<DIM>::NV * (TLN + ORDER + 1) * NLS + (MIXED ? 0 : 5 * NROWT * NLANE));
 }
 
 template <int DIM, int ORDER, int TLN = TL>
 constexpr size_t visc_smem_bytes()
 {
-    return sizeof(double) * ((size_t)(DIM == 3 ? V3NV : V2NV) * (TLN + ORDER + 1) * NLANE + 4 * (TLN + 1) * NLANE + 16 * NLANE);
+    return sizeof(double) * ((size_t)(DIM == 3 ? V3NV : V2NV) * (TLN + ORDER + 1) * NLS + 4 * (TLN + 1) * NLS + 16 * NLANE);
 }
 
 }  // namespace shock

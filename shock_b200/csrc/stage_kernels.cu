@@ -29,10 +29,10 @@ namespace shock {
 // ---------------------------------------------------------------------------
 // single-block kernels
 // ---------------------------------------------------------------------------
-__global__ void k_ghosts(Grid G, double *r, double *u, double *v, double *w, double *e)
+__global__ void k_ghosts(Grid G, long long nshell, double *r, double *u, double *v, double *w, double *e)
 {
-    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (o < G.NG) ghost_body(G, o, r, u, v, w, e);
+    long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (t < nshell) ghost_body(G, shell_index(G, t), r, u, v, w, e);
 }
 
 template <int DIM>
@@ -105,7 +105,8 @@ static inline unsigned blocks_for(long long n, int bs) { return (unsigned)((n + 
 void launch_ghosts(const Grid &G, double *const U[5], cudaStream_t s)
 {
     if (!(G.periodic[0] || G.periodic[1] || G.periodic[2])) return;
-    k_ghosts<<<blocks_for(G.NG, 256), 256, 0, s>>>(G, U[0], U[1], U[2], U[3], U[4]);
+    const long long ns = shell_points(G);
+    k_ghosts<<<blocks_for(ns, 256), 256, 0, s>>>(G, ns, U[0], U[1], U[2], U[3], U[4]);
 }
 
 void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s)

@@ -20,9 +20,17 @@ pytestmark = pytest.mark.gpu
 FP64, MIXED = shock_b200.SHOCK_FP64, shock_b200.SHOCK_MIXED
 
 
+# FP64 requests whose right-hand side SHOCK's own FP64 and 80-bit builds
+# agree on to ~1e-13 or better; on the WENO9 vortex they differ by ~1e-6 (its
+# smoothness indicators are ill-conditioned where the flow is nearly uniform),
+# so that one is checked alone-versus-mix only.
+WELL_CONDITIONED = {"vortex48", "tgv16_w5", "smooth2d_w9", "vcol20x20", "vortex32"}
+
+
 def _mix():
     return [
         (cases.isentropic_vortex(48, 3.0, 0.5), 7, FP64),
+        (cases.smooth_random(2, 9, (40, 36, 1), seed=11), 4, FP64),
         (cases.taylor_green(16, order=5, perturb=0.0, reynolds=800.0), 5, FP64),
         (cases.isentropic_vortex(40, 2.0, 0.3, order=9, inviscid=False, reynolds=2000.0), 4, FP64),
         (cases.taylor_green_2d(64, 5, 0.3, 500.0), 6, MIXED),
@@ -57,7 +65,7 @@ def test_serve_result_same_alone_and_in_mix():
         (a_state, _), = _run(alone, [(case, n, prec)])
         alone.close()
         assert np.array_equal(real(case, state), real(case, a_state)), case.name
-        if prec == FP64:
+        if prec == FP64 and case.name in WELL_CONDITIONED:
             s = shock_b200.Solver(case)
             s.steps(n)
             err = rel_err(real(case, state), real(case, s.state()))
