@@ -335,7 +335,13 @@ __device__ __forceinline__ void stage_weno(const Grid &G, const Phys &P, const T
     constexpr int NP = TLN + 2 * r + 2;
 #define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
     const int tid = threadIdx.y * NLANE + threadIdx.x;
-    for (int it = tid; it < NP * NLANE; it += NTHR) {
+    // unrolled over the thread's points (about three) so that all their
+    // global loads are in flight before the first shared-memory store
+    constexpr int NSTG = (NP * NLANE + NTHR - 1) / NTHR;
+#pragma unroll
+    for (int m = 0; m < NSTG; m++) {
+        const int it = tid + m * NTHR;
+        if (it >= NP * NLANE) continue;
         // along the contiguous axis consecutive threads take consecutive
         // points of a line (coalesced loads; the padded lane stride keeps the
         // shared-memory stores conflict-free), otherwise consecutive lines
@@ -822,7 +828,13 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
 
     // ---- stage: points c0-H .. c0+TLN+H-1 along the sweep ----------------------
     const int tid = row * NLANE + lane;
-    for (int it = tid; it < NP * NLANE; it += NTHR) {
+    // unrolled over the thread's points (about three) so that all their
+    // global loads are in flight before the first shared-memory store
+    constexpr int NSTG = (NP * NLANE + NTHR - 1) / NTHR;
+#pragma unroll
+    for (int m = 0; m < NSTG; m++) {
+        const int it = tid + m * NTHR;
+        if (it >= NP * NLANE) continue;
         // along the contiguous axis consecutive threads take consecutive
         // points of a line (coalesced), otherwise consecutive lines
         const int l = A::CONTIG ? it / NP : it % NLANE, t = A::CONTIG ? it % NP : it / NLANE;

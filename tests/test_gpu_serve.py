@@ -27,6 +27,17 @@ FP64, MIXED = shock_b200.SHOCK_FP64, shock_b200.SHOCK_MIXED
 WELL_CONDITIONED = {"vortex48", "tgv16_w5", "smooth2d_w9", "vcol20x20", "vortex32"}
 
 
+def _err(a, b):
+    """Normwise relative error per variable; velocity components relative to
+    the largest velocity component (w of a vortex column is rounding noise
+    around zero, so max|w| is no scale)."""
+    err = rel_err(a, b)
+    vs = max(np.abs(b[k]).max() for k in (1, 2, 3))
+    for k in (1, 2, 3):
+        err[k] = np.abs(a[k] - b[k]).max() / vs
+    return err
+
+
 def _mix():
     return [
         (cases.isentropic_vortex(48, 3.0, 0.5), 7, FP64),
@@ -68,7 +79,7 @@ def test_serve_result_same_alone_and_in_mix():
         if prec == FP64 and case.name in WELL_CONDITIONED:
             s = shock_b200.Solver(case)
             s.steps(n)
-            err = rel_err(real(case, state), real(case, s.state()))
+            err = _err(real(case, state), real(case, s.state()))
             s.close()
             assert (err <= 1e-12).all(), (case.name, err)
 
