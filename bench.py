@@ -147,6 +147,36 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def rank_helpers(world, device="cuda"):
+    """barrier() (all ranks, then the device) and max_over_ranks(x) for the
+    replicas run: every rank times its own copy of the work, the job's time is
+    the slowest rank's (collectives on `device`: "cuda" under NCCL, "cpu"
+    under gloo)."""
+    import torch
+    import torch.distributed as dist
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        if device == "cuda":
+            torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=device, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    return barrier, max_over_ranks
+
+
+def replica_value(units_per_rank, world, seconds_max):
+    """Whole-job throughput of the replicas run: every rank processed
+    units_per_rank; the job took the slowest rank's time."""
+    return units_per_rank * world / seconds_max
+
+
 def flush_l2(torch, buf):
     buf.zero_()
 
@@ -313,17 +343,7 @@ def main():
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
 
-    def barrier():
-        if world > 1:
-            dist.barrier()
-        torch.cuda.synchronize()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    barrier, max_over_ranks = rank_helpers(world, "cuda")
 
     if args.workload == "batch_vortex256":
         run_batch(args, world, rank, local, barrier, max_over_ranks)
@@ -359,7 +379,7 @@ def main():
     solver, ms64 = timed_device(shock_b200.SHOCK_FP64)
     clocks = sampler.stop()
     ms64 = max_over_ranks(ms64)
-    value = stage_cells * args.steps * world / (ms64 * 1e-3)
+    value = replica_value(stage_cells * args.steps, world, ms64 * 1e-3)
 
     mixed = None
     if not args.no_mixed:
