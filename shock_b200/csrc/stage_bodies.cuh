@@ -255,6 +255,10 @@ __device__ __forceinline__ T phi_w9(const T *f, const T *d, T eps)
             for (int b = a + 1; b < 5; b++) in = in + w9c<T>(k, c++) * f[k + b];
             acc = (a == 0) ? f[k] * in : acc + f[k + a] * in;
         }
+        // the indicator is a non-negative quadratic form; in FP32 rounding can
+        // make it slightly negative and cancel eps (1/t^2 overflows), so the
+        // FP32 form clamps it at zero.  The FP64 form keeps SHOCK's sequence.
+        if (std::is_same<T, float>::value) acc = acc > T(0) ? acc : T(0);
         T t = acc + eps;
         ot[k] = dk[k] * (T(1.) / (t * t));
     }
@@ -1072,23 +1076,12 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
 // RK stage update of the real points (src/Functions.c:2300-2365), with the
 // time-independent source J*S added to Q first.
 // ---------------------------------------------------------------------------
+// RK update of the real point at ghosted index o.
 template <int DIM>
-__device__ __forceinline__ void rk_body(const Grid &G, const RKCoef &K, double tau, const StageIn &in,
-                                        const Fields &F, double *o0, double *o1, double *o2, double *o3, double *o4,
-                                        int has_source, int t, bool zero_qs = false)
+__device__ __forceinline__ void rk_at(const RKCoef &K, double tau, const StageIn &in, const Fields &F, double *o0,
+                                      double *o1, double *o2, double *o3, double *o4, int has_source, long long o,
+                                      bool zero_qs)
 {
-    int i, j, k;
-    if (DIM == 3) {
-        k = t % G.n[2];
-        int r = t / G.n[2];
-        j = r % G.n[1];
-        i = r / G.n[1];
-    } else {
-        k = 0;
-        j = t % G.n[1];
-        i = t / G.n[1];
-    }
-    long long o = (long long)(i + G.g) * G.st[0] + (long long)(j + G.g) * G.st[1] + (DIM == 3 ? k + G.g : 0);
     double Q[5], Qs[5];
 #pragma unroll
     for (int c = 0; c < 5; c++) {
@@ -1107,6 +1100,27 @@ __device__ __forceinline__ void rk_body(const Grid &G, const RKCoef &K, double t
         if (DIM == 2 && c == 3) { outs[3][o] = 0.0; continue; }
         outs[c][o] = (K.a * F.Un[c][o] * F.Un[0][o] + K.b * in.U[c][o] * ro + tj * (K.c * Q[c] + K.d * Qs[c])) / rn;
     }
+}
+
+// RK update of real point number t (i slowest, k fastest over the real box).
+template <int DIM>
+__device__ __forceinline__ void rk_body(const Grid &G, const RKCoef &K, double tau, const StageIn &in,
+                                        const Fields &F, double *o0, double *o1, double *o2, double *o3, double *o4,
+                                        int has_source, int t, bool zero_qs = false)
+{
+    int i, j, k;
+    if (DIM == 3) {
+        k = t % G.n[2];
+        int r = t / G.n[2];
+        j = r % G.n[1];
+        i = r / G.n[1];
+    } else {
+        k = 0;
+        j = t % G.n[1];
+        i = t / G.n[1];
+    }
+    long long o = (long long)(i + G.g) * G.st[0] + (long long)(j + G.g) * G.st[1] + (DIM == 3 ? k + G.g : 0);
+    rk_at<DIM>(K, tau, in, F, o0, o1, o2, o3, o4, has_source, o, zero_qs);
 }
 
 

@@ -60,20 +60,35 @@ __global__ void __launch_bounds__(NTHR, ORDER == 5 ? 2 : 1)
     weno_body<DIM, ORDER, D, MIXED>(G, P, first, R, Uu, Vv, Ww, Ee, F, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
+// Viscous sweep tile length: 7 cells (one face per thread, three tiles per
+// SM) across the strided axes, 15 cells along the contiguous axis, whose
+// staging loads are coalesced along the line and gain little from shorter
+// tiles.
+template <int DIM, int D>
+struct ViscTile {
+    static constexpr int v = (D == DIM - 1) ? TL : 7;
+};
+
 template <int DIM, int ORDER, int D, bool MIXED>
-__global__ void __launch_bounds__(NTHR, 2)
+__global__ void __launch_bounds__(NTHR, ViscTile<DIM, D>::v == TL ? 2 : 3)
     k_visc(Grid G, Phys P, const double *__restrict__ Uu, const double *__restrict__ Vv,
            const double *__restrict__ Ww, Fields F)
 {
-    visc_body<DIM, ORDER, D, MIXED>(G, P, Uu, Vv, Ww, F, blockIdx.x, blockIdx.y, blockIdx.z);
+    visc_body<DIM, ORDER, D, MIXED, ViscTile<DIM, D>::v>(G, P, Uu, Vv, Ww, F, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
+// Rows of real points: x runs along the fastest real axis (k in 3D, j in
+// 2D), y and z over the others, so the ghosted index needs no division.
 template <int DIM>
-__global__ void k_rk(Grid G, RKCoef K, double tau, StageIn in, Fields F, double *o0, double *o1,
-                     double *o2, double *o3, double *o4, int has_source, int nreal)
+__global__ void __launch_bounds__(128) k_rk_rows(Grid G, RKCoef K, double tau, StageIn in, Fields F, double *o0,
+                                                 double *o1, double *o2, double *o3, double *o4, int has_source)
 {
-    int t = blockIdx.x * blockDim.x + threadIdx.x;
-    if (t < nreal) rk_body<DIM>(G, K, tau, in, F, o0, o1, o2, o3, o4, has_source, t);
+    const int nf = DIM == 3 ? G.n[2] : G.n[1];
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const long long o = DIM == 3 ? (long long)(blockIdx.z + G.g) * G.st[0] + (long long)(blockIdx.y + G.g) * G.st[1] + G.g + f
+                                 : (long long)(blockIdx.y + G.g) * G.st[0] + G.g + f;
+    rk_at<DIM>(K, tau, in, F, o0, o1, o2, o3, o4, has_source, o, false);
 }
 
 __global__ void k_add_source(Grid G, Fields F)
@@ -126,11 +141,11 @@ void launch_nodal(const Grid &G, const double *const U[5], const Fields &F, cuda
     else k_nodal<2, 9><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F);
 }
 
-template <int DIM, int D>
+template <int DIM, int D, int TLN = TL>
 static dim3 sweep_grid(const Grid &G)
 {
     using A = Axes<DIM, D>;
-    return dim3((G.n[D] + TL - 1) / TL, (G.n[A::LAT] + NLANE - 1) / NLANE, DIM == 3 ? G.n[A::OTH] : 1);
+    return dim3((G.n[D] + TLN - 1) / TLN, (G.n[A::LAT] + NLANE - 1) / NLANE, DIM == 3 ? G.n[A::OTH] : 1);
 }
 
 // G.order == 0 is the attribute pass: raise the dynamic shared-memory limit
@@ -151,12 +166,13 @@ static void weno_one(const Grid &G, const Phys &P, bool first, const double *con
 template <int DIM, int ORDER, int D, bool MIXED>
 static void visc_one(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s)
 {
-    constexpr size_t smem = visc_smem_bytes<DIM, ORDER>();
+    constexpr int VTL = ViscTile<DIM, D>::v;
+    constexpr size_t smem = visc_smem_bytes<DIM, ORDER, VTL>();
     if (!G.order) {
         cudaFuncSetAttribute(k_visc<DIM, ORDER, D, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         return;
     }
-    k_visc<DIM, ORDER, D, MIXED><<<sweep_grid<DIM, D>(G), dim3(NLANE, NROWT), smem, s>>>(G, P, U[1], U[2], U[3], F);
+    k_visc<DIM, ORDER, D, MIXED><<<sweep_grid<DIM, D, VTL>(G), dim3(NLANE, NROWT), smem, s>>>(G, P, U[1], U[2], U[3], F);
 }
 
 #define SHOCK_SWEEP_CASES(X)                                                           \
@@ -194,13 +210,14 @@ void launch_rk(const Grid &G, const RKCoef &rk, double tau, const double *const 
 {
     StageIn in;
     for (int c = 0; c < 5; c++) in.U[c] = Uin[c];
-    int nreal = G.n[0] * G.n[1] * (G.dim == 3 ? G.n[2] : 1);
+    const int nf = G.dim == 3 ? G.n[2] : G.n[1];
+    const dim3 grid((nf + 127) / 128, G.dim == 3 ? G.n[1] : G.n[0], G.dim == 3 ? G.n[0] : 1);
     if (G.dim == 3)
-        k_rk<3><<<blocks_for(nreal, 256), 256, 0, s>>>(G, rk, tau, in, F, Uout[0], Uout[1], Uout[2], Uout[3], Uout[4],
-                                                       has_source ? 1 : 0, nreal);
+        k_rk_rows<3><<<grid, 128, 0, s>>>(G, rk, tau, in, F, Uout[0], Uout[1], Uout[2], Uout[3], Uout[4],
+                                          has_source ? 1 : 0);
     else
-        k_rk<2><<<blocks_for(nreal, 256), 256, 0, s>>>(G, rk, tau, in, F, Uout[0], Uout[1], Uout[2], Uout[3], Uout[4],
-                                                       has_source ? 1 : 0, nreal);
+        k_rk_rows<2><<<grid, 128, 0, s>>>(G, rk, tau, in, F, Uout[0], Uout[1], Uout[2], Uout[3], Uout[4],
+                                          has_source ? 1 : 0);
 }
 
 void launch_add_source(const Grid &G, const Fields &F, cudaStream_t s)
