@@ -126,7 +126,7 @@ static void enqueue_rhs(shock_ctx *c, double *const in[5], int &nk)
     launch_prim(c->G, c->P, cin, c->F, s);
     nk++;
     if (!c->p.inviscid) {
-        launch_nodal(c->G, cin, c->F, s);
+        launch_nodal(c->G, c->p.precision, cin, c->F, s);
         nk++;
     }
     for (int d = 0; d < c->p.dim; d++) {
@@ -225,7 +225,10 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
     c->F.p = take(); c->F.T = take(); c->F.c = take(); c->F.mu = take();
     c->F.J = take();
     for (int f = 0; f < 9; f++) c->F.m[f] = take();
-    for (int f = 0; f < 12; f++) c->F.Nd[f] = p->inviscid ? nullptr : take();
+    for (int f = 0; f < 12; f++) {
+        c->F.Nd[f] = p->inviscid ? nullptr : take();
+        c->F.Ndf[f] = reinterpret_cast<float *>(c->F.Nd[f]);
+    }
     for (int f = 0; f < 5; f++) c->F.js[f] = nullptr;
     if (cudaMalloc(&c->F.flag, 64) != cudaSuccess) {
         cudaFree(c->pool);
@@ -499,7 +502,7 @@ int shock_profile_stage(shock_ctx *c, int max, char *names, float *ms, int *coun
     mark(nullptr);
     launch_ghosts(c->G, in, c->stream); mark("ghosts");
     launch_prim(c->G, c->P, cin, c->F, c->stream); mark("prim");
-    if (!c->p.inviscid) { launch_nodal(c->G, cin, c->F, c->stream); mark("nodal"); }
+    if (!c->p.inviscid) { launch_nodal(c->G, c->p.precision, cin, c->F, c->stream); mark("nodal"); }
     for (int d = 0; d < c->p.dim; d++) {
         launch_weno(c->G, c->P, c->p.precision, d, d == 0, cin, c->F, c->stream);
         nm.push_back(std::string("weno_") + dn[d]);

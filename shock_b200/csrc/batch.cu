@@ -453,7 +453,10 @@ int batch_add_block(shock_batch *b, const shock_params &pp, const HostBlock &hb,
     m.F.p = take(); m.F.T = take(); m.F.c = take(); m.F.mu = take();
     m.F.J = take();
     for (int f = 0; f < 9; f++) m.F.m[f] = take();
-    for (int f = 0; f < 12; f++) m.F.Nd[f] = p->inviscid ? nullptr : take();
+    for (int f = 0; f < 12; f++) {
+        m.F.Nd[f] = p->inviscid ? nullptr : take();
+        m.F.Ndf[f] = reinterpret_cast<float *>(m.F.Nd[f]);
+    }
     for (int f = 0; f < 5; f++) { m.F.js[f] = nullptr; m.F.Un[f] = m.buf[0][f]; m.F.U[0][f] = m.F.U[1][f] = nullptr; }
     m.F.flag = nullptr;
 
@@ -700,6 +703,35 @@ int shock_batch_get_tuning(const shock_batch *b, shock_batch_tuning *t)
     t->chunk = b->chunk;
     t->small_tile_max = b->small_tile_max;
     t->max_blocks_per_sm = batch_max_blocks_per_sm(b->dim, b->order, b->precision, b->launch.persistent);
+    return SHOCK_OK;
+}
+
+int shock_batch_check_barrier_timeout(int device, double timeout_ms, double *elapsed_ms)
+{
+    if (timeout_ms <= 0 || timeout_ms > 1000) return report_error(SHOCK_EINVAL, "timeout_ms must be in (0, 1000]");
+    CKB(cudaSetDevice(device));
+    BatchSync *sync = nullptr;
+    CKB(cudaMalloc(&sync, sizeof(BatchSync)));
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    cudaMemset(sync, 0, sizeof(BatchSync));
+    int sms = 1;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    cudaEventRecord(e0, 0);
+    launch_barrier_probe(sync, (unsigned long long)(timeout_ms * 1e6), sms, 0);
+    cudaEventRecord(e1, 0);
+    cudaError_t e = cudaDeviceSynchronize();
+    unsigned err = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&err, &sync->err, sizeof err, cudaMemcpyDeviceToHost);
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    if (elapsed_ms) *elapsed_ms = ms;
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    cudaFree(sync);
+    if (e != cudaSuccess) return report_error(SHOCK_ECUDA, "barrier probe: %s", cudaGetErrorString(e));
+    if (err) return report_error(SHOCK_ETIMEOUT, "grid barrier wait ran out after %.1f ms (as intended)", timeout_ms);
     return SHOCK_OK;
 }
 

@@ -61,7 +61,8 @@ __device__ __forceinline__ void stage_buffers(int un, int s, int &cur, int &out)
 
 // All CTAs of the grid meet here.  Returns false when the wait ran out or
 // another CTA reported a timeout; the caller then returns.
-__device__ bool grid_barrier(unsigned *bar, unsigned target, unsigned *err)
+__device__ bool grid_barrier(unsigned *bar, unsigned target, unsigned *err,
+                             unsigned long long timeout_ns = kBarrierTimeoutNs)
 {
     __shared__ int s_ok;
     __syncthreads();
@@ -72,7 +73,7 @@ __device__ bool grid_barrier(unsigned *bar, unsigned target, unsigned *err)
         const unsigned long long t0 = global_ns();
         while (load_acquire(bar) < target) {
             if (load_acquire(err)) { ok = 0; break; }
-            if (global_ns() - t0 > kBarrierTimeoutNs) {
+            if (global_ns() - t0 > timeout_ns) {
                 atomicExch(err, 1u);
                 ok = 0;
                 break;
@@ -155,7 +156,7 @@ __device__ __forceinline__ void run_item(int ph, const Member &M, const BatchIte
             if (o >= M.G.NG) break;
             if (ph == PH_PRIM)
                 prim_body<DIM>(M.G, M.P, o, U[0], U[1], U[2], U[3], U[4], M.F.p, M.F.T, M.F.c, M.F.mu);
-            else nodal_body<DIM, ORDER>(M.G, o, U[1], U[2], U[3], M.F.T, M.F);
+            else nodal_body<DIM, ORDER, MIXED>(M.G, o, U[1], U[2], U[3], M.F.T, M.F);
         }
         break;
     }
@@ -247,6 +248,15 @@ __global__ void __launch_bounds__(NTHR, MinBlocks<ORDER, PH>::v)
         run_phase<DIM, ORDER, MIXED>(ph, mem, items, plan, sync, stage, K, sm, cached);
         pending = true;
     }
+}
+
+// Check of the bounded waits: every CTA but the first arrives at a grid
+// barrier, which therefore never completes; each waiting CTA gives up after
+// timeout_ns, sets sync->err and returns.
+__global__ void k_barrier_probe(BatchSync *sync, unsigned long long timeout_ns)
+{
+    if (blockIdx.x == 0) return;   // the CTA that never arrives
+    grid_barrier(&sync->bar[0], gridDim.x, &sync->err, timeout_ns);
 }
 
 // End of a step: advance every running member's buffer rotation and step
@@ -407,6 +417,11 @@ cudaError_t launch_batch_stage(int dim, int order, int precision, const BatchLau
     SHOCK_BATCH_FORMS(S)
 #undef S
     return cudaErrorInvalidValue;
+}
+
+void launch_barrier_probe(BatchSync *sync, unsigned long long timeout_ns, int ctas, cudaStream_t s)
+{
+    k_barrier_probe<<<ctas, 32, 0, s>>>(sync, timeout_ns);
 }
 
 void launch_batch_advance(Member *mem, const BatchPlan *plan, int capacity, int time_order, BatchSync *sync,

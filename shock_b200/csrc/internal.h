@@ -66,6 +66,7 @@ struct Fields {
     double *p, *T, *c, *mu;
     double *J, *m[9];
     double *Nd[12];      // nodal derivatives, index 3*var+dir (u,v,w,T)
+    float *Ndf[12];      // the same stored in FP32 (mixed form; aliases the first half of Nd)
     double *js[5];       // source J*S or nullptr
     unsigned int *flag;  // device counters: [0] non-finite density count
 };
@@ -155,13 +156,14 @@ void batch_prepare_kernels();
 cudaError_t launch_batch_stage(int dim, int order, int precision, const BatchLaunch &L, const Member *mem,
                                const BatchItem *items, const BatchPlan *plan, BatchSync *sync, int stage,
                                const RKCoef &K, const int *phase_has_items, cudaStream_t s);
+void launch_barrier_probe(BatchSync *sync, unsigned long long timeout_ns, int ctas, cudaStream_t s);
 void launch_batch_advance(Member *mem, const BatchPlan *plan, int capacity, int time_order, BatchSync *sync,
                           cudaStream_t s);
 
 // Kernel launchers (stage_kernels.cu).
 void launch_ghosts(const Grid &G, double *const U[5], cudaStream_t s);
 void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s);
-void launch_nodal(const Grid &G, const double *const U[5], const Fields &F, cudaStream_t s);
+void launch_nodal(const Grid &G, int precision, const double *const U[5], const Fields &F, cudaStream_t s);
 void launch_weno(const Grid &G, const Phys &P, int precision, int d, bool first,
                  const double *const U[5], const Fields &F, cudaStream_t s);
 void launch_viscous(const Grid &G, const Phys &P, int precision, int d, const double *const U[5],

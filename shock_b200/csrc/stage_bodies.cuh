@@ -172,7 +172,14 @@ struct ZD<9> {
     }
 };
 
-template <int DIM, int ORDER>
+// Nodal derivative idx at o: FP64, or the FP32 copy in the mixed form.
+template <bool MIXED>
+__device__ __forceinline__ double ndv(const Fields &F, int idx, long long o)
+{
+    return MIXED ? (double)F.Ndf[idx][o] : F.Nd[idx][o];
+}
+
+template <int DIM, int ORDER, bool MIXED>
 __device__ __forceinline__ void nodal_body(const Grid &G, long long o, const double *__restrict__ U,
                                            const double *__restrict__ V, const double *__restrict__ W,
                                            const double *__restrict__ T, const Fields &F)
@@ -191,7 +198,8 @@ __device__ __forceinline__ void nodal_body(const Grid &G, long long o, const dou
             double acc = 0.0;
 #pragma unroll
             for (int l = 0; l <= 2 * H; l++) acc += ZD<ORDER>::node(l) * var[q][o + (l - H) * sd];
-            F.Nd[3 * q + d][o] = acc;
+            if (MIXED) F.Ndf[3 * q + d][o] = (float)acc;   // viscous-stencil input, FP32 in the mixed form
+            else F.Nd[3 * q + d][o] = acc;
         }
     }
 }
@@ -576,7 +584,7 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
     constexpr int r = (ORDER - 1) / 2;
     constexpr int NP = TLN + 2 * r + 2;
 #define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
-#define DL(v, t, l) dl[((v) * (NP - 1) + (t)) * NLANE + (l)]
+#define DL2(j, t, l) reinterpret_cast<const float2 *>(dl)[((t) * NLANE + (l)) * 5 + (j)]
     const int ta = r + f;
     const FaceState<float> s = face_state<DIM, ORDER, D, float, TLN>(P, sh, ta, lane);
     const double jh = (SH(WJ, ta, lane) + SH(WJ, ta + 1, lane)) / 2.0;
@@ -598,10 +606,11 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
 #pragma unroll
         for (int q = 0; q <= 2 * r; q++) {
             int t = f + q;
-            float lf = L0 * DL(0, t, lane) + L1 * DL(1, t, lane) + L2 * DL(2, t, lane) + L3 * DL(3, t, lane)
-                       + L4 * DL(4, t, lane);
-            float lu = L0 * DL(5, t, lane) + L1 * DL(6, t, lane) + L2 * DL(7, t, lane) + L3 * DL(8, t, lane)
-                       + L4 * DL(9, t, lane);
+            // the ten differences of a point are interleaved: five 8-byte loads
+            const float2 a0 = DL2(0, t, lane), a1 = DL2(1, t, lane), a2 = DL2(2, t, lane);
+            const float2 a3 = DL2(3, t, lane), a4 = DL2(4, t, lane);
+            float lf = L0 * a0.x + L1 * a0.y + L2 * a1.x + L3 * a1.y + L4 * a2.x;
+            float lu = L0 * a2.y + L1 * a3.x + L2 * a3.y + L3 * a4.x + L4 * a4.y;
             dp[q] = 0.5f * (lf + a * lu);
             dmv[q] = 0.5f * (lf - a * lu);
         }
@@ -626,7 +635,7 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
 #pragma unroll
     for (int q = 0; q < 5; q++) outd[q] = (double)out[q];
 #undef SH
-#undef DL
+#undef DL2
 }
 
 // Central part of the face flux (src/WENO.c:1754-1816), FP64.
@@ -680,7 +689,7 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
         // in the staging buffer, so two tiles share an SM.
         static_assert(5 * NFT <= 4 * NP, "face fluxes fit over four staged rows");
         double *fb = smem + (WU0 + 1) * NP * NLS;      // [5][NFT][NLS]
-        float *dl = (float *)(smem + WF0 * NP * NLS);   // [10][NP-1][NLANE] over the F region
+        float *dl = (float *)(smem + WF0 * NP * NLS);   // [NP-1][NLANE][10] over the F region
         double cen[FPT][5];
 #pragma unroll
         for (int k = 0; k < FPT; k++) {
@@ -710,7 +719,8 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
             int l = it % NLANE, t = it / NLANE;
             if (it < (NP - 1) * NLANE && T.l0 + l < G.g + T.nL && T.c0 - r + t < G.N[D])
 #pragma unroll
-                for (int q = 0; q < 10; q++) dl[(q * (NP - 1) + t) * NLANE + l] = dv[m][q];
+                for (int q = 0; q < 5; q++)
+                    reinterpret_cast<float2 *>(dl)[(t * NLANE + l) * 5 + q] = make_float2(dv[m][2 * q], dv[m][2 * q + 1]);
         }
 #pragma unroll
         for (int k = 0; k < FPT; k++) {
@@ -863,10 +873,10 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
             SH(V3V, t, l) = Vv[o];
             SH(V3W, t, l) = Ww[o];
             SH(V3T, t, l) = F.T[o];
-            SH(V3X0, t, l) = F.Nd[3 * MA + MA][o];   // d vel_MA / d xi_MA
-            SH(V3X1, t, l) = F.Nd[3 * MB + MB][o];   // d vel_MB / d xi_MB
-            SH(V3X2, t, l) = F.Nd[3 * D + MA][o];    // d vel_D / d xi_MA
-            SH(V3X3, t, l) = F.Nd[3 * D + MB][o];    // d vel_D / d xi_MB
+            SH(V3X0, t, l) = ndv<MIXED>(F, 3 * MA + MA, o);   // d vel_MA / d xi_MA
+            SH(V3X1, t, l) = ndv<MIXED>(F, 3 * MB + MB, o);   // d vel_MB / d xi_MB
+            SH(V3X2, t, l) = ndv<MIXED>(F, 3 * D + MA, o);    // d vel_D / d xi_MA
+            SH(V3X3, t, l) = ndv<MIXED>(F, 3 * D + MB, o);    // d vel_D / d xi_MB
             double mj = mu * J;
             SH(V3F1, t, l) = mj * (cd * cd);
             SH(V3FA, t, l) = mj * (cd * ca);
@@ -876,9 +886,9 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
             SH(V2U, t, l) = Uu[o];
             SH(V2V, t, l) = Vv[o];
             SH(V2T, t, l) = F.T[o];
-            SH(V2XU, t, l) = F.Nd[3 * 0 + E][o];
-            SH(V2XV, t, l) = F.Nd[3 * 1 + E][o];
-            SH(V2XT, t, l) = F.Nd[3 * 3 + E][o];
+            SH(V2XU, t, l) = ndv<MIXED>(F, 3 * 0 + E, o);
+            SH(V2XV, t, l) = ndv<MIXED>(F, 3 * 1 + E, o);
+            SH(V2XT, t, l) = ndv<MIXED>(F, 3 * 3 + E, o);
             SH(V2MJ, t, l) = mu * J;
             SH(V2AX, t, l) = F.m[3 * D + 0][o];
             SH(V2AY, t, l) = F.m[3 * D + 1][o];
@@ -893,21 +903,22 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
             const int jj = T.l0 + lane;                     // lateral axis of the zeta sweep is j
             const long long lb = T.base + (long long)lane * T.sL;   // (i, j, 0)
             const double *vs[4] = {Uu, Vv, Ww, F.T};
-            const double *xs[4] = {F.Nd[3 * MA + MA], F.Nd[3 * MB + MB], F.Nd[3 * D + MA], F.Nd[3 * D + MB]};
+            const int xs[4] = {3 * MA + MA, 3 * MB + MB, 3 * D + MA, 3 * D + MB};
 #pragma unroll
             for (int k2 = 0; k2 < 2; k2++) {
                 int idx = row * 2 + k2;                     // 0..15: side*8 + quantity
                 int side = idx >> 3, qn = idx & 7;
-                const double *src = qn < 4 ? vs[qn] : xs[qn - 4];
                 TS acc = 0;
                 if (qn < 4) {
+                    const double *src = vs[qn];
                     double ref = src[lb + jj];              // value near the stencil centre
 #pragma unroll
                     for (int l = 0; l < 2 * H; l++)
                         acc += (TS)ZD<ORDER>::half(l) * (TS)(src[lb + (jj + l - H + side)] - (MIXED ? ref : 0.0));
                 } else {
 #pragma unroll
-                    for (int l = 0; l < 2 * H; l++) acc += (TS)ZD<ORDER>::interp(l) * (TS)src[lb + (jj + l - H + side)];
+                    for (int l = 0; l < 2 * H; l++)
+                        acc += (TS)ZD<ORDER>::interp(l) * (TS)ndv<MIXED>(F, xs[qn - 4], lb + (jj + l - H + side));
                 }
                 QD(idx, lane) = (double)acc;
             }
@@ -1036,7 +1047,8 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
             const double F1 = SH(V3F1, ts, ln), FA = SH(V3FA, ts, ln), FB = SH(V3FB, ts, ln);
             const double nAA = SH(V3X0, ts, ln), nBB = SH(V3X1, ts, ln);
             const double nDA = SH(V3X2, ts, ln), nDB = SH(V3X3, ts, ln);
-            const double nDD = F.Nd[3 * D + D][o], nAD = F.Nd[3 * MA + D][o], nBD = F.Nd[3 * MB + D][o];
+            const double nDD = ndv<MIXED>(F, 3 * D + D, o), nAD = ndv<MIXED>(F, 3 * MA + D, o);
+            const double nBD = ndv<MIXED>(F, 3 * MB + D, o);
             double hD = nDD * (t43 * F1) + nAA * (-t23 * FA) + nBB * (-t23 * FB);
             double hA = nAD * F1 + nDA * FA;
             double hB = nBD * F1 + nDB * FB;
@@ -1054,7 +1066,7 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
             double av[2] = {ax, ay};
             double N[2][2];   // N[var][dir]
             N[0][E] = SH(V2XU, ts, ln); N[1][E] = SH(V2XV, ts, ln);
-            N[0][D] = F.Nd[3 * 0 + D][o]; N[1][D] = F.Nd[3 * 1 + D][o];
+            N[0][D] = ndv<MIXED>(F, 3 * 0 + D, o); N[1][D] = ndv<MIXED>(F, 3 * 1 + D, o);
             double hsum[2] = {0, 0};
 #pragma unroll
             for (int m = 0; m < 2; m++) {

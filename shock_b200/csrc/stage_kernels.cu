@@ -44,12 +44,12 @@ __global__ void k_prim(Grid G, Phys P, const double *__restrict__ R, const doubl
     if (o < G.NG) prim_body<DIM>(G, P, o, R, U, V, W, E, p, T, c, mu);
 }
 
-template <int DIM, int ORDER>
+template <int DIM, int ORDER, bool MIXED>
 __global__ void k_nodal(Grid G, const double *__restrict__ U, const double *__restrict__ V,
                         const double *__restrict__ W, const double *__restrict__ T, Fields F)
 {
     long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (o < G.NG) nodal_body<DIM, ORDER>(G, o, U, V, W, T, F);
+    if (o < G.NG) nodal_body<DIM, ORDER, MIXED>(G, o, U, V, W, T, F);
 }
 
 template <int DIM, int ORDER, int D, bool MIXED>
@@ -132,13 +132,17 @@ void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const F
         k_prim<2><<<blocks_for(G.NG, 256), 256, 0, s>>>(G, P, U[0], U[1], U[2], U[3], U[4], F.p, F.T, F.c, F.mu);
 }
 
-void launch_nodal(const Grid &G, const double *const U[5], const Fields &F, cudaStream_t s)
+void launch_nodal(const Grid &G, int precision, const double *const U[5], const Fields &F, cudaStream_t s)
 {
-    unsigned nb = blocks_for(G.NG, 256);
-    if (G.dim == 3 && G.order == 5) k_nodal<3, 5><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F);
-    else if (G.dim == 3) k_nodal<3, 9><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F);
-    else if (G.order == 5) k_nodal<2, 5><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F);
-    else k_nodal<2, 9><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F);
+    const unsigned nb = blocks_for(G.NG, 256);
+#define N(DIM, ORD)                                                                                    \
+    if (G.dim == DIM && G.order == ORD) {                                                              \
+        if (precision == SHOCK_MIXED) k_nodal<DIM, ORD, true><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F); \
+        else k_nodal<DIM, ORD, false><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F);                 \
+        return;                                                                                        \
+    }
+    N(3, 5) N(3, 9) N(2, 5) N(2, 9)
+#undef N
 }
 
 template <int DIM, int D, int TLN = TL>

@@ -110,7 +110,10 @@ extern "C" int shock_rhs_static(const shock_params *p, const double *geom13, dou
     F.T = scratch + ng;
     F.c = scratch + 2 * ng;
     F.mu = scratch + 3 * ng;
-    for (int f = 0; f < 12; f++) F.Nd[f] = p->inviscid ? nullptr : scratch + (4 + f) * ng;
+    for (int f = 0; f < 12; f++) {
+        F.Nd[f] = p->inviscid ? nullptr : scratch + (4 + f) * ng;
+        F.Ndf[f] = reinterpret_cast<float *>(F.Nd[f]);
+    }
 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     double *U[5];
@@ -124,7 +127,7 @@ extern "C" int shock_rhs_static(const shock_params *p, const double *geom13, dou
     if (!p->inviscid) CKS(cudaMemsetAsync(scratch + 4 * ng, 0, sizeof(double) * 12 * ng, s));
     launch_ghosts(G, U, s);
     launch_prim(G, P, cU, F, s);
-    if (!p->inviscid) launch_nodal(G, cU, F, s);
+    if (!p->inviscid) launch_nodal(G, p->precision, cU, F, s);
     for (int d = 0; d < p->dim; d++) launch_weno(G, P, p->precision, d, d == 0, cU, F, s);
     if (!p->inviscid)
         for (int d = 0; d < p->dim; d++) launch_viscous(G, P, p->precision, d, cU, F, s);
