@@ -207,6 +207,12 @@ int shock_batch_dims(const shock_batch *b, int member, int out6[6]);
 int shock_batch_download_state(shock_batch *b, int member, double *prim5);
 int shock_batch_set_tuning(shock_batch *b, const shock_batch_tuning *t);
 int shock_batch_get_tuning(const shock_batch *b, shock_batch_tuning *t);
+/* Check of the persistent stage kernel's bounded waits: launches one CTA per
+ * SM at a grid barrier that one CTA never reaches; every wait must give up
+ * after timeout_ms (at most 1000) and report it.  Returns SHOCK_ETIMEOUT
+ * when the waits ended as designed; *elapsed_ms receives the device time. */
+int shock_batch_check_barrier_timeout(int device, double timeout_ms, double *elapsed_ms);
+
 /* Active members, arena bytes in use / total, kernel launches per step. */
 int shock_batch_info(const shock_batch *b, int *members, size_t *arena_used, size_t *arena_total,
                      int *kernels_per_step);

@@ -83,7 +83,7 @@ def lib():
                          "shock_batch_add", "shock_batch_remove", "shock_batch_step", "shock_batch_step_async",
                          "shock_batch_sync", "shock_batch_last_ms", "shock_batch_steps_left",
                          "shock_batch_dims", "shock_batch_download_state", "shock_batch_set_tuning",
-                         "shock_batch_get_tuning", "shock_batch_info", "shock_server_create",
+                         "shock_batch_get_tuning", "shock_batch_info", "shock_batch_check_barrier_timeout", "shock_server_create",
                          "shock_server_set_tuning", "shock_server_submit", "shock_server_wait",
                          "shock_server_result", "shock_server_get_stats", "shock_server_destroy"):
                 getattr(L, name).restype = C.c_int

@@ -164,3 +164,18 @@ def test_batch_short_tiles_match_long_tiles(dim, order, precision):
             tol = max(tol, 1e-6)      # SHOCK's own FP64/80-bit RHS differ by ~1e-6 on the WENO9 vortex
         idx = [0, 1, 2, 3, 4] if dim == 3 else [0, 1, 2, 4]   # w is identically zero in 2D
         assert (err[idx] <= tol).all(), (c.name, err)
+
+
+def test_persistent_barrier_wait_is_bounded():
+    """A grid barrier that one CTA never reaches: every wait gives up after the
+    limit, the error comes back as SHOCK_ETIMEOUT, and the device stays usable."""
+    import ctypes as C
+    L = shock_b200.lib()
+    L.shock_batch_check_barrier_timeout.argtypes = [C.c_int, C.c_double, C.POINTER(C.c_double)]
+    ms = C.c_double()
+    rc = L.shock_batch_check_barrier_timeout(0, 20.0, C.byref(ms))
+    assert rc == -5, L.shock_last_error().decode()
+    assert 15.0 <= ms.value < 1000.0, ms.value
+    c = _vortices([32])[0]
+    ok, err = _close(real(c, _alone(c, 2)), real(c, _solo(c, 2)))
+    assert ok, err
