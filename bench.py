@@ -186,6 +186,10 @@ def flush_l2(torch, buf):
 # ---------------------------------------------------------------------------
 def _ref_worker(args):
     name, nsteps = args
+    # SHOCK's own code reports its set-up on stdout; keep the bench's stdout
+    # to the one JSON line
+    devnull = os.open(os.devnull, os.O_WRONLY)
+    os.dup2(devnull, 1)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from refbind import RefSolver
     if isinstance(name, tuple):          # (builder name, kwargs) of shock_b200.cases
