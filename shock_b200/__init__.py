@@ -56,6 +56,14 @@ class Params(C.Structure):
     ]
 
 
+def params_from_ini(path: str, base: Params = None) -> Params:
+    """shock_params with the config.ini keys of SHOCK's hot path read from path
+    (other fields taken from base, or zero)."""
+    p = Params() if base is None else base
+    _check(lib().shock_params_from_ini(os.fsencode(path), C.byref(p)))
+    return p
+
+
 def build_library(force: bool = False) -> str:
     """Compile shock_b200/csrc into libshock_b200.so (nvcc, sm_100a)."""
     if force or not os.path.exists(LIB_PATH):
@@ -83,7 +91,8 @@ def lib():
                          "shock_batch_add", "shock_batch_remove", "shock_batch_step", "shock_batch_step_async",
                          "shock_batch_sync", "shock_batch_last_ms", "shock_batch_steps_left",
                          "shock_batch_dims", "shock_batch_download_state", "shock_batch_set_tuning",
-                         "shock_batch_get_tuning", "shock_batch_info", "shock_batch_check_barrier_timeout", "shock_server_create",
+                         "shock_batch_get_tuning", "shock_batch_info", "shock_batch_check_barrier_timeout",
+                         "shock_params_from_ini", "shock_server_create",
                          "shock_server_set_tuning", "shock_server_submit", "shock_server_wait",
                          "shock_server_result", "shock_server_get_stats", "shock_server_destroy"):
                 getattr(L, name).restype = C.c_int
