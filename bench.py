@@ -521,6 +521,24 @@ def run_batch(args, world, rank, local, barrier, max_over_ranks):
     worst = np.zeros(5)
     for c, sm, s64 in zip(cs, out[shock_b200.SHOCK_MIXED]["states"], out[shock_b200.SHOCK_FP64]["states"]):
         worst = np.maximum(worst, _l2_conserved(c, sm, s64))
+    # the persistent form (one cooperative launch per RK stage) beside the
+    # tuner's choice, mixed precision
+    bp = shock_b200.Batch(2, 5, shock_b200.SHOCK_MIXED, arena_bytes=arena, device=local)
+    for c in cs:
+        bp.add(c, args.warmup + args.steps)
+    bp.set_tuning(persistent=1, blocks_per_sm=1)
+    occ = bp.tuning().max_blocks_per_sm
+    bp.set_tuning(persistent=1, blocks_per_sm=occ, chunk=1024)
+    bp.step(args.warmup)
+    barrier()
+    pers_ms = 0.0
+    for _ in range(args.steps):
+        bp.step(1)
+        pers_ms += bp.last_ms()
+    pers_launches = bp.info()["kernels_per_step"]
+    bp.close()
+    pers_ms = max_over_ranks(pers_ms)
+
     mixed_ms = out[shock_b200.SHOCK_MIXED]["ms"]
     fp64_ms = out[shock_b200.SHOCK_FP64]["ms"]
     value = pts * nstage * args.steps * world / (mixed_ms * 1e-3)
@@ -569,6 +587,9 @@ def run_batch(args, world, rank, local, barrier, max_over_ranks):
                        "launches_per_step": mix["info"]["kernels_per_step"]},
             "fp64": {"value": fp64_value, "ms_per_step": fp64_ms / args.steps,
                      "tuning": out[shock_b200.SHOCK_FP64]["tuning"]},
+            "persistent_form": {"value": pts * nstage * args.steps * world / (pers_ms * 1e-3),
+                                "ms_per_step": pers_ms / args.steps, "launches_per_step": pers_launches,
+                                "note": "one cooperative launch per RK stage with grid barriers, mixed"},
             "mixed_speedup": fp64_ms / mixed_ms,
             "mixed_vs_fp64_l2_max_over_members": {"rho": worst[0], "rho_u": worst[1], "rho_v": worst[2],
                                                   "rho_e": worst[4]},

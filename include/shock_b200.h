@@ -139,6 +139,13 @@ int shock_sync(shock_ctx *ctx);
  * *bad receives the count.  Returns SHOCK_ENAN when bad > 0. */
 int shock_check_nan(shock_ctx *ctx, int *bad);
 
+/* Post-processing values of the current state, computed on the device as
+ * CalcValuesForPost does for sampling and export (src/Functions.c:3687-3761,
+ * CalcLambda2 :5846-6071): out3 = 3*NG doubles, Mach number, |grad rho| and
+ * lambda2 (zero in 2D) on the real points, zero elsewhere.  Like SHOCK it
+ * uses the pressure and ghost values of the last stage's input. */
+int shock_post(shock_ctx *ctx, double *out3);
+
 /* Geometry after set-up: x,y,z,J,xi_x..zeta_z (13*NG doubles). */
 int shock_geometry(shock_ctx *ctx, double *out13);
 

@@ -297,6 +297,18 @@ void ref_mms_source(double *js5)
     copy_out(js5, &Qf, n);
 }
 
+/* SHOCK's own post-processing of U_lastStep as done for sampling
+ * (SHOCK.c:705 -> CalcValuesForPost, src/Functions.c:3687-3761); out3 =
+ * MachNumber, gradRho, Lambda2 (3*NG). */
+void ref_post(double *out3)
+{
+    CalcValuesForPost(&cfg, &msh, &U_last);
+    FLT *f[3] = {U_last.MachNumber, U_last.gradRho, U_last.Lambda2};
+    int n = NG;
+    for (int a = 0; a < 3; a++)
+        for (int o = 0; o < n; o++) out3[(size_t)a * n + o] = (double)f[a][o];
+}
+
 void ref_free(void)
 {
     if (!live) return;

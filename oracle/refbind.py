@@ -122,6 +122,13 @@ class RefSolver:
         self.lib.ref_get_geom(_ptr(g))
         return g.reshape((13,) + self.shape)
 
+    def post(self) -> np.ndarray:
+        """SHOCK's CalcValuesForPost on U_lastStep: Mach number, |grad rho|,
+        lambda2 (3 fields, ghosted)."""
+        q = np.zeros(3 * self.n)
+        self.lib.ref_post(_ptr(q))
+        return q.reshape((3,) + self.shape)
+
     def mms_source(self) -> np.ndarray:
         """J*S of the reference manufactured-solution source (5 fields)."""
         q = np.zeros(5 * self.n)

@@ -92,7 +92,7 @@ def lib():
                          "shock_batch_sync", "shock_batch_last_ms", "shock_batch_steps_left",
                          "shock_batch_dims", "shock_batch_download_state", "shock_batch_set_tuning",
                          "shock_batch_get_tuning", "shock_batch_info", "shock_batch_check_barrier_timeout",
-                         "shock_params_from_ini", "shock_server_create",
+                         "shock_params_from_ini", "shock_post", "shock_server_create",
                          "shock_server_set_tuning", "shock_server_submit", "shock_server_wait",
                          "shock_server_result", "shock_server_get_stats", "shock_server_destroy"):
                 getattr(L, name).restype = C.c_int
@@ -242,6 +242,14 @@ class Solver:
         a = np.ascontiguousarray(prim5, np.float64).ravel()
         assert a.size == 5 * self.n
         _check(self.lib.shock_upload_state(self.h, _ptr(a)))
+
+    def post(self) -> np.ndarray:
+        """Mach number, |grad rho| and lambda2 of the current state (3 fields,
+        ghosted; real points set), computed on the device as SHOCK's
+        CalcValuesForPost does for sampling."""
+        q = np.zeros(3 * self.n)
+        _check(self.lib.shock_post(self.h, _ptr(q)))
+        return q.reshape((3,) + self.shape)
 
     def geometry(self) -> np.ndarray:
         g = np.zeros(13 * self.n)

@@ -69,6 +69,7 @@ struct shock_ctx {
     size_t pool_bytes = 0;
     double *buf[3][5] = {};
     int un = 0;          // buffer holding U_lastStep (== running state between steps)
+    int last_in = 0;     // input buffer of the last stage run (its ghosts are U_lastStep's)
     bool has_source = false;
     RKCoef rk[4]{};
     cudaGraphExec_t step_graph[3] = {nullptr, nullptr, nullptr};
@@ -154,6 +155,18 @@ static void enqueue_step(shock_ctx *c, int un, int &nk)
         nk++;
         cur = out;
     }
+}
+
+// Input buffer of the last stage of a step that starts from buffer un.
+static int last_stage_input(const shock_ctx *c, int un)
+{
+    int cur = un;
+    for (int st = 0; st + 1 < c->p.time_order; st++) {
+        int out = 0;
+        while (out == un || out == cur) out++;
+        cur = out;
+    }
+    return cur;
 }
 
 static int final_buffer(const shock_ctx *c, int un)
@@ -291,6 +304,7 @@ int shock_set_dirichlet(shock_ctx *c, const double *exact9)
         for (int f = 0; f < 5; f++)
             CK(cudaMemcpy(c->buf[b][f], exact9 + (size_t)f * c->G.NG, nb, cudaMemcpyHostToDevice));
     c->un = 0;
+    c->last_in = 0;
     return SHOCK_OK;
 }
 
@@ -358,6 +372,7 @@ int shock_upload_state(shock_ctx *c, const double *prim5)
     CK(cudaSetDevice(c->device));
     size_t nb = sizeof(double) * c->G.NG;
     c->un = 0;
+    c->last_in = 0;
     for (int f = 0; f < 5; f++)
         CK(cudaMemcpyAsync(c->buf[0][f], prim5 + (size_t)f * c->G.NG, nb, cudaMemcpyHostToDevice, c->stream));
     // The stage buffers are written before they are read except for the
@@ -418,6 +433,7 @@ int shock_step_async(shock_ctx *c, int nsteps)
             c->kernels_per_step = nk;
         }
         CK(cudaGraphLaunch(c->step_graph[un], c->stream));
+        c->last_in = last_stage_input(c, un);
         c->un = final_buffer(c, un);
     }
     CK(cudaEventRecord(c->ev1, c->stream));
@@ -452,6 +468,23 @@ int shock_check_nan(shock_ctx *c, int *bad)
     CK(cudaStreamSynchronize(c->stream));
     *bad = (int)h;
     return h ? fail(SHOCK_ENAN, "%u non-finite densities", h) : SHOCK_OK;
+}
+
+int shock_post(shock_ctx *c, double *out3)
+{
+    if (!c || !out3) return fail(SHOCK_EINVAL, "null argument");
+    CK(cudaSetDevice(c->device));
+    const double *fin[5], *lst[5];
+    for (int q = 0; q < 5; q++) { fin[q] = c->buf[c->un][q]; lst[q] = c->buf[c->last_in][q]; }
+    // Q is free between steps: it holds the three outputs
+    for (int q = 0; q < 3; q++) CK(cudaMemsetAsync(c->F.Q[q], 0, sizeof(double) * c->G.NG, c->stream));
+    launch_post(c->G, c->p.mach, fin, lst, c->F.p, c->F, c->F.Q[0], c->F.Q[1], c->F.Q[2], c->stream);
+    CK(cudaGetLastError());
+    const size_t nb = sizeof(double) * c->G.NG;
+    for (int q = 0; q < 3; q++)
+        CK(cudaMemcpyAsync(out3 + (size_t)q * c->G.NG, c->F.Q[q], nb, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SHOCK_OK;
 }
 
 int shock_geometry(shock_ctx *c, double *out13)

@@ -173,6 +173,8 @@ void launch_rk(const Grid &G, const RKCoef &rk, double tau, const double *const 
 void launch_copy_state(const Grid &G, const double *const src[5], double *const dst[5], cudaStream_t s);
 void launch_nan_check(const Grid &G, const double *rho, unsigned int *flag, cudaStream_t s);
 void launch_add_source(const Grid &G, const Fields &F, cudaStream_t s);
+void launch_post(const Grid &G, double mach, const double *const fin[5], const double *const lst[5],
+                 const double *p, const Fields &F, double *ma, double *gr, double *l2, cudaStream_t s);
 void prepare_kernels();
 int report_error(int code, const char *fmt, ...);   // sets shock_last_error, returns code
 double fma_probe(int fp64, int sms, cudaStream_t s);

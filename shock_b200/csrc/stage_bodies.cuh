@@ -1147,6 +1147,108 @@ __device__ __forceinline__ void rk_body(const Grid &G, const RKCoef &K, double t
 }
 
 
+// ---------------------------------------------------------------------------
+// Post-processing values of the sampled state (src/Functions.c:3687-3761,
+// CalcLambda2 :5846-6071) at one real point o: Mach number, magnitude of the
+// density gradient and (3D) lambda2.  SHOCK samples U_lastStep, whose real
+// points are the final state while its ghost points and pressure are those
+// of the last stage's halo exchange and CalcValues; the caller passes the
+// final buffer (fin) and the last stage's input buffer (lst) for the ghosts.
+// ---------------------------------------------------------------------------
+template <int DIM, int ORDER>
+__device__ __forceinline__ void post_body(const Grid &G, double mach, const double *const fin[5],
+                                          const double *const lst[5], const double *p, const Fields &F, int i,
+                                          int j, int k, double *ma, double *gr, double *l2)
+{
+    const long long o = (long long)i * G.st[0] + (long long)j * G.st[1] + k;
+    // value of field f at the point shifted by s along axis a (the centre is real)
+    auto at = [&](int f, int a, int s) -> double {
+        const int c = (a == 0 ? i : a == 1 ? j : k) + s;
+        const bool real = c >= G.g && c < G.g + G.n[a];
+        const long long q = o + (long long)s * G.st[a];
+        return real ? fin[f][q] : lst[f][q];
+    };
+    const double u = fin[1][o], v = fin[2][o], w = fin[3][o], rho = fin[0][o];
+    ma[o] = (sqrt(u * u + v * v + w * w)) / sqrt(p[o] / rho) * mach;
+    const double dxi = 1.0, deta = 1.0, dzeta = 1.0;   // deltaXi etc., src/Functions.c:1957
+    const double a = (0.5 * at(0, 0, 1) - 0.5 * at(0, 0, -1)) / dxi;
+    const double b = (0.5 * at(0, 1, 1) - 0.5 * at(0, 1, -1)) / deta;
+    if (DIM == 2) {
+        const double t0 = a * F.m[0][o], t1 = b * F.m[3][o], t2 = a * F.m[1][o], t3 = b * F.m[4][o];
+        gr[o] = sqrt(t0 * t0 + t1 * t1 + t2 * t2 + t3 * t3);
+        return;
+    }
+    const double cz = (0.5 * at(0, 2, 1) - 0.5 * at(0, 2, -1)) / dzeta;
+    double sq = 0.0;
+    const double dd[3] = {a, b, cz};
+#pragma unroll
+    for (int comp = 0; comp < 3; comp++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            const double t = dd[d] * F.m[3 * d + comp][o];
+            sq = sq + t * t;
+        }
+    gr[o] = sqrt(sq);
+
+    // lambda2: velocity gradient from the mid-point interpolation stencil
+    constexpr int H = (ORDER + 1) / 2;
+    double dv[3][3];   // dv[var][dir] = d(u,v,w)/d(xi,eta,zeta)
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+#pragma unroll
+        for (int d = 0; d < 3; d++) {
+            double lo = 0.0, hi = 0.0;
+#pragma unroll
+            for (int m = 0; m <= ORDER; m++) {
+                lo += ZD<ORDER>::interp(m) * at(1 + q, d, m - H);
+                hi += ZD<ORDER>::interp(m) * at(1 + q, d, m - H + 1);
+            }
+            dv[q][d] = hi - lo;
+        }
+    double g[3][3];   // g[var][x]
+#pragma unroll
+    for (int q = 0; q < 3; q++)
+#pragma unroll
+        for (int x = 0; x < 3; x++)
+            g[q][x] = dv[q][0] * F.m[0 + x][o] + dv[q][1] * F.m[3 + x][o] + dv[q][2] * F.m[6 + x][o];
+    const double udx = g[0][0], udy = g[0][1], udz = g[0][2];
+    const double vdx = g[1][0], vdy = g[1][1], vdz = g[1][2];
+    const double wdx = g[2][0], wdy = g[2][1], wdz = g[2][2];
+    const double om12 = 0.5 * (udy - vdx), om13 = 0.5 * (udz - wdx), om23 = 0.5 * (vdz - wdy);
+    const double s11 = 0.5 * (udx), s12 = 0.5 * (udy + vdx), s13 = 0.5 * (udz + wdx);
+    const double s22 = 0.5 * (vdy), s23 = 0.5 * (vdz + wdy), s33 = 0.5 * (wdz);
+    const double oo11 = -om12 * om12 - om13 * om13, oo12 = -om13 * om23, oo13 = om12 * om23;
+    const double oo22 = -om12 * om12 - om23 * om23, oo23 = -om12 * om13, oo33 = -om13 * om13 - om23 * om23;
+    const double ss11 = s11 * s11 + s12 * s12 + s13 * s13, ss12 = s11 * s12 + s12 * s22 + s13 * s23;
+    const double ss13 = s11 * s13 + s12 * s23 + s13 * s33, ss22 = s12 * s12 + s22 * s22 + s23 * s23;
+    const double ss23 = s12 * s13 + s22 * s23 + s23 * s33, ss33 = s13 * s13 + s23 * s23 + s33 * s33;
+    const double a11 = ss11 + oo11, a12 = ss12 + oo12, a13 = ss13 + oo13;
+    const double a22 = ss22 + oo22, a23 = ss23 + oo23, a33 = ss33 + oo33;
+    // eigenvalues of the symmetric matrix from its characteristic cubic
+    const double f1 = -a11 - a22 - a33;
+    const double f2 = -a23 * a23 - a12 * a12 - a13 * a13 + a11 * a33 + a11 * a22 + a22 * a33;
+    const double f3 = -a11 * a22 * a33 + a11 * a23 * a23 + a22 * a13 * a13 + a33 * a12 * a12 - 2. * a12 * a13 * a23;
+    const double pp = -f1 * f1 / 3. + f2, qq = 2. * f1 * f1 * f1 / 27. - f1 * f2 / 3. + f3;
+    double rrr = pp < 0. ? -pp : pp;
+    rrr = sqrt(rrr / 3.);
+    const double al = acos(qq / (2. * rrr * rrr * rrr));
+    const double pi = 3.14159265358979323846264338327950288;
+    const double lam1 = -2. * rrr * cos(al / 3.) - f1 / 3;
+    const double lam2 = 2. * rrr * cos(pi / 3. - al / 3.) - f1 / 3;
+    const double lam3 = 2. * rrr * cos(pi / 3. + al / 3.) - f1 / 3;
+    double lamax = lam2 >= lam1 ? lam2 : lam1;
+    if (lam3 >= lamax) lamax = lam3;
+    double lamin = lam2 <= lam1 ? lam2 : lam1;
+    if (lam3 <= lamin) lamin = lam3;
+    double lam = 0.;
+    if (lam1 == lam2 || lam2 == lam3) lam = lam2;
+    if (lam1 > lamin && lam1 < lamax) lam = lam1;
+    else if (lam2 > lamin && lam2 < lamax) lam = lam2;
+    else if (lam3 > lamin && lam3 < lamax) lam = lam3;
+    if (lam >= 0.) lam = 0.;
+    l2[o] = lam;
+}
+
 // Dynamic shared memory of the sweep bodies.
 template <int DIM, int ORDER, bool MIXED, int TLN = TL>
 constexpr size_t weno_smem_bytes()

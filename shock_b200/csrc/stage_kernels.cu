@@ -224,6 +224,32 @@ void launch_rk(const Grid &G, const RKCoef &rk, double tau, const double *const 
                                           has_source ? 1 : 0);
 }
 
+template <int DIM, int ORDER>
+__global__ void __launch_bounds__(128) k_post(Grid G, double mach, StageIn fin, StageIn lst, const double *p, Fields F,
+                                              double *ma, double *gr, double *l2)
+{
+    const int nf = DIM == 3 ? G.n[2] : G.n[1];
+    const int f = blockIdx.x * blockDim.x + threadIdx.x;
+    if (f >= nf) return;
+    const int i = (DIM == 3 ? blockIdx.z : blockIdx.y) + G.g;
+    const int j = DIM == 3 ? blockIdx.y + G.g : f + G.g;
+    const int k = DIM == 3 ? f + G.g : 0;
+    post_body<DIM, ORDER>(G, mach, fin.U, lst.U, p, F, i, j, k, ma, gr, l2);
+}
+
+void launch_post(const Grid &G, double mach, const double *const fin[5], const double *const lst[5],
+                 const double *p, const Fields &F, double *ma, double *gr, double *l2, cudaStream_t s)
+{
+    StageIn a, b;
+    for (int c = 0; c < 5; c++) { a.U[c] = fin[c]; b.U[c] = lst[c]; }
+    const int nf = G.dim == 3 ? G.n[2] : G.n[1];
+    const dim3 grid((nf + 127) / 128, G.dim == 3 ? G.n[1] : G.n[0], G.dim == 3 ? G.n[0] : 1);
+#define PST(DIM, ORD) \
+    if (G.dim == DIM && G.order == ORD) { k_post<DIM, ORD><<<grid, 128, 0, s>>>(G, mach, a, b, p, F, ma, gr, l2); return; }
+    PST(3, 5) PST(3, 9) PST(2, 5) PST(2, 9)
+#undef PST
+}
+
 void launch_add_source(const Grid &G, const Fields &F, cudaStream_t s)
 {
     k_add_source<<<blocks_for(G.NG, 256), 256, 0, s>>>(G, F);

@@ -200,3 +200,24 @@ def test_mms_design_order(order, sizes, min_order):
     p_ref = np.log2(errs_ref[0] / errs_ref[1])
     assert (p_gpu >= min_order).all(), p_gpu
     assert np.abs(p_gpu - p_ref).max() < 0.02, (p_gpu, p_ref)
+
+
+@pytest.mark.parametrize("case", [
+    cases.smooth_random(3, 5, (16, 14, 15), seed=7, stretch=0.05),
+    cases.smooth_random(3, 9, (14, 12, 16), seed=8),
+    cases.isentropic_vortex(32, 3.0, 0.5),
+], ids=lambda c: c.name)
+def test_post_matches_reference(case):
+    """Device post-processing (Mach number, |grad rho|, lambda2) against
+    SHOCK's own CalcValuesForPost on U_lastStep after two steps.  lambda2
+    comes from the trigonometric roots of a cubic, whose libm and CUDA values
+    differ in the last bits, so it is compared at 1e-9 of its maximum."""
+    r = RefSolver(case)
+    r.steps(2)
+    ref = real(case, r.post())
+    s = _solver(case)
+    s.steps(2)
+    got = real(case, s.post())
+    err = rel_err(got, ref)
+    assert err[0] <= RHS_TOL and err[1] <= RHS_TOL, err
+    assert err[2] <= 1e-9, err
