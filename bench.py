@@ -405,7 +405,7 @@ def main():
     for _ in range(args.steps):
         solver.set_state(host.reshape((5,) + solver.shape))
         solver.steps(1)
-        host[:] = solver.state().ravel()
+        solver.state(out=host)
     t1 = time.perf_counter()
     barrier()
     e2e_s = max_over_ranks(t1 - t0)

@@ -232,9 +232,11 @@ class Solver:
         _check(self.lib.shock_last_step_ms(self.h, C.byref(v)))
         return v.value
 
-    def state(self) -> np.ndarray:
-        """rho,u,v,w,e (ghosted)."""
-        s = np.zeros(5 * self.n)
+    def state(self, out: np.ndarray = None) -> np.ndarray:
+        """rho,u,v,w,e (ghosted).  out: a C-contiguous float64 array of 5*NG
+        values to download into (pinned host memory makes this a direct DMA)."""
+        s = np.zeros(5 * self.n) if out is None else out
+        assert s.dtype == np.float64 and s.flags["C_CONTIGUOUS"] and s.size == 5 * self.n
         _check(self.lib.shock_download_state(self.h, _ptr(s), 0))
         return s.reshape((5,) + self.shape)
 
