@@ -86,6 +86,16 @@ def batch_cases(nmem=256, seed=4):
     return out
 
 
+def measured_traffic(workload, kernel, precision="fp64"):
+    """DRAM bytes (read + write) of one launch of `kernel` on `workload`, from
+    the ncu capture recorded in shock_b200/roofline.json (None if absent)."""
+    path = os.path.join(ROOT, "shock_b200", "roofline.json")
+    with open(path) as f:
+        t = json.load(f).get("traffic", {})
+    e = t.get(workload, {}).get(precision, {}).get(kernel)
+    return None if e is None else e["bytes"]
+
+
 def flops_per_cell_stage(case):
     path = os.path.join(ROOT, "shock_b200", "roofline.json")
     with open(path) as f:
@@ -421,7 +431,9 @@ def main():
     achieved = dom_flops / (dom[1] * 1e-3) / 1e12 if dom[1] > 0 else None
     roofline = {"bound": "fp64", "kernel": dom[0], "achieved": achieved, "peak": peaks["fp64_tflops"],
                 "unit": "TFLOP/s", "frac": (achieved / peaks["fp64_tflops"]) if achieved else None,
-                "traffic": None,
+                "traffic": measured_traffic(args.workload, dom[0]),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
+                                  "shock_b200/roofline.json (command recorded there)",
                 "peak_source": "measured on this GPU by shock_measure_fma_peak (register-only FP64 FMA loop)",
                 "flops_per_launch": dom_flops, "launch_ms": dom[1],
                 "step_fp64_tflops": fl["total"] * stage_cells * args.steps / (ms64 * 1e-3) / 1e12,
