@@ -148,15 +148,34 @@ __device__ __forceinline__ void run_item(int ph, const Member &M, const BatchIte
         }
         break;
     }
-    case PH_PRIM:
+    case PH_PRIM: {
+        // four points per thread: all loads before the stores
+        const long long o0 = (long long)it.a * chunk;
+        constexpr int NB = 4;
+        for (int j0 = tid; j0 < chunk; j0 += NB * NTHR) {
+            double v[NB][5];
+            long long oo[NB];
+#pragma unroll
+            for (int b = 0; b < NB; b++) {
+                oo[b] = o0 + j0 + b * NTHR;
+                if (j0 + b * NTHR < chunk && oo[b] < M.G.NG)
+#pragma unroll
+                    for (int f = 0; f < 5; f++) v[b][f] = (DIM == 2 && f == 3) ? 0.0 : U[f][oo[b]];
+            }
+#pragma unroll
+            for (int b = 0; b < NB; b++)
+                if (j0 + b * NTHR < chunk && oo[b] < M.G.NG)
+                    prim_store<DIM>(M.P, oo[b], v[b][0], v[b][1], v[b][2], v[b][3], v[b][4], M.F.p, M.F.T, M.F.c,
+                                    M.F.mu);
+        }
+        break;
+    }
     case PH_NODAL: {
         const long long o0 = (long long)it.a * chunk;
         for (int j = tid; j < chunk; j += NTHR) {
             const long long o = o0 + j;
             if (o >= M.G.NG) break;
-            if (ph == PH_PRIM)
-                prim_body<DIM>(M.G, M.P, o, U[0], U[1], U[2], U[3], U[4], M.F.p, M.F.T, M.F.c, M.F.mu);
-            else nodal_body<DIM, ORDER, MIXED>(M.G, o, U[1], U[2], U[3], M.F.T, M.F);
+            nodal_body<DIM, ORDER, MIXED>(M.G, o, U[1], U[2], U[3], M.F.T, M.F);
         }
         break;
     }
@@ -177,11 +196,26 @@ __device__ __forceinline__ void run_item(int ph, const Member &M, const BatchIte
         for (int c = 0; c < 5; c++) in.U[c] = U[c];
         const int nreal = M.G.n[0] * M.G.n[1] * (DIM == 3 ? M.G.n[2] : 1);
         const int t0 = it.a * chunk;
-        for (int j = tid; j < chunk; j += NTHR) {
-            const int t = t0 + j;
-            if (t >= nreal) break;
-            rk_body<DIM>(M.G, K, M.tau, in, M.F, M.buf[out][0], M.buf[out][1], M.buf[out][2], M.buf[out][3],
-                         M.buf[out][4], 0, t, stage == 0);
+        // two points per thread: both points' inputs loaded before the stores
+        constexpr int NB = 2;
+        const Grid &G = M.G;
+        for (int j0 = tid; j0 < chunk; j0 += NB * NTHR) {
+            RKIn x[NB];
+            long long oo[NB];
+            bool ok[NB];
+#pragma unroll
+            for (int b = 0; b < NB; b++) {
+                const int t = t0 + j0 + b * NTHR;
+                ok[b] = (j0 + b * NTHR < chunk) && t < nreal;
+                int i, j, k;
+                if (DIM == 3) { k = t % G.n[2]; const int rr = t / G.n[2]; j = rr % G.n[1]; i = rr / G.n[1]; }
+                else { k = 0; j = t % G.n[1]; i = t / G.n[1]; }
+                oo[b] = (long long)(i + G.g) * G.st[0] + (long long)(j + G.g) * G.st[1] + (DIM == 3 ? k + G.g : 0);
+                if (ok[b]) rk_load<DIM>(in, M.F, 0, oo[b], stage == 0, x[b]);
+            }
+#pragma unroll
+            for (int b = 0; b < NB; b++)
+                if (ok[b]) rk_finish<DIM>(K, M.tau, M.F, M.buf[out], oo[b], x[b]);
         }
         break;
     }

@@ -138,12 +138,23 @@ Class *get_class(shock_server *s, const shock_params &p, int &rc)
     rc = batch_create_in(p.dim, p.order, p.precision, p.time_order, s->arena, s->cfg.device, &c.b);
     if (rc) return nullptr;
     auto t = s->tunings.find(key);
+    shock_batch_tuning tu{};
     if (t != s->tunings.end()) {
-        rc = shock_batch_set_tuning(c.b, &t->second);
-        if (rc) {
-            shock_batch_destroy(c.b);
-            return nullptr;
-        }
+        tu = t->second;
+    } else {
+        // default: one launch per phase, so the classes' streams can share
+        // the SMs (a cooperative per-stage launch needs the whole GPU)
+        shock_batch_get_tuning(c.b, &tu);
+        tu.persistent = 0;
+        tu.blocks_per_sm = 1;
+        shock_batch_set_tuning(c.b, &tu);
+        shock_batch_get_tuning(c.b, &tu);
+        tu.blocks_per_sm = tu.max_blocks_per_sm < 2 ? tu.max_blocks_per_sm : 2;
+    }
+    rc = shock_batch_set_tuning(c.b, &tu);
+    if (rc) {
+        shock_batch_destroy(c.b);
+        return nullptr;
     }
     return &(s->classes[key] = c);
 }

@@ -103,18 +103,26 @@ __device__ __forceinline__ void ghost_body(const Grid &G, long long o, double *r
 // prim: CalcValues (p with fabs, T = |p/rho|, c, Sutherland mu or mu = 1).
 // ---------------------------------------------------------------------------
 template <int DIM>
+__device__ __forceinline__ void prim_store(const Phys &P, long long o, double rho, double u, double v, double w,
+                                           double e, double *p, double *T, double *c, double *mu);
+
+template <int DIM>
 __device__ __forceinline__ void prim_body(const Grid &G, const Phys &P, long long o, const double *__restrict__ R,
                                           const double *__restrict__ U, const double *__restrict__ V,
                                           const double *__restrict__ W, const double *__restrict__ E, double *p,
                                           double *T, double *c, double *mu)
 {
     (void)G;
-    double rho = R[o], u = U[o], v = V[o], e = E[o];
+    prim_store<DIM>(P, o, R[o], U[o], V[o], DIM == 3 ? W[o] : 0.0, E[o], p, T, c, mu);
+}
+
+// CalcValues at one point from its rho, u, v, w, e (w unused in 2D).
+template <int DIM>
+__device__ __forceinline__ void prim_store(const Phys &P, long long o, double rho, double u, double v, double w,
+                                           double e, double *p, double *T, double *c, double *mu)
+{
     double q2 = (u * u) + (v * v);
-    if (DIM == 3) {
-        double w = W[o];
-        q2 = q2 + (w * w);
-    }
+    if (DIM == 3) q2 = q2 + (w * w);
     double pp = fabs(rho * (P.gamma - 1.0) / P.ups * (e - 0.5 * q2));
     double pr = pp / rho;
     p[o] = pp;
@@ -1099,6 +1107,49 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
 // RK stage update of the real points (src/Functions.c:2300-2365), with the
 // time-independent source J*S added to Q first.
 // ---------------------------------------------------------------------------
+// Inputs of the RK update of one point, loaded ahead of the arithmetic so
+// that a thread can have several points' loads in flight.
+struct RKIn {
+    double Q[5], Qs[5], U[5], Un[5], J;
+};
+
+template <int DIM>
+__device__ __forceinline__ void rk_load(const StageIn &in, const Fields &F, int has_source, long long o, bool zero_qs,
+                                        RKIn &x)
+{
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+        x.Q[c] = F.Q[c][o];
+        if (has_source) x.Q[c] += F.js[c][o];
+        x.Qs[c] = zero_qs ? 0.0 : F.Qs[c][o];
+        x.U[c] = (DIM == 2 && c == 3) ? 0.0 : in.U[c][o];
+        x.Un[c] = (DIM == 2 && c == 3) ? 0.0 : F.Un[c][o];
+    }
+    x.J = F.J[o];
+}
+
+// The same arithmetic as rk_at on loaded inputs.
+template <int DIM>
+__device__ __forceinline__ void rk_finish(const RKCoef &K, double tau, const Fields &F, double *const outs[5],
+                                          long long o, const RKIn &x)
+{
+    double Qs[5];
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+        Qs[c] = x.Qs[c] + K.s * x.Q[c];
+        F.Qs[c][o] = Qs[c];
+    }
+    const double ro = x.U[0];
+    const double tj = tau / x.J;
+    const double rn = K.a * x.Un[0] + K.b * ro + tj * (K.c * x.Q[0] + K.d * Qs[0]);
+    outs[0][o] = rn;
+#pragma unroll
+    for (int c = 1; c < 5; c++) {
+        if (DIM == 2 && c == 3) { outs[3][o] = 0.0; continue; }
+        outs[c][o] = (K.a * x.Un[c] * x.Un[0] + K.b * x.U[c] * ro + tj * (K.c * x.Q[c] + K.d * Qs[c])) / rn;
+    }
+}
+
 // RK update of the real point at ghosted index o.
 template <int DIM>
 __device__ __forceinline__ void rk_at(const RKCoef &K, double tau, const StageIn &in, const Fields &F, double *o0,
