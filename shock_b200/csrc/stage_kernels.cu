@@ -35,13 +35,29 @@ __global__ void k_ghosts(Grid G, long long nshell, double *r, double *u, double 
     if (t < nshell) ghost_body(G, shell_index(G, t), r, u, v, w, e);
 }
 
+// One point per thread: prim is FP64-pipe heavy (pow, sqrt, divisions), and
+// batching points per thread measured slower.
+constexpr int PRIM_PTS = 1;
+
 template <int DIM>
 __global__ void k_prim(Grid G, Phys P, const double *__restrict__ R, const double *__restrict__ U,
                        const double *__restrict__ V, const double *__restrict__ W,
                        const double *__restrict__ E, double *p, double *T, double *c, double *mu)
 {
-    long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (o < G.NG) prim_body<DIM>(G, P, o, R, U, V, W, E, p, T, c, mu);
+    const long long base = blockIdx.x * (long long)blockDim.x * PRIM_PTS + threadIdx.x;
+    double v[PRIM_PTS][5];
+#pragma unroll
+    for (int b = 0; b < PRIM_PTS; b++) {
+        const long long o = base + (long long)b * blockDim.x;
+        if (o < G.NG) {
+            v[b][0] = R[o]; v[b][1] = U[o]; v[b][2] = V[o]; v[b][3] = DIM == 3 ? W[o] : 0.0; v[b][4] = E[o];
+        }
+    }
+#pragma unroll
+    for (int b = 0; b < PRIM_PTS; b++) {
+        const long long o = base + (long long)b * blockDim.x;
+        if (o < G.NG) prim_store<DIM>(P, o, v[b][0], v[b][1], v[b][2], v[b][3], v[b][4], p, T, c, mu);
+    }
 }
 
 template <int DIM, int ORDER, bool MIXED>
@@ -78,17 +94,28 @@ __global__ void __launch_bounds__(NTHR, ViscTile<DIM, D>::v == TL ? 2 : 3)
 }
 
 // Rows of real points: x runs along the fastest real axis (k in 3D, j in
-// 2D), y and z over the others, so the ghosted index needs no division.
+// 2D), y over pairs of rows of the next axis, z over the slowest, so the
+// ghosted index needs no division; each thread updates the same point of
+// two neighbouring rows, with both points' loads ahead of the stores.
 template <int DIM>
 __global__ void __launch_bounds__(128) k_rk_rows(Grid G, RKCoef K, double tau, StageIn in, Fields F, double *o0,
                                                  double *o1, double *o2, double *o3, double *o4, int has_source)
 {
     const int nf = DIM == 3 ? G.n[2] : G.n[1];
+    const int nm = DIM == 3 ? G.n[1] : G.n[0];
     const int f = blockIdx.x * blockDim.x + threadIdx.x;
     if (f >= nf) return;
-    const long long o = DIM == 3 ? (long long)(blockIdx.z + G.g) * G.st[0] + (long long)(blockIdx.y + G.g) * G.st[1] + G.g + f
-                                 : (long long)(blockIdx.y + G.g) * G.st[0] + G.g + f;
-    rk_at<DIM>(K, tau, in, F, o0, o1, o2, o3, o4, has_source, o, false);
+    const int r0 = 2 * blockIdx.y;
+    const long long sm = DIM == 3 ? G.st[1] : G.st[0];
+    const long long o = DIM == 3 ? (long long)(blockIdx.z + G.g) * G.st[0] + (long long)(r0 + G.g) * G.st[1] + G.g + f
+                                 : (long long)(r0 + G.g) * G.st[0] + G.g + f;
+    const bool two = r0 + 1 < nm;
+    double *const outs[5] = {o0, o1, o2, o3, o4};
+    RKIn x0, x1;
+    rk_load<DIM>(in, F, has_source, o, false, x0);
+    if (two) rk_load<DIM>(in, F, has_source, o + sm, false, x1);
+    rk_finish<DIM>(K, tau, F, outs, o, x0);
+    if (two) rk_finish<DIM>(K, tau, F, outs, o + sm, x1);
 }
 
 __global__ void k_add_source(Grid G, Fields F)
@@ -127,9 +154,9 @@ void launch_ghosts(const Grid &G, double *const U[5], cudaStream_t s)
 void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s)
 {
     if (G.dim == 3)
-        k_prim<3><<<blocks_for(G.NG, 256), 256, 0, s>>>(G, P, U[0], U[1], U[2], U[3], U[4], F.p, F.T, F.c, F.mu);
+        k_prim<3><<<blocks_for(G.NG, 256 * PRIM_PTS), 256, 0, s>>>(G, P, U[0], U[1], U[2], U[3], U[4], F.p, F.T, F.c, F.mu);
     else
-        k_prim<2><<<blocks_for(G.NG, 256), 256, 0, s>>>(G, P, U[0], U[1], U[2], U[3], U[4], F.p, F.T, F.c, F.mu);
+        k_prim<2><<<blocks_for(G.NG, 256 * PRIM_PTS), 256, 0, s>>>(G, P, U[0], U[1], U[2], U[3], U[4], F.p, F.T, F.c, F.mu);
 }
 
 void launch_nodal(const Grid &G, int precision, const double *const U[5], const Fields &F, cudaStream_t s)
@@ -215,7 +242,7 @@ void launch_rk(const Grid &G, const RKCoef &rk, double tau, const double *const 
     StageIn in;
     for (int c = 0; c < 5; c++) in.U[c] = Uin[c];
     const int nf = G.dim == 3 ? G.n[2] : G.n[1];
-    const dim3 grid((nf + 127) / 128, G.dim == 3 ? G.n[1] : G.n[0], G.dim == 3 ? G.n[0] : 1);
+    const dim3 grid((nf + 127) / 128, ((G.dim == 3 ? G.n[1] : G.n[0]) + 1) / 2, G.dim == 3 ? G.n[0] : 1);
     if (G.dim == 3)
         k_rk_rows<3><<<grid, 128, 0, s>>>(G, rk, tau, in, F, Uout[0], Uout[1], Uout[2], Uout[3], Uout[4],
                                           has_source ? 1 : 0);
