@@ -92,11 +92,12 @@ __device__ __forceinline__ void ghost_body(const Grid &G, long long o, double *r
     }
     if (!ghost) return;
     long long q = s.v[0] * G.st[0] + s.v[1] * G.st[1] + s.v[2];
-    r[o] = r[q];
-    u[o] = u[q];
-    v[o] = v[q];
-    w[o] = w[q];
-    e[o] = e[q];
+    const double a0 = r[q], a1 = u[q], a2 = v[q], a3 = w[q], a4 = e[q];   // loads ahead of the stores
+    r[o] = a0;
+    u[o] = a1;
+    v[o] = a2;
+    w[o] = a3;
+    e[o] = a4;
 }
 
 // ---------------------------------------------------------------------------
@@ -257,6 +258,35 @@ static __constant__ float c_w9is_f[5][15] = {
     {22658.f, -140251.f, 165153.f, -88297.f, 18079.f, 242723.f, -611976.f, 337018.f, -70237.f, 406293.f, -464976.f, 99213.f, 138563.f, -60871.f, 6908.f},
     {107918.f, -649501.f, 758823.f, -411487.f, 86329.f, 1020563.f, -2462076.f, 1358458.f, -288007.f, 1521393.f, -1704396.f, 364863.f, 482963.f, -208501.f, 22658.f},
 };
+
+// Packed FP32 arithmetic (two lanes per instruction) for the mixed form:
+// the + and - sides of a face have the same operations.
+__device__ __forceinline__ float2 f2(float a, float b) { return make_float2(a, b); }
+__device__ __forceinline__ float2 f2(float a) { return make_float2(a, a); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __ffma2_rn(b, f2(-1.f), a); }
+__device__ __forceinline__ float2 rcp2(float2 a) { return f2(__fdividef(1.f, a.x), __fdividef(1.f, a.y)); }
+
+// phi_w5 of two stencils at once: lane x the + side, lane y the - side.
+__device__ __forceinline__ float2 phi_w5x2(const float2 *d, float eps)
+{
+    const float2 a0 = sub2(d[0], d[1]), b0 = fma2(f2(-3.f), d[1], d[0]);
+    const float2 a1 = sub2(d[1], d[2]), b1 = add2(d[1], d[2]);
+    const float2 a2 = sub2(d[2], d[3]), b2 = fma2(f2(3.f), d[2], mul2(f2(-1.f), d[3]));
+    const float2 is0 = fma2(mul2(f2(13.f), a0), a0, mul2(mul2(f2(3.f), b0), b0));
+    const float2 is1 = fma2(mul2(f2(13.f), a1), a1, mul2(mul2(f2(3.f), b1), b1));
+    const float2 is2 = fma2(mul2(f2(13.f), a2), a2, mul2(mul2(f2(3.f), b2), b2));
+    const float2 e0 = add2(is0, f2(eps)), e1 = add2(is1, f2(eps)), e2 = add2(is2, f2(eps));
+    const float2 o0t = rcp2(mul2(e0, e0)), o1t = mul2(f2(6.f), rcp2(mul2(e1, e1)));
+    const float2 o2t = mul2(f2(3.f), rcp2(mul2(e2, e2)));
+    const float2 rs = rcp2(add2(add2(o0t, o1t), o2t));
+    const float2 o0 = mul2(o0t, rs), o2 = mul2(o2t, rs);
+    const float2 q1 = fma2(f2(-2.f), d[1], add2(d[0], d[2]));
+    const float2 q2 = fma2(f2(-2.f), d[2], add2(d[1], d[3]));
+    return fma2(mul2(f2(1.f / 6.f), sub2(o2, f2(0.5f))), q2, mul2(mul2(f2(1.f / 3.f), o0), q1));
+}
 
 template <typename T>
 __device__ __forceinline__ T w9c(int k, int i);
@@ -614,20 +644,35 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
 #pragma unroll
         for (int q = 0; q <= 2 * r; q++) {
             int t = f + q;
-            // the ten differences of a point are interleaved: five 8-byte loads
-            const float2 a0 = DL2(0, t, lane), a1 = DL2(1, t, lane), a2 = DL2(2, t, lane);
-            const float2 a3 = DL2(3, t, lane), a4 = DL2(4, t, lane);
-            float lf = L0 * a0.x + L1 * a0.y + L2 * a1.x + L3 * a1.y + L4 * a2.x;
-            float lu = L0 * a2.y + L1 * a3.x + L2 * a3.y + L3 * a4.x + L4 * a4.y;
-            dp[q] = 0.5f * (lf + a * lu);
-            dmv[q] = 0.5f * (lf - a * lu);
+            // five 8-byte loads per point: (flux, conserved) pairs for WENO5,
+            // the ten differences interleaved for WENO9
+            const float2 p0 = DL2(0, t, lane), p1 = DL2(1, t, lane), p2 = DL2(2, t, lane);
+            const float2 p3 = DL2(3, t, lane), p4 = DL2(4, t, lane);
+            if (ORDER == 5) {
+                // one packed multiply-add per characteristic row gives (lf, lu)
+                float2 acc = mul2(f2(L0), p0);
+                acc = fma2(f2(L1), p1, acc);
+                acc = fma2(f2(L2), p2, acc);
+                acc = fma2(f2(L3), p3, acc);
+                acc = fma2(f2(L4), p4, acc);
+                const float2 pm = mul2(f2(0.5f), fma2(f2(a, -a), f2(acc.y), f2(acc.x)));
+                dp[q] = pm.x;
+                dmv[q] = pm.y;
+            } else {
+                // WENO9 measured 58 % slower on the strided axes with the pair layout
+                const float lf = L0 * p0.x + L1 * p0.y + L2 * p1.x + L3 * p1.y + L4 * p2.x;
+                const float lu = L0 * p2.y + L1 * p3.x + L2 * p3.y + L3 * p4.x + L4 * p4.y;
+                dp[q] = 0.5f * (lf + a * lu);
+                dmv[q] = 0.5f * (lf - a * lu);
+            }
         }
         float phi;
         if (ORDER == 5) {
-            float dP[4], dM[4];
+            float2 dd[4];
 #pragma unroll
-            for (int q = 0; q < 4; q++) { dP[q] = dp[q]; dM[q] = dmv[2 * r - q]; }
-            phi = -phi_w5<float>(dP, eps) + phi_w5<float>(dM, eps);
+            for (int q = 0; q < 4; q++) dd[q] = f2(dp[q], dmv[2 * r - q]);
+            const float2 ph = phi_w5x2(dd, eps);
+            phi = -ph.x + ph.y;
         } else {
             float dP[8], dM[8], fp[9], fm[9];
 #pragma unroll
@@ -728,7 +773,8 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
             if (it < (NP - 1) * NLANE && T.l0 + l < G.g + T.nL && T.c0 - r + t < G.N[D])
 #pragma unroll
                 for (int q = 0; q < 5; q++)
-                    reinterpret_cast<float2 *>(dl)[(t * NLANE + l) * 5 + q] = make_float2(dv[m][2 * q], dv[m][2 * q + 1]);
+                    reinterpret_cast<float2 *>(dl)[(t * NLANE + l) * 5 + q] =
+                        ORDER == 5 ? make_float2(dv[m][q], dv[m][5 + q]) : make_float2(dv[m][2 * q], dv[m][2 * q + 1]);
         }
 #pragma unroll
         for (int k = 0; k < FPT; k++) {
@@ -810,11 +856,12 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
         else { ln = it % NLANE; cr = it / NLANE; }
         if (T.l0 + ln >= G.g + T.nL || T.c0 + cr > G.g + T.nD - 1) continue;
         long long o = T.base + (long long)ln * T.sL + (long long)(T.c0 + cr) * T.sD;
+        double prev[5];   // all five loads ahead of the stores
 #pragma unroll
-        for (int q = 0; q < 5; q++) {
-            double prev = first ? 0.0 : F.Q[q][o];
-            F.Q[q][o] = prev - (fh[(q * NFT + cr + 1) * NLS + ln] - fh[(q * NFT + cr) * NLS + ln]);
-        }
+        for (int q = 0; q < 5; q++) prev[q] = first ? 0.0 : F.Q[q][o];
+#pragma unroll
+        for (int q = 0; q < 5; q++)
+            F.Q[q][o] = prev[q] - (fh[(q * NFT + cr + 1) * NLS + ln] - fh[(q * NFT + cr) * NLS + ln]);
     }
 }
 
