@@ -551,9 +551,112 @@ __device__ __forceinline__ void add_right_col(const FaceState<T> &s, int ch, T p
     }
 }
 
+// Value indices (0..4 of the flux / conserved vectors) that row ch of the
+// left eigenvector matrix can weight with a nonzero product.  With the
+// diagonal 3D metric the unit normal has one nonzero component (along the
+// sweep axis D): the two entropy/vorticity rows ch != D then have exact
+// zeros everywhere except at the density and at the momentum of the third
+// axis a = 3 - D - ch.  In 2D the w momentum and its flux are exact zeros,
+// and row 2 has a zero energy entry (-gc nz).
+template <int DIM, int D>
+__host__ __device__ constexpr unsigned row_mask(int ch)
+{
+    return DIM == 2 ? (ch == 2 ? 0x07u : 0x17u)
+                    : (ch == D || ch >= 3) ? 0x1Fu : (1u | (1u << (1 + (3 - D - ch))));
+}
+
+__host__ __device__ constexpr int low_bit(unsigned m) { return (m & 1u) ? 0 : 1 + low_bit(m >> 1); }
+
+// (l.F + a l.U) / 2 and (l.F - a l.U) / 2 over the entries of mask M; the
+// products left out are exact zeros, so the sums are those of the full rows.
+template <unsigned M>
+__device__ __forceinline__ void dot_pm(const double *L, const double *fv, const double *uv, double a, double &pp,
+                                       double &pm)
+{
+    constexpr int i0 = low_bit(M);
+    double lf = L[i0] * fv[i0], lu = L[i0] * uv[i0];
+#pragma unroll
+    for (int i = i0 + 1; i < 5; i++)
+        if (M >> i & 1u) {
+            lf = lf + L[i] * fv[i];
+            lu = lu + L[i] * uv[i];
+        }
+    pp = 0.5 * (lf + a * lu);
+    pm = 0.5 * (lf - a * lu);
+}
+
+// Characteristic projection of the 2r+2 stencil points of face f on row LA
+// (and on row LB in the same pass when MB != 0: the two rows share their
+// shared-memory loads).
+template <int ORDER, int TLN, unsigned MA, unsigned MB>
+__device__ __forceinline__ void project_fp64(const double *sh, int f, int lane, double a, const double *LA,
+                                             const double *LB, double *PpA, double *PmA, double *PpB, double *PmB)
+{
+    constexpr int r = (ORDER - 1) / 2;
+    constexpr int NP = TLN + 2 * r + 2;
+    constexpr unsigned MU = MA | MB;
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
+#pragma unroll
+    for (int q = 0; q <= 2 * r + 1; q++) {
+        const int t = f + q;
+        asm volatile("" ::: "memory");   // issue this point's loads here, not all up front
+        double fv[5], uv[5];
+#pragma unroll
+        for (int i = 0; i < 5; i++)
+            if (MU >> i & 1u) {
+                fv[i] = SH(WF0 + i, t, lane);
+                uv[i] = SH(WU0 + i, t, lane);
+            }
+        dot_pm<MA>(LA, fv, uv, a, PpA[q], PmA[q]);
+        if (MB) dot_pm<(MB ? MB : 1u)>(LB, fv, uv, a, PpB[q], PmB[q]);
+    }
+#undef SH
+}
+
+// Phi+ - Phi- of one characteristic field from its projected split fluxes.
+template <int ORDER>
+__device__ __forceinline__ double weno_phi_fp64(const double *Pp, const double *Pm, double eps)
+{
+    constexpr int r = (ORDER - 1) / 2;
+    if (ORDER == 5) {
+        double dp[4], dm[4];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            dp[q] = Pp[q + 1] - Pp[q];
+            dm[q] = Pm[2 * r + 1 - q] - Pm[2 * r - q];
+        }
+        return -phi_w5<double>(dp, eps) + phi_w5<double>(dm, eps);
+    }
+    double fp[9], fm[9], dp[8], dm[8];
+#pragma unroll
+    for (int q = 0; q < 9; q++) { fp[q] = Pp[q]; fm[q] = Pm[2 * r + 1 - q]; }
+#pragma unroll
+    for (int q = 0; q < 8; q++) { dp[q] = fp[q + 1] - fp[q]; dm[q] = fm[q] - fm[q + 1]; }
+    return -phi_w9<double>(fp, dp, eps) + phi_w9<double>(fm, dm, eps);
+}
+
+// Characteristic rows CA and CB (CB < 0: CA alone) of one face.
+template <int DIM, int ORDER, int D, int TLN, int CA, int CB>
+__device__ __forceinline__ void weno_rows_fp64(const Phys &P, const FaceState<double> &s, const double *sh, int f,
+                                               int lane, double a, double *phi)
+{
+    constexpr int NS = ORDER + 1;
+    constexpr unsigned MA = row_mask<DIM, D>(CA), MB = CB >= 0 ? row_mask<DIM, D>(CB) : 0u;
+    asm volatile("" ::: "memory");
+    double LA[5], LB[5];
+    left_row<double>(s, CA, LA[0], LA[1], LA[2], LA[3], LA[4]);
+    if (CB >= 0) left_row<double>(s, CB, LB[0], LB[1], LB[2], LB[3], LB[4]);
+    double PpA[NS], PmA[NS], PpB[NS], PmB[NS];
+    project_fp64<ORDER, TLN, MA, MB>(sh, f, lane, a, LA, LB, PpA, PmA, PpB, PmB);
+    phi[CA] = weno_phi_fp64<ORDER>(PpA, PmA, P.eps64);
+    if (CB >= 0) phi[CB < 0 ? 0 : CB] = weno_phi_fp64<ORDER>(PpB, PmB, P.eps64);
+}
+
 // WENO part of the face flux in FP64 (src/WENO.c:296-430): split fluxes
 // F +/- lambda J_{i+1/2} U projected on the characteristic fields, Phi+,
 // Phi-, back-projection.  f: face index in the tile (points f..f+2r+1).
+// WENO5 takes the rows in three passes that share loads: the two sparse
+// entropy/vorticity rows, the full one, the two acoustic rows.
 template <int DIM, int ORDER, int D, int TLN = TL>
 __device__ __forceinline__ void face_weno_fp64(const Phys &P, const double *sh, int f, int lane, double *out)
 {
@@ -569,48 +672,27 @@ __device__ __forceinline__ void face_weno_fp64(const Phys &P, const double *sh, 
         double lm = SH(WLAM, f + q, lane);
         lam = lam < lm ? lm : lam;
     }
+#undef SH
     const double a = lam * jh;
+    double phi[5];
+    if (ORDER == 5) {
+        constexpr int C1 = DIM == 2 ? 0 : (D == 0 ? 1 : 0);
+        constexpr int C2 = DIM == 2 ? 1 : (D == 2 ? 1 : 2);
+        constexpr int CF = DIM == 2 ? 2 : D;
+        weno_rows_fp64<DIM, ORDER, D, TLN, C1, C2>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, CF, -1>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, 3, 4>(P, s, sh, f, lane, a, phi);
+    } else {
+        weno_rows_fp64<DIM, ORDER, D, TLN, 0, -1>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, 1, -1>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, 2, -1>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, 3, -1>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, 4, -1>(P, s, sh, f, lane, a, phi);
+    }
 #pragma unroll
     for (int q = 0; q < 5; q++) out[q] = 0.0;
-#pragma unroll 1
-    for (int ch = 0; ch < 5; ch++) {
-        // reload the window from shared memory in every iteration instead of
-        // holding 2r+2 points x 10 values in registers (keeps two tiles per SM)
-        asm volatile("" ::: "memory");
-        double L0, L1, L2, L3, L4;
-        left_row<double>(s, ch, L0, L1, L2, L3, L4);
-        double Pp[2 * r + 2], Pm[2 * r + 2];
 #pragma unroll
-        for (int q = 0; q <= 2 * r + 1; q++) {
-            int t = f + q;
-            asm volatile("" ::: "memory");   // issue this point's loads here, not all up front
-            double lf = L0 * SH(WF0 + 0, t, lane) + L1 * SH(WF0 + 1, t, lane) + L2 * SH(WF0 + 2, t, lane)
-                        + L3 * SH(WF0 + 3, t, lane) + L4 * SH(WF0 + 4, t, lane);
-            double lu = L0 * SH(WU0 + 0, t, lane) + L1 * SH(WU0 + 1, t, lane) + L2 * SH(WU0 + 2, t, lane)
-                        + L3 * SH(WU0 + 3, t, lane) + L4 * SH(WU0 + 4, t, lane);
-            Pp[q] = 0.5 * (lf + a * lu);
-            Pm[q] = 0.5 * (lf - a * lu);
-        }
-        double phi;
-        if (ORDER == 5) {
-            double dp[4], dm[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) {
-                dp[q] = Pp[q + 1] - Pp[q];
-                dm[q] = Pm[2 * r + 1 - q] - Pm[2 * r - q];
-            }
-            phi = -phi_w5<double>(dp, P.eps64) + phi_w5<double>(dm, P.eps64);
-        } else {
-            double fp[9], fm[9], dp[8], dm[8];
-#pragma unroll
-            for (int q = 0; q < 9; q++) { fp[q] = Pp[q]; fm[q] = Pm[2 * r + 1 - q]; }
-#pragma unroll
-            for (int q = 0; q < 8; q++) { dp[q] = fp[q + 1] - fp[q]; dm[q] = fm[q] - fm[q + 1]; }
-            phi = -phi_w9<double>(fp, dp, P.eps64) + phi_w9<double>(fm, dm, P.eps64);
-        }
-        add_right_col<double>(s, ch, phi, out);
-    }
-#undef SH
+    for (int ch = 0; ch < 5; ch++) add_right_col<double>(s, ch, phi[ch], out);
 }
 
 // Mixed form of the same: the projection, indicators, weights and
