@@ -695,6 +695,55 @@ __device__ __forceinline__ void face_weno_fp64(const Phys &P, const double *sh, 
     for (int ch = 0; ch < 5; ch++) add_right_col<double>(s, ch, phi[ch], out);
 }
 
+// Mixed WENO5: the projected differences of one point, (l.dF + a l.dU)/2 in
+// x and (l.dF - a l.dU)/2 in y, from its (flux, conserved) difference
+// pairs over the entries of mask M (packed FP32).
+template <unsigned M>
+__device__ __forceinline__ float2 dot_pm2(const float *L, const float2 *pv, float a)
+{
+    constexpr int i0 = low_bit(M);
+    float2 acc = mul2(f2(L[i0]), pv[i0]);
+#pragma unroll
+    for (int i = i0 + 1; i < 5; i++)
+        if (M >> i & 1u) acc = fma2(f2(L[i]), pv[i], acc);
+    return mul2(f2(0.5f), fma2(f2(a, -a), f2(acc.y), f2(acc.x)));
+}
+
+// Mixed WENO5, characteristic rows CA and CB (CB < 0: CA alone) of one face
+// in one pass over the five point differences.
+template <int DIM, int D, int TLN, int CA, int CB>
+__device__ __forceinline__ void weno5_rows_mixed(const FaceState<float> &s, const float *dl, int f, int lane, float a,
+                                                 float eps, float *phi)
+{
+    constexpr unsigned MA = row_mask<DIM, D>(CA), MB = CB >= 0 ? row_mask<DIM, D>(CB) : 0u, MU = MA | MB;
+    asm volatile("" ::: "memory");
+    float LA[5], LB[5];
+    left_row<float>(s, CA, LA[0], LA[1], LA[2], LA[3], LA[4]);
+    if (CB >= 0) left_row<float>(s, CB, LB[0], LB[1], LB[2], LB[3], LB[4]);
+    float2 pa[5], pb[5];
+#pragma unroll
+    for (int q = 0; q < 5; q++) {
+        const int t = f + q;
+        float2 pv[5];
+#pragma unroll
+        for (int i = 0; i < 5; i++)
+            if (MU >> i & 1u) pv[i] = reinterpret_cast<const float2 *>(dl)[(t * NLANE + lane) * 5 + i];
+        pa[q] = dot_pm2<MA>(LA, pv, a);
+        if (MB) pb[q] = dot_pm2<(MB ? MB : 1u)>(LB, pv, a);
+    }
+    float2 dd[4];
+#pragma unroll
+    for (int q = 0; q < 4; q++) dd[q] = f2(pa[q].x, pa[4 - q].y);
+    const float2 ha = phi_w5x2(dd, eps);
+    phi[CA] = -ha.x + ha.y;
+    if (CB >= 0) {
+#pragma unroll
+        for (int q = 0; q < 4; q++) dd[q] = f2(pb[q].x, pb[4 - q].y);
+        const float2 hb = phi_w5x2(dd, eps);
+        phi[CB < 0 ? 0 : CB] = -hb.x + hb.y;
+    }
+}
+
 // Mixed form of the same: the projection, indicators, weights and
 // back-projection in FP32 on FP64-formed point-to-point differences dl.
 template <int DIM, int ORDER, int D, int TLN = TL>
@@ -717,55 +766,50 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
     const float a = (float)(lam * jh);
     const float eps = P.eps32;
     float out[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-#pragma unroll 1
-    for (int ch = 0; ch < 5; ch++) {
-        asm volatile("" ::: "memory");
-        float L0, L1, L2, L3, L4;
-        left_row<float>(s, ch, L0, L1, L2, L3, L4);
-        float dp[2 * r + 1], dmv[2 * r + 1];
+    if (ORDER == 5) {
+        // three passes, as in the FP64 form: sparse rows, full row, acoustic rows
+        constexpr int C1 = DIM == 2 ? 0 : (D == 0 ? 1 : 0);
+        constexpr int C2 = DIM == 2 ? 1 : (D == 2 ? 1 : 2);
+        constexpr int CF = DIM == 2 ? 2 : D;
+        float phi[5];
+        weno5_rows_mixed<DIM, D, TLN, C1, C2>(s, dl, f, lane, a, eps, phi);
+        weno5_rows_mixed<DIM, D, TLN, CF, -1>(s, dl, f, lane, a, eps, phi);
+        weno5_rows_mixed<DIM, D, TLN, 3, 4>(s, dl, f, lane, a, eps, phi);
 #pragma unroll
-        for (int q = 0; q <= 2 * r; q++) {
-            int t = f + q;
-            // five 8-byte loads per point: (flux, conserved) pairs for WENO5,
-            // the ten differences interleaved for WENO9
-            const float2 p0 = DL2(0, t, lane), p1 = DL2(1, t, lane), p2 = DL2(2, t, lane);
-            const float2 p3 = DL2(3, t, lane), p4 = DL2(4, t, lane);
-            if (ORDER == 5) {
-                // one packed multiply-add per characteristic row gives (lf, lu)
-                float2 acc = mul2(f2(L0), p0);
-                acc = fma2(f2(L1), p1, acc);
-                acc = fma2(f2(L2), p2, acc);
-                acc = fma2(f2(L3), p3, acc);
-                acc = fma2(f2(L4), p4, acc);
-                const float2 pm = mul2(f2(0.5f), fma2(f2(a, -a), f2(acc.y), f2(acc.x)));
-                dp[q] = pm.x;
-                dmv[q] = pm.y;
-            } else {
-                // WENO9 measured 58 % slower on the strided axes with the pair layout
+        for (int ch = 0; ch < 5; ch++) add_right_col<float>(s, ch, phi[ch], out);
+    } else {
+#pragma unroll 1
+        for (int ch = 0; ch < 5; ch++) {
+            asm volatile("" ::: "memory");
+            float L0, L1, L2, L3, L4;
+            left_row<float>(s, ch, L0, L1, L2, L3, L4);
+            float dp[2 * r + 1], dmv[2 * r + 1];
+#pragma unroll
+            for (int q = 0; q <= 2 * r; q++) {
+                int t = f + q;
+                // the ten differences of a point are interleaved: five 8-byte
+                // loads (the WENO5 (flux, conserved) pair layout measured 58 %
+                // slower here)
+                const float2 p0 = DL2(0, t, lane), p1 = DL2(1, t, lane), p2 = DL2(2, t, lane);
+                const float2 p3 = DL2(3, t, lane), p4 = DL2(4, t, lane);
                 const float lf = L0 * p0.x + L1 * p0.y + L2 * p1.x + L3 * p1.y + L4 * p2.x;
                 const float lu = L0 * p2.y + L1 * p3.x + L2 * p3.y + L3 * p4.x + L4 * p4.y;
                 dp[q] = 0.5f * (lf + a * lu);
                 dmv[q] = 0.5f * (lf - a * lu);
             }
+            float phi;
+            {
+                float dP[8], dM[8], fp[9], fm[9];
+#pragma unroll
+                for (int q = 0; q < 8; q++) { dP[q] = dp[q]; dM[q] = dmv[2 * r - q]; }
+                fp[0] = 0.f;
+                fm[0] = 0.f;
+#pragma unroll
+                for (int q = 0; q < 8; q++) { fp[q + 1] = fp[q] + dP[q]; fm[q + 1] = fm[q] - dM[q]; }
+                phi = -phi_w9<float>(fp, dP, eps) + phi_w9<float>(fm, dM, eps);
+            }
+            add_right_col<float>(s, ch, phi, out);
         }
-        float phi;
-        if (ORDER == 5) {
-            float2 dd[4];
-#pragma unroll
-            for (int q = 0; q < 4; q++) dd[q] = f2(dp[q], dmv[2 * r - q]);
-            const float2 ph = phi_w5x2(dd, eps);
-            phi = -ph.x + ph.y;
-        } else {
-            float dP[8], dM[8], fp[9], fm[9];
-#pragma unroll
-            for (int q = 0; q < 8; q++) { dP[q] = dp[q]; dM[q] = dmv[2 * r - q]; }
-            fp[0] = 0.f;
-            fm[0] = 0.f;
-#pragma unroll
-            for (int q = 0; q < 8; q++) { fp[q + 1] = fp[q] + dP[q]; fm[q + 1] = fm[q] - dM[q]; }
-            phi = -phi_w9<float>(fp, dP, eps) + phi_w9<float>(fm, dM, eps);
-        }
-        add_right_col<float>(s, ch, phi, out);
     }
 #pragma unroll
     for (int q = 0; q < 5; q++) outd[q] = (double)out[q];
