@@ -1170,8 +1170,73 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
     __syncthreads();
 
     const double t23 = 2.0 / 3.0, t43 = 4.0 / 3.0;
+    // 3D with one face per row (7-cell tiles): rows 0 .. NFT/2-1 take two
+    // neighbouring faces each, so the 2H-1 stencil points the faces share are
+    // read from shared memory once; each face's sums keep their order
+    constexpr bool PAIR = (DIM == 3 && FPT == 1);
+    if (PAIR && row < NFT / 2 && T.lane_ok) {
+        const int f0 = 2 * row;          // faces f0, f0+1: staged points f0 .. f0+2H
+        const bool ok[2] = {(T.c0 - 1 + f0) <= G.g + T.nD - 1, (T.c0 + f0) <= G.g + T.nD - 1};
+        const int ta = f0 + H - 1;
+        double K1[2], KA[2], KB[2];
+#pragma unroll
+        for (int s2 = 0; s2 < 2; s2++) {
+            K1[s2] = 0.5 * (SH(V3F1, ta + s2, lane) + SH(V3F1, ta + s2 + 1, lane));
+            KA[s2] = 0.5 * (SH(V3FA, ta + s2, lane) + SH(V3FA, ta + s2 + 1, lane));
+            KB[s2] = 0.5 * (SH(V3FB, ta + s2, lane) + SH(V3FB, ta + s2 + 1, lane));
+        }
+        if (quirk) {
+#pragma unroll
+            for (int s2 = 0; s2 < 2; s2++)
+                if (ok[s2]) {
+                    FO(0, f0 + s2, lane) = K1[s2]; FO(1, f0 + s2, lane) = KA[s2]; FO(2, f0 + s2, lane) = KB[s2];
+                }
+        } else {
+            TS acc[2][8];
+            double ref[2][4];   // the mixed form differences against the face's left point
+#pragma unroll
+            for (int s2 = 0; s2 < 2; s2++) {
+#pragma unroll
+                for (int c = 0; c < 8; c++) acc[s2][c] = 0;
+#pragma unroll
+                for (int c = 0; c < 4; c++) ref[s2][c] = MIXED ? SH(V3U + c, ta + s2, lane) : 0.0;
+            }
+#pragma unroll
+            for (int l = 0; l <= 2 * H; l++) {
+                const int t = f0 + l;
+                double v8[8];
+#pragma unroll
+                for (int c = 0; c < 8; c++) v8[c] = SH(V3U + c, t, lane);   // u v w T, then X0..X3
+#pragma unroll
+                for (int s2 = 0; s2 < 2; s2++) {
+                    const int ll = l - s2;
+                    if (ll < 0 || ll >= 2 * H) continue;
+                    TS ch = (TS)ZD<ORDER>::half(ll), ci = (TS)ZD<ORDER>::interp(ll);
+#pragma unroll
+                    for (int c = 0; c < 4; c++) acc[s2][c] += ch * (TS)(v8[c] - ref[s2][c]);
+#pragma unroll
+                    for (int c = 4; c < 8; c++) acc[s2][c] += ci * (TS)v8[c];
+                }
+            }
+#pragma unroll
+            for (int s2 = 0; s2 < 2; s2++) {
+                if (!ok[s2]) continue;
+                const int f = f0 + s2;
+                double dvel[3] = {(double)acc[s2][0], (double)acc[s2][1], (double)acc[s2][2]};
+                double gD = dvel[D] * (t43 * K1[s2]) + (double)acc[s2][4] * (-t23 * KA[s2])
+                            + (double)acc[s2][5] * (-t23 * KB[s2]);
+                double gA = dvel[MA] * K1[s2] + (double)acc[s2][6] * KA[s2];
+                double gB = dvel[MB] * K1[s2] + (double)acc[s2][7] * KB[s2];
+                double g3[3];
+                g3[D] = gD; g3[MA] = gA; g3[MB] = gB;
+                FO(0, f, lane) = g3[0]; FO(1, f, lane) = g3[1]; FO(2, f, lane) = g3[2];
+                FO(3, f, lane) = (double)acc[s2][3] * K1[s2];
+            }
+        }
+    }
 #pragma unroll
     for (int k = 0; k < FPT; k++) {
+        if (PAIR) break;
         const int f = row + k * NROWT;   // face (c0-1+f)+1/2: staged points f .. f+2H-1
         if (!(T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1)) continue;
         const int ta = f + H - 1;        // staged index of the left point
