@@ -315,3 +315,80 @@ void ref_free(void)
     FreeMemory(&cfg, &msh, &U_last, &U_rk, &Fl, &Flh, &Qf, &Qsum, &film);
     live = 0;
 }
+
+#ifdef SHOCK_DROPIN
+/*
+ * The drop-in path (shock_b200/dropin/GPU.c): SHOCK's own set-up (ref_init
+ * above) and the core of startSimulation with GPU_CalcRungeKutta in place
+ * of CalcRungeKutta.  The periodic axes are described the way
+ * src/Load.c:355-400 describes a block that is its own neighbour: one
+ * interface per side, this rank as the neighbour rank, the float32
+ * Translation of the .sddc row (-period on the lower side, +period on the
+ * upper side).
+ */
+#include "GPU.h"
+
+static int *if_rank;
+static float **if_tr;
+static int if_n;
+
+static void dropin_interfaces_free(void)
+{
+    for (int i = 0; i < if_n; i++) free(if_tr[i]);
+    free(if_tr);
+    free(if_rank);
+    if_tr = NULL;
+    if_rank = NULL;
+    if_n = 0;
+}
+
+static void dropin_interfaces(void)
+{
+    int *side[3][2] = {{&cfg.InterfaceNeighbourLeft, &cfg.InterfaceNeighbourRight},
+                       {&cfg.InterfaceNeighbourBottom, &cfg.InterfaceNeighbourTop},
+                       {&cfg.InterfaceNeighbourBehind, &cfg.InterfaceNeighbourInFront}};
+    dropin_interfaces_free();
+    if_rank = malloc(6 * sizeof(int));
+    if_tr = malloc(6 * sizeof(float *));
+    for (int a = 0; a < MESHDIMENSIONS; a++)
+        for (int s = 0; s < 2; s++) {
+            if (!prm.periodic[a]) {
+                *side[a][s] = NO_NEIGHBOUR;
+                continue;
+            }
+            float *t = calloc(3, sizeof(float));
+            t[a] = (float)(s ? prm.period[a] : -prm.period[a]);
+            if_tr[if_n] = t;
+            if_rank[if_n] = cfg.MPI_rank;
+            *side[a][s] = if_n++;
+        }
+    cfg.MPI_rankNeighbours = if_rank;
+    cfg.Translation = if_tr;
+    cfg.NumberInterfaces = if_n;
+}
+
+int ref_dropin_create(int device)
+{
+    dropin_interfaces();
+    return GPU_Create(&cfg, &msh, &U_last, &Qf, device);
+}
+
+void ref_dropin_steps(int n)
+{
+    for (int s = 0; s < n; s++) {
+        GPU_CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh);
+        WriteValuesFromU1ToU2(&cfg, &U_rk, &U_last);
+    }
+}
+
+void ref_dropin_sync(void) { GPU_SyncHost(&cfg, &U_rk); }
+
+void ref_dropin_destroy(void)
+{
+    GPU_Destroy();
+    cfg.MPI_rankNeighbours = NULL;
+    cfg.Translation = NULL;
+    cfg.NumberInterfaces = 0;
+    dropin_interfaces_free();
+}
+#endif

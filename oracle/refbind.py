@@ -45,20 +45,24 @@ def ref_available(order: int, dim: int, extended: bool = False) -> bool:
     return os.path.exists(os.path.join(HERE, "_ref", f"libshockref{tag}_w{order}_{dim}d.so"))
 
 
+def dropin_available(order: int, dim: int) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", f"libshockdropin_w{order}_{dim}d.so"))
+
+
 class RefSolver:
     """One block of SHOCK's reference solver (one library per order/dim)."""
 
     _libs: dict = {}
 
-    def __init__(self, case, extended=False, external=None):
+    def __init__(self, case, extended=False, external=None, _lib="libshockref"):
         """extended=True loads the PRECISION=3 (80-bit long double) build.
         external=(exact9, js5): manufactured solution given as arrays on the
         ghosted block (the build with ref_harness/mms_external.c)."""
         self.case = case
         tag = "80" if extended else ("x" if external is not None else "")
-        key = (case.order, case.dim, tag)
+        key = (case.order, case.dim, _lib + tag)
         if key not in RefSolver._libs:
-            path = os.path.join(HERE, "_ref", f"libshockref{tag}_w{case.order}_{case.dim}d.so")
+            path = os.path.join(HERE, "_ref", f"{_lib}{tag}_w{case.order}_{case.dim}d.so")
             if not os.path.exists(path):
                 raise FileNotFoundError(path + " (run make -C oracle ref)")
             lib = C.CDLL(path, mode=os.RTLD_LOCAL)
@@ -138,6 +142,29 @@ class RefSolver:
     def mms_exact(self) -> np.ndarray:
         """Exact solution at every ghosted point after set-up (9 fields)."""
         return self.state(1)
+
+
+class DropinSolver(RefSolver):
+    """SHOCK's own set-up and time loop (ref_harness.c) running its time
+    steps on the GPU through the SHOCK-side binding shock_b200/dropin/GPU.c:
+    GPU_Create after the set-up, GPU_CalcRungeKutta in place of
+    CalcRungeKutta, GPU_SyncHost before the host reads U_RK
+    (oracle/_ref/libshockdropin_*.so, linked with libshock_b200.so)."""
+
+    def __init__(self, case, device: int = 0):
+        super().__init__(case, _lib="libshockdropin")
+        rc = self.lib.ref_dropin_create(C.c_int(device))
+        if rc != 0:
+            raise RuntimeError(f"GPU_Create returned {rc}")
+
+    def steps(self, n: int):
+        self.lib.ref_dropin_steps(C.c_int(n))
+
+    def sync(self):
+        self.lib.ref_dropin_sync()
+
+    def close(self):
+        self.lib.ref_dropin_destroy()
 
 
 class OcParams(C.Structure):
