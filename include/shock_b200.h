@@ -36,6 +36,14 @@ extern "C" {
 #define SHOCK_ETIMEOUT (-5) /* a bounded wait ran out */
 #define SHOCK_EBUSY (-6)    /* no free slot (serving) */
 
+/* Boundary condition of a non-periodic face (shock_params.bc), as SHOCK's
+ * BC.c fills its ghost layers; the ghost point of layer l mirrors the real
+ * point l cells inside the face (src/BC.c:638-2362). */
+#define SHOCK_BC_AUTO 0           /* periodic axis, or the manufactured solution's Dirichlet values */
+#define SHOCK_BC_WALL_VISCOUS 1   /* "BCWallViscous": no-slip adiabatic wall (src/BC.c:2657-2686) */
+#define SHOCK_BC_WALL_INVISCID 2  /* "BCWallInviscid": slip wall (src/BC.c:2688-2719) */
+#define SHOCK_BC_FARFIELD 3       /* "BCFarfield": zero-gradient copy (src/BC.c:2817-2859) */
+
 #define SHOCK_FP64 0        /* everything in FP64 (reference precision) */
 #define SHOCK_MIXED 1       /* FP32 WENO/viscous stencils, FP64 state/RK/metric/p-T recovery */
 
@@ -60,6 +68,9 @@ typedef struct shock_params {
     double period[3];   /* periodic Translation per axis (stored as float32 like src/Load.c:110) */
     int precision;      /* SHOCK_FP64 or SHOCK_MIXED */
     int zeta_fix;       /* 0: reproduce src/ZD.c:547-548 (zeta viscous stencil centred on j); 1: centred on k */
+    int bc[6];          /* per face in SHOCK's order Left, Right (i), Bottom, Top (j), Behind, InFront (k):
+                           SHOCK_BC_* (the CGNS BC type src/Load.c:46-97 assigns); SHOCK_BC_AUTO on
+                           every face of a periodic axis; zero-initialised callers get SHOCK_BC_AUTO */
 } shock_params;
 
 typedef struct shock_ctx shock_ctx;

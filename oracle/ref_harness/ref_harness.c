@@ -53,6 +53,7 @@ typedef struct {
     int mms_case;
     int periodic[3];
     double period[3];
+    int bc[6];          /* per face (Left..InFront): 0 none, 1 BCWallViscous, 2 BCWallInviscid, 3 BCFarfield */
 } ref_params;
 
 static struct strct_configuration cfg;
@@ -169,6 +170,13 @@ int ref_init(const ref_params *p, const double *x, const double *y, const double
     cfg.InterfaceNeighbourBehind = cfg.InterfaceNeighbourInFront = p->periodic[2] ? 0 : NO_NEIGHBOUR;
 
     DefineParameters(&cfg);
+    {
+        /* face BC names as src/Load.c:46-97 assigns them from the CGNS BC types */
+        char *side[6] = {cfg.BC_Left, cfg.BC_Right, cfg.BC_Bottom, cfg.BC_Top, cfg.BC_Behind, cfg.BC_InFront};
+        const char *name[4] = {NULL, cfg.BCWallViscous, cfg.BCWallInviscid, cfg.BCFarfield};
+        for (int f = 0; f < 6; f++)
+            if (p->bc[f] >= 1 && p->bc[f] <= 3) strcpy(side[f], name[p->bc[f]]);
+    }
 
     vx.ptr = (void *)x; vx.dt = RealDouble;
     vy.ptr = (void *)y; vy.dt = RealDouble;

@@ -37,6 +37,7 @@ class RefParams(C.Structure):
         ("t0", C.c_double), ("l0", C.c_double),
         ("inviscid", C.c_int), ("mms", C.c_int), ("mms_case", C.c_int),
         ("periodic", C.c_int * 3), ("period", C.c_double * 3),
+        ("bc", C.c_int * 6),
     ]
 
 
@@ -81,6 +82,8 @@ class RefSolver:
         for a in range(3):
             p.periodic[a] = int(case.periodic[a])
             p.period[a] = case.period[a]
+        for f in range(6):
+            p.bc[f] = int(getattr(case, "bc", (0,) * 6)[f])
         self.params = p
         f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
         x, y, z, u, v, w, pr, rho = (f(a) for a in case.real_fields())
@@ -202,6 +205,8 @@ class Oracle:
     """The CPU restatement, same calling convention as RefSolver."""
 
     def __init__(self, case, dirichlet9=None, source5=None):
+        if any(getattr(case, "bc", (0,) * 6)):
+            raise ValueError("the CPU restatement covers periodic and manufactured-solution faces only")
         lib = self.lib = _oracle_lib()
         p = OcParams()
         p.dim, p.order = case.dim, case.order

@@ -28,6 +28,12 @@ LIB_PATH = os.environ.get("SHOCK_B200_LIB", os.path.join(HERE, "libshock_b200.so
 
 SHOCK_FP64 = 0
 SHOCK_MIXED = 1
+SHOCK_EINVAL = -1
+# face boundary conditions (shock_params.bc), SHOCK's BC.c types
+SHOCK_BC_AUTO = 0
+SHOCK_BC_WALL_VISCOUS = 1
+SHOCK_BC_WALL_INVISCID = 2
+SHOCK_BC_FARFIELD = 3
 
 _lib = None
 _lock = threading.Lock()
@@ -53,6 +59,7 @@ class Params(C.Structure):
         ("inviscid", C.c_int), ("mms", C.c_int),
         ("periodic", C.c_int * 3), ("period", C.c_double * 3),
         ("precision", C.c_int), ("zeta_fix", C.c_int),
+        ("bc", C.c_int * 6),
     ]
 
 
@@ -132,6 +139,8 @@ def params_from_case(case, precision=SHOCK_FP64, zeta_fix=False) -> Params:
         p.period[a] = float(case.period[a])
     p.precision = int(precision)
     p.zeta_fix = int(bool(zeta_fix))
+    for f in range(6):
+        p.bc[f] = int(case.bc[f])
     return p
 
 

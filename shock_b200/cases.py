@@ -21,6 +21,8 @@ with seeded synthetic data (no dataset is involved):
   * ``decaying_turbulence`` -- random-phase solenoidal field, periodic cube
   * ``isentropic_vortex``-- 2D periodic isentropic vortex (ensemble members)
   * ``smooth_random``    -- smooth random periodic states for parity tests
+  * ``channel``          -- wall-bounded blocks (wall / farfield y faces) for the
+                            boundary-condition parity tests
 """
 from __future__ import annotations
 
@@ -60,6 +62,7 @@ class Case:
     mms_case: int = 0               # [ManufacturedSolution] case
     periodic: Tuple[bool, bool, bool] = (True, True, True)
     period: Tuple[float, float, float] = (1.0, 1.0, 1.0)
+    bc: Tuple[int, int, int, int, int, int] = (0, 0, 0, 0, 0, 0)   # SHOCK_BC_* per face (Left..InFront)
     name: str = "case"
 
     @property
@@ -146,6 +149,53 @@ def smooth_random(dim: int, order: int, n: Tuple[int, int, int], seed: int = 0,
              w=w, p=p, time_order=time_order, mach=mach, reynolds=reynolds,
              inviscid=inviscid, periodic=(True, True, dim == 3), period=L,
              name=f"smooth{dim}d_w{order}")
+    c.tau = cfl_tau(c)
+    return c
+
+
+BC_NAMES = {"wall_viscous": 1, "wall_inviscid": 2, "farfield": 3}
+
+
+def channel(dim: int, order: int, n: Tuple[int, int, int], bc: str = "wall_viscous", seed: int = 0,
+            mach: float = 0.3, reynolds: float = 500.0, inviscid: bool = False, time_order: int = 4,
+            stretch: float = 0.0, walls_i: bool = False) -> Case:
+    """Wall-bounded block: periodic in x (and z in 3D), the two y faces of
+    type ``bc`` (SHOCK's BCWallViscous / BCWallInviscid / BCFarfield).  The
+    wall-normal grid spans [0, 1] with both end points on the walls and an
+    optional tanh clustering towards them.  Initial state: a parabolic
+    streamwise profile plus smooth seeded perturbations.  walls_i=True also
+    closes the x faces (a box with walls on two axes)."""
+    rng = np.random.default_rng(seed)
+    ni, nj, nk = n[0], n[1], (n[2] if dim == 3 else 1)
+    Lx, Lz = 2.0, 1.0
+    xa = Lx * np.arange(ni) / (ni - 1 if walls_i else ni)
+    eta = np.arange(nj) / (nj - 1)
+    ya = 0.5 * (1.0 + np.tanh(stretch * (2 * eta - 1)) / math.tanh(stretch)) if stretch else eta
+    za = Lz * np.arange(nk) / nk if dim == 3 else np.zeros(1)
+    x, y, z = np.meshgrid(xa, ya, za, indexing="ij")
+    X, Z = 2 * math.pi * x / Lx, 2 * math.pi * z / Lz
+
+    def pert():
+        f = np.zeros_like(x)
+        for _ in range(2):
+            kx, kz = rng.integers(1, 3), (rng.integers(0, 3) if dim == 3 else 0)
+            f = f + rng.normal() * np.sin(math.pi * y) * np.sin(kx * X + kz * Z + rng.uniform(0, 2 * math.pi))
+        return f
+
+    amp = 0.05
+    u = 4.0 * y * (1.0 - y) + amp * pert()
+    v = amp * pert()
+    w = amp * pert() if dim == 3 else np.zeros_like(x)
+    rho = 1.0 + 0.02 * pert()
+    p = 1.0 + 0.02 * pert()
+    t = BC_NAMES[bc]
+    faces = [0, 0, t, t, 0, 0]
+    if walls_i:
+        faces[0] = faces[1] = t
+    c = Case(dim=dim, order=order, ni=ni, nj=nj, nk=nk, x=x, y=y, z=z, rho=rho, u=u, v=v, w=w, p=p,
+             time_order=time_order, mach=mach, reynolds=reynolds, inviscid=inviscid,
+             periodic=(not walls_i, False, dim == 3), period=(Lx, 1.0, Lz), bc=tuple(faces),
+             name=f"channel{dim}d_w{order}_{bc}")
     c.tau = cfl_tau(c)
     return c
 

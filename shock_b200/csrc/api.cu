@@ -110,6 +110,17 @@ Phys make_phys(const shock_params &p)
     P.eps32 = 10.f * sqrtf(1.17549435e-38f);          // 10*sqrt(FLT_MIN), the float build's value
     P.mms = p.mms ? 1 : 0;
     P.zeta_fix = p.zeta_fix;
+    // BC_Corrector_*Momentum of the ghost points (reset to 1 at set-up,
+    // src/Functions.c:6388-6509): -1 on every momentum at a no-slip wall
+    // (src/BC.c:2667-2669), -1 on the face-normal momentum at a slip wall
+    // (src/BC.c:2703-2705), 1 elsewhere
+    P.walls = 0;
+    for (int f = 0; f < 6; f++)
+        for (int q = 0; q < 3; q++) {
+            const int b = f < 2 * p.dim ? p.bc[f] : SHOCK_BC_AUTO;
+            P.mcorr[f][q] = b == SHOCK_BC_WALL_VISCOUS ? -1.0 : (b == SHOCK_BC_WALL_INVISCID && q == f / 2) ? -1.0 : 1.0;
+            if (b != SHOCK_BC_AUTO) P.walls = 1;
+        }
     return P;
 }
 
@@ -126,6 +137,10 @@ static void enqueue_rhs(shock_ctx *c, double *const in[5], int &nk)
     nk += (c->G.periodic[0] || c->G.periodic[1] || c->G.periodic[2]) ? 1 : 0;
     launch_prim(c->G, c->P, cin, c->F, s);
     nk++;
+    if (c->P.walls) {
+        launch_bc(c->G, cin, c->buf, c->F, false, s);
+        nk++;
+    }
     if (!c->p.inviscid) {
         launch_nodal(c->G, c->p.precision, cin, c->F, s);
         nk++;
@@ -190,6 +205,25 @@ int shock_device_count(int *n)
     return SHOCK_OK;
 }
 
+// Every face: periodic (SHOCK_BC_AUTO on a periodic axis), a
+// manufactured-solution Dirichlet face (SHOCK_BC_AUTO with mms), or one of
+// the wall / farfield types.
+static int check_faces(const shock_params *p)
+{
+    for (int a = 0; a < p->dim; a++)
+        for (int side = 0; side < 2; side++) {
+            const int f = 2 * a + side, b = p->bc[f];
+            if (b < SHOCK_BC_AUTO || b > SHOCK_BC_FARFIELD) return fail(SHOCK_EINVAL, "face %d: unknown bc %d", f, b);
+            if (p->periodic[a] && b != SHOCK_BC_AUTO)
+                return fail(SHOCK_EINVAL, "face %d: a periodic axis takes SHOCK_BC_AUTO", f);
+            if (!p->periodic[a] && b == SHOCK_BC_AUTO && !p->mms)
+                return fail(SHOCK_EINVAL, "face %d: neither periodic, a manufactured-solution face nor a bc", f);
+            if (p->mms && b != SHOCK_BC_AUTO)
+                return fail(SHOCK_EINVAL, "face %d: the manufactured solution sets every non-periodic face", f);
+        }
+    return SHOCK_OK;
+}
+
 int shock_create(const shock_params *p, const double *x, const double *y, const double *z, const double *u,
                  const double *v, const double *w, const double *pr, const double *rho, int device, shock_ctx **out)
 {
@@ -204,9 +238,7 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
     if (p->dim == 3 && !z) return fail(SHOCK_EINVAL, "z coordinates missing");
     if (p->dim == 3 && !p->inviscid && !p->zeta_fix && p->nj > p->nk)
         return fail(SHOCK_EINVAL, "zeta viscous stencil centred on j needs nj <= nk (src/ZD.c:547-548)");
-    for (int a = 0; a < p->dim; a++)
-        if (!p->periodic[a] && !p->mms)
-            return fail(SHOCK_EINVAL, "axis %d: only periodic or manufactured-solution faces are supported", a);
+    if (int rc = check_faces(p)) return rc;
     if (p->mach <= 0 || p->reynolds <= 0 || p->gamma <= 1.0 || p->tau <= 0) return fail(SHOCK_EINVAL, "bad physics");
 
     shock_ctx *c = new shock_ctx();
@@ -258,6 +290,11 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
     for (int f = 0; f < 9; f++) cudaMemcpy(c->F.m[f], hb.geo[4 + f].data(), nb, cudaMemcpyHostToDevice);
     for (int b = 0; b < 3; b++)
         for (int f = 0; f < 5; f++) cudaMemcpy(c->buf[b][f], hb.prim[f].data(), nb, cudaMemcpyHostToDevice);
+    if (c->P.walls) {
+        const double *b0[5] = {c->buf[0][0], c->buf[0][1], c->buf[0][2], c->buf[0][3], c->buf[0][4]};
+        launch_bc(G, b0, c->buf, c->F, true, c->stream);
+        cudaStreamSynchronize(c->stream);
+    }
     c->geo_host = std::move(hb.geo);
     cudaError_t e = cudaDeviceSynchronize();
     if (e != cudaSuccess) {
@@ -321,6 +358,7 @@ static int host_block(const shock_params *p, const double *x, const double *y, c
     if (!p || !x || !y || (p->dim == 3 && !z)) return fail(SHOCK_EINVAL, "null argument");
     if (p->dim != 2 && p->dim != 3) return fail(SHOCK_EINVAL, "dim must be 2 or 3");
     if (p->order != 5 && p->order != 9) return fail(SHOCK_EINVAL, "order must be 5 or 9");
+    if (int rc = check_faces(p)) return rc;
     size_t nr = (size_t)p->ni * p->nj * (p->dim == 3 ? p->nk : 1);
     std::vector<double> zero(nr, 0.0), one(nr, 1.0);
     build_block(*p, x, y, z ? z : zero.data(), zero.data(), zero.data(), zero.data(), one.data(), one.data(), hb);
@@ -535,6 +573,7 @@ int shock_profile_stage(shock_ctx *c, int max, char *names, float *ms, int *coun
     mark(nullptr);
     launch_ghosts(c->G, in, c->stream); mark("ghosts");
     launch_prim(c->G, c->P, cin, c->F, c->stream); mark("prim");
+    // (the wall fill is left out: it writes the ghost layers of every state buffer)
     if (!c->p.inviscid) { launch_nodal(c->G, c->p.precision, cin, c->F, c->stream); mark("nodal"); }
     for (int d = 0; d < c->p.dim; d++) {
         launch_weno(c->G, c->P, c->p.precision, d, d == 0, cin, c->F, c->stream);

@@ -189,6 +189,8 @@ int check_params(const shock_batch *b, const shock_params *p)
     if (p->mms) return report_error(SHOCK_EINVAL, "batch members must be periodic blocks (mms = 0)");
     for (int a = 0; a < p->dim; a++)
         if (!p->periodic[a]) return report_error(SHOCK_EINVAL, "axis %d is not periodic", a);
+    for (int f = 0; f < 6; f++)
+        if (p->bc[f] != SHOCK_BC_AUTO) return report_error(SHOCK_EINVAL, "face %d: only periodic faces here", f);
     if (p->mach <= 0 || p->reynolds <= 0 || p->gamma <= 1.0 || p->tau <= 0)
         return report_error(SHOCK_EINVAL, "bad physics");
     return SHOCK_OK;

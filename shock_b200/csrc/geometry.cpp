@@ -58,6 +58,33 @@ void extrapolate(std::vector<double> &f, const Box &b, int dim)
     }
 }
 
+// mirrorGhostCellsMetric (src/Functions.c:6849-7015): the ghost layers of
+// wall and farfield faces take J and the nine metric terms of the real point
+// they mirror, over the whole ghost-inclusive face, face by face in SHOCK's
+// order (so a later face mirrors what an earlier one wrote at an edge).
+void mirror_metric(const Layout &L, const shock_params &p, std::vector<std::vector<double>> &geo)
+{
+    for (int f = 0; f < 2 * p.dim; f++) {
+        const int b = p.bc[f];
+        if (b != SHOCK_BC_WALL_VISCOUS && b != SHOCK_BC_WALL_INVISCID && b != SHOCK_BC_FARFIELD) continue;
+        const int a = f / 2, side = f % 2;
+        int idx[3];
+        for (int l = 0; l < L.g; l++) {
+            const int gi = side ? L.g + L.n[a] + l : L.g - 1 - l;
+            const int si = side ? L.g + L.n[a] - 1 - l : L.g + l;
+            for (idx[0] = 0; idx[0] < L.N[0]; idx[0]++)
+                for (idx[1] = 0; idx[1] < L.N[1]; idx[1]++)
+                    for (idx[2] = 0; idx[2] < L.N[2]; idx[2]++) {
+                        if (idx[a] != gi) continue;
+                        int sv[3] = {idx[0], idx[1], idx[2]};
+                        sv[a] = si;
+                        const long long d = L.at(idx[0], idx[1], idx[2]), o = L.at(sv[0], sv[1], sv[2]);
+                        for (int q = 3; q < 13; q++) geo[q][d] = geo[q][o];
+                    }
+        }
+    }
+}
+
 }  // namespace
 
 // Periodic image copy over the ghost-inclusive slab of every periodic axis;
@@ -198,6 +225,7 @@ int build_block(const shock_params &p, const double *x, const double *y, const d
                 hb.geo[12][o] = (x_xi * y_eta - x_eta * y_xi) / Jv;
             }
     for (int r = 0; r < dim; r++) periodic_images(L, p, gf, 13, 3);
+    mirror_metric(L, p, hb.geo);
     return 0;
 }
 

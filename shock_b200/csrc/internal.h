@@ -45,6 +45,7 @@ struct Grid {
     long long st[3];
     long long NG;
     int periodic[3];
+    int bc[6];           // SHOCK_BC_* per face (Left, Right, Bottom, Top, Behind, InFront)
 };
 
 struct Phys {
@@ -52,6 +53,9 @@ struct Phys {
     float eps32;
     int mms;
     int zeta_fix;
+    int walls;           // some face is a wall or farfield face
+    double mcorr[6][3];  // per face: sign of the u,v,w convective momentum terms in its ghost
+                         // points (SHOCK's BC_Corrector_*Momentum, src/WENO.c:265-277)
 };
 
 struct StageIn {        // state read by a stage
@@ -131,6 +135,7 @@ inline Grid make_grid(const Layout &L, const shock_params &p)
         G.n[a] = L.n[a]; G.N[a] = L.N[a]; G.st[a] = L.st[a];
         G.periodic[a] = a < p.dim ? p.periodic[a] : 0;
     }
+    for (int f = 0; f < 6; f++) G.bc[f] = f < 2 * p.dim ? p.bc[f] : 0;
     G.NG = L.NG;
     return G;
 }
@@ -163,6 +168,10 @@ void launch_batch_advance(Member *mem, const BatchPlan *plan, int capacity, int 
 // Kernel launchers (stage_kernels.cu).
 void launch_ghosts(const Grid &G, double *const U[5], cudaStream_t s);
 void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s);
+// Wall and farfield ghost layers from state U into all three state buffers
+// (setup: SHOCK's set-up fill, state only); no launch without such faces.
+void launch_bc(const Grid &G, const double *const U[5], double *const bufs[3][5], const Fields &F, bool setup,
+               cudaStream_t s);
 void launch_nodal(const Grid &G, int precision, const double *const U[5], const Fields &F, cudaStream_t s);
 void launch_weno(const Grid &G, const Phys &P, int precision, int d, bool first,
                  const double *const U[5], const Fields &F, cudaStream_t s);

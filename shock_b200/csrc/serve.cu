@@ -329,6 +329,8 @@ int shock_server_submit(shock_server *s, const shock_params *p, const double *x,
     if (p->mms) return report_error(SHOCK_EINVAL, "requests must be periodic blocks (mms = 0)");
     for (int a = 0; a < p->dim; a++)
         if (!p->periodic[a]) return report_error(SHOCK_EINVAL, "axis %d is not periodic", a);
+    for (int f = 0; f < 6; f++)
+        if (p->bc[f] != SHOCK_BC_AUTO) return report_error(SHOCK_EINVAL, "face %d: only periodic faces here", f);
     const int g = (p->order + 1) / 2;
     if (p->ni < g + 1 || p->nj < g + 1 || (p->dim == 3 && p->nk < g + 1))
         return report_error(SHOCK_EINVAL, "block smaller than the stencil");

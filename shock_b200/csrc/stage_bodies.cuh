@@ -214,6 +214,104 @@ __device__ __forceinline__ void nodal_body(const Grid &G, long long o, const dou
 }
 
 // ---------------------------------------------------------------------------
+// Wall and farfield faces (src/BC.c:638-2362; point rules :2657-2719 and
+// :2817-2859).  Ghost layer l of face f (l cells outside the face) mirrors
+// the real point l cells inside, over the face's real tangential range; the
+// edges and corners of the ghost shell are not written (SHOCK's face loops
+// do not reach them).  The state goes to every state buffer: SHOCK fills
+// U_RK in place, so the next stage's periodic image copy reads the values
+// written here.  setup: the fill of SHOCK's set-up (src/SHOCK.c:237), which
+// runs before any CalcValues: theta is still zero there, so a slip wall gets
+// zero velocity, and p, T, c, mu are not written.
+// ---------------------------------------------------------------------------
+struct StateBufs {
+    double *U[3][5];
+};
+
+__device__ __forceinline__ double prod3(double x, double y, double z) { return __dmul_rn(__dmul_rn(x, y), z); }
+
+// Number of ghost points face f fills.
+__host__ __device__ inline long long bc_face_points(const Grid &G, int f)
+{
+    const int a = f / 2;
+    long long r = G.g;
+    for (int b = 0; b < G.dim; b++)
+        if (b != a) r *= G.n[b];
+    return r;
+}
+
+template <int DIM>
+__device__ __forceinline__ void bc_body(const Grid &G, const Fields &F, const double *const *in, const StateBufs &B,
+                                        int f, long long idx, bool setup)
+{
+    const int a = f / 2, side = f % 2;
+    const int tb = a == 0 ? 1 : 0, tc = a == 2 ? 1 : 2;   // tangential axes (tc = 2 is flat in 2D)
+    const long long nc = DIM == 3 ? G.n[tc] : 1, R = (long long)G.n[tb] * nc;
+    const int l = (int)(idx / R);
+    const long long r = idx - (long long)l * R;
+    int v[3];
+    v[tb] = G.g + (int)(r / nc);
+    v[tc] = DIM == 3 ? G.g + (int)(r % nc) : 0;
+    v[a] = side ? G.g + G.n[a] + l : G.g - 1 - l;
+    const long long o = v[0] * G.st[0] + v[1] * G.st[1] + v[2];
+    v[a] = side ? G.g + G.n[a] - 1 - l : G.g + l;
+    const long long s = v[0] * G.st[0] + v[1] * G.st[1] + v[2];
+
+    const int type = G.bc[f];
+    const double rho = in[0][s], u = in[1][s], vv = in[2][s], w = in[3][s], e = in[4][s];
+    double gv[3];
+    if (type == SHOCK_BC_WALL_VISCOUS) {
+        gv[0] = -u; gv[1] = -vv; gv[2] = -w;
+    } else if (type == SHOCK_BC_FARFIELD) {
+        gv[0] = u; gv[1] = vv; gv[2] = w;
+    } else {
+        // slip wall: contravariant velocities of the interior point (as
+        // CalcValues forms them, src/Functions.c:2406-2440; theta3 stays zero
+        // in 2D) with the face-normal one negated, turned back into u, v, w
+        // with the ghost point's metric by Cramer's rule, every product and
+        // sum rounded in the order src/BC.c:2697-2699 evaluates them
+        double th[3] = {0.0, 0.0, 0.0};
+        if (!setup)
+            for (int q = 0; q < DIM; q++) {
+                double t = __dadd_rn(__dmul_rn(u, F.m[3 * q][s]), __dmul_rn(vv, F.m[3 * q + 1][s]));
+                th[q] = DIM == 3 ? __dadd_rn(t, __dmul_rn(w, F.m[3 * q + 2][s])) : t;
+            }
+        th[a] = -th[a];
+        const double xx = F.m[0][o], xy = F.m[1][o], xz = F.m[2][o];
+        const double ex = F.m[3][o], ey = F.m[4][o], ez = F.m[5][o];
+        const double zx = F.m[6][o], zy = F.m[7][o], zz = F.m[8][o];
+        const double t1 = th[0], t2 = th[1], t3 = th[2];
+        const double du = prod3(-xx, ey, zz) + prod3(xx, ez, zy) + prod3(xy, ex, zz) - prod3(xy, ez, zx)
+                          - prod3(xz, ex, zy) + prod3(xz, ey, zx);
+        const double dw = prod3(xx, ey, zz) - prod3(xx, ez, zy) - prod3(xy, ex, zz) + prod3(xy, ez, zx)
+                          + prod3(xz, ex, zy) - prod3(xz, ey, zx);
+        const double nu = prod3(t1, ey, zz) - prod3(t1, ez, zy) - prod3(t2, xy, zz) + prod3(t2, xz, zy)
+                          + prod3(t3, xy, ez) - prod3(t3, xz, ey);
+        const double nv = prod3(-t1, ex, zz) + prod3(t1, ez, zx) + prod3(t2, xx, zz) - prod3(t2, xz, zx)
+                          - prod3(t3, xx, ez) + prod3(t3, xz, ex);
+        const double nw = prod3(-t1, ex, zy) + prod3(t1, ey, zx) + prod3(t2, xx, zy) - prod3(t2, xy, zx)
+                          - prod3(t3, xx, ey) + prod3(t3, xy, ex);
+        gv[0] = -nu / du;
+        gv[1] = -nv / du;
+        gv[2] = -nw / dw;
+    }
+#pragma unroll
+    for (int k = 0; k < 3; k++) {
+        B.U[k][0][o] = rho;
+        B.U[k][1][o] = gv[0];
+        B.U[k][2][o] = gv[1];
+        B.U[k][3][o] = gv[2];
+        B.U[k][4][o] = e;
+    }
+    if (!setup) {
+        F.p[o] = F.p[s];
+        F.T[o] = F.T[s];
+        F.c[o] = F.c[s];
+        F.mu[o] = F.mu[s];
+    }
+}
+
+// ---------------------------------------------------------------------------
 // WENO reconstruction weights (src/WENO.c:11-204).
 // ---------------------------------------------------------------------------
 // Reciprocal for the WENO5 nonlinear weights: FP64 keeps SHOCK's division;
@@ -429,9 +527,18 @@ __device__ __forceinline__ void stage_weno(const Grid &G, const Phys &P, const T
         }
         double rt = rho * th;
         SH(WF0 + 0, t, l) = J * rt;
-        SH(WF0 + 1, t, l) = J * (rt * u + mx * p * P.ups);
-        SH(WF0 + 2, t, l) = J * (rt * v + my * p * P.ups);
-        SH(WF0 + 3, t, l) = J * (rt * w + mz * p * P.ups);
+        const int wf = !P.walls ? -1 : pd < G.g ? 2 * D : (pd >= G.g + G.n[D] ? 2 * D + 1 : -1);
+        if (wf >= 0) {
+            // a ghost point of a wall face: SHOCK's BC_Corrector signs on the
+            // convective momentum terms (src/WENO.c:265-277)
+            SH(WF0 + 1, t, l) = J * (rt * u * P.mcorr[wf][0] + mx * p * P.ups);
+            SH(WF0 + 2, t, l) = J * (rt * v * P.mcorr[wf][1] + my * p * P.ups);
+            SH(WF0 + 3, t, l) = J * (rt * w * P.mcorr[wf][2] + mz * p * P.ups);
+        } else {
+            SH(WF0 + 1, t, l) = J * (rt * u + mx * p * P.ups);
+            SH(WF0 + 2, t, l) = J * (rt * v + my * p * P.ups);
+            SH(WF0 + 3, t, l) = J * (rt * w + mz * p * P.ups);
+        }
         SH(WF0 + 4, t, l) = J * (rt * (e + p / rho * P.ups));
         SH(WU0 + 0, t, l) = rho;
         SH(WU0 + 1, t, l) = rho * u;

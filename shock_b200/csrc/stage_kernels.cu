@@ -151,6 +151,34 @@ void launch_ghosts(const Grid &G, double *const U[5], cudaStream_t s)
     k_ghosts<<<blocks_for(ns, 256), 256, 0, s>>>(G, ns, U[0], U[1], U[2], U[3], U[4]);
 }
 
+template <int DIM>
+__global__ void __launch_bounds__(256) k_bc(Grid G, Fields F, StageIn in, StateBufs B, bool setup)
+{
+    const int f = blockIdx.y;
+    if (G.bc[f] == SHOCK_BC_AUTO) return;
+    const long long n = bc_face_points(G, f);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        bc_body<DIM>(G, F, in.U, B, f, i, setup);
+}
+
+void launch_bc(const Grid &G, const double *const U[5], double *const bufs[3][5], const Fields &F, bool setup,
+               cudaStream_t s)
+{
+    long long most = 0;
+    for (int f = 0; f < 2 * G.dim; f++)
+        if (G.bc[f] != SHOCK_BC_AUTO && bc_face_points(G, f) > most) most = bc_face_points(G, f);
+    if (!most) return;
+    StageIn in;
+    StateBufs B;
+    for (int q = 0; q < 5; q++) {
+        in.U[q] = U[q];
+        for (int k = 0; k < 3; k++) B.U[k][q] = bufs[k][q];
+    }
+    const dim3 grid(blocks_for(most, 256), 2 * G.dim);
+    if (G.dim == 3) k_bc<3><<<grid, 256, 0, s>>>(G, F, in, B, setup);
+    else k_bc<2><<<grid, 256, 0, s>>>(G, F, in, B, setup);
+}
+
 void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s)
 {
     if (G.dim == 3)

@@ -84,6 +84,8 @@ extern "C" int shock_rhs_static(const shock_params *p, const double *geom13, dou
     if (p->mms) return report_error(SHOCK_EINVAL, "shock_rhs_static takes periodic blocks only (mms = 0)");
     for (int a = 0; a < p->dim; a++)
         if (!p->periodic[a]) return report_error(SHOCK_EINVAL, "axis %d is not periodic", a);
+    for (int f = 0; f < 6; f++)
+        if (p->bc[f] != SHOCK_BC_AUTO) return report_error(SHOCK_EINVAL, "face %d: only periodic faces here", f);
     if (p->mach <= 0 || p->reynolds <= 0 || p->gamma <= 1.0) return report_error(SHOCK_EINVAL, "bad physics");
 
     Layout L;

@@ -18,7 +18,9 @@
  *     into U_lastStep (InitializeManufacturedSolution and the boundary
  *     fill) as Dirichlet values and J*S from SHOCK's own
  *     AddManufacturedSolutionSource as the source.
- * Faces of any other kind (walls, inflow, outflow, farfield) are rejected
+ *   - "BCWallViscous", "BCWallInviscid" and "BCFarfield" faces as
+ *     SHOCK_BC_WALL_VISCOUS, SHOCK_BC_WALL_INVISCID, SHOCK_BC_FARFIELD.
+ * Faces of any other kind (isothermal walls, inflow, outflow) are rejected
  * by the library with SHOCK_EINVAL.
  */
 #include <stdio.h>
@@ -95,6 +97,14 @@ int GPU_Create(struct strct_configuration *c, struct strct_mesh *m, struct strct
     sp.periodic[1] = self_periodic(c, c->InterfaceNeighbourBottom, c->InterfaceNeighbourTop, 1, &sp.period[1]);
     if (MESHDIMENSIONS == 3)
         sp.periodic[2] = self_periodic(c, c->InterfaceNeighbourBehind, c->InterfaceNeighbourInFront, 2, &sp.period[2]);
+    /* faces that are not interfaces: the BC names src/Load.c:46-97 assigned */
+    const char *face[6] = {c->BC_Left, c->BC_Right, c->BC_Bottom, c->BC_Top, c->BC_Behind, c->BC_InFront};
+    for (int f = 0; f < 2 * MESHDIMENSIONS; f++) {
+        if (sp.periodic[f / 2]) continue;
+        if (strcmp(face[f], c->BCWallViscous) == 0) sp.bc[f] = SHOCK_BC_WALL_VISCOUS;
+        else if (strcmp(face[f], c->BCWallInviscid) == 0) sp.bc[f] = SHOCK_BC_WALL_INVISCID;
+        else if (strcmp(face[f], c->BCFarfield) == 0) sp.bc[f] = SHOCK_BC_FARFIELD;
+    }
     const char *prec = getenv("SHOCK_B200_PRECISION");
     sp.precision = (prec && strcmp(prec, "mixed") == 0) ? SHOCK_MIXED : SHOCK_FP64;
     sp.zeta_fix = 0;

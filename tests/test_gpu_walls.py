@@ -1,0 +1,83 @@
+"""Wall and farfield faces on the GPU against SHOCK's own BC code.
+
+The reference is SHOCK's CPU build with the face BC names set as its
+loader sets them (BCWallViscous, BCWallInviscid, BCFarfield; src/BC.c).
+Tolerances as in test_gpu_parity.py: one right-hand side within
+max(1e-12, 2 * SHOCK's own FP64-vs-80-bit distance) per variable, and the
+state after 20 RK steps within 1e-10 relative L2.
+"""
+import numpy as np
+import pytest
+
+import shock_b200
+from _util import l2_rel, real, rel_err
+from refbind import DropinSolver, RefSolver, dropin_available, ref_available
+from shock_b200 import cases
+
+pytestmark = pytest.mark.gpu
+
+RHS_TOL = 1e-12
+L2_TOL = 1e-10
+
+CASES = {
+    "noslip_3d_w5": lambda: cases.channel(3, 5, (16, 12, 14), bc="wall_viscous", stretch=1.2),
+    "slip_3d_w9_euler": lambda: cases.channel(3, 9, (14, 12, 14), bc="wall_inviscid", inviscid=True),
+    "farfield_3d_w5": lambda: cases.channel(3, 5, (16, 12, 14), bc="farfield"),
+    "noslip_2d_w5": lambda: cases.channel(2, 5, (24, 20, 1), bc="wall_viscous", stretch=1.0),
+    "slip_2d_w9": lambda: cases.channel(2, 9, (24, 20, 1), bc="wall_inviscid"),
+    "noslip_box_2d_w5": lambda: cases.channel(2, 5, (20, 18, 1), bc="wall_viscous", walls_i=True),
+}
+
+
+def _need(c):
+    if not ref_available(c.order, c.dim) or not ref_available(c.order, c.dim, extended=True):
+        pytest.skip("reference build not present")
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_wall_rhs_matches_reference(name):
+    c = CASES[name]()
+    _need(c)
+    q = real(c, shock_b200.Solver(c).rhs())
+    ref, ref80 = real(c, RefSolver(c).rhs()), real(c, RefSolver(c, extended=True).rhs())
+    tol = np.maximum(RHS_TOL, 2.0 * rel_err(ref, ref80))
+    assert (rel_err(q, ref) <= tol).all(), (rel_err(q, ref), tol)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_wall_steps_match_reference(name):
+    c = CASES[name]()
+    _need(c)
+    s = shock_b200.Solver(c)
+    r = RefSolver(c)
+    s.steps(20)
+    r.steps(20)
+    err = l2_rel(real(c, s.state()), real(c, r.state()[:5]))
+    assert (err <= L2_TOL).all(), err
+
+
+def test_wall_mixed_precision_l2():
+    c = cases.channel(3, 5, (16, 12, 14), bc="wall_viscous", stretch=1.2)
+    a = shock_b200.Solver(c)
+    b = shock_b200.Solver(c, precision=shock_b200.SHOCK_MIXED)
+    a.steps(20)
+    b.steps(20)
+    err = l2_rel(real(c, b.state()), real(c, a.state()))
+    assert (err <= 1e-6).all(), err
+
+
+def test_wall_dropin_loop_matches_reference_loop():
+    c = CASES["noslip_3d_w5"]()
+    if not dropin_available(c.order, c.dim):
+        pytest.skip("drop-in harness not built")
+    r = RefSolver(c)
+    r.steps(20)
+    d = DropinSolver(c, device=0)
+    try:
+        d.steps(20)
+        d.sync()
+        st = real(c, d.state()[:5])
+    finally:
+        d.close()
+    err = l2_rel(st, real(c, r.state()[:5]))
+    assert (err <= L2_TOL).all(), err

@@ -1,0 +1,51 @@
+"""Wall and farfield faces on the host (no GPU): the block geometry built by
+the library (ghost metric mirrored at wall and farfield faces,
+src/Functions.c:6849-7015) against SHOCK's own set-up, bitwise; and the
+argument checks of the boundary-condition field."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+import shock_b200
+from refbind import RefSolver, ref_available
+from shock_b200 import cases
+
+CASES = [
+    (3, 5, (16, 12, 14), "wall_viscous", 1.2, False),
+    (3, 9, (14, 12, 14), "wall_inviscid", 0.0, False),
+    (2, 5, (24, 20, 1), "farfield", 0.0, False),
+    (2, 5, (20, 18, 1), "wall_viscous", 1.0, True),
+]
+
+
+@pytest.mark.parametrize("dim,order,n,bc,stretch,walls_i", CASES)
+def test_wall_geometry_matches_reference(dim, order, n, bc, stretch, walls_i):
+    if not ref_available(order, dim):
+        pytest.skip("reference build not present")
+    c = cases.channel(dim, order, n, bc=bc, stretch=stretch, walls_i=walls_i)
+    assert np.array_equal(shock_b200.host_geometry(c), RefSolver(c).geometry())
+
+
+def test_bc_argument_checks():
+    c = cases.channel(2, 5, (24, 20, 1), bc="wall_viscous")
+    lib = shock_b200.lib()
+    out = np.zeros((13,) + (c.ni + 6, c.nj + 6, 1))
+    x, y, z = (np.ascontiguousarray(a.transpose(2, 1, 0)).ravel() for a in (c.x, c.y, c.z))
+    dp = C.POINTER(C.c_double)
+
+    def geom(p):
+        return lib.shock_host_geometry(C.byref(p), x.ctypes.data_as(dp), y.ctypes.data_as(dp),
+                                       z.ctypes.data_as(dp), out.ctypes.data_as(dp))
+
+    ok = shock_b200.params_from_case(c)
+    assert geom(ok) == 0
+    bad = shock_b200.params_from_case(c)
+    bad.bc[0] = 1                      # a wall on a periodic axis
+    assert geom(bad) == shock_b200.SHOCK_EINVAL
+    bad = shock_b200.params_from_case(c)
+    bad.bc[2] = 7                      # unknown type
+    assert geom(bad) == shock_b200.SHOCK_EINVAL
+    bad = shock_b200.params_from_case(c)
+    bad.bc[2] = 0                      # a non-periodic face with nothing to fill it
+    assert geom(bad) == shock_b200.SHOCK_EINVAL
