@@ -43,6 +43,7 @@ extern "C" {
 #define SHOCK_BC_WALL_VISCOUS 1   /* "BCWallViscous": no-slip adiabatic wall (src/BC.c:2657-2686) */
 #define SHOCK_BC_WALL_INVISCID 2  /* "BCWallInviscid": slip wall (src/BC.c:2688-2719) */
 #define SHOCK_BC_FARFIELD 3       /* "BCFarfield": zero-gradient copy (src/BC.c:2817-2859) */
+#define SHOCK_BC_WALL_ISOTHERMAL 4 /* "BCWallViscousIsothermal": no-slip wall at T_wall (src/BC.c:2943-2977) */
 
 #define SHOCK_FP64 0        /* everything in FP64 (reference precision) */
 #define SHOCK_MIXED 1       /* FP32 WENO/viscous stencils, FP64 state/RK/metric/p-T recovery */
@@ -71,6 +72,7 @@ typedef struct shock_params {
     int bc[6];          /* per face in SHOCK's order Left, Right (i), Bottom, Top (j), Behind, InFront (k):
                            SHOCK_BC_* (the CGNS BC type src/Load.c:46-97 assigns); SHOCK_BC_AUTO on
                            every face of a periodic axis; zero-initialised callers get SHOCK_BC_AUTO */
+    double t_wall;      /* [BoundaryConditions] T_wall: ghost temperature of isothermal walls (SHOCK's default 1) */
 } shock_params;
 
 typedef struct shock_ctx shock_ctx;

@@ -53,7 +53,9 @@ typedef struct {
     int mms_case;
     int periodic[3];
     double period[3];
-    int bc[6];          /* per face (Left..InFront): 0 none, 1 BCWallViscous, 2 BCWallInviscid, 3 BCFarfield */
+    int bc[6];          /* per face (Left..InFront): 0 none, 1 BCWallViscous, 2 BCWallInviscid, 3 BCFarfield,
+                           4 BCWallViscousIsothermal */
+    double t_wall;      /* [BoundaryConditions] T_wall (src/Import.c:96) */
 } ref_params;
 
 static struct strct_configuration cfg;
@@ -173,9 +175,10 @@ int ref_init(const ref_params *p, const double *x, const double *y, const double
     {
         /* face BC names as src/Load.c:46-97 assigns them from the CGNS BC types */
         char *side[6] = {cfg.BC_Left, cfg.BC_Right, cfg.BC_Bottom, cfg.BC_Top, cfg.BC_Behind, cfg.BC_InFront};
-        const char *name[4] = {NULL, cfg.BCWallViscous, cfg.BCWallInviscid, cfg.BCFarfield};
+        const char *name[5] = {NULL, cfg.BCWallViscous, cfg.BCWallInviscid, cfg.BCFarfield, cfg.BCWallViscousIsothermal};
         for (int f = 0; f < 6; f++)
-            if (p->bc[f] >= 1 && p->bc[f] <= 3) strcpy(side[f], name[p->bc[f]]);
+            if (p->bc[f] >= 1 && p->bc[f] <= 4) strcpy(side[f], name[p->bc[f]]);
+        cfg.T_wall = p->t_wall;
     }
 
     vx.ptr = (void *)x; vx.dt = RealDouble;

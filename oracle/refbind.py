@@ -37,7 +37,7 @@ class RefParams(C.Structure):
         ("t0", C.c_double), ("l0", C.c_double),
         ("inviscid", C.c_int), ("mms", C.c_int), ("mms_case", C.c_int),
         ("periodic", C.c_int * 3), ("period", C.c_double * 3),
-        ("bc", C.c_int * 6),
+        ("bc", C.c_int * 6), ("t_wall", C.c_double),
     ]
 
 
@@ -84,6 +84,7 @@ class RefSolver:
             p.period[a] = case.period[a]
         for f in range(6):
             p.bc[f] = int(getattr(case, "bc", (0,) * 6)[f])
+        p.t_wall = float(getattr(case, "t_wall", 1.0))
         self.params = p
         f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
         x, y, z, u, v, w, pr, rho = (f(a) for a in case.real_fields())

@@ -34,6 +34,7 @@ SHOCK_BC_AUTO = 0
 SHOCK_BC_WALL_VISCOUS = 1
 SHOCK_BC_WALL_INVISCID = 2
 SHOCK_BC_FARFIELD = 3
+SHOCK_BC_WALL_ISOTHERMAL = 4
 
 _lib = None
 _lock = threading.Lock()
@@ -59,7 +60,7 @@ class Params(C.Structure):
         ("inviscid", C.c_int), ("mms", C.c_int),
         ("periodic", C.c_int * 3), ("period", C.c_double * 3),
         ("precision", C.c_int), ("zeta_fix", C.c_int),
-        ("bc", C.c_int * 6),
+        ("bc", C.c_int * 6), ("t_wall", C.c_double),
     ]
 
 
@@ -141,6 +142,7 @@ def params_from_case(case, precision=SHOCK_FP64, zeta_fix=False) -> Params:
     p.zeta_fix = int(bool(zeta_fix))
     for f in range(6):
         p.bc[f] = int(case.bc[f])
+    p.t_wall = float(case.t_wall)
     return p
 
 

@@ -63,6 +63,7 @@ class Case:
     periodic: Tuple[bool, bool, bool] = (True, True, True)
     period: Tuple[float, float, float] = (1.0, 1.0, 1.0)
     bc: Tuple[int, int, int, int, int, int] = (0, 0, 0, 0, 0, 0)   # SHOCK_BC_* per face (Left..InFront)
+    t_wall: float = 1.0             # [BoundaryConditions] T_wall (isothermal walls)
     name: str = "case"
 
     @property
@@ -153,14 +154,15 @@ def smooth_random(dim: int, order: int, n: Tuple[int, int, int], seed: int = 0,
     return c
 
 
-BC_NAMES = {"wall_viscous": 1, "wall_inviscid": 2, "farfield": 3}
+BC_NAMES = {"wall_viscous": 1, "wall_inviscid": 2, "farfield": 3, "wall_isothermal": 4}
 
 
 def channel(dim: int, order: int, n: Tuple[int, int, int], bc: str = "wall_viscous", seed: int = 0,
             mach: float = 0.3, reynolds: float = 500.0, inviscid: bool = False, time_order: int = 4,
-            stretch: float = 0.0, walls_i: bool = False) -> Case:
+            stretch: float = 0.0, walls_i: bool = False, prandtl: float = 0.72, t_wall: float = 1.0) -> Case:
     """Wall-bounded block: periodic in x (and z in 3D), the two y faces of
-    type ``bc`` (SHOCK's BCWallViscous / BCWallInviscid / BCFarfield).  The
+    type ``bc`` (SHOCK's BCWallViscous / BCWallInviscid / BCFarfield /
+    BCWallViscousIsothermal at t_wall).  The
     wall-normal grid spans [0, 1] with both end points on the walls and an
     optional tanh clustering towards them.  Initial state: a parabolic
     streamwise profile plus smooth seeded perturbations.  walls_i=True also
@@ -193,8 +195,8 @@ def channel(dim: int, order: int, n: Tuple[int, int, int], bc: str = "wall_visco
     if walls_i:
         faces[0] = faces[1] = t
     c = Case(dim=dim, order=order, ni=ni, nj=nj, nk=nk, x=x, y=y, z=z, rho=rho, u=u, v=v, w=w, p=p,
-             time_order=time_order, mach=mach, reynolds=reynolds, inviscid=inviscid,
-             periodic=(not walls_i, False, dim == 3), period=(Lx, 1.0, Lz), bc=tuple(faces),
+             time_order=time_order, mach=mach, reynolds=reynolds, inviscid=inviscid, prandtl=prandtl,
+             periodic=(not walls_i, False, dim == 3), period=(Lx, 1.0, Lz), bc=tuple(faces), t_wall=t_wall,
              name=f"channel{dim}d_w{order}_{bc}")
     c.tau = cfl_tau(c)
     return c

@@ -118,9 +118,13 @@ Phys make_phys(const shock_params &p)
     for (int f = 0; f < 6; f++)
         for (int q = 0; q < 3; q++) {
             const int b = f < 2 * p.dim ? p.bc[f] : SHOCK_BC_AUTO;
-            P.mcorr[f][q] = b == SHOCK_BC_WALL_VISCOUS ? -1.0 : (b == SHOCK_BC_WALL_INVISCID && q == f / 2) ? -1.0 : 1.0;
+            const bool noslip = b == SHOCK_BC_WALL_VISCOUS || b == SHOCK_BC_WALL_ISOTHERMAL;
+            P.mcorr[f][q] = noslip ? -1.0 : (b == SHOCK_BC_WALL_INVISCID && q == f / 2) ? -1.0 : 1.0;
             if (b != SHOCK_BC_AUTO) P.walls = 1;
         }
+    P.t_wall = p.t_wall;
+    P.gam_w = 1.0 / ((p.gamma - 1.0) * (p.mach * p.mach) * p.reynolds * 0.72);
+    for (int a = 0; a < 3; a++) P.iso_hi[a] = a < p.dim && p.bc[2 * a + 1] == SHOCK_BC_WALL_ISOTHERMAL;
     return P;
 }
 
@@ -138,7 +142,7 @@ static void enqueue_rhs(shock_ctx *c, double *const in[5], int &nk)
     launch_prim(c->G, c->P, cin, c->F, s);
     nk++;
     if (c->P.walls) {
-        launch_bc(c->G, cin, c->buf, c->F, false, s);
+        launch_bc(c->G, c->P, cin, c->buf, c->F, false, s);
         nk++;
     }
     if (!c->p.inviscid) {
@@ -213,7 +217,7 @@ static int check_faces(const shock_params *p)
     for (int a = 0; a < p->dim; a++)
         for (int side = 0; side < 2; side++) {
             const int f = 2 * a + side, b = p->bc[f];
-            if (b < SHOCK_BC_AUTO || b > SHOCK_BC_FARFIELD) return fail(SHOCK_EINVAL, "face %d: unknown bc %d", f, b);
+            if (b < SHOCK_BC_AUTO || b > SHOCK_BC_WALL_ISOTHERMAL) return fail(SHOCK_EINVAL, "face %d: unknown bc %d", f, b);
             if (p->periodic[a] && b != SHOCK_BC_AUTO)
                 return fail(SHOCK_EINVAL, "face %d: a periodic axis takes SHOCK_BC_AUTO", f);
             if (!p->periodic[a] && b == SHOCK_BC_AUTO && !p->mms)
@@ -292,7 +296,7 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
         for (int f = 0; f < 5; f++) cudaMemcpy(c->buf[b][f], hb.prim[f].data(), nb, cudaMemcpyHostToDevice);
     if (c->P.walls) {
         const double *b0[5] = {c->buf[0][0], c->buf[0][1], c->buf[0][2], c->buf[0][3], c->buf[0][4]};
-        launch_bc(G, b0, c->buf, c->F, true, c->stream);
+        launch_bc(G, c->P, b0, c->buf, c->F, true, c->stream);
         cudaStreamSynchronize(c->stream);
     }
     c->geo_host = std::move(hb.geo);

@@ -89,6 +89,7 @@ extern "C" int shock_params_from_ini(const char *path, shock_params *p)
     num("fluidproperties:r", p->gas_r);
     num("fluidproperties:t", p->t0);
     num("fluidproperties:l", p->l0);
+    num("boundaryconditions:t_wall", p->t_wall);
     boolean("options:inviscid", p->inviscid);
     boolean("options:manufacturedsolution", p->mms);
     return SHOCK_OK;

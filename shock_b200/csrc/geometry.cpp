@@ -66,7 +66,7 @@ void mirror_metric(const Layout &L, const shock_params &p, std::vector<std::vect
 {
     for (int f = 0; f < 2 * p.dim; f++) {
         const int b = p.bc[f];
-        if (b != SHOCK_BC_WALL_VISCOUS && b != SHOCK_BC_WALL_INVISCID && b != SHOCK_BC_FARFIELD) continue;
+        if (b == SHOCK_BC_AUTO) continue;   // every wall type and farfield (src/Functions.c:6856-6862)
         const int a = f / 2, side = f % 2;
         int idx[3];
         for (int l = 0; l < L.g; l++) {

@@ -242,7 +242,7 @@ __host__ __device__ inline long long bc_face_points(const Grid &G, int f)
 
 template <int DIM>
 __device__ __forceinline__ void bc_body(const Grid &G, const Fields &F, const double *const *in, const StateBufs &B,
-                                        int f, long long idx, bool setup)
+                                        int f, long long idx, bool setup, double t_wall)
 {
     const int a = f / 2, side = f % 2;
     const int tb = a == 0 ? 1 : 0, tc = a == 2 ? 1 : 2;   // tangential axes (tc = 2 is flat in 2D)
@@ -260,7 +260,7 @@ __device__ __forceinline__ void bc_body(const Grid &G, const Fields &F, const do
     const int type = G.bc[f];
     const double rho = in[0][s], u = in[1][s], vv = in[2][s], w = in[3][s], e = in[4][s];
     double gv[3];
-    if (type == SHOCK_BC_WALL_VISCOUS) {
+    if (type == SHOCK_BC_WALL_VISCOUS || type == SHOCK_BC_WALL_ISOTHERMAL) {
         gv[0] = -u; gv[1] = -vv; gv[2] = -w;
     } else if (type == SHOCK_BC_FARFIELD) {
         gv[0] = u; gv[1] = vv; gv[2] = w;
@@ -305,7 +305,7 @@ __device__ __forceinline__ void bc_body(const Grid &G, const Fields &F, const do
     }
     if (!setup) {
         F.p[o] = F.p[s];
-        F.T[o] = F.T[s];
+        F.T[o] = type == SHOCK_BC_WALL_ISOTHERMAL ? t_wall : F.T[s];
         F.c[o] = F.c[s];
         F.mu[o] = F.mu[s];
     }
@@ -1514,7 +1514,11 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
         if (DIM == 3) F.Q[3][o] = q3 + psi * (gp[2] - gmn[2]);
         double Aterm = vel[0] * (gp[0] - gmn[0]) + vel[1] * (gp[1] - gmn[1]);
         if (DIM == 3) Aterm += vel[2] * (gp[2] - gmn[2]);
-        F.Q[4][o] = q4 + 0.5 * (P.gam + P.gam) * (hp - hm) + psi * (Aterm + nodeB);
+        // heat flux: SHOCK weights the whole difference with the Gamma average of
+        // the cell and its upper neighbour (src/ZD.c:194), which differs only
+        // at the last cell below an isothermal wall (src/BC.c:2975-2976)
+        const double gup = (P.walls && P.iso_hi[D] && T.c0 + cr == G.g + T.nD - 1) ? P.gam_w : P.gam;
+        F.Q[4][o] = q4 + 0.5 * (gup + P.gam) * (hp - hm) + psi * (Aterm + nodeB);
     }
 #undef SH
 #undef FO

@@ -152,17 +152,17 @@ void launch_ghosts(const Grid &G, double *const U[5], cudaStream_t s)
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(256) k_bc(Grid G, Fields F, StageIn in, StateBufs B, bool setup)
+__global__ void __launch_bounds__(256) k_bc(Grid G, Fields F, StageIn in, StateBufs B, bool setup, double t_wall)
 {
     const int f = blockIdx.y;
     if (G.bc[f] == SHOCK_BC_AUTO) return;
     const long long n = bc_face_points(G, f);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        bc_body<DIM>(G, F, in.U, B, f, i, setup);
+        bc_body<DIM>(G, F, in.U, B, f, i, setup, t_wall);
 }
 
-void launch_bc(const Grid &G, const double *const U[5], double *const bufs[3][5], const Fields &F, bool setup,
-               cudaStream_t s)
+void launch_bc(const Grid &G, const Phys &P, const double *const U[5], double *const bufs[3][5], const Fields &F,
+               bool setup, cudaStream_t s)
 {
     long long most = 0;
     for (int f = 0; f < 2 * G.dim; f++)
@@ -175,8 +175,8 @@ void launch_bc(const Grid &G, const double *const U[5], double *const bufs[3][5]
         for (int k = 0; k < 3; k++) B.U[k][q] = bufs[k][q];
     }
     const dim3 grid(blocks_for(most, 256), 2 * G.dim);
-    if (G.dim == 3) k_bc<3><<<grid, 256, 0, s>>>(G, F, in, B, setup);
-    else k_bc<2><<<grid, 256, 0, s>>>(G, F, in, B, setup);
+    if (G.dim == 3) k_bc<3><<<grid, 256, 0, s>>>(G, F, in, B, setup, P.t_wall);
+    else k_bc<2><<<grid, 256, 0, s>>>(G, F, in, B, setup, P.t_wall);
 }
 
 void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s)

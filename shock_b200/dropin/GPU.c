@@ -18,10 +18,11 @@
  *     into U_lastStep (InitializeManufacturedSolution and the boundary
  *     fill) as Dirichlet values and J*S from SHOCK's own
  *     AddManufacturedSolutionSource as the source.
- *   - "BCWallViscous", "BCWallInviscid" and "BCFarfield" faces as
- *     SHOCK_BC_WALL_VISCOUS, SHOCK_BC_WALL_INVISCID, SHOCK_BC_FARFIELD.
- * Faces of any other kind (isothermal walls, inflow, outflow) are rejected
- * by the library with SHOCK_EINVAL.
+ *   - "BCWallViscous", "BCWallInviscid", "BCFarfield" and
+ *     "BCWallViscousIsothermal" faces as the SHOCK_BC_* types, with
+ *     [BoundaryConditions] T_wall.
+ * Faces of any other kind (moving walls, inflow, outflow) are rejected by
+ * the library with SHOCK_EINVAL.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -104,7 +105,9 @@ int GPU_Create(struct strct_configuration *c, struct strct_mesh *m, struct strct
         if (strcmp(face[f], c->BCWallViscous) == 0) sp.bc[f] = SHOCK_BC_WALL_VISCOUS;
         else if (strcmp(face[f], c->BCWallInviscid) == 0) sp.bc[f] = SHOCK_BC_WALL_INVISCID;
         else if (strcmp(face[f], c->BCFarfield) == 0) sp.bc[f] = SHOCK_BC_FARFIELD;
+        else if (strcmp(face[f], c->BCWallViscousIsothermal) == 0) sp.bc[f] = SHOCK_BC_WALL_ISOTHERMAL;
     }
+    sp.t_wall = c->T_wall;
     const char *prec = getenv("SHOCK_B200_PRECISION");
     sp.precision = (prec && strcmp(prec, "mixed") == 0) ? SHOCK_MIXED : SHOCK_FP64;
     sp.zeta_fix = 0;

@@ -1,7 +1,8 @@
 """Wall and farfield faces on the GPU against SHOCK's own BC code.
 
 The reference is SHOCK's CPU build with the face BC names set as its
-loader sets them (BCWallViscous, BCWallInviscid, BCFarfield; src/BC.c).
+loader sets them (BCWallViscous, BCWallInviscid, BCFarfield,
+BCWallViscousIsothermal; src/BC.c).
 Tolerances as in test_gpu_parity.py: one right-hand side within
 max(1e-12, 2 * SHOCK's own FP64-vs-80-bit distance) per variable, and the
 state after 20 RK steps within 1e-10 relative L2.
@@ -26,6 +27,10 @@ CASES = {
     "noslip_2d_w5": lambda: cases.channel(2, 5, (24, 20, 1), bc="wall_viscous", stretch=1.0),
     "slip_2d_w9": lambda: cases.channel(2, 9, (24, 20, 1), bc="wall_inviscid"),
     "noslip_box_2d_w5": lambda: cases.channel(2, 5, (20, 18, 1), bc="wall_viscous", walls_i=True),
+    # Prandtl 0.7 != the 0.72 SHOCK hard-codes for the wall's Gamma
+    "isothermal_3d_w5": lambda: cases.channel(3, 5, (16, 12, 14), bc="wall_isothermal", stretch=1.2,
+                                              prandtl=0.7, t_wall=1.05),
+    "isothermal_2d_w9": lambda: cases.channel(2, 9, (24, 20, 1), bc="wall_isothermal", prandtl=0.7, t_wall=0.95),
 }
 
 

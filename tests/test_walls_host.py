@@ -16,6 +16,7 @@ CASES = [
     (3, 9, (14, 12, 14), "wall_inviscid", 0.0, False),
     (2, 5, (24, 20, 1), "farfield", 0.0, False),
     (2, 5, (20, 18, 1), "wall_viscous", 1.0, True),
+    (3, 5, (16, 12, 14), "wall_isothermal", 1.2, False),
 ]
 
 
@@ -44,7 +45,7 @@ def test_bc_argument_checks():
     bad.bc[0] = 1                      # a wall on a periodic axis
     assert geom(bad) == shock_b200.SHOCK_EINVAL
     bad = shock_b200.params_from_case(c)
-    bad.bc[2] = 7                      # unknown type
+    bad.bc[2] = 9                      # unknown type
     assert geom(bad) == shock_b200.SHOCK_EINVAL
     bad = shock_b200.params_from_case(c)
     bad.bc[2] = 0                      # a non-periodic face with nothing to fill it
