@@ -80,8 +80,9 @@ typedef struct shock_ctx shock_ctx;
 /* Fill the config.ini keys of *p from a SHOCK config.ini (src/Import.c:36-238,
  * iniparser's rules): [Numerics] TimeOrder, Tau; [FluidProperties] Mach,
  * Reynolds, Prandtl, Gamma, R, T, L; [Options] Inviscid,
- * ManufacturedSolution.  Keys that are absent and all other fields (grid
- * sizes, dim, order, periodicity, precision) are left as they were. */
+ * ManufacturedSolution; [BoundaryConditions] T_wall.  Keys that are absent
+ * and all other fields (grid sizes, dim, order, periodicity, face types,
+ * precision) are left as they were. */
 int shock_params_from_ini(const char *path, shock_params *p);
 
 const char *shock_last_error(void);

@@ -25,6 +25,9 @@ L\t\t\t\t=1.0
 [Options]
 inviscid\t\t\t=TRUE\t;Viscous(0)/Inviscid(1)
 ManufacturedSolution\t\t=no
+
+[BoundaryConditions]
+T_wall\t\t\t\t=1.25
 """
 
 
@@ -36,7 +39,7 @@ def test_params_from_ini(tmp_path):
     p = shock_b200.params_from_ini(str(f), base)
     assert (p.time_order, p.tau, p.mach, p.reynolds) == (3, 0.00025, 0.1, 1600.0)
     assert (p.prandtl, p.gamma, p.gas_r, p.t0, p.l0) == (0.72, 1.4, 287.0, 300.0, 1.0)
-    assert p.inviscid == 1 and p.mms == 0
+    assert p.inviscid == 1 and p.mms == 0 and p.t_wall == 1.25
     assert (p.dim, p.order, p.ni) == (3, 9, 64)      # not config.ini keys: untouched
 
 
