@@ -45,6 +45,7 @@ WORKLOADS = {
     # name: (description, builder)
     "tgv64_w5": "3D curvilinear Taylor-Green vortex 64^3, WENO5, viscous, RK4, Ma=0.1, Re=1600",
     "tgv128_w5": "3D curvilinear Taylor-Green vortex 128^3, WENO5, viscous, RK4",
+    "turb128_w9": "3D decaying turbulence 128^3, WENO9, viscous, RK4, Mt=0.6",
     "turb256_w9": "3D decaying turbulence 256^3, WENO9, viscous, RK4, Mt=0.6",
     "turb512_w9": "3D decaying turbulence 512^3, WENO9, viscous, RK4, Mt=0.6",
     "tgv512_w5": "3D Taylor-Green vortex 512^3, WENO5, viscous, RK4",
@@ -64,6 +65,8 @@ def make_case(name):
         return cases.taylor_green(128, order=5)
     if name == "tgv512_w5":
         return cases.taylor_green(512, order=5)
+    if name == "turb128_w9":
+        return cases.decaying_turbulence(128, order=9)
     if name == "turb256_w9":
         return cases.decaying_turbulence(256, order=9)
     if name == "turb512_w9":
