@@ -331,8 +331,22 @@ __device__ __forceinline__ T phi_w5(const T *d, T eps)
     T is0 = T(13.) * (d[0] - d[1]) * (d[0] - d[1]) + T(3.) * (d[0] - T(3.) * d[1]) * (d[0] - T(3.) * d[1]);
     T is1 = T(13.) * (d[1] - d[2]) * (d[1] - d[2]) + T(3.) * (d[1] + d[2]) * (d[1] + d[2]);
     T is2 = T(13.) * (d[2] - d[3]) * (d[2] - d[3]) + T(3.) * (T(3.) * d[2] - d[3]) * (T(3.) * d[2] - d[3]);
-    T a0 = (is0 + eps) * (is0 + eps), a1 = (is1 + eps) * (is1 + eps), a2 = (is2 + eps) * (is2 + eps);
-    T o0t = wrcp<T>(a0), o1t = T(6.) * wrcp<T>(a1), o2t = T(3.) * wrcp<T>(a2);
+    T o0t, o1t, o2t;
+    if (std::is_same<T, double>::value) {
+        // 1/e0 and 1/e1 from one division (batch inversion): e = IS + eps >= eps,
+        // so e0*e1 >= eps^2, a normal number (eps = 10 sqrt(DBL_MIN)); the
+        // weights then differ from SHOCK's 1/(e*e) by a few ulp
+        const T e0 = is0 + eps, e1 = is1 + eps, e2 = is2 + eps;
+        const T q01 = T(1.) / (e0 * e1), r0 = q01 * e1, r1 = q01 * e0, r2 = T(1.) / e2;
+        o0t = r0 * r0;
+        o1t = T(6.) * (r1 * r1);
+        o2t = T(3.) * (r2 * r2);
+    } else {
+        T a0 = (is0 + eps) * (is0 + eps), a1 = (is1 + eps) * (is1 + eps), a2 = (is2 + eps) * (is2 + eps);
+        o0t = wrcp<T>(a0);
+        o1t = T(6.) * wrcp<T>(a1);
+        o2t = T(3.) * wrcp<T>(a2);
+    }
     T rs = wrcp<T>(o0t + o1t + o2t);
     T o0 = o0t * rs, o2 = o2t * rs;
     T q1 = d[0] - T(2.) * d[1] + d[2];
@@ -414,8 +428,18 @@ __device__ __forceinline__ T phi_w9(const T *f, const T *d, T eps)
         // make it slightly negative and cancel eps (1/t^2 overflows), so the
         // FP32 form clamps it at zero.  The FP64 form keeps SHOCK's sequence.
         if (std::is_same<T, float>::value) acc = acc > T(0) ? acc : T(0);
-        T t = acc + eps;
-        ot[k] = dk[k] * (T(1.) / (t * t));
+        ot[k] = acc + eps;   // t_k; the weights follow
+    }
+    if (std::is_same<T, double>::value) {
+        // reciprocals of t0..t3 from two divisions (batch inversion of pairs,
+        // as in phi_w5), t4 from a third
+        const T q01 = T(1.) / (ot[0] * ot[1]), q23 = T(1.) / (ot[2] * ot[3]);
+        const T r[5] = {q01 * ot[1], q01 * ot[0], q23 * ot[3], q23 * ot[2], T(1.) / ot[4]};
+#pragma unroll
+        for (int k = 0; k < 5; k++) ot[k] = dk[k] * (r[k] * r[k]);
+    } else {
+#pragma unroll
+        for (int k = 0; k < 5; k++) ot[k] = dk[k] * (T(1.) / (ot[k] * ot[k]));
     }
     T rs = T(1.) / (ot[0] + ot[1] + ot[2] + ot[3] + ot[4]);
     T o0 = ot[0] * rs, o2 = ot[2] * rs, o3 = ot[3] * rs, o4 = ot[4] * rs;
