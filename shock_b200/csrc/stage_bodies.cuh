@@ -331,22 +331,8 @@ __device__ __forceinline__ T phi_w5(const T *d, T eps)
     T is0 = T(13.) * (d[0] - d[1]) * (d[0] - d[1]) + T(3.) * (d[0] - T(3.) * d[1]) * (d[0] - T(3.) * d[1]);
     T is1 = T(13.) * (d[1] - d[2]) * (d[1] - d[2]) + T(3.) * (d[1] + d[2]) * (d[1] + d[2]);
     T is2 = T(13.) * (d[2] - d[3]) * (d[2] - d[3]) + T(3.) * (T(3.) * d[2] - d[3]) * (T(3.) * d[2] - d[3]);
-    T o0t, o1t, o2t;
-    if (std::is_same<T, double>::value) {
-        // 1/e0 and 1/e1 from one division (batch inversion): e = IS + eps >= eps,
-        // so e0*e1 >= eps^2, a normal number (eps = 10 sqrt(DBL_MIN)); the
-        // weights then differ from SHOCK's 1/(e*e) by a few ulp
-        const T e0 = is0 + eps, e1 = is1 + eps, e2 = is2 + eps;
-        const T q01 = T(1.) / (e0 * e1), r0 = q01 * e1, r1 = q01 * e0, r2 = T(1.) / e2;
-        o0t = r0 * r0;
-        o1t = T(6.) * (r1 * r1);
-        o2t = T(3.) * (r2 * r2);
-    } else {
-        T a0 = (is0 + eps) * (is0 + eps), a1 = (is1 + eps) * (is1 + eps), a2 = (is2 + eps) * (is2 + eps);
-        o0t = wrcp<T>(a0);
-        o1t = T(6.) * wrcp<T>(a1);
-        o2t = T(3.) * wrcp<T>(a2);
-    }
+    T a0 = (is0 + eps) * (is0 + eps), a1 = (is1 + eps) * (is1 + eps), a2 = (is2 + eps) * (is2 + eps);
+    T o0t = wrcp<T>(a0), o1t = T(6.) * wrcp<T>(a1), o2t = T(3.) * wrcp<T>(a2);
     T rs = wrcp<T>(o0t + o1t + o2t);
     T o0 = o0t * rs, o2 = o2t * rs;
     T q1 = d[0] - T(2.) * d[1] + d[2];
@@ -428,18 +414,8 @@ __device__ __forceinline__ T phi_w9(const T *f, const T *d, T eps)
         // make it slightly negative and cancel eps (1/t^2 overflows), so the
         // FP32 form clamps it at zero.  The FP64 form keeps SHOCK's sequence.
         if (std::is_same<T, float>::value) acc = acc > T(0) ? acc : T(0);
-        ot[k] = acc + eps;   // t_k; the weights follow
-    }
-    if (std::is_same<T, double>::value) {
-        // reciprocals of t0..t3 from two divisions (batch inversion of pairs,
-        // as in phi_w5), t4 from a third
-        const T q01 = T(1.) / (ot[0] * ot[1]), q23 = T(1.) / (ot[2] * ot[3]);
-        const T r[5] = {q01 * ot[1], q01 * ot[0], q23 * ot[3], q23 * ot[2], T(1.) / ot[4]};
-#pragma unroll
-        for (int k = 0; k < 5; k++) ot[k] = dk[k] * (r[k] * r[k]);
-    } else {
-#pragma unroll
-        for (int k = 0; k < 5; k++) ot[k] = dk[k] * (T(1.) / (ot[k] * ot[k]));
+        T t = acc + eps;
+        ot[k] = dk[k] * (T(1.) / (t * t));
     }
     T rs = T(1.) / (ot[0] + ot[1] + ot[2] + ot[3] + ot[4]);
     T o0 = ot[0] * rs, o2 = ot[2] * rs, o3 = ot[3] * rs, o4 = ot[4] * rs;
@@ -617,11 +593,11 @@ __device__ __forceinline__ FaceState<T> face_state(const Phys &P, const double *
 #undef SH
     s.q2 = s.u * s.u + s.v * s.v + s.w * s.w;
     s.ic = T(1) / s.c;
+    s.irho = T(1) / s.rho;
     const T ic2 = s.ic * s.ic;
     s.un = s.u * s.nx + s.v * s.ny + s.w * s.nz;
     s.gc = (s.gm - T(1)) * ic2;
     s.g1c = (s.gm - T(1)) * s.ic;                        // (gamma-1)/c
-    s.irho = T(1) / s.rho;
     s.isc = s.ic * T(0.70710678118654752440);            // 1/(c sqrt 2)
     s.kin = T(1) - T(0.5) * (s.gm - T(1)) * (s.q2 * ic2);
     s.hc = s.q2 / T(2) + s.c * s.c * (T)P.igm1;          // q^2/2 + c^2/(gamma-1)
@@ -744,6 +720,77 @@ __device__ __forceinline__ void project_fp64(const double *sh, int f, int lane, 
 #undef SH
 }
 
+// FP64 WENO weights with fewer divisions.  The reciprocals 1/e of the
+// smoothness terms e = IS + eps of both split stencils of a row come in
+// pairs from one division each (batch inversion: 1/e0 = e1/(e0 e1)); since
+// e >= eps = 10 sqrt(DBL_MIN), a product e0 e1 >= eps^2 is a normal number.
+// The weights then differ from SHOCK's 1/(e*e) by a few ulp.  The
+// normalising sums keep their own division: the product of two of them can
+// overflow near eps.
+__device__ __forceinline__ void w5_terms(const double *d, double eps, double *e)
+{
+    const double is0 = 13. * (d[0] - d[1]) * (d[0] - d[1]) + 3. * (d[0] - 3. * d[1]) * (d[0] - 3. * d[1]);
+    const double is1 = 13. * (d[1] - d[2]) * (d[1] - d[2]) + 3. * (d[1] + d[2]) * (d[1] + d[2]);
+    const double is2 = 13. * (d[2] - d[3]) * (d[2] - d[3]) + 3. * (3. * d[2] - d[3]) * (3. * d[2] - d[3]);
+    e[0] = is0 + eps;
+    e[1] = is1 + eps;
+    e[2] = is2 + eps;
+}
+
+__device__ __forceinline__ double w5_phi(const double *d, const double *r)
+{
+    const double o0t = r[0] * r[0], o1t = 6. * (r[1] * r[1]), o2t = 3. * (r[2] * r[2]);
+    const double rs = 1. / (o0t + o1t + o2t);
+    const double o0 = o0t * rs, o2 = o2t * rs;
+    const double q1 = d[0] - 2. * d[1] + d[2];
+    const double q2 = d[1] - 2. * d[2] + d[3];
+    return 1. / 3. * o0 * q1 + 1. / 6. * (o2 - 0.5) * q2;
+}
+
+__device__ __forceinline__ void w9_terms(const double *f, double eps, double *t)
+{
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        double acc = 0.0;
+        int c = 0;
+#pragma unroll
+        for (int a = 0; a < 5; a++) {
+            double in = w9c<double>(k, c++) * f[k + a];
+#pragma unroll
+            for (int b = a + 1; b < 5; b++) in = in + w9c<double>(k, c++) * f[k + b];
+            acc = (a == 0) ? f[k] * in : acc + f[k + a] * in;
+        }
+        t[k] = acc + eps;
+    }
+}
+
+__device__ __forceinline__ double w9_phi(const double *d, const double *r)
+{
+    const double dk[5] = {1. / 126., 10. / 63., 10. / 21., 20. / 63., 5. / 126.};
+    double ot[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) ot[k] = dk[k] * (r[k] * r[k]);
+    const double rs = 1. / (ot[0] + ot[1] + ot[2] + ot[3] + ot[4]);
+    const double o0 = ot[0] * rs, o2 = ot[2] * rs, o3 = ot[3] * rs, o4 = ot[4] * rs;
+    const double q1 = d[0] - 4. * d[1] + 6. * d[2] - 4. * d[3] + d[4];
+    const double q2 = d[1] - 4. * d[2] + 6. * d[3] - 4. * d[4] + d[5];
+    const double q3 = d[2] - 4. * d[3] + 6. * d[4] - 4. * d[5] + d[6];
+    const double q4 = d[3] - 4. * d[4] + 6. * d[5] - 4. * d[6] + d[7];
+    return 1. / 5. * o0 * q1 + 1. / 20. * o2 * q2 + 1. / 60. * o3 * (3. * q2 - 2. * q3)
+           + 1. / 60. * o4 * (3. * q2 - 2. * q3 + 3. * q4) - 1. / 840. * (39. * q2 - 14. * q3 + 3. * q4);
+}
+
+template <int N>
+__device__ __forceinline__ void pair_reciprocals(const double *e, double *r)
+{
+#pragma unroll
+    for (int k = 0; k < N; k += 2) {
+        const double q = 1. / (e[k] * e[k + 1]);
+        r[k] = q * e[k + 1];
+        r[k + 1] = q * e[k];
+    }
+}
+
 // Phi+ - Phi- of one characteristic field from its projected split fluxes.
 template <int ORDER>
 __device__ __forceinline__ double weno_phi_fp64(const double *Pp, const double *Pm, double eps)
@@ -756,14 +803,22 @@ __device__ __forceinline__ double weno_phi_fp64(const double *Pp, const double *
             dp[q] = Pp[q + 1] - Pp[q];
             dm[q] = Pm[2 * r + 1 - q] - Pm[2 * r - q];
         }
-        return -phi_w5<double>(dp, eps) + phi_w5<double>(dm, eps);
+        double e[6], rc[6];
+        w5_terms(dp, eps, e);
+        w5_terms(dm, eps, e + 3);
+        pair_reciprocals<6>(e, rc);
+        return -w5_phi(dp, rc) + w5_phi(dm, rc + 3);
     }
     double fp[9], fm[9], dp[8], dm[8];
 #pragma unroll
     for (int q = 0; q < 9; q++) { fp[q] = Pp[q]; fm[q] = Pm[2 * r + 1 - q]; }
 #pragma unroll
     for (int q = 0; q < 8; q++) { dp[q] = fp[q + 1] - fp[q]; dm[q] = fm[q] - fm[q + 1]; }
-    return -phi_w9<double>(fp, dp, eps) + phi_w9<double>(fm, dm, eps);
+    double t[10], rc[10];
+    w9_terms(fp, eps, t);
+    w9_terms(fm, eps, t + 5);
+    pair_reciprocals<10>(t, rc);
+    return -w9_phi(dp, rc) + w9_phi(dm, rc + 5);
 }
 
 // Characteristic rows CA and CB (CB < 0: CA alone) of one face.
