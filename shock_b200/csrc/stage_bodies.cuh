@@ -676,6 +676,8 @@ __host__ __device__ constexpr int low_bit(unsigned m) { return (m & 1u) ? 0 : 1 
 
 // (l.F + a l.U) / 2 and (l.F - a l.U) / 2 over the entries of mask M; the
 // products left out are exact zeros, so the sums are those of the full rows.
+// L holds the row already halved (exact), which takes the factor 1/2 out of
+// every point.
 template <unsigned M>
 __device__ __forceinline__ void dot_pm(const double *L, const double *fv, const double *uv, double a, double &pp,
                                        double &pm)
@@ -688,8 +690,8 @@ __device__ __forceinline__ void dot_pm(const double *L, const double *fv, const 
             lf = lf + L[i] * fv[i];
             lu = lu + L[i] * uv[i];
         }
-    pp = 0.5 * (lf + a * lu);
-    pm = 0.5 * (lf - a * lu);
+    pp = lf + a * lu;
+    pm = lf - a * lu;
 }
 
 // Characteristic projection of the 2r+2 stencil points of face f on row LA
@@ -832,6 +834,11 @@ __device__ __forceinline__ void weno_rows_fp64(const Phys &P, const FaceState<do
     double LA[5], LB[5];
     left_row<double>(s, CA, LA[0], LA[1], LA[2], LA[3], LA[4]);
     if (CB >= 0) left_row<double>(s, CB, LB[0], LB[1], LB[2], LB[3], LB[4]);
+#pragma unroll
+    for (int i = 0; i < 5; i++) {   // halved rows (dot_pm)
+        LA[i] *= 0.5;
+        if (CB >= 0) LB[i] *= 0.5;
+    }
     double PpA[NS], PmA[NS], PpB[NS], PmB[NS];
     project_fp64<ORDER, TLN, MA, MB>(sh, f, lane, a, LA, LB, PpA, PmA, PpB, PmB);
     phi[CA] = weno_phi_fp64<ORDER>(PpA, PmA, P.eps64);
@@ -892,7 +899,7 @@ __device__ __forceinline__ float2 dot_pm2(const float *L, const float2 *pv, floa
 #pragma unroll
     for (int i = i0 + 1; i < 5; i++)
         if (M >> i & 1u) acc = fma2(f2(L[i]), pv[i], acc);
-    return mul2(f2(0.5f), fma2(f2(a, -a), f2(acc.y), f2(acc.x)));
+    return fma2(f2(a, -a), f2(acc.y), f2(acc.x));   // L is the halved row
 }
 
 // Mixed WENO5, characteristic rows CA and CB (CB < 0: CA alone) of one face
@@ -906,6 +913,11 @@ __device__ __forceinline__ void weno5_rows_mixed(const FaceState<float> &s, cons
     float LA[5], LB[5];
     left_row<float>(s, CA, LA[0], LA[1], LA[2], LA[3], LA[4]);
     if (CB >= 0) left_row<float>(s, CB, LB[0], LB[1], LB[2], LB[3], LB[4]);
+#pragma unroll
+    for (int i = 0; i < 5; i++) {   // halved rows (dot_pm2)
+        LA[i] *= 0.5f;
+        if (CB >= 0) LB[i] *= 0.5f;
+    }
     float2 pa[5], pb[5];
 #pragma unroll
     for (int q = 0; q < 5; q++) {
@@ -969,6 +981,7 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
             asm volatile("" ::: "memory");
             float L0, L1, L2, L3, L4;
             left_row<float>(s, ch, L0, L1, L2, L3, L4);
+            L0 *= 0.5f; L1 *= 0.5f; L2 *= 0.5f; L3 *= 0.5f; L4 *= 0.5f;   // halved row
             float dp[2 * r + 1], dmv[2 * r + 1];
 #pragma unroll
             for (int q = 0; q <= 2 * r; q++) {
@@ -980,8 +993,8 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
                 const float2 p3 = DL2(3, t, lane), p4 = DL2(4, t, lane);
                 const float lf = L0 * p0.x + L1 * p0.y + L2 * p1.x + L3 * p1.y + L4 * p2.x;
                 const float lu = L0 * p2.y + L1 * p3.x + L2 * p3.y + L3 * p4.x + L4 * p4.y;
-                dp[q] = 0.5f * (lf + a * lu);
-                dmv[q] = 0.5f * (lf - a * lu);
+                dp[q] = lf + a * lu;
+                dmv[q] = lf - a * lu;
             }
             float phi;
             {
