@@ -1243,7 +1243,7 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
     using TS = typename std::conditional<MIXED, float, double>::type;   // stencil arithmetic
     constexpr int H = ZD<ORDER>::H;          // half stencil: l = 0..2H-1 around the face
     constexpr int NP = TLN + 2 * H;
-    constexpr int NV = DIM == 3 ? V3NV : V2NV;
+    constexpr int NV = DIM == 3 ? (int)V3NV : (int)V2NV;
     constexpr int MA = (D == 0) ? 1 : 0;     // 3D: the two non-sweep axes
     constexpr int MB = (D == 2) ? 1 : 2;
     const bool quirk = (DIM == 3 && D == 2 && !P.zeta_fix);
@@ -1824,7 +1824,7 @@ constexpr size_t weno_smem_bytes()
 template <int DIM, int ORDER, int TLN = TL>
 constexpr size_t visc_smem_bytes()
 {
-    return sizeof(double) * ((size_t)(DIM == 3 ? V3NV : V2NV) * (TLN + ORDER + 1) * NLS + 4 * (TLN + 1) * NLS + 16 * NLANE +
+    return sizeof(double) * ((size_t)(DIM == 3 ? (int)V3NV : (int)V2NV) * (TLN + ORDER + 1) * NLS + 4 * (TLN + 1) * NLS + 16 * NLANE +
                              (size_t)ViscCellIn<DIM, ORDER, TLN>::N * TLN * NLANE);
 }
 
