@@ -749,45 +749,54 @@ __device__ __forceinline__ double w5_phi(const double *d, const double *r)
     return 1. / 3. * o0 * q1 + 1. / 6. * (o2 - 0.5) * q2;
 }
 
-__device__ __forceinline__ void w9_terms(const double *f, double eps, double *t)
+// WENO9 smoothness terms t = IS + eps of one stencil (9 values f); the FP32
+// form clamps IS at zero (see phi_w9).
+template <typename T>
+__device__ __forceinline__ void w9_terms(const T *f, T eps, T *t)
 {
 #pragma unroll
     for (int k = 0; k < 5; k++) {
-        double acc = 0.0;
+        T acc = T(0);
         int c = 0;
 #pragma unroll
         for (int a = 0; a < 5; a++) {
-            double in = w9c<double>(k, c++) * f[k + a];
+            T in = w9c<T>(k, c++) * f[k + a];
 #pragma unroll
-            for (int b = a + 1; b < 5; b++) in = in + w9c<double>(k, c++) * f[k + b];
+            for (int b = a + 1; b < 5; b++) in = in + w9c<T>(k, c++) * f[k + b];
             acc = (a == 0) ? f[k] * in : acc + f[k + a] * in;
         }
+        if (std::is_same<T, float>::value) acc = acc > T(0) ? acc : T(0);
         t[k] = acc + eps;
     }
 }
 
-__device__ __forceinline__ double w9_phi(const double *d, const double *r)
+template <typename T>
+__device__ __forceinline__ T w9_phi(const T *d, const T *r)
 {
-    const double dk[5] = {1. / 126., 10. / 63., 10. / 21., 20. / 63., 5. / 126.};
-    double ot[5];
+    const T dk[5] = {T(1. / 126.), T(10. / 63.), T(10. / 21.), T(20. / 63.), T(5. / 126.)};
+    T ot[5];
 #pragma unroll
     for (int k = 0; k < 5; k++) ot[k] = dk[k] * (r[k] * r[k]);
-    const double rs = 1. / (ot[0] + ot[1] + ot[2] + ot[3] + ot[4]);
-    const double o0 = ot[0] * rs, o2 = ot[2] * rs, o3 = ot[3] * rs, o4 = ot[4] * rs;
-    const double q1 = d[0] - 4. * d[1] + 6. * d[2] - 4. * d[3] + d[4];
-    const double q2 = d[1] - 4. * d[2] + 6. * d[3] - 4. * d[4] + d[5];
-    const double q3 = d[2] - 4. * d[3] + 6. * d[4] - 4. * d[5] + d[6];
-    const double q4 = d[3] - 4. * d[4] + 6. * d[5] - 4. * d[6] + d[7];
-    return 1. / 5. * o0 * q1 + 1. / 20. * o2 * q2 + 1. / 60. * o3 * (3. * q2 - 2. * q3)
-           + 1. / 60. * o4 * (3. * q2 - 2. * q3 + 3. * q4) - 1. / 840. * (39. * q2 - 14. * q3 + 3. * q4);
+    const T rs = T(1.) / (ot[0] + ot[1] + ot[2] + ot[3] + ot[4]);
+    const T o0 = ot[0] * rs, o2 = ot[2] * rs, o3 = ot[3] * rs, o4 = ot[4] * rs;
+    const T q1 = d[0] - T(4.) * d[1] + T(6.) * d[2] - T(4.) * d[3] + d[4];
+    const T q2 = d[1] - T(4.) * d[2] + T(6.) * d[3] - T(4.) * d[4] + d[5];
+    const T q3 = d[2] - T(4.) * d[3] + T(6.) * d[4] - T(4.) * d[5] + d[6];
+    const T q4 = d[3] - T(4.) * d[4] + T(6.) * d[5] - T(4.) * d[6] + d[7];
+    return T(1. / 5.) * o0 * q1 + T(1. / 20.) * o2 * q2 + T(1. / 60.) * o3 * (T(3.) * q2 - T(2.) * q3)
+           + T(1. / 60.) * o4 * (T(3.) * q2 - T(2.) * q3 + T(3.) * q4)
+           - T(1. / 840.) * (T(39.) * q2 - T(14.) * q3 + T(3.) * q4);
 }
 
-template <int N>
-__device__ __forceinline__ void pair_reciprocals(const double *e, double *r)
+// In FP32 the clamped terms are at least eps32 = 10 sqrt(FLT_MIN), so a pair
+// product is normal too; a product that overflows gives zero reciprocals,
+// the zero weights 1/(t*t) gives there.
+template <int N, typename T>
+__device__ __forceinline__ void pair_reciprocals(const T *e, T *r)
 {
 #pragma unroll
     for (int k = 0; k < N; k += 2) {
-        const double q = 1. / (e[k] * e[k + 1]);
+        const T q = T(1.) / (e[k] * e[k + 1]);
         r[k] = q * e[k + 1];
         r[k + 1] = q * e[k];
     }
@@ -1005,7 +1014,11 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
                 fm[0] = 0.f;
 #pragma unroll
                 for (int q = 0; q < 8; q++) { fp[q + 1] = fp[q] + dP[q]; fm[q + 1] = fm[q] - dM[q]; }
-                phi = -phi_w9<float>(fp, dP, eps) + phi_w9<float>(fm, dM, eps);
+                float tt[10], rc[10];
+                w9_terms<float>(fp, eps, tt);
+                w9_terms<float>(fm, eps, tt + 5);
+                pair_reciprocals<10>(tt, rc);
+                phi = -w9_phi<float>(dP, rc) + w9_phi<float>(dM, rc + 5);
             }
             add_right_col<float>(s, ch, phi, out);
         }
