@@ -129,7 +129,9 @@ __device__ __forceinline__ void prim_store(const Phys &P, long long o, double rh
     p[o] = pp;
     T[o] = fabs(pr);
     c[o] = sqrt(P.ups * P.gamma * pp / rho);
-    mu[o] = P.mms ? 1.0 : ((1.0 + P.suth) * pow(pr, 1.5) / (pr + P.suth));
+    // Sutherland's law with T^1.5 as T sqrt(T) (pr >= 0): one correctly
+    // rounded square root instead of pow's log and exp, within an ulp of it
+    mu[o] = P.mms ? 1.0 : ((1.0 + P.suth) * (pr * sqrt(pr)) / (pr + P.suth));
 }
 
 // ---------------------------------------------------------------------------
