@@ -856,6 +856,39 @@ __device__ __forceinline__ void weno_rows_fp64(const Phys &P, const FaceState<do
     if (CB >= 0) phi[CB < 0 ? 0 : CB] = weno_phi_fp64<ORDER>(PpB, PmB, P.eps64);
 }
 
+// add_right_col for the diagonal 3D metric, column CH, normal along D
+// (n_D = nd, the other two components exact zeros): the products of the zero
+// components are left out, each remaining entry in the form add_right_col
+// evaluates it, so the sums are unchanged.
+template <int D, int CH>
+__device__ __forceinline__ void add_right_col_diag(const FaceState<double> &s, double phi, double *out)
+{
+    const double nd = D == 0 ? s.nx : D == 1 ? s.ny : s.nz;
+    const double vel[3] = {s.u, s.v, s.w};
+    if (CH == D) {
+        out[0] += nd * phi;
+#pragma unroll
+        for (int k = 0; k < 3; k++) out[1 + k] += vel[k] * nd * phi;
+        out[4] += s.q2 / 2. * nd * phi;
+    } else if (CH < 3) {
+        // column CH of the two with a zero normal component: the momentum of
+        // the third axis A and the energy (src/WENO.c:1176-1200)
+        constexpr int A = 3 - D - CH;
+        // sign of rho*nd in that momentum entry and of vel_A*nd in the energy
+        // entry, from the column's cross-product terms
+        constexpr bool plus = (CH == 0 && D == 2) || (CH == 1 && D == 0) || (CH == 2 && D == 1);
+        out[1 + A] += (plus ? s.rho * nd : -(s.rho * nd)) * phi;
+        out[4] += (s.rho * (plus ? vel[A] * nd : -(vel[A] * nd))) * phi;
+    } else {
+        const double sc = s.isc * phi;
+        const double cn = CH == 3 ? nd * s.c : -(nd * s.c);
+        out[0] += sc;
+#pragma unroll
+        for (int k = 0; k < 3; k++) out[1 + k] += (k == D ? vel[k] + cn : vel[k]) * sc;
+        out[4] += (CH == 3 ? s.hc + s.c * s.un : s.hc - s.c * s.un) * sc;
+    }
+}
+
 // WENO part of the face flux in FP64 (src/WENO.c:296-430): split fluxes
 // F +/- lambda J_{i+1/2} U projected on the characteristic fields, Phi+,
 // Phi-, back-projection.  f: face index in the tile (points f..f+2r+1).
@@ -895,8 +928,16 @@ __device__ __forceinline__ void face_weno_fp64(const Phys &P, const double *sh, 
     }
 #pragma unroll
     for (int q = 0; q < 5; q++) out[q] = 0.0;
+    if (DIM == 3) {
+        add_right_col_diag<D, 0>(s, phi[0], out);
+        add_right_col_diag<D, 1>(s, phi[1], out);
+        add_right_col_diag<D, 2>(s, phi[2], out);
+        add_right_col_diag<D, 3>(s, phi[3], out);
+        add_right_col_diag<D, 4>(s, phi[4], out);
+    } else {
 #pragma unroll
-    for (int ch = 0; ch < 5; ch++) add_right_col<double>(s, ch, phi[ch], out);
+        for (int ch = 0; ch < 5; ch++) add_right_col<double>(s, ch, phi[ch], out);
+    }
 }
 
 // Mixed WENO5: the projected differences of one point, (l.dF + a l.dU)/2 in

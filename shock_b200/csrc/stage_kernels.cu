@@ -69,7 +69,9 @@ __global__ void k_nodal(Grid G, const double *__restrict__ U, const double *__re
 }
 
 // Two tiles per SM, except FP64 WENO9 (its face needs about 170 registers
-// and a 122 KB tile); the mixed WENO9 tile (110 KB, 128 registers) fits twice.
+// and a 122 KB tile); the mixed WENO9 tile (110 KB, 128 registers) fits twice
+// (the driver's own shared-memory carveout gives that; asking for the full
+// carveout for every sweep measured 10 % slower mixed WENO5 sweeps).
 template <int DIM, int ORDER, int D, bool MIXED>
 __global__ void __launch_bounds__(NTHR, (ORDER == 5 || MIXED) ? 2 : 1)
     k_weno(Grid G, Phys P, bool first, const double *__restrict__ R, const double *__restrict__ Uu,
@@ -218,9 +220,6 @@ static void weno_one(const Grid &G, const Phys &P, bool first, const double *con
     constexpr size_t smem = weno_smem_bytes<DIM, ORDER, MIXED>();
     if (!G.order) {
         cudaFuncSetAttribute(k_weno<DIM, ORDER, D, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        // the whole unified L1 as shared memory: two 110 KB mixed WENO9 tiles
-        cudaFuncSetAttribute(k_weno<DIM, ORDER, D, MIXED>, cudaFuncAttributePreferredSharedMemoryCarveout,
-                             (int)cudaSharedmemCarveoutMaxShared);
         return;
     }
     k_weno<DIM, ORDER, D, MIXED><<<sweep_grid<DIM, D>(G), dim3(NLANE, NROWT), smem, s>>>(G, P, first, U[0], U[1],
