@@ -860,16 +860,16 @@ __device__ __forceinline__ void weno_rows_fp64(const Phys &P, const FaceState<do
 // (n_D = nd, the other two components exact zeros): the products of the zero
 // components are left out, each remaining entry in the form add_right_col
 // evaluates it, so the sums are unchanged.
-template <int D, int CH>
-__device__ __forceinline__ void add_right_col_diag(const FaceState<double> &s, double phi, double *out)
+template <int D, int CH, typename T>
+__device__ __forceinline__ void add_right_col_diag(const FaceState<T> &s, T phi, T *out)
 {
-    const double nd = D == 0 ? s.nx : D == 1 ? s.ny : s.nz;
-    const double vel[3] = {s.u, s.v, s.w};
+    const T nd = D == 0 ? s.nx : D == 1 ? s.ny : s.nz;
+    const T vel[3] = {s.u, s.v, s.w};
     if (CH == D) {
         out[0] += nd * phi;
 #pragma unroll
         for (int k = 0; k < 3; k++) out[1 + k] += vel[k] * nd * phi;
-        out[4] += s.q2 / 2. * nd * phi;
+        out[4] += s.q2 / T(2) * nd * phi;
     } else if (CH < 3) {
         // column CH of the two with a zero normal component: the momentum of
         // the third axis A and the energy (src/WENO.c:1176-1200)
@@ -880,8 +880,8 @@ __device__ __forceinline__ void add_right_col_diag(const FaceState<double> &s, d
         out[1 + A] += (plus ? s.rho * nd : -(s.rho * nd)) * phi;
         out[4] += (s.rho * (plus ? vel[A] * nd : -(vel[A] * nd))) * phi;
     } else {
-        const double sc = s.isc * phi;
-        const double cn = CH == 3 ? nd * s.c : -(nd * s.c);
+        const T sc = s.isc * phi;
+        const T cn = CH == 3 ? nd * s.c : -(nd * s.c);
         out[0] += sc;
 #pragma unroll
         for (int k = 0; k < 3; k++) out[1 + k] += (k == D ? vel[k] + cn : vel[k]) * sc;
@@ -1025,8 +1025,16 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
         weno5_rows_mixed<DIM, D, TLN, C1, C2>(s, dl, f, lane, a, eps, phi);
         weno5_rows_mixed<DIM, D, TLN, CF, -1>(s, dl, f, lane, a, eps, phi);
         weno5_rows_mixed<DIM, D, TLN, 3, 4>(s, dl, f, lane, a, eps, phi);
+        if (DIM == 3) {
+            add_right_col_diag<D, 0>(s, phi[0], out);
+            add_right_col_diag<D, 1>(s, phi[1], out);
+            add_right_col_diag<D, 2>(s, phi[2], out);
+            add_right_col_diag<D, 3>(s, phi[3], out);
+            add_right_col_diag<D, 4>(s, phi[4], out);
+        } else {
 #pragma unroll
-        for (int ch = 0; ch < 5; ch++) add_right_col<float>(s, ch, phi[ch], out);
+            for (int ch = 0; ch < 5; ch++) add_right_col<float>(s, ch, phi[ch], out);
+        }
     } else {
 #pragma unroll 1
         for (int ch = 0; ch < 5; ch++) {
