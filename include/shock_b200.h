@@ -44,6 +44,9 @@ extern "C" {
 #define SHOCK_BC_WALL_INVISCID 2  /* "BCWallInviscid": slip wall (src/BC.c:2688-2719) */
 #define SHOCK_BC_FARFIELD 3       /* "BCFarfield": zero-gradient copy (src/BC.c:2817-2859) */
 #define SHOCK_BC_WALL_ISOTHERMAL 4 /* "BCWallViscousIsothermal": no-slip wall at T_wall (src/BC.c:2943-2977) */
+#define SHOCK_BC_INFLOW_SUBSONIC 5   /* "BCInflow*" with Inflow-Normal-Subsonic (src/BC.c:2457-2503) */
+#define SHOCK_BC_INFLOW_SUPERSONIC 6 /* "BCInflow*" with Inflow-Normal-Supersonic (src/BC.c:2505-2542) */
+#define SHOCK_BC_OUTFLOW_SUBSONIC 7  /* "BCOutflow*" with Outflow-Normal-Subsonic (src/BC.c:2544-2570) */
 
 #define SHOCK_FP64 0        /* everything in FP64 (reference precision) */
 #define SHOCK_MIXED 1       /* FP32 WENO/viscous stencils, FP64 state/RK/metric/p-T recovery */
@@ -73,6 +76,11 @@ typedef struct shock_params {
                            SHOCK_BC_* (the CGNS BC type src/Load.c:46-97 assigns); SHOCK_BC_AUTO on
                            every face of a periodic axis; zero-initialised callers get SHOCK_BC_AUTO */
     double t_wall;      /* [BoundaryConditions] T_wall: ghost temperature of isothermal walls (SHOCK's default 1) */
+    double rho_inflow, p_inflow;  /* [BoundaryConditions] rho_inflow, p_inflow (inflow faces) */
+    double p_outflow;             /* [BoundaryConditions] p_outflow (outflow faces) */
+    double u_inflow[3];           /* cos/sin(AoA) * [InitializeValues] u0, 0 (src/Import.c:233-235): the inflow
+                                     velocity, and the velocity SHOCK's Initialize gives every ghost point
+                                     before the first fill (src/Functions.c:1327-1353) */
 } shock_params;
 
 typedef struct shock_ctx shock_ctx;
@@ -80,7 +88,8 @@ typedef struct shock_ctx shock_ctx;
 /* Fill the config.ini keys of *p from a SHOCK config.ini (src/Import.c:36-238,
  * iniparser's rules): [Numerics] TimeOrder, Tau; [FluidProperties] Mach,
  * Reynolds, Prandtl, Gamma, R, T, L; [Options] Inviscid,
- * ManufacturedSolution; [BoundaryConditions] T_wall.  Keys that are absent
+ * ManufacturedSolution; [BoundaryConditions] T_wall, rho_inflow, p_inflow,
+ * p_outflow, and AoA with [InitializeValues] u0 for u_inflow.  Keys that are absent
  * and all other fields (grid sizes, dim, order, periodicity, face types,
  * precision) are left as they were. */
 int shock_params_from_ini(const char *path, shock_params *p);

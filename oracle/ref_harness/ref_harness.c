@@ -56,6 +56,8 @@ typedef struct {
     int bc[6];          /* per face (Left..InFront): 0 none, 1 BCWallViscous, 2 BCWallInviscid, 3 BCFarfield,
                            4 BCWallViscousIsothermal */
     double t_wall;      /* [BoundaryConditions] T_wall (src/Import.c:96) */
+    double rho_inflow, p_inflow, p_outflow;   /* [BoundaryConditions] (src/Import.c:89-94) */
+    double u_inflow[3];                       /* src/Import.c:233-235 */
 } ref_params;
 
 static struct strct_configuration cfg;
@@ -167,6 +169,12 @@ int ref_init(const ref_params *p, const double *x, const double *y, const double
 #if MESHDIMENSIONS == 3
     cfg.zonesize[2] = p->nk;
 #endif
+    cfg.u_inflow = p->u_inflow[0];   /* Initialize gives every point this velocity */
+    cfg.v_inflow = p->u_inflow[1];
+    cfg.w_inflow = p->u_inflow[2];
+    cfg.rho_inflow = p->rho_inflow;
+    cfg.p_inflow = p->p_inflow;
+    cfg.p_out = p->p_outflow;
     cfg.InterfaceNeighbourLeft = cfg.InterfaceNeighbourRight = p->periodic[0] ? 0 : NO_NEIGHBOUR;
     cfg.InterfaceNeighbourBottom = cfg.InterfaceNeighbourTop = p->periodic[1] ? 0 : NO_NEIGHBOUR;
     cfg.InterfaceNeighbourBehind = cfg.InterfaceNeighbourInFront = p->periodic[2] ? 0 : NO_NEIGHBOUR;
@@ -175,10 +183,17 @@ int ref_init(const ref_params *p, const double *x, const double *y, const double
     {
         /* face BC names as src/Load.c:46-97 assigns them from the CGNS BC types */
         char *side[6] = {cfg.BC_Left, cfg.BC_Right, cfg.BC_Bottom, cfg.BC_Top, cfg.BC_Behind, cfg.BC_InFront};
-        const char *name[5] = {NULL, cfg.BCWallViscous, cfg.BCWallInviscid, cfg.BCFarfield, cfg.BCWallViscousIsothermal};
+        const char *name[8] = {NULL, cfg.BCWallViscous, cfg.BCWallInviscid, cfg.BCFarfield, cfg.BCWallViscousIsothermal,
+                               cfg.BCInflow, cfg.BCInflow, cfg.BCOutflow};
         for (int f = 0; f < 6; f++)
-            if (p->bc[f] >= 1 && p->bc[f] <= 4) strcpy(side[f], name[p->bc[f]]);
+            if (p->bc[f] >= 1 && p->bc[f] <= 7) strcpy(side[f], name[p->bc[f]]);
         cfg.T_wall = p->t_wall;
+        /* the one inflow / outflow option of the run (src/Import.c:62-87) */
+        for (int f = 0; f < 6; f++) {
+            if (p->bc[f] == 5) cfg.flag_BC_option_inflow_normal_sub = 1;
+            if (p->bc[f] == 6) cfg.flag_BC_option_inflow_normal_super = 1;
+            if (p->bc[f] == 7) cfg.flag_BC_option_outflow_normal_sub = 1;
+        }
     }
 
     vx.ptr = (void *)x; vx.dt = RealDouble;

@@ -38,6 +38,8 @@ class RefParams(C.Structure):
         ("inviscid", C.c_int), ("mms", C.c_int), ("mms_case", C.c_int),
         ("periodic", C.c_int * 3), ("period", C.c_double * 3),
         ("bc", C.c_int * 6), ("t_wall", C.c_double),
+        ("rho_inflow", C.c_double), ("p_inflow", C.c_double), ("p_outflow", C.c_double),
+        ("u_inflow", C.c_double * 3),
     ]
 
 
@@ -85,6 +87,11 @@ class RefSolver:
         for f in range(6):
             p.bc[f] = int(getattr(case, "bc", (0,) * 6)[f])
         p.t_wall = float(getattr(case, "t_wall", 1.0))
+        p.rho_inflow = float(getattr(case, "rho_inflow", 1.0))
+        p.p_inflow = float(getattr(case, "p_inflow", 1.0))
+        p.p_outflow = float(getattr(case, "p_outflow", 1.0))
+        for a in range(3):
+            p.u_inflow[a] = float(getattr(case, "u_inflow", (0.0, 0.0, 0.0))[a])
         self.params = p
         f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
         x, y, z, u, v, w, pr, rho = (f(a) for a in case.real_fields())

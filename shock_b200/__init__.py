@@ -35,6 +35,9 @@ SHOCK_BC_WALL_VISCOUS = 1
 SHOCK_BC_WALL_INVISCID = 2
 SHOCK_BC_FARFIELD = 3
 SHOCK_BC_WALL_ISOTHERMAL = 4
+SHOCK_BC_INFLOW_SUBSONIC = 5
+SHOCK_BC_INFLOW_SUPERSONIC = 6
+SHOCK_BC_OUTFLOW_SUBSONIC = 7
 
 _lib = None
 _lock = threading.Lock()
@@ -61,6 +64,8 @@ class Params(C.Structure):
         ("periodic", C.c_int * 3), ("period", C.c_double * 3),
         ("precision", C.c_int), ("zeta_fix", C.c_int),
         ("bc", C.c_int * 6), ("t_wall", C.c_double),
+        ("rho_inflow", C.c_double), ("p_inflow", C.c_double), ("p_outflow", C.c_double),
+        ("u_inflow", C.c_double * 3),
     ]
 
 
@@ -143,6 +148,9 @@ def params_from_case(case, precision=SHOCK_FP64, zeta_fix=False) -> Params:
     for f in range(6):
         p.bc[f] = int(case.bc[f])
     p.t_wall = float(case.t_wall)
+    p.rho_inflow, p.p_inflow, p.p_outflow = float(case.rho_inflow), float(case.p_inflow), float(case.p_outflow)
+    for a in range(3):
+        p.u_inflow[a] = float(case.u_inflow[a])
     return p
 
 

@@ -23,6 +23,7 @@ with seeded synthetic data (no dataset is involved):
   * ``smooth_random``    -- smooth random periodic states for parity tests
   * ``channel``          -- wall-bounded blocks (wall / farfield y faces) for the
                             boundary-condition parity tests
+  * ``duct``             -- through-flow blocks (inflow / outflow x faces)
 """
 from __future__ import annotations
 
@@ -64,6 +65,10 @@ class Case:
     period: Tuple[float, float, float] = (1.0, 1.0, 1.0)
     bc: Tuple[int, int, int, int, int, int] = (0, 0, 0, 0, 0, 0)   # SHOCK_BC_* per face (Left..InFront)
     t_wall: float = 1.0             # [BoundaryConditions] T_wall (isothermal walls)
+    rho_inflow: float = 1.0         # [BoundaryConditions] rho_inflow, p_inflow, p_outflow
+    p_inflow: float = 1.0
+    p_outflow: float = 1.0
+    u_inflow: Tuple[float, float, float] = (0.0, 0.0, 0.0)   # cos/sin(AoA)*u0, 0: also SHOCK's Initialize velocity
     name: str = "case"
 
     @property
@@ -154,7 +159,8 @@ def smooth_random(dim: int, order: int, n: Tuple[int, int, int], seed: int = 0,
     return c
 
 
-BC_NAMES = {"wall_viscous": 1, "wall_inviscid": 2, "farfield": 3, "wall_isothermal": 4}
+BC_NAMES = {"wall_viscous": 1, "wall_inviscid": 2, "farfield": 3, "wall_isothermal": 4,
+            "inflow_subsonic": 5, "inflow_supersonic": 6, "outflow_subsonic": 7}
 
 
 def channel(dim: int, order: int, n: Tuple[int, int, int], bc: str = "wall_viscous", seed: int = 0,
@@ -198,6 +204,49 @@ def channel(dim: int, order: int, n: Tuple[int, int, int], bc: str = "wall_visco
              time_order=time_order, mach=mach, reynolds=reynolds, inviscid=inviscid, prandtl=prandtl,
              periodic=(not walls_i, False, dim == 3), period=(Lx, 1.0, Lz), bc=tuple(faces), t_wall=t_wall,
              name=f"channel{dim}d_w{order}_{bc}")
+    c.tau = cfl_tau(c)
+    return c
+
+
+def duct(dim: int, order: int, n: Tuple[int, int, int], inflow: str = "inflow_subsonic", seed: int = 0,
+         mach: float = 0.5, reynolds: float = 500.0, inviscid: bool = False, time_order: int = 4,
+         walls: str = "") -> Case:
+    """Through-flow block: inflow on the x-lower face, subsonic outflow on the
+    x-upper face, periodic in y (and z), or ``walls`` ("wall_viscous", ...)
+    on the y faces.  The inflow state is rho_inflow = p_inflow = 1 moving at
+    u_inflow = (1, 0, 0) (in SHOCK's velocity units, Ma = mach); the initial
+    field is that state with smooth seeded perturbations; p_outflow is 0.98
+    of the inflow pressure."""
+    rng = np.random.default_rng(seed)
+    ni, nj, nk = n[0], n[1], (n[2] if dim == 3 else 1)
+    Lx, Ly, Lz = 2.0, 1.0, 1.0
+    xa = Lx * np.arange(ni) / (ni - 1)
+    ya = Ly * np.arange(nj) / (nj - 1 if walls else nj)
+    za = Lz * np.arange(nk) / nk if dim == 3 else np.zeros(1)
+    x, y, z = np.meshgrid(xa, ya, za, indexing="ij")
+    X, Y, Z = 2 * math.pi * x / Lx, 2 * math.pi * y / Ly, 2 * math.pi * z / Lz
+
+    def pert():
+        f = np.zeros_like(x)
+        for _ in range(2):
+            ky, kz = rng.integers(1, 3), (rng.integers(0, 3) if dim == 3 else 0)
+            f = f + rng.normal() * np.sin(math.pi * x / Lx) * np.sin(ky * Y + kz * Z + rng.uniform(0, 2 * math.pi))
+        return f
+
+    amp = 0.03
+    u = 1.0 + amp * pert()
+    v = amp * pert()
+    w = amp * pert() if dim == 3 else np.zeros_like(x)
+    rho = 1.0 + amp * pert()
+    p = 1.0 + amp * pert()
+    faces = [BC_NAMES[inflow], BC_NAMES["outflow_subsonic"], 0, 0, 0, 0]
+    if walls:
+        faces[2] = faces[3] = BC_NAMES[walls]
+    c = Case(dim=dim, order=order, ni=ni, nj=nj, nk=nk, x=x, y=y, z=z, rho=rho, u=u, v=v, w=w, p=p,
+             time_order=time_order, mach=mach, reynolds=reynolds, inviscid=inviscid,
+             periodic=(False, not walls, dim == 3), period=(Lx, Ly, Lz), bc=tuple(faces),
+             rho_inflow=1.0, p_inflow=1.0, p_outflow=0.98, u_inflow=(1.0, 0.0, 0.0),
+             name=f"duct{dim}d_w{order}_{inflow}")
     c.tau = cfl_tau(c)
     return c
 

@@ -123,6 +123,10 @@ Phys make_phys(const shock_params &p)
             if (b != SHOCK_BC_AUTO) P.walls = 1;
         }
     P.t_wall = p.t_wall;
+    P.rho_in = p.rho_inflow;
+    P.p_in = p.p_inflow;
+    P.p_out = p.p_outflow;
+    for (int a = 0; a < 3; a++) P.u_in[a] = p.u_inflow[a];
     P.gam_w = 1.0 / ((p.gamma - 1.0) * (p.mach * p.mach) * p.reynolds * 0.72);
     for (int a = 0; a < 3; a++) P.iso_hi[a] = a < p.dim && p.bc[2 * a + 1] == SHOCK_BC_WALL_ISOTHERMAL;
     return P;
@@ -141,10 +145,7 @@ static void enqueue_rhs(shock_ctx *c, double *const in[5], int &nk)
     nk += (c->G.periodic[0] || c->G.periodic[1] || c->G.periodic[2]) ? 1 : 0;
     launch_prim(c->G, c->P, cin, c->F, s);
     nk++;
-    if (c->P.walls) {
-        launch_bc(c->G, c->P, cin, c->buf, c->F, false, s);
-        nk++;
-    }
+    if (c->P.walls) nk += launch_bc(c->G, c->P, cin, c->buf, c->F, false, s);
     if (!c->p.inviscid) {
         launch_nodal(c->G, c->p.precision, cin, c->F, s);
         nk++;
@@ -214,10 +215,19 @@ int shock_device_count(int *n)
 // the wall / farfield types.
 static int check_faces(const shock_params *p)
 {
+    bool sub = false, super = false;
+    for (int f = 0; f < 2 * p->dim; f++) {
+        sub |= p->bc[f] == SHOCK_BC_INFLOW_SUBSONIC;
+        super |= p->bc[f] == SHOCK_BC_INFLOW_SUPERSONIC;
+    }
+    if (sub && super)   // SHOCK takes one inflow option per run (src/Import.c:62-75)
+        return fail(SHOCK_EINVAL, "subsonic and supersonic inflow faces in one block");
     for (int a = 0; a < p->dim; a++)
         for (int side = 0; side < 2; side++) {
             const int f = 2 * a + side, b = p->bc[f];
-            if (b < SHOCK_BC_AUTO || b > SHOCK_BC_WALL_ISOTHERMAL) return fail(SHOCK_EINVAL, "face %d: unknown bc %d", f, b);
+            if (b < SHOCK_BC_AUTO || b > SHOCK_BC_OUTFLOW_SUBSONIC) return fail(SHOCK_EINVAL, "face %d: unknown bc %d", f, b);
+            if ((b == SHOCK_BC_INFLOW_SUBSONIC || b == SHOCK_BC_INFLOW_SUPERSONIC) && (p->rho_inflow <= 0 || p->p_inflow <= 0))
+                return fail(SHOCK_EINVAL, "face %d: inflow needs rho_inflow > 0 and p_inflow > 0", f);
             if (p->periodic[a] && b != SHOCK_BC_AUTO)
                 return fail(SHOCK_EINVAL, "face %d: a periodic axis takes SHOCK_BC_AUTO", f);
             if (!p->periodic[a] && b == SHOCK_BC_AUTO && !p->mms)

@@ -8,6 +8,7 @@
 // (grid sizes, dimension and order come from the mesh and the build in
 // SHOCK, so the caller sets them).
 #include <cctype>
+#include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -90,6 +91,20 @@ extern "C" int shock_params_from_ini(const char *path, shock_params *p)
     num("fluidproperties:t", p->t0);
     num("fluidproperties:l", p->l0);
     num("boundaryconditions:t_wall", p->t_wall);
+    num("boundaryconditions:rho_inflow", p->rho_inflow);
+    num("boundaryconditions:p_inflow", p->p_inflow);
+    num("boundaryconditions:p_outflow", p->p_outflow);
+    // inflow velocity (src/Import.c:233-235): angle of attack in degrees and
+    // [InitializeValues] u0, SHOCK's defaults 0 and 1 for a missing one
+    if (kv.count("boundaryconditions:aoa") || kv.count("initializevalues:u0")) {
+        double aoa = 0.0, u0 = 1.0;
+        num("boundaryconditions:aoa", aoa);
+        num("initializevalues:u0", u0);
+        const double pi = 3.14159265358979323846;
+        p->u_inflow[0] = std::cos(aoa / 360 * 2 * pi) * u0;
+        p->u_inflow[1] = std::sin(aoa / 360 * 2 * pi) * u0;
+        p->u_inflow[2] = 0.0;
+    }
     boolean("options:inviscid", p->inviscid);
     boolean("options:manufacturedsolution", p->mms);
     return SHOCK_OK;

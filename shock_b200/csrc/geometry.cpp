@@ -66,7 +66,7 @@ void mirror_metric(const Layout &L, const shock_params &p, std::vector<std::vect
 {
     for (int f = 0; f < 2 * p.dim; f++) {
         const int b = p.bc[f];
-        if (b == SHOCK_BC_AUTO) continue;   // every wall type and farfield (src/Functions.c:6856-6862)
+        if (b == SHOCK_BC_AUTO || b > SHOCK_BC_WALL_ISOTHERMAL) continue;   // walls and farfield only (src/Functions.c:6856-6862)
         const int a = f / 2, side = f % 2;
         int idx[3];
         for (int l = 0; l < L.g; l++) {
@@ -130,10 +130,14 @@ int build_block(const shock_params &p, const double *x, const double *y, const d
     const double ups = 1.0 / (p.gamma * (p.mach * p.mach));
     const double gm = p.gamma;
 
-    // Initialize (src/Functions.c:1327-1353): rho0 = 1, u = v = w = 0, p0 = 1 on every point.
+    // Initialize (src/Functions.c:1327-1353): rho0 = 1, u = u_inflow, p0 = 1 on every point.
+    const double ui = p.u_inflow[0], vi = p.u_inflow[1], wi = p.u_inflow[2];
     for (long long o = 0; o < NG; o++) {
         hb.prim[0][o] = 1.0;
-        hb.prim[4][o] = (0.5 * ((0.0 * 0.0) + (0.0 * 0.0) + (0.0 * 0.0)) + 1.0 / 1.0 / (gm - 1.0) * ups);
+        hb.prim[1][o] = ui;
+        hb.prim[2][o] = vi;
+        hb.prim[3][o] = wi;
+        hb.prim[4][o] = (0.5 * ((ui * ui) + (vi * vi) + (wi * wi)) + 1.0 / 1.0 / (gm - 1.0) * ups);
     }
     // Real points from Fortran order (src/Functions.c:746-877).
     for (int k = 0; k < (dim == 3 ? p.nk : 1); k++)

@@ -57,6 +57,7 @@ struct Phys {
     double mcorr[6][3];  // per face: sign of the u,v,w convective momentum terms in its ghost
                          // points (SHOCK's BC_Corrector_*Momentum, src/WENO.c:265-277)
     double t_wall;       // ghost temperature of isothermal walls
+    double rho_in, p_in, u_in[3], p_out;   // inflow / outflow values
     double gam_w;        // Gamma of isothermal-wall ghost points (Prandtl 0.72, src/BC.c:2975-2976)
     int iso_hi[3];       // the upper face of the axis is an isothermal wall
 };
@@ -171,10 +172,11 @@ void launch_batch_advance(Member *mem, const BatchPlan *plan, int capacity, int 
 // Kernel launchers (stage_kernels.cu).
 void launch_ghosts(const Grid &G, double *const U[5], cudaStream_t s);
 void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s);
-// Wall and farfield ghost layers from state U into all three state buffers
-// (setup: SHOCK's set-up fill, state only); no launch without such faces.
-void launch_bc(const Grid &G, const Phys &P, const double *const U[5], double *const bufs[3][5], const Fields &F,
-               bool setup, cudaStream_t s);
+// Wall, farfield, inflow and outflow ghost layers from state U into all three
+// state buffers (setup: SHOCK's set-up fill, state only); no launch without
+// such faces.
+int launch_bc(const Grid &G, const Phys &P, const double *const U[5], double *const bufs[3][5], const Fields &F,
+              bool setup, cudaStream_t s);   // returns the number of launches
 void launch_nodal(const Grid &G, int precision, const double *const U[5], const Fields &F, cudaStream_t s);
 void launch_weno(const Grid &G, const Phys &P, int precision, int d, bool first,
                  const double *const U[5], const Fields &F, cudaStream_t s);

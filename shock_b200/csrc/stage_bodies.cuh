@@ -216,11 +216,12 @@ __device__ __forceinline__ void nodal_body(const Grid &G, long long o, const dou
 }
 
 // ---------------------------------------------------------------------------
-// Wall and farfield faces (src/BC.c:638-2362; point rules :2657-2719 and
-// :2817-2859).  Ghost layer l of face f (l cells outside the face) mirrors
-// the real point l cells inside, over the face's real tangential range; the
-// edges and corners of the ghost shell are not written (SHOCK's face loops
-// do not reach them).  The state goes to every state buffer: SHOCK fills
+// Wall, farfield, inflow and outflow faces (src/BC.c:638-2362; point rules
+// :2457-2570, :2657-2719, :2817-2859, :2943-2977).  Ghost layer l of face f
+// (l cells outside the face) mirrors the real point l cells inside, over the
+// face's real tangential range (walls, farfield: the edges and corners of
+// the ghost shell are not written) or its ghost-inclusive one (inflow,
+// outflow: later faces then overwrite shared edges, in SHOCK's face order).  The state goes to every state buffer: SHOCK fills
 // U_RK in place, so the next stage's periodic image copy reads the values
 // written here.  setup: the fill of SHOCK's set-up (src/SHOCK.c:237), which
 // runs before any CalcValues: theta is still zero there, so a slip wall gets
@@ -232,70 +233,114 @@ struct StateBufs {
 
 __device__ __forceinline__ double prod3(double x, double y, double z) { return __dmul_rn(__dmul_rn(x, y), z); }
 
+// Inflow and outflow faces fill the ghost-inclusive tangential range, edges
+// and corners included (src/BC.c:1344-2362); wall and farfield faces only
+// the real tangential range (src/BC.c:638-1343).
+__host__ __device__ inline bool bc_full_face(int type) { return type >= SHOCK_BC_INFLOW_SUBSONIC; }
+
 // Number of ghost points face f fills.
 __host__ __device__ inline long long bc_face_points(const Grid &G, int f)
 {
     const int a = f / 2;
+    const bool full = bc_full_face(G.bc[f]);
     long long r = G.g;
     for (int b = 0; b < G.dim; b++)
-        if (b != a) r *= G.n[b];
+        if (b != a) r *= full ? G.N[b] : G.n[b];
     return r;
 }
 
+// Contravariant velocities theta (as CalcValues forms them,
+// src/Functions.c:2406-2440; theta3 stays zero in 2D) of the state u, v, w
+// at point s, every product and sum rounded in SHOCK's order.
 template <int DIM>
-__device__ __forceinline__ void bc_body(const Grid &G, const Fields &F, const double *const *in, const StateBufs &B,
-                                        int f, long long idx, bool setup, double t_wall)
+__device__ __forceinline__ void bc_theta(const Fields &F, long long s, double u, double v, double w, double *th)
+{
+    th[0] = th[1] = th[2] = 0.0;
+    for (int q = 0; q < DIM; q++) {
+        double t = __dadd_rn(__dmul_rn(u, F.m[3 * q][s]), __dmul_rn(v, F.m[3 * q + 1][s]));
+        th[q] = DIM == 3 ? __dadd_rn(t, __dmul_rn(w, F.m[3 * q + 2][s])) : t;
+    }
+}
+
+// u, v, w from the contravariant velocities th with the metric at point o,
+// by Cramer's rule, every product and sum rounded in the order
+// src/BC.c:2697-2699 evaluates them.
+__device__ __forceinline__ void bc_cramer(const Fields &F, long long o, const double *th, double *gv)
+{
+    const double xx = F.m[0][o], xy = F.m[1][o], xz = F.m[2][o];
+    const double ex = F.m[3][o], ey = F.m[4][o], ez = F.m[5][o];
+    const double zx = F.m[6][o], zy = F.m[7][o], zz = F.m[8][o];
+    const double t1 = th[0], t2 = th[1], t3 = th[2];
+    const double du = prod3(-xx, ey, zz) + prod3(xx, ez, zy) + prod3(xy, ex, zz) - prod3(xy, ez, zx)
+                      - prod3(xz, ex, zy) + prod3(xz, ey, zx);
+    const double dw = prod3(xx, ey, zz) - prod3(xx, ez, zy) - prod3(xy, ex, zz) + prod3(xy, ez, zx)
+                      + prod3(xz, ex, zy) - prod3(xz, ey, zx);
+    const double nu = prod3(t1, ey, zz) - prod3(t1, ez, zy) - prod3(t2, xy, zz) + prod3(t2, xz, zy)
+                      + prod3(t3, xy, ez) - prod3(t3, xz, ey);
+    const double nv = prod3(-t1, ex, zz) + prod3(t1, ez, zx) + prod3(t2, xx, zz) - prod3(t2, xz, zx)
+                      - prod3(t3, xx, ez) + prod3(t3, xz, ex);
+    const double nw = prod3(-t1, ex, zy) + prod3(t1, ey, zx) + prod3(t2, xx, zy) - prod3(t2, xy, zx)
+                      - prod3(t3, xx, ey) + prod3(t3, xy, ex);
+    gv[0] = -nu / du;
+    gv[1] = -nv / du;
+    gv[2] = -nw / dw;
+}
+
+template <int DIM>
+__device__ __forceinline__ void bc_body(const Grid &G, const Phys &P, const Fields &F, const double *const *in,
+                                        const StateBufs &B, int f, long long idx, bool setup)
 {
     const int a = f / 2, side = f % 2;
     const int tb = a == 0 ? 1 : 0, tc = a == 2 ? 1 : 2;   // tangential axes (tc = 2 is flat in 2D)
-    const long long nc = DIM == 3 ? G.n[tc] : 1, R = (long long)G.n[tb] * nc;
+    const bool full = bc_full_face(G.bc[f]);
+    const int t0 = full ? 0 : G.g;                        // first tangential index
+    const long long nc = DIM == 3 ? (full ? G.N[tc] : G.n[tc]) : 1;
+    const long long R = (long long)(full ? G.N[tb] : G.n[tb]) * nc;
     const int l = (int)(idx / R);
     const long long r = idx - (long long)l * R;
     int v[3];
-    v[tb] = G.g + (int)(r / nc);
-    v[tc] = DIM == 3 ? G.g + (int)(r % nc) : 0;
+    v[tb] = t0 + (int)(r / nc);
+    v[tc] = DIM == 3 ? t0 + (int)(r % nc) : 0;
     v[a] = side ? G.g + G.n[a] + l : G.g - 1 - l;
     const long long o = v[0] * G.st[0] + v[1] * G.st[1] + v[2];
     v[a] = side ? G.g + G.n[a] - 1 - l : G.g + l;
     const long long s = v[0] * G.st[0] + v[1] * G.st[1] + v[2];
 
     const int type = G.bc[f];
-    const double rho = in[0][s], u = in[1][s], vv = in[2][s], w = in[3][s], e = in[4][s];
+    double rho = in[0][s], e = in[4][s];
+    const double u = in[1][s], vv = in[2][s], w = in[3][s];
     double gv[3];
+    // p, T, c, mu of the ghost point: the interior point's unless the rule sets them
+    double gp = F.p[s], gT = F.T[s], gc = F.c[s], gmu = F.mu[s];
     if (type == SHOCK_BC_WALL_VISCOUS || type == SHOCK_BC_WALL_ISOTHERMAL) {
         gv[0] = -u; gv[1] = -vv; gv[2] = -w;
+        if (type == SHOCK_BC_WALL_ISOTHERMAL) gT = P.t_wall;
     } else if (type == SHOCK_BC_FARFIELD) {
         gv[0] = u; gv[1] = vv; gv[2] = w;
-    } else {
-        // slip wall: contravariant velocities of the interior point (as
-        // CalcValues forms them, src/Functions.c:2406-2440; theta3 stays zero
-        // in 2D) with the face-normal one negated, turned back into u, v, w
-        // with the ghost point's metric by Cramer's rule, every product and
-        // sum rounded in the order src/BC.c:2697-2699 evaluates them
+    } else if (type == SHOCK_BC_WALL_INVISCID || type == SHOCK_BC_OUTFLOW_SUBSONIC) {
+        // slip wall: the interior point's contravariant velocities with the
+        // face-normal one negated; subsonic outflow: as they are
+        // (src/BC.c:2553-2558), with p = p_outflow; both turned back into
+        // u, v, w with the ghost point's metric
         double th[3] = {0.0, 0.0, 0.0};
-        if (!setup)
-            for (int q = 0; q < DIM; q++) {
-                double t = __dadd_rn(__dmul_rn(u, F.m[3 * q][s]), __dmul_rn(vv, F.m[3 * q + 1][s]));
-                th[q] = DIM == 3 ? __dadd_rn(t, __dmul_rn(w, F.m[3 * q + 2][s])) : t;
-            }
-        th[a] = -th[a];
-        const double xx = F.m[0][o], xy = F.m[1][o], xz = F.m[2][o];
-        const double ex = F.m[3][o], ey = F.m[4][o], ez = F.m[5][o];
-        const double zx = F.m[6][o], zy = F.m[7][o], zz = F.m[8][o];
-        const double t1 = th[0], t2 = th[1], t3 = th[2];
-        const double du = prod3(-xx, ey, zz) + prod3(xx, ez, zy) + prod3(xy, ex, zz) - prod3(xy, ez, zx)
-                          - prod3(xz, ex, zy) + prod3(xz, ey, zx);
-        const double dw = prod3(xx, ey, zz) - prod3(xx, ez, zy) - prod3(xy, ex, zz) + prod3(xy, ez, zx)
-                          + prod3(xz, ex, zy) - prod3(xz, ey, zx);
-        const double nu = prod3(t1, ey, zz) - prod3(t1, ez, zy) - prod3(t2, xy, zz) + prod3(t2, xz, zy)
-                          + prod3(t3, xy, ez) - prod3(t3, xz, ey);
-        const double nv = prod3(-t1, ex, zz) + prod3(t1, ez, zx) + prod3(t2, xx, zz) - prod3(t2, xz, zx)
-                          - prod3(t3, xx, ez) + prod3(t3, xz, ex);
-        const double nw = prod3(-t1, ex, zy) + prod3(t1, ey, zx) + prod3(t2, xx, zy) - prod3(t2, xy, zx)
-                          - prod3(t3, xx, ey) + prod3(t3, xy, ex);
-        gv[0] = -nu / du;
-        gv[1] = -nv / du;
-        gv[2] = -nw / dw;
+        if (!setup) bc_theta<DIM>(F, s, u, vv, w, th);
+        if (type == SHOCK_BC_WALL_INVISCID) th[a] = -th[a];
+        else gp = P.p_out;
+        bc_cramer(F, o, th, gv);
+    } else {
+        // inflow (src/BC.c:2457-2542): the inflow state, e and c from it
+        gv[0] = P.u_in[0]; gv[1] = P.u_in[1]; gv[2] = P.u_in[2];
+        rho = P.rho_in;
+        gp = P.p_in;
+        const double q2 = __dadd_rn(__dadd_rn(__dmul_rn(gv[0], gv[0]), __dmul_rn(gv[1], gv[1])), __dmul_rn(gv[2], gv[2]));
+        e = __dadd_rn(__dmul_rn(0.5, q2), __dmul_rn(__ddiv_rn(__ddiv_rn(gp, rho), P.gamma - 1.0), P.ups));
+        gc = sqrt(__ddiv_rn(__dmul_rn(__dmul_rn(P.ups, P.gamma), gp), rho));
+        if (type == SHOCK_BC_INFLOW_SUPERSONIC) {
+            // T and Sutherland's mu of the inflow state (src/BC.c:2538-2541)
+            const double pr = P.p_in / P.rho_in;
+            gT = pr;
+            gmu = (1.0 + P.suth) * (pr * sqrt(pr)) / (pr + P.suth);
+        }
     }
 #pragma unroll
     for (int k = 0; k < 3; k++) {
@@ -306,10 +351,10 @@ __device__ __forceinline__ void bc_body(const Grid &G, const Fields &F, const do
         B.U[k][4][o] = e;
     }
     if (!setup) {
-        F.p[o] = F.p[s];
-        F.T[o] = type == SHOCK_BC_WALL_ISOTHERMAL ? t_wall : F.T[s];
-        F.c[o] = F.c[s];
-        F.mu[o] = F.mu[s];
+        F.p[o] = gp;
+        F.T[o] = gT;
+        F.c[o] = gc;
+        F.mu[o] = gmu;
     }
 }
 

@@ -156,31 +156,47 @@ void launch_ghosts(const Grid &G, double *const U[5], cudaStream_t s)
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(256) k_bc(Grid G, Fields F, StageIn in, StateBufs B, bool setup, double t_wall)
+__global__ void __launch_bounds__(256) k_bc(Grid G, Phys P, Fields F, StageIn in, StateBufs B, bool setup, int f0)
 {
-    const int f = blockIdx.y;
+    const int f = f0 + blockIdx.y;
     if (G.bc[f] == SHOCK_BC_AUTO) return;
     const long long n = bc_face_points(G, f);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        bc_body<DIM>(G, F, in.U, B, f, i, setup, t_wall);
+        bc_body<DIM>(G, P, F, in.U, B, f, i, setup);
 }
 
-void launch_bc(const Grid &G, const Phys &P, const double *const U[5], double *const bufs[3][5], const Fields &F,
-               bool setup, cudaStream_t s)
+int launch_bc(const Grid &G, const Phys &P, const double *const U[5], double *const bufs[3][5], const Fields &F,
+              bool setup, cudaStream_t s)
 {
     long long most = 0;
     for (int f = 0; f < 2 * G.dim; f++)
         if (G.bc[f] != SHOCK_BC_AUTO && bc_face_points(G, f) > most) most = bc_face_points(G, f);
-    if (!most) return;
+    if (!most) return 0;
     StageIn in;
     StateBufs B;
     for (int q = 0; q < 5; q++) {
         in.U[q] = U[q];
         for (int k = 0; k < 3; k++) B.U[k][q] = bufs[k][q];
     }
-    const dim3 grid(blocks_for(most, 256), 2 * G.dim);
-    if (G.dim == 3) k_bc<3><<<grid, 256, 0, s>>>(G, F, in, B, setup, P.t_wall);
-    else k_bc<2><<<grid, 256, 0, s>>>(G, F, in, B, setup, P.t_wall);
+    bool full = false;
+    for (int f = 0; f < 2 * G.dim; f++) full |= bc_full_face(G.bc[f]);
+    if (!full) {   // wall / farfield faces share no ghost point: one launch
+        const dim3 grid(blocks_for(most, 256), 2 * G.dim);
+        if (G.dim == 3) k_bc<3><<<grid, 256, 0, s>>>(G, P, F, in, B, setup, 0);
+        else k_bc<2><<<grid, 256, 0, s>>>(G, P, F, in, B, setup, 0);
+        return 1;
+    }
+    // inflow / outflow faces overlap at edges and read ghosts an earlier face
+    // wrote: one launch per face, in SHOCK's order
+    int n = 0;
+    for (int f = 0; f < 2 * G.dim; f++) {
+        if (G.bc[f] == SHOCK_BC_AUTO) continue;
+        const dim3 grid(blocks_for(bc_face_points(G, f), 256), 1);
+        if (G.dim == 3) k_bc<3><<<grid, 256, 0, s>>>(G, P, F, in, B, setup, f);
+        else k_bc<2><<<grid, 256, 0, s>>>(G, P, F, in, B, setup, f);
+        n++;
+    }
+    return n;
 }
 
 void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s)

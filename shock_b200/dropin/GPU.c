@@ -20,9 +20,12 @@
  *     AddManufacturedSolutionSource as the source.
  *   - "BCWallViscous", "BCWallInviscid", "BCFarfield" and
  *     "BCWallViscousIsothermal" faces as the SHOCK_BC_* types, with
- *     [BoundaryConditions] T_wall.
- * Faces of any other kind (moving walls, inflow, outflow) are rejected by
- * the library with SHOCK_EINVAL.
+ *     [BoundaryConditions] T_wall; inflow faces with the
+ *     Inflow-Normal-Subsonic or -Supersonic option and outflow faces with
+ *     Outflow-Normal-Subsonic, with rho_inflow, p_inflow, p_outflow and the
+ *     inflow velocity.
+ * Faces of any other kind (moving walls, Riemann / isentropic inflow,
+ * Riemann / Rudy outflow) are rejected by the library with SHOCK_EINVAL.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -106,8 +109,19 @@ int GPU_Create(struct strct_configuration *c, struct strct_mesh *m, struct strct
         else if (strcmp(face[f], c->BCWallInviscid) == 0) sp.bc[f] = SHOCK_BC_WALL_INVISCID;
         else if (strcmp(face[f], c->BCFarfield) == 0) sp.bc[f] = SHOCK_BC_FARFIELD;
         else if (strcmp(face[f], c->BCWallViscousIsothermal) == 0) sp.bc[f] = SHOCK_BC_WALL_ISOTHERMAL;
+        else if (strncmp(face[f], c->BCInflow, strlen(c->BCInflow)) == 0)   /* BCInflow, -Subsonic, -Supersonic */
+            sp.bc[f] = c->flag_BC_option_inflow_normal_super == 1 ? SHOCK_BC_INFLOW_SUPERSONIC
+                     : c->flag_BC_option_inflow_normal_sub == 1 ? SHOCK_BC_INFLOW_SUBSONIC : -1;
+        else if (strncmp(face[f], c->BCOutflow, strlen(c->BCOutflow)) == 0)   /* BCOutflow, -Subsonic */
+            sp.bc[f] = c->flag_BC_option_outflow_normal_sub == 1 ? SHOCK_BC_OUTFLOW_SUBSONIC : -1;
     }
     sp.t_wall = c->T_wall;
+    sp.rho_inflow = c->rho_inflow;
+    sp.p_inflow = c->p_inflow;
+    sp.p_outflow = c->p_out;
+    sp.u_inflow[0] = c->u_inflow;
+    sp.u_inflow[1] = c->v_inflow;
+    sp.u_inflow[2] = c->w_inflow;
     const char *prec = getenv("SHOCK_B200_PRECISION");
     sp.precision = (prec && strcmp(prec, "mixed") == 0) ? SHOCK_MIXED : SHOCK_FP64;
     sp.zeta_fix = 0;

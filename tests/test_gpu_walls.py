@@ -2,10 +2,11 @@
 
 The reference is SHOCK's CPU build with the face BC names set as its
 loader sets them (BCWallViscous, BCWallInviscid, BCFarfield,
-BCWallViscousIsothermal; src/BC.c).
+BCWallViscousIsothermal, BCInflow, BCOutflow; src/BC.c) and the inflow /
+outflow options of its config.ini.
 Tolerances as in test_gpu_parity.py: one right-hand side within
 max(1e-12, 2 * SHOCK's own FP64-vs-80-bit distance) per variable, and the
-state after 20 RK steps within 1e-10 relative L2.
+state after 20 RK steps within max(1e-10, 2 * that distance) relative L2.
 """
 import numpy as np
 import pytest
@@ -31,6 +32,12 @@ CASES = {
     "isothermal_3d_w5": lambda: cases.channel(3, 5, (16, 12, 14), bc="wall_isothermal", stretch=1.2,
                                               prandtl=0.7, t_wall=1.05),
     "isothermal_2d_w9": lambda: cases.channel(2, 9, (24, 20, 1), bc="wall_isothermal", prandtl=0.7, t_wall=0.95),
+    # through-flow: inflow on the x-lower face, subsonic outflow on the x-upper face
+    "duct_sub_3d_w5": lambda: cases.duct(3, 5, (20, 12, 14)),
+    "duct_super_3d_w9_euler": lambda: cases.duct(3, 9, (20, 12, 14), inflow="inflow_supersonic", mach=2.0,
+                                                 inviscid=True),
+    "duct_sub_walls_2d_w5": lambda: cases.duct(2, 5, (28, 18, 1), walls="wall_viscous"),
+    "duct_super_2d_w9": lambda: cases.duct(2, 9, (28, 20, 1), inflow="inflow_supersonic", mach=2.0),
 }
 
 
@@ -51,14 +58,20 @@ def test_wall_rhs_matches_reference(name):
 
 @pytest.mark.parametrize("name", sorted(CASES))
 def test_wall_steps_match_reference(name):
+    """20 steps within max(1e-10, 2 * SHOCK's own FP64-vs-80-bit distance)
+    relative L2: the supersonic WENO9 ducts amplify rounding, SHOCK's two
+    builds there drift apart by up to 3e-8."""
     c = CASES[name]()
     _need(c)
     s = shock_b200.Solver(c)
-    r = RefSolver(c)
+    r, r80 = RefSolver(c), RefSolver(c, extended=True)
     s.steps(20)
     r.steps(20)
-    err = l2_rel(real(c, s.state()), real(c, r.state()[:5]))
-    assert (err <= L2_TOL).all(), err
+    r80.steps(20)
+    ref = real(c, r.state()[:5])
+    tol = np.maximum(L2_TOL, 2.0 * l2_rel(ref, real(c, r80.state()[:5])))
+    err = l2_rel(real(c, s.state()), ref)
+    assert (err <= tol).all(), (err, tol)
 
 
 def test_wall_mixed_precision_l2():

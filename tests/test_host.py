@@ -1,5 +1,7 @@
 """Host-side pieces that need no GPU: config.ini reading, batch member sizes,
 the seeded serving stream and the tuning table keys."""
+import math
+
 import numpy as np
 
 import shock_b200
@@ -28,6 +30,13 @@ ManufacturedSolution\t\t=no
 
 [BoundaryConditions]
 T_wall\t\t\t\t=1.25
+rho_inflow\t\t\t=1.1
+p_inflow\t\t\t=0.9
+p_outflow\t\t\t=0.8
+AoA\t\t\t\t=30
+
+[InitializeValues]
+u0\t\t\t\t=2.0
 """
 
 
@@ -40,6 +49,8 @@ def test_params_from_ini(tmp_path):
     assert (p.time_order, p.tau, p.mach, p.reynolds) == (3, 0.00025, 0.1, 1600.0)
     assert (p.prandtl, p.gamma, p.gas_r, p.t0, p.l0) == (0.72, 1.4, 287.0, 300.0, 1.0)
     assert p.inviscid == 1 and p.mms == 0 and p.t_wall == 1.25
+    assert (p.rho_inflow, p.p_inflow, p.p_outflow) == (1.1, 0.9, 0.8)
+    assert abs(p.u_inflow[0] - 2.0 * math.cos(math.pi / 6)) < 1e-15 and abs(p.u_inflow[1] - 1.0) < 1e-15
     assert (p.dim, p.order, p.ni) == (3, 9, 64)      # not config.ini keys: untouched
 
 

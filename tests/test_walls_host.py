@@ -20,6 +20,26 @@ CASES = [
 ]
 
 
+@pytest.mark.parametrize("inflow,walls", [("inflow_subsonic", ""), ("inflow_supersonic", "wall_viscous")])
+def test_duct_geometry_matches_reference(inflow, walls):
+    if not ref_available(5, 2):
+        pytest.skip("reference build not present")
+    c = cases.duct(2, 5, (28, 18, 1), inflow=inflow, walls=walls)
+    assert np.array_equal(shock_b200.host_geometry(c), RefSolver(c).geometry())
+
+
+def test_mixed_inflow_options_rejected():
+    c = cases.duct(2, 5, (28, 18, 1))
+    p = shock_b200.params_from_case(c)
+    p.bc[1] = shock_b200.SHOCK_BC_INFLOW_SUPERSONIC   # subsonic and supersonic inflow in one block
+    x, y, z = (np.ascontiguousarray(a.transpose(2, 1, 0)).ravel() for a in (c.x, c.y, c.z))
+    out = np.zeros((13,) + (c.ni + 6, c.nj + 6, 1))
+    dp = C.POINTER(C.c_double)
+    rc = shock_b200.lib().shock_host_geometry(C.byref(p), x.ctypes.data_as(dp), y.ctypes.data_as(dp),
+                                              z.ctypes.data_as(dp), out.ctypes.data_as(dp))
+    assert rc == shock_b200.SHOCK_EINVAL
+
+
 @pytest.mark.parametrize("dim,order,n,bc,stretch,walls_i", CASES)
 def test_wall_geometry_matches_reference(dim, order, n, bc, stretch, walls_i):
     if not ref_available(order, dim):
