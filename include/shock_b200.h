@@ -47,6 +47,9 @@ extern "C" {
 #define SHOCK_BC_INFLOW_SUBSONIC 5   /* "BCInflow*" with Inflow-Normal-Subsonic (src/BC.c:2457-2503) */
 #define SHOCK_BC_INFLOW_SUPERSONIC 6 /* "BCInflow*" with Inflow-Normal-Supersonic (src/BC.c:2505-2542) */
 #define SHOCK_BC_OUTFLOW_SUBSONIC 7  /* "BCOutflow*" with Outflow-Normal-Subsonic (src/BC.c:2544-2570) */
+#define SHOCK_BC_INFLOW_RIEMANN 8    /* "BCInflow*" with Inflow-Riemann-Subsonic (src/BC.c:2404-2455) */
+#define SHOCK_BC_INFLOW_ISENTROPIC 9 /* "BCInflow*" with Inflow-Isentrop-Subsonic (src/BC.c:2363-2402) */
+#define SHOCK_BC_OUTFLOW_RIEMANN 10  /* "BCOutflow*" with Outflow-Riemann-Subsonic (src/BC.c:2572-2622) */
 
 #define SHOCK_FP64 0        /* everything in FP64 (reference precision) */
 #define SHOCK_MIXED 1       /* FP32 WENO/viscous stencils, FP64 state/RK/metric/p-T recovery */

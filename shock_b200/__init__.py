@@ -38,6 +38,9 @@ SHOCK_BC_WALL_ISOTHERMAL = 4
 SHOCK_BC_INFLOW_SUBSONIC = 5
 SHOCK_BC_INFLOW_SUPERSONIC = 6
 SHOCK_BC_OUTFLOW_SUBSONIC = 7
+SHOCK_BC_INFLOW_RIEMANN = 8
+SHOCK_BC_INFLOW_ISENTROPIC = 9
+SHOCK_BC_OUTFLOW_RIEMANN = 10
 
 _lib = None
 _lock = threading.Lock()

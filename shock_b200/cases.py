@@ -160,7 +160,8 @@ def smooth_random(dim: int, order: int, n: Tuple[int, int, int], seed: int = 0,
 
 
 BC_NAMES = {"wall_viscous": 1, "wall_inviscid": 2, "farfield": 3, "wall_isothermal": 4,
-            "inflow_subsonic": 5, "inflow_supersonic": 6, "outflow_subsonic": 7}
+            "inflow_subsonic": 5, "inflow_supersonic": 6, "outflow_subsonic": 7,
+            "inflow_riemann": 8, "inflow_isentropic": 9, "outflow_riemann": 10}
 
 
 def channel(dim: int, order: int, n: Tuple[int, int, int], bc: str = "wall_viscous", seed: int = 0,
@@ -210,10 +211,10 @@ def channel(dim: int, order: int, n: Tuple[int, int, int], bc: str = "wall_visco
 
 def duct(dim: int, order: int, n: Tuple[int, int, int], inflow: str = "inflow_subsonic", seed: int = 0,
          mach: float = 0.5, reynolds: float = 500.0, inviscid: bool = False, time_order: int = 4,
-         walls: str = "") -> Case:
-    """Through-flow block: inflow on the x-lower face, subsonic outflow on the
-    x-upper face, periodic in y (and z), or ``walls`` ("wall_viscous", ...)
-    on the y faces.  The inflow state is rho_inflow = p_inflow = 1 moving at
+         walls: str = "", outflow: str = "outflow_subsonic") -> Case:
+    """Through-flow block: inflow of kind ``inflow`` on the x-lower face,
+    outflow of kind ``outflow`` on the x-upper face, periodic in y (and z),
+    or ``walls`` ("wall_viscous", ...) on the y faces.  The inflow state is rho_inflow = p_inflow = 1 moving at
     u_inflow = (1, 0, 0) (in SHOCK's velocity units, Ma = mach); the initial
     field is that state with smooth seeded perturbations; p_outflow is 0.98
     of the inflow pressure."""
@@ -239,14 +240,14 @@ def duct(dim: int, order: int, n: Tuple[int, int, int], inflow: str = "inflow_su
     w = amp * pert() if dim == 3 else np.zeros_like(x)
     rho = 1.0 + amp * pert()
     p = 1.0 + amp * pert()
-    faces = [BC_NAMES[inflow], BC_NAMES["outflow_subsonic"], 0, 0, 0, 0]
+    faces = [BC_NAMES[inflow], BC_NAMES[outflow], 0, 0, 0, 0]
     if walls:
         faces[2] = faces[3] = BC_NAMES[walls]
     c = Case(dim=dim, order=order, ni=ni, nj=nj, nk=nk, x=x, y=y, z=z, rho=rho, u=u, v=v, w=w, p=p,
              time_order=time_order, mach=mach, reynolds=reynolds, inviscid=inviscid,
              periodic=(False, not walls, dim == 3), period=(Lx, Ly, Lz), bc=tuple(faces),
              rho_inflow=1.0, p_inflow=1.0, p_outflow=0.98, u_inflow=(1.0, 0.0, 0.0),
-             name=f"duct{dim}d_w{order}_{inflow}")
+             name=f"duct{dim}d_w{order}_{inflow}_{outflow}")
     c.tau = cfl_tau(c)
     return c
 

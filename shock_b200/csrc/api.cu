@@ -126,6 +126,7 @@ Phys make_phys(const shock_params &p)
     P.rho_in = p.rho_inflow;
     P.p_in = p.p_inflow;
     P.p_out = p.p_outflow;
+    P.mach = p.mach;
     for (int a = 0; a < 3; a++) P.u_in[a] = p.u_inflow[a];
     P.gam_w = 1.0 / ((p.gamma - 1.0) * (p.mach * p.mach) * p.reynolds * 0.72);
     for (int a = 0; a < 3; a++) P.iso_hi[a] = a < p.dim && p.bc[2 * a + 1] == SHOCK_BC_WALL_ISOTHERMAL;
@@ -215,18 +216,24 @@ int shock_device_count(int *n)
 // the wall / farfield types.
 static int check_faces(const shock_params *p)
 {
-    bool sub = false, super = false;
+    // SHOCK takes one inflow and one outflow option per run (src/Import.c:62-87)
+    int inflow = 0, outflow = 0;
     for (int f = 0; f < 2 * p->dim; f++) {
-        sub |= p->bc[f] == SHOCK_BC_INFLOW_SUBSONIC;
-        super |= p->bc[f] == SHOCK_BC_INFLOW_SUPERSONIC;
+        const int b = p->bc[f];
+        const bool in = b == SHOCK_BC_INFLOW_SUBSONIC || b == SHOCK_BC_INFLOW_SUPERSONIC || b == SHOCK_BC_INFLOW_RIEMANN
+                        || b == SHOCK_BC_INFLOW_ISENTROPIC;
+        const bool out = b == SHOCK_BC_OUTFLOW_SUBSONIC || b == SHOCK_BC_OUTFLOW_RIEMANN;
+        if (in && inflow && inflow != b) return fail(SHOCK_EINVAL, "two inflow options in one block");
+        if (out && outflow && outflow != b) return fail(SHOCK_EINVAL, "two outflow options in one block");
+        if (in) inflow = b;
+        if (out) outflow = b;
     }
-    if (sub && super)   // SHOCK takes one inflow option per run (src/Import.c:62-75)
-        return fail(SHOCK_EINVAL, "subsonic and supersonic inflow faces in one block");
     for (int a = 0; a < p->dim; a++)
         for (int side = 0; side < 2; side++) {
             const int f = 2 * a + side, b = p->bc[f];
-            if (b < SHOCK_BC_AUTO || b > SHOCK_BC_OUTFLOW_SUBSONIC) return fail(SHOCK_EINVAL, "face %d: unknown bc %d", f, b);
-            if ((b == SHOCK_BC_INFLOW_SUBSONIC || b == SHOCK_BC_INFLOW_SUPERSONIC) && (p->rho_inflow <= 0 || p->p_inflow <= 0))
+            if (b < SHOCK_BC_AUTO || b > SHOCK_BC_OUTFLOW_RIEMANN) return fail(SHOCK_EINVAL, "face %d: unknown bc %d", f, b);
+            if ((b == SHOCK_BC_INFLOW_SUBSONIC || b == SHOCK_BC_INFLOW_SUPERSONIC || b == SHOCK_BC_INFLOW_RIEMANN
+                 || b == SHOCK_BC_INFLOW_ISENTROPIC) && (p->rho_inflow <= 0 || p->p_inflow <= 0))
                 return fail(SHOCK_EINVAL, "face %d: inflow needs rho_inflow > 0 and p_inflow > 0", f);
             if (p->periodic[a] && b != SHOCK_BC_AUTO)
                 return fail(SHOCK_EINVAL, "face %d: a periodic axis takes SHOCK_BC_AUTO", f);

@@ -58,6 +58,7 @@ struct Phys {
                          // points (SHOCK's BC_Corrector_*Momentum, src/WENO.c:265-277)
     double t_wall;       // ghost temperature of isothermal walls
     double rho_in, p_in, u_in[3], p_out;   // inflow / outflow values
+    double mach;         // free-stream Mach number (Riemann inflow / outflow: c_inf = 1/Ma)
     double gam_w;        // Gamma of isothermal-wall ghost points (Prandtl 0.72, src/BC.c:2975-2976)
     int iso_hi[3];       // the upper face of the axis is an isothermal wall
 };

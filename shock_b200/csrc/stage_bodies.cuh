@@ -328,12 +328,47 @@ __device__ __forceinline__ void bc_body(const Grid &G, const Phys &P, const Fiel
         else gp = P.p_out;
         bc_cramer(F, o, th, gv);
     } else {
-        // inflow (src/BC.c:2457-2542): the inflow state, e and c from it
-        gv[0] = P.u_in[0]; gv[1] = P.u_in[1]; gv[2] = P.u_in[2];
-        rho = P.rho_in;
-        gp = P.p_in;
+        // inflow and Riemann outflow (src/BC.c:2363-2542, :2572-2622): a
+        // ghost state (rho, u, v, w, p), then e and c from it.  In set-up
+        // mode the interior c and theta are zero, as in SHOCK's set-up fill,
+        // which runs before the first CalcValues.
+        const double g1 = P.gamma - 1.0;
+        if (type == SHOCK_BC_INFLOW_SUBSONIC || type == SHOCK_BC_INFLOW_SUPERSONIC) {
+            gv[0] = P.u_in[0]; gv[1] = P.u_in[1]; gv[2] = P.u_in[2];
+            rho = P.rho_in;
+            gp = P.p_in;
+        } else if (type == SHOCK_BC_INFLOW_ISENTROPIC) {
+            // the interior point's contravariant velocities, the density of
+            // the isentrope through the inflow state at that speed
+            // (src/BC.c:2363-2402), each operation rounded in SHOCK's order
+            double th[3] = {0.0, 0.0, 0.0};
+            if (!setup) bc_theta<DIM>(F, s, u, vv, w, th);
+            bc_cramer(F, o, th, gv);
+            double k = __ddiv_rn(pow(P.rho_in, P.gamma), P.p_in);
+            k = __dmul_rn(__dmul_rn(__dmul_rn(__ddiv_rn(__dmul_rn(k, g1), P.gamma), P.gamma), P.mach), P.mach);
+            k = __dmul_rn(k, __ddiv_rn(__dmul_rn(gv[0], gv[0]), 2.0));
+            rho = pow(__dsub_rn(pow(P.rho_in, g1), k), __ddiv_rn(1.0, g1));
+            gp = __dmul_rn(P.p_in, pow(__ddiv_rn(rho, P.rho_in), P.gamma));
+        } else {
+            // Riemann invariants between the interior point and the free
+            // stream, c_inf = 1/Ma (src/BC.c:2404-2455 inflow: v, w and the
+            // reference density and pressure of the inflow; :2572-2622
+            // outflow: those of the interior point)
+            const bool in_r = type == SHOCK_BC_INFLOW_RIEMANN;
+            const double cinf = __ddiv_rn(1.0, P.mach), cii = setup ? 0.0 : gc;
+            const double half = __dmul_rn(0.5, __dadd_rn(u, P.u_in[0]));
+            const double jump = __ddiv_rn(__dsub_rn(cinf, cii), g1);
+            gv[0] = in_r ? __dadd_rn(half, jump) : __dsub_rn(half, jump);
+            gv[1] = in_r ? P.u_in[1] : vv;
+            gv[2] = in_r ? P.u_in[2] : w;
+            const double cm = __dmul_rn(0.5, __dadd_rn(cii, cinf));
+            const double du = __dmul_rn(__dmul_rn(0.25, g1), __dsub_rn(P.u_in[0], u));
+            const double d1 = in_r ? __ddiv_rn(__dadd_rn(cm, du), cinf) : __ddiv_rn(__dsub_rn(cm, du), cii);
+            rho = __dmul_rn(in_r ? P.rho_in : rho, pow(d1, __ddiv_rn(2., g1)));
+            gp = __dmul_rn(in_r ? P.p_in : gp, pow(d1, __ddiv_rn(__dmul_rn(2., P.gamma), g1)));
+        }
         const double q2 = __dadd_rn(__dadd_rn(__dmul_rn(gv[0], gv[0]), __dmul_rn(gv[1], gv[1])), __dmul_rn(gv[2], gv[2]));
-        e = __dadd_rn(__dmul_rn(0.5, q2), __dmul_rn(__ddiv_rn(__ddiv_rn(gp, rho), P.gamma - 1.0), P.ups));
+        e = __dadd_rn(__dmul_rn(0.5, q2), __dmul_rn(__ddiv_rn(__ddiv_rn(gp, rho), g1), P.ups));
         gc = sqrt(__ddiv_rn(__dmul_rn(__dmul_rn(P.ups, P.gamma), gp), rho));
         if (type == SHOCK_BC_INFLOW_SUPERSONIC) {
             // T and Sutherland's mu of the inflow state (src/BC.c:2538-2541)

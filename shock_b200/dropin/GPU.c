@@ -21,11 +21,12 @@
  *   - "BCWallViscous", "BCWallInviscid", "BCFarfield" and
  *     "BCWallViscousIsothermal" faces as the SHOCK_BC_* types, with
  *     [BoundaryConditions] T_wall; inflow faces with the
- *     Inflow-Normal-Subsonic or -Supersonic option and outflow faces with
- *     Outflow-Normal-Subsonic, with rho_inflow, p_inflow, p_outflow and the
- *     inflow velocity.
- * Faces of any other kind (moving walls, Riemann / isentropic inflow,
- * Riemann / Rudy outflow) are rejected by the library with SHOCK_EINVAL.
+ *     Inflow-Normal-Subsonic, -Supersonic, Inflow-Riemann-Subsonic or
+ *     Inflow-Isentrop-Subsonic option and outflow faces with
+ *     Outflow-Normal-Subsonic or Outflow-Riemann-Subsonic, with rho_inflow,
+ *     p_inflow, p_outflow and the inflow velocity.
+ * Faces of any other kind (moving walls, Rudy outflow) are rejected by the
+ * library with SHOCK_EINVAL.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -111,9 +112,12 @@ int GPU_Create(struct strct_configuration *c, struct strct_mesh *m, struct strct
         else if (strcmp(face[f], c->BCWallViscousIsothermal) == 0) sp.bc[f] = SHOCK_BC_WALL_ISOTHERMAL;
         else if (strncmp(face[f], c->BCInflow, strlen(c->BCInflow)) == 0)   /* BCInflow, -Subsonic, -Supersonic */
             sp.bc[f] = c->flag_BC_option_inflow_normal_super == 1 ? SHOCK_BC_INFLOW_SUPERSONIC
-                     : c->flag_BC_option_inflow_normal_sub == 1 ? SHOCK_BC_INFLOW_SUBSONIC : -1;
+                     : c->flag_BC_option_inflow_normal_sub == 1 ? SHOCK_BC_INFLOW_SUBSONIC
+                     : c->flag_BC_option_inflow_riemann_sub == 1 ? SHOCK_BC_INFLOW_RIEMANN
+                     : c->flag_BC_option_inflow_isentrop_sub == 1 ? SHOCK_BC_INFLOW_ISENTROPIC : -1;
         else if (strncmp(face[f], c->BCOutflow, strlen(c->BCOutflow)) == 0)   /* BCOutflow, -Subsonic */
-            sp.bc[f] = c->flag_BC_option_outflow_normal_sub == 1 ? SHOCK_BC_OUTFLOW_SUBSONIC : -1;
+            sp.bc[f] = c->flag_BC_option_outflow_normal_sub == 1 ? SHOCK_BC_OUTFLOW_SUBSONIC
+                     : c->flag_BC_option_outflow_riemann_sub == 1 ? SHOCK_BC_OUTFLOW_RIEMANN : -1;
     }
     sp.t_wall = c->T_wall;
     sp.rho_inflow = c->rho_inflow;

@@ -3,7 +3,8 @@
 The reference is SHOCK's CPU build with the face BC names set as its
 loader sets them (BCWallViscous, BCWallInviscid, BCFarfield,
 BCWallViscousIsothermal, BCInflow, BCOutflow; src/BC.c) and the inflow /
-outflow options of its config.ini.
+outflow options of its config.ini (Normal-Subsonic, Normal-Supersonic,
+Riemann-Subsonic, Isentrop-Subsonic).
 Tolerances as in test_gpu_parity.py: one right-hand side within
 max(1e-12, 2 * SHOCK's own FP64-vs-80-bit distance) per variable, and the
 state after 20 RK steps within max(1e-10, 2 * that distance) relative L2.
@@ -38,6 +39,14 @@ CASES = {
                                                  inviscid=True),
     "duct_sub_walls_2d_w5": lambda: cases.duct(2, 5, (28, 18, 1), walls="wall_viscous"),
     "duct_super_2d_w9": lambda: cases.duct(2, 9, (28, 20, 1), inflow="inflow_supersonic", mach=2.0),
+    # Riemann-invariant inflow and outflow, isentropic inflow
+    "duct_riemann_3d_w5": lambda: cases.duct(3, 5, (20, 12, 14), inflow="inflow_riemann", outflow="outflow_riemann"),
+    "duct_riemann_walls_2d_w9": lambda: cases.duct(2, 9, (28, 20, 1), inflow="inflow_riemann",
+                                                   outflow="outflow_riemann", walls="wall_viscous"),
+    "duct_isentropic_3d_w9_euler": lambda: cases.duct(3, 9, (20, 12, 14), inflow="inflow_isentropic",
+                                                      inviscid=True),
+    "duct_isentropic_slip_2d_w5": lambda: cases.duct(2, 5, (28, 18, 1), inflow="inflow_isentropic",
+                                                     outflow="outflow_riemann", walls="wall_inviscid"),
 }
 
 

@@ -20,24 +20,36 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("inflow,walls", [("inflow_subsonic", ""), ("inflow_supersonic", "wall_viscous")])
-def test_duct_geometry_matches_reference(inflow, walls):
+@pytest.mark.parametrize("inflow,walls,outflow", [("inflow_subsonic", "", "outflow_subsonic"),
+                                                   ("inflow_supersonic", "wall_viscous", "outflow_subsonic"),
+                                                   ("inflow_riemann", "", "outflow_riemann"),
+                                                   ("inflow_isentropic", "wall_inviscid", "outflow_riemann")])
+def test_duct_geometry_matches_reference(inflow, walls, outflow):
     if not ref_available(5, 2):
         pytest.skip("reference build not present")
-    c = cases.duct(2, 5, (28, 18, 1), inflow=inflow, walls=walls)
+    c = cases.duct(2, 5, (28, 18, 1), inflow=inflow, walls=walls, outflow=outflow)
     assert np.array_equal(shock_b200.host_geometry(c), RefSolver(c).geometry())
 
 
-def test_mixed_inflow_options_rejected():
-    c = cases.duct(2, 5, (28, 18, 1))
+@pytest.mark.parametrize("face,bc", [(1, shock_b200.SHOCK_BC_INFLOW_SUPERSONIC),
+                                     (1, shock_b200.SHOCK_BC_INFLOW_RIEMANN),
+                                     (0, shock_b200.SHOCK_BC_OUTFLOW_RIEMANN)])
+def test_mixed_inflow_outflow_options_rejected(face, bc):
+    """SHOCK takes one inflow and one outflow option per run: a block with
+    subsonic inflow on the x-lower face and subsonic outflow on the x-upper
+    face cannot also carry another inflow or outflow kind."""
+    c = cases.duct(2, 5, (28, 18, 1), walls="wall_viscous")
     p = shock_b200.params_from_case(c)
-    p.bc[1] = shock_b200.SHOCK_BC_INFLOW_SUPERSONIC   # subsonic and supersonic inflow in one block
+    p.bc[2 + face] = bc
     x, y, z = (np.ascontiguousarray(a.transpose(2, 1, 0)).ravel() for a in (c.x, c.y, c.z))
     out = np.zeros((13,) + (c.ni + 6, c.nj + 6, 1))
     dp = C.POINTER(C.c_double)
     rc = shock_b200.lib().shock_host_geometry(C.byref(p), x.ctypes.data_as(dp), y.ctypes.data_as(dp),
                                               z.ctypes.data_as(dp), out.ctypes.data_as(dp))
     assert rc == shock_b200.SHOCK_EINVAL
+    p.bc[2 + face] = shock_b200.SHOCK_BC_WALL_VISCOUS
+    assert shock_b200.lib().shock_host_geometry(C.byref(p), x.ctypes.data_as(dp), y.ctypes.data_as(dp),
+                                                z.ctypes.data_as(dp), out.ctypes.data_as(dp)) == 0
 
 
 @pytest.mark.parametrize("dim,order,n,bc,stretch,walls_i", CASES)
@@ -65,7 +77,7 @@ def test_bc_argument_checks():
     bad.bc[0] = 1                      # a wall on a periodic axis
     assert geom(bad) == shock_b200.SHOCK_EINVAL
     bad = shock_b200.params_from_case(c)
-    bad.bc[2] = 9                      # unknown type
+    bad.bc[2] = 11                     # unknown type
     assert geom(bad) == shock_b200.SHOCK_EINVAL
     bad = shock_b200.params_from_case(c)
     bad.bc[2] = 0                      # a non-periodic face with nothing to fill it
