@@ -50,6 +50,7 @@ extern "C" {
 #define SHOCK_BC_INFLOW_RIEMANN 8    /* "BCInflow*" with Inflow-Riemann-Subsonic (src/BC.c:2404-2455) */
 #define SHOCK_BC_INFLOW_ISENTROPIC 9 /* "BCInflow*" with Inflow-Isentrop-Subsonic (src/BC.c:2363-2402) */
 #define SHOCK_BC_OUTFLOW_RIEMANN 10  /* "BCOutflow*" with Outflow-Riemann-Subsonic (src/BC.c:2572-2622) */
+#define SHOCK_BC_OUTFLOW_RUDY 11     /* "BCOutflow*" with Outflow-Rudy-Subsonic (src/BC.c:2624-2655) */
 
 #define SHOCK_FP64 0        /* everything in FP64 (reference precision) */
 #define SHOCK_MIXED 1       /* FP32 WENO/viscous stencils, FP64 state/RK/metric/p-T recovery */

@@ -183,10 +183,11 @@ int ref_init(const ref_params *p, const double *x, const double *y, const double
     {
         /* face BC names as src/Load.c:46-97 assigns them from the CGNS BC types */
         char *side[6] = {cfg.BC_Left, cfg.BC_Right, cfg.BC_Bottom, cfg.BC_Top, cfg.BC_Behind, cfg.BC_InFront};
-        const char *name[11] = {NULL, cfg.BCWallViscous, cfg.BCWallInviscid, cfg.BCFarfield, cfg.BCWallViscousIsothermal,
-                                cfg.BCInflow, cfg.BCInflow, cfg.BCOutflow, cfg.BCInflow, cfg.BCInflow, cfg.BCOutflow};
+        const char *name[12] = {NULL, cfg.BCWallViscous, cfg.BCWallInviscid, cfg.BCFarfield, cfg.BCWallViscousIsothermal,
+                                cfg.BCInflow, cfg.BCInflow, cfg.BCOutflow, cfg.BCInflow, cfg.BCInflow, cfg.BCOutflow,
+                                cfg.BCOutflow};
         for (int f = 0; f < 6; f++)
-            if (p->bc[f] >= 1 && p->bc[f] <= 10) strcpy(side[f], name[p->bc[f]]);
+            if (p->bc[f] >= 1 && p->bc[f] <= 11) strcpy(side[f], name[p->bc[f]]);
         cfg.T_wall = p->t_wall;
         /* the one inflow / outflow option of the run (src/Import.c:62-87) */
         for (int f = 0; f < 6; f++) {
@@ -196,6 +197,7 @@ int ref_init(const ref_params *p, const double *x, const double *y, const double
             if (p->bc[f] == 8) cfg.flag_BC_option_inflow_riemann_sub = 1;
             if (p->bc[f] == 9) cfg.flag_BC_option_inflow_isentrop_sub = 1;
             if (p->bc[f] == 10) cfg.flag_BC_option_outflow_riemann_sub = 1;
+            if (p->bc[f] == 11) cfg.flag_BC_option_outflow_rudy_sub = 1;
         }
     }
 

@@ -41,6 +41,7 @@ SHOCK_BC_OUTFLOW_SUBSONIC = 7
 SHOCK_BC_INFLOW_RIEMANN = 8
 SHOCK_BC_INFLOW_ISENTROPIC = 9
 SHOCK_BC_OUTFLOW_RIEMANN = 10
+SHOCK_BC_OUTFLOW_RUDY = 11
 
 _lib = None
 _lock = threading.Lock()

@@ -161,7 +161,7 @@ def smooth_random(dim: int, order: int, n: Tuple[int, int, int], seed: int = 0,
 
 BC_NAMES = {"wall_viscous": 1, "wall_inviscid": 2, "farfield": 3, "wall_isothermal": 4,
             "inflow_subsonic": 5, "inflow_supersonic": 6, "outflow_subsonic": 7,
-            "inflow_riemann": 8, "inflow_isentropic": 9, "outflow_riemann": 10}
+            "inflow_riemann": 8, "inflow_isentropic": 9, "outflow_riemann": 10, "outflow_rudy": 11}
 
 
 def channel(dim: int, order: int, n: Tuple[int, int, int], bc: str = "wall_viscous", seed: int = 0,

@@ -68,6 +68,8 @@ struct shock_ctx {
     double *pool = nullptr;
     size_t pool_bytes = 0;
     double *buf[3][5] = {};
+    double *plast[6] = {};         // Rudy outflow faces: U_lastStep's p at their ghost points
+    double *plast_pool = nullptr;
     int un = 0;          // buffer holding U_lastStep (== running state between steps)
     int last_in = 0;     // input buffer of the last stage run (its ghosts are U_lastStep's)
     bool has_source = false;
@@ -127,6 +129,10 @@ Phys make_phys(const shock_params &p)
     P.p_in = p.p_inflow;
     P.p_out = p.p_outflow;
     P.mach = p.mach;
+    // DefineParameters (src/Functions.c:1759-1763): c0 = sqrt(gamma R T0),
+    // u0 = c0 Ma, AlphaNonRef = 0.25 L0 / u0
+    P.alpha = 0.25 * p.l0 / (sqrt(p.gamma * p.gas_r * p.t0) * p.mach);
+    P.tau = p.tau;
     for (int a = 0; a < 3; a++) P.u_in[a] = p.u_inflow[a];
     P.gam_w = 1.0 / ((p.gamma - 1.0) * (p.mach * p.mach) * p.reynolds * 0.72);
     for (int a = 0; a < 3; a++) P.iso_hi[a] = a < p.dim && p.bc[2 * a + 1] == SHOCK_BC_WALL_ISOTHERMAL;
@@ -146,7 +152,7 @@ static void enqueue_rhs(shock_ctx *c, double *const in[5], int &nk)
     nk += (c->G.periodic[0] || c->G.periodic[1] || c->G.periodic[2]) ? 1 : 0;
     launch_prim(c->G, c->P, cin, c->F, s);
     nk++;
-    if (c->P.walls) nk += launch_bc(c->G, c->P, cin, c->buf, c->F, false, s);
+    if (c->P.walls) nk += launch_bc(c->G, c->P, cin, c->buf, c->F, c->plast, false, s);
     if (!c->p.inviscid) {
         launch_nodal(c->G, c->p.precision, cin, c->F, s);
         nk++;
@@ -175,6 +181,11 @@ static void enqueue_step(shock_ctx *c, int un, int &nk)
         launch_rk(c->G, c->rk[st], c->p.tau, cin, c->buf[out], F, c->has_source, c->stream);
         nk++;
         cur = out;
+    }
+    // end of the step: U_RK's p becomes U_lastStep's (src/SHOCK.c:661-664)
+    if (c->plast_pool) {
+        launch_bc_save(c->G, c->F, c->plast, c->stream);
+        nk++;
     }
 }
 
@@ -217,21 +228,29 @@ int shock_device_count(int *n)
 static int check_faces(const shock_params *p)
 {
     // SHOCK takes one inflow and one outflow option per run (src/Import.c:62-87)
-    int inflow = 0, outflow = 0;
+    int inflow = 0, outflow = 0, in_axes = 0, rudy_axes = 0;
     for (int f = 0; f < 2 * p->dim; f++) {
         const int b = p->bc[f];
         const bool in = b == SHOCK_BC_INFLOW_SUBSONIC || b == SHOCK_BC_INFLOW_SUPERSONIC || b == SHOCK_BC_INFLOW_RIEMANN
                         || b == SHOCK_BC_INFLOW_ISENTROPIC;
-        const bool out = b == SHOCK_BC_OUTFLOW_SUBSONIC || b == SHOCK_BC_OUTFLOW_RIEMANN;
+        const bool out = b == SHOCK_BC_OUTFLOW_SUBSONIC || b == SHOCK_BC_OUTFLOW_RIEMANN || b == SHOCK_BC_OUTFLOW_RUDY;
         if (in && inflow && inflow != b) return fail(SHOCK_EINVAL, "two inflow options in one block");
         if (out && outflow && outflow != b) return fail(SHOCK_EINVAL, "two outflow options in one block");
-        if (in) inflow = b;
+        if (in) inflow = b, in_axes |= 1 << (f / 2);
         if (out) outflow = b;
+        if (b == SHOCK_BC_OUTFLOW_RUDY) rudy_axes |= 1 << (f / 2);
     }
+    // Rudy's outflow reads U_lastStep's speed of sound at its interior
+    // points, which SHOCK leaves zero unless an inflow face's set-up fill
+    // wrote it there: an inflow face on another axis shares those points.
+    if (rudy_axes && (in_axes & ~rudy_axes))
+        return fail(SHOCK_EINVAL, "Rudy outflow with an inflow face on another axis");
+    if (rudy_axes && (p->l0 <= 0 || p->gas_r <= 0 || p->t0 <= 0))
+        return fail(SHOCK_EINVAL, "Rudy outflow needs l0, gas_r and t0 > 0 (AlphaNonRef)");
     for (int a = 0; a < p->dim; a++)
         for (int side = 0; side < 2; side++) {
             const int f = 2 * a + side, b = p->bc[f];
-            if (b < SHOCK_BC_AUTO || b > SHOCK_BC_OUTFLOW_RIEMANN) return fail(SHOCK_EINVAL, "face %d: unknown bc %d", f, b);
+            if (b < SHOCK_BC_AUTO || b > SHOCK_BC_OUTFLOW_RUDY) return fail(SHOCK_EINVAL, "face %d: unknown bc %d", f, b);
             if ((b == SHOCK_BC_INFLOW_SUBSONIC || b == SHOCK_BC_INFLOW_SUPERSONIC || b == SHOCK_BC_INFLOW_RIEMANN
                  || b == SHOCK_BC_INFLOW_ISENTROPIC) && (p->rho_inflow <= 0 || p->p_inflow <= 0))
                 return fail(SHOCK_EINVAL, "face %d: inflow needs rho_inflow > 0 and p_inflow > 0", f);
@@ -311,9 +330,39 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
     for (int f = 0; f < 9; f++) cudaMemcpy(c->F.m[f], hb.geo[4 + f].data(), nb, cudaMemcpyHostToDevice);
     for (int b = 0; b < 3; b++)
         for (int f = 0; f < 5; f++) cudaMemcpy(c->buf[b][f], hb.prim[f].data(), nb, cudaMemcpyHostToDevice);
+    // a Rudy face's ghost points: g layers over the ghost-inclusive face
+    auto rudy_face_points = [&](int f) {
+        long long r = G.g;
+        for (int b = 0; b < G.dim; b++)
+            if (b != f / 2) r *= G.N[b];
+        return r;
+    };
+    long long rudy_pts = 0;
+    for (int f = 0; f < 2 * p->dim; f++)
+        if (p->bc[f] == SHOCK_BC_OUTFLOW_RUDY) rudy_pts += rudy_face_points(f);
+    if (rudy_pts) {
+        // U_lastStep's p before the set-up fill: InitializeValues_p0 = 1 on
+        // every point (src/Functions.c:1327-1353), the block's pressure on the
+        // real points
+        std::vector<double> p0(G.NG, 1.0);
+        for (int k = 0; k < (p->dim == 3 ? p->nk : 1); k++)
+            for (int j = 0; j < p->nj; j++)
+                for (int i = 0; i < p->ni; i++)
+                    p0[c->L.at(i + c->L.g, j + c->L.g, p->dim == 3 ? k + c->L.g : 0)] =
+                        pr[((size_t)k * p->nj + j) * p->ni + i];
+        cudaMemcpy(c->F.p, p0.data(), nb, cudaMemcpyHostToDevice);
+        if (cudaMalloc(&c->plast_pool, sizeof(double) * rudy_pts) != cudaSuccess) {
+            shock_destroy(c);
+            return fail(SHOCK_ENOMEM, "Rudy outflow buffer");
+        }
+        double *q2 = c->plast_pool;
+        for (int f = 0; f < 2 * p->dim; f++)
+            if (p->bc[f] == SHOCK_BC_OUTFLOW_RUDY) { c->plast[f] = q2; q2 += rudy_face_points(f); }
+    }
     if (c->P.walls) {
         const double *b0[5] = {c->buf[0][0], c->buf[0][1], c->buf[0][2], c->buf[0][3], c->buf[0][4]};
-        launch_bc(G, c->P, b0, c->buf, c->F, true, c->stream);
+        launch_bc(G, c->P, b0, c->buf, c->F, c->plast, true, c->stream);
+        if (rudy_pts) launch_bc_save(G, c->F, c->plast, c->stream);
         cudaStreamSynchronize(c->stream);
     }
     c->geo_host = std::move(hb.geo);
@@ -336,6 +385,7 @@ int shock_destroy(shock_ctx *c)
     if (c->F.js[0]) cudaFree(c->F.js[0]);
     if (c->pool) cudaFree(c->pool);
     if (c->F.flag) cudaFree(c->F.flag);
+    if (c->plast_pool) cudaFree(c->plast_pool);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);

@@ -59,6 +59,7 @@ struct Phys {
     double t_wall;       // ghost temperature of isothermal walls
     double rho_in, p_in, u_in[3], p_out;   // inflow / outflow values
     double mach;         // free-stream Mach number (Riemann inflow / outflow: c_inf = 1/Ma)
+    double alpha, tau;   // Rudy outflow: AlphaNonRef = 0.25 L0/u0 (src/Functions.c:1763), the time step
     double gam_w;        // Gamma of isothermal-wall ghost points (Prandtl 0.72, src/BC.c:2975-2976)
     int iso_hi[3];       // the upper face of the axis is an isothermal wall
 };
@@ -176,8 +177,13 @@ void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const F
 // Wall, farfield, inflow and outflow ghost layers from state U into all three
 // state buffers (setup: SHOCK's set-up fill, state only); no launch without
 // such faces.
+// plast[f]: U_lastStep's pressure at the ghost points of face f, for Rudy
+// outflow faces (nullptr elsewhere).
 int launch_bc(const Grid &G, const Phys &P, const double *const U[5], double *const bufs[3][5], const Fields &F,
-              bool setup, cudaStream_t s);   // returns the number of launches
+              double *const plast[6], bool setup, cudaStream_t s);   // returns the number of launches
+// plast[f] <- F.p at the ghost points of each Rudy outflow face f: SHOCK's
+// copy of U_RK's p into U_lastStep at the end of a step (src/SHOCK.c:661-664).
+void launch_bc_save(const Grid &G, const Fields &F, double *const plast[6], cudaStream_t s);
 void launch_nodal(const Grid &G, int precision, const double *const U[5], const Fields &F, cudaStream_t s);
 void launch_weno(const Grid &G, const Phys &P, int precision, int d, bool first,
                  const double *const U[5], const Fields &F, cudaStream_t s);

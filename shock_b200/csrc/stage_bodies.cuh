@@ -229,6 +229,7 @@ __device__ __forceinline__ void nodal_body(const Grid &G, long long o, const dou
 // ---------------------------------------------------------------------------
 struct StateBufs {
     double *U[3][5];
+    double *plast[6];   // per Rudy outflow face: U_lastStep's p at its ghost points, in face-point order
 };
 
 __device__ __forceinline__ double prod3(double x, double y, double z) { return __dmul_rn(__dmul_rn(x, y), z); }
@@ -237,6 +238,28 @@ __device__ __forceinline__ double prod3(double x, double y, double z) { return _
 // and corners included (src/BC.c:1344-2362); wall and farfield faces only
 // the real tangential range (src/BC.c:638-1343).
 __host__ __device__ inline bool bc_full_face(int type) { return type >= SHOCK_BC_INFLOW_SUBSONIC; }
+
+// Ghost point o of face f's face-point idx (ghost layer l outside the face)
+// and the point s it mirrors (l cells inside).
+template <int DIM>
+__device__ __forceinline__ void bc_points(const Grid &G, int f, long long idx, long long &o, long long &s)
+{
+    const int a = f / 2, side = f % 2;
+    const int tb = a == 0 ? 1 : 0, tc = a == 2 ? 1 : 2;   // tangential axes (tc = 2 is flat in 2D)
+    const bool full = bc_full_face(G.bc[f]);
+    const int t0 = full ? 0 : G.g;                        // first tangential index
+    const long long nc = DIM == 3 ? (full ? G.N[tc] : G.n[tc]) : 1;
+    const long long R = (long long)(full ? G.N[tb] : G.n[tb]) * nc;
+    const int l = (int)(idx / R);
+    const long long r = idx - (long long)l * R;
+    int v[3];
+    v[tb] = t0 + (int)(r / nc);
+    v[tc] = DIM == 3 ? t0 + (int)(r % nc) : 0;
+    v[a] = side ? G.g + G.n[a] + l : G.g - 1 - l;
+    o = v[0] * G.st[0] + v[1] * G.st[1] + v[2];
+    v[a] = side ? G.g + G.n[a] - 1 - l : G.g + l;
+    s = v[0] * G.st[0] + v[1] * G.st[1] + v[2];
+}
 
 // Number of ghost points face f fills.
 __host__ __device__ inline long long bc_face_points(const Grid &G, int f)
@@ -290,21 +313,9 @@ template <int DIM>
 __device__ __forceinline__ void bc_body(const Grid &G, const Phys &P, const Fields &F, const double *const *in,
                                         const StateBufs &B, int f, long long idx, bool setup)
 {
-    const int a = f / 2, side = f % 2;
-    const int tb = a == 0 ? 1 : 0, tc = a == 2 ? 1 : 2;   // tangential axes (tc = 2 is flat in 2D)
-    const bool full = bc_full_face(G.bc[f]);
-    const int t0 = full ? 0 : G.g;                        // first tangential index
-    const long long nc = DIM == 3 ? (full ? G.N[tc] : G.n[tc]) : 1;
-    const long long R = (long long)(full ? G.N[tb] : G.n[tb]) * nc;
-    const int l = (int)(idx / R);
-    const long long r = idx - (long long)l * R;
-    int v[3];
-    v[tb] = t0 + (int)(r / nc);
-    v[tc] = DIM == 3 ? t0 + (int)(r % nc) : 0;
-    v[a] = side ? G.g + G.n[a] + l : G.g - 1 - l;
-    const long long o = v[0] * G.st[0] + v[1] * G.st[1] + v[2];
-    v[a] = side ? G.g + G.n[a] - 1 - l : G.g + l;
-    const long long s = v[0] * G.st[0] + v[1] * G.st[1] + v[2];
+    const int a = f / 2;
+    long long o, s;
+    bc_points<DIM>(G, f, idx, o, s);
 
     const int type = G.bc[f];
     double rho = in[0][s], e = in[4][s];
@@ -317,15 +328,29 @@ __device__ __forceinline__ void bc_body(const Grid &G, const Phys &P, const Fiel
         if (type == SHOCK_BC_WALL_ISOTHERMAL) gT = P.t_wall;
     } else if (type == SHOCK_BC_FARFIELD) {
         gv[0] = u; gv[1] = vv; gv[2] = w;
-    } else if (type == SHOCK_BC_WALL_INVISCID || type == SHOCK_BC_OUTFLOW_SUBSONIC) {
+    } else if (type == SHOCK_BC_WALL_INVISCID || type == SHOCK_BC_OUTFLOW_SUBSONIC || type == SHOCK_BC_OUTFLOW_RUDY) {
         // slip wall: the interior point's contravariant velocities with the
-        // face-normal one negated; subsonic outflow: as they are
-        // (src/BC.c:2553-2558), with p = p_outflow; both turned back into
-        // u, v, w with the ghost point's metric
+        // face-normal one negated; subsonic and Rudy outflow: as they are
+        // (src/BC.c:2553-2558, :2633-2639); all turned back into u, v, w with
+        // the ghost point's metric
         double th[3] = {0.0, 0.0, 0.0};
         if (!setup) bc_theta<DIM>(F, s, u, vv, w, th);
         if (type == SHOCK_BC_WALL_INVISCID) th[a] = -th[a];
-        else gp = P.p_out;
+        else if (type == SHOCK_BC_OUTFLOW_SUBSONIC) gp = P.p_out;
+        else {
+            // Rudy (src/BC.c:2643-2648): U_lastStep's ghost pressure relaxed
+            // towards p_outflow at the rate AlphaNonRef per unit time, plus
+            // rho_L c_L (u - u_L) / Upsilon with U_lastStep's speed of sound
+            // at the interior point -- a field SHOCK allocates zeroed and
+            // never forms there (the face checks exclude the set-up inflow
+            // fills that would), so that term is a signed zero; rho scaled
+            // with p from the interior point, e, c, mu and T copied.  In the
+            // set-up fill U_lastStep is the state being filled: its p at o.
+            const double pl = setup ? F.p[o] : B.plast[f][idx];
+            const double at = __dmul_rn(P.alpha, P.tau);
+            gp = __ddiv_rn(__dadd_rn(pl, __dmul_rn(at, P.p_out)), __dadd_rn(1.0, at));
+            rho = __dmul_rn(__ddiv_rn(gp, F.p[s]), rho);
+        }
         bc_cramer(F, o, th, gv);
     } else {
         // inflow and Riemann outflow (src/BC.c:2363-2542, :2572-2622): a
@@ -385,8 +410,10 @@ __device__ __forceinline__ void bc_body(const Grid &G, const Phys &P, const Fiel
         B.U[k][3][o] = gv[2];
         B.U[k][4][o] = e;
     }
+    // the set-up fill leaves p as SHOCK's leaves U_lastStep's (Rudy's
+    // outflow starts from it); T, c, mu only from the first stage on
+    F.p[o] = gp;
     if (!setup) {
-        F.p[o] = gp;
         F.T[o] = gT;
         F.c[o] = gc;
         F.mu[o] = gmu;

@@ -165,8 +165,35 @@ __global__ void __launch_bounds__(256) k_bc(Grid G, Phys P, Fields F, StageIn in
         bc_body<DIM>(G, P, F, in.U, B, f, i, setup);
 }
 
+template <int DIM>
+__global__ void __launch_bounds__(256) k_bc_save(Grid G, Fields F, StateBufs B)
+{
+    const int f = blockIdx.y;
+    if (G.bc[f] != SHOCK_BC_OUTFLOW_RUDY) return;
+    const long long n = bc_face_points(G, f);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        long long o, s;
+        bc_points<DIM>(G, f, i, o, s);
+        B.plast[f][i] = F.p[o];
+    }
+}
+
+void launch_bc_save(const Grid &G, const Fields &F, double *const plast[6], cudaStream_t s)
+{
+    long long most = 0;
+    StateBufs B{};
+    for (int f = 0; f < 2 * G.dim; f++) {
+        B.plast[f] = plast[f];
+        if (G.bc[f] == SHOCK_BC_OUTFLOW_RUDY && bc_face_points(G, f) > most) most = bc_face_points(G, f);
+    }
+    if (!most) return;
+    const dim3 grid(blocks_for(most, 256), 2 * G.dim);
+    if (G.dim == 3) k_bc_save<3><<<grid, 256, 0, s>>>(G, F, B);
+    else k_bc_save<2><<<grid, 256, 0, s>>>(G, F, B);
+}
+
 int launch_bc(const Grid &G, const Phys &P, const double *const U[5], double *const bufs[3][5], const Fields &F,
-              bool setup, cudaStream_t s)
+              double *const plast[6], bool setup, cudaStream_t s)
 {
     long long most = 0;
     for (int f = 0; f < 2 * G.dim; f++)
@@ -178,6 +205,7 @@ int launch_bc(const Grid &G, const Phys &P, const double *const U[5], double *co
         in.U[q] = U[q];
         for (int k = 0; k < 3; k++) B.U[k][q] = bufs[k][q];
     }
+    for (int f = 0; f < 6; f++) B.plast[f] = plast[f];
     bool full = false;
     for (int f = 0; f < 2 * G.dim; f++) full |= bc_full_face(G.bc[f]);
     if (!full) {   // wall / farfield faces share no ghost point: one launch

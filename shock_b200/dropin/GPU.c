@@ -23,10 +23,10 @@
  *     [BoundaryConditions] T_wall; inflow faces with the
  *     Inflow-Normal-Subsonic, -Supersonic, Inflow-Riemann-Subsonic or
  *     Inflow-Isentrop-Subsonic option and outflow faces with
- *     Outflow-Normal-Subsonic or Outflow-Riemann-Subsonic, with rho_inflow,
- *     p_inflow, p_outflow and the inflow velocity.
- * Faces of any other kind (moving walls, Rudy outflow) are rejected by the
- * library with SHOCK_EINVAL.
+ *     Outflow-Normal-Subsonic, -Riemann-Subsonic or -Rudy-Subsonic, with
+ *     rho_inflow, p_inflow, p_outflow and the inflow velocity.
+ * Faces of any other kind (moving walls) are rejected by the library with
+ * SHOCK_EINVAL.
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -117,7 +117,8 @@ int GPU_Create(struct strct_configuration *c, struct strct_mesh *m, struct strct
                      : c->flag_BC_option_inflow_isentrop_sub == 1 ? SHOCK_BC_INFLOW_ISENTROPIC : -1;
         else if (strncmp(face[f], c->BCOutflow, strlen(c->BCOutflow)) == 0)   /* BCOutflow, -Subsonic */
             sp.bc[f] = c->flag_BC_option_outflow_normal_sub == 1 ? SHOCK_BC_OUTFLOW_SUBSONIC
-                     : c->flag_BC_option_outflow_riemann_sub == 1 ? SHOCK_BC_OUTFLOW_RIEMANN : -1;
+                     : c->flag_BC_option_outflow_riemann_sub == 1 ? SHOCK_BC_OUTFLOW_RIEMANN
+                     : c->flag_BC_option_outflow_rudy_sub == 1 ? SHOCK_BC_OUTFLOW_RUDY : -1;
     }
     sp.t_wall = c->T_wall;
     sp.rho_inflow = c->rho_inflow;

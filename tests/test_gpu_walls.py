@@ -4,7 +4,7 @@ The reference is SHOCK's CPU build with the face BC names set as its
 loader sets them (BCWallViscous, BCWallInviscid, BCFarfield,
 BCWallViscousIsothermal, BCInflow, BCOutflow; src/BC.c) and the inflow /
 outflow options of its config.ini (Normal-Subsonic, Normal-Supersonic,
-Riemann-Subsonic, Isentrop-Subsonic).
+Riemann-Subsonic, Isentrop-Subsonic, Rudy-Subsonic).
 Tolerances as in test_gpu_parity.py: one right-hand side within
 max(1e-12, 2 * SHOCK's own FP64-vs-80-bit distance) per variable, and the
 state after 20 RK steps within max(1e-10, 2 * that distance) relative L2.
@@ -47,7 +47,20 @@ CASES = {
                                                       inviscid=True),
     "duct_isentropic_slip_2d_w5": lambda: cases.duct(2, 5, (28, 18, 1), inflow="inflow_isentropic",
                                                      outflow="outflow_riemann", walls="wall_inviscid"),
+    # Rudy's outflow: U_lastStep's ghost pressure relaxed towards p_outflow;
+    # L0 = 200 m makes AlphaNonRef * tau about 1e-3 per step
+    "duct_rudy_3d_w5": lambda: cases.duct(3, 5, (20, 12, 14), outflow="outflow_rudy"),
+    "duct_rudy_walls_2d_w9": lambda: _with(cases.duct(2, 9, (28, 20, 1), inflow="inflow_riemann",
+                                                      outflow="outflow_rudy", walls="wall_viscous"), l0=200.0),
+    "duct_rudy_slip_3d_w9_euler": lambda: _with(cases.duct(3, 9, (20, 12, 14), outflow="outflow_rudy",
+                                                           walls="wall_inviscid", inviscid=True), l0=200.0),
 }
+
+
+def _with(c, **kw):
+    for k, v in kw.items():
+        setattr(c, k, v)
+    return c
 
 
 def _need(c):

@@ -52,6 +52,28 @@ def test_mixed_inflow_outflow_options_rejected(face, bc):
                                                 z.ctypes.data_as(dp), out.ctypes.data_as(dp)) == 0
 
 
+def test_rudy_outflow_checks():
+    """Rudy's outflow takes an inflow face on its own axis only (on another
+    axis the inflow's set-up fill would give U_lastStep a speed of sound at
+    the outflow's interior points) and needs L0, R, T0 for AlphaNonRef."""
+    c = cases.duct(2, 5, (28, 18, 1), outflow="outflow_rudy", walls="wall_viscous")
+    x, y, z = (np.ascontiguousarray(a.transpose(2, 1, 0)).ravel() for a in (c.x, c.y, c.z))
+    out = np.zeros((13,) + (c.ni + 6, c.nj + 6, 1))
+    dp = C.POINTER(C.c_double)
+
+    def geom(p):
+        return shock_b200.lib().shock_host_geometry(C.byref(p), x.ctypes.data_as(dp), y.ctypes.data_as(dp),
+                                                    z.ctypes.data_as(dp), out.ctypes.data_as(dp))
+
+    assert geom(shock_b200.params_from_case(c)) == 0
+    p = shock_b200.params_from_case(c)
+    p.bc[3] = shock_b200.SHOCK_BC_INFLOW_SUBSONIC
+    assert geom(p) == shock_b200.SHOCK_EINVAL
+    p = shock_b200.params_from_case(c)
+    p.l0 = 0.0
+    assert geom(p) == shock_b200.SHOCK_EINVAL
+
+
 @pytest.mark.parametrize("dim,order,n,bc,stretch,walls_i", CASES)
 def test_wall_geometry_matches_reference(dim, order, n, bc, stretch, walls_i):
     if not ref_available(order, dim):
@@ -77,7 +99,7 @@ def test_bc_argument_checks():
     bad.bc[0] = 1                      # a wall on a periodic axis
     assert geom(bad) == shock_b200.SHOCK_EINVAL
     bad = shock_b200.params_from_case(c)
-    bad.bc[2] = 11                     # unknown type
+    bad.bc[2] = 12                     # unknown type
     assert geom(bad) == shock_b200.SHOCK_EINVAL
     bad = shock_b200.params_from_case(c)
     bad.bc[2] = 0                      # a non-periodic face with nothing to fill it
