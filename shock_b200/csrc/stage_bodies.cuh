@@ -458,12 +458,33 @@ static __constant__ double c_w9is[5][15] = {
     {22658., -140251., 165153., -88297., 18079., 242723., -611976., 337018., -70237., 406293., -464976., 99213., 138563., -60871., 6908.},
     {107918., -649501., 758823., -411487., 86329., 1020563., -2462076., 1358458., -288007., 1521393., -1704396., 364863., 482963., -208501., 22658.},
 };
-static __constant__ float c_w9is_f[5][15] = {
-    {22658.f, -208501.f, 364863.f, -288007.f, 86329.f, 482963.f, -1704396.f, 1358458.f, -411487.f, 1521393.f, -2462076.f, 758823.f, 1020563.f, -649501.f, 107918.f},
-    {6908.f, -60871.f, 99213.f, -70237.f, 18079.f, 138563.f, -464976.f, 337018.f, -88297.f, 406293.f, -611976.f, 165153.f, 242723.f, -140251.f, 22658.f},
-    {6908.f, -51001.f, 67923.f, -38947.f, 8209.f, 104963.f, -299076.f, 179098.f, -38947.f, 231153.f, -299076.f, 67923.f, 104963.f, -51001.f, 6908.f},
-    {22658.f, -140251.f, 165153.f, -88297.f, 18079.f, 242723.f, -611976.f, 337018.f, -70237.f, 406293.f, -464976.f, 99213.f, 138563.f, -60871.f, 6908.f},
-    {107918.f, -649501.f, 758823.f, -411487.f, 86329.f, 1020563.f, -2462076.f, 1358458.f, -288007.f, 1521393.f, -1704396.f, 364863.f, 482963.f, -208501.f, 22658.f},
+// The FP32 form of the same indicators.  Each of SHOCK's forms annihilates
+// constants (its rows sum to zero), so it is a positive-definite form in the
+// sub-stencil's four first differences d0..d3, and with the exact LDL^T
+// factorisation of that 4x4 form (rational L, D > 0)
+//     IS = D0 y0^2 + D1 y1^2 + D2 y2^2 + D3 y3^2,
+//     y3 = d3, y2 = d2 + L32 d3, y1 = d1 + L21 d2 + L31 d3,
+//     y0 = d0 + L10 d1 + L20 d2 + L30 d3,
+// the same value as a sum of non-negative terms.  The integer form's terms
+// are up to 10^4 times IS and cancel, which costs FP32 about 1e-3 of IS;
+// these terms do not (a few units of FP32 rounding).
+// Per sub-stencil: {L10, L20, L21, L30, L31, L32}, then {D0, D1, D2, D3}.
+static __constant__ float c_w9ldl[5][10] = {
+    {float(-163185. / 45316.), float(100839. / 22658.), float(-41089198. / 14249315.), float(-86329. / 45316.),
+     float(1813059. / 838195.), float(-350813921. / 232768856.),
+     22658.f, float(299235615. / 90632.), float(39105167808. / 14249315.), float(116566909305. / 29096107.)},
+    {float(-47055. / 13816.), float(26079. / 6908.), float(-12448558. / 5880675.), float(-18079. / 13816.),
+     float(5686883. / 5880675.), float(-146761231. / 232768856.),
+     6908.f, float(123494175. / 27632.), float(13035055936. / 1960225.), float(116566909305. / 29096107.)},
+    {float(-37185. / 13816.), float(15369. / 6908.), float(-1032654. / 838195.), float(-8209. / 13816.),
+     float(5686883. / 14249315.), float(-20636113. / 51089708.),
+     6908.f, float(299235615. / 27632.), float(8583070944. / 838195.), float(233133818610. / 217131259.)},
+    {float(-94935. / 45316.), float(35109. / 22658.), float(-106728718. / 110863235.), float(-18079. / 45316.),
+     float(30822003. / 110863235.), float(-1745642471. / 4217089556.),
+     22658.f, float(2328127935. / 90632.), float(101210149344. / 15837605.), float(233133818610. / 1054272389.)},
+    {float(-433665. / 215836.), float(162579. / 107918.), float(-945305518. / 890329635.), float(-86329. / 215836.),
+     float(290071763. / 890329635.), float(-8384962321. / 17843974736.),
+     107918.f, float(18696922335. / 431672.), float(999262585216. / 296776545.), float(16652415615. / 318642406.)},
 };
 
 // Packed FP32 arithmetic (two lanes per instruction) for the mixed form:
@@ -499,43 +520,6 @@ template <typename T>
 __device__ __forceinline__ T w9c(int k, int i);
 template <>
 __device__ __forceinline__ double w9c<double>(int k, int i) { return c_w9is[k][i]; }
-template <>
-__device__ __forceinline__ float w9c<float>(int k, int i) { return c_w9is_f[k][i]; }
-
-// f: 9 stencil values, d: 8 differences.
-template <typename T>
-__device__ __forceinline__ T phi_w9(const T *f, const T *d, T eps)
-{
-    const T dk[5] = {T(1. / 126.), T(10. / 63.), T(10. / 21.), T(20. / 63.), T(5. / 126.)};
-    T ot[5];
-#pragma unroll
-    for (int k = 0; k < 5; k++) {
-        T acc = T(0);
-        int c = 0;
-#pragma unroll
-        for (int a = 0; a < 5; a++) {
-            T in = w9c<T>(k, c++) * f[k + a];
-#pragma unroll
-            for (int b = a + 1; b < 5; b++) in = in + w9c<T>(k, c++) * f[k + b];
-            acc = (a == 0) ? f[k] * in : acc + f[k + a] * in;
-        }
-        // the indicator is a non-negative quadratic form; in FP32 rounding can
-        // make it slightly negative and cancel eps (1/t^2 overflows), so the
-        // FP32 form clamps it at zero.  The FP64 form keeps SHOCK's sequence.
-        if (std::is_same<T, float>::value) acc = acc > T(0) ? acc : T(0);
-        T t = acc + eps;
-        ot[k] = dk[k] * (T(1.) / (t * t));
-    }
-    T rs = T(1.) / (ot[0] + ot[1] + ot[2] + ot[3] + ot[4]);
-    T o0 = ot[0] * rs, o2 = ot[2] * rs, o3 = ot[3] * rs, o4 = ot[4] * rs;
-    T q1 = d[0] - T(4.) * d[1] + T(6.) * d[2] - T(4.) * d[3] + d[4];
-    T q2 = d[1] - T(4.) * d[2] + T(6.) * d[3] - T(4.) * d[4] + d[5];
-    T q3 = d[2] - T(4.) * d[3] + T(6.) * d[4] - T(4.) * d[5] + d[6];
-    T q4 = d[3] - T(4.) * d[4] + T(6.) * d[5] - T(4.) * d[6] + d[7];
-    return T(1. / 5.) * o0 * q1 + T(1. / 20.) * o2 * q2 + T(1. / 60.) * o3 * (T(3.) * q2 - T(2.) * q3)
-           + T(1. / 60.) * o4 * (T(3.) * q2 - T(2.) * q3 + T(3.) * q4)
-           - T(1. / 840.) * (T(39.) * q2 - T(14.) * q3 + T(3.) * q4);
-}
 
 // ---------------------------------------------------------------------------
 // Sweep geometry: sweep axis D, lateral axis (32 lines, the fastest
@@ -858,8 +842,8 @@ __device__ __forceinline__ double w5_phi(const double *d, const double *r)
     return 1. / 3. * o0 * q1 + 1. / 6. * (o2 - 0.5) * q2;
 }
 
-// WENO9 smoothness terms t = IS + eps of one stencil (9 values f); the FP32
-// form clamps IS at zero (see phi_w9).
+// WENO9 smoothness terms t = IS + eps of one stencil (9 values f), SHOCK's
+// integer forms in its order (FP64).
 template <typename T>
 __device__ __forceinline__ void w9_terms(const T *f, T eps, T *t)
 {
@@ -874,8 +858,23 @@ __device__ __forceinline__ void w9_terms(const T *f, T eps, T *t)
             for (int b = a + 1; b < 5; b++) in = in + w9c<T>(k, c++) * f[k + b];
             acc = (a == 0) ? f[k] * in : acc + f[k + a] * in;
         }
-        if (std::is_same<T, float>::value) acc = acc > T(0) ? acc : T(0);
         t[k] = acc + eps;
+    }
+}
+
+// The same terms in FP32 from the stencil's eight first differences d, by
+// the factorised forms (c_w9ldl).  The indicators are even in d, so the
+// minus side's stencil takes its differences with either sign.
+__device__ __forceinline__ void w9_terms_diff(const float *d, float eps, float *t)
+{
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const float *x = d + k, *c = c_w9ldl[k];
+        const float y0 = fmaf(c[3], x[3], fmaf(c[1], x[2], fmaf(c[0], x[1], x[0])));
+        const float y1 = fmaf(c[4], x[3], fmaf(c[2], x[2], x[1]));
+        const float y2 = fmaf(c[5], x[3], x[2]);
+        const float is = fmaf(c[6] * y0, y0, fmaf(c[7] * y1, y1, fmaf(c[8] * y2, y2, c[9] * x[3] * x[3])));
+        t[k] = is + eps;
     }
 }
 
@@ -897,9 +896,9 @@ __device__ __forceinline__ T w9_phi(const T *d, const T *r)
            - T(1. / 840.) * (T(39.) * q2 - T(14.) * q3 + T(3.) * q4);
 }
 
-// In FP32 the clamped terms are at least eps32 = 10 sqrt(FLT_MIN), so a pair
-// product is normal too; a product that overflows gives zero reciprocals,
-// the zero weights 1/(t*t) gives there.
+// In FP32 the terms (a non-negative indicator plus eps32 = 10 sqrt(FLT_MIN))
+// are at least eps32, so a pair product is normal too; a product that
+// overflows gives zero reciprocals, the zero weights 1/(t*t) gives there.
 template <int N, typename T>
 __device__ __forceinline__ void pair_reciprocals(const T *e, T *r)
 {
@@ -1165,16 +1164,12 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
             }
             float phi;
             {
-                float dP[8], dM[8], fp[9], fm[9];
+                float dP[8], dM[8];
 #pragma unroll
                 for (int q = 0; q < 8; q++) { dP[q] = dp[q]; dM[q] = dmv[2 * r - q]; }
-                fp[0] = 0.f;
-                fm[0] = 0.f;
-#pragma unroll
-                for (int q = 0; q < 8; q++) { fp[q + 1] = fp[q] + dP[q]; fm[q + 1] = fm[q] - dM[q]; }
                 float tt[10], rc[10];
-                w9_terms<float>(fp, eps, tt);
-                w9_terms<float>(fm, eps, tt + 5);
+                w9_terms_diff(dP, eps, tt);
+                w9_terms_diff(dM, eps, tt + 5);
                 pair_reciprocals<10>(tt, rc);
                 phi = -w9_phi<float>(dP, rc) + w9_phi<float>(dM, rc + 5);
             }

@@ -54,6 +54,9 @@ CASES = {
                                                       outflow="outflow_rudy", walls="wall_viscous"), l0=200.0),
     "duct_rudy_slip_3d_w9_euler": lambda: _with(cases.duct(3, 9, (20, 12, 14), outflow="outflow_rudy",
                                                            walls="wall_inviscid", inviscid=True), l0=200.0),
+    # three-stage RK: the step ends on another state buffer
+    "duct_rudy_rk3_2d_w5": lambda: _with(cases.duct(2, 5, (28, 18, 1), inflow="inflow_riemann", outflow="outflow_rudy",
+                                                    walls="wall_viscous", time_order=3), l0=200.0),
 }
 
 
@@ -96,8 +99,9 @@ def test_wall_steps_match_reference(name):
     assert (err <= tol).all(), (err, tol)
 
 
-def test_wall_mixed_precision_l2():
-    c = cases.channel(3, 5, (16, 12, 14), bc="wall_viscous", stretch=1.2)
+@pytest.mark.parametrize("name", ["noslip_3d_w5", "duct_rudy_3d_w5", "duct_riemann_walls_2d_w9"])
+def test_wall_mixed_precision_l2(name):
+    c = CASES[name]()
     a = shock_b200.Solver(c)
     b = shock_b200.Solver(c, precision=shock_b200.SHOCK_MIXED)
     a.steps(20)
@@ -106,12 +110,18 @@ def test_wall_mixed_precision_l2():
     assert (err <= 1e-6).all(), err
 
 
-def test_wall_dropin_loop_matches_reference_loop():
-    c = CASES["noslip_3d_w5"]()
+@pytest.mark.parametrize("name", ["noslip_3d_w5", "duct_sub_3d_w5", "duct_riemann_3d_w5", "duct_rudy_3d_w5",
+                                  "duct_isentropic_slip_2d_w5"])
+def test_wall_dropin_loop_matches_reference_loop(name):
+    """SHOCK's own time loop with the binding (GPU.c) in place of
+    CalcRungeKutta: the binding maps SHOCK's face names and inflow /
+    outflow option flags to the library's face types."""
+    c = CASES[name]()
     if not dropin_available(c.order, c.dim):
         pytest.skip("drop-in harness not built")
-    r = RefSolver(c)
+    r, r80 = RefSolver(c), RefSolver(c, extended=True)
     r.steps(20)
+    r80.steps(20)
     d = DropinSolver(c, device=0)
     try:
         d.steps(20)
@@ -119,5 +129,7 @@ def test_wall_dropin_loop_matches_reference_loop():
         st = real(c, d.state()[:5])
     finally:
         d.close()
-    err = l2_rel(st, real(c, r.state()[:5]))
-    assert (err <= L2_TOL).all(), err
+    ref = real(c, r.state()[:5])
+    tol = np.maximum(L2_TOL, 2.0 * l2_rel(ref, real(c, r80.state()[:5])))
+    err = l2_rel(st, ref)
+    assert (err <= tol).all(), (err, tol)
