@@ -242,8 +242,10 @@ static int check_faces(const shock_params *p)
     }
     // Rudy's outflow reads U_lastStep's speed of sound at its interior
     // points, which SHOCK leaves zero unless an inflow face's set-up fill
-    // wrote it there: an inflow face on another axis shares those points.
-    if (rudy_axes && (in_axes & ~rudy_axes))
+    // wrote it there: an inflow face on an axis other than a Rudy face's
+    // shares those points.  So inflow and Rudy faces may only share one axis.
+    const bool one_axis = in_axes == rudy_axes && !(in_axes & (in_axes - 1));
+    if (rudy_axes && in_axes && !one_axis)
         return fail(SHOCK_EINVAL, "Rudy outflow with an inflow face on another axis");
     if (rudy_axes && (p->l0 <= 0 || p->gas_r <= 0 || p->t0 <= 0))
         return fail(SHOCK_EINVAL, "Rudy outflow needs l0, gas_r and t0 > 0 (AlphaNonRef)");

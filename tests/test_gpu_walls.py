@@ -54,6 +54,9 @@ CASES = {
                                                       outflow="outflow_rudy", walls="wall_viscous"), l0=200.0),
     "duct_rudy_slip_3d_w9_euler": lambda: _with(cases.duct(3, 9, (20, 12, 14), outflow="outflow_rudy",
                                                            walls="wall_inviscid", inviscid=True), l0=200.0),
+    # Rudy faces on two axes sharing a corner, walls on the others
+    "box_rudy_2d_w5": lambda: _with(cases.duct(2, 5, (28, 18, 1), outflow="outflow_rudy", walls="wall_viscous"),
+                                    bc=(1, 11, 1, 11, 0, 0), l0=200.0),
     # three-stage RK: the step ends on another state buffer
     "duct_rudy_rk3_2d_w5": lambda: _with(cases.duct(2, 5, (28, 18, 1), inflow="inflow_riemann", outflow="outflow_rudy",
                                                     walls="wall_viscous", time_order=3), l0=200.0),

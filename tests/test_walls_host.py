@@ -69,6 +69,12 @@ def test_rudy_outflow_checks():
     p = shock_b200.params_from_case(c)
     p.bc[3] = shock_b200.SHOCK_BC_INFLOW_SUBSONIC
     assert geom(p) == shock_b200.SHOCK_EINVAL
+    # Rudy faces on two axes: the x-lower inflow shares points with the y one
+    p = shock_b200.params_from_case(c)
+    p.bc[3] = shock_b200.SHOCK_BC_OUTFLOW_RUDY
+    assert geom(p) == shock_b200.SHOCK_EINVAL
+    p.bc[0] = shock_b200.SHOCK_BC_WALL_VISCOUS
+    assert geom(p) == 0
     p = shock_b200.params_from_case(c)
     p.l0 = 0.0
     assert geom(p) == shock_b200.SHOCK_EINVAL
