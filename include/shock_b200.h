@@ -146,6 +146,14 @@ int shock_host_mms_baseline(const shock_params *p, const double *x, const double
 /* Host <-> device state (rho,u,v,w,e; 5*NG doubles, ghosted).
  * which = 0: U_RK (the running state), 1: U_lastStep. */
 int shock_upload_state(shock_ctx *ctx, const double *prim5);
+
+/* U_lastStep's pressure p (NG doubles, ghosted, SHOCK's layout) that goes with
+ * a state loaded by shock_upload_state, e.g. after SHOCK's NaN reset reloads
+ * U_RK and then U_lastStep, p included, from a backup (src/SHOCK.c:598-601,
+ * 661-664).  Only Rudy outflow faces read it, at their ghost points
+ * (src/BC.c:2643-2646); a no-op for blocks without one.  No reference
+ * counterpart: SHOCK keeps this pressure in U_lastStep->p. */
+int shock_upload_last_pressure(shock_ctx *ctx, const double *p);
 int shock_download_state(shock_ctx *ctx, double *prim5, int which);
 
 /* One right-hand side at the current state, in CalcRungeKutta's stage

@@ -295,6 +295,13 @@ void ref_set_state(const double *in)
         for (int o = 0; o < n; o++) { a[f][o] = (FLT)in[(size_t)f * n + o]; b[f][o] = (FLT)in[(size_t)f * n + o]; }
 }
 
+/* Overwrite p (NG) of U_lastStep. */
+void ref_set_last_p(const double *in)
+{
+    int n = NG;
+    for (int o = 0; o < n; o++) U_last.p[o] = (FLT)in[o];
+}
+
 /* out: x,y,z,J,xi_x,xi_y,xi_z,eta_x,eta_y,eta_z,zeta_x,zeta_y,zeta_z (13*NG). */
 void ref_get_geom(double *out)
 {

@@ -131,6 +131,12 @@ class RefSolver:
         assert a.size == 5 * self.n
         self.lib.ref_set_state(_ptr(a))
 
+    def set_last_pressure(self, p: np.ndarray):
+        """p of U_lastStep (ghosted)."""
+        a = np.ascontiguousarray(p, dtype=np.float64).ravel()
+        assert a.size == self.n
+        self.lib.ref_set_last_p(_ptr(a))
+
     def geometry(self) -> np.ndarray:
         """x,y,z,J,xi_x,xi_y,xi_z,eta_x,eta_y,eta_z,zeta_x,zeta_y,zeta_z."""
         g = np.zeros(13 * self.n)

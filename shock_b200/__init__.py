@@ -99,7 +99,8 @@ def lib():
             L.shock_last_error.restype = C.c_char_p
             L.shock_create.argtypes = [C.POINTER(Params)] + [_dp] * 8 + [C.c_int, C.POINTER(C.c_void_p)]
             for name in ("shock_destroy", "shock_dims", "shock_set_dirichlet", "shock_set_source",
-                         "shock_upload_state", "shock_download_state", "shock_rhs", "shock_step",
+                         "shock_upload_state", "shock_upload_last_pressure", "shock_download_state", "shock_rhs",
+                         "shock_step",
                          "shock_step_async", "shock_sync", "shock_check_nan", "shock_geometry",
                          "shock_device_bytes", "shock_last_step_ms", "shock_kernels_per_step",
                          "shock_mms_baseline", "shock_profile_stage", "shock_measure_fma_peak",
@@ -267,6 +268,13 @@ class Solver:
         a = np.ascontiguousarray(prim5, np.float64).ravel()
         assert a.size == 5 * self.n
         _check(self.lib.shock_upload_state(self.h, _ptr(a)))
+
+    def set_last_pressure(self, p):
+        """U_lastStep's pressure (ghosted) for the state set_state loaded:
+        Rudy outflow faces start from it."""
+        a = np.ascontiguousarray(p, np.float64).ravel()
+        assert a.size == self.n
+        _check(self.lib.shock_upload_last_pressure(self.h, _ptr(a)))
 
     def post(self) -> np.ndarray:
         """Mach number, |grad rho| and lambda2 of the current state (3 fields,

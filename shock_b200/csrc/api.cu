@@ -184,7 +184,7 @@ static void enqueue_step(shock_ctx *c, int un, int &nk)
     }
     // end of the step: U_RK's p becomes U_lastStep's (src/SHOCK.c:661-664)
     if (c->plast_pool) {
-        launch_bc_save(c->G, c->F, c->plast, c->stream);
+        launch_bc_save(c->G, c->F.p, c->plast, c->stream);
         nk++;
     }
 }
@@ -364,7 +364,7 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
     if (c->P.walls) {
         const double *b0[5] = {c->buf[0][0], c->buf[0][1], c->buf[0][2], c->buf[0][3], c->buf[0][4]};
         launch_bc(G, c->P, b0, c->buf, c->F, c->plast, true, c->stream);
-        if (rudy_pts) launch_bc_save(G, c->F, c->plast, c->stream);
+        if (rudy_pts) launch_bc_save(G, c->F.p, c->plast, c->stream);
         cudaStreamSynchronize(c->stream);
     }
     c->geo_host = std::move(hb.geo);
@@ -495,6 +495,24 @@ int shock_upload_state(shock_ctx *c, const double *prim5)
             for (int f = 0; f < 5; f++)
                 CK(cudaMemcpyAsync(c->buf[b][f], c->buf[0][f], nb, cudaMemcpyDeviceToDevice, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return SHOCK_OK;
+}
+
+int shock_upload_last_pressure(shock_ctx *c, const double *p)
+{
+    if (!c || !p) return fail(SHOCK_EINVAL, "null argument");
+    if (!c->plast_pool) return SHOCK_OK;
+    CK(cudaSetDevice(c->device));
+    const size_t nb = sizeof(double) * c->G.NG;
+    double *tmp = nullptr;
+    if (cudaMalloc(&tmp, nb) != cudaSuccess) return fail(SHOCK_ENOMEM, "cudaMalloc of %zu bytes failed", nb);
+    cudaError_t e = cudaMemcpyAsync(tmp, p, nb, cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) {
+        launch_bc_save(c->G, tmp, c->plast, c->stream);
+        e = cudaStreamSynchronize(c->stream);
+    }
+    cudaFree(tmp);
+    if (e != cudaSuccess) return fail(SHOCK_ECUDA, "shock_upload_last_pressure: %s", cudaGetErrorString(e));
     return SHOCK_OK;
 }
 

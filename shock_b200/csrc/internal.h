@@ -181,9 +181,10 @@ void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const F
 // outflow faces (nullptr elsewhere).
 int launch_bc(const Grid &G, const Phys &P, const double *const U[5], double *const bufs[3][5], const Fields &F,
               double *const plast[6], bool setup, cudaStream_t s);   // returns the number of launches
-// plast[f] <- F.p at the ghost points of each Rudy outflow face f: SHOCK's
-// copy of U_RK's p into U_lastStep at the end of a step (src/SHOCK.c:661-664).
-void launch_bc_save(const Grid &G, const Fields &F, double *const plast[6], cudaStream_t s);
+// plast[f] <- p at the ghost points of each Rudy outflow face f (p: a ghosted
+// field, F.p for SHOCK's copy of U_RK's p into U_lastStep at the end of a
+// step, src/SHOCK.c:661-664).
+void launch_bc_save(const Grid &G, const double *p, double *const plast[6], cudaStream_t s);
 void launch_nodal(const Grid &G, int precision, const double *const U[5], const Fields &F, cudaStream_t s);
 void launch_weno(const Grid &G, const Phys &P, int precision, int d, bool first,
                  const double *const U[5], const Fields &F, cudaStream_t s);

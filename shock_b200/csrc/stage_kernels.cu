@@ -166,7 +166,7 @@ __global__ void __launch_bounds__(256) k_bc(Grid G, Phys P, Fields F, StageIn in
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(256) k_bc_save(Grid G, Fields F, StateBufs B)
+__global__ void __launch_bounds__(256) k_bc_save(Grid G, const double *__restrict__ p, StateBufs B)
 {
     const int f = blockIdx.y;
     if (G.bc[f] != SHOCK_BC_OUTFLOW_RUDY) return;
@@ -174,11 +174,11 @@ __global__ void __launch_bounds__(256) k_bc_save(Grid G, Fields F, StateBufs B)
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         long long o, s;
         bc_points<DIM>(G, f, i, o, s);
-        B.plast[f][i] = F.p[o];
+        B.plast[f][i] = p[o];
     }
 }
 
-void launch_bc_save(const Grid &G, const Fields &F, double *const plast[6], cudaStream_t s)
+void launch_bc_save(const Grid &G, const double *p, double *const plast[6], cudaStream_t s)
 {
     long long most = 0;
     StateBufs B{};
@@ -188,8 +188,8 @@ void launch_bc_save(const Grid &G, const Fields &F, double *const plast[6], cuda
     }
     if (!most) return;
     const dim3 grid(blocks_for(most, 256), 2 * G.dim);
-    if (G.dim == 3) k_bc_save<3><<<grid, 256, 0, s>>>(G, F, B);
-    else k_bc_save<2><<<grid, 256, 0, s>>>(G, F, B);
+    if (G.dim == 3) k_bc_save<3><<<grid, 256, 0, s>>>(G, p, B);
+    else k_bc_save<2><<<grid, 256, 0, s>>>(G, p, B);
 }
 
 int launch_bc(const Grid &G, const Phys &P, const double *const U[5], double *const bufs[3][5], const Fields &F,

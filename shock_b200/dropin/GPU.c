@@ -198,6 +198,11 @@ void GPU_UploadState(struct strct_configuration *c, struct strct_U *U_RK)
         for (size_t o = 0; o < ng; o++) g_buf[f * ng + o] = (double)srcf[f][o];
     int rc = shock_upload_state(g_ctx, g_buf);
     if (rc) fail("shock_upload_state", rc);
+    /* SHOCK's reset gives U_lastStep the same p (src/SHOCK.c:598-601,
+     * 661-664); Rudy outflow faces read it at their ghost points */
+    for (size_t o = 0; o < ng; o++) g_buf[o] = (double)U_RK->p[o];
+    rc = shock_upload_last_pressure(g_ctx, g_buf);
+    if (rc) fail("shock_upload_last_pressure", rc);
     g_host_behind = 0;
 }
 

@@ -102,6 +102,35 @@ def test_wall_steps_match_reference(name):
     assert (err <= tol).all(), (err, tol)
 
 
+@pytest.mark.parametrize("name", ["duct_rudy_walls_2d_w9", "box_rudy_2d_w5"])
+def test_rudy_reset_to_backup_matches_reference(name):
+    """SHOCK's NaN reset reloads U_RK and U_lastStep, p included, from a
+    backup (src/SHOCK.c:598-601, 661-664): both solvers go back to SHOCK's
+    state after 3 steps once they have run 7, then run 10 more.  The Rudy
+    faces start again from the backup's ghost pressure."""
+    c = CASES[name]()
+    _need(c)
+    refs = [RefSolver(c), RefSolver(c, extended=True)]
+    backups = []
+    for r in refs:
+        r.steps(3)
+        backups.append(r.state())
+        r.steps(4)
+    s = shock_b200.Solver(c)
+    s.steps(7)
+    for r, b in zip(refs, backups):
+        r.set_state(b[:5])
+        r.set_last_pressure(b[5])
+    s.set_state(backups[0][:5])
+    s.set_last_pressure(backups[0][5])
+    for x in refs + [s]:
+        x.steps(10)
+    ref = real(c, refs[0].state()[:5])
+    tol = np.maximum(L2_TOL, 2.0 * l2_rel(ref, real(c, refs[1].state()[:5])))
+    err = l2_rel(real(c, s.state()), ref)
+    assert (err <= tol).all(), (err, tol)
+
+
 @pytest.mark.parametrize("name", ["noslip_3d_w5", "duct_rudy_3d_w5", "duct_riemann_walls_2d_w9"])
 def test_wall_mixed_precision_l2(name):
     c = CASES[name]()
