@@ -102,6 +102,22 @@ def test_wall_steps_match_reference(name):
     assert (err <= tol).all(), (err, tol)
 
 
+@pytest.mark.parametrize("name", ["noslip_3d_w5", "duct_rudy_walls_2d_w9", "duct_isentropic_slip_2d_w5"])
+def test_wall_100_steps_match_reference(name):
+    """100 RK steps within max(1e-10, 2 * SHOCK's own FP64-vs-80-bit
+    distance) relative L2, the bar of the periodic parity tests."""
+    c = CASES[name]()
+    _need(c)
+    s = shock_b200.Solver(c)
+    r, r80 = RefSolver(c), RefSolver(c, extended=True)
+    for x in (s, r, r80):
+        x.steps(100)
+    ref = real(c, r.state()[:5])
+    tol = np.maximum(L2_TOL, 2.0 * l2_rel(ref, real(c, r80.state()[:5])))
+    err = l2_rel(real(c, s.state()), ref)
+    assert (err <= tol).all(), (err, tol)
+
+
 @pytest.mark.parametrize("name", ["duct_rudy_walls_2d_w9", "box_rudy_2d_w5"])
 def test_rudy_reset_to_backup_matches_reference(name):
     """SHOCK's NaN reset reloads U_RK and U_lastStep, p included, from a
