@@ -1,27 +1,36 @@
 """Benchmark: cell-stage updates/s of SHOCK's per-RK-stage right-hand side.
 
-Default workload (N=1): the 3D curvilinear Taylor-Green vortex, 64^3
-periodic points with every coordinate perturbed by x_i += 0.05 sin(x_j)
-sin(x_k), Ma = 0.1, Re = 1600, WENO5, viscous, RK4, FP64 (plain form).
-A step is one RK4 time step (4 stage right-hand sides + updates) over the
-whole block.  Inputs are synthetic (seedless analytic initial state).
+Default workload (N=1): 3D decaying compressible turbulence on a 512^3
+uniform periodic cube, WENO9, viscous, RK4, FP64 (plain form): the largest
+configuration that fits one GPU (about 58 GB of device memory).  The initial
+velocity is a seeded random-phase solenoidal field, E(k) ~ k^4 exp(-2(k/4)^2),
+at turbulent Mach 0.6, rho = 1, p = 1/gamma, Re_lambda = 100 (synthetic
+inputs; no dataset is involved).  A step is one RK4 time step (4 stage
+right-hand sides + updates) over the whole block.
 
 Metric: cell-stage updates/s = real points x stages x steps x ranks / time.
   value  -- device time with the state resident in HBM (CUDA events on the
-            solver's stream around each step's graph), the L2 flushed
-            (256 MiB write) between timed steps because the 64^3 state fits
-            in the 126 MB L2.
+            solver's stream around each step's graph); the 512^3 state is
+            far larger than L2 (small blocks get the L2 flushed by a 256 MiB
+            write between timed steps).  The timed step graphs carry an event
+            after every launch, so the per-kernel times (roofline.kernels_ms_
+            per_step) are measured over the same timed steps and add up to
+            the step time.
   e2e    -- the same steps through the public C ABI with host buffers:
             every step uploads the state from pinned host memory
             (shock_upload_state), runs it (shock_step) and reads the state
             back (shock_download_state); host wall clock around the three
             synchronous calls.
-The mixed form (FP32 stencils, FP64 state) is reported beside it.
+The mixed form (FP32 stencils, FP64 state) is timed the same way beside it,
+and both forms are run on to 50 steps (the configuration's run length) from
+the same initial state: "mixed.l2_vs_fp64" is the relative L2 of each
+conserved variable of the mixed form against the FP64 form.
 
 --impl reference: SHOCK's own CPU code (oracle/_ref, the unmodified
-reference sources) on the same workload, one single-block process per host
-core, each advancing its own copy; aggregate cell-stage/s over a bounded
-sample of steps.  Under torchrun only rank 0 runs it.
+reference sources) on a bounded sample of the workload (REF_SAMPLES), one
+single-block process per host core, each advancing its own copy by the same
+--warmup and --steps RK4 steps; aggregate cell-stage/s over the slowest
+process.  Under torchrun only rank 0 runs it.
 
 Multi-GPU (torchrun, N>1): replicas only -- every rank advances its own
 copy of the block (no data exchange on the path), value sums all ranks
@@ -89,14 +98,22 @@ def batch_cases(nmem=256, seed=4):
     return out
 
 
-def measured_traffic(workload, kernel, precision="fp64"):
+def measured_traffic(workload, kernel, points, precision="fp64"):
     """DRAM bytes (read + write) of one launch of `kernel` on `workload`, from
-    the ncu capture recorded in shock_b200/roofline.json (None if absent)."""
+    an ncu capture recorded in shock_b200/roofline.json: the workload's own,
+    or that of a smaller block of the same flow and order scaled by the
+    points one launch processes (None if neither is recorded)."""
     path = os.path.join(ROOT, "shock_b200", "roofline.json")
     with open(path) as f:
         t = json.load(f).get("traffic", {})
     e = t.get(workload, {}).get(precision, {}).get(kernel)
-    return None if e is None else e["bytes"]
+    if e is not None:
+        return e["bytes"]
+    for src in t.get(workload, {}).get("scaled_from", []):
+        e = t.get(src, {}).get(precision, {}).get(kernel)
+        if e is not None and e.get("points"):
+            return e["bytes"] * points / e["points"]
+    return None
 
 
 def flops_per_cell_stage(case):
@@ -198,42 +215,55 @@ def flush_l2(torch, buf):
 # reference arm (CPU)
 # ---------------------------------------------------------------------------
 def _ref_worker(args):
-    name, nsteps = args
+    spec, nsteps, nwarm = args
     # SHOCK's own code reports its set-up on stdout; keep the bench's stdout
     # to the one JSON line
     devnull = os.open(os.devnull, os.O_WRONLY)
     os.dup2(devnull, 1)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     from refbind import RefSolver
-    if isinstance(name, tuple):          # (builder name, kwargs) of shock_b200.cases
-        from shock_b200 import cases
-        case = getattr(cases, name[0])(**name[1])
-    else:
-        case = make_case(name)
+    from shock_b200 import cases
+    case = getattr(cases, spec[0])(**spec[1])
     r = RefSolver(case)
-    r.steps(1)                      # warm-up (first touch)
+    r.steps(nwarm)                  # warm-up (first touch)
     t = r.time_steps(nsteps)
     return t, case.real_points * case.time_order * nsteps
 
 
-def reference_throughput(name, steps, procs):
+def reference_throughput(spec, steps, warmup, procs):
+    """procs processes, each advancing its own copy of the block `spec` (a
+    shock_b200.cases builder and its arguments) by warmup untimed and steps
+    timed RK steps; aggregate cell-stage/s over the slowest process."""
     ctx = mp.get_context("spawn")
-    spec = CPU_SAMPLE.get(name, name)
     with ctx.Pool(procs) as pool:
-        res = pool.map(_ref_worker, [(spec, steps)] * procs)
+        res = pool.map(_ref_worker, [(spec, steps, warmup)] * procs)
     tmax = max(t for t, _ in res)
     cells = sum(c for _, c in res)
     return cells / tmax, tmax, res
 
 
-# SHOCK's CPU build keeps about 300 doubles per ghosted point, so a 512^3
-# block (about 340 GB) does not fit in host memory: the reference arm of the
-# 512^3 workloads times 128^3 blocks of the same flow and order instead and
-# reports per-cell-stage rates.
-CPU_SAMPLE = {
-    "turb512_w9": ("decaying_turbulence", {"n": 128, "order": 9}),
-    "tgv512_w5": ("taylor_green", {"n": 128, "order": 5}),
+# The CPU sample of each single-block workload: the block itself where one RK4
+# step of SHOCK's CPU code takes a few seconds, else a 64^3 (WENO5) or 48^3
+# (WENO9) block of the same flow and order, about 2 s per RK4 step on one
+# core (a 512^3 block needs about 340 GB in SHOCK's CPU build, about 300
+# doubles per ghosted point, and one RK4 step of a 128^3 WENO9 block takes
+# about half a minute per core).
+REF_SAMPLES = {
+    "tgv64_w5": (("taylor_green", {"n": 64, "order": 5}), "the tgv64_w5 block"),
+    "tgv128_w5": (("taylor_green", {"n": 64, "order": 5}), "a 64^3 block of the same flow and order"),
+    "tgv512_w5": (("taylor_green", {"n": 64, "order": 5}), "a 64^3 block of the same flow and order"),
+    "turb128_w9": (("decaying_turbulence", {"n": 48, "order": 9}), "a 48^3 block of the same flow and order"),
+    "turb256_w9": (("decaying_turbulence", {"n": 48, "order": 9}), "a 48^3 block of the same flow and order"),
+    "turb512_w9": (("decaying_turbulence", {"n": 48, "order": 9}), "a 48^3 block of the same flow and order"),
+    "mms64_w5": (("mms_square", {"n": 64, "order": 5, "family": "baseline"}), "the mms64_w5 block"),
 }
+
+
+def ref_sample(workload):
+    spec, what = REF_SAMPLES[workload]
+    kw = spec[1]
+    pts = kw["n"] ** (2 if spec[0] == "mms_square" else 3)
+    return spec, pts, what
 
 
 def _host_avail_bytes():
@@ -257,7 +287,7 @@ def ref_procs(points=64 ** 3, order=5):
     return max(1, min(os.cpu_count() or 1, 32, int(0.5 * _host_avail_bytes() // per)))
 
 
-def batch_reference_sample(procs, steps=1, seed=4):
+def batch_reference_sample(procs, steps=1, warmup=1, seed=4):
     """SHOCK's own CPU code on a sample of the batch members: one member per
     process (the first `procs` members), `steps` timed RK4 steps each."""
     import numpy as np
@@ -269,26 +299,30 @@ def batch_reference_sample(procs, steps=1, seed=4):
                                             "mach_inf": float(rng.uniform(0.2, 0.8))}))
     ctx = mp.get_context("spawn")
     with ctx.Pool(procs) as pool:
-        res = pool.map(_ref_worker, [(sp, steps) for sp in specs[:procs]])
+        res = pool.map(_ref_worker, [(sp, steps, warmup) for sp in specs[:procs]])
     tmax = max(t for t, _ in res)
     cells = sum(c for _, c in res)
     return cells / tmax, tmax
 
 
-def run_reference(args, rank):
+def run_reference(args, rank, world):
+    """SHOCK's own CPU implementation of the path (oracle/_ref) on the host
+    cores: every process advances its own copy of the workload's CPU sample
+    by --warmup untimed and --steps timed RK4 steps (each step a bounded
+    sample of the workload); rank 0 only."""
     if rank != 0:
         return
     if args.workload == "batch_vortex256":
         procs = ref_procs(256 ** 2, 5)
-        v, t = batch_reference_sample(procs, steps=max(1, min(args.steps, args.ref_steps)))
+        v, t = batch_reference_sample(procs, steps=args.steps, warmup=args.warmup)
         print(json.dumps({
             "metric": "cell-stage updates/s", "value": v, "unit": "cell-stage updates/s", "impl": "reference",
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3 / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "description": WORKLOADS[args.workload]},
             "cpu_baseline": {"value": v, "unit": "cell-stage updates/s", "cores": procs, "kind": "reference",
                              "sample": f"first {procs} batch members, one SHOCK process each (oracle/_ref), "
-                                       f"timed RK4 steps; {t:.1f} s"},
+                                       f"{args.steps} timed RK4 steps; {t:.1f} s"},
             "e2e": {"value": v, "unit": "cell-stage updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}))
         return
     if args.workload == "serve_poisson":
@@ -301,24 +335,19 @@ def run_reference(args, rank):
     if not ref_available(order, dim):
         print(json.dumps({"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent)"}))
         return
-    sample = CPU_SAMPLE.get(args.workload)
-    case = make_case(args.workload) if sample is None else None
-    pts = case.real_points if case is not None else sample[1]["n"] ** 3
+    spec, pts, what = ref_sample(args.workload)
     procs = ref_procs(pts, order)
-    steps = max(1, min(args.steps, args.ref_steps))
-    v, t, _ = reference_throughput(args.workload, steps, procs)
-    what = f"the {args.workload} block" if sample is None else \
-        f"a {sample[1]['n']}^3 block of the same flow and order (512^3 does not fit in host memory)"
+    v, t, _ = reference_throughput(spec, args.steps, args.warmup, procs)
     line = {
         "metric": "cell-stage updates/s", "value": v, "unit": "cell-stage updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": pts * 4 * 1e3 / v * procs, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": t * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
-                   "points": pts, "stages_per_step": 4},
+        "config": bench_config(args.workload, world),
         "cpu_baseline": {"value": v, "unit": "cell-stage updates/s", "cores": procs, "kind": "reference",
-                         "sample": f"{procs} single-block processes x {steps} timed RK4 steps (after 1 warm-up step) "
-                                   f"of {what}, SHOCK's own C code (oracle/_ref); {t:.1f} s"},
+                         "sample": f"{procs} single-block processes, each {args.warmup} warm-up and {args.steps} "
+                                   f"timed RK4 steps of {what}, SHOCK's own C code (oracle/_ref); slowest "
+                                   f"process {t:.1f} s; a step of the line = one RK4 step of every process"},
         "e2e": {"value": v, "unit": "cell-stage updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -327,16 +356,20 @@ def run_reference(args, rank):
 # ---------------------------------------------------------------------------
 # GPU arm
 # ---------------------------------------------------------------------------
+L2_CACHE_BYTES = 126 * 2 ** 20
+L2_STEPS = 50      # mixed-vs-FP64 comparison after this many steps (the 512^3 configuration's run length)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--workload", default="tgv64_w5", choices=sorted(WORKLOADS))
-    ap.add_argument("--ref-steps", type=int, default=3, help="cap on timed RK steps in the reference arm")
+    ap.add_argument("--workload", default="turb512_w9", choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--no-l2", action="store_true", help="skip the mixed-vs-FP64 L2 run")
     ap.add_argument("--tune-budget", type=float, default=60.0, help="seconds the batch autotuner may spend")
     ap.add_argument("--requests", type=int, default=48, help="serve_poisson: requests in the stream")
     ap.add_argument("--hbm-gb", type=float, default=150.0, help="serve_poisson: HBM budget")
@@ -348,7 +381,7 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
 
     if args.impl == "reference":
-        run_reference(args, rank)
+        run_reference(args, rank, world)
         return
 
     import numpy as np
@@ -375,41 +408,50 @@ def main():
 
     case = make_case(args.workload)
     stage_cells = case.real_points * case.time_order
-    flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    g2 = case.order + 1
+    state_bytes = 5 * 8 * (case.ni + g2) * (case.nj + g2) * ((case.nk + g2) if case.dim == 3 else 1)
+    # the stage streams the state and about 45 other fields: blocks whose
+    # state alone is below the L2 size get the L2 flushed between steps
+    flush = None
+    if state_bytes < 4 * L2_CACHE_BYTES:
+        flush = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device="cuda")
+    l2_steps = max(L2_STEPS, args.warmup + args.steps)
 
-    def timed_device(precision):
+    def run_form(precision, sampler=None):
+        """W warm-up steps, K timed steps (step graph with an event after every
+        launch: per-kernel device times over the timed region), then untimed
+        steps up to l2_steps; returns the solver and its figures."""
         s = shock_b200.Solver(case, precision=precision, device=local)
+        s.set_kernel_timing(True)
         for _ in range(args.warmup):
             s.steps(1)
+        s.set_kernel_timing(True)          # clear what the warm-up accumulated
         barrier()
+        if sampler:
+            sampler.start()
         total_ms = 0.0
         for _ in range(args.steps):
-            flush_l2(torch, flush)
-            torch.cuda.synchronize()
+            if flush is not None:
+                flush.zero_()
+                torch.cuda.synchronize()
             s.steps(1)
             total_ms += s.last_ms()
+        clocks = sampler.stop() if sampler else None
         barrier()
-        return s, total_ms
+        kt, ksteps = s.kernel_times()
+        s.set_kernel_timing(False)
+        rest = l2_steps - args.warmup - args.steps
+        if rest > 0 and not args.no_l2:
+            s.steps(rest)
+        return s, total_ms, kt, ksteps, clocks
 
-    sampler = ClockSampler(local)
-    sampler.start()
-    solver, ms64 = timed_device(shock_b200.SHOCK_FP64)
-    clocks = sampler.stop()
+    solver, ms64, kt64, ksteps, clocks = run_form(shock_b200.SHOCK_FP64, ClockSampler(local))
     ms64 = max_over_ranks(ms64)
     value = replica_value(stage_cells * args.steps, world, ms64 * 1e-3)
+    state64 = None if args.no_l2 else solver.state()
 
-    mixed = None
-    if not args.no_mixed:
-        try:
-            smix, msmix = timed_device(shock_b200.SHOCK_MIXED)
-            msmix = max_over_ranks(msmix)
-            mixed = {"value": stage_cells * args.steps * world / (msmix * 1e-3),
-                     "ms_per_step": msmix / args.steps}
-            del smix
-        except shock_b200.ShockError as e:
-            mixed = {"error": str(e)}
-
-    # end to end through the C ABI with pinned host buffers
+    # end to end through the C ABI with pinned host buffers: every step
+    # uploads that step's input state, runs the step and reads the result back
     n5 = 5 * solver.n
     host = torch.empty(n5, dtype=torch.float64, pin_memory=True).numpy()
     host[:] = solver.state().ravel()
@@ -424,39 +466,60 @@ def main():
     e2e_s = max_over_ranks(t1 - t0)
     e2e = {"value": stage_cells * args.steps * world / e2e_s, "unit": "cell-stage updates/s",
            "h2d_bytes_per_step": 8 * n5, "d2h_bytes_per_step": 8 * n5}
+    launches = solver.kernels_per_step() * args.steps
+    del host
+    solver.close()
 
-    # per-kernel profile of one stage and the roofline of the dominant kernel
-    prof = solver_profile(solver)
+    mixed = None
+    if not args.no_mixed:
+        try:
+            smix, msmix, ktmix, _, clocks_mix = run_form(shock_b200.SHOCK_MIXED, ClockSampler(local))
+            msmix = max_over_ranks(msmix)
+            mixed = {"value": stage_cells * args.steps * world / (msmix * 1e-3),
+                     "ms_per_step": msmix / args.steps, "speedup_vs_fp64": ms64 / msmix,
+                     "kernels_ms_per_step": {k: v[0] / args.steps for k, v in ktmix.items()},
+                     "clocks": clocks_mix}
+            if state64 is not None:
+                l2 = l2_conserved(case, smix.state(), state64)
+                mixed["l2_vs_fp64"] = {"steps": l2_steps, "rho": l2[0], "rho_u": l2[1], "rho_v": l2[2],
+                                       "rho_w": l2[3], "rho_e": l2[4],
+                                       "definition": "relative L2 over the real points of each conserved "
+                                                     "variable, mixed form against the FP64 form after the "
+                                                     "same steps from the same initial state"}
+            smix.close()
+        except shock_b200.ShockError as e:
+            mixed = {"error": str(e)}
+
+    # roofline of the dominant kernel: SHOCK's FP64 operations per launch over
+    # its average launch time in the timed region
     fl = flops_per_cell_stage(case)
     peaks = measure_peaks(local)
-    dom = max(prof, key=lambda kv: kv[1]) if prof else ("n/a", 0.0)
-    dom_flops = fl.get(dom[0], 0.0) * case.real_points
-    achieved = dom_flops / (dom[1] * 1e-3) / 1e12 if dom[1] > 0 else None
-    roofline = {"bound": "fp64", "kernel": dom[0], "achieved": achieved, "peak": peaks["fp64_tflops"],
-                "unit": "TFLOP/s", "frac": (achieved / peaks["fp64_tflops"]) if achieved else None,
-                "traffic": measured_traffic(args.workload, dom[0]),
-                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch, "
-                                  "shock_b200/roofline.json (command recorded there)",
-                "peak_source": "measured on this GPU by shock_measure_fma_peak (register-only FP64 FMA loop)",
-                "flops_per_launch": dom_flops, "launch_ms": dom[1],
-                "step_fp64_tflops": fl["total"] * stage_cells * args.steps / (ms64 * 1e-3) / 1e12,
-                "step_frac": fl["total"] * stage_cells * args.steps / (ms64 * 1e-3) / 1e12 / peaks["fp64_tflops"],
-                "kernels_ms": {k: v for k, v in prof}}
+    dom = max(kt64.items(), key=lambda kv: kv[1][0])
+    dom_name, (dom_ms_total, dom_launches) = dom
+    launch_ms = dom_ms_total / dom_launches
+    dom_flops = fl.get(dom_name, 0.0) * case.real_points
+    achieved = dom_flops / (launch_ms * 1e-3) / 1e12
+    step_tf = fl["total"] * stage_cells * args.steps / (ms64 * 1e-3) / 1e12
+    roofline = {"bound": "fp64", "kernel": dom_name, "achieved": achieved, "peak": peaks["fp64_tflops"],
+                "unit": "TFLOP/s", "frac": achieved / peaks["fp64_tflops"],
+                "traffic": measured_traffic(args.workload, dom_name, case.real_points),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one launch "
+                                  "(shock_b200/roofline.json records the capture and its scaling)",
+                "peak_source": "measured on this GPU by shock_measure_fma_peak (register-only FP64 FMA loop); "
+                               "MEASURED_PEAKS.json has HBM and bf16 figures only",
+                "frac_of_nominal_40tf": achieved / 40.0,
+                "flops_per_launch": dom_flops, "launch_ms": launch_ms, "launches_timed": dom_launches,
+                "step_fp64_tflops": step_tf, "step_frac": step_tf / peaks["fp64_tflops"],
+                "kernels_ms_per_step": {k: v[0] / args.steps for k, v in kt64.items()},
+                "kernels_sum_ms_per_step": sum(v[0] for v in kt64.values()) / args.steps,
+                "hbm": {"algorithmic_bytes_per_cell_stage": (200 if case.dim == 3 else 160),
+                        "achieved_gbs": (200 if case.dim == 3 else 160) * stage_cells * args.steps
+                        / (ms64 * 1e-3) / 1e9,
+                        "peak_gbs": measured_hbm_gbs()}}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sys.path.insert(0, os.path.join(ROOT, "oracle"))
-        from refbind import ref_available
-        if ref_available(case.order, case.dim):
-            sample = CPU_SAMPLE.get(args.workload)
-            pts = case.real_points if sample is None else sample[1]["n"] ** 3
-            procs = ref_procs(pts, case.order)
-            v, tmax, _ = reference_throughput(args.workload, 1, procs)
-            what = f"the {args.workload} block" if sample is None else \
-                f"a {sample[1]['n']}^3 block of the same flow and order (512^3 does not fit in host memory)"
-            cpu = {"value": v, "unit": "cell-stage updates/s", "cores": procs, "kind": "reference",
-                   "sample": f"{procs} single-block processes x 1 RK4 step of {what}, "
-                             f"SHOCK's own C code (oracle/_ref); {tmax:.1f} s"}
+        cpu = cpu_baseline_sample(args.workload, case)
 
     if rank == 0:
         line = {
@@ -464,11 +527,8 @@ def main():
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms64 / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": args.workload, "description": WORKLOADS[args.workload],
-                       "points": case.real_points, "stages_per_step": case.time_order,
-                       "l2": "flushed (256 MiB write) between timed steps",
-                       "parallelism": f"replicas x{world}"},
-            "mixed": mixed, "e2e": e2e, "gpu_launches": solver.kernels_per_step() * args.steps,
+            "config": bench_config(args.workload, world),
+            "mixed": mixed, "e2e": e2e, "gpu_launches": launches,
             "roofline": roofline, "cpu_baseline": cpu, "clocks": clocks,
             "fp32_peak_tflops": peaks["fp32_tflops"],
         }
@@ -477,19 +537,67 @@ def main():
         dist.destroy_process_group()
 
 
-def _l2_conserved(case, a, r):
-    """Relative L2 of each conserved variable (real points) between two states."""
+def bench_config(workload, world):
+    """The config object of both arms' lines (same keys, same values)."""
+    from shock_b200 import cases as _c  # noqa: F401
+    info = WORKLOAD_INFO.get(workload, {})
+    cfg = {"workload": workload, "description": WORKLOADS[workload], "parallelism": f"replicas x{world}"}
+    cfg.update(info)
+    return cfg
+
+
+# points, stages per step and the L2 treatment of each single-block workload
+WORKLOAD_INFO = {
+    "tgv64_w5": {"points": 64 ** 3, "stages_per_step": 4, "l2": "flushed (256 MiB write) between timed steps"},
+    "tgv128_w5": {"points": 128 ** 3, "stages_per_step": 4, "l2": "flushed (256 MiB write) between timed steps"},
+    "turb128_w9": {"points": 128 ** 3, "stages_per_step": 4, "l2": "inputs (state 0.9 GB) larger than L2"},
+    "turb256_w9": {"points": 256 ** 3, "stages_per_step": 4, "l2": "inputs (state 6.4 GB) larger than L2"},
+    "turb512_w9": {"points": 512 ** 3, "stages_per_step": 4, "l2": "inputs (state 5.7 GB, 58 GB in all) larger than L2"},
+    "tgv512_w5": {"points": 512 ** 3, "stages_per_step": 4, "l2": "inputs (state 5.5 GB, 56 GB in all) larger than L2"},
+    "mms64_w5": {"points": 64 ** 2, "stages_per_step": 4, "l2": "flushed (256 MiB write) between timed steps"},
+}
+
+
+def measured_hbm_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f).get("hbm_gbs")
+    except (OSError, ValueError):
+        return None
+
+
+def cpu_baseline_sample(workload, case):
+    """SHOCK's own CPU code (oracle/_ref) on a bounded sample of the workload:
+    one single-block process per host core, a few RK4 steps each."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from refbind import ref_available
+    if not ref_available(case.order, case.dim):
+        return None
+    spec, pts, what = ref_sample(workload)
+    procs = ref_procs(pts, case.order)
+    v, tmax, _ = reference_throughput(spec, CPU_BASELINE_STEPS, 1, procs)
+    return {"value": v, "unit": "cell-stage updates/s", "cores": procs, "kind": "reference",
+            "sample": f"{procs} single-block processes x {CPU_BASELINE_STEPS} timed RK4 steps (after 1 warm-up "
+                      f"step) of {what}, SHOCK's own C code (oracle/_ref); {tmax:.1f} s"}
+
+
+CPU_BASELINE_STEPS = 3
+
+
+def l2_conserved(case, a, r):
+    """Relative L2 of each conserved variable (rho, rho u, rho v, rho w, rho e)
+    over the real points between two states of SHOCK's variables; one
+    variable at a time, so a 512^3 block needs little extra host memory."""
     import numpy as np
     g = case.ghosts
-    sl = (slice(None), slice(g, g + case.ni), slice(g, g + case.nj),
-          slice(g, g + case.nk) if case.dim == 3 else slice(None))
-    a, r = a[sl], r[sl]
-    ca = np.stack([a[0], a[0] * a[1], a[0] * a[2], a[0] * a[3], a[0] * a[4]])
-    cr = np.stack([r[0], r[0] * r[1], r[0] * r[2], r[0] * r[3], r[0] * r[4]])
+    sl = (slice(g, g + case.ni), slice(g, g + case.nj), slice(g, g + case.nk) if case.dim == 3 else slice(None))
+    ra, rr = a[0][sl], r[0][sl]
     out = np.zeros(5)
     for k in range(5):
-        den = np.sqrt(np.mean(cr[k] ** 2))
-        num = np.sqrt(np.mean((ca[k] - cr[k]) ** 2))
+        ca = ra if k == 0 else ra * a[k][sl]
+        cr = rr if k == 0 else rr * r[k][sl]
+        den = float(np.sqrt(np.mean(np.square(cr))))
+        num = float(np.sqrt(np.mean(np.square(ca - cr))))
         out[k] = 0.0 if den == 0 and num == 0 else num / (den or 1.0)
     return out
 
@@ -535,7 +643,7 @@ def run_batch(args, world, rank, local, barrier, max_over_ranks):
         b.close()
     worst = np.zeros(5)
     for c, sm, s64 in zip(cs, out[shock_b200.SHOCK_MIXED]["states"], out[shock_b200.SHOCK_FP64]["states"]):
-        worst = np.maximum(worst, _l2_conserved(c, sm, s64))
+        worst = np.maximum(worst, l2_conserved(c, sm, s64))
     # the persistent form (one cooperative launch per RK stage) beside the
     # tuner's choice, mixed precision
     bp = shock_b200.Batch(2, 5, shock_b200.SHOCK_MIXED, arena_bytes=arena, device=local)
@@ -585,7 +693,7 @@ def run_batch(args, world, rank, local, barrier, max_over_ranks):
         from refbind import ref_available
         if ref_available(5, 2):
             procs = ref_procs(256 ** 2, 5)
-            v, t = batch_reference_sample(procs, steps=1)
+            v, t = batch_reference_sample(procs, steps=1, warmup=1)
             cpu = {"value": v, "unit": "cell-stage updates/s", "cores": procs, "kind": "reference",
                    "sample": f"first {procs} batch members, one SHOCK process each (oracle/_ref), 1 timed RK4 step; "
                              f"{t:.1f} s"}
@@ -671,23 +779,6 @@ def run_serve(args, world, rank, local, barrier, max_over_ranks):
             "e2e": {"value": f64["throughput"] * world, "unit": "cell-stage updates/s",
                     "note": "requests enter as host arrays and results return to host memory"},
         }))
-
-
-def solver_profile(solver):
-    import ctypes as C
-    L = solver.lib
-    names = C.create_string_buffer(48 * 32)
-    ms = (C.c_float * 32)()
-    cnt = C.c_int()
-    best = {}
-    for _ in range(5):
-        rc = L.shock_profile_stage(solver.h, 32, names, ms, C.byref(cnt))
-        if rc != 0:
-            return []
-        for i in range(cnt.value):
-            nm = names.raw[48 * i:48 * i + 48].split(b"\0")[0].decode()
-            best[nm] = min(best.get(nm, 1e30), ms[i])
-    return list(best.items())
 
 
 def measure_peaks(device):

@@ -85,6 +85,10 @@ typedef struct shock_params {
     double u_inflow[3];           /* cos/sin(AoA) * [InitializeValues] u0, 0 (src/Import.c:233-235): the inflow
                                      velocity, and the velocity SHOCK's Initialize gives every ghost point
                                      before the first fill (src/Functions.c:1327-1353) */
+    double weno_eps;    /* epsilon of the WENO weights 1/(IS + eps)^2: 0 gives SHOCK's 10*sqrt(DBL_MIN)
+                           (10*sqrt(FLT_MIN) in the FP32 stencils; src/Functions.c:1829, "reference
+                           mode"); > 0 sets it ("clean mode", e.g. the 1e-6 src/Functions.c:1818,1825
+                           leaves commented out, which restores the design order at smooth extrema) */
 } shock_params;
 
 typedef struct shock_ctx shock_ctx;
@@ -170,6 +174,15 @@ int shock_step(shock_ctx *ctx, int nsteps);
 int shock_step_async(shock_ctx *ctx, int nsteps);
 int shock_sync(shock_ctx *ctx);
 
+/* The time step used by the following steps: SHOCK changes numericalTau
+ * inside its time loop (x TauDecelerator_factor after a NaN reset,
+ * src/SHOCK.c:590; back to numericalTauStart, :638; x TauAccelerator_factor,
+ * :654), and CalcRungeKutta and the Rudy outflow fill (src/BC.c:2643-2646)
+ * read it every step.  Waits for queued steps; the step graphs are captured
+ * again on the next step when tau changes. */
+int shock_set_tau(shock_ctx *ctx, double tau);
+int shock_get_tau(const shock_ctx *ctx, double *tau);
+
 /* NaN/Inf scan of rho over the real points (src/Functions.c:5419-5467);
  * *bad receives the count.  Returns SHOCK_ENAN when bad > 0. */
 int shock_check_nan(shock_ctx *ctx, int *bad);
@@ -194,11 +207,21 @@ int shock_last_step_ms(shock_ctx *ctx, float *ms);
 /* Number of kernel launches in one captured time step. */
 int shock_kernels_per_step(const shock_ctx *ctx, int *n);
 
-/* Time every kernel of one stage right-hand side plus the RK update
- * separately (CUDA events between launches, outside any graph).  names
- * receives up to max entries of 48 characters each, ms the times in
- * milliseconds; *count the number of kernels. */
-int shock_profile_stage(shock_ctx *ctx, int max, char *names, float *ms, int *count);
+/* Per-kernel device time inside the captured step graph.  on = 1 captures
+ * the step graphs again with an event record after every launch and
+ * starts accumulating; each shock_step / shock_step_async step then waits
+ * for its graph and charges the time between consecutive events to the
+ * launch before it, so the per-kernel times of a step add up to that
+ * step's graph time.  on = 0 returns to the plain graphs.  Accumulators
+ * are cleared by every shock_set_kernel_timing call. */
+int shock_set_kernel_timing(shock_ctx *ctx, int on);
+/* Accumulated times since timing was switched on: names receives up to max
+ * entries of 48 characters ("qsum_clear", "ghosts", "prim", "bc", "nodal",
+ * "weno_xi".."weno_zeta", "visc_xi".."visc_zeta", "rk", "bc_save"), ms the
+ * total milliseconds, launches the number of launches timed under each
+ * name, *count the number of names and *steps the number of steps timed. */
+int shock_kernel_times(const shock_ctx *ctx, int max, char *names, double *ms, long long *launches, int *count,
+                       long long *steps);
 
 /* FP64 and FP32 fused multiply-add throughput of a device in TFLOP/s,
  * measured with a register-only FMA loop (roofline denominators). */
@@ -297,7 +320,7 @@ typedef struct shock_server_stats {
     double busy_ms;          /* device time of all rounds */
     size_t arena_used, arena_total;
     double uptime_s;
-    int loop_error;
+    int loop_error;          /* the last error a round met (the requests of that class failed with it), or 0 */
 } shock_server_stats;
 
 int shock_server_create(const shock_server_config *cfg, shock_server **out);
@@ -345,10 +368,11 @@ int shock_server_destroy(shock_server *s);
  *           there and the call returns without waiting.
  *
  * The intermediate fields (p, T, c, mu, 12 nodal derivatives) live in one
- * fixed 64 MiB array per device inside the library.  The first call on a
- * device sets up that device (finds the array's address and raises the
- * kernels' shared-memory limits), so make one call on each device before
- * any stream capture.  The array is shared by all calls on a device and
+ * fixed 64 MiB array per device inside the library.  Every call looks up
+ * that array's device address (a host-side lookup); the first call on a
+ * device, and the first after a cudaDeviceReset, also raises the kernels'
+ * shared-memory limits, so make one call on each device before any stream
+ * capture.  The array is shared by all calls on a device and
  * keeps what the last call left in it: calls that may overlap in time (on
  * different streams, or from different host threads) race and give wrong
  * results; serialise them, e.g. on one stream.  Part of the array is

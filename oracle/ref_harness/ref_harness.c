@@ -354,6 +354,76 @@ void ref_free(void)
     live = 0;
 }
 
+/*
+ * The control around the step in startSimulation's time loop
+ * (SHOCK.c:557-663), reduced to what decides the state: after each step the
+ * NaN check; on a NaN, tau *= decel and U_RK is reloaded from the last
+ * backup, whose iteration the loop resumes from (SHOCK.c:576-622); else,
+ * every accel_every iterations, tau *= accel (the accelerator,
+ * SHOCK.c:642-657); U_RK -> U_lastStep; every backup_every iterations
+ * U_lastStep -> backup.  At iteration nan_at (once) a NaN density is
+ * planted in U_RK on the host, standing in for a blown-up step.  The ops
+ * are SHOCK's own calls or the drop-in binding's, so the two runs differ
+ * only in where the steps run.
+ */
+typedef struct {
+    void (*step)(void);
+    int (*nan)(void);
+    void (*sync)(void);     /* device -> host U_RK (drop-in only) */
+    void (*upload)(void);   /* host U_RK -> device (drop-in only) */
+} loop_ops;
+
+static int control_loop(int nsteps, int nan_at, double decel, int accel_every, double accel, int backup_every,
+                        const loop_ops *ops)
+{
+    int it = 0, backup_it = 0, resets = 0, planted = 0;
+    WriteValuesFromU1ToU2(&cfg, &U_last, &U_b1);
+    while (it < nsteps) {
+        it++;
+        ops->step();
+        if (it == nan_at && !planted) {
+            ops->sync();
+            U_rk.rho[(size_t)cfg.int_iStartReal * cfg.int_jMeshPointsGhostCells * cfg.int_kMeshPointsGhostCells
+                     + (size_t)cfg.int_jStartReal * cfg.int_kMeshPointsGhostCells + cfg.int_kStartReal] = NAN;
+            ops->upload();
+            planted = 1;
+        }
+        if (ops->nan()) {
+            cfg.numericalTau *= decel;
+            WriteValuesFromU1ToU2(&cfg, &U_b1, &U_rk);
+            ops->upload();
+            it = backup_it;
+            resets++;
+        } else if (accel_every > 0 && it % accel_every == 0) {
+            cfg.numericalTau *= accel;
+        }
+        WriteValuesFromU1ToU2(&cfg, &U_rk, &U_last);
+        if (backup_every > 0 && it % backup_every == 0) {
+            ops->sync();
+            WriteValuesFromU1ToU2(&cfg, &U_rk, &U_last);
+            WriteValuesFromU1ToU2(&cfg, &U_last, &U_b1);
+            backup_it = it;
+        }
+    }
+    ops->sync();
+    WriteValuesFromU1ToU2(&cfg, &U_rk, &U_last);
+    return resets;
+}
+
+static void cpu_step(void) { CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh); }
+static int cpu_nan(void) { return checkNAN(&cfg, &U_rk, &msh); }
+static void nothing(void) {}
+
+/* The loop above with SHOCK's own CalcRungeKutta and checkNAN; returns the
+ * number of NaN resets. */
+int ref_control_loop(int nsteps, int nan_at, double decel, int accel_every, double accel, int backup_every)
+{
+    const loop_ops ops = {cpu_step, cpu_nan, nothing, nothing};
+    return control_loop(nsteps, nan_at, decel, accel_every, accel, backup_every, &ops);
+}
+
+double ref_tau(void) { return (double)cfg.numericalTau; }
+
 #ifdef SHOCK_DROPIN
 /*
  * The drop-in path (shock_b200/dropin/GPU.c): SHOCK's own set-up (ref_init
@@ -420,6 +490,19 @@ void ref_dropin_steps(int n)
 }
 
 void ref_dropin_sync(void) { GPU_SyncHost(&cfg, &U_rk); }
+
+static void gpu_step(void) { GPU_CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh); }
+static int gpu_nan(void) { return GPU_CheckNAN(&cfg, &U_rk, &msh); }
+static void gpu_upload(void) { GPU_UploadState(&cfg, &U_rk); }
+
+/* The control loop with the binding: GPU_CalcRungeKutta, GPU_CheckNAN,
+ * GPU_SyncHost before the host reads U_RK, GPU_UploadState after it writes
+ * U_RK. */
+int ref_dropin_control_loop(int nsteps, int nan_at, double decel, int accel_every, double accel, int backup_every)
+{
+    const loop_ops ops = {gpu_step, gpu_nan, ref_dropin_sync, gpu_upload};
+    return control_loop(nsteps, nan_at, decel, accel_every, accel, backup_every, &ops);
+}
 
 void ref_dropin_destroy(void)
 {

@@ -120,6 +120,22 @@ class RefSolver:
     def time_steps(self, n: int) -> float:
         return self.lib.ref_time_steps(C.c_int(n))
 
+    def control_loop(self, nsteps, nan_at=0, decel=0.7, accel_every=0, accel=1.1, backup_every=5) -> int:
+        """startSimulation's control around the step (ref_harness.c
+        control_loop): NaN check and reset from the last backup with
+        tau *= decel, tau *= accel every accel_every iterations, a NaN
+        planted at iteration nan_at.  Returns the number of resets."""
+        f = getattr(self.lib, self._loop_fn)
+        f.restype = C.c_int
+        f.argtypes = [C.c_int, C.c_int, C.c_double, C.c_int, C.c_double, C.c_int]
+        return f(nsteps, nan_at, decel, accel_every, accel, backup_every)
+
+    _loop_fn = "ref_control_loop"
+
+    def tau(self) -> float:
+        self.lib.ref_tau.restype = C.c_double
+        return self.lib.ref_tau()
+
     def state(self, which: int = 0) -> np.ndarray:
         """rho,u,v,w,e,p,T,c,mue of U_RK (0) or U_lastStep (1)."""
         s = np.zeros(9 * self.n)
@@ -168,6 +184,8 @@ class DropinSolver(RefSolver):
     CalcRungeKutta, GPU_SyncHost before the host reads U_RK
     (oracle/_ref/libshockdropin_*.so, linked with libshock_b200.so)."""
 
+    _loop_fn = "ref_dropin_control_loop"
+
     def __init__(self, case, device: int = 0):
         super().__init__(case, _lib="libshockdropin")
         rc = self.lib.ref_dropin_create(C.c_int(device))
@@ -211,6 +229,7 @@ def _oracle_lib():
         for name in ("oc_dims", "oc_set_dirichlet", "oc_set_source", "oc_set_state",
                      "oc_get_state", "oc_get_geom", "oc_rhs", "oc_steps", "oc_free"):
             getattr(lib, name).argtypes = None
+        lib.oc_set_weno_eps.argtypes = [C.c_void_p, C.c_double]
         _oclib = lib
     return _oclib
 
@@ -218,7 +237,7 @@ def _oracle_lib():
 class Oracle:
     """The CPU restatement, same calling convention as RefSolver."""
 
-    def __init__(self, case, dirichlet9=None, source5=None):
+    def __init__(self, case, dirichlet9=None, source5=None, weno_eps=0.0):
         if any(getattr(case, "bc", (0,) * 6)):
             raise ValueError("the CPU restatement covers periodic and manufactured-solution faces only")
         lib = self.lib = _oracle_lib()
@@ -247,6 +266,8 @@ class Oracle:
         if source5 is not None:
             a = np.ascontiguousarray(source5, np.float64).ravel()
             lib.oc_set_source(self.h, _ptr(a))
+        if weno_eps > 0:
+            lib.oc_set_weno_eps(self.h, C.c_double(weno_eps))
 
     def __del__(self):
         try:

@@ -780,6 +780,8 @@ static void rk_update(oc_solver *s, int st)
             }
 }
 
+void oc_set_weno_eps(oc_solver *s, double eps) { s->eps = eps; }
+
 void oc_steps(oc_solver *s, int n)
 {
     for (int it = 0; it < n; it++) {

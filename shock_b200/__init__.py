@@ -69,7 +69,7 @@ class Params(C.Structure):
         ("precision", C.c_int), ("zeta_fix", C.c_int),
         ("bc", C.c_int * 6), ("t_wall", C.c_double),
         ("rho_inflow", C.c_double), ("p_inflow", C.c_double), ("p_outflow", C.c_double),
-        ("u_inflow", C.c_double * 3),
+        ("u_inflow", C.c_double * 3), ("weno_eps", C.c_double),
     ]
 
 
@@ -103,7 +103,8 @@ def lib():
                          "shock_step",
                          "shock_step_async", "shock_sync", "shock_check_nan", "shock_geometry",
                          "shock_device_bytes", "shock_last_step_ms", "shock_kernels_per_step",
-                         "shock_mms_baseline", "shock_profile_stage", "shock_measure_fma_peak",
+                         "shock_mms_baseline", "shock_set_kernel_timing", "shock_kernel_times", "shock_measure_fma_peak",
+                         "shock_set_tau", "shock_get_tau",
                          "shock_host_geometry", "shock_host_mms_baseline", "shock_rhs_static",
                          "shock_batch_create", "shock_batch_destroy", "shock_batch_member_bytes",
                          "shock_batch_add", "shock_batch_remove", "shock_batch_step", "shock_batch_step_async",
@@ -136,7 +137,7 @@ def _ptr(a):
     return a.ctypes.data_as(_dp)
 
 
-def params_from_case(case, precision=SHOCK_FP64, zeta_fix=False) -> Params:
+def params_from_case(case, precision=SHOCK_FP64, zeta_fix=False, weno_eps=0.0) -> Params:
     p = Params()
     p.dim, p.order = case.dim, case.order
     p.ni, p.nj, p.nk = case.ni, case.nj, (case.nk if case.dim == 3 else 1)
@@ -156,6 +157,7 @@ def params_from_case(case, precision=SHOCK_FP64, zeta_fix=False) -> Params:
     p.rho_inflow, p.p_inflow, p.p_outflow = float(case.rho_inflow), float(case.p_inflow), float(case.p_outflow)
     for a in range(3):
         p.u_inflow[a] = float(case.u_inflow[a])
+    p.weno_eps = float(weno_eps)
     return p
 
 
@@ -194,10 +196,10 @@ class Solver:
     """One block of SHOCK's stage right-hand side on a CUDA device."""
 
     def __init__(self, case, precision=SHOCK_FP64, device: int = 0, zeta_fix: bool = False,
-                 dirichlet9=None, source5=None):
+                 dirichlet9=None, source5=None, weno_eps: float = 0.0):
         self.case = case
         self.lib = lib()
-        self.params = params_from_case(case, precision, zeta_fix)
+        self.params = params_from_case(case, precision, zeta_fix, weno_eps)
         f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
         arrs = [f(a) for a in case.real_fields()]
         h = C.c_void_p()
@@ -244,6 +246,15 @@ class Solver:
 
     def steps(self, n: int):
         _check(self.lib.shock_step(self.h, C.c_int(n)))
+
+    def set_tau(self, tau: float):
+        """The time step of the following steps (SHOCK's numericalTau)."""
+        _check(self.lib.shock_set_tau(self.h, C.c_double(tau)))
+
+    def tau(self) -> float:
+        t = C.c_double()
+        _check(self.lib.shock_get_tau(self.h, C.byref(t)))
+        return t.value
 
     def steps_async(self, n: int):
         _check(self.lib.shock_step_async(self.h, C.c_int(n)))
@@ -305,6 +316,24 @@ class Solver:
         n = C.c_int()
         _check(self.lib.shock_kernels_per_step(self.h, C.byref(n)))
         return n.value
+
+    def set_kernel_timing(self, on: bool = True):
+        """Time every launch inside the step graph (event nodes between
+        launches) from now on; clears the accumulated times."""
+        _check(self.lib.shock_set_kernel_timing(self.h, int(bool(on))))
+
+    def kernel_times(self):
+        """({name: (total ms, launches)}, steps timed) since timing was switched on."""
+        names = C.create_string_buffer(48 * 64)
+        ms = (C.c_double * 64)()
+        nl = (C.c_longlong * 64)()
+        cnt, steps = C.c_int(), C.c_longlong()
+        _check(self.lib.shock_kernel_times(self.h, 64, names, ms, nl, C.byref(cnt), C.byref(steps)))
+        out = {}
+        for i in range(cnt.value):
+            nm = names.raw[48 * i:48 * i + 48].split(b"\0")[0].decode()
+            out[nm] = (ms[i], nl[i])
+        return out, steps.value
 
     def real(self, a: np.ndarray) -> np.ndarray:
         """Real-point view of a ghosted field array (..., NIg, NJg, NKg)."""

@@ -79,6 +79,15 @@ struct shock_ctx {
     float last_ms = 0.f;
     int kernels_per_step = 0;
     std::vector<std::vector<double>> geo_host;
+    // kernel timing inside the step graph (shock_set_kernel_timing): an event
+    // record node after every launch, the time between consecutive events
+    // charged to the launch before it
+    bool timing = false;
+    std::vector<cudaEvent_t> tev;
+    std::vector<std::string> tname;
+    int tmark = 0;
+    std::vector<std::pair<std::string, std::pair<double, long long>>> tacc;   // name -> (ms, launches)
+    long long tsteps = 0;
 };
 
 namespace shock {
@@ -110,6 +119,10 @@ Phys make_phys(const shock_params &p)
     P.gam = 1.0 / ((p.gamma - 1.0) * (p.mach * p.mach) * p.reynolds * p.prandtl);
     P.eps64 = 10. * sqrt(2.2250738585072014e-308);   // 10*sqrt(DBL_MIN), src/Functions.c:1829
     P.eps32 = 10.f * sqrtf(1.17549435e-38f);          // 10*sqrt(FLT_MIN), the float build's value
+    if (p.weno_eps > 0) {                              // clean mode (src/Functions.c:1818,1825)
+        P.eps64 = p.weno_eps;
+        P.eps32 = (float)p.weno_eps;
+    }
     P.mms = p.mms ? 1 : 0;
     P.zeta_fix = p.zeta_fix;
     // BC_Corrector_*Momentum of the ghost points (reset to 1 at set-up,
@@ -143,28 +156,52 @@ Phys make_phys(const shock_params &p)
 
 static void set_rk(shock_ctx *c) { rk_coefficients(c->p.time_order, c->rk); }
 
+constexpr int kMaxMarks = 128;   // event marks per time step (about 14 per stage)
+
+// End of a timed interval: everything queued since the previous mark is
+// charged to `name`.  A no-op unless kernel timing is on.
+static void mark(shock_ctx *c, const char *name)
+{
+    if (!c->timing || c->tmark >= kMaxMarks) return;
+    cudaEventRecord(c->tev[c->tmark], c->stream);
+    c->tname[c->tmark] = name;
+    c->tmark++;
+}
+
 // Launch the right-hand side of one stage on state `in`.
 static void enqueue_rhs(shock_ctx *c, double *const in[5], int &nk)
 {
     cudaStream_t s = c->stream;
     const double *cin[5] = {in[0], in[1], in[2], in[3], in[4]};
-    launch_ghosts(c->G, in, s);
-    nk += (c->G.periodic[0] || c->G.periodic[1] || c->G.periodic[2]) ? 1 : 0;
+    static const char *wn[3] = {"weno_xi", "weno_eta", "weno_zeta"};
+    static const char *vn[3] = {"visc_xi", "visc_eta", "visc_zeta"};
+    if (c->G.periodic[0] || c->G.periodic[1] || c->G.periodic[2]) {
+        launch_ghosts(c->G, in, s);
+        nk++;
+        mark(c, "ghosts");
+    }
     launch_prim(c->G, c->P, cin, c->F, s);
     nk++;
-    if (c->P.walls) nk += launch_bc(c->G, c->P, cin, c->buf, c->F, c->plast, false, s);
+    mark(c, "prim");
+    if (c->P.walls) {
+        nk += launch_bc(c->G, c->P, cin, c->buf, c->F, c->plast, false, s);
+        mark(c, "bc");
+    }
     if (!c->p.inviscid) {
         launch_nodal(c->G, c->p.precision, cin, c->F, s);
         nk++;
+        mark(c, "nodal");
     }
     for (int d = 0; d < c->p.dim; d++) {
         launch_weno(c->G, c->P, c->p.precision, d, d == 0, cin, c->F, s);
         nk++;
+        mark(c, wn[d]);
     }
     if (!c->p.inviscid)
         for (int d = 0; d < c->p.dim; d++) {
             launch_viscous(c->G, c->P, c->p.precision, d, cin, c->F, s);
             nk++;
+            mark(c, vn[d]);
         }
 }
 
@@ -180,12 +217,14 @@ static void enqueue_step(shock_ctx *c, int un, int &nk)
         for (int q = 0; q < 5; q++) F.Un[q] = c->buf[un][q];
         launch_rk(c->G, c->rk[st], c->p.tau, cin, c->buf[out], F, c->has_source, c->stream);
         nk++;
+        mark(c, "rk");
         cur = out;
     }
     // end of the step: U_RK's p becomes U_lastStep's (src/SHOCK.c:661-664)
     if (c->plast_pool) {
         launch_bc_save(c->G, c->F.p, c->plast, c->stream);
         nk++;
+        mark(c, "bc_save");
     }
 }
 
@@ -282,6 +321,7 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
         return fail(SHOCK_EINVAL, "zeta viscous stencil centred on j needs nj <= nk (src/ZD.c:547-548)");
     if (int rc = check_faces(p)) return rc;
     if (p->mach <= 0 || p->reynolds <= 0 || p->gamma <= 1.0 || p->tau <= 0) return fail(SHOCK_EINVAL, "bad physics");
+    if (!(p->weno_eps >= 0)) return fail(SHOCK_EINVAL, "weno_eps must be >= 0");
 
     shock_ctx *c = new shock_ctx();
     c->p = *p;
@@ -390,6 +430,7 @@ int shock_destroy(shock_ctx *c)
     if (c->plast_pool) cudaFree(c->plast_pool);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    for (auto e : c->tev) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return SHOCK_OK;
@@ -533,7 +574,10 @@ int shock_rhs(shock_ctx *c, double *q5)
     if (!c || !q5) return fail(SHOCK_EINVAL, "null argument");
     CK(cudaSetDevice(c->device));
     int nk = 0;
+    const bool timing = c->timing;   // kernel timing covers the step graphs only
+    c->timing = false;
     enqueue_rhs(c, c->buf[c->un], nk);
+    c->timing = timing;
     if (c->has_source) launch_add_source(c->G, c->F, c->stream);
     CK(cudaGetLastError());
     size_t nb = sizeof(double) * c->G.NG;
@@ -554,7 +598,10 @@ int shock_step_async(shock_ctx *c, int nsteps)
             cudaGraph_t gr;
             CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
             int nk = 0;
+            c->tmark = 0;
+            mark(c, "start");
             for (int q = 0; q < 5; q++) CK(cudaMemsetAsync(c->F.Qs[q], 0, sizeof(double) * c->G.NG, c->stream));
+            mark(c, "qsum_clear");
             enqueue_step(c, un, nk);
             CK(cudaStreamEndCapture(c->stream, &gr));
             CK(cudaGraphInstantiate(&c->step_graph[un], gr, 0));
@@ -564,6 +611,24 @@ int shock_step_async(shock_ctx *c, int nsteps)
         CK(cudaGraphLaunch(c->step_graph[un], c->stream));
         c->last_in = last_stage_input(c, un);
         c->un = final_buffer(c, un);
+        if (c->timing) {
+            // the graph's event nodes are rewritten by its next replay: read
+            // them now
+            CK(cudaStreamSynchronize(c->stream));
+            for (int i = 1; i < c->tmark; i++) {
+                float ms = 0.f;
+                CK(cudaEventElapsedTime(&ms, c->tev[i - 1], c->tev[i]));
+                auto it = c->tacc.begin();
+                while (it != c->tacc.end() && it->first != c->tname[i]) ++it;
+                if (it == c->tacc.end()) {
+                    c->tacc.push_back({c->tname[i], {0.0, 0}});
+                    it = c->tacc.end() - 1;
+                }
+                it->second.first += ms;
+                it->second.second += 1;
+            }
+            c->tsteps++;
+        }
     }
     CK(cudaEventRecord(c->ev1, c->stream));
     return SHOCK_OK;
@@ -584,6 +649,29 @@ int shock_step(shock_ctx *c, int nsteps)
     int rc = shock_step_async(c, nsteps);
     if (rc) return rc;
     return shock_sync(c);
+}
+
+int shock_set_tau(shock_ctx *c, double tau)
+{
+    if (!c) return fail(SHOCK_EINVAL, "null argument");
+    if (!(tau > 0) || !std::isfinite(tau)) return fail(SHOCK_EINVAL, "tau must be positive and finite");
+    if (tau == c->p.tau) return SHOCK_OK;
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    c->p.tau = tau;
+    c->P.tau = tau;   // Rudy outflow relaxes its ghost pressure over tau (src/BC.c:2643-2646)
+    // tau is a kernel argument of the RK update and the boundary fill: the
+    // step graphs are captured again on the next step
+    for (int i = 0; i < 3; i++)
+        if (c->step_graph[i]) { cudaGraphExecDestroy(c->step_graph[i]); c->step_graph[i] = nullptr; }
+    return SHOCK_OK;
+}
+
+int shock_get_tau(const shock_ctx *c, double *tau)
+{
+    if (!c || !tau) return fail(SHOCK_EINVAL, "null argument");
+    *tau = c->p.tau;
+    return SHOCK_OK;
 }
 
 int shock_check_nan(shock_ctx *c, int *bad)
@@ -645,57 +733,38 @@ int shock_kernels_per_step(const shock_ctx *c, int *n)
     return SHOCK_OK;
 }
 
-int shock_profile_stage(shock_ctx *c, int max, char *names, float *ms, int *count)
+int shock_set_kernel_timing(shock_ctx *c, int on)
 {
-    if (!c || !names || !ms || !count) return fail(SHOCK_EINVAL, "null argument");
+    if (!c) return fail(SHOCK_EINVAL, "null argument");
     CK(cudaSetDevice(c->device));
-    std::vector<cudaEvent_t> ev;
-    std::vector<std::string> nm;
-    auto mark = [&](const char *name) {
-        cudaEvent_t e;
-        cudaEventCreate(&e);
-        cudaEventRecord(e, c->stream);
-        ev.push_back(e);
-        if (name) nm.push_back(name);
-    };
-    double *const *in = c->buf[c->un];
-    const double *cin[5] = {in[0], in[1], in[2], in[3], in[4]};
-    static const char *dn[3] = {"xi", "eta", "zeta"};
-    mark(nullptr);
-    launch_ghosts(c->G, in, c->stream); mark("ghosts");
-    launch_prim(c->G, c->P, cin, c->F, c->stream); mark("prim");
-    // (the wall fill is left out: it writes the ghost layers of every state buffer)
-    if (!c->p.inviscid) { launch_nodal(c->G, c->p.precision, cin, c->F, c->stream); mark("nodal"); }
-    for (int d = 0; d < c->p.dim; d++) {
-        launch_weno(c->G, c->P, c->p.precision, d, d == 0, cin, c->F, c->stream);
-        nm.push_back(std::string("weno_") + dn[d]);
-        cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, c->stream); ev.push_back(e);
-    }
-    if (!c->p.inviscid)
-        for (int d = 0; d < c->p.dim; d++) {
-            launch_viscous(c->G, c->P, c->p.precision, d, cin, c->F, c->stream);
-            nm.push_back(std::string("visc_") + dn[d]);
-            cudaEvent_t e; cudaEventCreate(&e); cudaEventRecord(e, c->stream); ev.push_back(e);
-        }
-    // RK update into a scratch buffer (the running state is left untouched)
-    int out = (c->un + 1) % 3;
-    Fields F = c->F;
-    for (int q = 0; q < 5; q++) F.Un[q] = c->buf[c->un][q];
-    launch_rk(c->G, c->rk[0], c->p.tau, cin, c->buf[out], F, c->has_source, c->stream); mark("rk");
     CK(cudaStreamSynchronize(c->stream));
-    CK(cudaGetLastError());
-    int n = (int)nm.size();
-    for (int i = 0; i < n && i < max; i++) {
-        float t = 0;
-        cudaEventElapsedTime(&t, ev[i], ev[i + 1]);
-        ms[i] = t;
-        strncpy(names + 48 * i, nm[i].c_str(), 47);
+    if (on && c->tev.empty()) {
+        c->tev.resize(kMaxMarks);
+        c->tname.resize(kMaxMarks);
+        for (auto &e : c->tev) CK(cudaEventCreate(&e));
+    }
+    // the step graphs are captured again, with or without the event nodes
+    for (int i = 0; i < 3; i++)
+        if (c->step_graph[i]) { cudaGraphExecDestroy(c->step_graph[i]); c->step_graph[i] = nullptr; }
+    c->timing = on != 0;
+    c->tacc.clear();
+    c->tsteps = 0;
+    return SHOCK_OK;
+}
+
+int shock_kernel_times(const shock_ctx *c, int max, char *names, double *ms, long long *launches, int *count,
+                       long long *steps)
+{
+    if (!c || !names || !ms || !launches || !count || !steps) return fail(SHOCK_EINVAL, "null argument");
+    const int n = (int)c->tacc.size() < max ? (int)c->tacc.size() : max;
+    for (int i = 0; i < n; i++) {
+        strncpy(names + 48 * i, c->tacc[i].first.c_str(), 47);
         names[48 * i + 47] = 0;
+        ms[i] = c->tacc[i].second.first;
+        launches[i] = c->tacc[i].second.second;
     }
-    for (auto e : ev) cudaEventDestroy(e);
-    for (int q = 0; q < 5; q++) CK(cudaMemsetAsync(c->F.Qs[q], 0, sizeof(double) * c->G.NG, c->stream));
-    CK(cudaStreamSynchronize(c->stream));
-    *count = n < max ? n : max;
+    *count = n;
+    *steps = c->tsteps;
     return SHOCK_OK;
 }
 

@@ -198,6 +198,7 @@ void launch_add_source(const Grid &G, const Fields &F, cudaStream_t s);
 void launch_post(const Grid &G, double mach, const double *const fin[5], const double *const lst[5],
                  const double *p, const Fields &F, double *ma, double *gr, double *l2, cudaStream_t s);
 void prepare_kernels();
+bool kernels_prepared();   // the current context has the limits prepare_kernels sets
 int report_error(int code, const char *fmt, ...);   // sets shock_last_error, returns code
 double fma_probe(int fp64, int sms, cudaStream_t s);
 

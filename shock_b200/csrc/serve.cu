@@ -91,7 +91,7 @@ struct shock_server {
     // statistics
     long long completed = 0, failed = 0, rounds = 0, steps_launched = 0;
     double cell_stages = 0, busy_ms = 0;
-    int loop_error = 0;
+    int last_error = 0;   // the last error a round met (its requests failed with it)
     double now() const { return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count(); }
 };
 
@@ -175,7 +175,7 @@ void admit(shock_server *s, std::unique_lock<std::mutex> &lk)
         lk.unlock();
         if (c) rc = batch_add_block(c->b, r->p, r->hb, r->nsteps, &member);
         lk.lock();
-        if (rc == SHOCK_ENOMEM) {                           // fragmentation: retry after a release
+        if (rc == SHOCK_ENOMEM && c && s->running > 0) {   // arena fragmentation: retry after a release
             s->queue.push_front(r->id);
             return;
         }
@@ -226,55 +226,76 @@ void loop_main(shock_server *s)
             active.push_back(&c);
         }
         lk.unlock();
-        int err = 0;
+        // a class whose step or sync failed (e.g. a grid-barrier wait that
+        // ran out, after which its members' state is half-updated) fails all
+        // of its running requests; the others finish as usual
+        std::map<Class *, int> class_err;
         for (Class *c : active) {
             int rc = shock_batch_step_async(c->b, c->launched);
-            if (rc) err = rc;
+            if (rc) class_err[c] = rc;
         }
         for (Class *c : active) {
             int rc = shock_batch_sync(c->b);
-            if (rc) err = rc;
+            if (rc && !class_err.count(c)) class_err[c] = rc;
             float ms = 0.f;
             shock_batch_last_ms(c->b, &ms);
-            if (ms > 0) c->ms_per_step = ms / c->launched;
+            if (ms > 0 && !rc) c->ms_per_step = ms / c->launched;
             s->busy_ms += ms;
         }
-        // harvest finished members
-        std::vector<std::pair<Class *, int>> done;
-        for (Class *c : active)
+        // harvest finished members, and every member of a failed class
+        struct Out { Class *c; int member; int rc; };
+        std::vector<Out> done;
+        for (Class *c : active) {
+            auto ce = class_err.find(c);
             for (auto &m : c->running) {
+                if (ce != class_err.end()) { done.push_back({c, m.first, ce->second}); continue; }
                 int left = 1;
                 shock_batch_steps_left(c->b, m.first, &left);
-                if (left == 0) done.push_back({c, m.first});
+                if (left == 0) done.push_back({c, m.first, SHOCK_OK});
             }
+        }
         std::vector<Request *> finished;
         for (auto &d : done) {
             lk.lock();
-            Request *r = s->reqs[d.first->running[d.second]].get();
+            Request *r = s->reqs[d.c->running[d.member]].get();
             lk.unlock();
-            int dims[6];
-            shock_batch_dims(d.first->b, d.second, dims);
-            r->result.assign(5 * (size_t)dims[0] * dims[1] * dims[2], 0.0);
-            memcpy(r->dims, dims, sizeof dims);
-            int rc = shock_batch_download_state(d.first->b, d.second, r->result.data());
-            if (!rc) rc = shock_batch_remove(d.first->b, d.second);
-            if (rc) err = rc;
+            int rc = d.rc;
+            if (!rc) {
+                int dims[6];
+                shock_batch_dims(d.c->b, d.member, dims);
+                r->result.assign(5 * (size_t)dims[0] * dims[1] * dims[2], 0.0);
+                memcpy(r->dims, dims, sizeof dims);
+                rc = shock_batch_download_state(d.c->b, d.member, r->result.data());
+            }
+            const int rrm = shock_batch_remove(d.c->b, d.member);
+            if (!rc) rc = rrm;
+            d.rc = rc;
+            if (rc) std::vector<double>().swap(r->result);
             finished.push_back(r);
         }
+        int err = 0;
+        for (auto &ce : class_err) err = ce.second;
         lk.lock();
         s->rounds++;
         for (Class *c : active) s->steps_launched += c->launched;
         for (size_t i = 0; i < done.size(); i++) {
             Request *r = finished[i];
-            done[i].first->running.erase(done[i].second);
-            r->state = RQ_DONE;
+            done[i].c->running.erase(done[i].member);
             r->t_done = s->now();
             s->running--;
+            if (done[i].rc) {
+                r->state = RQ_FAILED;
+                r->error = done[i].rc;
+                s->failed++;
+                err = done[i].rc;
+                continue;
+            }
+            r->state = RQ_DONE;
             s->completed++;
             const long long pts = (long long)r->p.ni * r->p.nj * (r->p.dim == 3 ? r->p.nk : 1);
             s->cell_stages += (double)pts * r->p.time_order * r->nsteps;
         }
-        if (err) s->loop_error = err;
+        if (err) s->last_error = err;
         if (!done.empty()) s->cv_done.notify_all();
     }
 }
@@ -350,7 +371,6 @@ int shock_server_submit(shock_server *s, const shock_params *p, const double *x,
     for (int f = 0; f < 8; f++)
         if (src[f]) r->in[f].assign(src[f], src[f] + n);
     std::lock_guard<std::mutex> g2(s->mu);
-    if (s->loop_error) return report_error(s->loop_error, "serving loop stopped after an error");
     r->id = s->next_id++;
     r->t_submit = s->now();
     *id = r->id;
@@ -368,10 +388,9 @@ int shock_server_wait(shock_server *s, long long id, double timeout_s)
     if (it == s->reqs.end()) return report_error(SHOCK_EINVAL, "no such request %lld", id);
     Request *r = it->second.get();
     bool ok = s->cv_done.wait_for(lk, std::chrono::duration<double>(timeout_s),
-                                  [&] { return r->state == RQ_DONE || r->state == RQ_FAILED || s->loop_error; });
+                                  [&] { return r->state == RQ_DONE || r->state == RQ_FAILED; });
     if (!ok) return report_error(SHOCK_ETIMEOUT, "request %lld not finished after %.3f s", id, timeout_s);
     if (r->state == RQ_FAILED) return report_error(r->error, "request %lld failed", id);
-    if (r->state != RQ_DONE) return report_error(s->loop_error, "serving loop stopped after an error");
     return SHOCK_OK;
 }
 
@@ -414,7 +433,7 @@ int shock_server_get_stats(shock_server *s, shock_server_stats *st)
     st->arena_used = arena_used(s->arena);
     st->arena_total = arena_total(s->arena);
     st->uptime_s = s->now();
-    st->loop_error = s->loop_error;
+    st->loop_error = s->last_error;
     return SHOCK_OK;
 }
 

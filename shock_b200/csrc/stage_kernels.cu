@@ -379,6 +379,15 @@ void prepare_kernels()
 #undef A
 }
 
+// True when the current context already has the sweep kernels' raised
+// shared-memory limits (checked on the largest WENO tile).
+bool kernels_prepared()
+{
+    cudaFuncAttributes a{};
+    if (cudaFuncGetAttributes(&a, k_weno<3, 9, 0, false>) != cudaSuccess) return false;
+    return a.maxDynamicSharedSizeBytes >= (int)weno_smem_bytes<3, 9, false>();
+}
+
 void launch_copy_state(const Grid &G, const double *const src[5], double *const dst[5], cudaStream_t s)
 {
     for (int c = 0; c < 5; c++) cudaMemcpyAsync(dst[c], src[c], sizeof(double) * G.NG, cudaMemcpyDeviceToDevice, s);

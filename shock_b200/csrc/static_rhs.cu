@@ -33,10 +33,7 @@ namespace {
 constexpr int kScratchFields = 16;
 static __device__ __align__(256) double g_scratch[(size_t)kScratchFields * SHOCK_STATIC_MAX_POINTS];
 
-// Device address of g_scratch on each device, found once per device.
-constexpr int kMaxDevices = 64;
 std::mutex g_setup_mu;
-double *g_scratch_addr[kMaxDevices] = {};
 
 #define CKS(call)                                                                                           \
     do {                                                                                                    \
@@ -44,26 +41,26 @@ double *g_scratch_addr[kMaxDevices] = {};
         if (e_ != cudaSuccess) return report_error(SHOCK_ECUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
     } while (0)
 
-// Set-up for the current device: look up where g_scratch lives there and
-// raise the sweep kernels' shared-memory limits.  Runs on the first call on
-// each device only.
+// Set-up for the current device: look up where g_scratch lives there (on
+// every call: a host-side lookup, so the address is right even after a
+// cudaDeviceReset or under another context on the same ordinal) and raise
+// the sweep kernels' shared-memory limits when the current context does not
+// have them yet (the first call on a device, or the first after a reset).
 int scratch_for_current_device(double **out)
 {
     int dev = -1;
     CKS(cudaGetDevice(&dev));
-    if (dev < 0 || dev >= kMaxDevices) return report_error(SHOCK_EINVAL, "device ordinal %d out of range", dev);
+    void *addr = nullptr;
+    cudaError_t e = cudaGetSymbolAddress(&addr, g_scratch);
+    if (e != cudaSuccess || !addr)
+        return report_error(SHOCK_ECUDA, "cudaGetSymbolAddress of the scratch array on device %d: %s", dev,
+                            cudaGetErrorString(e));
     std::lock_guard<std::mutex> lock(g_setup_mu);
-    if (!g_scratch_addr[dev]) {
-        void *addr = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&addr, g_scratch);
-        if (e != cudaSuccess || !addr)
-            return report_error(SHOCK_ECUDA, "cudaGetSymbolAddress of the scratch array on device %d: %s", dev,
-                                cudaGetErrorString(e));
+    if (!kernels_prepared()) {
         prepare_kernels();
         CKS(cudaGetLastError());
-        g_scratch_addr[dev] = static_cast<double *>(addr);
     }
-    *out = g_scratch_addr[dev];
+    *out = static_cast<double *>(addr);
     return SHOCK_OK;
 }
 

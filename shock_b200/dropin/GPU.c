@@ -44,6 +44,7 @@
 static shock_ctx *g_ctx;
 static int g_host_behind;   /* the device state is newer than the host U_RK */
 static double *g_buf;       /* 5*NG doubles */
+static double g_tau;        /* the numericalTau the device steps with */
 
 static size_t ghosted_points(const struct strct_configuration *c)
 {
@@ -160,6 +161,7 @@ int GPU_Create(struct strct_configuration *c, struct strct_mesh *m, struct strct
     }
     g_buf = malloc(5 * ng * sizeof(double));
     g_host_behind = 0;
+    g_tau = sp.tau;
     /* start from the host state exactly as SHOCK's set-up left it (e as
      * postprocessLoad or the manufactured solution formed it) */
     const FLT *s5[5] = {U_lastStep->rho, U_lastStep->u, U_lastStep->v, U_lastStep->w, U_lastStep->e};
@@ -172,10 +174,36 @@ void GPU_CalcRungeKutta(struct strct_configuration *c, struct strct_mesh *m, str
                         struct strct_U *U_RK, struct strct_Flux *Q, struct strct_Flux *Q_sum,
                         struct strct_Flux *Flux, struct strct_Flux *Flux_PlusHalf)
 {
-    (void)c; (void)m; (void)U_lastStep; (void)U_RK; (void)Q; (void)Q_sum; (void)Flux; (void)Flux_PlusHalf;
+    (void)m; (void)U_lastStep; (void)U_RK; (void)Q; (void)Q_sum; (void)Flux; (void)Flux_PlusHalf;
+    /* SHOCK's time loop changes numericalTau after a NaN reset and in its
+     * accelerator (src/SHOCK.c:590,638,654); CalcRungeKutta reads it every
+     * step */
+    if ((double)c->numericalTau != g_tau) {
+        int rt = shock_set_tau(g_ctx, (double)c->numericalTau);
+        if (rt) fail("shock_set_tau", rt);
+        g_tau = (double)c->numericalTau;
+    }
     int rc = shock_step(g_ctx, 1);
     if (rc) fail("shock_step", rc);
     g_host_behind = 1;
+}
+
+int GPU_CheckNAN(struct strct_configuration *c, struct strct_U *U_RK, struct strct_mesh *m)
+{
+    int bad = 0;
+    int rc = shock_check_nan(g_ctx, &bad);
+    if (rc && rc != SHOCK_ENAN) fail("shock_check_nan", rc);
+    /* every rank learns whether any rank saw one, as checkNAN's own
+     * all-gather does (src/Functions.c:5451-5466) */
+    int *all = (int *)calloc((size_t)c->MPI_size, sizeof(int)), sum = 0;
+    MPI_Allgather(&bad, 1, MPI_INT, all, 1, MPI_INT, c->MPI_comm);
+    for (int r = 0; r < c->MPI_size; r++) sum += all[r];
+    free(all);
+    if (sum == 0) return 0;
+    /* a non-finite density somewhere: bring U_RK to the host and let SHOCK's
+     * own checkNAN mark it (flag_NAN, the marked values NANExport writes) */
+    GPU_SyncHost(c, U_RK);
+    return checkNAN(c, U_RK, m);
 }
 
 void GPU_SyncHost(struct strct_configuration *c, struct strct_U *U_RK)

@@ -2,13 +2,18 @@
  * GPU.h -- SHOCK-side binding of libshock_b200 (include/shock_b200.h).
  *
  * A SHOCK build adds GPU.c/GPU.h to its src/ directory, links
- * libshock_b200.so, and changes SHOCK.c in three places:
+ * libshock_b200.so, and changes SHOCK.c in these places:
  *   - after the set-up chain, before startSimulation (src/SHOCK.c:288):
  *       GPU_Create(&config, &mesh, &U_lastStep, &Q, device);
  *   - in startSimulation (src/SHOCK.c:565): GPU_CalcRungeKutta(...) with
  *     CalcRungeKutta's arguments, in place of CalcRungeKutta;
- *   - before the host reads U_RK (checkNAN, sampling, export:
- *     src/SHOCK.c:577,663,698-717): GPU_SyncHost(&config, &U_RK);
+ *   - the per-step NaN check (src/SHOCK.c:577): GPU_CheckNAN(...) with
+ *     checkNAN's arguments, in place of checkNAN (no download unless a
+ *     non-finite density is found);
+ *   - after a NaN reset reloads U_RK from a backup (src/SHOCK.c:598-621):
+ *     GPU_UploadState(&config, &U_RK);
+ *   - before the host reads U_RK or U_lastStep (backups, sampling, export:
+ *     src/SHOCK.c:663-717): GPU_SyncHost(&config, &U_RK);
  * and calls GPU_Destroy() at the end of the run.
  */
 #ifndef SHOCK_GPU_H
@@ -26,12 +31,19 @@ int GPU_Create(struct strct_configuration *config, struct strct_mesh *mesh, stru
                struct strct_Flux *Q, int device);
 
 /* One time step on the device: the signature of CalcRungeKutta
- * (src/Functions.h:206-214).  The host copies of U_lastStep and U_RK are
- * not updated (see GPU_SyncHost).  On error: printf + MPI_Abort, as SHOCK
- * reports its own errors. */
+ * (src/Functions.h:206-214), with config->numericalTau as the time step
+ * (forwarded to the device whenever SHOCK's loop has changed it).  The host
+ * copies of U_lastStep and U_RK are not updated (see GPU_SyncHost).  On
+ * error: printf + MPI_Abort, as SHOCK reports its own errors. */
 void GPU_CalcRungeKutta(struct strct_configuration *config, struct strct_mesh *mesh,
                         struct strct_U *U_lastStep, struct strct_U *U_RK, struct strct_Flux *Q,
                         struct strct_Flux *Q_sum, struct strct_Flux *Flux, struct strct_Flux *Flux_PlusHalf);
+
+/* checkNAN (src/Functions.c:5419-5467) on the device state: 0 when no
+ * rank has a non-finite density in its real points (no download);
+ * otherwise U_RK is brought to the host and SHOCK's own checkNAN marks it
+ * and returns 1.  Collective over the ranks, like checkNAN. */
+int GPU_CheckNAN(struct strct_configuration *config, struct strct_U *U_RK, struct strct_mesh *mesh);
 
 /* Copies the device state (rho,u,v,w,e of U_RK, ghosted) into U_RK when
  * the device is ahead of the host. */

@@ -58,3 +58,16 @@ def conserved(prim5):
     """rho, rho u, rho v, rho w, rho e from SHOCK's state variables."""
     r = prim5[0]
     return np.stack([r, r * prim5[1], r * prim5[2], r * prim5[3], r * prim5[4]])
+
+
+def reference_floor(case, nsteps):
+    """Per-variable distance (normwise, as rel_err) between SHOCK's FP64 and
+    80-bit builds after nsteps steps of `case`: the reference's own rounding
+    error on it, or None when the reference builds are absent."""
+    from refbind import RefSolver, ref_available
+    if not (ref_available(case.order, case.dim) and ref_available(case.order, case.dim, extended=True)):
+        return None
+    a, b = RefSolver(case), RefSolver(case, extended=True)
+    a.steps(nsteps)
+    b.steps(nsteps)
+    return rel_err(real(case, a.state()[:5]), real(case, b.state()[:5]))

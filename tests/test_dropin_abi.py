@@ -16,7 +16,8 @@ def test_dropin_binding_exports():
         pytest.skip("drop-in harness not built (make -C oracle with the reference sources)")
     header = open(os.path.join(ROOT, "shock_b200", "dropin", "GPU.h")).read()
     names = re.findall(r"\b(GPU_\w+)\s*\(", header)
-    assert set(names) == {"GPU_Create", "GPU_CalcRungeKutta", "GPU_SyncHost", "GPU_UploadState", "GPU_Destroy"}
+    assert set(names) == {"GPU_Create", "GPU_CalcRungeKutta", "GPU_CheckNAN", "GPU_SyncHost", "GPU_UploadState",
+                          "GPU_Destroy"}
     lib = ctypes.CDLL(LIB, mode=os.RTLD_LOCAL)
     for n in names:
         assert hasattr(lib, n), n

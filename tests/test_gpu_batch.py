@@ -14,7 +14,7 @@ import numpy as np
 import pytest
 
 import shock_b200
-from _util import conserved, l2_rel, real, rel_err
+from _util import conserved, l2_rel, real, reference_floor, rel_err
 from shock_b200 import cases
 
 pytestmark = pytest.mark.gpu
@@ -159,11 +159,17 @@ def test_batch_short_tiles_match_long_tiles(dim, order, precision):
         b.close()
     for c, a, r in zip(cs, out[1], out[0]):
         err = rel_err(real(c, a), real(c, r))
-        tol = 1e-12 if precision == shock_b200.SHOCK_FP64 else 1e-6
-        if c.name.startswith("vortex") and order == 9:
-            tol = max(tol, 1e-6)      # SHOCK's own FP64/80-bit RHS differ by ~1e-6 on the WENO9 vortex
+        tol = np.full(5, 1e-12 if precision == shock_b200.SHOCK_FP64 else 1e-6)
+        if precision == shock_b200.SHOCK_FP64 and c.name.startswith("vortex") and order == 9:
+            # the WENO9 smoothness indicators are ill-conditioned in the nearly
+            # uniform far field: SHOCK's own FP64 and 80-bit builds differ there
+            # by far more than 1e-12, so the bound is twice that distance
+            floor = reference_floor(c, 3)
+            if floor is None:
+                pytest.skip("reference builds absent")
+            tol = np.maximum(tol, 2.0 * floor)
         idx = [0, 1, 2, 3, 4] if dim == 3 else [0, 1, 2, 4]   # w is identically zero in 2D
-        assert (err[idx] <= tol).all(), (c.name, err)
+        assert (err[idx] <= tol[idx]).all(), (c.name, err, tol)
 
 
 def test_persistent_barrier_wait_is_bounded():
