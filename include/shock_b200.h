@@ -160,6 +160,14 @@ int shock_upload_state(shock_ctx *ctx, const double *prim5);
 int shock_upload_last_pressure(shock_ctx *ctx, const double *p);
 int shock_download_state(shock_ctx *ctx, double *prim5, int which);
 
+/* U_RK's pressure p after the last step (NG doubles, ghosted): the field
+ * the last stage's CalcValues and boundary fill wrote (src/Functions.c:
+ * 2392-2481, src/BC.c), which SHOCK copies into U_lastStep with the state
+ * (src/SHOCK.c:661-664) and keeps in its backups.  Rudy outflow faces
+ * read it back at their ghost points after a reset (see
+ * shock_upload_last_pressure). */
+int shock_download_pressure(shock_ctx *ctx, double *p);
+
 /* One right-hand side at the current state, in CalcRungeKutta's stage
  * order without the RK update (src/Functions.c:2111-2293); q5 = 5*NG
  * doubles (real points written, ghosts zero). */
@@ -213,7 +221,8 @@ int shock_kernels_per_step(const shock_ctx *ctx, int *n);
  * for its graph and charges the time between consecutive events to the
  * launch before it, so the per-kernel times of a step add up to that
  * step's graph time.  on = 0 returns to the plain graphs.  Accumulators
- * are cleared by every shock_set_kernel_timing call. */
+ * are cleared by every shock_set_kernel_timing call; calling it with on = 1
+ * while timing is on only clears them (the graphs are kept). */
 int shock_set_kernel_timing(shock_ctx *ctx, int on);
 /* Accumulated times since timing was switched on: names receives up to max
  * entries of 48 characters ("qsum_clear", "ghosts", "prim", "bc", "nodal",

@@ -104,7 +104,7 @@ def lib():
                          "shock_step_async", "shock_sync", "shock_check_nan", "shock_geometry",
                          "shock_device_bytes", "shock_last_step_ms", "shock_kernels_per_step",
                          "shock_mms_baseline", "shock_set_kernel_timing", "shock_kernel_times", "shock_measure_fma_peak",
-                         "shock_set_tau", "shock_get_tau",
+                         "shock_set_tau", "shock_get_tau", "shock_download_pressure",
                          "shock_host_geometry", "shock_host_mms_baseline", "shock_rhs_static",
                          "shock_batch_create", "shock_batch_destroy", "shock_batch_member_bytes",
                          "shock_batch_add", "shock_batch_remove", "shock_batch_step", "shock_batch_step_async",
@@ -274,6 +274,12 @@ class Solver:
         assert s.dtype == np.float64 and s.flags["C_CONTIGUOUS"] and s.size == 5 * self.n
         _check(self.lib.shock_download_state(self.h, _ptr(s), 0))
         return s.reshape((5,) + self.shape)
+
+    def pressure(self) -> np.ndarray:
+        """U_RK's p after the last step (ghosted)."""
+        s = np.zeros(self.n)
+        _check(self.lib.shock_download_pressure(self.h, _ptr(s)))
+        return s.reshape(self.shape)
 
     def set_state(self, prim5):
         a = np.ascontiguousarray(prim5, np.float64).ravel()

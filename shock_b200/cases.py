@@ -106,16 +106,25 @@ def _mesh(dim, n, lo, length, endpoint):
 
 
 def cfl_tau(case: Case, cfl: float = 0.5) -> float:
-    """tau = cfl / max over cells of sum_d (|theta_d| + c |grad xi_d|) on the
-    initial state, with |grad xi_d| = 1/spacing of the Cartesian skeleton."""
+    """tau = cfl / max over cells of sum_d (|theta_d| + c |grad xi_d| +
+    2 nu |grad xi_d|^2) on the initial state, with |grad xi_d| = 1/spacing
+    of the Cartesian skeleton and nu = max(4/3, gamma/Pr) mu / (rho Re) the
+    largest diffusivity of SHOCK's viscous terms (momentum, and heat: in
+    SHOCK's units T diffuses at gamma mu / (rho Re Pr) whatever the Mach
+    number), mu taken as 1.  The viscous part matters only on fine grids at
+    low Reynolds number: on the 64^2 unit-square manufactured solution at
+    Re = 100 the convective estimate alone gives a step about three times
+    RK4's stability limit of the sixth-order viscous stencils (SHOCK's own
+    build diverges after some 25 steps there)."""
     ups = 1.0 / (case.gamma * case.mach ** 2)
     c = np.sqrt(ups * case.gamma * case.p / case.rho)
     vel = (case.u, case.v, case.w)
     n = (case.ni, case.nj, case.nk)
+    nu = 0.0 if case.inviscid else max(4.0 / 3.0, case.gamma / case.prandtl) / (case.rho * case.reynolds)
     s = np.zeros_like(case.rho)
     for a in range(case.dim):
         h = case.period[a] / n[a] if case.periodic[a] else case.period[a] / (n[a] - 1)
-        s = s + (np.abs(vel[a]) + c) / h
+        s = s + (np.abs(vel[a]) + c) / h + 2.0 * nu / (h * h)
     return float(cfl / s.max())
 
 

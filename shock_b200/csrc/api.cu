@@ -163,7 +163,9 @@ constexpr int kMaxMarks = 128;   // event marks per time step (about 14 per stag
 static void mark(shock_ctx *c, const char *name)
 {
     if (!c->timing || c->tmark >= kMaxMarks) return;
-    cudaEventRecord(c->tev[c->tmark], c->stream);
+    // an event record node in the captured graph (a plain record during
+    // capture would only order the capture's streams)
+    cudaEventRecordWithFlags(c->tev[c->tmark], c->stream, cudaEventRecordExternal);
     c->tname[c->tmark] = name;
     c->tmark++;
 }
@@ -569,6 +571,15 @@ int shock_download_state(shock_ctx *c, double *prim5, int which)
     return SHOCK_OK;
 }
 
+int shock_download_pressure(shock_ctx *c, double *p)
+{
+    if (!c || !p) return fail(SHOCK_EINVAL, "null argument");
+    CK(cudaSetDevice(c->device));
+    CK(cudaMemcpyAsync(p, c->F.p, sizeof(double) * c->G.NG, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    return SHOCK_OK;
+}
+
 int shock_rhs(shock_ctx *c, double *q5)
 {
     if (!c || !q5) return fail(SHOCK_EINVAL, "null argument");
@@ -744,8 +755,11 @@ int shock_set_kernel_timing(shock_ctx *c, int on)
         for (auto &e : c->tev) CK(cudaEventCreate(&e));
     }
     // the step graphs are captured again, with or without the event nodes
-    for (int i = 0; i < 3; i++)
-        if (c->step_graph[i]) { cudaGraphExecDestroy(c->step_graph[i]); c->step_graph[i] = nullptr; }
+    // (only when timing is switched on or off: switching it on again just
+    // clears the accumulators)
+    if ((on != 0) != c->timing)
+        for (int i = 0; i < 3; i++)
+            if (c->step_graph[i]) { cudaGraphExecDestroy(c->step_graph[i]); c->step_graph[i] = nullptr; }
     c->timing = on != 0;
     c->tacc.clear();
     c->tsteps = 0;

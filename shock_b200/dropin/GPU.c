@@ -215,6 +215,11 @@ void GPU_SyncHost(struct strct_configuration *c, struct strct_U *U_RK)
     FLT *dst[5] = {U_RK->rho, U_RK->u, U_RK->v, U_RK->w, U_RK->e};
     for (int f = 0; f < 5; f++)
         for (size_t o = 0; o < ng; o++) dst[f][o] = (FLT)g_buf[f * ng + o];
+    /* and U_RK's p, which SHOCK copies into U_lastStep and its backups
+     * (Rudy outflow faces read it back after a reset) */
+    rc = shock_download_pressure(g_ctx, g_buf);
+    if (rc) fail("shock_download_pressure", rc);
+    for (size_t o = 0; o < ng; o++) U_RK->p[o] = (FLT)g_buf[o];
     g_host_behind = 0;
 }
 

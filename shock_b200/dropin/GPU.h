@@ -45,8 +45,8 @@ void GPU_CalcRungeKutta(struct strct_configuration *config, struct strct_mesh *m
  * and returns 1.  Collective over the ranks, like checkNAN. */
 int GPU_CheckNAN(struct strct_configuration *config, struct strct_U *U_RK, struct strct_mesh *mesh);
 
-/* Copies the device state (rho,u,v,w,e of U_RK, ghosted) into U_RK when
- * the device is ahead of the host. */
+/* Copies the device state (rho,u,v,w,e and p of U_RK, ghosted) into U_RK
+ * when the device is ahead of the host. */
 void GPU_SyncHost(struct strct_configuration *config, struct strct_U *U_RK);
 
 /* Pushes a host-modified U_RK (e.g. after a NaN reset) to the device. */
