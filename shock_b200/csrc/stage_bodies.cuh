@@ -862,22 +862,6 @@ __device__ __forceinline__ void w9_terms(const T *f, T eps, T *t)
     }
 }
 
-// The same terms in FP32 from the stencil's eight first differences d, by
-// the factorised forms (c_w9ldl).  The indicators are even in d, so the
-// minus side's stencil takes its differences with either sign.
-__device__ __forceinline__ void w9_terms_diff(const float *d, float eps, float *t)
-{
-#pragma unroll
-    for (int k = 0; k < 5; k++) {
-        const float *x = d + k, *c = c_w9ldl[k];
-        const float y0 = fmaf(c[3], x[3], fmaf(c[1], x[2], fmaf(c[0], x[1], x[0])));
-        const float y1 = fmaf(c[4], x[3], fmaf(c[2], x[2], x[1]));
-        const float y2 = fmaf(c[5], x[3], x[2]);
-        const float is = fmaf(c[6] * y0, y0, fmaf(c[7] * y1, y1, fmaf(c[8] * y2, y2, c[9] * x[3] * x[3])));
-        t[k] = is + eps;
-    }
-}
-
 template <typename T>
 __device__ __forceinline__ T w9_phi(const T *d, const T *r)
 {
@@ -1100,6 +1084,100 @@ __device__ __forceinline__ void weno5_rows_mixed(const FaceState<float> &s, cons
     }
 }
 
+// The WENO9 smoothness terms in FP32 from a stencil's eight first
+// differences d, by the factorised forms (c_w9ldl), for both split stencils
+// at once: lane x the plus side, lane y the minus side (packed FP32).  The
+// indicators are even in d, so the minus side's stencil takes its
+// differences with either sign.
+__device__ __forceinline__ void w9_terms_diff2(const float2 *d, float eps, float2 *t)
+{
+#pragma unroll
+    for (int k = 0; k < 5; k++) {
+        const float2 *x = d + k;
+        const float *c = c_w9ldl[k];
+        const float2 y0 = fma2(f2(c[3]), x[3], fma2(f2(c[1]), x[2], fma2(f2(c[0]), x[1], x[0])));
+        const float2 y1 = fma2(f2(c[4]), x[3], fma2(f2(c[2]), x[2], x[1]));
+        const float2 y2 = fma2(f2(c[5]), x[3], x[2]);
+        const float2 is = fma2(mul2(f2(c[6]), y0), y0,
+                               fma2(mul2(f2(c[7]), y1), y1, fma2(mul2(f2(c[8]), y2), y2, mul2(mul2(f2(c[9]), x[3]), x[3]))));
+        t[k] = add2(is, f2(eps));
+    }
+}
+
+// w9_phi of both split stencils (lanes as in w9_terms_diff2) from their
+// differences d and the reciprocals r of their smoothness terms.
+__device__ __forceinline__ float2 w9_phi2(const float2 *d, const float2 *r)
+{
+    const float dk[5] = {float(1. / 126.), float(10. / 63.), float(10. / 21.), float(20. / 63.), float(5. / 126.)};
+    float2 ot[5];
+#pragma unroll
+    for (int k = 0; k < 5; k++) ot[k] = mul2(f2(dk[k]), mul2(r[k], r[k]));
+    const float2 rs = rcp2(add2(add2(add2(add2(ot[0], ot[1]), ot[2]), ot[3]), ot[4]));
+    const float2 o0 = mul2(ot[0], rs), o2 = mul2(ot[2], rs), o3 = mul2(ot[3], rs), o4 = mul2(ot[4], rs);
+    float2 q[4];   // fourth differences d[k] - 4 d[k+1] + 6 d[k+2] - 4 d[k+3] + d[k+4]
+#pragma unroll
+    for (int k = 0; k < 4; k++)
+        q[k] = add2(fma2(f2(-4.f), d[k + 3], fma2(f2(6.f), d[k + 2], fma2(f2(-4.f), d[k + 1], d[k]))), d[k + 4]);
+    const float2 c32 = fma2(f2(-2.f), q[2], mul2(f2(3.f), q[1]));           // 3 q2 - 2 q3
+    const float2 c323 = fma2(f2(3.f), q[3], c32);                           // 3 q2 - 2 q3 + 3 q4
+    const float2 lin = fma2(f2(3.f), q[3], fma2(f2(-14.f), q[2], mul2(f2(39.f), q[1])));
+    float2 ph = mul2(f2(-1.f / 840.f), lin);
+    ph = fma2(mul2(f2(1.f / 60.f), o4), c323, ph);
+    ph = fma2(mul2(f2(1.f / 60.f), o3), c32, ph);
+    ph = fma2(mul2(f2(1.f / 20.f), o2), q[1], ph);
+    return fma2(mul2(f2(1.f / 5.f), o0), q[0], ph);
+}
+
+// Mixed WENO9, characteristic row CH of one face: the nine projected point
+// differences as (plus, minus) pairs from the (flux, conserved) difference
+// pairs over the entries the row can weight, then both split stencils'
+// indicators, weights and Phi in packed FP32.  Returns Phi- - Phi+.
+template <int DIM, int D, int TLN, int CH>
+__device__ __forceinline__ float weno9_row_mixed(const FaceState<float> &s, const float *dl, int f, int lane, float a,
+                                                 float eps)
+{
+    constexpr unsigned M = row_mask<DIM, D>(CH);
+    asm volatile("" ::: "memory");
+    float L[5];
+    left_row<float>(s, CH, L[0], L[1], L[2], L[3], L[4]);
+#pragma unroll
+    for (int i = 0; i < 5; i++) L[i] *= 0.5f;   // halved row (dot_pm2)
+    float2 pd[9];
+#pragma unroll
+    for (int q = 0; q < 9; q++) {
+        const int t = f + q;
+        asm volatile("" ::: "memory");   // issue this point's loads here, not all up front
+        float2 pv[5];
+#pragma unroll
+        for (int i = 0; i < 5; i++)
+            if (M >> i & 1u) pv[i] = reinterpret_cast<const float2 *>(dl)[(t * NLANE + lane) * 5 + i];
+        pd[q] = dot_pm2<M>(L, pv, a);
+    }
+    // plus side: differences 0..7; minus side: 8..1 (SHOCK's mirrored stencil)
+    float2 dd[8];
+#pragma unroll
+    for (int q = 0; q < 8; q++) dd[q] = f2(pd[q].x, pd[8 - q].y);
+    float2 t[5], rc[5];
+    w9_terms_diff2(dd, eps, t);
+#pragma unroll
+    for (int k = 0; k < 5; k++) {   // the plus and minus terms of stencil k share one division
+        const float qk = __fdividef(1.f, t[k].x * t[k].y);
+        rc[k] = f2(qk * t[k].y, qk * t[k].x);
+    }
+    const float2 ph = w9_phi2(dd, rc);
+    return -ph.x + ph.y;
+}
+
+// Row CH of the mixed WENO9 face and its back-projection into out.
+template <int DIM, int D, int TLN, int CH>
+__device__ __forceinline__ void weno9_row_mixed_add(const FaceState<float> &s, const float *dl, int f, int lane,
+                                                    float a, float eps, float *out)
+{
+    const float phi = weno9_row_mixed<DIM, D, TLN, CH>(s, dl, f, lane, a, eps);
+    if (DIM == 3) add_right_col_diag<D, CH>(s, phi, out);
+    else add_right_col<float>(s, CH, phi, out);
+}
+
 // Mixed form of the same: the projection, indicators, weights and
 // back-projection in FP32 on FP64-formed point-to-point differences dl.
 template <int DIM, int ORDER, int D, int TLN = TL>
@@ -1142,38 +1220,17 @@ __device__ __forceinline__ void face_weno_mixed(const Phys &P, const double *sh,
             for (int ch = 0; ch < 5; ch++) add_right_col<float>(s, ch, phi[ch], out);
         }
     } else {
+        // one row at a time (a loop the compiler does not interleave: the
+        // five rows unrolled together need about 240 registers)
 #pragma unroll 1
         for (int ch = 0; ch < 5; ch++) {
-            asm volatile("" ::: "memory");
-            float L0, L1, L2, L3, L4;
-            left_row<float>(s, ch, L0, L1, L2, L3, L4);
-            L0 *= 0.5f; L1 *= 0.5f; L2 *= 0.5f; L3 *= 0.5f; L4 *= 0.5f;   // halved row
-            float dp[2 * r + 1], dmv[2 * r + 1];
-#pragma unroll
-            for (int q = 0; q <= 2 * r; q++) {
-                int t = f + q;
-                // the ten differences of a point are interleaved: five 8-byte
-                // loads (the WENO5 (flux, conserved) pair layout measured 58 %
-                // slower here)
-                const float2 p0 = DL2(0, t, lane), p1 = DL2(1, t, lane), p2 = DL2(2, t, lane);
-                const float2 p3 = DL2(3, t, lane), p4 = DL2(4, t, lane);
-                const float lf = L0 * p0.x + L1 * p0.y + L2 * p1.x + L3 * p1.y + L4 * p2.x;
-                const float lu = L0 * p2.y + L1 * p3.x + L2 * p3.y + L3 * p4.x + L4 * p4.y;
-                dp[q] = lf + a * lu;
-                dmv[q] = lf - a * lu;
+            switch (ch) {
+            case 0: weno9_row_mixed_add<DIM, D, TLN, 0>(s, dl, f, lane, a, eps, out); break;
+            case 1: weno9_row_mixed_add<DIM, D, TLN, 1>(s, dl, f, lane, a, eps, out); break;
+            case 2: weno9_row_mixed_add<DIM, D, TLN, 2>(s, dl, f, lane, a, eps, out); break;
+            case 3: weno9_row_mixed_add<DIM, D, TLN, 3>(s, dl, f, lane, a, eps, out); break;
+            default: weno9_row_mixed_add<DIM, D, TLN, 4>(s, dl, f, lane, a, eps, out); break;
             }
-            float phi;
-            {
-                float dP[8], dM[8];
-#pragma unroll
-                for (int q = 0; q < 8; q++) { dP[q] = dp[q]; dM[q] = dmv[2 * r - q]; }
-                float tt[10], rc[10];
-                w9_terms_diff(dP, eps, tt);
-                w9_terms_diff(dM, eps, tt + 5);
-                pair_reciprocals<10>(tt, rc);
-                phi = -w9_phi<float>(dP, rc) + w9_phi<float>(dM, rc + 5);
-            }
-            add_right_col<float>(s, ch, phi, out);
         }
     }
 #pragma unroll
@@ -1264,8 +1321,7 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
             if (it < (NP - 1) * NLANE && T.l0 + l < G.g + T.nL && T.c0 - r + t < G.N[D])
 #pragma unroll
                 for (int q = 0; q < 5; q++)
-                    reinterpret_cast<float2 *>(dl)[(t * NLANE + l) * 5 + q] =
-                        ORDER == 5 ? make_float2(dv[m][q], dv[m][5 + q]) : make_float2(dv[m][2 * q], dv[m][2 * q + 1]);
+                    reinterpret_cast<float2 *>(dl)[(t * NLANE + l) * 5 + q] = make_float2(dv[m][q], dv[m][5 + q]);
         }
 #pragma unroll
         for (int k = 0; k < FPT; k++) {
@@ -1984,7 +2040,9 @@ __device__ __forceinline__ void post_body(const Grid &G, double mach, const doub
 template <int DIM, int ORDER, bool MIXED, int TLN = TL>
 constexpr size_t weno_smem_bytes()
 {
-    return sizeof(double) * ((size_t)WenoNV<DIM>::NV * (TLN + ORDER + 1) * NLS + (MIXED ? 0 : 5 * NROWT * NLANE));
+    // (+ the face-flux buffer of the first faces when a thread takes two)
+    return sizeof(double) * ((size_t)WenoNV<DIM>::NV * (TLN + ORDER + 1) * NLS +
+                             ((MIXED || TLN + 1 == NROWT) ? 0 : 5 * NROWT * NLANE));
 }
 
 template <int DIM, int ORDER, int TLN = TL>

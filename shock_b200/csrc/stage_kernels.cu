@@ -68,16 +68,45 @@ __global__ void k_nodal(Grid G, const double *__restrict__ U, const double *__re
     if (o < G.NG) nodal_body<DIM, ORDER, MIXED>(G, o, U, V, W, T, F);
 }
 
-// Two tiles per SM, except FP64 WENO9 (its face needs about 170 registers
-// and a 122 KB tile); the mixed WENO9 tile (110 KB, 128 registers) fits twice
+#ifndef SHOCK_W9_FP64_TL
+#define SHOCK_W9_FP64_TL 7
+#endif
+#ifndef SHOCK_W9_FP64_MINB
+#define SHOCK_W9_FP64_MINB 2
+#endif
+
+// Sweep tile of the WENO kernels: 15 cells (two faces per thread) and two
+// tiles per SM (128 registers); the mixed WENO9 tile (110 KB) fits twice
 // (the driver's own shared-memory carveout gives that; asking for the full
-// carveout for every sweep measured 10 % slower mixed WENO5 sweeps).
+// carveout for every sweep measured 10 % slower mixed WENO5 sweeps).  The
+// 3D FP64 WENO9 face is the largest: its 15-cell tile (116 KB) fits once
+// per SM, so it takes 7-cell tiles (one face per thread, 72 KB) held to 128
+// registers without spills, two per SM (sweeps 28-34 % faster at 256^3 than
+// one 15-cell tile per SM; three 7-cell tiles per SM spill and measured
+// 8-21 % slower than two).  The 2D FP64 WENO9 face (two nonzero normal
+// components, full rows) spills at 128 registers and keeps the 15-cell tile.
+#ifndef SHOCK_W9_MIXED_TL
+#define SHOCK_W9_MIXED_TL 15
+#endif
+#ifndef SHOCK_W9_MIXED_MINB
+#define SHOCK_W9_MIXED_MINB 2
+#endif
+template <int DIM, int ORDER, bool MIXED>
+struct WenoTile {
+    static constexpr bool w9_3d_fp64 = DIM == 3 && ORDER == 9 && !MIXED;
+    static constexpr bool w9_mixed = ORDER == 9 && MIXED;
+    static constexpr int tl = w9_3d_fp64 ? SHOCK_W9_FP64_TL : w9_mixed ? SHOCK_W9_MIXED_TL : TL;
+    static constexpr int minb = w9_3d_fp64 ? SHOCK_W9_FP64_MINB : w9_mixed ? SHOCK_W9_MIXED_MINB
+                                                                           : (ORDER == 9 && !MIXED) ? 1 : 2;
+};
+
 template <int DIM, int ORDER, int D, bool MIXED>
-__global__ void __launch_bounds__(NTHR, (ORDER == 5 || MIXED) ? 2 : 1)
+__global__ void __launch_bounds__(NTHR, (WenoTile<DIM, ORDER, MIXED>::minb))
     k_weno(Grid G, Phys P, bool first, const double *__restrict__ R, const double *__restrict__ Uu,
            const double *__restrict__ Vv, const double *__restrict__ Ww, const double *__restrict__ Ee, Fields F)
 {
-    weno_body<DIM, ORDER, D, MIXED>(G, P, first, R, Uu, Vv, Ww, Ee, F, blockIdx.x, blockIdx.y, blockIdx.z);
+    weno_body<DIM, ORDER, D, MIXED, WenoTile<DIM, ORDER, MIXED>::tl>(G, P, first, R, Uu, Vv, Ww, Ee, F, blockIdx.x,
+                                                                      blockIdx.y, blockIdx.z);
 }
 
 // Viscous sweep tile length: 7 cells (one face per thread, three tiles per
@@ -261,13 +290,14 @@ template <int DIM, int ORDER, int D, bool MIXED>
 static void weno_one(const Grid &G, const Phys &P, bool first, const double *const U[5], const Fields &F,
                      cudaStream_t s)
 {
-    constexpr size_t smem = weno_smem_bytes<DIM, ORDER, MIXED>();
+    constexpr int WTL = WenoTile<DIM, ORDER, MIXED>::tl;
+    constexpr size_t smem = weno_smem_bytes<DIM, ORDER, MIXED, WTL>();
     if (!G.order) {
         cudaFuncSetAttribute(k_weno<DIM, ORDER, D, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         return;
     }
-    k_weno<DIM, ORDER, D, MIXED><<<sweep_grid<DIM, D>(G), dim3(NLANE, NROWT), smem, s>>>(G, P, first, U[0], U[1],
-                                                                                        U[2], U[3], U[4], F);
+    k_weno<DIM, ORDER, D, MIXED><<<sweep_grid<DIM, D, WTL>(G), dim3(NLANE, NROWT), smem, s>>>(G, P, first, U[0], U[1],
+                                                                                             U[2], U[3], U[4], F);
 }
 
 template <int DIM, int ORDER, int D, bool MIXED>
@@ -385,7 +415,7 @@ bool kernels_prepared()
 {
     cudaFuncAttributes a{};
     if (cudaFuncGetAttributes(&a, k_weno<3, 9, 0, false>) != cudaSuccess) return false;
-    return a.maxDynamicSharedSizeBytes >= (int)weno_smem_bytes<3, 9, false>();
+    return a.maxDynamicSharedSizeBytes >= (int)weno_smem_bytes<3, 9, false, WenoTile<3, 9, false>::tl>();
 }
 
 void launch_copy_state(const Grid &G, const double *const src[5], double *const dst[5], cudaStream_t s)

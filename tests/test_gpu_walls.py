@@ -84,38 +84,40 @@ def test_wall_rhs_matches_reference(name):
     assert (rel_err(q, ref) <= tol).all(), (rel_err(q, ref), tol)
 
 
-@pytest.mark.parametrize("name", sorted(CASES))
-def test_wall_steps_match_reference(name):
-    """20 steps within max(1e-10, 2 * SHOCK's own FP64-vs-80-bit distance)
-    relative L2: the supersonic WENO9 ducts amplify rounding, SHOCK's two
-    builds there drift apart by up to 3e-8."""
-    c = CASES[name]()
-    _need(c)
-    s = shock_b200.Solver(c)
-    r, r80 = RefSolver(c), RefSolver(c, extended=True)
-    s.steps(20)
-    r.steps(20)
-    r80.steps(20)
-    ref = real(c, r.state()[:5])
-    tol = np.maximum(L2_TOL, 2.0 * l2_rel(ref, real(c, r80.state()[:5])))
-    err = l2_rel(real(c, s.state()), ref)
-    assert (err <= tol).all(), (err, tol)
-
-
-@pytest.mark.parametrize("name", ["noslip_3d_w5", "duct_rudy_walls_2d_w9", "duct_isentropic_slip_2d_w5"])
-def test_wall_100_steps_match_reference(name):
-    """100 RK steps within max(1e-10, 2 * SHOCK's own FP64-vs-80-bit
-    distance) relative L2, the bar of the periodic parity tests."""
-    c = CASES[name]()
-    _need(c)
+def _check_steps(c, nsteps, parity, label):
+    """The GPU state after nsteps against SHOCK's FP64 and 80-bit builds.
+    Bound, per variable (relative L2): 1e-10, or where SHOCK's own FP64 build
+    drifts further than that from its 80-bit build (floor; the WENO9 and
+    supersonic ducts amplify rounding, up to 3e-8 in 20 steps), the GPU must
+    stay within 2 floors of the 80-bit answer, i.e. about as accurate as
+    SHOCK's FP64 build, and so within 3 floors of the FP64 build."""
     s = shock_b200.Solver(c)
     r, r80 = RefSolver(c), RefSolver(c, extended=True)
     for x in (s, r, r80):
-        x.steps(100)
-    ref = real(c, r.state()[:5])
-    tol = np.maximum(L2_TOL, 2.0 * l2_rel(ref, real(c, r80.state()[:5])))
-    err = l2_rel(real(c, s.state()), ref)
-    assert (err <= tol).all(), (err, tol)
+        x.steps(nsteps)
+    ref, ref80, st = real(c, r.state()[:5]), real(c, r80.state()[:5]), real(c, s.state())
+    floor = l2_rel(ref, ref80)
+    err64, err80 = l2_rel(st, ref), l2_rel(st, ref80)
+    parity(label, c.name, f"{nsteps} steps L2 vs SHOCK FP64", err64, np.maximum(L2_TOL, 3.0 * floor), floor)
+    assert (err80 <= np.maximum(L2_TOL, 2.0 * floor)).all(), (err80, floor)
+    assert (err64 <= np.maximum(L2_TOL, 3.0 * floor)).all(), (err64, floor)
+
+
+@pytest.mark.parametrize("name", sorted(CASES))
+def test_wall_steps_match_reference(name, parity):
+    """20 steps (bound: _check_steps)."""
+    c = CASES[name]()
+    _need(c)
+    _check_steps(c, 20, parity, "walls_20")
+
+
+@pytest.mark.parametrize("name", ["noslip_3d_w5", "duct_rudy_walls_2d_w9", "duct_isentropic_slip_2d_w5"])
+def test_wall_100_steps_match_reference(name, parity):
+    """100 RK steps (bound: _check_steps), the length of the periodic parity
+    tests."""
+    c = CASES[name]()
+    _need(c)
+    _check_steps(c, 100, parity, "walls_100")
 
 
 @pytest.mark.parametrize("name", ["duct_rudy_walls_2d_w9", "box_rudy_2d_w5"])
