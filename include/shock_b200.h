@@ -351,6 +351,64 @@ int shock_server_get_stats(shock_server *s, shock_server_stats *st);
 /* Stop the loop (requests not finished are dropped) and free everything. */
 int shock_server_destroy(shock_server *s);
 
+/* ------------------------------------------------------------------------
+ * Blocks of a division on one device.  SHOCK runs one block per MPI rank,
+ * the blocks described by the .sddc division file (src/Load.c:191-250,
+ * 355-400), and exchanges their interface layers with MPI before each
+ * stage (TransferFlowParameterWithGhosts, src/Functions.c:3580-3684).  Here
+ * every block of the division lives on one device and the exchange is two
+ * kernels per pass (pack all faces, then unpack all), in SHOCK's passes:
+ * one per stage, two (2D) or three (3D) with viscous terms
+ * (src/Functions.c:2117-2136).  The geometry set-up exchanges coordinates
+ * and metric terms the way SHOCK's TransferMeshParameter does
+ * (src/Functions.c:3481-3578, src/SHOCK.c:174-205).
+ * ------------------------------------------------------------------------ */
+typedef struct shock_block {
+    int ni, nj, nk;            /* real points of the block (the .sddc corners) */
+    int bc[6];                 /* face types of faces without a neighbour, SHOCK_BC_AUTO on the others */
+    int neighbour[6];          /* block across each face (Left, Right, Bottom, Top, Behind, InFront), -1 for
+                                  none; the neighbour's opposite face touches this face with the identity
+                                  orientation (.sddc transform 1,2,3), and a block may be its own neighbour
+                                  (a periodic axis of one block) */
+    float translation[6][3];   /* the .sddc Translation of each face: added to the coordinates received
+                                  across it (a periodic wrap: minus / plus the period) */
+    const double *x, *y, *z, *u, *v, *w, *p, *rho;   /* real points, Fortran order (as shock_create) */
+} shock_block;
+
+typedef struct shock_multi shock_multi;
+
+/* A division of nblocks blocks on one device.  p gives the run's keys
+ * (dim, order, time_order, tau, physics, precision, the [BoundaryConditions]
+ * values, zeta_fix, weno_eps); its sizes, periodic, period and bc fields are
+ * not used (the blocks carry them).  Faces that name each other must agree
+ * in their lateral sizes.  Manufactured-solution runs are single-block
+ * (SHOCK_EINVAL). */
+int shock_multi_create(const shock_params *p, int nblocks, const shock_block *blocks, int device,
+                       shock_multi **out);
+int shock_multi_destroy(shock_multi *m);
+/* Host-only set-up of a division's geometry, no device: out13[b] receives
+ * block b's 13*NG geometry (as shock_geometry). */
+int shock_host_multi_geometry(const shock_params *p, int nblocks, const shock_block *blocks, double *const *out13);
+/* Ghosted sizes and first real index of a block (as shock_dims). */
+int shock_multi_dims(const shock_multi *m, int block, int out6[6]);
+/* A block's geometry after set-up (13*NG, as shock_geometry). */
+int shock_multi_geometry(shock_multi *m, int block, double *out13);
+/* nsteps time steps of every block (one CUDA graph per step); waits. */
+int shock_multi_step(shock_multi *m, int nsteps);
+/* One right-hand side of every block at the current state; q5 receives
+ * block's (5*NG, as shock_rhs). */
+int shock_multi_rhs(shock_multi *m, int block, double *q5);
+/* A block's rho,u,v,w,e (5*NG, ghosted). */
+int shock_multi_download_state(shock_multi *m, int block, double *prim5);
+int shock_multi_upload_state(shock_multi *m, int block, const double *prim5);
+/* The time step of the following steps (as shock_set_tau). */
+int shock_multi_set_tau(shock_multi *m, double tau);
+/* checkNAN over every block; SHOCK_ENAN when any density is non-finite. */
+int shock_multi_check_nan(shock_multi *m, int *bad);
+/* Number of blocks, kernel launches per step, device time (ms) of the last
+ * shock_multi_step call. */
+int shock_multi_info(const shock_multi *m, int *nblocks, int *kernels_per_step, float *last_ms);
+
 /* Largest block (ghosted points NIg*NJg*NKg) shock_rhs_static accepts. */
 #define SHOCK_STATIC_MAX_POINTS 524288
 

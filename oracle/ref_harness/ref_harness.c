@@ -100,6 +100,7 @@ static void periodic_pass(int a, FLT **fields, int nf, const float *trans)
             }
 }
 
+#ifndef REF_MULTIRANK
 /* Replaces Functions.c:3481 for a single periodic block. */
 void TransferMeshParameter(struct strct_configuration *pc, struct strct_mesh *pm)
 {
@@ -121,6 +122,12 @@ void TransferFlowParameterWithGhosts(struct strct_configuration *pc, struct strc
     for (int a = 0; a < MESHDIMENSIONS; a++)
         if (prm.periodic[a]) periodic_pass(a, f, 5, NULL);
 }
+#endif
+
+/* Interface set-up of a rank (multi-rank build): what loadFile takes from
+ * the .sddc division file (src/Load.c:355-400), applied before
+ * postprocessLoad. */
+static void (*g_iface_hook)(void);
 
 void ref_free(void);
 
@@ -201,6 +208,8 @@ int ref_init(const ref_params *p, const double *x, const double *y, const double
         }
     }
 
+    if (g_iface_hook) g_iface_hook();
+
     vx.ptr = (void *)x; vx.dt = RealDouble;
     vy.ptr = (void *)y; vy.dt = RealDouble;
     vz.ptr = (void *)z; vz.dt = RealDouble;
@@ -246,7 +255,12 @@ void ref_rhs(double *q)
 {
     int n = NG;
     DeleteQ(&cfg, &Qf);
+    /* as many exchange passes as CalcRungeKutta makes (Functions.c:2117-2136) */
     TransferFlowParameterWithGhosts(&cfg, &msh, &U_rk);
+    if (cfg.flag_Inviscid != 1) {
+        TransferFlowParameterWithGhosts(&cfg, &msh, &U_rk);
+        if (MESHDIMENSIONS == 3) TransferFlowParameterWithGhosts(&cfg, &msh, &U_rk);
+    }
     CalcValues(&cfg, &msh, &U_rk);
     SetAllBoundaryConditions(&cfg, &msh, &U_rk, &U_last);
     CalcFluxesInXiDirection(&cfg, &msh, &U_rk, &Fl, &Flh, &Qf);
@@ -511,5 +525,132 @@ void ref_dropin_destroy(void)
     cfg.Translation = NULL;
     cfg.NumberInterfaces = 0;
     dropin_interfaces_free();
+}
+#endif
+
+#ifdef REF_MULTIRANK
+#include <sys/mman.h>
+/*
+ * Multi-rank runs of SHOCK's own code (the oracle of the blocks-on-one-GPU
+ * path): block b of a Cartesian division runs as rank b of ref_harness/
+ * mpi_shm.c, with the interfaces loadFile would read from the .sddc file
+ * (src/Load.c:191-250, 355-400) -- identity transform (1,2,3), the point
+ * ranges of the two touching faces in each block's own 1-based indices and
+ * the float32 Translation the receiving side adds -- and SHOCK's own
+ * TransferMeshParameter / TransferFlowParameterWithGhosts exchanging them.
+ */
+int shm_run(int nranks, size_t slot_bytes, int (*body)(int rank, void *arg), void *arg);
+
+typedef struct {
+    int nblocks;
+    const ref_params *blk;        /* per block (sizes, face types; periodic = 0) */
+    const int *neigh;             /* [nblocks][6] neighbour across each face, -1: none */
+    const float *trans;           /* [nblocks][6][3] Translation of each face */
+    const double *const *in;      /* [nblocks][8] x,y,z,u,v,w,p,rho (real points, Fortran order) */
+    int nrhs;                     /* 1: also one right-hand side at the initial state */
+    int nsteps;
+    double *out;                  /* shared: per block 13*NG geometry, 5*NG rhs, 9*NG state */
+    const size_t *out_off;        /* [nblocks] offset of each block's output */
+} mr_job;
+
+static const mr_job *g_job;
+static int g_rank_blk;
+static int mr_rank[6];
+static float *mr_tr[6];
+static int *mr_tf[6];
+static cgsize_t *mr_rng[6], *mr_drng[6];
+static float *mr_rc[6], *mr_ra[6];
+
+static void mr_interfaces(void)
+{
+    const int b = g_rank_blk, dim = MESHDIMENSIONS;
+    const ref_params *p = &g_job->blk[b];
+    int *side[6] = {&cfg.InterfaceNeighbourLeft, &cfg.InterfaceNeighbourRight, &cfg.InterfaceNeighbourBottom,
+                    &cfg.InterfaceNeighbourTop, &cfg.InterfaceNeighbourBehind, &cfg.InterfaceNeighbourInFront};
+    static int ranks[6];
+    static int *tf[6];
+    static cgsize_t *rng[6], *drng[6];
+    static float *tr[6], *rc[6], *ra[6];
+    int ii = 0;
+    for (int f = 0; f < 6; f++) {
+        const int nb = f < 2 * dim ? g_job->neigh[6 * b + f] : -1;
+        if (nb < 0) { *side[f] = NO_NEIGHBOUR; continue; }
+        const int a = f / 2, hi = f % 2;
+        const ref_params *q = &g_job->blk[nb];
+        const int me_n[3] = {p->ni, p->nj, p->nk}, nb_n[3] = {q->ni, q->nj, q->nk};
+        tf[ii] = mr_tf[ii];
+        rng[ii] = mr_rng[ii];
+        drng[ii] = mr_drng[ii];
+        tr[ii] = mr_tr[ii];
+        rc[ii] = mr_rc[ii];
+        ra[ii] = mr_ra[ii];
+        for (int c = 0; c < dim; c++) {
+            tf[ii][c] = c + 1;
+            rng[ii][c] = 1;
+            rng[ii][dim + c] = me_n[c];
+            drng[ii][c] = 1;
+            drng[ii][dim + c] = nb_n[c];
+        }
+        rng[ii][a] = rng[ii][dim + a] = hi ? me_n[a] : 1;          /* my face */
+        drng[ii][a] = drng[ii][dim + a] = hi ? 1 : nb_n[a];        /* the neighbour's opposite face */
+        for (int c = 0; c < 3; c++) {
+            tr[ii][c] = g_job->trans[(6 * b + f) * 3 + c];
+            rc[ii][c] = 0.f;
+            ra[ii][c] = 0.f;
+        }
+        ranks[ii] = nb;
+        *side[f] = ii++;
+    }
+    cfg.NumberInterfaces = ii;
+    cfg.MPI_rankNeighbours = ranks;
+    cfg.TransformMatrixOfInterface = tf;
+    cfg.RangeOfInterface = rng;
+    cfg.DonorRangeOfInterface = drng;
+    cfg.Translation = tr;
+    cfg.RotationCenter = rc;
+    cfg.RotationAngle = ra;
+    cfg.MPI_rank = b;
+    cfg.MPI_size = g_job->nblocks;
+    for (int c = 0; c < MESHDIMENSIONS; c++) cfg.offset[c] = 0;
+}
+
+static int mr_body(int rank, void *arg)
+{
+    g_job = (const mr_job *)arg;
+    g_rank_blk = rank;
+    for (int i = 0; i < 6; i++) {
+        mr_tf[i] = calloc(3, sizeof(int));
+        mr_rng[i] = calloc(6, sizeof(cgsize_t));
+        mr_drng[i] = calloc(6, sizeof(cgsize_t));
+        mr_tr[i] = calloc(3, sizeof(float));
+        mr_rc[i] = calloc(3, sizeof(float));
+        mr_ra[i] = calloc(3, sizeof(float));
+    }
+    g_iface_hook = mr_interfaces;
+    const double *const *in = g_job->in + 8 * rank;
+    if (ref_init(&g_job->blk[rank], in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7])) return 1;
+    const int n = NG;
+    double *o = g_job->out + g_job->out_off[rank];
+    ref_get_geom(o);
+    if (g_job->nrhs) ref_rhs(o + 13 * (size_t)n);
+    ref_steps(g_job->nsteps);
+    ref_get_state(o + 18 * (size_t)n, 0);
+    return 0;
+}
+
+/* Runs the division on nblocks processes; out receives, per block at
+ * out_off[b], the geometry (13*NG), one right-hand side at the initial state
+ * (5*NG, when nrhs) and the state after nsteps steps (9*NG: rho,u,v,w,e,p,
+ * T,c,mue).  Returns 0 on success. */
+int refmpi_run(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const double *const *in,
+               int nrhs, int nsteps, double *out, const size_t *out_off, size_t out_len, size_t slot_bytes)
+{
+    double *shared = mmap(NULL, out_len * sizeof(double), PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
+    if (shared == MAP_FAILED) return -1;
+    mr_job job = {nblocks, blk, neigh, trans, in, nrhs, nsteps, shared, out_off};
+    int rc = shm_run(nblocks, slot_bytes, mr_body, &job);
+    memcpy(out, shared, out_len * sizeof(double));
+    munmap(shared, out_len * sizeof(double));
+    return rc;
 }
 #endif

@@ -296,3 +296,82 @@ class Oracle:
         g = np.zeros(13 * self.n)
         self.lib.oc_get_geom(self.h, _ptr(g))
         return g.reshape((13,) + self.shape)
+
+
+# ---------------------------------------------------------------------------
+# SHOCK's own code on several ranks (oracle/_ref/libshockmpi_*): the blocks of
+# a division (shock_b200.cases.split) as the ranks of one run, exchanging
+# their interfaces with SHOCK's TransferMeshParameter and
+# TransferFlowParameterWithGhosts over the forked shared-memory stand-in for
+# MPI (ref_harness/mpi_shm.c).  The ranks are forked from a fresh process
+# started with multiprocessing's "spawn" method, so no GPU context is ever
+# forked.
+# ---------------------------------------------------------------------------
+def multirank_available(order: int, dim: int) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", f"libshockmpi_w{order}_{dim}d.so"))
+
+
+def _ref_params(case) -> "RefParams":
+    p = RefParams()
+    p.ni, p.nj, p.nk = case.ni, case.nj, (case.nk if case.dim == 3 else 1)
+    p.time_order = case.time_order
+    p.tau, p.mach, p.reynolds = case.tau, case.mach, case.reynolds
+    p.prandtl, p.gamma, p.gas_r, p.t0, p.l0 = case.prandtl, case.gamma, case.gas_r, case.t0, case.l0
+    p.inviscid = int(case.inviscid)
+    p.mms = 0
+    p.mms_case = 0
+    for a in range(3):
+        p.periodic[a] = 0
+        p.period[a] = 0.0
+    for f in range(6):
+        p.bc[f] = int(case.bc[f])
+    p.t_wall = float(case.t_wall)
+    p.rho_inflow, p.p_inflow, p.p_outflow = float(case.rho_inflow), float(case.p_inflow), float(case.p_outflow)
+    for a in range(3):
+        p.u_inflow[a] = float(case.u_inflow[a])
+    return p
+
+
+def _multirank_worker(division, nsteps, rhs):
+    case = division.case
+    lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockmpi_w{case.order}_{case.dim}d.so"), mode=os.RTLD_LOCAL)
+    lib.refmpi_run.restype = C.c_int
+    nb = len(division.blocks)
+    g2 = case.order + 1
+    shapes = [(b.ni + g2, b.nj + g2, (b.nk + g2) if case.dim == 3 else 1) for b in division.blocks]
+    ng = [s[0] * s[1] * s[2] for s in shapes]
+    off = np.zeros(nb, dtype=np.uint64)
+    for b in range(1, nb):
+        off[b] = off[b - 1] + 27 * ng[b - 1]
+    total = int(off[-1]) + 27 * ng[-1]
+    params = (RefParams * nb)(*[_ref_params(b) for b in division.blocks])
+    f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
+    keep = [[f(a) for a in b.real_fields()] for b in division.blocks]
+    ptrs = (C.POINTER(C.c_double) * (8 * nb))(*[_ptr(a) for fl in keep for a in fl])
+    neigh = np.ascontiguousarray(division.neighbour, dtype=np.int32)
+    trans = np.ascontiguousarray(division.translation, dtype=np.float32)
+    out = np.zeros(total)
+    face = max(max(s[0] * s[1], s[1] * s[2], s[0] * s[2]) for s in shapes)
+    slot = 13 * (g2 // 2) * face * 8
+    rc = lib.refmpi_run(C.c_int(nb), params, neigh.ctypes.data_as(C.POINTER(C.c_int)),
+                        trans.ctypes.data_as(C.POINTER(C.c_float)), ptrs, C.c_int(int(rhs)), C.c_int(nsteps),
+                        _ptr(out), off.ctypes.data_as(C.POINTER(C.c_size_t)), C.c_size_t(total), C.c_size_t(slot))
+    if rc != 0:
+        raise RuntimeError(f"multi-rank reference run failed ({rc})")
+    res = []
+    for b in range(nb):
+        o, n = int(off[b]), ng[b]
+        res.append({"geometry": out[o:o + 13 * n].reshape((13,) + shapes[b]),
+                    "rhs": out[o + 13 * n:o + 18 * n].reshape((5,) + shapes[b]),
+                    "state": out[o + 18 * n:o + 27 * n].reshape((9,) + shapes[b])})
+    return res
+
+
+def run_multirank(division, nsteps: int, rhs: bool = False):
+    """Per block: geometry (13, ghosted), one right-hand side at the initial
+    state (5, when rhs) and the state after nsteps steps (9: rho,u,v,w,e,p,
+    T,c,mue) of SHOCK's own multi-rank run of the division."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        return pool.apply(_multirank_worker, (division, nsteps, rhs))

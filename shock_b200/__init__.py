@@ -105,6 +105,10 @@ def lib():
                          "shock_device_bytes", "shock_last_step_ms", "shock_kernels_per_step",
                          "shock_mms_baseline", "shock_set_kernel_timing", "shock_kernel_times", "shock_measure_fma_peak",
                          "shock_set_tau", "shock_get_tau", "shock_download_pressure",
+                         "shock_multi_create", "shock_multi_destroy", "shock_multi_dims", "shock_multi_geometry",
+                         "shock_multi_step", "shock_multi_rhs", "shock_multi_download_state",
+                         "shock_multi_upload_state", "shock_multi_set_tau", "shock_multi_check_nan",
+                         "shock_multi_info", "shock_host_multi_geometry",
                          "shock_host_geometry", "shock_host_mms_baseline", "shock_rhs_static",
                          "shock_batch_create", "shock_batch_destroy", "shock_batch_member_bytes",
                          "shock_batch_add", "shock_batch_remove", "shock_batch_step", "shock_batch_step_async",
@@ -122,6 +126,9 @@ def lib():
             L.shock_server_submit.argtypes = [C.c_void_p, C.POINTER(Params)] + [_dp] * 8 + [
                 C.c_int, C.POINTER(C.c_longlong)]
             L.shock_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_double]
+            L.shock_multi_create.argtypes = [C.POINTER(Params), C.c_int, C.c_void_p, C.c_int,
+                                             C.POINTER(C.c_void_p)]
+            L.shock_host_multi_geometry.argtypes = [C.POINTER(Params), C.c_int, C.c_void_p, C.c_void_p]
             L.shock_server_result.argtypes = [C.c_void_p, C.c_longlong, _dp, C.c_size_t, C.c_void_p]
             _lib = L
         return _lib
@@ -348,6 +355,129 @@ class Solver:
         if c.dim == 3:
             return a[..., g[0]:g[0] + c.ni, g[1]:g[1] + c.nj, g[2]:g[2] + c.nk]
         return a[..., g[0]:g[0] + c.ni, g[1]:g[1] + c.nj, :]
+
+
+class Block(C.Structure):
+    """Mirror of struct shock_block (include/shock_b200.h)."""
+    _fields_ = [("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int), ("bc", C.c_int * 6),
+                ("neighbour", C.c_int * 6), ("translation", (C.c_float * 3) * 6)] + \
+               [(n, _dp) for n in ("x", "y", "z", "u", "v", "w", "p", "rho")]
+
+
+def _division_blocks(division):
+    """(Block array, kept field arrays) of a division for the C ABI."""
+    case = division.case
+    f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
+    nb = len(division.blocks)
+    arr = (Block * nb)()
+    keep = []
+    for b, bc in enumerate(division.blocks):
+        B = arr[b]
+        B.ni, B.nj, B.nk = bc.ni, bc.nj, (bc.nk if case.dim == 3 else 1)
+        for q in range(6):
+            B.bc[q] = int(bc.bc[q])
+            B.neighbour[q] = int(division.neighbour[b, q])
+            for c in range(3):
+                B.translation[q][c] = float(division.translation[b, q, c])
+        fields = [f(a) for a in bc.real_fields()]
+        keep.append(fields)
+        for name, a in zip(("x", "y", "z", "u", "v", "w", "p", "rho"), fields):
+            setattr(B, name, _ptr(a))
+    return arr, keep
+
+
+def host_multi_geometry(division):
+    """Per block geometry (13, ghosted) of a division, built on the host with
+    the interfaces exchanged as SHOCK's ranks exchange them (no device)."""
+    case = division.case
+    arr, keep = _division_blocks(division)
+    g2 = case.order + 1
+    outs = [np.zeros((13, b.ni + g2, b.nj + g2, (b.nk + g2) if case.dim == 3 else 1)) for b in division.blocks]
+    ptrs = (_dp * len(outs))(*[_ptr(o) for o in outs])
+    p = params_from_case(case)
+    _check(lib().shock_host_multi_geometry(C.byref(p), len(outs), arr, ptrs))
+    return outs
+
+
+class Multi:
+    """The blocks of a division (shock_b200.cases.split) on one device,
+    their interfaces exchanged on the device before every stage, as SHOCK's
+    ranks exchange them (shock_multi_*)."""
+
+    def __init__(self, division, precision=SHOCK_FP64, device: int = 0, zeta_fix: bool = False,
+                 weno_eps: float = 0.0):
+        self.division = division
+        self.lib = lib()
+        case = division.case
+        self.params = params_from_case(case, precision, zeta_fix, weno_eps)
+        nb = len(division.blocks)
+        arr, self._keep = _division_blocks(division)
+        h = C.c_void_p()
+        _check(self.lib.shock_multi_create(C.byref(self.params), nb, arr, int(device), C.byref(h)))
+        self.h = h
+        self._keep = None
+        self.nblocks = nb
+        self.shapes, self.starts = [], []
+        for b in range(nb):
+            d = (C.c_int * 6)()
+            _check(self.lib.shock_multi_dims(self.h, b, d))
+            self.shapes.append((d[0], d[1], d[2]))
+            self.starts.append((d[3], d[4], d[5]))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.lib.shock_multi_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _n(self, b):
+        s = self.shapes[b]
+        return s[0] * s[1] * s[2]
+
+    def steps(self, n: int):
+        _check(self.lib.shock_multi_step(self.h, C.c_int(n)))
+
+    def rhs(self, b: int) -> np.ndarray:
+        q = np.zeros(5 * self._n(b))
+        _check(self.lib.shock_multi_rhs(self.h, int(b), _ptr(q)))
+        return q.reshape((5,) + self.shapes[b])
+
+    def state(self, b: int) -> np.ndarray:
+        s = np.zeros(5 * self._n(b))
+        _check(self.lib.shock_multi_download_state(self.h, int(b), _ptr(s)))
+        return s.reshape((5,) + self.shapes[b])
+
+    def geometry(self, b: int) -> np.ndarray:
+        g = np.zeros(13 * self._n(b))
+        _check(self.lib.shock_multi_geometry(self.h, int(b), _ptr(g)))
+        return g.reshape((13,) + self.shapes[b])
+
+    def set_tau(self, tau: float):
+        _check(self.lib.shock_multi_set_tau(self.h, C.c_double(tau)))
+
+    def info(self) -> dict:
+        nb, nk, ms = C.c_int(), C.c_int(), C.c_float()
+        _check(self.lib.shock_multi_info(self.h, C.byref(nb), C.byref(nk), C.byref(ms)))
+        return {"blocks": nb.value, "kernels_per_step": nk.value, "last_ms": ms.value}
+
+    def assemble(self, per_block):
+        """The whole block's real points from per-block ghosted arrays
+        (leading axis kept), for comparison with a single-block solve."""
+        case = self.division.case
+        g = case.ghosts
+        lead = per_block[0].shape[0]
+        out = np.zeros((lead, case.ni, case.nj, case.nk if case.dim == 3 else 1))
+        for b, a in enumerate(per_block):
+            bc, lo = self.division.blocks[b], self.division.lo[b]
+            k0 = g if case.dim == 3 else 0
+            out[:, lo[0]:lo[0] + bc.ni, lo[1]:lo[1] + bc.nj, lo[2]:lo[2] + (bc.nk if case.dim == 3 else 1)] = \
+                a[:, g:g + bc.ni, g:g + bc.nj, k0:k0 + (bc.nk if case.dim == 3 else 1)]
+        return out
 
 
 class BatchTuning(C.Structure):

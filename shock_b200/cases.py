@@ -465,3 +465,67 @@ def serving_stream(count: int, seed: int = 5, rate: float = 200.0, min_points: i
                 vortex_column(n, n, beta, mach, order=order, reynolds=re)
         out.append((t, case, nsteps))
     return out
+
+
+@dataclasses.dataclass
+class Division:
+    """A Cartesian division of one block into parts[0] x parts[1] (x parts[2])
+    blocks, as SHOCK's .sddc division files describe one (the layout
+    TOOLS/generatedivfile/generatedivfile_3.c writes): block rank
+    r = (k * parts[1] + j) * parts[0] + i, each with its real-point slice of
+    the case, the block across each face (Left, Right, Bottom, Top, Behind,
+    InFront; -1 at a face of the whole block that is not periodic, which
+    keeps the case's face type) and the float32 Translation the face adds to
+    coordinates it receives (minus / plus the period where a periodic axis
+    wraps around)."""
+    case: Case
+    parts: Tuple[int, int, int]
+    blocks: list                    # Case per block (sizes, fields; periodic False; bc on outer faces)
+    neighbour: np.ndarray           # (nblocks, 6) int
+    translation: np.ndarray         # (nblocks, 6, 3) float32
+    lo: np.ndarray                  # (nblocks, 3) first real index of each block in the whole block
+
+
+def split(case: Case, parts: Tuple[int, ...]) -> Division:
+    parts = tuple(parts) + (1,) * (3 - len(parts))
+    if case.dim == 2:
+        parts = (parts[0], parts[1], 1)
+    n = (case.ni, case.nj, case.nk if case.dim == 3 else 1)
+    cuts = []
+    for a in range(3):
+        q, r = divmod(n[a], parts[a])
+        sizes = [q + (1 if i < r else 0) for i in range(parts[a])]
+        cuts.append(np.concatenate([[0], np.cumsum(sizes)]).astype(int))
+    nb = parts[0] * parts[1] * parts[2]
+    neigh = -np.ones((nb, 6), dtype=np.int32)
+    trans = np.zeros((nb, 6, 3), dtype=np.float32)
+    lo = np.zeros((nb, 3), dtype=np.int64)
+    blocks = []
+    for k in range(parts[2]):
+        for j in range(parts[1]):
+            for i in range(parts[0]):
+                r = (k * parts[1] + j) * parts[0] + i
+                idx = (i, j, k)
+                sl = tuple(slice(cuts[a][idx[a]], cuts[a][idx[a] + 1]) for a in range(3))
+                lo[r] = [cuts[a][idx[a]] for a in range(3)]
+                bc = [0] * 6
+                for a in range(case.dim):
+                    for side in (0, 1):
+                        f = 2 * a + side
+                        m = list(idx)
+                        m[a] += 1 if side else -1
+                        if 0 <= m[a] < parts[a]:
+                            neigh[r, f] = (m[2] * parts[1] + m[1]) * parts[0] + m[0]
+                        elif case.periodic[a]:
+                            m[a] %= parts[a]
+                            neigh[r, f] = (m[2] * parts[1] + m[1]) * parts[0] + m[0]
+                            trans[r, f, a] = np.float32(case.period[a] if side else -case.period[a])
+                        else:
+                            bc[f] = case.bc[f]
+                sub = case.replace(ni=int(sl[0].stop - sl[0].start), nj=int(sl[1].stop - sl[1].start),
+                                   nk=int(sl[2].stop - sl[2].start) if case.dim == 3 else 1,
+                                   x=case.x[sl], y=case.y[sl], z=case.z[sl], rho=case.rho[sl], u=case.u[sl],
+                                   v=case.v[sl], w=case.w[sl], p=case.p[sl], periodic=(False, False, False),
+                                   bc=tuple(bc), name=f"{case.name}_b{r}")
+                blocks.append(sub)
+    return Division(case=case, parts=parts, blocks=blocks, neighbour=neigh, translation=trans, lo=lo)

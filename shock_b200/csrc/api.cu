@@ -65,6 +65,7 @@ struct shock_ctx {
     Fields F{};
     int device = 0;
     cudaStream_t stream = nullptr;
+    bool own_stream = true;   // false for the blocks of a division (they share its stream)
     double *pool = nullptr;
     size_t pool_bytes = 0;
     double *buf[3][5] = {};
@@ -255,6 +256,8 @@ static int final_buffer(const shock_ctx *c, int un)
 
 extern "C" {
 
+static int ctx_setup(shock_ctx *c, HostBlock &hb, const double *pr, cudaStream_t stream);
+
 const char *shock_last_error(void) { return g_err.c_str(); }
 
 int shock_device_count(int *n)
@@ -266,7 +269,7 @@ int shock_device_count(int *n)
 // Every face: periodic (SHOCK_BC_AUTO on a periodic axis), a
 // manufactured-solution Dirichlet face (SHOCK_BC_AUTO with mms), or one of
 // the wall / farfield types.
-static int check_faces(const shock_params *p)
+static int check_faces(const shock_params *p, unsigned iface = 0u)
 {
     // SHOCK takes one inflow and one outflow option per run (src/Import.c:62-87)
     int inflow = 0, outflow = 0, in_axes = 0, rudy_axes = 0;
@@ -299,8 +302,10 @@ static int check_faces(const shock_params *p)
                 return fail(SHOCK_EINVAL, "face %d: inflow needs rho_inflow > 0 and p_inflow > 0", f);
             if (p->periodic[a] && b != SHOCK_BC_AUTO)
                 return fail(SHOCK_EINVAL, "face %d: a periodic axis takes SHOCK_BC_AUTO", f);
-            if (!p->periodic[a] && b == SHOCK_BC_AUTO && !p->mms)
-                return fail(SHOCK_EINVAL, "face %d: neither periodic, a manufactured-solution face nor a bc", f);
+            if ((iface >> f & 1u) && b != SHOCK_BC_AUTO)
+                return fail(SHOCK_EINVAL, "face %d: an interface face takes SHOCK_BC_AUTO", f);
+            if (!p->periodic[a] && b == SHOCK_BC_AUTO && !p->mms && !(iface >> f & 1u))
+                return fail(SHOCK_EINVAL, "face %d: neither periodic, an interface, a manufactured-solution face nor a bc", f);
             if (p->mms && b != SHOCK_BC_AUTO)
                 return fail(SHOCK_EINVAL, "face %d: the manufactured solution sets every non-periodic face", f);
         }
@@ -330,6 +335,20 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
     c->device = device;
     HostBlock hb;
     build_block(*p, x, y, z, u, v, w, pr, rho, hb);
+    const int rc = ctx_setup(c, hb, pr, nullptr);
+    if (rc) return rc;
+    *out = c;
+    return SHOCK_OK;
+}
+
+// Device set-up of a context whose p and device are set, from its host-built
+// block (geometry and initial state) and the block's real-point pressure
+// (Fortran order).  stream: the stream to run on (nullptr: a stream of its
+// own).  On failure the context is freed.
+static int ctx_setup(shock_ctx *c, HostBlock &hb, const double *pr, cudaStream_t stream)
+{
+    const shock_params *p = &c->p;
+    const int device = c->device;
     c->L = hb.L;
     c->G = make_grid(c->L, *p);
     Grid &G = c->G;
@@ -365,7 +384,12 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
         return fail(SHOCK_ENOMEM, "flag allocation");
     }
     prepare_kernels();
-    cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (stream) {
+        c->stream = stream;
+        c->own_stream = false;
+    } else {
+        cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    }
     cudaEventCreate(&c->ev0);
     cudaEventCreate(&c->ev1);
 
@@ -415,7 +439,6 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
         shock_destroy(c);
         return fail(SHOCK_ECUDA, "set-up upload: %s", cudaGetErrorString(e));
     }
-    *out = c;
     return SHOCK_OK;
 }
 
@@ -433,7 +456,7 @@ int shock_destroy(shock_ctx *c)
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     for (auto e : c->tev) cudaEventDestroy(e);
-    if (c->stream) cudaStreamDestroy(c->stream);
+    if (c->stream && c->own_stream) cudaStreamDestroy(c->stream);
     delete c;
     return SHOCK_OK;
 }
@@ -794,6 +817,375 @@ int shock_measure_fma_peak(int device, double *fp64_tflops, double *fp32_tflops)
     *fp32_tflops = fma_probe(0, prop.multiProcessorCount, s);
     cudaStreamDestroy(s);
     CK(cudaGetLastError());
+    return SHOCK_OK;
+}
+
+// ---------------------------------------------------------------------------
+// Blocks of a division on one device (shock_multi_*): every block is a
+// context on the division's stream; before each stage's CalcValues the
+// blocks exchange their interface layers in SHOCK's passes (one, or two / three
+// with viscous terms in 2D / 3D, src/Functions.c:2117-2136), each pass all
+// packs before all unpacks, as the ranks of an MPI run exchange them
+// (src/Functions.c:3580-3684).
+// ---------------------------------------------------------------------------
+}  // extern "C"
+
+struct shock_multi {
+    shock_params p{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<shock_ctx *> blk;
+    std::vector<BlockLink> links;
+    XFace *faces[3] = {nullptr, nullptr, nullptr};   // exchange tables for state buffer 0, 1, 2
+    int nfaces = 0;
+    long long most = 0, total = 0;
+    double *stage = nullptr;
+    int npass = 1;
+    int un = 0;
+    cudaGraphExec_t step_graph[3] = {nullptr, nullptr, nullptr};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.f;
+    int kernels_per_step = 0;
+};
+
+static void multi_exchange(shock_multi *m, int cur, int &nk)
+{
+    for (int pass = 0; pass < m->npass; pass++) {
+        launch_exchange_pass(m->faces[cur], m->nfaces, m->most, m->total, m->stage, m->stream);
+        if (m->nfaces) nk += 2;
+    }
+}
+
+static void multi_enqueue_step(shock_multi *m, int un, int &nk)
+{
+    int cur = un;
+    for (int st = 0; st < m->p.time_order; st++) {
+        int out = 0;
+        while (out == un || out == cur) out++;
+        multi_exchange(m, cur, nk);
+        for (shock_ctx *c : m->blk) enqueue_rhs(c, c->buf[cur], nk);
+        for (shock_ctx *c : m->blk) {
+            const double *cin[5] = {c->buf[cur][0], c->buf[cur][1], c->buf[cur][2], c->buf[cur][3], c->buf[cur][4]};
+            Fields F = c->F;
+            for (int q = 0; q < 5; q++) F.Un[q] = c->buf[un][q];
+            launch_rk(c->G, c->rk[st], c->p.tau, cin, c->buf[out], F, c->has_source, m->stream);
+            nk++;
+        }
+        cur = out;
+    }
+    for (shock_ctx *c : m->blk)
+        if (c->plast_pool) {
+            launch_bc_save(c->G, c->F.p, c->plast, m->stream);
+            nk++;
+        }
+}
+
+extern "C" {
+
+int shock_multi_destroy(shock_multi *m)
+{
+    if (!m) return SHOCK_OK;
+    cudaSetDevice(m->device);
+    if (m->stream) cudaStreamSynchronize(m->stream);
+    for (int i = 0; i < 3; i++)
+        if (m->step_graph[i]) cudaGraphExecDestroy(m->step_graph[i]);
+    for (shock_ctx *c : m->blk) shock_destroy(c);
+    for (int i = 0; i < 3; i++)
+        if (m->faces[i]) cudaFree(m->faces[i]);
+    if (m->stage) cudaFree(m->stage);
+    if (m->ev0) cudaEventDestroy(m->ev0);
+    if (m->ev1) cudaEventDestroy(m->ev1);
+    if (m->stream) cudaStreamDestroy(m->stream);
+    delete m;
+    return SHOCK_OK;
+}
+
+int shock_multi_create(const shock_params *p, int nblocks, const shock_block *blocks, int device, shock_multi **out)
+{
+    if (!p || !blocks || !out || nblocks < 1) return fail(SHOCK_EINVAL, "bad argument");
+    if (p->dim != 2 && p->dim != 3) return fail(SHOCK_EINVAL, "dim must be 2 or 3");
+    if (p->order != 5 && p->order != 9) return fail(SHOCK_EINVAL, "order must be 5 or 9");
+    if (p->time_order != 3 && p->time_order != 4) return fail(SHOCK_EINVAL, "time_order must be 3 or 4");
+    if (p->precision != SHOCK_FP64 && p->precision != SHOCK_MIXED) return fail(SHOCK_EINVAL, "bad precision");
+    if (p->mms) return fail(SHOCK_EINVAL, "a division takes no manufactured solution");
+    if (p->mach <= 0 || p->reynolds <= 0 || p->gamma <= 1.0 || p->tau <= 0) return fail(SHOCK_EINVAL, "bad physics");
+    if (!(p->weno_eps >= 0)) return fail(SHOCK_EINVAL, "weno_eps must be >= 0");
+    const int dim = p->dim, g = (p->order + 1) / 2;
+    std::vector<shock_params> ps(nblocks, *p);
+    std::vector<BlockLink> links(nblocks);
+    std::vector<const double *> in(8 * (size_t)nblocks);
+    for (int b = 0; b < nblocks; b++) {
+        const shock_block &B = blocks[b];
+        shock_params &q = ps[b];
+        q.ni = B.ni; q.nj = B.nj; q.nk = dim == 3 ? B.nk : 1;
+        if (q.ni < g + 1 || q.nj < g + 1 || (dim == 3 && q.nk < g + 1))
+            return fail(SHOCK_EINVAL, "block %d smaller than the stencil (%d points per axis needed)", b, g + 1);
+        if (dim == 3 && !p->inviscid && !p->zeta_fix && q.nj > q.nk)
+            return fail(SHOCK_EINVAL, "block %d: zeta viscous stencil centred on j needs nj <= nk (src/ZD.c:547-548)", b);
+        if (!B.x || !B.y || (dim == 3 && !B.z) || !B.u || !B.v || !B.w || !B.p || !B.rho)
+            return fail(SHOCK_EINVAL, "block %d: null field", b);
+        unsigned iface = 0u;
+        for (int a = 0; a < 3; a++) { q.periodic[a] = 0; q.period[a] = 0.0; }
+        for (int f = 0; f < 6; f++) {
+            const int nb = f < 2 * dim ? B.neighbour[f] : -1;
+            if (nb < -1 || nb >= nblocks) return fail(SHOCK_EINVAL, "block %d face %d: no block %d", b, f, nb);
+            links[b].neighbour[f] = nb;
+            for (int c = 0; c < 3; c++) links[b].translation[f][c] = B.translation[f][c];
+            q.bc[f] = f < 2 * dim ? B.bc[f] : SHOCK_BC_AUTO;
+            if (nb >= 0) iface |= 1u << f;
+        }
+        if (int rc = check_faces(&q, iface)) return fail(rc, "block %d: %s", b, g_err.c_str());
+        const double *f8[8] = {B.x, B.y, dim == 3 ? B.z : B.x, B.u, B.v, B.w, B.p, B.rho};
+        for (int k = 0; k < 8; k++) in[8 * (size_t)b + k] = f8[k];
+    }
+    // the faces that touch: the neighbour's opposite face names this block,
+    // and their lateral extents agree (identity orientation)
+    for (int b = 0; b < nblocks; b++)
+        for (int f = 0; f < 2 * dim; f++) {
+            const int nb = links[b].neighbour[f];
+            if (nb < 0) continue;
+            if (links[nb].neighbour[f ^ 1] != b)
+                return fail(SHOCK_EINVAL, "block %d face %d: block %d's opposite face does not name it back", b, f, nb);
+            const int n0[3] = {ps[b].ni, ps[b].nj, ps[b].nk}, n1[3] = {ps[nb].ni, ps[nb].nj, ps[nb].nk};
+            for (int a = 0; a < dim; a++)
+                if (a != f / 2 && n0[a] != n1[a])
+                    return fail(SHOCK_EINVAL, "block %d face %d: %d points along axis %d, block %d has %d", b, f, n0[a],
+                                a, nb, n1[a]);
+            if (n1[f / 2] < g) return fail(SHOCK_EINVAL, "block %d: fewer real layers than ghost layers", nb);
+        }
+    std::vector<HostBlock> hbs;
+    build_blocks(ps, in, links, hbs);
+
+    shock_multi *m = new shock_multi();
+    m->p = *p;
+    m->device = device;
+    m->links = links;
+    m->npass = p->inviscid ? 1 : (dim == 3 ? 3 : 2);
+    if (cudaSetDevice(device) != cudaSuccess) { delete m; return fail(SHOCK_ECUDA, "cudaSetDevice(%d)", device); }
+    cudaStreamCreateWithFlags(&m->stream, cudaStreamNonBlocking);
+    cudaEventCreate(&m->ev0);
+    cudaEventCreate(&m->ev1);
+    for (int b = 0; b < nblocks; b++) {
+        shock_ctx *c = new shock_ctx();
+        c->p = ps[b];
+        c->device = device;
+        const int rc = ctx_setup(c, hbs[b], blocks[b].p, m->stream);
+        std::vector<std::vector<double>>().swap(hbs[b].geo);
+        std::vector<std::vector<double>>().swap(hbs[b].prim);
+        if (rc) { shock_multi_destroy(m); return rc; }
+        m->blk.push_back(c);
+    }
+    // exchange tables, one per state buffer
+    std::vector<XFace> xf[3];
+    for (int b = 0; b < nblocks; b++)
+        for (int f = 0; f < 2 * dim; f++) {
+            const int nb = links[b].neighbour[f];
+            if (nb < 0) continue;
+            const Layout &R = m->blk[b]->L, &S = m->blk[nb]->L;
+            int rlo[3], rhi[3], slo[3], shi[3];
+            face_region(R, f, false, rlo, rhi);
+            face_region(S, f ^ 1, true, slo, shi);
+            XFace x{};
+            long long n = 1;
+            for (int a = 0; a < 3; a++) {
+                x.ext[a] = rhi[a] - rlo[a] + 1;
+                x.rlo[a] = rlo[a];
+                x.slo[a] = slo[a];
+                x.rst[a] = R.st[a];
+                x.sst[a] = S.st[a];
+                n *= x.ext[a];
+            }
+            x.off = m->total;
+            m->total += n;
+            if (n > m->most) m->most = n;
+            for (int u = 0; u < 3; u++) {
+                for (int q = 0; q < 5; q++) {
+                    x.src[q] = m->blk[nb]->buf[u][q];
+                    x.dst[q] = m->blk[b]->buf[u][q];
+                }
+                xf[u].push_back(x);
+            }
+        }
+    m->nfaces = (int)xf[0].size();
+    if (m->nfaces) {
+        if (cudaMalloc(&m->stage, sizeof(double) * 5 * (size_t)m->total) != cudaSuccess) {
+            shock_multi_destroy(m);
+            return fail(SHOCK_ENOMEM, "exchange staging buffer");
+        }
+        for (int u = 0; u < 3; u++) {
+            if (cudaMalloc(&m->faces[u], sizeof(XFace) * m->nfaces) != cudaSuccess) {
+                shock_multi_destroy(m);
+                return fail(SHOCK_ENOMEM, "exchange tables");
+            }
+            cudaMemcpy(m->faces[u], xf[u].data(), sizeof(XFace) * m->nfaces, cudaMemcpyHostToDevice);
+        }
+    }
+    CK(cudaDeviceSynchronize());
+    *out = m;
+    return SHOCK_OK;
+}
+
+int shock_host_multi_geometry(const shock_params *p, int nblocks, const shock_block *blocks, double *const *out13)
+{
+    if (!p || !blocks || !out13 || nblocks < 1) return fail(SHOCK_EINVAL, "bad argument");
+    std::vector<shock_params> ps(nblocks, *p);
+    std::vector<BlockLink> links(nblocks);
+    std::vector<const double *> in(8 * (size_t)nblocks);
+    std::vector<double> zero;
+    for (int b = 0; b < nblocks; b++) {
+        const shock_block &B = blocks[b];
+        shock_params &q = ps[b];
+        q.ni = B.ni; q.nj = B.nj; q.nk = p->dim == 3 ? B.nk : 1;
+        if (!B.x || !B.y || (p->dim == 3 && !B.z)) return fail(SHOCK_EINVAL, "block %d: null coordinates", b);
+        for (int a = 0; a < 3; a++) { q.periodic[a] = 0; q.period[a] = 0.0; }
+        for (int f = 0; f < 6; f++) {
+            const int nb = f < 2 * p->dim ? B.neighbour[f] : -1;
+            if (nb < -1 || nb >= nblocks) return fail(SHOCK_EINVAL, "block %d face %d: no block %d", b, f, nb);
+            links[b].neighbour[f] = nb;
+            for (int c = 0; c < 3; c++) links[b].translation[f][c] = B.translation[f][c];
+            q.bc[f] = f < 2 * p->dim ? B.bc[f] : SHOCK_BC_AUTO;
+        }
+        const size_t nr = (size_t)q.ni * q.nj * q.nk;
+        if (zero.size() < nr) zero.assign(nr, 0.0);
+        in[8 * (size_t)b + 0] = B.x;
+        in[8 * (size_t)b + 1] = B.y;
+        in[8 * (size_t)b + 2] = p->dim == 3 ? B.z : B.x;
+    }
+    std::vector<std::vector<double>> ones(nblocks);
+    for (int b = 0; b < nblocks; b++) {
+        const size_t nr = (size_t)ps[b].ni * ps[b].nj * ps[b].nk;
+        ones[b].assign(nr, 1.0);
+        for (int k = 3; k < 6; k++) in[8 * (size_t)b + k] = zero.data();
+        in[8 * (size_t)b + 6] = ones[b].data();
+        in[8 * (size_t)b + 7] = ones[b].data();
+    }
+    std::vector<HostBlock> hbs;
+    build_blocks(ps, in, links, hbs);
+    for (int b = 0; b < nblocks; b++)
+        for (int f = 0; f < 13; f++)
+            memcpy(out13[b] + (size_t)f * hbs[b].L.NG, hbs[b].geo[f].data(), sizeof(double) * hbs[b].L.NG);
+    return SHOCK_OK;
+}
+
+int shock_multi_dims(const shock_multi *m, int block, int out6[6])
+{
+    if (!m || block < 0 || block >= (int)m->blk.size()) return fail(SHOCK_EINVAL, "bad block");
+    return shock_dims(m->blk[block], out6);
+}
+
+int shock_multi_geometry(shock_multi *m, int block, double *out13)
+{
+    if (!m || block < 0 || block >= (int)m->blk.size()) return fail(SHOCK_EINVAL, "bad block");
+    return shock_geometry(m->blk[block], out13);
+}
+
+int shock_multi_step(shock_multi *m, int nsteps)
+{
+    if (!m || nsteps < 0) return fail(SHOCK_EINVAL, "bad argument");
+    CK(cudaSetDevice(m->device));
+    CK(cudaEventRecord(m->ev0, m->stream));
+    for (int it = 0; it < nsteps; it++) {
+        const int un = m->un;
+        if (!m->step_graph[un]) {
+            cudaGraph_t gr;
+            CK(cudaStreamBeginCapture(m->stream, cudaStreamCaptureModeThreadLocal));
+            int nk = 0;
+            for (shock_ctx *c : m->blk)
+                for (int q = 0; q < 5; q++) CK(cudaMemsetAsync(c->F.Qs[q], 0, sizeof(double) * c->G.NG, m->stream));
+            multi_enqueue_step(m, un, nk);
+            CK(cudaStreamEndCapture(m->stream, &gr));
+            CK(cudaGraphInstantiate(&m->step_graph[un], gr, 0));
+            cudaGraphDestroy(gr);
+            m->kernels_per_step = nk;
+        }
+        CK(cudaGraphLaunch(m->step_graph[un], m->stream));
+        const int last = last_stage_input(m->blk[0], un), fin = final_buffer(m->blk[0], un);
+        for (shock_ctx *c : m->blk) { c->un = fin; c->last_in = last; }
+        m->un = fin;
+    }
+    CK(cudaEventRecord(m->ev1, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    CK(cudaGetLastError());
+    cudaEventElapsedTime(&m->last_ms, m->ev0, m->ev1);
+    return SHOCK_OK;
+}
+
+int shock_multi_rhs(shock_multi *m, int block, double *q5)
+{
+    if (!m || !q5 || block < 0 || block >= (int)m->blk.size()) return fail(SHOCK_EINVAL, "bad argument");
+    CK(cudaSetDevice(m->device));
+    int nk = 0;
+    multi_exchange(m, m->un, nk);
+    for (shock_ctx *c : m->blk) enqueue_rhs(c, c->buf[m->un], nk);
+    CK(cudaGetLastError());
+    shock_ctx *c = m->blk[block];
+    const size_t nb = sizeof(double) * c->G.NG;
+    for (int f = 0; f < 5; f++) CK(cudaMemcpyAsync(q5 + (size_t)f * c->G.NG, c->F.Q[f], nb, cudaMemcpyDeviceToHost, m->stream));
+    CK(cudaStreamSynchronize(m->stream));
+    return SHOCK_OK;
+}
+
+int shock_multi_download_state(shock_multi *m, int block, double *prim5)
+{
+    if (!m || block < 0 || block >= (int)m->blk.size()) return fail(SHOCK_EINVAL, "bad block");
+    return shock_download_state(m->blk[block], prim5, 0);
+}
+
+int shock_multi_upload_state(shock_multi *m, int block, const double *prim5)
+{
+    if (!m || block < 0 || block >= (int)m->blk.size()) return fail(SHOCK_EINVAL, "bad block");
+    if (m->un != 0) {
+        // the blocks keep one buffer rotation: bring every other block's
+        // state into buffer 0 first
+        for (shock_ctx *c : m->blk) {
+            if (c->un == 0) continue;
+            for (int q = 0; q < 5; q++)
+                CK(cudaMemcpyAsync(c->buf[0][q], c->buf[c->un][q], sizeof(double) * c->G.NG, cudaMemcpyDeviceToDevice,
+                                   m->stream));
+            c->un = 0;
+            c->last_in = 0;
+        }
+        CK(cudaStreamSynchronize(m->stream));
+        m->un = 0;
+    }
+    return shock_upload_state(m->blk[block], prim5);
+}
+
+int shock_multi_set_tau(shock_multi *m, double tau)
+{
+    if (!m) return fail(SHOCK_EINVAL, "null argument");
+    if (!(tau > 0) || !std::isfinite(tau)) return fail(SHOCK_EINVAL, "tau must be positive and finite");
+    if (tau == m->p.tau) return SHOCK_OK;
+    CK(cudaSetDevice(m->device));
+    CK(cudaStreamSynchronize(m->stream));
+    for (shock_ctx *c : m->blk)
+        if (int rc = shock_set_tau(c, tau)) return rc;
+    m->p.tau = tau;
+    for (int i = 0; i < 3; i++)
+        if (m->step_graph[i]) { cudaGraphExecDestroy(m->step_graph[i]); m->step_graph[i] = nullptr; }
+    return SHOCK_OK;
+}
+
+int shock_multi_check_nan(shock_multi *m, int *bad)
+{
+    if (!m || !bad) return fail(SHOCK_EINVAL, "null argument");
+    int total = 0;
+    for (shock_ctx *c : m->blk) {
+        int nb = 0;
+        const int rc = shock_check_nan(c, &nb);
+        if (rc && rc != SHOCK_ENAN) return rc;
+        total += nb;
+    }
+    *bad = total;
+    return total ? fail(SHOCK_ENAN, "%d non-finite densities", total) : SHOCK_OK;
+}
+
+int shock_multi_info(const shock_multi *m, int *nblocks, int *kernels_per_step, float *last_ms)
+{
+    if (!m) return fail(SHOCK_EINVAL, "null argument");
+    if (nblocks) *nblocks = (int)m->blk.size();
+    if (kernels_per_step) *kernels_per_step = m->kernels_per_step;
+    if (last_ms) *last_ms = m->last_ms;
     return SHOCK_OK;
 }
 

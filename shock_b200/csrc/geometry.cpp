@@ -116,9 +116,35 @@ void periodic_images(const Layout &L, const shock_params &p, double **f, int nf,
     }
 }
 
-int build_block(const shock_params &p, const double *x, const double *y, const double *z,
-                const double *u, const double *v, const double *w, const double *pr,
-                const double *rho, HostBlock &hb)
+namespace {
+
+// The +1 extended grid of a block (the *_extrapolate arrays,
+// src/Functions.c:6690-6848): the ghosted coordinates one point further out
+// on every side, its outermost layer extrapolated.
+struct ExtGrid {
+    Box e;
+    std::vector<double> xe, ye, ze;
+};
+
+// The block's ghosted coordinates into the interior of its extended grid.
+void copy_ext(const HostBlock &hb, ExtGrid &eg)
+{
+    const Layout &L = hb.L;
+    for (int i = 0; i < L.N[0]; i++)
+        for (int j = 0; j < L.N[1]; j++)
+            for (int k = 0; k < L.N[2]; k++) {
+                long long ee = eg.e.at(i + 1, j + 1, L.dim == 3 ? k + 1 : 0), o = L.at(i, j, k);
+                eg.xe[ee] = hb.geo[0][o];
+                eg.ye[ee] = hb.geo[1][o];
+                eg.ze[ee] = hb.geo[2][o];
+            }
+}
+
+// Initialize, the real points and the extrapolated ghost coordinates of one
+// block (src/Functions.c:746-877, 1327-1353, 6511-6848).
+void block_start(const shock_params &p, const double *x, const double *y, const double *z, const double *u,
+                 const double *v, const double *w, const double *pr, const double *rho, HostBlock &hb, Box &b,
+                 ExtGrid &eg)
 {
     const int dim = p.dim;
     Layout &L = hb.L;
@@ -155,7 +181,6 @@ int build_block(const shock_params &p, const double *x, const double *y, const d
                 hb.prim[4][o] = (0.5 * ((u[f] * u[f]) + (v[f] * v[f]) + (w[f] * w[f])) + pr[f] / rho[f] / (gm - 1.0) * ups);
             }
 
-    Box b;
     for (int a = 0; a < 3; a++) {
         b.sr[a] = a < dim ? L.g : 0;
         b.er[a] = a < dim ? L.g + L.n[a] - 1 : 0;
@@ -167,7 +192,7 @@ int build_block(const shock_params &p, const double *x, const double *y, const d
     if (dim == 3) extrapolate(Z, b, dim);
 
     // +1 extended grid (the *_extrapolate arrays, src/Functions.c:6690-6848).
-    Box e;
+    Box &e = eg.e;
     int NE[3];
     for (int a = 0; a < 3; a++) NE[a] = a < dim ? L.N[a] + 2 : 1;
     e.st[0] = (long long)NE[1] * NE[2]; e.st[1] = NE[2]; e.st[2] = 1;
@@ -177,27 +202,25 @@ int build_block(const shock_params &p, const double *x, const double *y, const d
         e.eg[a] = a < dim ? b.eg[a] + 2 : 0;
     }
     const long long NEtot = (long long)NE[0] * NE[1] * NE[2];
-    std::vector<double> xe(NEtot, 0.0), ye(NEtot, 0.0), ze(NEtot, 0.0);
-    auto copy_ext = [&]() {
-        for (int i = 0; i < L.N[0]; i++)
-            for (int j = 0; j < L.N[1]; j++)
-                for (int k = 0; k < L.N[2]; k++) {
-                    long long ee = e.at(i + 1, j + 1, dim == 3 ? k + 1 : 0), o = L.at(i, j, k);
-                    xe[ee] = X[o]; ye[ee] = Y[o]; ze[ee] = Z[o];
-                }
-    };
-    copy_ext();
-    extrapolate(xe, e, dim);
-    extrapolate(ye, e, dim);
-    if (dim == 3) extrapolate(ze, e, dim);
+    eg.xe.assign(NEtot, 0.0);
+    eg.ye.assign(NEtot, 0.0);
+    eg.ze.assign(NEtot, 0.0);
+    copy_ext(hb, eg);
+    extrapolate(eg.xe, e, dim);
+    extrapolate(eg.ye, e, dim);
+    if (dim == 3) extrapolate(eg.ze, e, dim);
+}
 
-    double *gf[13] = {X.data(), Y.data(), Z.data(), hb.geo[4].data(), hb.geo[5].data(), hb.geo[6].data(),
-                      hb.geo[7].data(), hb.geo[8].data(), hb.geo[9].data(), hb.geo[10].data(),
-                      hb.geo[11].data(), hb.geo[12].data(), hb.geo[3].data()};
-    for (int r = 0; r < dim; r++) periodic_images(L, p, gf, 13, 3);
-
-    // CreateMetric on the extended grid.
-    copy_ext();
+// CreateMetric (src/Functions.c:6388-6509) on the extended grid, after the
+// ghost coordinates have their interface / periodic values: J and the nine
+// metric terms on every ghosted point (3D cross terms zeroed, :6479-6484).
+void create_metric(const shock_params &p, HostBlock &hb, ExtGrid &eg)
+{
+    const int dim = p.dim;
+    const Layout &L = hb.L;
+    copy_ext(hb, eg);
+    const Box &e = eg.e;
+    const std::vector<double> &xe = eg.xe, &ye = eg.ye, &ze = eg.ze;
     std::vector<double> &J = hb.geo[3];
     for (int i = 0; i < L.N[0]; i++)
         for (int j = 0; j < L.N[1]; j++)
@@ -228,8 +251,107 @@ int build_block(const shock_params &p, const double *x, const double *y, const d
                 hb.geo[11][o] = (x_eta * z_xi - x_xi * z_eta) / Jv;
                 hb.geo[12][o] = (x_xi * y_eta - x_eta * y_xi) / Jv;
             }
-    for (int r = 0; r < dim; r++) periodic_images(L, p, gf, 13, 3);
+}
+
+}  // namespace
+
+int build_block(const shock_params &p, const double *x, const double *y, const double *z,
+                const double *u, const double *v, const double *w, const double *pr,
+                const double *rho, HostBlock &hb)
+{
+    Box b;
+    ExtGrid eg;
+    block_start(p, x, y, z, u, v, w, pr, rho, hb, b, eg);
+    const Layout &L = hb.L;
+    double *gf[13] = {hb.geo[0].data(), hb.geo[1].data(), hb.geo[2].data(), hb.geo[4].data(), hb.geo[5].data(),
+                      hb.geo[6].data(), hb.geo[7].data(), hb.geo[8].data(), hb.geo[9].data(), hb.geo[10].data(),
+                      hb.geo[11].data(), hb.geo[12].data(), hb.geo[3].data()};
+    for (int r = 0; r < p.dim; r++) periodic_images(L, p, gf, 13, 3);
+    create_metric(p, hb, eg);
+    for (int r = 0; r < p.dim; r++) periodic_images(L, p, gf, 13, 3);
     mirror_metric(L, p, hb.geo);
+    return 0;
+}
+
+// Region of a face of a block: the g layers next to face f (send: the first
+// or last real layers; receive: the ghost layers beyond it), ghost-inclusive
+// along the other axes (src/Functions.c:360-700, the *_WithGhosts ranges).
+void face_region(const Layout &L, int f, bool send, int lo[3], int hi[3])
+{
+    const int a = f / 2, side = f % 2;
+    for (int c = 0; c < 3; c++) { lo[c] = 0; hi[c] = L.N[c] - 1; }
+    if (send) {
+        lo[a] = side ? L.g + L.n[a] - L.g : L.g;
+        hi[a] = lo[a] + L.g - 1;
+    } else {
+        lo[a] = side ? L.g + L.n[a] : 0;
+        hi[a] = lo[a] + L.g - 1;
+    }
+}
+
+// One TransferMeshParameter over every interface of the division
+// (src/Functions.c:3481-3578): all blocks pack their send regions (x, y, z,
+// the nine metric terms, J), then every receiving face unpacks its
+// neighbour's into its ghost layers, adding the face's float32 Translation
+// to the coordinates (src/Functions.c:2628-2694; identity orientation, so
+// the metric factors are 1).
+void transfer_mesh(std::vector<HostBlock> &hbs, const std::vector<BlockLink> &links)
+{
+    static const int order13[13] = {0, 1, 2, 4, 5, 6, 7, 8, 9, 10, 11, 12, 3};   // SHOCK's buffer order
+    std::vector<std::vector<double>> buf(hbs.size() * 6);
+    for (size_t b = 0; b < hbs.size(); b++)
+        for (int f = 0; f < 2 * hbs[b].L.dim; f++) {
+            const int nb = links[b].neighbour[f];
+            if (nb < 0) continue;
+            // the neighbour's opposite face sends to this face
+            const Layout &S = hbs[nb].L;
+            int lo[3], hi[3];
+            face_region(S, f ^ 1, true, lo, hi);
+            std::vector<double> &q = buf[b * 6 + f];
+            for (int fld = 0; fld < 13; fld++)
+                for (int i = lo[0]; i <= hi[0]; i++)
+                    for (int j = lo[1]; j <= hi[1]; j++)
+                        for (int k = lo[2]; k <= hi[2]; k++) q.push_back(hbs[nb].geo[order13[fld]][S.at(i, j, k)]);
+        }
+    for (size_t b = 0; b < hbs.size(); b++)
+        for (int f = 0; f < 2 * hbs[b].L.dim; f++) {
+            if (links[b].neighbour[f] < 0) continue;
+            const Layout &R = hbs[b].L;
+            int lo[3], hi[3];
+            face_region(R, f, false, lo, hi);
+            const std::vector<double> &q = buf[b * 6 + f];
+            size_t n = 0;
+            for (int fld = 0; fld < 13; fld++)
+                for (int i = lo[0]; i <= hi[0]; i++)
+                    for (int j = lo[1]; j <= hi[1]; j++)
+                        for (int k = lo[2]; k <= hi[2]; k++) {
+                            double v = q[n++];
+                            if (fld < 3) v = v + links[b].translation[f][fld];
+                            hbs[b].geo[order13[fld]][R.at(i, j, k)] = v;
+                        }
+        }
+}
+
+// The set-up chain of SHOCK.c:main (src/SHOCK.c:138-223) for every block of
+// a division at once, the interfaces exchanged as the ranks would: blocks
+// start, DIM mesh transfers, CreateMetric, DIM mesh transfers, metric
+// mirrored at wall faces.
+int build_blocks(const std::vector<shock_params> &ps, const std::vector<const double *> &in,
+                 const std::vector<BlockLink> &links, std::vector<HostBlock> &hbs)
+{
+    const size_t nb = ps.size();
+    hbs.assign(nb, HostBlock());
+    std::vector<Box> bx(nb);
+    std::vector<ExtGrid> eg(nb);
+    for (size_t b = 0; b < nb; b++) {
+        const double *const *f = &in[8 * b];
+        block_start(ps[b], f[0], f[1], f[2], f[3], f[4], f[5], f[6], f[7], hbs[b], bx[b], eg[b]);
+    }
+    const int dim = ps[0].dim;
+    for (int r = 0; r < dim; r++) transfer_mesh(hbs, links);
+    for (size_t b = 0; b < nb; b++) create_metric(ps[b], hbs[b], eg[b]);
+    for (int r = 0; r < dim; r++) transfer_mesh(hbs, links);
+    for (size_t b = 0; b < nb; b++) mirror_metric(hbs[b].L, ps[b], hbs[b].geo);
     return 0;
 }
 

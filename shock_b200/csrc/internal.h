@@ -32,6 +32,22 @@ struct HostBlock {
 int build_block(const shock_params &p, const double *x, const double *y, const double *z,
                 const double *u, const double *v, const double *w, const double *pr,
                 const double *rho, HostBlock &hb);
+
+// Interfaces of one block of a division: the block across each face (the
+// neighbour's opposite face touches it, identity orientation) or -1, and
+// the float32 Translation the face adds to the coordinates it receives.
+struct BlockLink {
+    int neighbour[6];
+    float translation[6][3];
+};
+// Set-up of all blocks of a division with their interfaces exchanged as
+// SHOCK's ranks exchange them; in: 8 pointers per block (x,y,z,u,v,w,p,rho).
+int build_blocks(const std::vector<shock_params> &ps, const std::vector<const double *> &in,
+                 const std::vector<BlockLink> &links, std::vector<HostBlock> &hbs);
+// The g layers next to face f of a block: send = its first / last real
+// layers, otherwise its ghost layers beyond the face; ghost-inclusive along
+// the other axes.  Inclusive index bounds.
+void face_region(const Layout &L, int f, bool send, int lo[3], int hi[3]);
 void periodic_images(const Layout &L, const shock_params &p, double **f, int nf, int ncoord);
 void mms_baseline_fields(const Layout &L, const shock_params &p, const std::vector<std::vector<double>> &geo,
                          double *exact9, double *js5);
@@ -193,6 +209,22 @@ void launch_viscous(const Grid &G, const Phys &P, int precision, int d, const do
 void launch_rk(const Grid &G, const RKCoef &rk, double tau, const double *const Uin[5],
                double *const Uout[5], const Fields &F, bool has_source, cudaStream_t s);
 void launch_copy_state(const Grid &G, const double *const src[5], double *const dst[5], cudaStream_t s);
+
+// One receiving face of a division's halo exchange: the g layers the
+// neighbour sends (its send region of the opposite face) and this block's
+// ghost layers that take them, point for point in the same (i,j,k) order.
+struct XFace {
+    const double *src[5];   // sender's rho,u,v,w,e (the buffer in use)
+    double *dst[5];         // receiver's
+    long long sst[3], rst[3];
+    int slo[3], rlo[3], ext[3];
+    long long off;          // first point of the face in the staging buffer
+};
+// One pass of SHOCK's TransferFlowParameterWithGhosts over a division: every
+// face packs (all reads see the state before the pass), then every face
+// unpacks.  stage: 5 * total doubles.
+void launch_exchange_pass(const XFace *faces, int nfaces, long long most, long long total, double *stage,
+                          cudaStream_t s);
 void launch_nan_check(const Grid &G, const double *rho, unsigned int *flag, cudaStream_t s);
 void launch_add_source(const Grid &G, const Fields &F, cudaStream_t s);
 void launch_post(const Grid &G, double mach, const double *const fin[5], const double *const lst[5],

@@ -418,6 +418,42 @@ bool kernels_prepared()
     return a.maxDynamicSharedSizeBytes >= (int)weno_smem_bytes<3, 9, false, WenoTile<3, 9, false>::tl>();
 }
 
+// Halo exchange between the blocks of a division (src/Functions.c:3580-3684
+// with WriteValuesFromUToBuffer / WriteValuesFromBufferToU, :2697-2863, for
+// the identity orientation): blockIdx.y is the receiving face, x strides
+// over its points.
+template <bool PACK>
+__global__ void __launch_bounds__(256) k_exchange(const XFace *__restrict__ faces, long long total,
+                                                  double *__restrict__ stage)
+{
+    const XFace &F = faces[blockIdx.y];
+    const long long n = (long long)F.ext[0] * F.ext[1] * F.ext[2];
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % F.ext[2]);
+        const long long r = t / F.ext[2];
+        const int j = (int)(r % F.ext[1]), i = (int)(r / F.ext[1]);
+        const long long q = F.off + t;
+        if (PACK) {
+            const long long o = (long long)(F.slo[0] + i) * F.sst[0] + (long long)(F.slo[1] + j) * F.sst[1] + F.slo[2] + k;
+#pragma unroll
+            for (int c = 0; c < 5; c++) stage[c * total + q] = F.src[c][o];
+        } else {
+            const long long o = (long long)(F.rlo[0] + i) * F.rst[0] + (long long)(F.rlo[1] + j) * F.rst[1] + F.rlo[2] + k;
+#pragma unroll
+            for (int c = 0; c < 5; c++) F.dst[c][o] = stage[c * total + q];
+        }
+    }
+}
+
+void launch_exchange_pass(const XFace *faces, int nfaces, long long most, long long total, double *stage,
+                          cudaStream_t s)
+{
+    if (!nfaces) return;
+    const dim3 grid(blocks_for(most, 256) < 1024 ? blocks_for(most, 256) : 1024, nfaces);
+    k_exchange<true><<<grid, 256, 0, s>>>(faces, total, stage);
+    k_exchange<false><<<grid, 256, 0, s>>>(faces, total, stage);
+}
+
 void launch_copy_state(const Grid &G, const double *const src[5], double *const dst[5], cudaStream_t s)
 {
     for (int c = 0; c < 5; c++) cudaMemcpyAsync(dst[c], src[c], sizeof(double) * G.NG, cudaMemcpyDeviceToDevice, s);
