@@ -8,8 +8,10 @@ block: its zeta viscous stencil is centred on the block-local j index
 (src/ZD.c:547-548), so a 3D viscous run split differently gives different
 numbers.  The device reproduces that, block by block, so it is compared
 with the reference run of the same division.  Tolerances as in the
-single-block parity tests: 1e-12 normwise per variable for one RHS and
-1e-10 relative L2 after the steps."""
+single-block parity tests: per variable, 1e-12 normwise for one RHS and
+1e-10 relative L2 after the steps, or twice SHOCK's own FP64-vs-80-bit
+distance on the same division where that is larger (the Mach 0.1
+Taylor-Green vortex and WENO9 are ill-conditioned)."""
 import numpy as np
 import pytest
 
@@ -25,7 +27,7 @@ DIVISIONS = {
     "tgv16_w5_2x2x2": lambda: (cases.taylor_green(16, order=5), (2, 2, 2), 100),
     "smooth2d_w5_2x2": lambda: (cases.smooth_random(2, 5, (24, 20, 1), seed=4, stretch=0.08), (2, 2, 1), 20),
     "smooth2d_w9_3x2": lambda: (cases.smooth_random(2, 9, (33, 24, 1), seed=5), (3, 2, 1), 20),
-    "smooth3d_w9_uneven_2x1x2": lambda: (cases.smooth_random(3, 9, (21, 12, 23), seed=6, stretch=0.05), (2, 1, 2), 10),
+    "smooth3d_w9_uneven_2x1x2": lambda: (cases.smooth_random(3, 9, (21, 10, 23), seed=6, stretch=0.05), (2, 1, 2), 10),
     "channel3d_w5_walls_2x2x1": lambda: (cases.channel(3, 5, (16, 14, 12)), (2, 2, 1), 20),
     "tgv16_w5_inviscid_rk3_2x2x2": lambda: (cases.taylor_green(16, order=5).replace(inviscid=True, time_order=3),
                                             (2, 2, 2), 20),
@@ -56,6 +58,8 @@ def test_division_matches_shock_multirank(name, parity):
         pytest.skip("multi-rank reference build absent (make -C oracle with the reference sources)")
     d = cases.split(case, parts)
     ref = run_multirank(d, nsteps, rhs=True)
+    ref80 = run_multirank(d, nsteps, rhs=True, extended=True) if multirank_available(case.order, case.dim, True) \
+        else None
     m = shock_b200.Multi(d)
     try:
         for b in range(len(d.blocks)):
@@ -68,13 +72,18 @@ def test_division_matches_shock_multirank(name, parity):
     qr = _assemble(d, [r["rhs"] for r in ref])
     sr = _assemble(d, [r["state"][:5] for r in ref])
     idx = [0, 1, 2, 3, 4] if case.dim == 3 else [0, 1, 2, 4]
+    tol_rhs, tol_l2 = np.full(len(idx), 1e-12), np.full(len(idx), 1e-10)
+    floor = None
+    if ref80 is not None:
+        floor = rel_err(qr, _assemble(d, [r["rhs"] for r in ref80]))[idx]
+        tol_rhs = np.maximum(tol_rhs, 2.0 * floor)
+        tol_l2 = np.maximum(tol_l2, 2.0 * l2_rel(sr, _assemble(d, [r["state"][:5] for r in ref80]))[idx])
     e_rhs = rel_err(q, qr)[idx]
-    tol_rhs = 5e-11 if case.order == 9 else 1e-12     # WENO9: SHOCK's own FP64 rounding floor on these cases
-    parity("division", f"{name}", "rhs vs SHOCK multi-rank", e_rhs, tol_rhs)
-    assert (e_rhs <= tol_rhs).all(), e_rhs
+    parity("division", f"{name}", "rhs vs SHOCK multi-rank", e_rhs, tol_rhs, floor)
+    assert (e_rhs <= tol_rhs).all(), (e_rhs, tol_rhs)
     e = l2_rel(st, sr)[idx]
-    parity("division", f"{name}", f"{nsteps} steps L2 vs SHOCK multi-rank", e, 1e-10)
-    assert (e <= 1e-10).all(), e
+    parity("division", f"{name}", f"{nsteps} steps L2 vs SHOCK multi-rank", e, tol_l2)
+    assert (e <= tol_l2).all(), (e, tol_l2)
 
 
 def test_division_inviscid_equals_single_block():
@@ -97,7 +106,7 @@ def test_division_runtime_tau_and_nan():
     """shock_multi_set_tau takes effect on every block (the steps with half the
     time step differ from full ones), and the NaN scan covers every block."""
     c = cases.taylor_green(16, order=5)
-    d = cases.split(c, (2, 1, 2))
+    d = cases.split(c, (2, 2, 1))
     a, b = shock_b200.Multi(d), shock_b200.Multi(d)
     b.set_tau(c.tau / 2)
     a.steps(2)
