@@ -202,6 +202,34 @@ int shock_check_nan(shock_ctx *ctx, int *bad);
  * uses the pressure and ghost values of the last stage's input. */
 int shock_post(shock_ctx *ctx, double *out3);
 
+/* Probes: the pressure and velocity history of SHOCK's PressureHistory /
+ * VelocityHistory options (WriteValuesForPressureHistory /
+ * WriteValuesForVelocityHistory, src/Functions.c:5381-5417, after every
+ * step, src/SHOCK.c:722-734), recorded on the device by the step graph.
+ * ijk3: n ghosted indices (i,j,k) (SHOCK's ijk_PressureHistory_P points);
+ * capacity: steps the device history holds.  n = 0 removes the probes.
+ * The step graphs are captured again. */
+int shock_set_probes(shock_ctx *ctx, int n, const int *ijk3, int capacity);
+/* The history since the last call: out4 receives steps x n x (p, u, v, w)
+ * of U_lastStep after each step (p: the pressure the step's last stage
+ * formed, which SHOCK copies into U_lastStep); *steps the number of steps
+ * (at most max_steps).  The history is then cleared.  SHOCK_ENOMEM when
+ * steps were not recorded because the history was full. */
+int shock_probe_history(shock_ctx *ctx, double *out4, int max_steps, int *steps);
+
+/* Film: SHOCK's samples (CalcValuesForPost then WriteValuesFromUToFilm,
+ * src/SHOCK.c:698-717, src/Functions.c:2510-2556) kept on the device so that
+ * sampling does not download the state.  shock_film_reserve holds
+ * max_frames frames (0 frees them); shock_film_sample appends one frame of
+ * U_lastStep, queued on the context's stream; shock_film_download copies
+ * up to max_frames frames to out, each 8 fields (rho, u, v, w, p,
+ * |grad rho|, Mach number, lambda2) over the real points (i slowest, k
+ * fastest, the Film layout), and sets *frames.  SHOCK_ENOMEM when the film
+ * is full. */
+int shock_film_reserve(shock_ctx *ctx, int max_frames);
+int shock_film_sample(shock_ctx *ctx);
+int shock_film_download(shock_ctx *ctx, double *out, int max_frames, int *frames);
+
 /* Geometry after set-up: x,y,z,J,xi_x..zeta_z (13*NG doubles). */
 int shock_geometry(shock_ctx *ctx, double *out13);
 

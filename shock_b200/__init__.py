@@ -108,7 +108,8 @@ def lib():
                          "shock_multi_create", "shock_multi_destroy", "shock_multi_dims", "shock_multi_geometry",
                          "shock_multi_step", "shock_multi_rhs", "shock_multi_download_state",
                          "shock_multi_upload_state", "shock_multi_set_tau", "shock_multi_check_nan",
-                         "shock_multi_info", "shock_host_multi_geometry",
+                         "shock_multi_info", "shock_host_multi_geometry", "shock_set_probes",
+                         "shock_probe_history", "shock_film_reserve", "shock_film_sample", "shock_film_download",
                          "shock_host_geometry", "shock_host_mms_baseline", "shock_rhs_static",
                          "shock_batch_create", "shock_batch_destroy", "shock_batch_member_bytes",
                          "shock_batch_add", "shock_batch_remove", "shock_batch_step", "shock_batch_step_async",
@@ -281,6 +282,39 @@ class Solver:
         assert s.dtype == np.float64 and s.flags["C_CONTIGUOUS"] and s.size == 5 * self.n
         _check(self.lib.shock_download_state(self.h, _ptr(s), 0))
         return s.reshape((5,) + self.shape)
+
+    def set_probes(self, ijk, capacity: int = 1024):
+        """Record p, u, v, w of U_lastStep at ghosted points ijk (a list of
+        (i, j, k)) after every step, on the device."""
+        a = np.ascontiguousarray(np.asarray(ijk, dtype=np.int32).reshape(-1, 3))
+        self._nprobes = a.shape[0]
+        _check(self.lib.shock_set_probes(self.h, C.c_int(a.shape[0]), a.ctypes.data_as(C.POINTER(C.c_int)),
+                                         C.c_int(capacity)))
+
+    def probe_history(self, max_steps: int = 1024) -> np.ndarray:
+        """(steps, probes, 4): p, u, v, w after each step since the last call."""
+        n = getattr(self, "_nprobes", 0)
+        out = np.zeros(max(1, max_steps * n * 4))
+        steps = C.c_int()
+        _check(self.lib.shock_probe_history(self.h, _ptr(out), C.c_int(max_steps), C.byref(steps)))
+        return out[:steps.value * n * 4].reshape(steps.value, n, 4)
+
+    def film_reserve(self, frames: int):
+        _check(self.lib.shock_film_reserve(self.h, C.c_int(frames)))
+        self._film_cap = frames
+
+    def film_sample(self):
+        _check(self.lib.shock_film_sample(self.h))
+
+    def film(self) -> np.ndarray:
+        """(frames, 8, ni, nj, nk): rho, u, v, w, p, |grad rho|, Mach, lambda2."""
+        c = self.case
+        nk = c.nk if c.dim == 3 else 1
+        cap = getattr(self, "_film_cap", 0)
+        out = np.zeros(max(1, cap * 8 * c.ni * c.nj * nk))
+        frames = C.c_int()
+        _check(self.lib.shock_film_download(self.h, _ptr(out), C.c_int(cap), C.byref(frames)))
+        return out[:frames.value * 8 * c.ni * c.nj * nk].reshape(frames.value, 8, c.ni, c.nj, nk)
 
     def pressure(self) -> np.ndarray:
         """U_RK's p after the last step (ghosted)."""

@@ -89,6 +89,14 @@ struct shock_ctx {
     int tmark = 0;
     std::vector<std::pair<std::string, std::pair<double, long long>>> tacc;   // name -> (ms, launches)
     long long tsteps = 0;
+    // probes (pressure / velocity history) recorded by the step graph
+    long long *probe_idx = nullptr;
+    int n_probes = 0, probe_cap = 0;
+    double *probe_hist = nullptr;
+    unsigned *probe_count = nullptr;
+    // Film frames sampled on the device
+    double *film = nullptr;
+    int film_cap = 0, film_frames = 0;
 };
 
 namespace shock {
@@ -228,6 +236,13 @@ static void enqueue_step(shock_ctx *c, int un, int &nk)
         launch_bc_save(c->G, c->F.p, c->plast, c->stream);
         nk++;
         mark(c, "bc_save");
+    }
+    // the pressure and velocity histories of U_lastStep (src/SHOCK.c:722-734)
+    if (c->n_probes) {
+        launch_probe_record(c->probe_idx, c->n_probes, c->F.p, c->buf[cur], c->probe_hist, c->probe_cap,
+                            c->probe_count, c->stream);
+        nk++;
+        mark(c, "probes");
     }
 }
 
@@ -453,6 +468,10 @@ int shock_destroy(shock_ctx *c)
     if (c->pool) cudaFree(c->pool);
     if (c->F.flag) cudaFree(c->F.flag);
     if (c->plast_pool) cudaFree(c->plast_pool);
+    if (c->probe_idx) cudaFree(c->probe_idx);
+    if (c->probe_hist) cudaFree(c->probe_hist);
+    if (c->probe_count) cudaFree(c->probe_count);
+    if (c->film) cudaFree(c->film);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     for (auto e : c->tev) cudaEventDestroy(e);
@@ -735,6 +754,108 @@ int shock_post(shock_ctx *c, double *out3)
     for (int q = 0; q < 3; q++)
         CK(cudaMemcpyAsync(out3 + (size_t)q * c->G.NG, c->F.Q[q], nb, cudaMemcpyDeviceToHost, c->stream));
     CK(cudaStreamSynchronize(c->stream));
+    return SHOCK_OK;
+}
+
+int shock_set_probes(shock_ctx *c, int n, const int *ijk3, int capacity)
+{
+    if (!c || n < 0 || (n && (!ijk3 || capacity < 1))) return fail(SHOCK_EINVAL, "bad argument");
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    std::vector<long long> idx(n);
+    for (int q = 0; q < n; q++) {
+        const int *v = ijk3 + 3 * q;
+        for (int a = 0; a < 3; a++)
+            if (v[a] < 0 || v[a] >= c->L.N[a]) return fail(SHOCK_EINVAL, "probe %d outside the ghosted block", q);
+        idx[q] = c->L.at(v[0], v[1], v[2]);
+    }
+    if (c->probe_idx) cudaFree(c->probe_idx);
+    if (c->probe_hist) cudaFree(c->probe_hist);
+    c->probe_idx = nullptr;
+    c->probe_hist = nullptr;
+    c->n_probes = 0;
+    c->probe_cap = 0;
+    if (n) {
+        if (!c->probe_count && cudaMalloc(&c->probe_count, sizeof(unsigned)) != cudaSuccess)
+            return fail(SHOCK_ENOMEM, "probe counter");
+        if (cudaMalloc(&c->probe_idx, sizeof(long long) * n) != cudaSuccess ||
+            cudaMalloc(&c->probe_hist, sizeof(double) * 4 * (size_t)n * capacity) != cudaSuccess)
+            return fail(SHOCK_ENOMEM, "probe history of %d steps", capacity);
+        CK(cudaMemcpy(c->probe_idx, idx.data(), sizeof(long long) * n, cudaMemcpyHostToDevice));
+        CK(cudaMemset(c->probe_count, 0, sizeof(unsigned)));
+        c->n_probes = n;
+        c->probe_cap = capacity;
+    }
+    // the step graphs are captured again with (or without) the recording
+    for (int i = 0; i < 3; i++)
+        if (c->step_graph[i]) { cudaGraphExecDestroy(c->step_graph[i]); c->step_graph[i] = nullptr; }
+    return SHOCK_OK;
+}
+
+int shock_probe_history(shock_ctx *c, double *out4, int max_steps, int *steps)
+{
+    if (!c || !steps || (max_steps > 0 && !out4)) return fail(SHOCK_EINVAL, "bad argument");
+    *steps = 0;
+    if (!c->n_probes) return SHOCK_OK;
+    CK(cudaSetDevice(c->device));
+    unsigned count = 0;
+    CK(cudaMemcpyAsync(&count, c->probe_count, sizeof count, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    const int got = (int)(count > (unsigned)c->probe_cap ? (unsigned)c->probe_cap : count);
+    const int take = got < max_steps ? got : max_steps;
+    if (take > 0)
+        CK(cudaMemcpy(out4, c->probe_hist, sizeof(double) * 4 * (size_t)c->n_probes * take, cudaMemcpyDeviceToHost));
+    CK(cudaMemset(c->probe_count, 0, sizeof(unsigned)));
+    *steps = take;
+    if (count > (unsigned)c->probe_cap || take < got)
+        return fail(SHOCK_ENOMEM, "probe history full: steps after the first %d were not recorded", take);
+    return SHOCK_OK;
+}
+
+int shock_film_reserve(shock_ctx *c, int max_frames)
+{
+    if (!c || max_frames < 0) return fail(SHOCK_EINVAL, "bad argument");
+    CK(cudaSetDevice(c->device));
+    CK(cudaStreamSynchronize(c->stream));
+    if (c->film) cudaFree(c->film);
+    c->film = nullptr;
+    c->film_cap = c->film_frames = 0;
+    if (!max_frames) return SHOCK_OK;
+    const size_t nr = (size_t)c->L.n[0] * c->L.n[1] * c->L.n[2];
+    if (cudaMalloc(&c->film, sizeof(double) * 8 * nr * (size_t)max_frames) != cudaSuccess)
+        return fail(SHOCK_ENOMEM, "film of %d frames", max_frames);
+    c->film_cap = max_frames;
+    return SHOCK_OK;
+}
+
+int shock_film_sample(shock_ctx *c)
+{
+    if (!c) return fail(SHOCK_EINVAL, "null argument");
+    if (c->film_frames >= c->film_cap) return fail(SHOCK_ENOMEM, "film full (%d frames)", c->film_cap);
+    CK(cudaSetDevice(c->device));
+    const double *fin[5], *lst[5];
+    for (int q = 0; q < 5; q++) { fin[q] = c->buf[c->un][q]; lst[q] = c->buf[c->last_in][q]; }
+    // CalcValuesForPost on U_lastStep (src/SHOCK.c:705-709) into Q, free between steps
+    for (int q = 0; q < 3; q++) CK(cudaMemsetAsync(c->F.Q[q], 0, sizeof(double) * c->G.NG, c->stream));
+    launch_post(c->G, c->p.mach, fin, lst, c->F.p, c->F, c->F.Q[0], c->F.Q[1], c->F.Q[2], c->stream);
+    const size_t nr = (size_t)c->L.n[0] * c->L.n[1] * c->L.n[2];
+    launch_film_gather(c->G, fin, c->F.p, c->F.Q[1], c->F.Q[0], c->F.Q[2], c->film + 8 * nr * (size_t)c->film_frames,
+                       c->stream);
+    CK(cudaGetLastError());
+    c->film_frames++;
+    return SHOCK_OK;
+}
+
+int shock_film_download(shock_ctx *c, double *out, int max_frames, int *frames)
+{
+    if (!c || !frames || (max_frames > 0 && !out)) return fail(SHOCK_EINVAL, "bad argument");
+    CK(cudaSetDevice(c->device));
+    const int take = c->film_frames < max_frames ? c->film_frames : max_frames;
+    const size_t nr = (size_t)c->L.n[0] * c->L.n[1] * c->L.n[2];
+    if (take > 0)
+        CK(cudaMemcpyAsync(out, c->film, sizeof(double) * 8 * nr * (size_t)take, cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaStreamSynchronize(c->stream));
+    *frames = take;
     return SHOCK_OK;
 }
 

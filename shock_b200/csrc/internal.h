@@ -210,6 +210,16 @@ void launch_rk(const Grid &G, const RKCoef &rk, double tau, const double *const 
                double *const Uout[5], const Fields &F, bool has_source, cudaStream_t s);
 void launch_copy_state(const Grid &G, const double *const src[5], double *const dst[5], cudaStream_t s);
 
+// Probe history: p (U_lastStep's pressure) and u, v, w of the state after
+// the step at n ghosted indices, appended at slot *count of hist
+// ([cap][n][4]) while *count < cap (*count then saturates at cap + 1).
+void launch_probe_record(const long long *idx, int n, const double *p, const double *const U[5], double *hist,
+                         int cap, unsigned *count, cudaStream_t s);
+// One Film frame: rho, u, v, w, p, |grad rho|, Mach, lambda2 of the real
+// points (i slowest, k fastest, SHOCK's Film order) from ghosted fields.
+void launch_film_gather(const Grid &G, const double *const U[5], const double *p, const double *gr,
+                        const double *ma, const double *l2, double *frame, cudaStream_t s);
+
 // One receiving face of a division's halo exchange: the g layers the
 // neighbour sends (its send region of the opposite face) and this block's
 // ghost layers that take them, point for point in the same (i,j,k) order.

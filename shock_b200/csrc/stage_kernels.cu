@@ -418,6 +418,65 @@ bool kernels_prepared()
     return a.maxDynamicSharedSizeBytes >= (int)weno_smem_bytes<3, 9, false, WenoTile<3, 9, false>::tl>();
 }
 
+// WriteValuesForPressureHistory / WriteValuesForVelocityHistory
+// (src/Functions.c:5381-5417) after a step, into a device history.
+__global__ void k_probe_record(const long long *__restrict__ idx, int n, const double *__restrict__ p, StageIn U,
+                               double *hist, int cap, unsigned *count)
+{
+    const unsigned slot = *count;   // the previous step's increment is complete (stream order)
+    const int t = threadIdx.x;
+    if (slot < (unsigned)cap)
+        for (int q = t; q < n; q += blockDim.x) {
+            const long long o = idx[q];
+            double *h = hist + ((size_t)slot * n + q) * 4;
+            h[0] = p[o];
+            h[1] = U.U[1][o];
+            h[2] = U.U[2][o];
+            h[3] = U.U[3][o];
+        }
+    __syncthreads();
+    if (t == 0 && slot <= (unsigned)cap) *count = slot + 1;
+}
+
+void launch_probe_record(const long long *idx, int n, const double *p, const double *const U[5], double *hist,
+                         int cap, unsigned *count, cudaStream_t s)
+{
+    StageIn in;
+    for (int c = 0; c < 5; c++) in.U[c] = U[c];
+    k_probe_record<<<1, 256, 0, s>>>(idx, n, p, in, hist, cap, count);
+}
+
+// WriteValuesFromUToFilm (src/Functions.c:2510-2556) into a device frame.
+__global__ void k_film_gather(Grid G, StageIn U, const double *__restrict__ p, const double *__restrict__ gr,
+                              const double *__restrict__ ma, const double *__restrict__ l2, double *frame)
+{
+    const long long nr = (long long)G.n[0] * G.n[1] * G.n[2];
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < nr; t += (long long)gridDim.x * blockDim.x) {
+        const int k = (int)(t % G.n[2]);
+        const long long r = t / G.n[2];
+        const int j = (int)(r % G.n[1]), i = (int)(r / G.n[1]);
+        const long long o = (long long)(i + G.g) * G.st[0] + (long long)(j + G.g) * G.st[1] + (G.dim == 3 ? k + G.g : 0);
+        frame[0 * nr + t] = U.U[0][o];
+        frame[1 * nr + t] = U.U[1][o];
+        frame[2 * nr + t] = U.U[2][o];
+        frame[3 * nr + t] = U.U[3][o];
+        frame[4 * nr + t] = p[o];
+        frame[5 * nr + t] = gr[o];
+        frame[6 * nr + t] = ma[o];
+        frame[7 * nr + t] = l2[o];
+    }
+}
+
+void launch_film_gather(const Grid &G, const double *const U[5], const double *p, const double *gr,
+                        const double *ma, const double *l2, double *frame, cudaStream_t s)
+{
+    StageIn in;
+    for (int c = 0; c < 5; c++) in.U[c] = U[c];
+    const long long nr = (long long)G.n[0] * G.n[1] * G.n[2];
+    const unsigned nb = blocks_for(nr, 256) < 4096 ? blocks_for(nr, 256) : 4096;
+    k_film_gather<<<nb, 256, 0, s>>>(G, in, p, gr, ma, l2, frame);
+}
+
 // Halo exchange between the blocks of a division (src/Functions.c:3580-3684
 // with WriteValuesFromUToBuffer / WriteValuesFromBufferToU, :2697-2863, for
 // the identity orientation): blockIdx.y is the receiving face, x strides
