@@ -206,7 +206,8 @@ int shock_post(shock_ctx *ctx, double *out3);
  * VelocityHistory options (WriteValuesForPressureHistory /
  * WriteValuesForVelocityHistory, src/Functions.c:5381-5417, after every
  * step, src/SHOCK.c:722-734), recorded on the device by the step graph.
- * ijk3: n ghosted indices (i,j,k) (SHOCK's ijk_PressureHistory_P points);
+ * ijk3: n ghosted indices (i,j,k) of real points (SHOCK's
+ * ijk_PressureHistory_P points; others are rejected with SHOCK_EINVAL);
  * capacity: steps the device history holds.  n = 0 removes the probes.
  * The step graphs are captured again. */
 int shock_set_probes(shock_ctx *ctx, int n, const int *ijk3, int capacity);

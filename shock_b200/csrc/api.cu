@@ -765,8 +765,10 @@ int shock_set_probes(shock_ctx *c, int n, const int *ijk3, int capacity)
     std::vector<long long> idx(n);
     for (int q = 0; q < n; q++) {
         const int *v = ijk3 + 3 * q;
+        // SHOCK places probes on real points only (src/Functions.c:5152-5160)
         for (int a = 0; a < 3; a++)
-            if (v[a] < 0 || v[a] >= c->L.N[a]) return fail(SHOCK_EINVAL, "probe %d outside the ghosted block", q);
+            if (a < c->p.dim ? (v[a] < c->L.g || v[a] >= c->L.g + c->L.n[a]) : v[a] != 0)
+                return fail(SHOCK_EINVAL, "probe %d is not a real point", q);
         idx[q] = c->L.at(v[0], v[1], v[2]);
     }
     if (c->probe_idx) cudaFree(c->probe_idx);

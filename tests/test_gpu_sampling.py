@@ -26,25 +26,34 @@ def test_probe_history_matches_reference(case, parity):
     _need(case)
     g = case.ghosts
     pts = [(g, g, g if case.dim == 3 else 0), (g + 5, g + 3, g + 2 if case.dim == 3 else 0),
-           (g + case.ni - 1, g + case.nj - 1, g + case.nk - 1 if case.dim == 3 else 0),
-           (g - 1, g + 2, g + 1 if case.dim == 3 else 0)]   # the last one a ghost point
+           (g + case.ni - 1, g + case.nj - 1, g + case.nk - 1 if case.dim == 3 else 0)]
     s = shock_b200.Solver(case)
+    with pytest.raises(shock_b200.ShockError):
+        s.set_probes([(g - 1, g, g if case.dim == 3 else 0)])     # SHOCK keeps probes on real points
     s.set_probes(pts, capacity=16)
     s.steps(6)
     hist = s.probe_history()
-    r = RefSolver(case)
-    ref = []
-    for _ in range(6):
-        r.steps(1)
-        st = r.state(1)      # U_lastStep: rho,u,v,w,e,p,T,c,mue
-        ref.append([[st[5][p], st[1][p], st[2][p], st[3][p]] for p in pts])
-    ref = np.array(ref)
+
+    def reference(extended):
+        r = RefSolver(case, extended=extended)
+        out = []
+        for _ in range(6):
+            r.steps(1)
+            st = r.state(1)      # U_lastStep: rho,u,v,w,e,p,T,c,mue
+            out.append([[st[5][p], st[1][p], st[2][p], st[3][p]] for p in pts])
+        return np.array(out)
+
+    ref = reference(False)
     assert hist.shape == ref.shape
     scale = np.abs(ref).max(axis=(0, 1))
     scale[scale == 0] = 1.0
     err = np.abs(hist - ref).max(axis=(0, 1)) / scale
-    parity("probes", case.name, "p,u,v,w history (6 steps)", err, 1e-12)
-    assert (err <= 1e-12).all(), err
+    tol = np.full(4, 1e-12)
+    if ref_available(case.order, case.dim, extended=True):
+        # twice SHOCK's own FP64-vs-80-bit distance where that is larger (WENO9 ducts)
+        tol = np.maximum(tol, 2.0 * np.abs(reference(True) - ref).max(axis=(0, 1)) / scale)
+    parity("probes", case.name, "p,u,v,w history (6 steps)", err, tol)
+    assert (err <= tol).all(), (err, tol)
     # the history was cleared, and a full history reports the lost steps
     assert s.probe_history().shape[0] == 0
     s.set_probes(pts[:1], capacity=2)
