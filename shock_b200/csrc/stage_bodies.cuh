@@ -449,8 +449,10 @@ __device__ __forceinline__ T phi_w5(const T *d, T eps)
     return T(1. / 3.) * o0 * q1 + T(1. / 6.) * (o2 - T(0.5)) * q2;
 }
 
-// WENO9 smoothness-indicator quadratic forms (src/WENO.c:25-53), stored
-// as the upper triangle per sub-stencil.
+// SHOCK's WENO9 smoothness indicators (src/WENO.c:25-53): integer quadratic
+// forms in a sub-stencil's five values, upper triangle row by row.  The
+// kernels evaluate them in the factorised forms below; the test of the
+// factorisation reads this table.
 static __constant__ double c_w9is[5][15] = {
     {22658., -208501., 364863., -288007., 86329., 482963., -1704396., 1358458., -411487., 1521393., -2462076., 758823., 1020563., -649501., 107918.},
     {6908., -60871., 99213., -70237., 18079., 138563., -464976., 337018., -88297., 406293., -611976., 165153., 242723., -140251., 22658.},
@@ -486,6 +488,27 @@ static __constant__ float c_w9ldl[5][10] = {
      float(290071763. / 890329635.), float(-8384962321. / 17843974736.),
      107918.f, float(18696922335. / 431672.), float(999262585216. / 296776545.), float(16652415615. / 318642406.)},
 };
+// The same factorisation in FP64: the FP64 WENO9 indicators in 14 operations
+// per sub-stencil instead of the 20 of the integer form, and without its
+// cancellation (SHOCK's own FP64 rounding of the integer form is the larger
+// error of the two).
+static __constant__ double c_w9ldl64[5][10] = {
+    {double(-163185. / 45316.), double(100839. / 22658.), double(-41089198. / 14249315.), double(-86329. / 45316.),
+     double(1813059. / 838195.), double(-350813921. / 232768856.),
+     22658., double(299235615. / 90632.), double(39105167808. / 14249315.), double(116566909305. / 29096107.)},
+    {double(-47055. / 13816.), double(26079. / 6908.), double(-12448558. / 5880675.), double(-18079. / 13816.),
+     double(5686883. / 5880675.), double(-146761231. / 232768856.),
+     6908., double(123494175. / 27632.), double(13035055936. / 1960225.), double(116566909305. / 29096107.)},
+    {double(-37185. / 13816.), double(15369. / 6908.), double(-1032654. / 838195.), double(-8209. / 13816.),
+     double(5686883. / 14249315.), double(-20636113. / 51089708.),
+     6908., double(299235615. / 27632.), double(8583070944. / 838195.), double(233133818610. / 217131259.)},
+    {double(-94935. / 45316.), double(35109. / 22658.), double(-106728718. / 110863235.), double(-18079. / 45316.),
+     double(30822003. / 110863235.), double(-1745642471. / 4217089556.),
+     22658., double(2328127935. / 90632.), double(101210149344. / 15837605.), double(233133818610. / 1054272389.)},
+    {double(-433665. / 215836.), double(162579. / 107918.), double(-945305518. / 890329635.), double(-86329. / 215836.),
+     double(290071763. / 890329635.), double(-8384962321. / 17843974736.),
+     107918., double(18696922335. / 431672.), double(999262585216. / 296776545.), double(16652415615. / 318642406.)},
+};
 
 // Packed FP32 arithmetic (two lanes per instruction) for the mixed form:
 // the + and - sides of a face have the same operations.
@@ -515,11 +538,6 @@ __device__ __forceinline__ float2 phi_w5x2(const float2 *d, float eps)
     const float2 q2 = fma2(f2(-2.f), d[2], add2(d[1], d[3]));
     return fma2(mul2(f2(1.f / 6.f), sub2(o2, f2(0.5f))), q2, mul2(mul2(f2(1.f / 3.f), o0), q1));
 }
-
-template <typename T>
-__device__ __forceinline__ T w9c(int k, int i);
-template <>
-__device__ __forceinline__ double w9c<double>(int k, int i) { return c_w9is[k][i]; }
 
 // ---------------------------------------------------------------------------
 // Sweep geometry: sweep axis D, lateral axis (32 lines, the fastest
@@ -842,23 +860,20 @@ __device__ __forceinline__ double w5_phi(const double *d, const double *r)
     return 1. / 3. * o0 * q1 + 1. / 6. * (o2 - 0.5) * q2;
 }
 
-// WENO9 smoothness terms t = IS + eps of one stencil (9 values f), SHOCK's
-// integer forms in its order (FP64).
-template <typename T>
-__device__ __forceinline__ void w9_terms(const T *f, T eps, T *t)
+// WENO9 smoothness terms t = IS + eps of one stencil from its eight first
+// differences d by the factorised forms (c_w9ldl64), FP64.  The indicators
+// are even in d, so the minus side's stencil takes its differences with
+// either sign.
+__device__ __forceinline__ void w9_terms_diff64(const double *d, double eps, double *t)
 {
 #pragma unroll
     for (int k = 0; k < 5; k++) {
-        T acc = T(0);
-        int c = 0;
-#pragma unroll
-        for (int a = 0; a < 5; a++) {
-            T in = w9c<T>(k, c++) * f[k + a];
-#pragma unroll
-            for (int b = a + 1; b < 5; b++) in = in + w9c<T>(k, c++) * f[k + b];
-            acc = (a == 0) ? f[k] * in : acc + f[k + a] * in;
-        }
-        t[k] = acc + eps;
+        const double *x = d + k, *c = c_w9ldl64[k];
+        const double y0 = fma(c[3], x[3], fma(c[1], x[2], fma(c[0], x[1], x[0])));
+        const double y1 = fma(c[4], x[3], fma(c[2], x[2], x[1]));
+        const double y2 = fma(c[5], x[3], x[2]);
+        const double is = fma(c[6] * y0, y0, fma(c[7] * y1, y1, fma(c[8] * y2, y2, c[9] * x[3] * x[3])));
+        t[k] = is + eps;
     }
 }
 
@@ -918,8 +933,8 @@ __device__ __forceinline__ double weno_phi_fp64(const double *Pp, const double *
 #pragma unroll
     for (int q = 0; q < 8; q++) { dp[q] = fp[q + 1] - fp[q]; dm[q] = fm[q] - fm[q + 1]; }
     double t[10], rc[10];
-    w9_terms(fp, eps, t);
-    w9_terms(fm, eps, t + 5);
+    w9_terms_diff64(dp, eps, t);
+    w9_terms_diff64(dm, eps, t + 5);
     pair_reciprocals<10>(t, rc);
     return -w9_phi(dp, rc) + w9_phi(dm, rc + 5);
 }

@@ -1,10 +1,12 @@
-"""The FP32 WENO9 smoothness indicators are SHOCK's integer quadratic forms
-(src/WENO.c:25-53) rewritten on first differences as sums of squares.
+"""The WENO9 smoothness indicators of the kernels (FP32 and FP64) are
+SHOCK's integer quadratic forms (src/WENO.c:25-53) rewritten on first
+differences as sums of squares.
 
-Both tables are read from the kernel source.  On random stencils the
-factorised form must give SHOCK's value exactly (the table holds exact
-rationals), and in FP32 it must stay within a few units of FP32 rounding,
-where the integer form loses up to about 1e-3 to cancellation.
+The tables are read from the kernel source.  On random stencils the
+factorised form must give SHOCK's value exactly (the tables hold exact
+rationals, the FP32 and FP64 tables the same ones), and in FP32 / FP64 it
+must stay within a few units of rounding, where the integer form loses up
+to about 1e-3 (FP32) to cancellation.
 """
 import os
 import re
@@ -26,7 +28,7 @@ def _table(name):
         for item in (x.strip() for x in row.split(",")):
             if not item:
                 continue
-            m = re.fullmatch(r"float\((-?\d+)\. / (\d+)\.\)", item)
+            m = re.fullmatch(r"(?:float|double)\((-?\d+)\. / (\d+)\.\)", item)
             if m:
                 vals.append(Fraction(int(m.group(1)), int(m.group(2))))
             else:
@@ -99,3 +101,41 @@ def test_factorised_indicators_fp32_accuracy():
     print(f"FP32 relative error: factorised {worst_new:.2e}, integer form {worst_old:.2e}")
     assert worst_new < 1e-5, worst_new
     assert worst_old > 20 * worst_new, (worst_old, worst_new)
+
+
+def test_fp64_table_is_the_fp32_one():
+    assert _table("c_w9ldl64[5][10]") == _table("c_w9ldl[5][10]")
+
+
+def test_factorised_indicators_fp64_accuracy():
+    """In FP64 the factorised form is at least as accurate as the integer form
+    SHOCK evaluates, to a few units of FP64 rounding."""
+    ints, ldl = _table("c_w9is[5][15]"), _table("c_w9ldl64[5][10]")
+    rng = np.random.default_rng(13)
+    worst_new = worst_old = 0.0
+    for k in range(5):
+        t64 = [float(x) for x in ldl[k]]
+        c64 = [float(x) for x in ints[k]]
+        for trial in range(300):
+            kind = trial % 3
+            if kind == 0:
+                x = np.cumsum(rng.normal(size=5))
+            elif kind == 1:
+                x = rng.normal() + rng.normal() * np.linspace(0, 1, 5) + 1e-6 * rng.normal(size=5)
+            else:
+                x = np.where(np.arange(5) < 1 + trial % 4, 1.0, -1.0) + 1e-8 * rng.normal(size=5)
+            exact = float(_shock_form(ints[k], [Fraction(float(v)) for v in x]))
+            d = np.diff(x)
+            new = _ldl_form(t64, d)
+            old, i = 0.0, 0
+            for a in range(5):
+                inner = 0.0
+                for b in range(a, 5):
+                    inner = inner + c64[i] * x[b]
+                    i += 1
+                old = old + x[a] * inner
+            worst_new = max(worst_new, abs(float(new) - exact) / exact)
+            worst_old = max(worst_old, abs(float(old) - exact) / exact)
+    print(f"FP64 relative error: factorised {worst_new:.2e}, integer form {worst_old:.2e}")
+    assert worst_new < 1e-14, worst_new
+    assert worst_old >= worst_new, (worst_old, worst_new)
