@@ -89,6 +89,9 @@ typedef struct shock_params {
                            (10*sqrt(FLT_MIN) in the FP32 stencils; src/Functions.c:1829, "reference
                            mode"); > 0 sets it ("clean mode", e.g. the 1e-6 src/Functions.c:1818,1825
                            leaves commented out, which restores the design order at smooth extrema) */
+    int full_metric;    /* 3D: 0 gives SHOCK's metric with the cross derivatives of the coordinates zeroed
+                           (src/Functions.c:6479-6484, "reference mode"); 1 keeps them (the full curvilinear
+                           metric, "clean mode"; FP64 form only) */
 } shock_params;
 
 typedef struct shock_ctx shock_ctx;

@@ -43,9 +43,10 @@ class RefParams(C.Structure):
     ]
 
 
-def ref_available(order: int, dim: int, extended: bool = False) -> bool:
+def ref_available(order: int, dim: int, extended: bool = False, full: bool = False) -> bool:
     tag = "80" if extended else ""
-    return os.path.exists(os.path.join(HERE, "_ref", f"libshockref{tag}_w{order}_{dim}d.so"))
+    name = "libshockreffull" if full else "libshockref"
+    return os.path.exists(os.path.join(HERE, "_ref", f"{name}{tag}_w{order}_{dim}d.so"))
 
 
 def dropin_available(order: int, dim: int) -> bool:
@@ -57,11 +58,15 @@ class RefSolver:
 
     _libs: dict = {}
 
-    def __init__(self, case, extended=False, external=None, _lib="libshockref"):
+    def __init__(self, case, extended=False, external=None, _lib="libshockref", full=False):
         """extended=True loads the PRECISION=3 (80-bit long double) build.
         external=(exact9, js5): manufactured solution given as arrays on the
-        ghosted block (the build with ref_harness/mms_external.c)."""
+        ghosted block (the build with ref_harness/mms_external.c).
+        full=True: the build that keeps the 3D metric's cross derivatives
+        (src/Functions.c:6479-6484 left out, 3D only)."""
         self.case = case
+        if full:
+            _lib = "libshockreffull"
         tag = "80" if extended else ("x" if external is not None else "")
         key = (case.order, case.dim, _lib + tag)
         if key not in RefSolver._libs:

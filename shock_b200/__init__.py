@@ -69,7 +69,7 @@ class Params(C.Structure):
         ("precision", C.c_int), ("zeta_fix", C.c_int),
         ("bc", C.c_int * 6), ("t_wall", C.c_double),
         ("rho_inflow", C.c_double), ("p_inflow", C.c_double), ("p_outflow", C.c_double),
-        ("u_inflow", C.c_double * 3), ("weno_eps", C.c_double),
+        ("u_inflow", C.c_double * 3), ("weno_eps", C.c_double), ("full_metric", C.c_int),
     ]
 
 
@@ -145,7 +145,7 @@ def _ptr(a):
     return a.ctypes.data_as(_dp)
 
 
-def params_from_case(case, precision=SHOCK_FP64, zeta_fix=False, weno_eps=0.0) -> Params:
+def params_from_case(case, precision=SHOCK_FP64, zeta_fix=False, weno_eps=0.0, full_metric=False) -> Params:
     p = Params()
     p.dim, p.order = case.dim, case.order
     p.ni, p.nj, p.nk = case.ni, case.nj, (case.nk if case.dim == 3 else 1)
@@ -166,6 +166,7 @@ def params_from_case(case, precision=SHOCK_FP64, zeta_fix=False, weno_eps=0.0) -
     for a in range(3):
         p.u_inflow[a] = float(case.u_inflow[a])
     p.weno_eps = float(weno_eps)
+    p.full_metric = int(bool(full_metric))
     return p
 
 
@@ -179,12 +180,12 @@ def _fortran_coords(case):
     return f(case.x), f(case.y), f(case.z)
 
 
-def host_geometry(case) -> np.ndarray:
+def host_geometry(case, full_metric=False) -> np.ndarray:
     """Block geometry (x,y,z,J, 9 metrics; ghosted) built on the host, no device."""
     shp = _ghosted_shape(case)
     out = np.zeros((13,) + shp)
     x, y, z = _fortran_coords(case)
-    p = params_from_case(case)
+    p = params_from_case(case, full_metric=full_metric)
     _check(lib().shock_host_geometry(C.byref(p), _ptr(x), _ptr(y), _ptr(z), _ptr(out)))
     return out
 
@@ -204,10 +205,10 @@ class Solver:
     """One block of SHOCK's stage right-hand side on a CUDA device."""
 
     def __init__(self, case, precision=SHOCK_FP64, device: int = 0, zeta_fix: bool = False,
-                 dirichlet9=None, source5=None, weno_eps: float = 0.0):
+                 dirichlet9=None, source5=None, weno_eps: float = 0.0, full_metric: bool = False):
         self.case = case
         self.lib = lib()
-        self.params = params_from_case(case, precision, zeta_fix, weno_eps)
+        self.params = params_from_case(case, precision, zeta_fix, weno_eps, full_metric)
         f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
         arrs = [f(a) for a in case.real_fields()]
         h = C.c_void_p()

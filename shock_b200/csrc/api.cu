@@ -134,6 +134,7 @@ Phys make_phys(const shock_params &p)
     }
     P.mms = p.mms ? 1 : 0;
     P.zeta_fix = p.zeta_fix;
+    P.full = (p.dim == 3 && p.full_metric) ? 1 : 0;
     // BC_Corrector_*Momentum of the ghost points (reset to 1 at set-up,
     // src/Functions.c:6388-6509): -1 on every momentum at a no-slip wall
     // (src/BC.c:2667-2669), -1 on the face-normal momentum at a slip wall
@@ -199,7 +200,7 @@ static void enqueue_rhs(shock_ctx *c, double *const in[5], int &nk)
         mark(c, "bc");
     }
     if (!c->p.inviscid) {
-        launch_nodal(c->G, c->p.precision, cin, c->F, s);
+        launch_nodal(c->G, c->P, c->p.precision, cin, c->F, s);
         nk++;
         mark(c, "nodal");
     }
@@ -344,6 +345,8 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
     if (int rc = check_faces(p)) return rc;
     if (p->mach <= 0 || p->reynolds <= 0 || p->gamma <= 1.0 || p->tau <= 0) return fail(SHOCK_EINVAL, "bad physics");
     if (!(p->weno_eps >= 0)) return fail(SHOCK_EINVAL, "weno_eps must be >= 0");
+    if (p->dim == 3 && p->full_metric && p->precision != SHOCK_FP64)
+        return fail(SHOCK_EINVAL, "full_metric is an FP64 form (precision SHOCK_FP64)");
 
     shock_ctx *c = new shock_ctx();
     c->p = *p;
@@ -1033,6 +1036,8 @@ int shock_multi_create(const shock_params *p, int nblocks, const shock_block *bl
     if (p->mms) return fail(SHOCK_EINVAL, "a division takes no manufactured solution");
     if (p->mach <= 0 || p->reynolds <= 0 || p->gamma <= 1.0 || p->tau <= 0) return fail(SHOCK_EINVAL, "bad physics");
     if (!(p->weno_eps >= 0)) return fail(SHOCK_EINVAL, "weno_eps must be >= 0");
+    if (p->dim == 3 && p->full_metric && p->precision != SHOCK_FP64)
+        return fail(SHOCK_EINVAL, "full_metric is an FP64 form (precision SHOCK_FP64)");
     const int dim = p->dim, g = (p->order + 1) / 2;
     std::vector<shock_params> ps(nblocks, *p);
     std::vector<BlockLink> links(nblocks);

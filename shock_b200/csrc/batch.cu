@@ -187,6 +187,7 @@ int check_params(const shock_batch *b, const shock_params *p)
     if (p->dim == 3 && !p->inviscid && !p->zeta_fix && p->nj > p->nk)
         return report_error(SHOCK_EINVAL, "zeta viscous stencil centred on j needs nj <= nk (src/ZD.c:547-548)");
     if (p->mms) return report_error(SHOCK_EINVAL, "batch members must be periodic blocks (mms = 0)");
+    if (p->dim == 3 && p->full_metric) return report_error(SHOCK_EINVAL, "batch members use the diagonal 3D metric (full_metric = 0)");
     for (int a = 0; a < p->dim; a++)
         if (!p->periodic[a]) return report_error(SHOCK_EINVAL, "axis %d is not periodic", a);
     for (int f = 0; f < 6; f++)

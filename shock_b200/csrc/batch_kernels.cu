@@ -175,7 +175,7 @@ __device__ __forceinline__ void run_item(int ph, const Member &M, const BatchIte
         for (int j = tid; j < chunk; j += NTHR) {
             const long long o = o0 + j;
             if (o >= M.G.NG) break;
-            nodal_body<DIM, ORDER, MIXED>(M.G, o, U[1], U[2], U[3], M.F.T, M.F);
+            nodal_body<DIM, ORDER, MIXED>(M.G, o, U[1], U[2], U[3], M.F.T, M.F, false);
         }
         break;
     }

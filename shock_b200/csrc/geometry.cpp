@@ -233,6 +233,13 @@ void create_metric(const shock_params &p, HostBlock &hb, ExtGrid &eg)
                 double z_xi, z_eta, x_zeta, y_zeta, z_zeta;
                 if (dim == 2) {
                     z_xi = 0.0; z_eta = 0.0; x_zeta = 0.0; y_zeta = 0.0; z_zeta = 1.0;
+                } else if (p.full_metric) {
+                    // the full metric: the cross derivatives SHOCK zeroes are kept
+                    z_xi = (-0.5 * ze[e.at(ie - 1, je, ke)] + 0.5 * ze[e.at(ie + 1, je, ke)]);
+                    z_eta = (-0.5 * ze[e.at(ie, je - 1, ke)] + 0.5 * ze[e.at(ie, je + 1, ke)]);
+                    x_zeta = (-0.5 * xe[e.at(ie, je, ke - 1)] + 0.5 * xe[e.at(ie, je, ke + 1)]);
+                    y_zeta = (-0.5 * ye[e.at(ie, je, ke - 1)] + 0.5 * ye[e.at(ie, je, ke + 1)]);
+                    z_zeta = (-0.5 * ze[e.at(ie, je, ke - 1)] + 0.5 * ze[e.at(ie, je, ke + 1)]);
                 } else {
                     z_zeta = (-0.5 * ze[e.at(ie, je, ke - 1)] + 0.5 * ze[e.at(ie, je, ke + 1)]);
                     y_xi = 0.0; z_xi = 0.0; x_eta = 0.0; z_eta = 0.0; x_zeta = 0.0; y_zeta = 0.0;

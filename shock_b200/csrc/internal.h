@@ -69,6 +69,7 @@ struct Phys {
     float eps32;
     int mms;
     int zeta_fix;
+    int full;            // 3D: the full curvilinear metric (cross terms kept)
     int walls;           // some face is a wall or farfield face
     double mcorr[6][3];  // per face: sign of the u,v,w convective momentum terms in its ghost
                          // points (SHOCK's BC_Corrector_*Momentum, src/WENO.c:265-277)
@@ -201,7 +202,8 @@ int launch_bc(const Grid &G, const Phys &P, const double *const U[5], double *co
 // field, F.p for SHOCK's copy of U_RK's p into U_lastStep at the end of a
 // step, src/SHOCK.c:661-664).
 void launch_bc_save(const Grid &G, const double *p, double *const plast[6], cudaStream_t s);
-void launch_nodal(const Grid &G, int precision, const double *const U[5], const Fields &F, cudaStream_t s);
+void launch_nodal(const Grid &G, const Phys &P, int precision, const double *const U[5], const Fields &F,
+                  cudaStream_t s);
 void launch_weno(const Grid &G, const Phys &P, int precision, int d, bool first,
                  const double *const U[5], const Fields &F, cudaStream_t s);
 void launch_viscous(const Grid &G, const Phys &P, int precision, int d, const double *const U[5],

@@ -348,6 +348,7 @@ int shock_server_submit(shock_server *s, const shock_params *p, const double *x,
         (p->time_order != 3 && p->time_order != 4) || (p->precision != SHOCK_FP64 && p->precision != SHOCK_MIXED))
         return report_error(SHOCK_EINVAL, "bad request class");
     if (p->mms) return report_error(SHOCK_EINVAL, "requests must be periodic blocks (mms = 0)");
+    if (p->dim == 3 && p->full_metric) return report_error(SHOCK_EINVAL, "requests use the diagonal 3D metric (full_metric = 0)");
     for (int a = 0; a < p->dim; a++)
         if (!p->periodic[a]) return report_error(SHOCK_EINVAL, "axis %d is not periodic", a);
     for (int f = 0; f < 6; f++)

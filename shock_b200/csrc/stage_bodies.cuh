@@ -193,7 +193,7 @@ __device__ __forceinline__ double ndv(const Fields &F, int idx, long long o)
 template <int DIM, int ORDER, bool MIXED>
 __device__ __forceinline__ void nodal_body(const Grid &G, long long o, const double *__restrict__ U,
                                            const double *__restrict__ V, const double *__restrict__ W,
-                                           const double *__restrict__ T, const Fields &F)
+                                           const double *__restrict__ T, const Fields &F, bool with_T)
 {
     constexpr int H = ZD<ORDER>::H;
     Idx3 p = unflatten(G, o);
@@ -204,7 +204,7 @@ __device__ __forceinline__ void nodal_body(const Grid &G, long long o, const dou
         long long sd = G.st[d];
 #pragma unroll
         for (int q = 0; q < 4; q++) {
-            if (DIM == 3 && q == 3) continue;   // T derivatives unused with the diagonal 3D metric
+            if (DIM == 3 && q == 3 && !with_T) continue;   // T derivatives unused with the diagonal 3D metric
             if (DIM == 2 && q == 2) continue;   // no w in 2D
             double acc = 0.0;
 #pragma unroll
@@ -562,9 +562,11 @@ static_assert(TL == TL_HOST && NTHR == NTHR_HOST, "host copies of the tile const
 // Per-point values staged for the WENO face computation.
 enum { WF0 = 0, WU0 = 5, WVU = 10, WVV, WVW, WC, WLAM, WJ, WN0 };
 
-template <int DIM>
+// FULL: the 3D curvilinear metric with its cross terms (three normal
+// components per point); otherwise the diagonal 3D metric has one.
+template <int DIM, bool FULL = false>
 struct WenoNV {
-    static constexpr int NN = DIM == 3 ? 1 : 2;   // stored components of the unit normal
+    static constexpr int NN = DIM == 3 ? (FULL ? 3 : 1) : 2;   // stored components of the unit normal
     static constexpr int NV = WN0 + NN;
 };
 
@@ -594,7 +596,7 @@ __device__ __forceinline__ Tile make_tile(const Grid &G, int lane, int bx, int b
 
 // Stage point fluxes, conserved variables, face-state inputs and the local
 // spectral radius of NP points per lane: points c0-1-r .. c0+TLN+r.
-template <int DIM, int ORDER, int D, int TLN = TL>
+template <int DIM, int ORDER, int D, int TLN = TL, bool FULL = false>
 __device__ __forceinline__ void stage_weno(const Grid &G, const Phys &P, const Tile &T, double *sh,
                                            const double *__restrict__ R, const double *__restrict__ Uu,
                                            const double *__restrict__ Vv, const double *__restrict__ Ww,
@@ -622,7 +624,13 @@ __device__ __forceinline__ void stage_weno(const Grid &G, const Phys &P, const T
         double rho = R[o], u = Uu[o], v = Vv[o], w = (DIM == 3) ? Ww[o] : 0.0, e = Ee[o];
         double p = F.p[o], c = F.c[o], J = F.J[o];
         double mx, my, mz, th, nrm;
-        if (DIM == 3) {
+        if (DIM == 3 && FULL) {
+            mx = F.m[3 * D + 0][o];
+            my = F.m[3 * D + 1][o];
+            mz = F.m[3 * D + 2][o];
+            th = u * mx + v * my + w * mz;
+            nrm = sqrt(mx * mx + my * my + mz * mz);
+        } else if (DIM == 3) {
             double mm = F.m[3 * D + D][o];
             mx = D == 0 ? mm : 0.0;
             my = D == 1 ? mm : 0.0;
@@ -662,7 +670,11 @@ __device__ __forceinline__ void stage_weno(const Grid &G, const Phys &P, const T
         SH(WC, t, l) = c;
         SH(WLAM, t, l) = fabs(th) + c * nrm;
         SH(WJ, t, l) = J;
-        if (DIM == 3) {
+        if (DIM == 3 && FULL) {
+            SH(WN0, t, l) = mx / nrm;
+            SH(WN0 + 1, t, l) = my / nrm;
+            SH(WN0 + 2, t, l) = mz / nrm;
+        } else if (DIM == 3) {
             SH(WN0, t, l) = (D == 0 ? mx : D == 1 ? my : mz) / nrm;
         } else {
             SH(WN0, t, l) = mx / nrm;
@@ -678,7 +690,7 @@ struct FaceState {
     T u, v, w, rho, c, nx, ny, nz, q2, un, gc, irho, isc, kin, gm, ic, g1c, hc;
 };
 
-template <int DIM, int ORDER, int D, typename T, int TLN = TL>
+template <int DIM, int ORDER, int D, typename T, int TLN = TL, bool FULL = false>
 __device__ __forceinline__ FaceState<T> face_state(const Phys &P, const double *sh, int ta, int lane)
 {
     constexpr int r = (ORDER - 1) / 2;
@@ -691,7 +703,11 @@ __device__ __forceinline__ FaceState<T> face_state(const Phys &P, const double *
     s.w = T(0.5) * (T)(SH(WVW, ta, lane) + SH(WVW, ta + 1, lane));
     s.rho = T(0.5) * (T)(SH(WU0, ta, lane) + SH(WU0, ta + 1, lane));
     s.c = T(0.5) * (T)(SH(WC, ta, lane) + SH(WC, ta + 1, lane));
-    if (DIM == 3) {
+    if (DIM == 3 && FULL) {
+        s.nx = T(0.5) * (T)(SH(WN0, ta, lane) + SH(WN0, ta + 1, lane));
+        s.ny = T(0.5) * (T)(SH(WN0 + 1, ta, lane) + SH(WN0 + 1, ta + 1, lane));
+        s.nz = T(0.5) * (T)(SH(WN0 + 2, ta, lane) + SH(WN0 + 2, ta + 1, lane));
+    } else if (DIM == 3) {
         T nd = T(0.5) * (T)(SH(WN0, ta, lane) + SH(WN0, ta + 1, lane));
         s.nx = D == 0 ? nd : T(0);
         s.ny = D == 1 ? nd : T(0);
@@ -775,11 +791,12 @@ __device__ __forceinline__ void add_right_col(const FaceState<T> &s, int ch, T p
 // sweep axis D): the two entropy/vorticity rows ch != D then have exact
 // zeros everywhere except at the density and at the momentum of the third
 // axis a = 3 - D - ch.  In 2D the w momentum and its flux are exact zeros,
-// and row 2 has a zero energy entry (-gc nz).
-template <int DIM, int D>
+// and row 2 has a zero energy entry (-gc nz).  The full 3D metric has no
+// zero entries.
+template <int DIM, int D, bool FULL = false>
 __host__ __device__ constexpr unsigned row_mask(int ch)
 {
-    return DIM == 2 ? (ch == 2 ? 0x07u : 0x17u)
+    return FULL ? 0x1Fu : DIM == 2 ? (ch == 2 ? 0x07u : 0x17u)
                     : (ch == D || ch >= 3) ? 0x1Fu : (1u | (1u << (1 + (3 - D - ch))));
 }
 
@@ -940,12 +957,12 @@ __device__ __forceinline__ double weno_phi_fp64(const double *Pp, const double *
 }
 
 // Characteristic rows CA and CB (CB < 0: CA alone) of one face.
-template <int DIM, int ORDER, int D, int TLN, int CA, int CB>
+template <int DIM, int ORDER, int D, int TLN, int CA, int CB, bool FULL = false>
 __device__ __forceinline__ void weno_rows_fp64(const Phys &P, const FaceState<double> &s, const double *sh, int f,
                                                int lane, double a, double *phi)
 {
     constexpr int NS = ORDER + 1;
-    constexpr unsigned MA = row_mask<DIM, D>(CA), MB = CB >= 0 ? row_mask<DIM, D>(CB) : 0u;
+    constexpr unsigned MA = row_mask<DIM, D, FULL>(CA), MB = CB >= 0 ? row_mask<DIM, D, FULL>(CB) : 0u;
     asm volatile("" ::: "memory");
     double LA[5], LB[5];
     left_row<double>(s, CA, LA[0], LA[1], LA[2], LA[3], LA[4]);
@@ -999,14 +1016,14 @@ __device__ __forceinline__ void add_right_col_diag(const FaceState<T> &s, T phi,
 // Phi-, back-projection.  f: face index in the tile (points f..f+2r+1).
 // WENO5 takes the rows in three passes that share loads: the two sparse
 // entropy/vorticity rows, the full one, the two acoustic rows.
-template <int DIM, int ORDER, int D, int TLN = TL>
+template <int DIM, int ORDER, int D, int TLN = TL, bool FULL = false>
 __device__ __forceinline__ void face_weno_fp64(const Phys &P, const double *sh, int f, int lane, double *out)
 {
     constexpr int r = (ORDER - 1) / 2;
     constexpr int NP = TLN + 2 * r + 2;
 #define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
     const int ta = r + f;
-    const FaceState<double> s = face_state<DIM, ORDER, D, double, TLN>(P, sh, ta, lane);
+    const FaceState<double> s = face_state<DIM, ORDER, D, double, TLN, FULL>(P, sh, ta, lane);
     const double jh = (SH(WJ, ta, lane) + SH(WJ, ta + 1, lane)) / 2.0;
     double lam = 0.0;
 #pragma unroll
@@ -1017,23 +1034,24 @@ __device__ __forceinline__ void face_weno_fp64(const Phys &P, const double *sh, 
 #undef SH
     const double a = lam * jh;
     double phi[5];
+    constexpr bool DIAG = DIM == 3 && !FULL;   // one nonzero normal component
     if (ORDER == 5) {
-        constexpr int C1 = DIM == 2 ? 0 : (D == 0 ? 1 : 0);
-        constexpr int C2 = DIM == 2 ? 1 : (D == 2 ? 1 : 2);
-        constexpr int CF = DIM == 2 ? 2 : D;
-        weno_rows_fp64<DIM, ORDER, D, TLN, C1, C2>(P, s, sh, f, lane, a, phi);
-        weno_rows_fp64<DIM, ORDER, D, TLN, CF, -1>(P, s, sh, f, lane, a, phi);
-        weno_rows_fp64<DIM, ORDER, D, TLN, 3, 4>(P, s, sh, f, lane, a, phi);
+        constexpr int C1 = !DIAG ? 0 : (D == 0 ? 1 : 0);
+        constexpr int C2 = !DIAG ? 1 : (D == 2 ? 1 : 2);
+        constexpr int CF = !DIAG ? 2 : D;
+        weno_rows_fp64<DIM, ORDER, D, TLN, C1, C2, FULL>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, CF, -1, FULL>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, 3, 4, FULL>(P, s, sh, f, lane, a, phi);
     } else {
-        weno_rows_fp64<DIM, ORDER, D, TLN, 0, -1>(P, s, sh, f, lane, a, phi);
-        weno_rows_fp64<DIM, ORDER, D, TLN, 1, -1>(P, s, sh, f, lane, a, phi);
-        weno_rows_fp64<DIM, ORDER, D, TLN, 2, -1>(P, s, sh, f, lane, a, phi);
-        weno_rows_fp64<DIM, ORDER, D, TLN, 3, -1>(P, s, sh, f, lane, a, phi);
-        weno_rows_fp64<DIM, ORDER, D, TLN, 4, -1>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, 0, -1, FULL>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, 1, -1, FULL>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, 2, -1, FULL>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, 3, -1, FULL>(P, s, sh, f, lane, a, phi);
+        weno_rows_fp64<DIM, ORDER, D, TLN, 4, -1, FULL>(P, s, sh, f, lane, a, phi);
     }
 #pragma unroll
     for (int q = 0; q < 5; q++) out[q] = 0.0;
-    if (DIM == 3) {
+    if (DIAG) {
         add_right_col_diag<D, 0>(s, phi[0], out);
         add_right_col_diag<D, 1>(s, phi[1], out);
         add_right_col_diag<D, 2>(s, phi[2], out);
@@ -1276,7 +1294,7 @@ __device__ __forceinline__ double central(const double *sh, int NP, int q, int t
 // ---------------------------------------------------------------------------
 // WENO5 fits 128 registers (two tiles per SM); the WENO9 face needs more,
 // so it runs one tile per SM without spilling.
-template <int DIM, int ORDER, int D, bool MIXED, int TLN = TL>
+template <int DIM, int ORDER, int D, bool MIXED, int TLN = TL, bool FULL = false>
 __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool first, const double *__restrict__ R,
                                           const double *__restrict__ Uu, const double *__restrict__ Vv,
                                           const double *__restrict__ Ww, const double *__restrict__ Ee,
@@ -1284,7 +1302,8 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
 {
     constexpr int r = (ORDER - 1) / 2;
     constexpr int NP = TLN + 2 * r + 2;
-    constexpr int NV = WenoNV<DIM>::NV;
+    constexpr int NV = WenoNV<DIM, FULL>::NV;
+    static_assert(!(FULL && (MIXED || DIM != 3)), "the full metric is a 3D FP64 form");
     constexpr int NFT = TLN + 1;                        // faces per line
     constexpr int FPT = NFT / NROWT;                    // faces per thread
     static_assert(NFT % NROWT == 0 && (FPT == 1 || FPT == 2), "tile length");
@@ -1294,7 +1313,7 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
     const int lane = threadIdx.x, row = threadIdx.y;
     const Tile T = make_tile<DIM, D, TLN>(G, lane, bx, by, bz);
 
-    stage_weno<DIM, ORDER, D, TLN>(G, P, T, sh, R, Uu, Vv, Ww, Ee, F);
+    stage_weno<DIM, ORDER, D, TLN, FULL>(G, P, T, sh, R, Uu, Vv, Ww, Ee, F);
     __syncthreads();
     if (MIXED) {
         // Central parts first, into registers (they need the FP64 point
@@ -1365,7 +1384,7 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
     const bool ok0 = T.lane_ok && (T.c0 - 1 + row) <= G.g + T.nD - 1;
     if (ok0) {
         double w5[5];
-        face_weno_fp64<DIM, ORDER, D, TLN>(P, sh, row, lane, w5);
+        face_weno_fp64<DIM, ORDER, D, TLN, FULL>(P, sh, row, lane, w5);
 #pragma unroll
         for (int q = 0; q < 5; q++) res[q] = w5[q] + central<ORDER>(sh, NP, q, r + row, lane);
     }
@@ -1384,7 +1403,7 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
         const int f = row;
         if (T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1) {
             double w5[5];
-            face_weno_fp64<DIM, ORDER, D, TLN>(P, sh, f, lane, w5);
+            face_weno_fp64<DIM, ORDER, D, TLN, FULL>(P, sh, f, lane, w5);
 #pragma unroll
             for (int q = 0; q < 5; q++) f0[(q * NROWT + row) * NLANE + lane] = w5[q] + central<ORDER>(sh, NP, q, r + f, lane);
         }
@@ -1395,7 +1414,7 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
         ok1 = T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1;
         if (ok1) {
             double w5[5];
-            face_weno_fp64<DIM, ORDER, D, TLN>(P, sh, f, lane, w5);
+            face_weno_fp64<DIM, ORDER, D, TLN, FULL>(P, sh, f, lane, w5);
 #pragma unroll
             for (int q = 0; q < 5; q++) res[q] = w5[q] + central<ORDER>(sh, NP, q, r + f, lane);
         }
@@ -1855,6 +1874,244 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
 }
 
 // ---------------------------------------------------------------------------
+// visc_full: the viscous flux difference with the full 3D curvilinear metric
+// (src/ZD.c:47-694 over the 30 factors of src/Functions.c:6245-6386, all of
+// them nonzero), FP64.  Per point the tile stages u, v, w, T, the eight
+// nodal derivatives of u, v, w, T across the sweep, mu J and the nine metric
+// terms; a face combines its twelve derivatives with the factors
+//   K[i][k][m] = J ( delta_ik a.grad(xi_m) + a_k dxi_m/dx_i - 2/3 a_i dxi_m/dx_k ),
+//   heat[m]    = J a.grad(xi_m),   a = grad(xi_D),
+// weighted by mu at both face points and averaged.
+// ---------------------------------------------------------------------------
+enum { VFU = 0, VFV, VFW, VFT, VFX, VFMJ = VFX + 8, VFG, VFNV = VFG + 9 };
+
+// Momentum (g[0..2]) and heat (h) flux of one face from its derivatives
+// Dv[k][m] (velocity component k along direction m) and DT[m]; ta is the
+// staged index of the face's left point.
+template <int D, int NP>
+__device__ __forceinline__ void visc_face_full(const double *sh, int ta, int lane, const double (&Dv)[3][3],
+                                               const double (&DT)[3], double *g, double &h)
+{
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
+    const double t23 = 2.0 / 3.0;
+    g[0] = g[1] = g[2] = 0.0;
+    h = 0.0;
+#pragma unroll
+    for (int side = 0; side < 2; side++) {
+        const int t = ta + side;
+        const double mj = SH(VFMJ, t, lane);
+        double gm[3][3];
+#pragma unroll
+        for (int m = 0; m < 3; m++)
+#pragma unroll
+            for (int x = 0; x < 3; x++) gm[m][x] = SH(VFG + 3 * m + x, t, lane);
+        double s3[3] = {0.0, 0.0, 0.0}, sh0 = 0.0;
+#pragma unroll
+        for (int m = 0; m < 3; m++) {
+            const double adot = gm[D][0] * gm[m][0] + gm[D][1] * gm[m][1] + gm[D][2] * gm[m][2];
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    const double K = (i == k ? adot : 0.0) + gm[D][k] * gm[m][i] - t23 * gm[D][i] * gm[m][k];
+                    s3[i] += Dv[k][m] * K;
+                }
+            sh0 += DT[m] * adot;
+        }
+#pragma unroll
+        for (int i = 0; i < 3; i++) g[i] += 0.5 * mj * s3[i];
+        h += 0.5 * mj * sh0;
+    }
+#undef SH
+}
+
+template <int ORDER, int D, int TLN>
+__device__ __forceinline__ void visc_body_full(const Grid &G, const Phys &P, const double *__restrict__ Uu,
+                                               const double *__restrict__ Vv, const double *__restrict__ Ww,
+                                               const Fields &F, int bx, int by, int bz)
+{
+    using A = Axes<3, D>;
+    constexpr int H = ZD<ORDER>::H;
+    constexpr int NP = TLN + 2 * H;
+    constexpr int MA = (D == 0) ? 1 : 0;     // the two non-sweep axes
+    constexpr int MB = (D == 2) ? 1 : 2;
+    constexpr int NFT = TLN + 1;
+    constexpr int FPT = NFT / NROWT;
+    static_assert(NFT % NROWT == 0 && (FPT == 1 || FPT == 2), "tile length");
+    const bool quirk = (D == 2 && !P.zeta_fix);
+
+    extern __shared__ double smem[];
+    double *sh = smem;                       // [VFNV][NP][NLS]
+    double *fo = smem + VFNV * NP * NLS;     // [8][NFT][NLS]: the face fluxes (quirk: plus-side set, minus-side set)
+    double *qd = fo + 8 * NFT * NLS;         // quirk: [24][NLANE] per-line half-point derivatives
+#define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
+#define FO(c, f, l) fo[((c) * NFT + (f)) * NLS + (l)]
+#define QD(c, l) qd[(c) * NLANE + (l)]
+
+    const int lane = threadIdx.x, row = threadIdx.y;
+    const Tile T = make_tile<3, D, TLN>(G, lane, bx, by, bz);
+    const int tid = row * NLANE + lane;
+    constexpr int NSTG = (NP * NLANE + NTHR - 1) / NTHR;
+#pragma unroll
+    for (int m = 0; m < NSTG; m++) {
+        const int it = tid + m * NTHR;
+        if (it >= NP * NLANE) continue;
+        const int l = A::CONTIG ? it / NP : it % NLANE, t = A::CONTIG ? it % NP : it / NLANE;
+        const int pd = T.c0 - H + t;
+        if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
+        const long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
+        SH(VFU, t, l) = Uu[o];
+        SH(VFV, t, l) = Vv[o];
+        SH(VFW, t, l) = Ww[o];
+        SH(VFT, t, l) = F.T[o];
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            SH(VFX + 2 * q, t, l) = F.Nd[3 * q + MA][o];
+            SH(VFX + 2 * q + 1, t, l) = F.Nd[3 * q + MB][o];
+        }
+        SH(VFMJ, t, l) = F.mu[o] * F.J[o];
+#pragma unroll
+        for (int q = 0; q < 9; q++) SH(VFG + q, t, l) = F.m[q][o];
+    }
+    if (quirk && T.lane_ok) {
+        // half-point stencils along k centred on the j index (src/ZD.c:547-548),
+        // the same for every cell of the line: per side the derivatives of
+        // u, v, w, T along zeta and the interpolated u, v, w, T derivatives
+        // along xi and eta, 24 values per lane, 3 per row
+        const int jj = T.l0 + lane;
+        const long long lb = T.base + (long long)lane * T.sL;   // (i, j, 0)
+        const double *vs[4] = {Uu, Vv, Ww, F.T};
+#pragma unroll
+        for (int k3 = 0; k3 < 3; k3++) {
+            const int idx = row * 3 + k3;                       // side*12 + quantity
+            const int side = idx / 12, qn = idx % 12;
+            double acc = 0.0;
+            if (qn < 4) {
+#pragma unroll
+                for (int l = 0; l < 2 * H; l++) acc += ZD<ORDER>::half(l) * vs[qn][lb + (jj + l - H + side)];
+            } else {
+                const int var = (qn - 4) >> 1, ax = ((qn - 4) & 1) ? MB : MA;
+#pragma unroll
+                for (int l = 0; l < 2 * H; l++)
+                    acc += ZD<ORDER>::interp(l) * F.Nd[3 * var + ax][lb + (jj + l - H + side)];
+            }
+            QD(idx, lane) = acc;
+        }
+    }
+    __syncthreads();
+
+#pragma unroll
+    for (int k = 0; k < FPT; k++) {
+        const int f = row + k * NROWT;   // face (c0-1+f)+1/2: staged points f .. f+2H-1
+        if (!(T.lane_ok && (T.c0 - 1 + f) <= G.g + T.nD - 1)) continue;
+        const int ta = f + H - 1;
+        double Dv[3][3], DT[3], g3[3], hh;
+        if (quirk) {
+            // the plus-side set (the upper face of cell f-1) into 0..3, the
+            // minus-side set (the lower face of cell f) into 4..7
+#pragma unroll
+            for (int side = 1; side >= 0; side--) {
+                const int b = side * 12;
+#pragma unroll
+                for (int q = 0; q < 3; q++) {
+                    Dv[q][D] = QD(b + q, lane);
+                    Dv[q][MA] = QD(b + 4 + 2 * q, lane);
+                    Dv[q][MB] = QD(b + 5 + 2 * q, lane);
+                }
+                DT[D] = QD(b + 3, lane);
+                DT[MA] = QD(b + 10, lane);
+                DT[MB] = QD(b + 11, lane);
+                visc_face_full<D, NP>(sh, ta, lane, Dv, DT, g3, hh);
+                const int c0 = side ? 0 : 4;
+                FO(c0 + 0, f, lane) = g3[0]; FO(c0 + 1, f, lane) = g3[1]; FO(c0 + 2, f, lane) = g3[2];
+                FO(c0 + 3, f, lane) = hh;
+            }
+        } else {
+            double acc[12];
+#pragma unroll
+            for (int q = 0; q < 12; q++) acc[q] = 0.0;
+#pragma unroll
+            for (int l = 0; l < 2 * H; l++) {
+                const int t = f + l;
+                const double ch = ZD<ORDER>::half(l), ci = ZD<ORDER>::interp(l);
+#pragma unroll
+                for (int q = 0; q < 4; q++) acc[q] += ch * SH(VFU + q, t, lane);
+#pragma unroll
+                for (int q = 0; q < 8; q++) acc[4 + q] += ci * SH(VFX + q, t, lane);
+            }
+#pragma unroll
+            for (int q = 0; q < 3; q++) {
+                Dv[q][D] = acc[q];
+                Dv[q][MA] = acc[4 + 2 * q];
+                Dv[q][MB] = acc[5 + 2 * q];
+            }
+            DT[D] = acc[3];
+            DT[MA] = acc[10];
+            DT[MB] = acc[11];
+            visc_face_full<D, NP>(sh, ta, lane, Dv, DT, g3, hh);
+            FO(0, f, lane) = g3[0]; FO(1, f, lane) = g3[1]; FO(2, f, lane) = g3[2];
+            FO(3, f, lane) = hh;
+        }
+    }
+    __syncthreads();
+
+    const double t23 = 2.0 / 3.0;
+    for (int it = row * NLANE + lane; it < TLN * NLANE; it += NTHR) {
+        int cr, ln;
+        if (A::CONTIG) { cr = it % TLN; ln = it / TLN; }
+        else { ln = it % NLANE; cr = it / NLANE; }
+        if (T.l0 + ln >= G.g + T.nL || T.c0 + cr > G.g + T.nD - 1) continue;
+        const long long o = T.base + (long long)ln * T.sL + (long long)(T.c0 + cr) * T.sD;
+        const int ts = cr + H;
+        const int cm = quirk ? 4 : 0;
+        double dg[3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) dg[q] = FO(q, cr + 1, ln) - FO(cm + q, cr, ln);
+        const double dh = FO(3, cr + 1, ln) - FO(cm + 3, cr, ln);
+        const double vel[3] = {SH(VFU, ts, ln), SH(VFV, ts, ln), SH(VFW, ts, ln)};
+        // node term: mu sum_i N[i][D] sum_{k,m} N[k][m] Fac[i][k][m] at the cell
+        double N[3][3];
+#pragma unroll
+        for (int q = 0; q < 3; q++) {
+            N[q][D] = F.Nd[3 * q + D][o];
+            N[q][MA] = SH(VFX + 2 * q, ts, ln);
+            N[q][MB] = SH(VFX + 2 * q + 1, ts, ln);
+        }
+        double gm[3][3];
+#pragma unroll
+        for (int m = 0; m < 3; m++)
+#pragma unroll
+            for (int x = 0; x < 3; x++) gm[m][x] = SH(VFG + 3 * m + x, ts, ln);
+        double hs[3] = {0.0, 0.0, 0.0};
+#pragma unroll
+        for (int m = 0; m < 3; m++) {
+            const double adot = gm[D][0] * gm[m][0] + gm[D][1] * gm[m][1] + gm[D][2] * gm[m][2];
+#pragma unroll
+            for (int k = 0; k < 3; k++)
+#pragma unroll
+                for (int i = 0; i < 3; i++) {
+                    const double K = (i == k ? adot : 0.0) + gm[D][k] * gm[m][i] - t23 * gm[D][i] * gm[m][k];
+                    hs[i] += N[k][m] * K;
+                }
+        }
+        const double nodeB = SH(VFMJ, ts, ln) * (N[0][D] * hs[0] + N[1][D] * hs[1] + N[2][D] * hs[2]);
+        const double psi = P.psi;
+        const double q1 = F.Q[1][o], q2 = F.Q[2][o], q3 = F.Q[3][o], q4 = F.Q[4][o];
+        F.Q[1][o] = q1 + psi * dg[0];
+        F.Q[2][o] = q2 + psi * dg[1];
+        F.Q[3][o] = q3 + psi * dg[2];
+        const double Aterm = vel[0] * dg[0] + vel[1] * dg[1] + vel[2] * dg[2];
+        // the heat flux's Gamma average of the cell and its upper neighbour
+        // (src/ZD.c:194): Gamma_wall at the last cell below an isothermal wall
+        const double gup = (P.walls && P.iso_hi[D] && T.c0 + cr == G.g + T.nD - 1) ? P.gam_w : P.gam;
+        F.Q[4][o] = q4 + 0.5 * (gup + P.gam) * dh + psi * (Aterm + nodeB);
+    }
+#undef SH
+#undef FO
+#undef QD
+}
+
+// ---------------------------------------------------------------------------
 // RK stage update of the real points (src/Functions.c:2300-2365), with the
 // time-independent source J*S added to Q first.
 // ---------------------------------------------------------------------------
@@ -2052,12 +2309,18 @@ __device__ __forceinline__ void post_body(const Grid &G, double mach, const doub
 }
 
 // Dynamic shared memory of the sweep bodies.
-template <int DIM, int ORDER, bool MIXED, int TLN = TL>
+template <int DIM, int ORDER, bool MIXED, int TLN = TL, bool FULL = false>
 constexpr size_t weno_smem_bytes()
 {
     // (+ the face-flux buffer of the first faces when a thread takes two)
-    return sizeof(double) * ((size_t)WenoNV<DIM>::NV * (TLN + ORDER + 1) * NLS +
+    return sizeof(double) * ((size_t)WenoNV<DIM, FULL>::NV * (TLN + ORDER + 1) * NLS +
                              ((MIXED || TLN + 1 == NROWT) ? 0 : 5 * NROWT * NLANE));
+}
+
+template <int ORDER, int TLN>
+constexpr size_t visc_full_smem_bytes()
+{
+    return sizeof(double) * ((size_t)VFNV * (TLN + ORDER + 1) * NLS + 8 * (TLN + 1) * NLS + 24 * NLANE);
 }
 
 template <int DIM, int ORDER, int TLN = TL>

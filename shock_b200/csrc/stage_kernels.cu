@@ -62,10 +62,10 @@ __global__ void k_prim(Grid G, Phys P, const double *__restrict__ R, const doubl
 
 template <int DIM, int ORDER, bool MIXED>
 __global__ void k_nodal(Grid G, const double *__restrict__ U, const double *__restrict__ V,
-                        const double *__restrict__ W, const double *__restrict__ T, Fields F)
+                        const double *__restrict__ W, const double *__restrict__ T, Fields F, bool with_T)
 {
     long long o = blockIdx.x * (long long)blockDim.x + threadIdx.x;
-    if (o < G.NG) nodal_body<DIM, ORDER, MIXED>(G, o, U, V, W, T, F);
+    if (o < G.NG) nodal_body<DIM, ORDER, MIXED>(G, o, U, V, W, T, F, with_T);
 }
 
 #ifndef SHOCK_W9_FP64_TL
@@ -117,6 +117,25 @@ template <int DIM, int D>
 struct ViscTile {
     static constexpr int v = (D == DIM - 1) ? TL : 7;
 };
+
+// The full 3D metric (FP64): the WENO face with full characteristic rows
+// takes the 15-cell tile and one tile per SM, as the 2D WENO9 face; the
+// viscous tile stages 22 values per point, one tile per SM.
+template <int ORDER, int D>
+__global__ void __launch_bounds__(NTHR, ORDER == 5 ? 2 : 1)
+    k_weno_full(Grid G, Phys P, bool first, const double *__restrict__ R, const double *__restrict__ Uu,
+                const double *__restrict__ Vv, const double *__restrict__ Ww, const double *__restrict__ Ee, Fields F)
+{
+    weno_body<3, ORDER, D, false, TL, true>(G, P, first, R, Uu, Vv, Ww, Ee, F, blockIdx.x, blockIdx.y, blockIdx.z);
+}
+
+template <int ORDER, int D>
+__global__ void __launch_bounds__(NTHR, 1)
+    k_visc_full(Grid G, Phys P, const double *__restrict__ Uu, const double *__restrict__ Vv,
+                const double *__restrict__ Ww, Fields F)
+{
+    visc_body_full<ORDER, D, ViscTile<3, D>::v>(G, P, Uu, Vv, Ww, F, blockIdx.x, blockIdx.y, blockIdx.z);
+}
 
 template <int DIM, int ORDER, int D, bool MIXED>
 __global__ void __launch_bounds__(NTHR, ViscTile<DIM, D>::v == TL ? 2 : 3)
@@ -264,13 +283,15 @@ void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const F
         k_prim<2><<<blocks_for(G.NG, 256 * PRIM_PTS), 256, 0, s>>>(G, P, U[0], U[1], U[2], U[3], U[4], F.p, F.T, F.c, F.mu);
 }
 
-void launch_nodal(const Grid &G, int precision, const double *const U[5], const Fields &F, cudaStream_t s)
+void launch_nodal(const Grid &G, const Phys &P, int precision, const double *const U[5], const Fields &F,
+                  cudaStream_t s)
 {
     const unsigned nb = blocks_for(G.NG, 256);
+    const bool wT = P.full != 0;   // the full 3D metric also reads the temperature derivatives
 #define N(DIM, ORD)                                                                                    \
     if (G.dim == DIM && G.order == ORD) {                                                              \
-        if (precision == SHOCK_MIXED) k_nodal<DIM, ORD, true><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F); \
-        else k_nodal<DIM, ORD, false><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F);                 \
+        if (precision == SHOCK_MIXED) k_nodal<DIM, ORD, true><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F, wT); \
+        else k_nodal<DIM, ORD, false><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F, wT);                 \
         return;                                                                                        \
     }
     N(3, 5) N(3, 9) N(2, 5) N(2, 9)
@@ -300,6 +321,31 @@ static void weno_one(const Grid &G, const Phys &P, bool first, const double *con
                                                                                              U[2], U[3], U[4], F);
 }
 
+template <int ORDER, int D>
+static void weno_full_one(const Grid &G, const Phys &P, bool first, const double *const U[5], const Fields &F,
+                          cudaStream_t s)
+{
+    constexpr size_t smem = weno_smem_bytes<3, ORDER, false, TL, true>();
+    if (!G.order) {
+        cudaFuncSetAttribute(k_weno_full<ORDER, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        return;
+    }
+    k_weno_full<ORDER, D><<<sweep_grid<3, D, TL>(G), dim3(NLANE, NROWT), smem, s>>>(G, P, first, U[0], U[1], U[2],
+                                                                                    U[3], U[4], F);
+}
+
+template <int ORDER, int D>
+static void visc_full_one(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s)
+{
+    constexpr int VTL = ViscTile<3, D>::v;
+    constexpr size_t smem = visc_full_smem_bytes<ORDER, VTL>();
+    if (!G.order) {
+        cudaFuncSetAttribute(k_visc_full<ORDER, D>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        return;
+    }
+    k_visc_full<ORDER, D><<<sweep_grid<3, D, VTL>(G), dim3(NLANE, NROWT), smem, s>>>(G, P, U[1], U[2], U[3], F);
+}
+
 template <int DIM, int ORDER, int D, bool MIXED>
 static void visc_one(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s)
 {
@@ -321,7 +367,8 @@ void launch_weno(const Grid &G, const Phys &P, int precision, int d, bool first,
 {
 #define W(DIM, ORD, D)                                                                  \
     if (G.dim == DIM && G.order == ORD && d == D) {                                      \
-        if (precision == SHOCK_MIXED) weno_one<DIM, ORD, D, true>(G, P, first, U, F, s); \
+        if (DIM == 3 && P.full) weno_full_one<ORD, D>(G, P, first, U, F, s);              \
+        else if (precision == SHOCK_MIXED) weno_one<DIM, ORD, D, true>(G, P, first, U, F, s); \
         else weno_one<DIM, ORD, D, false>(G, P, first, U, F, s);                         \
         return;                                                                          \
     }
@@ -334,7 +381,8 @@ void launch_viscous(const Grid &G, const Phys &P, int precision, int d, const do
 {
 #define V(DIM, ORD, D)                                                               \
     if (G.dim == DIM && G.order == ORD && d == D) {                                   \
-        if (precision == SHOCK_MIXED) visc_one<DIM, ORD, D, true>(G, P, U, F, s);     \
+        if (DIM == 3 && P.full) visc_full_one<ORD, D>(G, P, U, F, s);                  \
+        else if (precision == SHOCK_MIXED) visc_one<DIM, ORD, D, true>(G, P, U, F, s); \
         else visc_one<DIM, ORD, D, false>(G, P, U, F, s);                             \
         return;                                                                       \
     }
@@ -407,6 +455,9 @@ void prepare_kernels()
     visc_one<DIM, ORD, D, false>(G, P, U, F, 0); visc_one<DIM, ORD, D, true>(G, P, U, F, 0);
     SHOCK_SWEEP_CASES(A)
 #undef A
+#define AF(ORD, D) weno_full_one<ORD, D>(G, P, true, U, F, 0); visc_full_one<ORD, D>(G, P, U, F, 0);
+    AF(5, 0) AF(5, 1) AF(5, 2) AF(9, 0) AF(9, 1) AF(9, 2)
+#undef AF
 }
 
 // True when the current context already has the sweep kernels' raised

@@ -79,6 +79,8 @@ extern "C" int shock_rhs_static(const shock_params *p, const double *geom13, dou
     if (p->dim == 3 && !p->inviscid && !p->zeta_fix && p->nj > p->nk)
         return report_error(SHOCK_EINVAL, "zeta viscous stencil centred on j needs nj <= nk (src/ZD.c:547-548)");
     if (p->mms) return report_error(SHOCK_EINVAL, "shock_rhs_static takes periodic blocks only (mms = 0)");
+    if (p->dim == 3 && p->full_metric && p->precision != SHOCK_FP64)
+        return report_error(SHOCK_EINVAL, "full_metric is an FP64 form (precision SHOCK_FP64)");
     for (int a = 0; a < p->dim; a++)
         if (!p->periodic[a]) return report_error(SHOCK_EINVAL, "axis %d is not periodic", a);
     for (int f = 0; f < 6; f++)
@@ -126,7 +128,7 @@ extern "C" int shock_rhs_static(const shock_params *p, const double *geom13, dou
     if (!p->inviscid) CKS(cudaMemsetAsync(scratch + 4 * ng, 0, sizeof(double) * 12 * ng, s));
     launch_ghosts(G, U, s);
     launch_prim(G, P, cU, F, s);
-    if (!p->inviscid) launch_nodal(G, p->precision, cU, F, s);
+    if (!p->inviscid) launch_nodal(G, P, p->precision, cU, F, s);
     for (int d = 0; d < p->dim; d++) launch_weno(G, P, p->precision, d, d == 0, cU, F, s);
     if (!p->inviscid)
         for (int d = 0; d < p->dim; d++) launch_viscous(G, P, p->precision, d, cU, F, s);
