@@ -30,10 +30,31 @@ def skewed(order, n, seed):
     return c
 
 
+def skewed_bounded(c):
+    """The same shear on a block with wall, farfield, inflow or outflow
+    faces: the displacements keep the periodic axes periodic and move the
+    bounded faces off their planes."""
+    L = c.period
+    X, Y, Z = c.x.copy(), c.y.copy(), c.z.copy()
+    tp = 2 * math.pi
+    per = c.periodic
+
+    def wave(a, arr):   # periodic along a periodic axis, a half wave across a bounded one
+        return np.sin(tp * arr / L[a]) if per[a] else np.cos(math.pi * arr / L[a])
+
+    c.x = X + 0.03 * L[0] * wave(1, Y) * wave(2, Z)
+    c.y = Y + 0.03 * L[1] * wave(0, X) * wave(2, Z)
+    c.z = Z + 0.03 * L[2] * wave(0, X) * wave(1, Y)
+    c.tau = cases.cfl_tau(c)
+    c.name = "skewed_" + c.name
+    return c
+
+
 CASES = {
     "tgv12_w5": lambda: cases.taylor_green(12, order=5),
     "tgv12_w9": lambda: cases.taylor_green(12, order=9),
     "skewed_w5": lambda: skewed(5, (14, 11, 13), 3),
+    "skewed_channel_w5": lambda: skewed_bounded(cases.channel(3, 5, (14, 11, 12), bc="wall_inviscid")),
 }
 
 

@@ -14,7 +14,7 @@ import shock_b200
 from _util import real, rel_err
 from refbind import RefSolver, ref_available
 from shock_b200 import cases
-from test_full_metric_host import skewed
+from test_full_metric_host import skewed, skewed_bounded
 
 pytestmark = pytest.mark.gpu
 
@@ -34,6 +34,15 @@ CASES = {
     "skewed_w5": lambda: skewed(5, (18, 14, 16), 3),
     "skewed_w9": lambda: skewed(9, (20, 16, 17), 5),
     "skewed_w5_inviscid": lambda: _with(skewed(5, (16, 15, 17), 4), inviscid=True),
+    # faces: no-slip, slip and isothermal walls, farfield, inflow and outflow
+    "channel_wall_viscous_w5": lambda: skewed_bounded(cases.channel(3, 5, (16, 12, 14), bc="wall_viscous")),
+    "channel_wall_inviscid_w9": lambda: skewed_bounded(cases.channel(3, 9, (18, 14, 16), bc="wall_inviscid")),
+    "channel_wall_isothermal_w5": lambda: skewed_bounded(cases.channel(3, 5, (16, 12, 14), bc="wall_isothermal",
+                                                                       t_wall=1.1)),
+    "channel_farfield_w5": lambda: skewed_bounded(cases.channel(3, 5, (16, 12, 14), bc="farfield")),
+    "duct_riemann_rudy_w5": lambda: skewed_bounded(_with(cases.duct(3, 5, (18, 12, 13), inflow="inflow_riemann",
+                                                                    outflow="outflow_rudy"), l0=200.0)),
+    "duct_subsonic_w9": lambda: skewed_bounded(cases.duct(3, 9, (20, 14, 15))),
 }
 
 
