@@ -11,7 +11,13 @@
  *                   the (source, destination) mailbox and completes at once;
  *                   MPI_Irecv records the request, MPI_Test takes a full slot
  *                   with the matching tag (messages of one tag arrive in
- *                   order);
+ *                   order).  A rank's receives complete in the order it
+ *                   posted them: MPI leaves that order open, and SHOCK
+ *                   unpacks each interface as its receive completes, with
+ *                   the ghost corners of neighbouring interfaces written by
+ *                   both, so its results depend on the order.  Posting order
+ *                   is the schedule in which every message has arrived before
+ *                   the receiver polls, and makes the runs reproducible;
  *   collectives     Barrier (sense-reversing counter), Allgather, Reduce
  *                   (SUM, MAX), Bcast through a shared staging area;
  *   waits           every spin gives up after SHM_WAIT_S seconds and aborts
@@ -58,7 +64,11 @@ typedef struct {
     int used, src, tag, recv;
     void *buf;
     size_t bytes;
+    size_t post;              /* posting order */
+    int done;                 /* data received, not yet reported */
 } req_t;
+
+static size_t g_posted;
 
 static req_t g_req[4096];
 
@@ -176,7 +186,7 @@ int MPI_Irecv(void *b, int n, MPI_Datatype t, int s, int tag, MPI_Comm c, MPI_Re
     (void)c;
     for (int i = 1; i < 4096; i++)
         if (!g_req[i].used) {
-            g_req[i] = (req_t){1, s, tag, 1, b, (size_t)n * dtype_size(t)};
+            g_req[i] = (req_t){1, s, tag, 1, b, (size_t)n * dtype_size(t), ++g_posted, 0};
             *r = i;
             return 0;
         }
@@ -210,7 +220,17 @@ int MPI_Test(MPI_Request *r, int *f, MPI_Status *st)
     (void)st;
     if (*r == MPI_REQUEST_NULL) { *f = 1; return 0; }
     req_t *q = &g_req[*r];
-    *f = try_recv(q);
+    /* complete the pending receives posted up to this one, oldest first */
+    for (;;) {
+        req_t *old = NULL;
+        for (int i = 1; i < 4096; i++) {
+            req_t *c = &g_req[i];
+            if (c->used && c->recv && !c->done && c->post <= q->post && (!old || c->post < old->post)) old = c;
+        }
+        if (!old || !try_recv(old)) break;
+        old->done = 1;
+    }
+    *f = q->done;
     if (*f) { q->used = 0; *r = MPI_REQUEST_NULL; }
     return 0;
 }
