@@ -399,12 +399,18 @@ typedef struct shock_block {
     int ni, nj, nk;            /* real points of the block (the .sddc corners) */
     int bc[6];                 /* face types of faces without a neighbour, SHOCK_BC_AUTO on the others */
     int neighbour[6];          /* block across each face (Left, Right, Bottom, Top, Behind, InFront), -1 for
-                                  none; the neighbour's opposite face touches this face with the identity
-                                  orientation (.sddc transform 1,2,3), and a block may be its own neighbour
-                                  (a periodic axis of one block) */
+                                  none; a block may be its own neighbour (a periodic axis of one block) */
     float translation[6][3];   /* the .sddc Translation of each face: added to the coordinates received
                                   across it (a periodic wrap: minus / plus the period) */
     const double *x, *y, *z, *u, *v, *w, *p, *rho;   /* real points, Fortran order (as shock_create) */
+    int transform[6][3];       /* the .sddc Transform of each face's interface (src/Load.c:191-250,
+                                  src/Functions.c:3902-4286): entry a is +-(1 + the neighbour's axis that
+                                  this block's axis a runs along), negative where it runs the other way; all
+                                  zero is the identity 1,2,3.  The neighbour's face that touches face f
+                                  (axis a, side s) is its axis |T[a]|-1 on side s when T[a] < 0, on the
+                                  other side when T[a] > 0; that face must name this block back with the
+                                  inverse transform.  Velocities are Cartesian and cross unchanged; the
+                                  metric rows are permuted and signed as SHOCK's transfer does. */
 } shock_block;
 
 typedef struct shock_multi shock_multi;

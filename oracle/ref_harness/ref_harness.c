@@ -546,6 +546,7 @@ typedef struct {
     const ref_params *blk;        /* per block (sizes, face types; periodic = 0) */
     const int *neigh;             /* [nblocks][6] neighbour across each face, -1: none */
     const float *trans;           /* [nblocks][6][3] Translation of each face */
+    const int *tfm;               /* [nblocks][6][3] Transform of each face's interface */
     const double *const *in;      /* [nblocks][8] x,y,z,u,v,w,p,rho (real points, Fortran order) */
     int nrhs;                     /* 1: also one right-hand side at the initial state */
     int nsteps;
@@ -578,6 +579,10 @@ static void mr_interfaces(void)
         const int a = f / 2, hi = f % 2;
         const ref_params *q = &g_job->blk[nb];
         const int me_n[3] = {p->ni, p->nj, p->nk}, nb_n[3] = {q->ni, q->nj, q->nk};
+        const int *T = g_job->tfm + (6 * b + f) * 3;
+        /* the neighbour's face that touches this one: its axis |T[a]|-1, on
+           the far side when the two normal axes run the same way */
+        const int da = abs(T[a]) - 1, dhi = hi ^ (T[a] > 0 ? 1 : 0);
         tf[ii] = mr_tf[ii];
         rng[ii] = mr_rng[ii];
         drng[ii] = mr_drng[ii];
@@ -585,14 +590,14 @@ static void mr_interfaces(void)
         rc[ii] = mr_rc[ii];
         ra[ii] = mr_ra[ii];
         for (int c = 0; c < dim; c++) {
-            tf[ii][c] = c + 1;
+            tf[ii][c] = T[c];
             rng[ii][c] = 1;
             rng[ii][dim + c] = me_n[c];
             drng[ii][c] = 1;
             drng[ii][dim + c] = nb_n[c];
         }
         rng[ii][a] = rng[ii][dim + a] = hi ? me_n[a] : 1;          /* my face */
-        drng[ii][a] = drng[ii][dim + a] = hi ? 1 : nb_n[a];        /* the neighbour's opposite face */
+        drng[ii][da] = drng[ii][dim + da] = dhi ? nb_n[da] : 1;    /* the neighbour's face */
         for (int c = 0; c < 3; c++) {
             tr[ii][c] = g_job->trans[(6 * b + f) * 3 + c];
             rc[ii][c] = 0.f;
@@ -642,12 +647,13 @@ static int mr_body(int rank, void *arg)
  * out_off[b], the geometry (13*NG), one right-hand side at the initial state
  * (5*NG, when nrhs) and the state after nsteps steps (9*NG: rho,u,v,w,e,p,
  * T,c,mue).  Returns 0 on success. */
-int refmpi_run(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const double *const *in,
-               int nrhs, int nsteps, double *out, const size_t *out_off, size_t out_len, size_t slot_bytes)
+int refmpi_run(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const int *tfm,
+               const double *const *in, int nrhs, int nsteps, double *out, const size_t *out_off, size_t out_len,
+               size_t slot_bytes)
 {
     double *shared = mmap(NULL, out_len * sizeof(double), PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
     if (shared == MAP_FAILED) return -1;
-    mr_job job = {nblocks, blk, neigh, trans, in, nrhs, nsteps, shared, out_off};
+    mr_job job = {nblocks, blk, neigh, trans, tfm, in, nrhs, nsteps, shared, out_off};
     int rc = shm_run(nblocks, slot_bytes, mr_body, &job);
     memcpy(out, shared, out_len * sizeof(double));
     munmap(shared, out_len * sizeof(double));

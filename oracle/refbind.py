@@ -312,8 +312,8 @@ class Oracle:
 # started with multiprocessing's "spawn" method, so no GPU context is ever
 # forked.
 # ---------------------------------------------------------------------------
-def multirank_available(order: int, dim: int, extended: bool = False) -> bool:
-    tag = "80" if extended else ""
+def multirank_available(order: int, dim: int, extended: bool = False, full: bool = False) -> bool:
+    tag = ("full" if full else "") + ("80" if extended else "")
     return os.path.exists(os.path.join(HERE, "_ref", f"libshockmpi{tag}_w{order}_{dim}d.so"))
 
 
@@ -338,9 +338,9 @@ def _ref_params(case) -> "RefParams":
     return p
 
 
-def _multirank_worker(division, nsteps, rhs, extended):
+def _multirank_worker(division, nsteps, rhs, extended, full=False):
     case = division.case
-    tag = "80" if extended else ""
+    tag = ("full" if full else "") + ("80" if extended else "")
     lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockmpi{tag}_w{case.order}_{case.dim}d.so"), mode=os.RTLD_LOCAL)
     lib.refmpi_run.restype = C.c_int
     nb = len(division.blocks)
@@ -357,11 +357,13 @@ def _multirank_worker(division, nsteps, rhs, extended):
     ptrs = (C.POINTER(C.c_double) * (8 * nb))(*[_ptr(a) for fl in keep for a in fl])
     neigh = np.ascontiguousarray(division.neighbour, dtype=np.int32)
     trans = np.ascontiguousarray(division.translation, dtype=np.float32)
+    tfm = np.ascontiguousarray(division.transform, dtype=np.int32)
     out = np.zeros(total)
     face = max(max(s[0] * s[1], s[1] * s[2], s[0] * s[2]) for s in shapes)
     slot = 13 * (g2 // 2) * face * 16       # long double in the 80-bit build
     rc = lib.refmpi_run(C.c_int(nb), params, neigh.ctypes.data_as(C.POINTER(C.c_int)),
-                        trans.ctypes.data_as(C.POINTER(C.c_float)), ptrs, C.c_int(int(rhs)), C.c_int(nsteps),
+                        trans.ctypes.data_as(C.POINTER(C.c_float)), tfm.ctypes.data_as(C.POINTER(C.c_int)), ptrs,
+                        C.c_int(int(rhs)), C.c_int(nsteps),
                         _ptr(out), off.ctypes.data_as(C.POINTER(C.c_size_t)), C.c_size_t(total), C.c_size_t(slot))
     if rc != 0:
         raise RuntimeError(f"multi-rank reference run failed ({rc})")
@@ -374,12 +376,12 @@ def _multirank_worker(division, nsteps, rhs, extended):
     return res
 
 
-def run_multirank(division, nsteps: int, rhs: bool = False, extended: bool = False):
+def run_multirank(division, nsteps: int, rhs: bool = False, extended: bool = False, full: bool = False):
     """Per block: geometry (13, ghosted), one right-hand side at the initial
     state (5, when rhs) and the state after nsteps steps (9: rho,u,v,w,e,p,
     T,c,mue) of SHOCK's own multi-rank run of the division (extended: the
-    80-bit build)."""
+    80-bit build; full: the build with the full 3D metric)."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
-        return pool.apply(_multirank_worker, (division, nsteps, rhs, extended))
+        return pool.apply(_multirank_worker, (division, nsteps, rhs, extended, full))

@@ -396,7 +396,8 @@ class Block(C.Structure):
     """Mirror of struct shock_block (include/shock_b200.h)."""
     _fields_ = [("ni", C.c_int), ("nj", C.c_int), ("nk", C.c_int), ("bc", C.c_int * 6),
                 ("neighbour", C.c_int * 6), ("translation", (C.c_float * 3) * 6)] + \
-               [(n, _dp) for n in ("x", "y", "z", "u", "v", "w", "p", "rho")]
+               [(n, _dp) for n in ("x", "y", "z", "u", "v", "w", "p", "rho")] + \
+               [("transform", (C.c_int * 3) * 6)]
 
 
 def _division_blocks(division):
@@ -414,6 +415,7 @@ def _division_blocks(division):
             B.neighbour[q] = int(division.neighbour[b, q])
             for c in range(3):
                 B.translation[q][c] = float(division.translation[b, q, c])
+                B.transform[q][c] = int(division.transform[b, q, c])
         fields = [f(a) for a in bc.real_fields()]
         keep.append(fields)
         for name, a in zip(("x", "y", "z", "u", "v", "w", "p", "rho"), fields):
@@ -421,7 +423,7 @@ def _division_blocks(division):
     return arr, keep
 
 
-def host_multi_geometry(division):
+def host_multi_geometry(division, full_metric=False):
     """Per block geometry (13, ghosted) of a division, built on the host with
     the interfaces exchanged as SHOCK's ranks exchange them (no device)."""
     case = division.case
@@ -429,7 +431,7 @@ def host_multi_geometry(division):
     g2 = case.order + 1
     outs = [np.zeros((13, b.ni + g2, b.nj + g2, (b.nk + g2) if case.dim == 3 else 1)) for b in division.blocks]
     ptrs = (_dp * len(outs))(*[_ptr(o) for o in outs])
-    p = params_from_case(case)
+    p = params_from_case(case, full_metric=full_metric)
     _check(lib().shock_host_multi_geometry(C.byref(p), len(outs), arr, ptrs))
     return outs
 
@@ -440,11 +442,11 @@ class Multi:
     ranks exchange them (shock_multi_*)."""
 
     def __init__(self, division, precision=SHOCK_FP64, device: int = 0, zeta_fix: bool = False,
-                 weno_eps: float = 0.0):
+                 weno_eps: float = 0.0, full_metric: bool = False):
         self.division = division
         self.lib = lib()
         case = division.case
-        self.params = params_from_case(case, precision, zeta_fix, weno_eps)
+        self.params = params_from_case(case, precision, zeta_fix, weno_eps, full_metric)
         nb = len(division.blocks)
         arr, self._keep = _division_blocks(division)
         h = C.c_void_p()
@@ -510,8 +512,8 @@ class Multi:
         for b, a in enumerate(per_block):
             bc, lo = self.division.blocks[b], self.division.lo[b]
             k0 = g if case.dim == 3 else 0
-            out[:, lo[0]:lo[0] + bc.ni, lo[1]:lo[1] + bc.nj, lo[2]:lo[2] + (bc.nk if case.dim == 3 else 1)] = \
-                a[:, g:g + bc.ni, g:g + bc.nj, k0:k0 + (bc.nk if case.dim == 3 else 1)]
+            r = self.division.from_block(b, a[:, g:g + bc.ni, g:g + bc.nj, k0:k0 + (bc.nk if case.dim == 3 else 1)])
+            out[:, lo[0]:lo[0] + r.shape[1], lo[1]:lo[1] + r.shape[2], lo[2]:lo[2] + r.shape[3]] = r
         return out
 
 

@@ -484,6 +484,106 @@ class Division:
     neighbour: np.ndarray           # (nblocks, 6) int
     translation: np.ndarray         # (nblocks, 6, 3) float32
     lo: np.ndarray                  # (nblocks, 3) first real index of each block in the whole block
+    transform: Optional[np.ndarray] = None   # (nblocks, 6, 3) int: the .sddc Transform per face (1,2,3)
+    axes: Optional[np.ndarray] = None        # (nblocks, 3) int: the whole block's axis each block axis runs along
+    flips: Optional[np.ndarray] = None       # (nblocks, 3) bool: ... and whether it runs the other way
+
+    def __post_init__(self):
+        nb = len(self.blocks)
+        if self.axes is None:
+            self.axes = np.tile(np.arange(3), (nb, 1))
+            self.flips = np.zeros((nb, 3), dtype=bool)
+        if self.transform is None:
+            self.transform = _transforms(self.neighbour, self.axes, self.flips, self.case.dim)
+
+    def to_block(self, b, a):
+        """Array a of the whole block's shape (..., ni, nj, nk) seen from
+        block b's index order (its slice, then its axes as it holds them)."""
+        bl = self.blocks[b]
+        n = (bl.ni, bl.nj, bl.nk if self.case.dim == 3 else 1)
+        sl = [slice(None)] * (a.ndim - 3)
+        whole = [None, None, None]
+        for c in range(3):
+            ax = self.axes[b, c]
+            whole[ax] = slice(int(self.lo[b, ax]), int(self.lo[b, ax]) + n[c])
+        s = a[tuple(sl + whole)]
+        lead = a.ndim - 3
+        s = np.transpose(s, list(range(lead)) + [lead + int(x) for x in self.axes[b]])
+        for c in range(3):
+            if self.flips[b, c]:
+                s = np.flip(s, axis=lead + c)
+        return s
+
+    def from_block(self, b, a):
+        """Block b's real-point array (..., its own index order) in the whole
+        block's axis order (the inverse of to_block's reordering)."""
+        lead = a.ndim - 3
+        for c in range(3):
+            if self.flips[b, c]:
+                a = np.flip(a, axis=lead + c)
+        inv = [int(np.nonzero(self.axes[b] == w)[0][0]) for w in range(3)]
+        return np.transpose(a, list(range(lead)) + [lead + c for c in inv])
+
+
+def _transforms(neigh, axes, flips, dim):
+    """The .sddc Transform of every interface from the blocks' orientations:
+    entry c of face f of block b is +-(1 + the axis of the neighbour that b's
+    axis c runs along), negative where the two run opposite ways."""
+    nb = neigh.shape[0]
+    t = np.zeros((nb, 6, 3), dtype=np.int32)
+    for b in range(nb):
+        for f in range(2 * dim):
+            n = neigh[b, f]
+            if n < 0:
+                continue
+            for c in range(3):
+                d = int(np.nonzero(axes[n] == axes[b, c])[0][0])
+                s = -1 if flips[b, c] != flips[n, d] else 1
+                t[b, f, c] = s * (d + 1)
+    return t
+
+
+def rotate_block(division: "Division", b: int, axes: Tuple[int, int, int], flips: Tuple[bool, bool, bool]):
+    """The same division with block b holding its points in another index
+    order: its new axis c runs along its old axis axes[c], reversed where
+    flips[c] (a zone meshed in another orientation, as a .sddc file with
+    non-identity Transforms describes one).  Faces, neighbours, face types,
+    translations and every interface's Transform follow."""
+    import copy
+    d = copy.copy(division)
+    dim = d.case.dim
+    axes = tuple(int(a) for a in axes)
+    flips = tuple(bool(x) for x in flips)
+    old = d.blocks[b]
+    nold = (old.ni, old.nj, old.nk if dim == 3 else 1)
+
+    def re(a):
+        s = np.transpose(np.asarray(a), axes)
+        for c in range(3):
+            if flips[c]:
+                s = np.flip(s, axis=c)
+        return np.ascontiguousarray(s)
+
+    neigh = d.neighbour.copy()
+    trans = d.translation.copy()
+    bc = list(old.bc)
+    for c in range(3):
+        for side in (0, 1):
+            of = 2 * axes[c] + (side ^ int(flips[c]))
+            neigh[b, 2 * c + side] = division.neighbour[b, of]
+            trans[b, 2 * c + side] = division.translation[b, of]
+            bc[2 * c + side] = old.bc[of]
+    new = old.replace(ni=nold[axes[0]], nj=nold[axes[1]], nk=nold[axes[2]] if dim == 3 else 1,
+                      x=re(old.x), y=re(old.y), z=re(old.z), rho=re(old.rho), u=re(old.u), v=re(old.v),
+                      w=re(old.w), p=re(old.p), bc=tuple(bc))
+    blocks = list(d.blocks)
+    blocks[b] = new
+    ax = d.axes.copy()
+    fl = d.flips.copy()
+    ax[b] = [division.axes[b, axes[c]] for c in range(3)]
+    fl[b] = [bool(division.flips[b, axes[c]]) ^ flips[c] for c in range(3)]
+    return Division(case=d.case, parts=d.parts, blocks=blocks, neighbour=neigh, translation=trans, lo=d.lo,
+                    axes=ax, flips=fl)
 
 
 def split(case: Case, parts: Tuple[int, ...]) -> Division:

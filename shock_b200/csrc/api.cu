@@ -180,8 +180,10 @@ static void mark(shock_ctx *c, const char *name)
     c->tmark++;
 }
 
-// Launch the right-hand side of one stage on state `in`.
-static void enqueue_rhs(shock_ctx *c, double *const in[5], int &nk)
+// Launch the right-hand side of one stage on state `in`.  rk (may be null):
+// the stage's RK update, done by the last sweep where the form allows it;
+// returns true when it was.
+static bool enqueue_rhs(shock_ctx *c, double *const in[5], int &nk, const RKFuse *rk = nullptr)
 {
     cudaStream_t s = c->stream;
     const double *cin[5] = {in[0], in[1], in[2], in[3], in[4]};
@@ -204,17 +206,50 @@ static void enqueue_rhs(shock_ctx *c, double *const in[5], int &nk)
         nk++;
         mark(c, "nodal");
     }
+    if (!c->p.inviscid && fused_sweeps(c->G, c->P, c->p.precision)) {
+        static const char *fn[3] = {"weno_visc_xi", "weno_visc_eta", "weno_visc_zeta"};
+        static const char *fr[3] = {"weno_visc_rk_xi", "weno_visc_rk_eta", "weno_visc_rk_zeta"};
+        bool done = false;
+        for (int d = 0; d < c->p.dim; d++) {
+            const bool last = d == c->p.dim - 1;
+            done = launch_weno_visc(c->G, c->P, c->p.precision, d, d == 0, cin, c->F, s, last ? rk : nullptr);
+            nk++;
+            mark(c, done ? fr[d] : fn[d]);
+        }
+        return done;
+    }
     for (int d = 0; d < c->p.dim; d++) {
         launch_weno(c->G, c->P, c->p.precision, d, d == 0, cin, c->F, s);
         nk++;
         mark(c, wn[d]);
     }
-    if (!c->p.inviscid)
-        for (int d = 0; d < c->p.dim; d++) {
-            launch_viscous(c->G, c->P, c->p.precision, d, cin, c->F, s);
-            nk++;
-            mark(c, vn[d]);
-        }
+    if (c->p.inviscid) return false;
+    // the separate viscous sweeps: the last one ends the stage where its
+    // form has an RK part (not the full metric's viscous sweep)
+    static const char *vr[3] = {"visc_rk_xi", "visc_rk_eta", "visc_rk_zeta"};
+    bool done = false;
+    for (int d = 0; d < c->p.dim; d++) {
+        const bool last = d == c->p.dim - 1;
+        done = launch_viscous(c->G, c->P, c->p.precision, d, cin, c->F, s, last ? rk : nullptr);
+        nk++;
+        mark(c, done ? vr[d] : vn[d]);
+    }
+    return done;
+}
+
+// The RK update of stage st from state `in` to `out` (U_lastStep `un`).
+static RKFuse rk_fuse(shock_ctx *c, int st, int in, int out, int un)
+{
+    RKFuse r{};
+    r.K = c->rk[st];
+    r.tau = c->p.tau;
+    for (int q = 0; q < 5; q++) {
+        r.in.U[q] = c->buf[in][q];
+        r.Un[q] = c->buf[un][q];
+        r.out[q] = c->buf[out][q];
+    }
+    r.has_source = c->has_source ? 1 : 0;
+    return r;
 }
 
 static void enqueue_step(shock_ctx *c, int un, int &nk)
@@ -223,13 +258,15 @@ static void enqueue_step(shock_ctx *c, int un, int &nk)
     for (int st = 0; st < c->p.time_order; st++) {
         int out = 0;
         while (out == un || out == cur) out++;
-        enqueue_rhs(c, c->buf[cur], nk);
-        const double *cin[5] = {c->buf[cur][0], c->buf[cur][1], c->buf[cur][2], c->buf[cur][3], c->buf[cur][4]};
-        Fields F = c->F;
-        for (int q = 0; q < 5; q++) F.Un[q] = c->buf[un][q];
-        launch_rk(c->G, c->rk[st], c->p.tau, cin, c->buf[out], F, c->has_source, c->stream);
-        nk++;
-        mark(c, "rk");
+        const RKFuse rf = rk_fuse(c, st, cur, out, un);
+        if (!enqueue_rhs(c, c->buf[cur], nk, &rf)) {
+            const double *cin[5] = {c->buf[cur][0], c->buf[cur][1], c->buf[cur][2], c->buf[cur][3], c->buf[cur][4]};
+            Fields F = c->F;
+            for (int q = 0; q < 5; q++) F.Un[q] = c->buf[un][q];
+            launch_rk(c->G, c->rk[st], c->p.tau, cin, c->buf[out], F, c->has_source, c->stream);
+            nk++;
+            mark(c, "rk");
+        }
         cur = out;
     }
     // end of the step: U_RK's p becomes U_lastStep's (src/SHOCK.c:661-664)
@@ -989,8 +1026,14 @@ static void multi_enqueue_step(shock_multi *m, int un, int &nk)
         int out = 0;
         while (out == un || out == cur) out++;
         multi_exchange(m, cur, nk);
-        for (shock_ctx *c : m->blk) enqueue_rhs(c, c->buf[cur], nk);
+        std::vector<char> rk_done;
         for (shock_ctx *c : m->blk) {
+            const RKFuse rf = rk_fuse(c, st, cur, out, un);
+            rk_done.push_back(enqueue_rhs(c, c->buf[cur], nk, &rf) ? 1 : 0);
+        }
+        for (size_t b = 0; b < m->blk.size(); b++) {
+            if (rk_done[b]) continue;
+            shock_ctx *c = m->blk[b];
             const double *cin[5] = {c->buf[cur][0], c->buf[cur][1], c->buf[cur][2], c->buf[cur][3], c->buf[cur][4]};
             Fields F = c->F;
             for (int q = 0; q < 5; q++) F.Un[q] = c->buf[un][q];
@@ -1058,7 +1101,10 @@ int shock_multi_create(const shock_params *p, int nblocks, const shock_block *bl
             const int nb = f < 2 * dim ? B.neighbour[f] : -1;
             if (nb < -1 || nb >= nblocks) return fail(SHOCK_EINVAL, "block %d face %d: no block %d", b, f, nb);
             links[b].neighbour[f] = nb;
-            for (int c = 0; c < 3; c++) links[b].translation[f][c] = B.translation[f][c];
+            for (int c = 0; c < 3; c++) {
+                links[b].translation[f][c] = B.translation[f][c];
+                links[b].tf[f][c] = B.transform[f][c];
+            }
             q.bc[f] = f < 2 * dim ? B.bc[f] : SHOCK_BC_AUTO;
             if (nb >= 0) iface |= 1u << f;
         }
@@ -1066,21 +1112,9 @@ int shock_multi_create(const shock_params *p, int nblocks, const shock_block *bl
         const double *f8[8] = {B.x, B.y, dim == 3 ? B.z : B.x, B.u, B.v, B.w, B.p, B.rho};
         for (int k = 0; k < 8; k++) in[8 * (size_t)b + k] = f8[k];
     }
-    // the faces that touch: the neighbour's opposite face names this block,
-    // and their lateral extents agree (identity orientation)
-    for (int b = 0; b < nblocks; b++)
-        for (int f = 0; f < 2 * dim; f++) {
-            const int nb = links[b].neighbour[f];
-            if (nb < 0) continue;
-            if (links[nb].neighbour[f ^ 1] != b)
-                return fail(SHOCK_EINVAL, "block %d face %d: block %d's opposite face does not name it back", b, f, nb);
-            const int n0[3] = {ps[b].ni, ps[b].nj, ps[b].nk}, n1[3] = {ps[nb].ni, ps[nb].nj, ps[nb].nk};
-            for (int a = 0; a < dim; a++)
-                if (a != f / 2 && n0[a] != n1[a])
-                    return fail(SHOCK_EINVAL, "block %d face %d: %d points along axis %d, block %d has %d", b, f, n0[a],
-                                a, nb, n1[a]);
-            if (n1[f / 2] < g) return fail(SHOCK_EINVAL, "block %d: fewer real layers than ghost layers", nb);
-        }
+    // the faces that touch name each other with inverse transforms, and
+    // their extents agree
+    if (int rc = check_links(dim, g, ps, links)) return rc;
     std::vector<HostBlock> hbs;
     build_blocks(ps, in, links, hbs);
 
@@ -1110,19 +1144,28 @@ int shock_multi_create(const shock_params *p, int nblocks, const shock_block *bl
             const int nb = links[b].neighbour[f];
             if (nb < 0) continue;
             const Layout &R = m->blk[b]->L, &S = m->blk[nb]->L;
+            const FaceMap fm = face_map(links[b], f);
             int rlo[3], rhi[3], slo[3], shi[3];
             face_region(R, f, false, rlo, rhi);
-            face_region(S, f ^ 1, true, slo, shi);
+            face_region(S, fm.fd, true, slo, shi);
             XFace x{};
             long long n = 1;
             for (int a = 0; a < 3; a++) {
                 x.ext[a] = rhi[a] - rlo[a] + 1;
+                x.sext[a] = shi[a] - slo[a] + 1;
+                x.map[a] = fm.axis[a];
+                x.flip[a] = fm.flip[a];
                 x.rlo[a] = rlo[a];
                 x.slo[a] = slo[a];
                 x.rst[a] = R.st[a];
                 x.sst[a] = S.st[a];
                 n *= x.ext[a];
             }
+            for (int a = 0; a < 3; a++)   // every receiver point reads inside the sender's region
+                if (x.ext[a] != x.sext[x.map[a]]) {
+                    shock_multi_destroy(m);
+                    return fail(SHOCK_EINVAL, "block %d face %d: receive and send regions differ along axis %d", b, f, a);
+                }
             x.off = m->total;
             m->total += n;
             if (n > m->most) m->most = n;
@@ -1170,7 +1213,10 @@ int shock_host_multi_geometry(const shock_params *p, int nblocks, const shock_bl
             const int nb = f < 2 * p->dim ? B.neighbour[f] : -1;
             if (nb < -1 || nb >= nblocks) return fail(SHOCK_EINVAL, "block %d face %d: no block %d", b, f, nb);
             links[b].neighbour[f] = nb;
-            for (int c = 0; c < 3; c++) links[b].translation[f][c] = B.translation[f][c];
+            for (int c = 0; c < 3; c++) {
+                links[b].translation[f][c] = B.translation[f][c];
+                links[b].tf[f][c] = B.transform[f][c];
+            }
             q.bc[f] = f < 2 * p->dim ? B.bc[f] : SHOCK_BC_AUTO;
         }
         const size_t nr = (size_t)q.ni * q.nj * q.nk;
@@ -1187,6 +1233,7 @@ int shock_host_multi_geometry(const shock_params *p, int nblocks, const shock_bl
         in[8 * (size_t)b + 6] = ones[b].data();
         in[8 * (size_t)b + 7] = ones[b].data();
     }
+    if (int rc = check_links(p->dim, (p->order + 1) / 2, ps, links)) return rc;
     std::vector<HostBlock> hbs;
     build_blocks(ps, in, links, hbs);
     for (int b = 0; b < nblocks; b++)

@@ -11,6 +11,8 @@
 // This file is compiled without FMA contraction (see the Makefile).
 #include "internal.h"
 
+#include <array>
+#include <cstdlib>
 #include <cstring>
 
 namespace shock {
@@ -296,46 +298,130 @@ void face_region(const Layout &L, int f, bool send, int lo[3], int hi[3])
     }
 }
 
+FaceMap face_map(const BlockLink &l, int f)
+{
+    FaceMap m;
+    const int *T = l.tf[f];
+    for (int c = 0; c < 3; c++) {
+        m.axis[c] = std::abs(T[c]) - 1;
+        m.flip[c] = T[c] < 0;
+    }
+    // the face of the neighbour that touches: on the far side of its axis
+    // when the normal axes run the same way, on the same side otherwise
+    // (the sign check_TransformationMatrix derives from the two ranges)
+    const int a = f / 2, hi = f % 2;
+    m.fd = 2 * m.axis[a] + (hi ^ (T[a] > 0 ? 1 : 0));
+    return m;
+}
+
+int check_links(int dim, int g, const std::vector<shock_params> &ps, std::vector<BlockLink> &links)
+{
+    const int nb = (int)links.size();
+    for (int b = 0; b < nb; b++)
+        for (int f = 0; f < 2 * dim; f++) {
+            if (links[b].neighbour[f] < 0) continue;
+            int *T = links[b].tf[f];
+            if (!T[0] && !T[1] && !T[2])
+                for (int c = 0; c < 3; c++) T[c] = c + 1;
+            if (dim == 2) {
+                if (T[2] != 0 && T[2] != 3)
+                    return report_error(SHOCK_EINVAL, "block %d face %d: 2D transform with third entry %d", b, f, T[2]);
+                T[2] = 3;
+            }
+            int seen = 0;
+            for (int c = 0; c < dim; c++) {
+                const int ax = std::abs(T[c]);
+                if (ax < 1 || ax > dim || (seen >> ax & 1))
+                    return report_error(SHOCK_EINVAL, "block %d face %d: transform (%d,%d,%d) is not a signed permutation",
+                                        b, f, T[0], T[1], T[2]);
+                seen |= 1 << ax;
+            }
+        }
+    for (int b = 0; b < nb; b++)
+        for (int f = 0; f < 2 * dim; f++) {
+            const int n = links[b].neighbour[f];
+            if (n < 0) continue;
+            const FaceMap m = face_map(links[b], f);
+            if (links[n].neighbour[m.fd] != b)
+                return report_error(SHOCK_EINVAL, "block %d face %d: face %d of block %d, which touches it, does not name it back",
+                                    b, f, m.fd, n);
+            const FaceMap r = face_map(links[n], m.fd);
+            for (int c = 0; c < dim; c++)
+                if (r.axis[m.axis[c]] != c || r.flip[m.axis[c]] != m.flip[c])
+                    return report_error(SHOCK_EINVAL, "block %d face %d: block %d's transform back is not the inverse", b, f, n);
+            const int n0[3] = {ps[b].ni, ps[b].nj, ps[b].nk}, n1[3] = {ps[n].ni, ps[n].nj, ps[n].nk};
+            for (int c = 0; c < dim; c++)
+                if (c != f / 2 && n0[c] != n1[m.axis[c]])
+                    return report_error(SHOCK_EINVAL, "block %d face %d: %d points along axis %d, block %d has %d along axis %d",
+                                        b, f, n0[c], c, n, n1[m.axis[c]], m.axis[c]);
+            if (n1[m.axis[f / 2]] < g) return report_error(SHOCK_EINVAL, "block %d: fewer real layers than ghost layers", n);
+        }
+    return SHOCK_OK;
+}
+
 // One TransferMeshParameter over every interface of the division
 // (src/Functions.c:3481-3578): all blocks pack their send regions (x, y, z,
-// the nine metric terms, J), then every receiving face unpacks its
-// neighbour's into its ghost layers, adding the face's float32 Translation
-// to the coordinates (src/Functions.c:2628-2694; identity orientation, so
-// the metric factors are 1).
+// J and the nine metric terms) in their own index order, then every
+// receiving face unpacks its neighbour's into its ghost layers through the
+// interface's transform (get_ijkTransformMesh, src/Functions.c:4315-4410):
+// its axes mapped onto the neighbour's and reversed where the transform is
+// negative, each metric row taken from the neighbour's row of the axis it
+// runs along with the transform's sign, and the face's float32 Translation
+// added to the coordinates (src/Functions.c:2628-2694).
 void transfer_mesh(std::vector<HostBlock> &hbs, const std::vector<BlockLink> &links)
 {
-    static const int order13[13] = {0, 1, 2, 4, 5, 6, 7, 8, 9, 10, 11, 12, 3};   // SHOCK's buffer order
     std::vector<std::vector<double>> buf(hbs.size() * 6);
+    std::vector<FaceMap> maps(hbs.size() * 6);
+    std::vector<std::array<int, 3>> sext(hbs.size() * 6);
     for (size_t b = 0; b < hbs.size(); b++)
         for (int f = 0; f < 2 * hbs[b].L.dim; f++) {
             const int nb = links[b].neighbour[f];
             if (nb < 0) continue;
-            // the neighbour's opposite face sends to this face
+            const FaceMap m = face_map(links[b], f);
+            maps[b * 6 + f] = m;
             const Layout &S = hbs[nb].L;
             int lo[3], hi[3];
-            face_region(S, f ^ 1, true, lo, hi);
+            face_region(S, m.fd, true, lo, hi);
+            for (int c = 0; c < 3; c++) sext[b * 6 + f][c] = hi[c] - lo[c] + 1;
             std::vector<double> &q = buf[b * 6 + f];
             for (int fld = 0; fld < 13; fld++)
                 for (int i = lo[0]; i <= hi[0]; i++)
                     for (int j = lo[1]; j <= hi[1]; j++)
-                        for (int k = lo[2]; k <= hi[2]; k++) q.push_back(hbs[nb].geo[order13[fld]][S.at(i, j, k)]);
+                        for (int k = lo[2]; k <= hi[2]; k++) q.push_back(hbs[nb].geo[fld][S.at(i, j, k)]);
         }
     for (size_t b = 0; b < hbs.size(); b++)
         for (int f = 0; f < 2 * hbs[b].L.dim; f++) {
             if (links[b].neighbour[f] < 0) continue;
+            const FaceMap &m = maps[b * 6 + f];
+            const std::array<int, 3> &e = sext[b * 6 + f];
             const Layout &R = hbs[b].L;
             int lo[3], hi[3];
             face_region(R, f, false, lo, hi);
             const std::vector<double> &q = buf[b * 6 + f];
-            size_t n = 0;
-            for (int fld = 0; fld < 13; fld++)
-                for (int i = lo[0]; i <= hi[0]; i++)
-                    for (int j = lo[1]; j <= hi[1]; j++)
-                        for (int k = lo[2]; k <= hi[2]; k++) {
-                            double v = q[n++];
+            const size_t cnt = (size_t)e[0] * e[1] * e[2];
+            // field fld of this block from the neighbour's field src[fld], times sgn[fld]
+            int src[13];
+            double sgn[13];
+            for (int fld = 0; fld < 4; fld++) { src[fld] = fld; sgn[fld] = 1.0; }
+            for (int row = 0; row < 3; row++)
+                for (int x = 0; x < 3; x++) {
+                    src[4 + 3 * row + x] = 4 + 3 * m.axis[row] + x;
+                    sgn[4 + 3 * row + x] = m.flip[row] ? -1.0 : 1.0;
+                }
+            for (int i = lo[0]; i <= hi[0]; i++)
+                for (int j = lo[1]; j <= hi[1]; j++)
+                    for (int k = lo[2]; k <= hi[2]; k++) {
+                        const int r[3] = {i - lo[0], j - lo[1], k - lo[2]};
+                        int d[3];
+                        for (int c = 0; c < 3; c++) d[m.axis[c]] = m.flip[c] ? e[m.axis[c]] - 1 - r[c] : r[c];
+                        const size_t t = ((size_t)d[0] * e[1] + d[1]) * e[2] + d[2];
+                        for (int fld = 0; fld < 13; fld++) {
+                            double v = q[(size_t)src[fld] * cnt + t];
                             if (fld < 3) v = v + links[b].translation[f][fld];
-                            hbs[b].geo[order13[fld]][R.at(i, j, k)] = v;
+                            else if (fld >= 4) v = sgn[fld] * v;
+                            hbs[b].geo[fld][R.at(i, j, k)] = v;
                         }
+                    }
         }
 }
 

@@ -39,7 +39,20 @@ int build_block(const shock_params &p, const double *x, const double *y, const d
 struct BlockLink {
     int neighbour[6];
     float translation[6][3];
+    int tf[6][3];   // the .sddc Transform of each face's interface (all zero: the identity)
 };
+// How face f of a block meets its neighbour (src/Functions.c:3902-4286,
+// :4287-4410): the neighbour's face fd that touches it, and for each axis c
+// of the block the neighbour's axis it runs along (axis[c]) and whether it
+// runs the other way (flip[c]).
+struct FaceMap {
+    int fd, axis[3], flip[3];
+};
+FaceMap face_map(const BlockLink &l, int f);
+// Normalise the transforms of a division's interfaces and check that each
+// is named from both sides with inverse transforms and matching extents;
+// SHOCK_OK, or SHOCK_EINVAL with the error text set.
+int check_links(int dim, int g, const std::vector<shock_params> &ps, std::vector<BlockLink> &links);
 // Set-up of all blocks of a division with their interfaces exchanged as
 // SHOCK's ranks exchange them; in: 8 pointers per block (x,y,z,u,v,w,p,rho).
 int build_blocks(const std::vector<shock_params> &ps, const std::vector<const double *> &in,
@@ -100,6 +113,17 @@ struct Fields {
 
 struct RKCoef {
     double a, b, c, d, s;
+};
+
+// The RK update of a stage done in the cell update of its last sweep, where
+// each cell's Q is complete: Q is then neither stored nor read back.
+struct RKFuse {
+    RKCoef K;
+    double tau;
+    StageIn in;          // the stage's input state
+    const double *Un[5]; // U_lastStep
+    double *out[5];      // the stage's output state
+    int has_source;
 };
 
 // ---------------------------------------------------------------------------
@@ -206,8 +230,14 @@ void launch_nodal(const Grid &G, const Phys &P, int precision, const double *con
                   cudaStream_t s);
 void launch_weno(const Grid &G, const Phys &P, int precision, int d, bool first,
                  const double *const U[5], const Fields &F, cudaStream_t s);
-void launch_viscous(const Grid &G, const Phys &P, int precision, int d, const double *const U[5],
-                    const Fields &F, cudaStream_t s);
+// rk (may be null): the last direction's sweep also does the stage's RK update.
+// true when this launch also did the stage's RK update.
+bool launch_viscous(const Grid &G, const Phys &P, int precision, int d, const double *const U[5],
+                    const Fields &F, cudaStream_t s, const RKFuse *rk = nullptr);
+// The fused WENO + viscous sweeps (one launch per direction) serve this form.
+bool fused_sweeps(const Grid &G, const Phys &P, int precision);
+bool launch_weno_visc(const Grid &G, const Phys &P, int precision, int d, bool first, const double *const U[5],
+                      const Fields &F, cudaStream_t s, const RKFuse *rk = nullptr);
 void launch_rk(const Grid &G, const RKCoef &rk, double tau, const double *const Uin[5],
                double *const Uout[5], const Fields &F, bool has_source, cudaStream_t s);
 void launch_copy_state(const Grid &G, const double *const src[5], double *const dst[5], cudaStream_t s);
@@ -229,7 +259,9 @@ struct XFace {
     const double *src[5];   // sender's rho,u,v,w,e (the buffer in use)
     double *dst[5];         // receiver's
     long long sst[3], rst[3];
-    int slo[3], rlo[3], ext[3];
+    int slo[3], rlo[3];
+    int ext[3], sext[3];    // receive / send region extents
+    int map[3], flip[3];    // receiver axis c runs along sender axis map[c], reversed if flip[c]
     long long off;          // first point of the face in the staging buffer
 };
 // One pass of SHOCK's TransferFlowParameterWithGhosts over a division: every

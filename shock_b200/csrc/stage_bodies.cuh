@@ -1294,7 +1294,10 @@ __device__ __forceinline__ double central(const double *sh, int NP, int q, int t
 // ---------------------------------------------------------------------------
 // WENO5 fits 128 registers (two tiles per SM); the WENO9 face needs more,
 // so it runs one tile per SM without spilling.
-template <int DIM, int ORDER, int D, bool MIXED, int TLN = TL, bool FULL = false>
+// KEEP_FH: the first part of the fused WENO + viscous sweep; the face fluxes
+// are left at the start of shared memory for visc_body<..., FUSED> instead
+// of being differenced into Q.
+template <int DIM, int ORDER, int D, bool MIXED, int TLN = TL, bool FULL = false, bool KEEP_FH = false>
 __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool first, const double *__restrict__ R,
                                           const double *__restrict__ Uu, const double *__restrict__ Vv,
                                           const double *__restrict__ Ww, const double *__restrict__ Ee,
@@ -1429,6 +1432,14 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
     }
     __syncthreads();
     }
+    if (KEEP_FH) {
+        if (MIXED) {   // the mixed form's face fluxes sit over the conserved-variable rows
+            static_assert(!MIXED || 5 * NFT <= (WU0 + 1) * NP, "face-flux copy regions are disjoint");
+            for (int e = row * NLANE + lane; e < 5 * NFT * NLS; e += NTHR) smem[e] = fh[e];
+            __syncthreads();
+        }
+        return;
+    }
     // flux difference into Q; along a contiguous axis the threads walk the
     // cells of one line (coalesced), otherwise one line per lane
     for (int it = row * NLANE + lane; it < TLN * NLANE; it += NTHR) {
@@ -1443,6 +1454,53 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
 #pragma unroll
         for (int q = 0; q < 5; q++)
             F.Q[q][o] = prev[q] - (fh[(q * NFT + cr + 1) * NLS + ln] - fh[(q * NFT + cr) * NLS + ln]);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// RK stage update of the real points (src/Functions.c:2300-2365), with the
+// time-independent source J*S added to Q first.
+// ---------------------------------------------------------------------------
+// Inputs of the RK update of one point, loaded ahead of the arithmetic so
+// that a thread can have several points' loads in flight.
+struct RKIn {
+    double Q[5], Qs[5], U[5], Un[5], J;
+};
+
+template <int DIM>
+__device__ __forceinline__ void rk_load(const StageIn &in, const Fields &F, int has_source, long long o, bool zero_qs,
+                                        RKIn &x)
+{
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+        x.Q[c] = F.Q[c][o];
+        if (has_source) x.Q[c] += F.js[c][o];
+        x.Qs[c] = zero_qs ? 0.0 : F.Qs[c][o];
+        x.U[c] = (DIM == 2 && c == 3) ? 0.0 : in.U[c][o];
+        x.Un[c] = (DIM == 2 && c == 3) ? 0.0 : F.Un[c][o];
+    }
+    x.J = F.J[o];
+}
+
+// The same arithmetic as rk_at on loaded inputs.
+template <int DIM>
+__device__ __forceinline__ void rk_finish(const RKCoef &K, double tau, const Fields &F, double *const outs[5],
+                                          long long o, const RKIn &x)
+{
+    double Qs[5];
+#pragma unroll
+    for (int c = 0; c < 5; c++) {
+        Qs[c] = x.Qs[c] + K.s * x.Q[c];
+        F.Qs[c][o] = Qs[c];
+    }
+    const double ro = x.U[0];
+    const double tj = tau / x.J;
+    const double rn = K.a * x.Un[0] + K.b * ro + tj * (K.c * x.Q[0] + K.d * Qs[0]);
+    outs[0][o] = rn;
+#pragma unroll
+    for (int c = 1; c < 5; c++) {
+        if (DIM == 2 && c == 3) { outs[3][o] = 0.0; continue; }
+        outs[c][o] = (K.a * x.Un[c] * x.Un[0] + K.b * x.U[c] * ro + tj * (K.c * x.Q[c] + K.d * Qs[c])) / rn;
     }
 }
 
@@ -1490,10 +1548,19 @@ struct ViscCellIn {
 enum { V3U = 0, V3V, V3W, V3T, V3X0, V3X1, V3X2, V3X3, V3F1, V3FA, V3FB, V3NV };
 enum { V2U = 0, V2V, V2T, V2XU, V2XV, V2XT, V2MJ, V2AX, V2AY, V2BX, V2BY, V2NV };
 
-template <int DIM, int ORDER, int D, bool MIXED, int TLN = TL>
+// FUSED: the second part of the fused WENO + viscous sweep.  The WENO face
+// fluxes of the same tile are at the start of shared memory (left there by
+// weno_body<..., KEEP_FH>); the cell update forms Q = Q_prev - (flux
+// difference) + the viscous terms in one pass (first: Q_prev = 0), the same
+// operations in the same order as the two separate sweeps.
+// RKF (the last direction's sweep): the cell update goes on to the stage's
+// RK update with the complete Q (rk_finish, as k_rk_rows does it); Q itself
+// is not stored.
+template <int DIM, int ORDER, int D, bool MIXED, int TLN = TL, bool FUSED = false, bool RKF = false>
 __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const double *__restrict__ Uu,
                                           const double *__restrict__ Vv, const double *__restrict__ Ww,
-                                          const Fields &F, int bx, int by, int bz)
+                                          const Fields &F, int bx, int by, int bz, bool first = false,
+                                          const RKFuse rkf = RKFuse{})
 {
     using A = Axes<DIM, D>;
     using TS = typename std::conditional<MIXED, float, double>::type;   // stencil arithmetic
@@ -1505,15 +1572,16 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
     const bool quirk = (DIM == 3 && D == 2 && !P.zeta_fix);
 
     extern __shared__ double smem[];
-    double *sh = smem;                       // [NV][NP][NLANE]
     constexpr int NFT = TLN + 1;             // faces per line
     constexpr int FPT = NFT / NROWT;         // faces per thread
     static_assert(NFT % NROWT == 0 && (FPT == 1 || FPT == 2), "tile length");
-    double *fo = smem + NV * NP * NLS;       // [4][NFT][NLS]
+    const double *wf = smem;                 // FUSED: [5][NFT][NLS] WENO face fluxes
+    double *sh = FUSED ? smem + 5 * NFT * NLS : smem;   // [NV][NP][NLANE]
+    double *fo = sh + NV * NP * NLS;         // [4][NFT][NLS]
     double *qd = fo + 4 * NFT * NLS;         // quirk: [16][NLANE] per-line half-point values
     double *cq = qd + 16 * NLANE;            // [ViscCellIn::N][TLN * NLANE] prefetched cell inputs
     constexpr int CQS = TLN * NLANE;
-    constexpr bool PF = ViscCellIn<DIM, ORDER, TLN>::prefetch;
+    constexpr bool PF = ViscCellIn<DIM, ORDER, TLN>::prefetch && !FUSED;
 #define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
 #define FO(c, f, l) fo[((c) * NFT + (f)) * NLS + (l)]
 #define QD(c, l) qd[(c) * NLANE + (l)]
@@ -1854,9 +1922,51 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
             nodeB = SH(V2MJ, ts, ln) * (N[0][D] * hsum[0] + N[1][D] * hsum[1]);
         }
         const double psi = P.psi;
-        const double q1 = PF ? cq[0 * CQS + it] : F.Q[1][o], q2 = PF ? cq[1 * CQS + it] : F.Q[2][o];
-        const double q3 = DIM == 3 ? (PF ? cq[2 * CQS + it] : F.Q[3][o]) : 0.0;
-        const double q4 = PF ? cq[(DIM == 3 ? 3 : 2) * CQS + it] : F.Q[4][o];
+        double q0 = 0.0, q1, q2, q3, q4, q3w = 0.0;   // q3w: the 2D w component (no viscous term)
+        if (FUSED) {
+            // the WENO part of this direction: Q_prev - (flux difference)
+            double wq[5];
+#pragma unroll
+            for (int q = 0; q < 5; q++) wq[q] = first ? 0.0 : F.Q[q][o];
+#pragma unroll
+            for (int q = 0; q < 5; q++) wq[q] = wq[q] - (wf[(q * NFT + cr + 1) * NLS + ln] - wf[(q * NFT + cr) * NLS + ln]);
+            if (!RKF) {
+                F.Q[0][o] = wq[0];
+                if (DIM == 2) F.Q[3][o] = wq[3];
+            }
+            q0 = wq[0]; q1 = wq[1]; q2 = wq[2]; q3 = DIM == 3 ? wq[3] : 0.0; q3w = wq[3]; q4 = wq[4];
+        } else {
+            q1 = PF ? cq[0 * CQS + it] : F.Q[1][o];
+            q2 = PF ? cq[1 * CQS + it] : F.Q[2][o];
+            q3 = DIM == 3 ? (PF ? cq[2 * CQS + it] : F.Q[3][o]) : 0.0;
+            q4 = PF ? cq[(DIM == 3 ? 3 : 2) * CQS + it] : F.Q[4][o];
+            if (RKF) {
+                q0 = F.Q[0][o];
+                if (DIM == 2) q3w = F.Q[3][o];
+            }
+        }
+        if (RKF) {
+            // the complete Q of the cell, each component as it would be
+            // stored, then the RK update of the point
+            const double gup = (P.walls && P.iso_hi[D] && T.c0 + cr == G.g + T.nD - 1) ? P.gam_w : P.gam;
+            double Aterm = vel[0] * (gp[0] - gmn[0]) + vel[1] * (gp[1] - gmn[1]);
+            if (DIM == 3) Aterm += vel[2] * (gp[2] - gmn[2]);
+            const double qf[5] = {q0, q1 + psi * (gp[0] - gmn[0]), q2 + psi * (gp[1] - gmn[1]),
+                                  DIM == 3 ? q3 + psi * (gp[2] - gmn[2]) : q3w,
+                                  q4 + 0.5 * (gup + P.gam) * (hp - hm) + psi * (Aterm + nodeB)};
+            RKIn x;
+#pragma unroll
+            for (int c = 0; c < 5; c++) {
+                x.Q[c] = qf[c];
+                if (rkf.has_source) x.Q[c] += F.js[c][o];
+                x.Qs[c] = F.Qs[c][o];
+                x.U[c] = (DIM == 2 && c == 3) ? 0.0 : rkf.in.U[c][o];
+                x.Un[c] = (DIM == 2 && c == 3) ? 0.0 : rkf.Un[c][o];
+            }
+            x.J = F.J[o];
+            rk_finish<DIM>(rkf.K, rkf.tau, F, rkf.out, o, x);
+            continue;
+        }
         F.Q[1][o] = q1 + psi * (gp[0] - gmn[0]);
         F.Q[2][o] = q2 + psi * (gp[1] - gmn[1]);
         if (DIM == 3) F.Q[3][o] = q3 + psi * (gp[2] - gmn[2]);
@@ -2111,53 +2221,6 @@ __device__ __forceinline__ void visc_body_full(const Grid &G, const Phys &P, con
 #undef QD
 }
 
-// ---------------------------------------------------------------------------
-// RK stage update of the real points (src/Functions.c:2300-2365), with the
-// time-independent source J*S added to Q first.
-// ---------------------------------------------------------------------------
-// Inputs of the RK update of one point, loaded ahead of the arithmetic so
-// that a thread can have several points' loads in flight.
-struct RKIn {
-    double Q[5], Qs[5], U[5], Un[5], J;
-};
-
-template <int DIM>
-__device__ __forceinline__ void rk_load(const StageIn &in, const Fields &F, int has_source, long long o, bool zero_qs,
-                                        RKIn &x)
-{
-#pragma unroll
-    for (int c = 0; c < 5; c++) {
-        x.Q[c] = F.Q[c][o];
-        if (has_source) x.Q[c] += F.js[c][o];
-        x.Qs[c] = zero_qs ? 0.0 : F.Qs[c][o];
-        x.U[c] = (DIM == 2 && c == 3) ? 0.0 : in.U[c][o];
-        x.Un[c] = (DIM == 2 && c == 3) ? 0.0 : F.Un[c][o];
-    }
-    x.J = F.J[o];
-}
-
-// The same arithmetic as rk_at on loaded inputs.
-template <int DIM>
-__device__ __forceinline__ void rk_finish(const RKCoef &K, double tau, const Fields &F, double *const outs[5],
-                                          long long o, const RKIn &x)
-{
-    double Qs[5];
-#pragma unroll
-    for (int c = 0; c < 5; c++) {
-        Qs[c] = x.Qs[c] + K.s * x.Q[c];
-        F.Qs[c][o] = Qs[c];
-    }
-    const double ro = x.U[0];
-    const double tj = tau / x.J;
-    const double rn = K.a * x.Un[0] + K.b * ro + tj * (K.c * x.Q[0] + K.d * Qs[0]);
-    outs[0][o] = rn;
-#pragma unroll
-    for (int c = 1; c < 5; c++) {
-        if (DIM == 2 && c == 3) { outs[3][o] = 0.0; continue; }
-        outs[c][o] = (K.a * x.Un[c] * x.Un[0] + K.b * x.U[c] * ro + tj * (K.c * x.Q[c] + K.d * Qs[c])) / rn;
-    }
-}
-
 // RK update of the real point at ghosted index o.
 template <int DIM>
 __device__ __forceinline__ void rk_at(const RKCoef &K, double tau, const StageIn &in, const Fields &F, double *o0,
@@ -2315,6 +2378,18 @@ constexpr size_t weno_smem_bytes()
     // (+ the face-flux buffer of the first faces when a thread takes two)
     return sizeof(double) * ((size_t)WenoNV<DIM, FULL>::NV * (TLN + ORDER + 1) * NLS +
                              ((MIXED || TLN + 1 == NROWT) ? 0 : 5 * NROWT * NLANE));
+}
+
+// The fused WENO + viscous sweep: the WENO part's buffer, or the WENO face
+// fluxes followed by the viscous part's buffer, whichever is larger.
+template <int DIM, int ORDER, bool MIXED, int TLN>
+constexpr size_t weno_visc_smem_bytes()
+{
+    const size_t w = weno_smem_bytes<DIM, ORDER, MIXED, TLN>();
+    const size_t v = sizeof(double) * ((size_t)5 * (TLN + 1) * NLS +
+                                       (size_t)(DIM == 3 ? (int)V3NV : (int)V2NV) * (TLN + ORDER + 1) * NLS +
+                                       4 * (TLN + 1) * NLS + 16 * NLANE);
+    return w > v ? w : v;
 }
 
 template <int ORDER, int TLN>

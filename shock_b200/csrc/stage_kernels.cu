@@ -118,6 +118,35 @@ struct ViscTile {
     static constexpr int v = (D == DIM - 1) ? TL : 7;
 };
 
+// Fused WENO + viscous sweep of one direction on the WENO tile: the
+// viscous loads of one tile overlap the WENO arithmetic of the other tile on
+// the SM, and Q is read and written once per direction instead of twice.
+// The mixed form keeps the separate sweeps: its WENO9 tile with the
+// viscous buffer would not fit twice per SM, and its fused WENO5 sweeps
+// measured 8 % slower than the separate ones (the FP32 WENO part is
+// shorter, so less of the viscous loads hides behind it).
+template <int ORDER, bool MIXED>
+struct FuseVisc {
+#ifdef SHOCK_NO_FUSED_SWEEPS
+    static constexpr bool on = false;
+#else
+    static constexpr bool on = !MIXED;
+#endif
+};
+
+template <int DIM, int ORDER, int D, bool MIXED, bool RKF>
+__global__ void __launch_bounds__(NTHR, (WenoTile<DIM, ORDER, MIXED>::minb))
+    k_weno_visc(Grid G, Phys P, bool first, const double *__restrict__ R, const double *__restrict__ Uu,
+                const double *__restrict__ Vv, const double *__restrict__ Ww, const double *__restrict__ Ee, Fields F,
+                RKFuse rk)
+{
+    constexpr int TLW = WenoTile<DIM, ORDER, MIXED>::tl;
+    weno_body<DIM, ORDER, D, MIXED, TLW, false, true>(G, P, first, R, Uu, Vv, Ww, Ee, F, blockIdx.x, blockIdx.y,
+                                                      blockIdx.z);
+    visc_body<DIM, ORDER, D, MIXED, TLW, true, RKF>(G, P, Uu, Vv, Ww, F, blockIdx.x, blockIdx.y, blockIdx.z, first,
+                                                    rk);
+}
+
 // The full 3D metric (FP64): the WENO face with full characteristic rows
 // takes the 15-cell tile and one tile per SM, as the 2D WENO9 face; the
 // viscous tile stages 22 values per point, one tile per SM.
@@ -137,12 +166,13 @@ __global__ void __launch_bounds__(NTHR, 1)
     visc_body_full<ORDER, D, ViscTile<3, D>::v>(G, P, Uu, Vv, Ww, F, blockIdx.x, blockIdx.y, blockIdx.z);
 }
 
-template <int DIM, int ORDER, int D, bool MIXED>
+template <int DIM, int ORDER, int D, bool MIXED, bool RKF>
 __global__ void __launch_bounds__(NTHR, ViscTile<DIM, D>::v == TL ? 2 : 3)
     k_visc(Grid G, Phys P, const double *__restrict__ Uu, const double *__restrict__ Vv,
-           const double *__restrict__ Ww, Fields F)
+           const double *__restrict__ Ww, Fields F, RKFuse rk)
 {
-    visc_body<DIM, ORDER, D, MIXED, ViscTile<DIM, D>::v>(G, P, Uu, Vv, Ww, F, blockIdx.x, blockIdx.y, blockIdx.z);
+    visc_body<DIM, ORDER, D, MIXED, ViscTile<DIM, D>::v, false, RKF>(G, P, Uu, Vv, Ww, F, blockIdx.x, blockIdx.y,
+                                                                     blockIdx.z, false, rk);
 }
 
 // Rows of real points: x runs along the fastest real axis (k in 3D, j in
@@ -321,6 +351,37 @@ static void weno_one(const Grid &G, const Phys &P, bool first, const double *con
                                                                                              U[2], U[3], U[4], F);
 }
 
+// The RK update goes into the last fused sweep with WENO9 only: there its
+// loads hide behind the longer WENO arithmetic (the WENO9 zeta sweep took
+// 56 us more at 128^3 against 70 us for the separate update), while the
+// WENO5 sweep lost more (94 us) than the separate update costs.
+template <int DIM, int ORDER, int D, bool MIXED>
+static bool weno_visc_one(const Grid &G, const Phys &P, bool first, const double *const U[5], const Fields &F,
+                          cudaStream_t s, const RKFuse *rk)
+{
+    if constexpr (FuseVisc<ORDER, MIXED>::on) {
+        constexpr int WTL = WenoTile<DIM, ORDER, MIXED>::tl;
+        constexpr size_t smem = weno_visc_smem_bytes<DIM, ORDER, MIXED, WTL>();
+        constexpr bool LAST = D == DIM - 1 && ORDER == 9;   // sweeps that can end the stage
+        if (!G.order) {
+            cudaFuncSetAttribute(k_weno_visc<DIM, ORDER, D, MIXED, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+            if (LAST)
+                cudaFuncSetAttribute(k_weno_visc<DIM, ORDER, D, MIXED, LAST>,
+                                     cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+            return false;
+        }
+        if (LAST && rk) {
+            k_weno_visc<DIM, ORDER, D, MIXED, LAST><<<sweep_grid<DIM, D, WTL>(G), dim3(NLANE, NROWT), smem, s>>>(
+                G, P, first, U[0], U[1], U[2], U[3], U[4], F, *rk);
+            return true;
+        }
+        k_weno_visc<DIM, ORDER, D, MIXED, false><<<sweep_grid<DIM, D, WTL>(G), dim3(NLANE, NROWT), smem, s>>>(
+            G, P, first, U[0], U[1], U[2], U[3], U[4], F, RKFuse{});
+    }
+    return false;
+}
+
 template <int ORDER, int D>
 static void weno_full_one(const Grid &G, const Phys &P, bool first, const double *const U[5], const Fields &F,
                           cudaStream_t s)
@@ -347,15 +408,28 @@ static void visc_full_one(const Grid &G, const Phys &P, const double *const U[5]
 }
 
 template <int DIM, int ORDER, int D, bool MIXED>
-static void visc_one(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s)
+static bool visc_one(const Grid &G, const Phys &P, const double *const U[5], const Fields &F, cudaStream_t s,
+                     const RKFuse *rk = nullptr)
 {
     constexpr int VTL = ViscTile<DIM, D>::v;
     constexpr size_t smem = visc_smem_bytes<DIM, ORDER, VTL>();
+    constexpr bool LAST = D == DIM - 1;   // only the last direction's sweep can end the stage
     if (!G.order) {
-        cudaFuncSetAttribute(k_visc<DIM, ORDER, D, MIXED>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        return;
+        cudaFuncSetAttribute(k_visc<DIM, ORDER, D, MIXED, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
+        if (LAST)
+            cudaFuncSetAttribute(k_visc<DIM, ORDER, D, MIXED, LAST>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)smem);
+        return false;
     }
-    k_visc<DIM, ORDER, D, MIXED><<<sweep_grid<DIM, D, VTL>(G), dim3(NLANE, NROWT), smem, s>>>(G, P, U[1], U[2], U[3], F);
+    if (LAST && rk) {
+        k_visc<DIM, ORDER, D, MIXED, LAST><<<sweep_grid<DIM, D, VTL>(G), dim3(NLANE, NROWT), smem, s>>>(
+            G, P, U[1], U[2], U[3], F, *rk);
+        return true;
+    }
+    k_visc<DIM, ORDER, D, MIXED, false><<<sweep_grid<DIM, D, VTL>(G), dim3(NLANE, NROWT), smem, s>>>(
+        G, P, U[1], U[2], U[3], F, RKFuse{});
+    return false;
 }
 
 #define SHOCK_SWEEP_CASES(X)                                                           \
@@ -376,18 +450,38 @@ void launch_weno(const Grid &G, const Phys &P, int precision, int d, bool first,
 #undef W
 }
 
-void launch_viscous(const Grid &G, const Phys &P, int precision, int d, const double *const U[5],
-                    const Fields &F, cudaStream_t s)
+bool fused_sweeps(const Grid &G, const Phys &P, int precision)
 {
-#define V(DIM, ORD, D)                                                               \
-    if (G.dim == DIM && G.order == ORD && d == D) {                                   \
-        if (DIM == 3 && P.full) visc_full_one<ORD, D>(G, P, U, F, s);                  \
-        else if (precision == SHOCK_MIXED) visc_one<DIM, ORD, D, true>(G, P, U, F, s); \
-        else visc_one<DIM, ORD, D, false>(G, P, U, F, s);                             \
-        return;                                                                       \
+    if (P.full) return false;
+    return G.order == 5 ? (precision == SHOCK_MIXED ? FuseVisc<5, true>::on : FuseVisc<5, false>::on)
+                        : (precision == SHOCK_MIXED ? FuseVisc<9, true>::on : FuseVisc<9, false>::on);
+}
+
+bool launch_weno_visc(const Grid &G, const Phys &P, int precision, int d, bool first, const double *const U[5],
+                      const Fields &F, cudaStream_t s, const RKFuse *rk)
+{
+#define WV(DIM, ORD, D)                                                                                  \
+    if (G.dim == DIM && G.order == ORD && d == D) {                                                       \
+        if (precision == SHOCK_MIXED) return weno_visc_one<DIM, ORD, D, true>(G, P, first, U, F, s, rk);  \
+        return weno_visc_one<DIM, ORD, D, false>(G, P, first, U, F, s, rk);                               \
+    }
+    SHOCK_SWEEP_CASES(WV)
+#undef WV
+    return false;
+}
+
+bool launch_viscous(const Grid &G, const Phys &P, int precision, int d, const double *const U[5],
+                    const Fields &F, cudaStream_t s, const RKFuse *rk)
+{
+#define V(DIM, ORD, D)                                                                          \
+    if (G.dim == DIM && G.order == ORD && d == D) {                                              \
+        if (DIM == 3 && P.full) { visc_full_one<ORD, D>(G, P, U, F, s); return false; }           \
+        if (precision == SHOCK_MIXED) return visc_one<DIM, ORD, D, true>(G, P, U, F, s, rk);      \
+        return visc_one<DIM, ORD, D, false>(G, P, U, F, s, rk);                                   \
     }
     SHOCK_SWEEP_CASES(V)
 #undef V
+    return false;
 }
 
 void launch_rk(const Grid &G, const RKCoef &rk, double tau, const double *const Uin[5], double *const Uout[5],
@@ -452,6 +546,8 @@ void prepare_kernels()
     G.order = 0;
 #define A(DIM, ORD, D)                                                                         \
     weno_one<DIM, ORD, D, false>(G, P, true, U, F, 0); weno_one<DIM, ORD, D, true>(G, P, true, U, F, 0); \
+    weno_visc_one<DIM, ORD, D, false>(G, P, true, U, F, 0, nullptr);                               \
+    weno_visc_one<DIM, ORD, D, true>(G, P, true, U, F, 0, nullptr);                                \
     visc_one<DIM, ORD, D, false>(G, P, U, F, 0); visc_one<DIM, ORD, D, true>(G, P, U, F, 0);
     SHOCK_SWEEP_CASES(A)
 #undef A
@@ -529,25 +625,34 @@ void launch_film_gather(const Grid &G, const double *const U[5], const double *p
 }
 
 // Halo exchange between the blocks of a division (src/Functions.c:3580-3684
-// with WriteValuesFromUToBuffer / WriteValuesFromBufferToU, :2697-2863, for
-// the identity orientation): blockIdx.y is the receiving face, x strides
-// over its points.
+// with WriteValuesFromUToBuffer / WriteValuesFromBufferToU, :2697-2863):
+// blockIdx.y is the receiving face, x strides over its points.  The sender
+// packs its region in its own index order; the receiver reads each of its
+// points through the interface's transform (get_ijkTransformWithGhosts,
+// :4287-4313): its axis c runs along the sender's axis map[c], reversed
+// where flip[c].
 template <bool PACK>
 __global__ void __launch_bounds__(256) k_exchange(const XFace *__restrict__ faces, long long total,
                                                   double *__restrict__ stage)
 {
     const XFace &F = faces[blockIdx.y];
-    const long long n = (long long)F.ext[0] * F.ext[1] * F.ext[2];
+    const int *e = PACK ? F.sext : F.ext;
+    const long long n = (long long)e[0] * e[1] * e[2];
     for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < n; t += (long long)gridDim.x * blockDim.x) {
-        const int k = (int)(t % F.ext[2]);
-        const long long r = t / F.ext[2];
-        const int j = (int)(r % F.ext[1]), i = (int)(r / F.ext[1]);
-        const long long q = F.off + t;
+        const int k = (int)(t % e[2]);
+        const long long r = t / e[2];
+        const int j = (int)(r % e[1]), i = (int)(r / e[1]);
         if (PACK) {
+            const long long q = F.off + t;
             const long long o = (long long)(F.slo[0] + i) * F.sst[0] + (long long)(F.slo[1] + j) * F.sst[1] + F.slo[2] + k;
 #pragma unroll
             for (int c = 0; c < 5; c++) stage[c * total + q] = F.src[c][o];
         } else {
+            const int rr[3] = {i, j, k};
+            int d[3];
+#pragma unroll
+            for (int c = 0; c < 3; c++) d[F.map[c]] = F.flip[c] ? F.sext[F.map[c]] - 1 - rr[c] : rr[c];
+            const long long q = F.off + ((long long)d[0] * F.sext[1] + d[1]) * F.sext[2] + d[2];
             const long long o = (long long)(F.rlo[0] + i) * F.rst[0] + (long long)(F.rlo[1] + j) * F.rst[1] + F.rlo[2] + k;
 #pragma unroll
             for (int c = 0; c < 5; c++) F.dst[c][o] = stage[c * total + q];

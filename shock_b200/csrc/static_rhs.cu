@@ -129,9 +129,13 @@ extern "C" int shock_rhs_static(const shock_params *p, const double *geom13, dou
     launch_ghosts(G, U, s);
     launch_prim(G, P, cU, F, s);
     if (!p->inviscid) launch_nodal(G, P, p->precision, cU, F, s);
-    for (int d = 0; d < p->dim; d++) launch_weno(G, P, p->precision, d, d == 0, cU, F, s);
-    if (!p->inviscid)
-        for (int d = 0; d < p->dim; d++) launch_viscous(G, P, p->precision, d, cU, F, s);
+    if (!p->inviscid && fused_sweeps(G, P, p->precision)) {
+        for (int d = 0; d < p->dim; d++) launch_weno_visc(G, P, p->precision, d, d == 0, cU, F, s);
+    } else {
+        for (int d = 0; d < p->dim; d++) launch_weno(G, P, p->precision, d, d == 0, cU, F, s);
+        if (!p->inviscid)
+            for (int d = 0; d < p->dim; d++) launch_viscous(G, P, p->precision, d, cU, F, s);
+    }
     CKS(cudaGetLastError());
     return SHOCK_OK;
 }

@@ -31,7 +31,32 @@ DIVISIONS = {
     "channel3d_w5_walls_2x2x1": lambda: (cases.channel(3, 5, (16, 14, 12)), (2, 2, 1), 20),
     "tgv16_w5_inviscid_rk3_2x2x2": lambda: (cases.taylor_green(16, order=5).replace(inviscid=True, time_order=3),
                                             (2, 2, 2), 20),
+    # zones meshed in other orientations (.sddc Transforms other than 1,2,3):
+    # (block, its new axes in terms of its old ones, which run reversed), all
+    # proper rotations; 3D blocks with permuted axes take the full metric
+    # (their metric is in the cross terms the reference mode zeroes)
+    "tgv16_w5_2x2x1_rotated_full": lambda: (cases.taylor_green(16, order=5), (2, 2, 1), 20,
+                                            [(1, (1, 0, 2), (True, False, False)),
+                                             (3, (0, 1, 2), (True, True, False))], True),
+    "smooth2d_w5_2x2_rotated": lambda: (cases.smooth_random(2, 5, (24, 20, 1), seed=4, stretch=0.08), (2, 2, 1), 20,
+                                        [(2, (1, 0, 2), (False, True, False))]),
+    "smooth3d_w9_2x1x2_rotated_full": lambda: (cases.smooth_random(3, 9, (21, 10, 23), seed=6, stretch=0.05),
+                                               (2, 1, 2), 10, [(3, (1, 0, 2), (False, False, True))], True),
+    "channel3d_w5_walls_2x2x1_rotated": lambda: (cases.channel(3, 5, (16, 14, 12)), (2, 2, 1), 20,
+                                                 [(0, (0, 1, 2), (True, True, False))]),
 }
+
+
+def division(name):
+    """(case, division, steps, full metric) of a named division, its rotated
+    blocks applied."""
+    case, parts, nsteps, *more = DIVISIONS[name]()
+    rot = more[0] if more else []
+    full = more[1] if len(more) > 1 else False
+    d = cases.split(case, parts)
+    for b, axes, flips in rot:
+        d = cases.rotate_block(d, b, axes, flips)
+    return case, d, nsteps, full
 
 
 def _real(case, block, a):
@@ -45,22 +70,21 @@ def _assemble(d, per_block):
     c = d.case
     out = np.zeros((per_block[0].shape[0], c.ni, c.nj, c.nk if c.dim == 3 else 1))
     for b, a in enumerate(per_block):
-        blk, lo = d.blocks[b], d.lo[b]
-        nk = blk.nk if c.dim == 3 else 1
-        out[:, lo[0]:lo[0] + blk.ni, lo[1]:lo[1] + blk.nj, lo[2]:lo[2] + nk] = _real(c, blk, a)
+        lo = d.lo[b]
+        r = d.from_block(b, _real(c, d.blocks[b], a))
+        out[:, lo[0]:lo[0] + r.shape[1], lo[1]:lo[1] + r.shape[2], lo[2]:lo[2] + r.shape[3]] = r
     return out
 
 
 @pytest.mark.parametrize("name", sorted(DIVISIONS))
 def test_division_matches_shock_multirank(name, parity):
-    case, parts, nsteps = DIVISIONS[name]()
-    if not multirank_available(case.order, case.dim):
+    case, d, nsteps, full = division(name)
+    if not multirank_available(case.order, case.dim, full=full):
         pytest.skip("multi-rank reference build absent (make -C oracle with the reference sources)")
-    d = cases.split(case, parts)
-    ref = run_multirank(d, nsteps, rhs=True)
-    ref80 = run_multirank(d, nsteps, rhs=True, extended=True) if multirank_available(case.order, case.dim, True) \
-        else None
-    m = shock_b200.Multi(d)
+    ref = run_multirank(d, nsteps, rhs=True, full=full)
+    ref80 = run_multirank(d, nsteps, rhs=True, extended=True, full=full) \
+        if multirank_available(case.order, case.dim, True, full=full) else None
+    m = shock_b200.Multi(d, full_metric=full)
     try:
         for b in range(len(d.blocks)):
             assert np.array_equal(m.geometry(b), ref[b]["geometry"]), b

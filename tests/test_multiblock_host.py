@@ -16,17 +16,43 @@ DIVISIONS = {
     "smooth2d_w5_2x2": lambda: (cases.smooth_random(2, 5, (24, 20, 1), seed=4, stretch=0.08), (2, 2, 1)),
     "smooth3d_w9_uneven_2x1x2": lambda: (cases.smooth_random(3, 9, (21, 12, 23), seed=6, stretch=0.05), (2, 1, 2)),
     "channel3d_w5_walls_2x2x1": lambda: (cases.channel(3, 5, (16, 14, 12)), (2, 2, 1)),
+    # zones meshed in other orientations (.sddc Transforms other than 1,2,3):
+    # (block, its new axes in terms of its old ones, which run reversed), all
+    # proper rotations.  A 3D block with permuted axes has its metric in the
+    # cross terms, so those divisions take the full metric (SHOCK's
+    # full-metric multi-rank build); reversed axes alone keep the diagonal one.
+    "tgv16_w5_2x2x1_rotated_full": lambda: (cases.taylor_green(16, order=5), (2, 2, 1),
+                                            [(1, (1, 0, 2), (True, False, False)), (3, (0, 1, 2), (True, True, False))],
+                                            True),
+    "tgv12_w5_2x2x2_rotated_all_full": lambda: (cases.taylor_green(12, order=5), (2, 2, 2), [
+        (b, ((1, 0, 2), (2, 0, 1), (0, 2, 1), (1, 2, 0))[b % 4],
+         ((1, 0, 0), (1, 1, 0), (0, 0, 1), (0, 0, 0), (0, 1, 0), (0, 1, 1), (1, 1, 1), (1, 0, 1))[b])
+        for b in range(8)], True),
+    "smooth2d_w5_2x2_rotated": lambda: (cases.smooth_random(2, 5, (24, 20, 1), seed=4, stretch=0.08), (2, 2, 1),
+                                        [(2, (1, 0, 2), (False, True, False)), (1, (0, 1, 2), (True, True, False))]),
+    "channel3d_w5_walls_2x2x1_rotated": lambda: (cases.channel(3, 5, (16, 14, 12)), (2, 2, 1),
+                                                 [(0, (0, 1, 2), (True, True, False))]),
 }
+
+
+def division(name):
+    """(case, division, full metric) of a named division, its rotated blocks applied."""
+    case, parts, *more = DIVISIONS[name]()
+    rot = more[0] if more else []
+    full = more[1] if len(more) > 1 else False
+    d = cases.split(case, parts)
+    for b, axes, flips in rot:
+        d = cases.rotate_block(d, b, axes, [bool(x) for x in flips])
+    return case, d, full
 
 
 @pytest.mark.parametrize("name", sorted(DIVISIONS))
 def test_division_geometry_matches_shock_multirank(name):
-    case, parts = DIVISIONS[name]()
-    if not multirank_available(case.order, case.dim):
+    case, d, full = division(name)
+    if not multirank_available(case.order, case.dim, full=full):
         pytest.skip("multi-rank reference build absent (make -C oracle with the reference sources)")
-    d = cases.split(case, parts)
-    got = shock_b200.host_multi_geometry(d)
-    ref = run_multirank(d, 0)
+    got = shock_b200.host_multi_geometry(d, full_metric=full)
+    ref = run_multirank(d, 0, full=full)
     for b in range(len(d.blocks)):
         assert np.array_equal(got[b], ref[b]["geometry"]), (name, b)
 
