@@ -550,6 +550,31 @@ struct Axes {
     static constexpr bool CONTIG = (D == DIM - 1);   // sweep along the contiguous axis
 };
 
+// Along the contiguous axis consecutive threads walk the points of one
+// line.  Each line gets a power-of-two number of thread slots (the slots
+// past its N points idle), so that a half-warp never holds points of two
+// lines: with the lane stride NLS = 33 its 8-byte shared-memory accesses
+// then fall in 16 distinct bank pairs, where a half-warp across a line
+// break hits the same banks twice.  A line of N = 1 (mod 16) points
+// crosses its breaks without a conflict (the jump is one bank pair, as
+// within the line), so its staging keeps the dense mapping rather than pay
+// for idle slots.  Measured at 512^3 (WENO5 / WENO9 steps): 286.4 / 504.3 ms
+// with the dense mapping everywhere, 284.5 / 500.6 ms with slots in the
+// cell updates, 282.1 / 513.0 ms with slots in every staging too.
+#ifndef SHOCK_CONTIG_LINE_SLOTS
+#define SHOCK_CONTIG_LINE_SLOTS 1
+#endif
+template <int N>
+__host__ __device__ constexpr int line_slots()
+{
+    return SHOCK_CONTIG_LINE_SLOTS ? (N <= 8 ? 8 : N <= 16 ? 16 : 32) : N;
+}
+template <int N>
+__host__ __device__ constexpr int stage_slots()
+{
+    return N % 16 == 1 ? N : line_slots<N>();
+}
+
 constexpr int TL = 15;         // cells per tile along the sweep
 constexpr int NFACE = TL + 1;  // faces per tile line
 constexpr int NLANE = 32;      // lines per tile
@@ -609,15 +634,17 @@ __device__ __forceinline__ void stage_weno(const Grid &G, const Phys &P, const T
     const int tid = threadIdx.y * NLANE + threadIdx.x;
     // unrolled over the thread's points (about three) so that all their
     // global loads are in flight before the first shared-memory store
-    constexpr int NSTG = (NP * NLANE + NTHR - 1) / NTHR;
+    constexpr int SL = A::CONTIG ? stage_slots<NP>() : NP;   // thread slots per line
+    constexpr int NSTG = (SL * NLANE + NTHR - 1) / NTHR;
 #pragma unroll
     for (int m = 0; m < NSTG; m++) {
         const int it = tid + m * NTHR;
-        if (it >= NP * NLANE) continue;
+        if (it >= SL * NLANE) continue;
         // along the contiguous axis consecutive threads take consecutive
         // points of a line (coalesced loads; the padded lane stride keeps the
         // shared-memory stores conflict-free), otherwise consecutive lines
-        const int l = A::CONTIG ? it / NP : it % NLANE, t = A::CONTIG ? it % NP : it / NLANE;
+        const int l = A::CONTIG ? it / SL : it % NLANE, t = A::CONTIG ? it % SL : it / NLANE;
+        if (t >= NP) continue;
         int pd = T.c0 - 1 - r + t;
         if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
         long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
@@ -1442,9 +1469,10 @@ __device__ __forceinline__ void weno_body(const Grid &G, const Phys &P, bool fir
     }
     // flux difference into Q; along a contiguous axis the threads walk the
     // cells of one line (coalesced), otherwise one line per lane
-    for (int it = row * NLANE + lane; it < TLN * NLANE; it += NTHR) {
+    constexpr int SC = Axes<DIM, D>::CONTIG ? line_slots<TLN>() : TLN;   // thread slots per line
+    for (int it = row * NLANE + lane; it < SC * NLANE; it += NTHR) {
         int cr, ln;
-        if (Axes<DIM, D>::CONTIG) { cr = it % TLN; ln = it / TLN; }
+        if (Axes<DIM, D>::CONTIG) { cr = it % SC; ln = it / SC; if (cr >= TLN) continue; }
         else { ln = it % NLANE; cr = it / NLANE; }
         if (T.l0 + ln >= G.g + T.nL || T.c0 + cr > G.g + T.nD - 1) continue;
         long long o = T.base + (long long)ln * T.sL + (long long)(T.c0 + cr) * T.sD;
@@ -1580,7 +1608,8 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
     double *fo = sh + NV * NP * NLS;         // [4][NFT][NLS]
     double *qd = fo + 4 * NFT * NLS;         // quirk: [16][NLANE] per-line half-point values
     double *cq = qd + 16 * NLANE;            // [ViscCellIn::N][TLN * NLANE] prefetched cell inputs
-    constexpr int CQS = TLN * NLANE;
+    constexpr int SC = A::CONTIG ? line_slots<TLN>() : TLN;   // thread slots per line (cell update)
+    constexpr int CQS = SC * NLANE;
     constexpr bool PF = ViscCellIn<DIM, ORDER, TLN>::prefetch && !FUSED;
 #define SH(v, t, l) sh[((v) * NP + (t)) * NLS + (l)]
 #define FO(c, f, l) fo[((c) * NFT + (f)) * NLS + (l)]
@@ -1593,14 +1622,16 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
     const int tid = row * NLANE + lane;
     // unrolled over the thread's points (about three) so that all their
     // global loads are in flight before the first shared-memory store
-    constexpr int NSTG = (NP * NLANE + NTHR - 1) / NTHR;
+    constexpr int SL = A::CONTIG ? stage_slots<NP>() : NP;   // thread slots per line
+    constexpr int NSTG = (SL * NLANE + NTHR - 1) / NTHR;
 #pragma unroll
     for (int m = 0; m < NSTG; m++) {
         const int it = tid + m * NTHR;
-        if (it >= NP * NLANE) continue;
+        if (it >= SL * NLANE) continue;
         // along the contiguous axis consecutive threads take consecutive
         // points of a line (coalesced), otherwise consecutive lines
-        const int l = A::CONTIG ? it / NP : it % NLANE, t = A::CONTIG ? it % NP : it / NLANE;
+        const int l = A::CONTIG ? it / SL : it % NLANE, t = A::CONTIG ? it % SL : it / NLANE;
+        if (t >= NP) continue;
         int pd = T.c0 - H + t;
         if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
         long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
@@ -1636,9 +1667,9 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
     }
     // prefetch the cell update's global inputs (same cell-to-thread map as the
     // update below); they arrive while the faces are computed
-    for (int it = row * NLANE + threadIdx.x; PF && it < TLN * NLANE; it += NTHR) {
+    for (int it = row * NLANE + threadIdx.x; PF && it < SC * NLANE; it += NTHR) {
         int cr, ln;
-        if (A::CONTIG) { cr = it % TLN; ln = it / TLN; }
+        if (A::CONTIG) { cr = it % SC; ln = it / SC; if (cr >= TLN) continue; }
         else { ln = it % NLANE; cr = it / NLANE; }
         if (T.l0 + ln >= G.g + T.nL || T.c0 + cr > G.g + T.nD - 1) continue;
         const long long o = T.base + (long long)ln * T.sL + (long long)(T.c0 + cr) * T.sD;
@@ -1842,9 +1873,9 @@ __device__ __forceinline__ void visc_body(const Grid &G, const Phys &P, const do
 
     // ---- cell update: along a contiguous axis the threads walk the cells of
     // one line (coalesced), otherwise one line per thread lane ----------------
-    for (int it = row * NLANE + threadIdx.x; it < TLN * NLANE; it += NTHR) {
+    for (int it = row * NLANE + threadIdx.x; it < SC * NLANE; it += NTHR) {
         int cr, ln;
-        if (A::CONTIG) { cr = it % TLN; ln = it / TLN; }
+        if (A::CONTIG) { cr = it % SC; ln = it / SC; if (cr >= TLN) continue; }
         else { ln = it % NLANE; cr = it / NLANE; }
         if (T.l0 + ln >= G.g + T.nL || T.c0 + cr > G.g + T.nD - 1) continue;
         long long o = T.base + (long long)ln * T.sL + (long long)(T.c0 + cr) * T.sD;
@@ -2061,12 +2092,14 @@ __device__ __forceinline__ void visc_body_full(const Grid &G, const Phys &P, con
     const int lane = threadIdx.x, row = threadIdx.y;
     const Tile T = make_tile<3, D, TLN>(G, lane, bx, by, bz);
     const int tid = row * NLANE + lane;
-    constexpr int NSTG = (NP * NLANE + NTHR - 1) / NTHR;
+    constexpr int SL = A::CONTIG ? stage_slots<NP>() : NP;   // thread slots per line
+    constexpr int NSTG = (SL * NLANE + NTHR - 1) / NTHR;
 #pragma unroll
     for (int m = 0; m < NSTG; m++) {
         const int it = tid + m * NTHR;
-        if (it >= NP * NLANE) continue;
-        const int l = A::CONTIG ? it / NP : it % NLANE, t = A::CONTIG ? it % NP : it / NLANE;
+        if (it >= SL * NLANE) continue;
+        const int l = A::CONTIG ? it / SL : it % NLANE, t = A::CONTIG ? it % SL : it / NLANE;
+        if (t >= NP) continue;
         const int pd = T.c0 - H + t;
         if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
         const long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
@@ -2166,9 +2199,10 @@ __device__ __forceinline__ void visc_body_full(const Grid &G, const Phys &P, con
     __syncthreads();
 
     const double t23 = 2.0 / 3.0;
-    for (int it = row * NLANE + lane; it < TLN * NLANE; it += NTHR) {
+    constexpr int SC = A::CONTIG ? line_slots<TLN>() : TLN;   // thread slots per line
+    for (int it = row * NLANE + lane; it < SC * NLANE; it += NTHR) {
         int cr, ln;
-        if (A::CONTIG) { cr = it % TLN; ln = it / TLN; }
+        if (A::CONTIG) { cr = it % SC; ln = it / SC; if (cr >= TLN) continue; }
         else { ln = it % NLANE; cr = it / NLANE; }
         if (T.l0 + ln >= G.g + T.nL || T.c0 + cr > G.g + T.nD - 1) continue;
         const long long o = T.base + (long long)ln * T.sL + (long long)(T.c0 + cr) * T.sD;
@@ -2380,6 +2414,43 @@ constexpr size_t weno_smem_bytes()
                              ((MIXED || TLN + 1 == NROWT) ? 0 : 5 * NROWT * NLANE));
 }
 
+// The fused sweep's viscous inputs that its WENO part does not load, asked
+// into L2 when the tile starts (prefetch.global.L2), so that the viscous
+// staging after the WENO arithmetic finds them there instead of in HBM.
+template <int DIM, int ORDER, int D, int TLN>
+__device__ __forceinline__ void visc_l2_prefetch(const Grid &G, const Fields &F, int bx, int by, int bz)
+{
+    using A = Axes<DIM, D>;
+    constexpr int H = ZD<ORDER>::H;
+    constexpr int NP = TLN + 2 * H;
+    const Tile T = make_tile<DIM, D, TLN>(G, threadIdx.x, bx, by, bz);
+    const int tid = threadIdx.y * NLANE + threadIdx.x;
+    for (int it = tid; it < NP * NLANE; it += NTHR) {
+        const int l = A::CONTIG ? it / NP : it % NLANE, t = A::CONTIG ? it % NP : it / NLANE;
+        const int pd = T.c0 - H + t;
+        if (T.l0 + l >= G.g + T.nL || pd >= G.N[D]) continue;
+        const long long o = T.base + (long long)l * T.sL + (long long)pd * T.sD;
+        const double *src[11];
+        int n = 0;
+        src[n++] = F.T + o;
+        src[n++] = F.mu + o;
+        if (DIM == 3) {
+            constexpr int MA = (D == 0) ? 1 : 0, MB = (D == 2) ? 1 : 2;
+            const int nd[7] = {3 * MA + MA, 3 * MB + MB, 3 * D + MA, 3 * D + MB, 3 * D + D, 3 * MA + D, 3 * MB + D};
+            for (int q = 0; q < 7; q++) src[n++] = F.Nd[nd[q]] + o;
+            src[n++] = F.m[4 * MA] + o;
+            src[n++] = F.m[4 * MB] + o;
+        } else {
+            constexpr int E = 1 - D;
+            const int nd[5] = {E, 3 + E, 9 + E, D, 3 + D};
+            for (int q = 0; q < 5; q++) src[n++] = F.Nd[nd[q]] + o;
+            src[n++] = F.m[3 * E + 0] + o;
+            src[n++] = F.m[3 * E + 1] + o;
+        }
+        for (int q = 0; q < n; q++) asm volatile("prefetch.global.L2 [%0];" ::"l"(src[q]));
+    }
+}
+
 // The fused WENO + viscous sweep: the WENO part's buffer, or the WENO face
 // fluxes followed by the viscous part's buffer, whichever is larger.
 template <int DIM, int ORDER, bool MIXED, int TLN>
@@ -2402,7 +2473,7 @@ template <int DIM, int ORDER, int TLN = TL>
 constexpr size_t visc_smem_bytes()
 {
     return sizeof(double) * ((size_t)(DIM == 3 ? (int)V3NV : (int)V2NV) * (TLN + ORDER + 1) * NLS + 4 * (TLN + 1) * NLS + 16 * NLANE +
-                             (size_t)ViscCellIn<DIM, ORDER, TLN>::N * TLN * NLANE);
+                             (size_t)ViscCellIn<DIM, ORDER, TLN>::N * line_slots<TLN>() * NLANE);
 }
 
 }  // namespace shock

@@ -125,6 +125,9 @@ struct ViscTile {
 // viscous buffer would not fit twice per SM, and its fused WENO5 sweeps
 // measured 8 % slower than the separate ones (the FP32 WENO part is
 // shorter, so less of the viscous loads hides behind it).
+#ifndef SHOCK_FUSED_L2_PREFETCH
+#define SHOCK_FUSED_L2_PREFETCH 1
+#endif
 template <int ORDER, bool MIXED>
 struct FuseVisc {
 #ifdef SHOCK_NO_FUSED_SWEEPS
@@ -141,6 +144,11 @@ __global__ void __launch_bounds__(NTHR, (WenoTile<DIM, ORDER, MIXED>::minb))
                 RKFuse rk)
 {
     constexpr int TLW = WenoTile<DIM, ORDER, MIXED>::tl;
+    // with WENO5 only: at 512^3 it took the WENO5 step from 296.2 to 289.9 ms,
+    // the WENO9 one from 490.3 to 508.9 ms (the longer WENO9 part issues
+    // enough of its own memory work, and the prefetches cost it issue slots)
+    if (SHOCK_FUSED_L2_PREFETCH && ORDER == 5)
+        visc_l2_prefetch<DIM, ORDER, D, TLW>(G, F, blockIdx.x, blockIdx.y, blockIdx.z);
     weno_body<DIM, ORDER, D, MIXED, TLW, false, true>(G, P, first, R, Uu, Vv, Ww, Ee, F, blockIdx.x, blockIdx.y,
                                                       blockIdx.z);
     visc_body<DIM, ORDER, D, MIXED, TLW, true, RKF>(G, P, Uu, Vv, Ww, F, blockIdx.x, blockIdx.y, blockIdx.z, first,
