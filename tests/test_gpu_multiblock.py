@@ -7,7 +7,11 @@ SHOCK's results depend on the division itself, not only on the whole
 block: its zeta viscous stencil is centred on the block-local j index
 (src/ZD.c:547-548), so a 3D viscous run split differently gives different
 numbers.  The device reproduces that, block by block, so it is compared
-with the reference run of the same division.  Tolerances as in the
+with the reference run of the same division.  Divisions with zones meshed
+in other orientations (.sddc Transforms other than 1,2,3; blocks re-indexed
+by cases.rotate_block) check the transformed exchange; a 3D block with
+permuted axes needs the full metric, so those run against SHOCK's
+full-metric multi-rank build.  Tolerances as in the
 single-block parity tests: per variable, 1e-12 normwise for one RHS and
 1e-10 relative L2 after the steps, or twice SHOCK's own FP64-vs-80-bit
 distance on the same division where that is larger (the Mach 0.1

@@ -3,7 +3,9 @@ geometry set-up with the interfaces exchanged (shock_host_multi_geometry)
 against SHOCK's own multi-rank run of the same division (oracle/_ref/
 libshockmpi_*: SHOCK's TransferMeshParameter between ranks over the forked
 shared-memory stand-in for MPI), bit for bit on every ghosted point of
-every block; and the division bookkeeping."""
+every block, also for divisions whose zones are meshed in other
+orientations (.sddc Transforms other than 1,2,3); and the division
+bookkeeping."""
 import numpy as np
 import pytest
 
@@ -71,3 +73,46 @@ def test_split_bookkeeping():
     dc = cases.split(ch, (1, 2, 1))
     assert dc.neighbour[0, 2] == -1 and dc.blocks[0].bc[2] == ch.bc[2]
     assert dc.neighbour[0, 3] == 1 and dc.blocks[0].bc[3] == 0
+
+
+def test_rotated_division_bookkeeping():
+    """cases.rotate_block re-indexes a block's fields and faces; every
+    interface is then named from both sides with inverse Transforms, and
+    turning the block back gives the original division."""
+    c = cases.taylor_green(12, order=5)
+    d0 = cases.split(c, (2, 2, 1))
+    d = cases.rotate_block(d0, 1, (1, 0, 2), (True, False, False))
+    assert d.blocks[1].ni == d0.blocks[1].nj and d.blocks[1].nj == d0.blocks[1].ni
+    assert np.array_equal(d.to_block(1, np.stack([c.x, c.y])), np.stack([d.blocks[1].x, d.blocks[1].y]))
+    assert np.array_equal(d.from_block(1, d.blocks[1].u[None]), d0.blocks[1].u[None])
+    for b in range(4):
+        for f in range(6):
+            n = d.neighbour[b, f]
+            if n < 0:
+                continue
+            t = d.transform[b, f]
+            a, hi = f // 2, f % 2
+            fd = 2 * (abs(t[a]) - 1) + (hi ^ int(t[a] > 0))
+            assert d.neighbour[n, fd] == b
+            back = d.transform[n, fd]
+            for ax in range(3):
+                assert back[abs(t[ax]) - 1] == np.sign(t[ax]) * (ax + 1)
+    # turning block 1 back: new axis c runs along old axis (1,0,2)[c]; undo with the inverse
+    d2 = cases.rotate_block(d, 1, (1, 0, 2), (False, True, False))
+    assert np.array_equal(d2.blocks[1].x, d0.blocks[1].x) and np.array_equal(d2.transform, d0.transform)
+
+
+def test_inconsistent_transforms_rejected():
+    """An interface whose two sides do not carry inverse Transforms, or a
+    Transform that is not a signed permutation, is refused (SHOCK_EINVAL)."""
+    c = cases.taylor_green(12, order=5)
+    d = cases.rotate_block(cases.split(c, (2, 2, 1)), 1, (1, 0, 2), (True, False, False))
+    bad = cases.Division(case=d.case, parts=d.parts, blocks=d.blocks, neighbour=d.neighbour,
+                         translation=d.translation, lo=d.lo, transform=d.transform.copy(), axes=d.axes,
+                         flips=d.flips)
+    bad.transform[0, 0] = [2, 1, 3]   # block 0's left face: not the inverse of what block 1 holds
+    with pytest.raises(shock_b200.ShockError):
+        shock_b200.host_multi_geometry(bad)
+    bad.transform[0, 0] = [2, 2, 3]   # not a permutation
+    with pytest.raises(shock_b200.ShockError):
+        shock_b200.host_multi_geometry(bad)
