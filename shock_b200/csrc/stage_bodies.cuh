@@ -2417,8 +2417,9 @@ constexpr size_t weno_smem_bytes()
 // The fused sweep's viscous inputs that its WENO part does not load, asked
 // into L2 when the tile starts (prefetch.global.L2), so that the viscous
 // staging after the WENO arithmetic finds them there instead of in HBM.
-template <int DIM, int ORDER, int D, int TLN>
-__device__ __forceinline__ void visc_l2_prefetch(const Grid &G, const Fields &F, int bx, int by, int bz)
+template <int DIM, int ORDER, int D, int TLN, bool RKF = false>
+__device__ __forceinline__ void visc_l2_prefetch(const Grid &G, const Fields &F, int bx, int by, int bz,
+                                                 const RKFuse &rk = RKFuse{})
 {
     using A = Axes<DIM, D>;
     constexpr int H = ZD<ORDER>::H;
@@ -2448,6 +2449,13 @@ __device__ __forceinline__ void visc_l2_prefetch(const Grid &G, const Fields &F,
             src[n++] = F.m[3 * E + 1] + o;
         }
         for (int q = 0; q < n; q++) asm volatile("prefetch.global.L2 [%0];" ::"l"(src[q]));
+        if (RKF && t >= H && t < H + TLN && pd <= G.g + T.nD - 1)   // the RK update's inputs at the cells
+            for (int c = 0; c < 5; c++) {
+                if (DIM == 2 && c == 3) continue;
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(F.Qs[c] + o));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(rk.in.U[c] + o));
+                asm volatile("prefetch.global.L2 [%0];" ::"l"(rk.Un[c] + o));
+            }
     }
 }
 

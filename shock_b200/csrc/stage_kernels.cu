@@ -128,6 +128,9 @@ struct ViscTile {
 #ifndef SHOCK_FUSED_L2_PREFETCH
 #define SHOCK_FUSED_L2_PREFETCH 1
 #endif
+#ifndef SHOCK_W5_RK_FUSE
+#define SHOCK_W5_RK_FUSE 1
+#endif
 template <int ORDER, bool MIXED>
 struct FuseVisc {
 #ifdef SHOCK_NO_FUSED_SWEEPS
@@ -148,7 +151,7 @@ __global__ void __launch_bounds__(NTHR, (WenoTile<DIM, ORDER, MIXED>::minb))
     // the WENO9 one from 490.3 to 508.9 ms (the longer WENO9 part issues
     // enough of its own memory work, and the prefetches cost it issue slots)
     if (SHOCK_FUSED_L2_PREFETCH && ORDER == 5)
-        visc_l2_prefetch<DIM, ORDER, D, TLW>(G, F, blockIdx.x, blockIdx.y, blockIdx.z);
+        visc_l2_prefetch<DIM, ORDER, D, TLW, RKF>(G, F, blockIdx.x, blockIdx.y, blockIdx.z, rk);
     weno_body<DIM, ORDER, D, MIXED, TLW, false, true>(G, P, first, R, Uu, Vv, Ww, Ee, F, blockIdx.x, blockIdx.y,
                                                       blockIdx.z);
     visc_body<DIM, ORDER, D, MIXED, TLW, true, RKF>(G, P, Uu, Vv, Ww, F, blockIdx.x, blockIdx.y, blockIdx.z, first,
@@ -359,10 +362,13 @@ static void weno_one(const Grid &G, const Phys &P, bool first, const double *con
                                                                                              U[2], U[3], U[4], F);
 }
 
-// The RK update goes into the last fused sweep with WENO9 only: there its
-// loads hide behind the longer WENO arithmetic (the WENO9 zeta sweep took
-// 56 us more at 128^3 against 70 us for the separate update), while the
-// WENO5 sweep lost more (94 us) than the separate update costs.
+// The RK update goes into the last fused sweep.  With WENO9 its loads hide
+// behind the longer WENO arithmetic (the zeta sweep took 56 us more at
+// 128^3 against 70 us for the separate update).  With WENO5 they hide only
+// when the tile asks for them in L2 as it starts (visc_l2_prefetch): without
+// that the sweep grew by more (94 us) than the separate update costs; with
+// it the 512^3 WENO5 step takes 280.0 ms against 284.9 ms with the separate
+// update.
 template <int DIM, int ORDER, int D, bool MIXED>
 static bool weno_visc_one(const Grid &G, const Phys &P, bool first, const double *const U[5], const Fields &F,
                           cudaStream_t s, const RKFuse *rk)
@@ -370,7 +376,7 @@ static bool weno_visc_one(const Grid &G, const Phys &P, bool first, const double
     if constexpr (FuseVisc<ORDER, MIXED>::on) {
         constexpr int WTL = WenoTile<DIM, ORDER, MIXED>::tl;
         constexpr size_t smem = weno_visc_smem_bytes<DIM, ORDER, MIXED, WTL>();
-        constexpr bool LAST = D == DIM - 1 && ORDER == 9;   // sweeps that can end the stage
+        constexpr bool LAST = D == DIM - 1 && (ORDER == 9 || SHOCK_W5_RK_FUSE);   // sweeps that can end the stage
         if (!G.order) {
             cudaFuncSetAttribute(k_weno_visc<DIM, ORDER, D, MIXED, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                  (int)smem);
