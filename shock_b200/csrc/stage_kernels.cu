@@ -68,6 +68,70 @@ __global__ void k_nodal(Grid G, const double *__restrict__ U, const double *__re
     if (o < G.NG) nodal_body<DIM, ORDER, MIXED>(G, o, U, V, W, T, F, with_T);
 }
 
+// 3D nodal derivatives, each thread a column of CI points along i: the i
+// stencil's loads (a plane apart, served from L2) are shared by the column
+// through a register window; the j and k stencils are per point as in
+// nodal_body.  Every sum is nodal_body's, term by term in the same order.
+#ifndef SHOCK_NODAL_COLUMN
+#define SHOCK_NODAL_COLUMN 4
+#endif
+template <int ORDER, bool MIXED, int CI>
+__global__ void __launch_bounds__(256) k_nodal_col(Grid G, const double *__restrict__ U,
+                                                   const double *__restrict__ V, const double *__restrict__ W,
+                                                   const double *__restrict__ T, Fields F, bool with_T)
+{
+    constexpr int H = ZD<ORDER>::H;
+    const long long jk = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+    if (jk >= (long long)G.N[1] * G.N[2]) return;
+    const int j = (int)(jk / G.N[2]), k = (int)(jk % G.N[2]);
+    const int i0 = blockIdx.y * CI;
+    const bool rj = is_real(G, 1, j), rk = is_real(G, 2, k);
+    const double *var[4] = {U, V, W, T};
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+        if (q == 3 && !with_T) continue;
+        const double *a = var[q];
+        double win[CI + 2 * H];
+#pragma unroll
+        for (int m = 0; m < CI + 2 * H; m++) {
+            const int ii = i0 - H + m;
+            win[m] = (ii >= 0 && ii < G.N[0]) ? a[(long long)ii * G.st[0] + jk] : 0.0;
+        }
+#pragma unroll
+        for (int c = 0; c < CI; c++) {
+            const int i = i0 + c;
+            if (i >= G.N[0]) break;
+            const long long o = (long long)i * G.st[0] + jk;
+            double d[3];
+            const bool wr[3] = {is_real(G, 0, i), rj, rk};
+            if (wr[0]) {
+                double acc = 0.0;
+#pragma unroll
+                for (int l = 0; l <= 2 * H; l++) acc += ZD<ORDER>::node(l) * win[c + l];
+                d[0] = acc;
+            }
+            if (wr[1]) {
+                double acc = 0.0;
+#pragma unroll
+                for (int l = 0; l <= 2 * H; l++) acc += ZD<ORDER>::node(l) * a[o + (l - H) * G.st[1]];
+                d[1] = acc;
+            }
+            if (wr[2]) {
+                double acc = 0.0;
+#pragma unroll
+                for (int l = 0; l <= 2 * H; l++) acc += ZD<ORDER>::node(l) * a[o + (l - H)];
+                d[2] = acc;
+            }
+#pragma unroll
+            for (int e = 0; e < 3; e++) {
+                if (!wr[e]) continue;
+                if (MIXED) F.Ndf[3 * q + e][o] = (float)d[e];
+                else F.Nd[3 * q + e][o] = d[e];
+            }
+        }
+    }
+}
+
 #ifndef SHOCK_W9_FP64_TL
 #define SHOCK_W9_FP64_TL 7
 #endif
@@ -327,8 +391,22 @@ void launch_prim(const Grid &G, const Phys &P, const double *const U[5], const F
 void launch_nodal(const Grid &G, const Phys &P, int precision, const double *const U[5], const Fields &F,
                   cudaStream_t s)
 {
-    const unsigned nb = blocks_for(G.NG, 256);
     const bool wT = P.full != 0;   // the full 3D metric also reads the temperature derivatives
+    if (SHOCK_NODAL_COLUMN > 1 && G.dim == 3) {
+        constexpr int CI = SHOCK_NODAL_COLUMN > 1 ? SHOCK_NODAL_COLUMN : 2;
+        const dim3 grid(blocks_for((long long)G.N[1] * G.N[2], 256), (G.N[0] + CI - 1) / CI);
+#define NC(ORD, MIX) k_nodal_col<ORD, MIX, CI><<<grid, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F, wT)
+        if (G.order == 5) {
+            if (precision == SHOCK_MIXED) NC(5, true);
+            else NC(5, false);
+        } else {
+            if (precision == SHOCK_MIXED) NC(9, true);
+            else NC(9, false);
+        }
+#undef NC
+        return;
+    }
+    const unsigned nb = blocks_for(G.NG, 256);
 #define N(DIM, ORD)                                                                                    \
     if (G.dim == DIM && G.order == ORD) {                                                              \
         if (precision == SHOCK_MIXED) k_nodal<DIM, ORD, true><<<nb, 256, 0, s>>>(G, U[1], U[2], U[3], F.T, F, wT); \
