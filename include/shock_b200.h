@@ -427,6 +427,19 @@ int shock_multi_destroy(shock_multi *m);
 /* Host-only set-up of a division's geometry, no device: out13[b] receives
  * block b's 13*NG geometry (as shock_geometry). */
 int shock_host_multi_geometry(const shock_params *p, int nblocks, const shock_block *blocks, double *const *out13);
+/* One rank's row of a SHOCK .sddc division file, the file loadDivision
+ * reads (src/Load.c:191-250; replaces that reader for a host that hands the
+ * whole division to shock_multi_create): the block's sizes from its corners
+ * and, per face, the neighbour (0-based, -1 for none), Translation and
+ * Transform, the Transform's face-axis sign derived from the point ranges as
+ * check_TransformationMatrix does (src/Functions.c:3902-4005).  out's bc is
+ * set to SHOCK_BC_AUTO and its field pointers are left as they were; the
+ * face types and fields come from the grid file.  nranks must match the
+ * file's size (SHOCK_EINVAL otherwise); swap = 1 swaps the byte order, as
+ * SHOCK's SwapDivFile = 2 does.  corners (may be NULL): the 1-based first
+ * point of each axis, then the last. */
+int shock_read_division(const char *path, int dim, int nranks, int rank, int swap, shock_block *out,
+                        long long corners[6]);
 /* Ghosted sizes and first real index of a block (as shock_dims). */
 int shock_multi_dims(const shock_multi *m, int block, int out6[6]);
 /* A block's geometry after set-up (13*NG, as shock_geometry). */

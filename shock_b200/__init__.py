@@ -423,6 +423,28 @@ def _division_blocks(division):
     return arr, keep
 
 
+def read_division(path, dim, nranks, swap=False):
+    """Every rank's row of a SHOCK .sddc division file (shock_read_division):
+    (neighbour (n,6), translation (n,6,3), transform (n,6,3), corners (n,6),
+    sizes (n,3))."""
+    nb = np.zeros((nranks, 6), np.int32)
+    tr = np.zeros((nranks, 6, 3), np.float32)
+    tf = np.zeros((nranks, 6, 3), np.int32)
+    co = np.zeros((nranks, 6), np.int64)
+    sz = np.zeros((nranks, 3), np.int64)
+    for r in range(nranks):
+        B = Block()
+        c6 = (C.c_longlong * 6)()
+        _check(lib().shock_read_division(str(path).encode(), int(dim), int(nranks), r, int(bool(swap)),
+                                         C.byref(B), c6))
+        nb[r] = list(B.neighbour)
+        tr[r] = [list(B.translation[f]) for f in range(6)]
+        tf[r] = [list(B.transform[f]) for f in range(6)]
+        co[r] = list(c6)
+        sz[r] = (B.ni, B.nj, B.nk)
+    return nb, tr, tf, co, sz
+
+
 def host_multi_geometry(division, full_metric=False):
     """Per block geometry (13, ghosted) of a division, built on the host with
     the interfaces exchanged as SHOCK's ranks exchange them (no device)."""

@@ -525,6 +525,44 @@ class Division:
         return np.transpose(a, list(range(lead)) + [lead + c for c in inv])
 
 
+def write_division(division: "Division", path: str, zone: str = "zone"):
+    """Write the division as a SHOCK .sddc file (the layout loadDivision
+    reads, src/Load.c:191-250, little-endian, which SHOCK reads unswapped on
+    x86): per rank the zone name, the block's first and last point in the
+    whole block, and per face
+    the neighbour (1-based, 0 for none), the Transform, this side's and the
+    donor's point ranges (block-local, 1-based), rotation centre and angle
+    (zero) and the Translation."""
+    import struct
+    dim = division.case.dim
+    rows = []
+    for b, bl in enumerate(division.blocks):
+        n = (bl.ni, bl.nj, bl.nk)[:dim]
+        lo = [int(division.lo[b, int(division.axes[b, c])]) for c in range(dim)]
+        row = zone.encode()[:32].ljust(32, b"\0")
+        row += struct.pack(f"<{2 * dim}q", *[lo[c] + 1 for c in range(dim)], *[lo[c] + n[c] for c in range(dim)])
+        for f in range(2 * dim):
+            nb = int(division.neighbour[b, f])
+            t = [int(x) for x in division.transform[b, f][:dim]]
+            rng = [1] * dim + list(n)
+            drng = [0] * (2 * dim)
+            if nb >= 0:
+                a, hi = f // 2, f % 2
+                rng[a] = rng[dim + a] = n[a] if hi else 1
+                dn = (division.blocks[nb].ni, division.blocks[nb].nj, division.blocks[nb].nk)[:dim]
+                da, dhi = abs(t[a]) - 1, hi ^ (1 if t[a] > 0 else 0)
+                drng = [1] * dim + list(dn)
+                drng[da] = drng[dim + da] = dn[da] if dhi else 1
+            else:
+                t = [0] * dim
+                rng = [0] * (2 * dim)
+            row += struct.pack(f"<i{dim}i{2 * dim}q{2 * dim}q9f", nb + 1 if nb >= 0 else 0, *t, *rng, *drng,
+                               0.0, 0.0, 0.0, 0.0, 0.0, 0.0, *[float(x) for x in division.translation[b, f]])
+        rows.append(row)
+    with open(path, "wb") as fh:
+        fh.write(b"".join(rows))
+
+
 def _transforms(neigh, axes, flips, dim):
     """The .sddc Transform of every interface from the blocks' orientations:
     entry c of face f of block b is +-(1 + the axis of the neighbour that b's
