@@ -265,6 +265,57 @@ REF_SAMPLES = {
 }
 
 
+# SHOCK's MPI path on the host cores: a division of a sample block of the
+# same flow and order, one rank per core, SHOCK's own set-up and
+# TransferFlowParameterWithGhosts between the ranks over the forked
+# shared-memory MPI stand-in (oracle/_ref/libshockmpi_*).  Every axis is
+# split in two or more (SHOCK's self-periodic exchange takes one axis per
+# rank at most) and each block keeps nj <= nk (its j-centred zeta stencil).
+MPI_SAMPLES = {
+    "w9": ("decaying_turbulence", {"n": 96, "order": 9}),
+    "w5": ("taylor_green", {"n": 128, "order": 5}),
+}
+MPI_PARTS = {16: (4, 2, 2), 8: (2, 2, 2), 4: (2, 2, 1)}
+
+
+def mpi_reference(workload, steps, warmup):
+    """Cell-stage updates/s of SHOCK's MPI code path on a bounded sample:
+    the division's steps timed as the difference between a run of
+    warmup + steps and one of warmup steps (the same set-up in both).
+    None where the sample does not apply or the build is absent."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from refbind import multirank_available, run_multirank
+    from shock_b200 import cases
+    if workload not in WORKLOAD_INFO or "w" not in workload or workload.startswith("mms"):
+        return None
+    key = "w9" if "w9" in workload else "w5"
+    spec = MPI_SAMPLES[key]
+    order = spec[1]["order"]
+    if not multirank_available(order, 3):
+        return None
+    n = spec[1]["n"]
+    per = 300 * 8 * (n + order + 1) ** 3   # SHOCK's arrays for the whole sample, about 300 doubles a point
+    cores = os.cpu_count() or 1
+    procs = max([p for p in MPI_PARTS if p <= cores] or [0])
+    if not procs or per > 0.5 * _host_avail_bytes():
+        return None
+    case = getattr(cases, spec[0])(**spec[1])
+    d = cases.split(case, MPI_PARTS[procs])
+    t0 = time.perf_counter()
+    run_multirank(d, warmup)
+    t1 = time.perf_counter()
+    run_multirank(d, warmup + steps)
+    t2 = time.perf_counter()
+    dt = max((t2 - t1) - (t1 - t0), 1e-9)
+    v = case.real_points * 4 * steps / dt
+    parts = "x".join(str(x) for x in MPI_PARTS[procs])
+    return {"value": v, "unit": "cell-stage updates/s", "cores": procs, "kind": "reference", "seconds": dt,
+            "sample": f"SHOCK's MPI code path (oracle/_ref/libshockmpi_*: its own set-up and halo exchange between "
+                      f"ranks over the forked shared-memory MPI stand-in), a {n}^3 block of the same flow and order "
+                      f"divided {parts} ({procs} ranks, one per core), {steps} RK4 steps timed as the difference "
+                      f"of runs of {warmup + steps} and {warmup} steps ({dt:.1f} s)"}
+
+
 def ref_sample(workload):
     spec, what = REF_SAMPLES[workload]
     kw = spec[1]
@@ -344,16 +395,24 @@ def run_reference(args, rank, world):
     spec, pts, what = ref_sample(args.workload)
     procs = ref_procs(pts, order)
     v, t, _ = reference_throughput(spec, args.steps, args.warmup, procs)
+    replicas = {"value": v, "unit": "cell-stage updates/s", "cores": procs, "kind": "reference",
+                "sample": f"{procs} single-block processes, each {args.warmup} warm-up and {args.steps} "
+                          f"timed RK4 steps of {what}, SHOCK's own C code (oracle/_ref); slowest "
+                          f"process {t:.1f} s; a step of the line = one RK4 step of every process"}
+    # SHOCK's MPI path (a division with its halo exchange) where the sample
+    # applies: the line's value; the single-block replicas beside it
+    mpi = mpi_reference(args.workload, args.steps, args.warmup)
+    base = mpi if mpi is not None else replicas
+    v = base["value"]
+    ms = (t if mpi is None else mpi["seconds"]) * 1e3 / args.steps
     line = {
         "metric": "cell-stage updates/s", "value": v, "unit": "cell-stage updates/s", "impl": "reference",
         "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": t * 1e3 / args.steps, "higher_is_better": True, "scaling": "weak",
+        "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": bench_config(args.workload, world),
-        "cpu_baseline": {"value": v, "unit": "cell-stage updates/s", "cores": procs, "kind": "reference",
-                         "sample": f"{procs} single-block processes, each {args.warmup} warm-up and {args.steps} "
-                                   f"timed RK4 steps of {what}, SHOCK's own C code (oracle/_ref); slowest "
-                                   f"process {t:.1f} s; a step of the line = one RK4 step of every process"},
+        "cpu_baseline": base,
+        "single_block_replicas": replicas if mpi is not None else None,
         "e2e": {"value": v, "unit": "cell-stage updates/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -586,12 +645,17 @@ def cpu_baseline_sample(workload, case):
     from refbind import ref_available
     if not ref_available(case.order, case.dim):
         return None
+    mpi = mpi_reference(workload, CPU_BASELINE_STEPS, 1)
     spec, pts, what = ref_sample(workload)
     procs = ref_procs(pts, case.order)
     v, tmax, _ = reference_throughput(spec, CPU_BASELINE_STEPS, 1, procs)
-    return {"value": v, "unit": "cell-stage updates/s", "cores": procs, "kind": "reference",
-            "sample": f"{procs} single-block processes x {CPU_BASELINE_STEPS} timed RK4 steps (after 1 warm-up "
-                      f"step) of {what}, SHOCK's own C code (oracle/_ref); {tmax:.1f} s"}
+    replicas = {"value": v, "unit": "cell-stage updates/s", "cores": procs, "kind": "reference",
+                "sample": f"{procs} single-block processes x {CPU_BASELINE_STEPS} timed RK4 steps (after 1 warm-up "
+                          f"step) of {what}, SHOCK's own C code (oracle/_ref); {tmax:.1f} s"}
+    if mpi is None:
+        return replicas
+    mpi["single_block_replicas"] = replicas
+    return mpi
 
 
 CPU_BASELINE_STEPS = 3
