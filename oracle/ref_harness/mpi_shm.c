@@ -20,6 +20,9 @@
  *                   the receiver polls, and makes the runs reproducible;
  *   collectives     Barrier (sense-reversing counter), Allgather, Reduce
  *                   (SUM, MAX), Bcast through a shared staging area;
+ *   MPI-IO          read-only, independent: a file is a POSIX descriptor,
+ *                   the view a byte displacement (what loadDivision,
+ *                   src/Load.c:191-250, uses to read its rank's row);
  *   waits           every spin gives up after SHM_WAIT_S seconds and aborts
  *                   the whole job (a rank that never arrives is an error of
  *                   the test set-up, not something to wait out).
@@ -31,7 +34,9 @@
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
+#include <fcntl.h>
 #include <sys/mman.h>
+#include <sys/stat.h>
 #include <sys/wait.h>
 #include <time.h>
 #include <unistd.h>
@@ -318,6 +323,68 @@ int MPI_Type_create_subarray(int a, const int *b, const int *c, const int *d, in
 { (void)a; (void)b; (void)c; (void)d; (void)e; *g = f; return 0; }
 int MPI_Type_commit(MPI_Datatype *t) { (void)t; return 0; }
 int MPI_Type_size(MPI_Datatype t, int *s) { *s = (int)dtype_size(t); return 0; }
+
+#define SHM_FILES 8
+static struct { int open, fd; MPI_Offset pos; } g_file[SHM_FILES];
+
+static int file_slot(MPI_File fh) { return fh >= 0 && fh < SHM_FILES && g_file[fh].open ? fh : -1; }
+
+int MPI_File_open(MPI_Comm c, const char *name, int amode, MPI_Info info, MPI_File *fh)
+{
+    (void)c; (void)info;
+    if (amode != MPI_MODE_RDONLY) return 1;
+    for (int i = 0; i < SHM_FILES; i++)
+        if (!g_file[i].open) {
+            const int fd = open(name, O_RDONLY);
+            if (fd < 0) return 1;
+            g_file[i].open = 1;
+            g_file[i].fd = fd;
+            g_file[i].pos = 0;
+            *fh = i;
+            return 0;
+        }
+    return 1;
+}
+
+int MPI_File_get_size(MPI_File fh, MPI_Offset *size)
+{
+    struct stat st;
+    const int i = file_slot(fh);
+    if (i < 0 || fstat(g_file[i].fd, &st)) return 1;
+    *size = (MPI_Offset)st.st_size;
+    return 0;
+}
+
+int MPI_File_set_view(MPI_File fh, MPI_Offset disp, MPI_Datatype et, MPI_Datatype ft, const char *rep, MPI_Info info)
+{
+    (void)info;
+    const int i = file_slot(fh);
+    if (i < 0 || et != MPI_CHAR || ft != MPI_CHAR || strcmp(rep, "native")) return 1;
+    g_file[i].pos = disp;
+    return 0;
+}
+
+int MPI_File_read(MPI_File fh, void *buf, int n, MPI_Datatype t, MPI_Status *st)
+{
+    (void)st;
+    const int i = file_slot(fh);
+    const size_t bytes = (size_t)n * dtype_size(t);
+    if (i < 0) return 1;
+    const ssize_t got = pread(g_file[i].fd, buf, bytes, (off_t)g_file[i].pos);
+    if (got < 0 || (size_t)got != bytes) return 1;
+    g_file[i].pos += got;
+    return 0;
+}
+
+int MPI_File_close(MPI_File *fh)
+{
+    const int i = file_slot(*fh);
+    if (i < 0) return 1;
+    close(g_file[i].fd);
+    g_file[i].open = 0;
+    *fh = -1;
+    return 0;
+}
 
 /*
  * Run body(rank, arg) on nranks forked processes sharing the mailboxes

@@ -538,8 +538,20 @@ void ref_dropin_destroy(void)
  * ranges of the two touching faces in each block's own 1-based indices and
  * the float32 Translation the receiving side adds -- and SHOCK's own
  * TransferMeshParameter / TransferFlowParameterWithGhosts exchanging them.
+ * Or, given a .sddc file, each rank reads its interfaces with SHOCK's own
+ * loadDivision (ref_harness/load_division.c) and takes them into its
+ * configuration as loadFile does (src/Load.c:355-400).
  */
 int shm_run(int nranks, size_t slot_bytes, int (*body)(int rank, void *arg), void *arg);
+
+typedef struct {
+    int neighbour;
+    int transform[3];
+    long long range[6], drange[6];
+    float rc[3], ra[3], tr[3];
+} ref_iface;
+int ref_load_division(struct strct_configuration *pc, const char *path, int rank, int nranks, long long corners[6],
+                      ref_iface faces[6]);
 
 typedef struct {
     int nblocks;
@@ -552,6 +564,8 @@ typedef struct {
     int nsteps;
     double *out;                  /* shared: per block 13*NG geometry, 5*NG rhs, 9*NG state */
     const size_t *out_off;        /* [nblocks] offset of each block's output */
+    const char *division;         /* a .sddc file to read the interfaces from, or NULL */
+    int swap;                     /* SHOCK's SwapDivFile for that file: 0 auto, 1 never, 2 always */
 } mr_job;
 
 static const mr_job *g_job;
@@ -561,10 +575,66 @@ static float *mr_tr[6];
 static int *mr_tf[6];
 static cgsize_t *mr_rng[6], *mr_drng[6];
 static float *mr_rc[6], *mr_ra[6];
+static ref_iface mr_file[6];
+
+/* The interfaces of this rank's row of the division file, as loadFile takes
+ * them into the configuration (src/Load.c:355-400): an index per face that
+ * has a neighbour, in face order, and the neighbour's rank one less than the
+ * file's. */
+static void mr_file_interfaces(void)
+{
+    const int dim = MESHDIMENSIONS;
+    int *side[6] = {&cfg.InterfaceNeighbourLeft, &cfg.InterfaceNeighbourRight, &cfg.InterfaceNeighbourBottom,
+                    &cfg.InterfaceNeighbourTop, &cfg.InterfaceNeighbourBehind, &cfg.InterfaceNeighbourInFront};
+    static int ranks[6];
+    static int *tf[6];
+    static cgsize_t *rng[6], *drng[6];
+    static float *tr[6], *rc[6], *ra[6];
+    int ii = 0;
+    for (int f = 0; f < 6; f++) {
+        const ref_iface *x = &mr_file[f];
+        if (f >= 2 * dim || !x->neighbour) { *side[f] = NO_NEIGHBOUR; continue; }
+        tf[ii] = mr_tf[ii];
+        rng[ii] = mr_rng[ii];
+        drng[ii] = mr_drng[ii];
+        tr[ii] = mr_tr[ii];
+        rc[ii] = mr_rc[ii];
+        ra[ii] = mr_ra[ii];
+        for (int c = 0; c < dim; c++) {
+            tf[ii][c] = x->transform[c];
+            rng[ii][c] = x->range[c];
+            rng[ii][dim + c] = x->range[3 + c];
+            drng[ii][c] = x->drange[c];
+            drng[ii][dim + c] = x->drange[3 + c];
+        }
+        for (int c = 0; c < 3; c++) {
+            tr[ii][c] = x->tr[c];
+            rc[ii][c] = x->rc[c];
+            ra[ii][c] = x->ra[c];
+        }
+        ranks[ii] = x->neighbour - 1;
+        *side[f] = ii++;
+    }
+    cfg.NumberInterfaces = ii;
+    cfg.MPI_rankNeighbours = ranks;
+    cfg.TransformMatrixOfInterface = tf;
+    cfg.RangeOfInterface = rng;
+    cfg.DonorRangeOfInterface = drng;
+    cfg.Translation = tr;
+    cfg.RotationCenter = rc;
+    cfg.RotationAngle = ra;
+    cfg.MPI_rank = g_rank_blk;
+    cfg.MPI_size = g_job->nblocks;
+    for (int c = 0; c < MESHDIMENSIONS; c++) cfg.offset[c] = 0;
+}
 
 static void mr_interfaces(void)
 {
     const int b = g_rank_blk, dim = MESHDIMENSIONS;
+    if (g_job->division) {
+        mr_file_interfaces();
+        return;
+    }
     const ref_params *p = &g_job->blk[b];
     int *side[6] = {&cfg.InterfaceNeighbourLeft, &cfg.InterfaceNeighbourRight, &cfg.InterfaceNeighbourBottom,
                     &cfg.InterfaceNeighbourTop, &cfg.InterfaceNeighbourBehind, &cfg.InterfaceNeighbourInFront};
@@ -631,6 +701,16 @@ static int mr_body(int rank, void *arg)
         mr_rc[i] = calloc(3, sizeof(float));
         mr_ra[i] = calloc(3, sizeof(float));
     }
+    if (g_job->division) {
+        /* the row's block must be the block this rank is given */
+        const ref_params *p = &g_job->blk[rank];
+        const long long n[3] = {p->ni, p->nj, MESHDIMENSIONS == 3 ? p->nk : 1};
+        long long corners[6];
+        cfg.flag_swapDivisionFile = g_job->swap;
+        ref_load_division(&cfg, g_job->division, rank, g_job->nblocks, corners, mr_file);
+        for (int a = 0; a < 3; a++)
+            if (corners[3 + a] - corners[a] + 1 != n[a]) return 1;
+    }
     g_iface_hook = mr_interfaces;
     const double *const *in = g_job->in + 8 * rank;
     if (ref_init(&g_job->blk[rank], in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7])) return 1;
@@ -643,6 +723,10 @@ static int mr_body(int rank, void *arg)
     return 0;
 }
 
+int refmpi_run_file(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const int *tfm,
+                    const double *const *in, int nrhs, int nsteps, double *out, const size_t *out_off,
+                    size_t out_len, size_t slot_bytes, const char *division, int swap);
+
 /* Runs the division on nblocks processes; out receives, per block at
  * out_off[b], the geometry (13*NG), one right-hand side at the initial state
  * (5*NG, when nrhs) and the state after nsteps steps (9*NG: rho,u,v,w,e,p,
@@ -651,9 +735,20 @@ int refmpi_run(int nblocks, const ref_params *blk, const int *neigh, const float
                const double *const *in, int nrhs, int nsteps, double *out, const size_t *out_off, size_t out_len,
                size_t slot_bytes)
 {
+    return refmpi_run_file(nblocks, blk, neigh, trans, tfm, in, nrhs, nsteps, out, out_off, out_len, slot_bytes,
+                           NULL, 0);
+}
+
+/* The same with the interfaces read from the division file `division` by
+ * SHOCK's loadDivision (neigh, trans and tfm unused), swap as SHOCK's
+ * SwapDivFile option. */
+int refmpi_run_file(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const int *tfm,
+                    const double *const *in, int nrhs, int nsteps, double *out, const size_t *out_off,
+                    size_t out_len, size_t slot_bytes, const char *division, int swap)
+{
     double *shared = mmap(NULL, out_len * sizeof(double), PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
     if (shared == MAP_FAILED) return -1;
-    mr_job job = {nblocks, blk, neigh, trans, tfm, in, nrhs, nsteps, shared, out_off};
+    mr_job job = {nblocks, blk, neigh, trans, tfm, in, nrhs, nsteps, shared, out_off, division, swap};
     int rc = shm_run(nblocks, slot_bytes, mr_body, &job);
     memcpy(out, shared, out_len * sizeof(double));
     munmap(shared, out_len * sizeof(double));

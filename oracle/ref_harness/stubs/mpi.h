@@ -14,6 +14,7 @@ typedef int MPI_Datatype;
 typedef int MPI_Op;
 typedef int MPI_Request;
 typedef int MPI_File;
+typedef long long MPI_Offset;
 typedef struct { int MPI_SOURCE, MPI_TAG, MPI_ERROR; } MPI_Status;
 
 #define MPI_COMM_WORLD 0
@@ -60,5 +61,12 @@ int MPI_Type_create_subarray(int, const int *, const int *, const int *, int,
                              MPI_Datatype, MPI_Datatype *);
 int MPI_Type_commit(MPI_Datatype *);
 int MPI_Type_size(MPI_Datatype, int *);
+/* MPI-IO, read-only: what loadDivision (src/Load.c:191-250) calls; defined
+   in mpi_shm.c only. */
+int MPI_File_open(MPI_Comm, const char *, int, MPI_Info, MPI_File *);
+int MPI_File_get_size(MPI_File, MPI_Offset *);
+int MPI_File_set_view(MPI_File, MPI_Offset, MPI_Datatype, MPI_Datatype, const char *, MPI_Info);
+int MPI_File_read(MPI_File, void *, int, MPI_Datatype, MPI_Status *);
+int MPI_File_close(MPI_File *);
 
 #endif

@@ -338,11 +338,12 @@ def _ref_params(case) -> "RefParams":
     return p
 
 
-def _multirank_worker(division, nsteps, rhs, extended, full=False):
+def _multirank_worker(division, nsteps, rhs, extended, full=False, division_file=None, swap=0):
     case = division.case
     tag = ("full" if full else "") + ("80" if extended else "")
     lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockmpi{tag}_w{case.order}_{case.dim}d.so"), mode=os.RTLD_LOCAL)
     lib.refmpi_run.restype = C.c_int
+    lib.refmpi_run_file.restype = C.c_int
     nb = len(division.blocks)
     g2 = case.order + 1
     shapes = [(b.ni + g2, b.nj + g2, (b.nk + g2) if case.dim == 3 else 1) for b in division.blocks]
@@ -361,10 +362,12 @@ def _multirank_worker(division, nsteps, rhs, extended, full=False):
     out = np.zeros(total)
     face = max(max(s[0] * s[1], s[1] * s[2], s[0] * s[2]) for s in shapes)
     slot = 13 * (g2 // 2) * face * 16       # long double in the 80-bit build
-    rc = lib.refmpi_run(C.c_int(nb), params, neigh.ctypes.data_as(C.POINTER(C.c_int)),
-                        trans.ctypes.data_as(C.POINTER(C.c_float)), tfm.ctypes.data_as(C.POINTER(C.c_int)), ptrs,
-                        C.c_int(int(rhs)), C.c_int(nsteps),
-                        _ptr(out), off.ctypes.data_as(C.POINTER(C.c_size_t)), C.c_size_t(total), C.c_size_t(slot))
+    path = None if division_file is None else os.fsencode(str(division_file))
+    rc = lib.refmpi_run_file(C.c_int(nb), params, neigh.ctypes.data_as(C.POINTER(C.c_int)),
+                             trans.ctypes.data_as(C.POINTER(C.c_float)), tfm.ctypes.data_as(C.POINTER(C.c_int)), ptrs,
+                             C.c_int(int(rhs)), C.c_int(nsteps),
+                             _ptr(out), off.ctypes.data_as(C.POINTER(C.c_size_t)), C.c_size_t(total),
+                             C.c_size_t(slot), C.c_char_p(path), C.c_int(swap))
     if rc != 0:
         raise RuntimeError(f"multi-rank reference run failed ({rc})")
     res = []
@@ -376,12 +379,18 @@ def _multirank_worker(division, nsteps, rhs, extended, full=False):
     return res
 
 
-def run_multirank(division, nsteps: int, rhs: bool = False, extended: bool = False, full: bool = False):
+def run_multirank(division, nsteps: int, rhs: bool = False, extended: bool = False, full: bool = False,
+                  division_file=None, swap: int = 0):
     """Per block: geometry (13, ghosted), one right-hand side at the initial
     state (5, when rhs) and the state after nsteps steps (9: rho,u,v,w,e,p,
     T,c,mue) of SHOCK's own multi-rank run of the division (extended: the
-    80-bit build; full: the build with the full 3D metric)."""
+    80-bit build; full: the build with the full 3D metric).  With
+    division_file, each rank reads its interfaces from that .sddc file with
+    SHOCK's own loadDivision (src/Load.c:191-250; swap: its SwapDivFile
+    option, 0 auto, 1 never, 2 always) instead of from the division's
+    neighbour, translation and transform tables; the blocks' sizes and
+    fields still come from the division."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
-        return pool.apply(_multirank_worker, (division, nsteps, rhs, extended, full))
+        return pool.apply(_multirank_worker, (division, nsteps, rhs, extended, full, division_file, swap))

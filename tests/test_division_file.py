@@ -2,14 +2,19 @@
 cases.write_division in the layout loadDivision reads, read back by the
 library's shock_read_division, including the Transform sign SHOCK derives
 from the point ranges (check_TransformationMatrix, src/Functions.c:3902-4005),
-the byte-swapped form (SwapDivFile) and a wrong rank count."""
+the byte-swapped form (SwapDivFile) and a wrong rank count; and the same
+files read by SHOCK itself: its ranks load their rows with its own
+loadDivision, take them in as loadFile does and set up their geometry, bit
+for bit the geometry the library sets up from its reading of the file."""
 import struct
 
 import numpy as np
 import pytest
 
 import shock_b200
+from refbind import multirank_available, run_multirank
 from shock_b200 import cases
+from test_multiblock_host import DIVISIONS, division as named_division
 
 
 def _division(rotated):
@@ -88,6 +93,73 @@ def test_byte_swapped_division_file(tmp_path):
     nb, tr, tf, _, _ = shock_b200.read_division(path, 3, len(d.blocks), swap=True)
     assert np.array_equal(nb, d.neighbour) and np.array_equal(tr, d.translation)
     assert np.array_equal(tf, np.where(d.neighbour[..., None] >= 0, d.transform, 0))
+
+
+def _read_back(d, path, swap=False):
+    nb, tr, tf, _, _ = shock_b200.read_division(path, d.case.dim, len(d.blocks), swap=swap)
+    return cases.Division(case=d.case, parts=d.parts, blocks=d.blocks, neighbour=nb, translation=tr, lo=d.lo,
+                          transform=tf, axes=d.axes, flips=d.flips)
+
+
+def _flip_face_axis_entries(d, path):
+    """Negate every interface's Transform entry of its own face axis in the
+    file, as grid tools write it; returns how many were negated."""
+    dim = d.case.dim
+    raw = bytearray(path.read_bytes())
+    row = len(raw) // len(d.blocks)
+    ifblock = 4 + dim * 4 + 4 * dim * 8 + 9 * 4
+    flipped = 0
+    for b in range(len(d.blocks)):
+        for f in range(2 * dim):
+            off = b * row + 32 + 2 * dim * 8 + f * ifblock + 4 + 4 * (f // 2)
+            (v,) = struct.unpack_from("<i", raw, off)
+            if v:
+                struct.pack_into("<i", raw, off, -v)
+                flipped += 1
+    path.write_bytes(bytes(raw))
+    return flipped
+
+
+def _swap_file(d, path):
+    """The file with every number byte-swapped (a big-endian writer)."""
+    dim = d.case.dim
+    raw = path.read_bytes()
+    row = len(raw) // len(d.blocks)
+    sizes = [4] * (1 + dim) + [8] * (4 * dim) + [4] * 9
+    out = bytearray()
+    for b in range(len(d.blocks)):
+        r = raw[b * row:(b + 1) * row]
+        out += r[:32]
+        out += b"".join(r[32 + 8 * i:40 + 8 * i][::-1] for i in range(2 * dim))
+        pos = 32 + 16 * dim
+        for f in range(2 * dim):
+            for sz in sizes:
+                out += r[pos:pos + sz][::-1]
+                pos += sz
+    path.write_bytes(bytes(out))
+
+
+@pytest.mark.parametrize("form", ["as_written", "face_axis_signs_flipped", "byte_swapped"])
+@pytest.mark.parametrize("name", sorted(DIVISIONS))
+def test_shock_reads_the_same_division(tmp_path, name, form):
+    case, d, full = named_division(name)
+    if not multirank_available(case.order, case.dim, full=full):
+        pytest.skip("multi-rank reference build absent (make -C oracle with the reference sources)")
+    if form != "as_written" and "rotated" not in name:
+        pytest.skip("the altered forms run on the rotated divisions")
+    path = tmp_path / "div.sddc"
+    cases.write_division(d, str(path))
+    swap = False
+    if form == "face_axis_signs_flipped":
+        assert _flip_face_axis_entries(d, path) == int((d.neighbour[:, :2 * case.dim] >= 0).sum())
+    elif form == "byte_swapped":
+        _swap_file(d, path)
+        swap = True
+    got = shock_b200.host_multi_geometry(_read_back(d, path, swap), full_metric=full)
+    # SHOCK's SwapDivFile: 2 swaps always, 0 decides by the host's byte order
+    ref = run_multirank(d, 0, full=full, division_file=path, swap=2 if swap else 0)
+    for b in range(len(d.blocks)):
+        assert np.array_equal(got[b], ref[b]["geometry"]), (name, form, b)
 
 
 def test_division_file_size_checked(tmp_path):
