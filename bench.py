@@ -302,14 +302,17 @@ def mpi_reference(workload, steps, warmup):
     case = getattr(cases, spec[0])(**spec[1])
     d = cases.split(case, MPI_PARTS[procs])
     t0 = time.perf_counter()
-    run_multirank(d, warmup)
+    r1 = run_multirank(d, warmup)
     t1 = time.perf_counter()
-    run_multirank(d, warmup + steps)
+    r2 = run_multirank(d, warmup + steps)
     t2 = time.perf_counter()
     dt = max((t2 - t1) - (t1 - t0), 1e-9)
     v = case.real_points * 4 * steps / dt
+    # SHOCK's own comm_time over the timed steps, the slowest rank
+    comm = max(b2["comm_time"] - b1["comm_time"] for b1, b2 in zip(r1, r2))
     parts = "x".join(str(x) for x in MPI_PARTS[procs])
     return {"value": v, "unit": "cell-stage updates/s", "cores": procs, "kind": "reference", "seconds": dt,
+            "comm_seconds": comm, "comm_share": comm / dt,
             "sample": f"SHOCK's MPI code path (oracle/_ref/libshockmpi_*: its own set-up and halo exchange between "
                       f"ranks over the forked shared-memory MPI stand-in), a {n}^3 block of the same flow and order "
                       f"divided {parts} ({procs} ranks, one per core), {steps} RK4 steps timed as the difference "

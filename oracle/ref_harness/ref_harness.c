@@ -566,6 +566,7 @@ typedef struct {
     const size_t *out_off;        /* [nblocks] offset of each block's output */
     const char *division;         /* a .sddc file to read the interfaces from, or NULL */
     int swap;                     /* SHOCK's SwapDivFile for that file: 0 auto, 1 never, 2 always */
+    double *comm;                 /* shared: per rank SHOCK's comm_time after the steps */
 } mr_job;
 
 static const mr_job *g_job;
@@ -718,14 +719,16 @@ static int mr_body(int rank, void *arg)
     double *o = g_job->out + g_job->out_off[rank];
     ref_get_geom(o);
     if (g_job->nrhs) ref_rhs(o + 13 * (size_t)n);
+    cfg.comm_time = 0.0;          /* count the steps' exchanges only */
     ref_steps(g_job->nsteps);
     ref_get_state(o + 18 * (size_t)n, 0);
+    g_job->comm[rank] = cfg.comm_time;
     return 0;
 }
 
 int refmpi_run_file(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const int *tfm,
                     const double *const *in, int nrhs, int nsteps, double *out, const size_t *out_off,
-                    size_t out_len, size_t slot_bytes, const char *division, int swap);
+                    size_t out_len, size_t slot_bytes, const char *division, int swap, double *comm_time);
 
 /* Runs the division on nblocks processes; out receives, per block at
  * out_off[b], the geometry (13*NG), one right-hand side at the initial state
@@ -736,22 +739,28 @@ int refmpi_run(int nblocks, const ref_params *blk, const int *neigh, const float
                size_t slot_bytes)
 {
     return refmpi_run_file(nblocks, blk, neigh, trans, tfm, in, nrhs, nsteps, out, out_off, out_len, slot_bytes,
-                           NULL, 0);
+                           NULL, 0, NULL);
 }
 
 /* The same with the interfaces read from the division file `division` by
- * SHOCK's loadDivision (neigh, trans and tfm unused), swap as SHOCK's
- * SwapDivFile option. */
+ * SHOCK's loadDivision when it is not NULL (neigh, trans and tfm unused),
+ * swap as SHOCK's SwapDivFile option; comm_time (when not NULL) receives
+ * per rank the seconds SHOCK counted in its halo exchange during the steps
+ * (its comm_time, src/Functions.c:3683, which includes waiting for the
+ * neighbours' messages). */
 int refmpi_run_file(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const int *tfm,
                     const double *const *in, int nrhs, int nsteps, double *out, const size_t *out_off,
-                    size_t out_len, size_t slot_bytes, const char *division, int swap)
+                    size_t out_len, size_t slot_bytes, const char *division, int swap, double *comm_time)
 {
-    double *shared = mmap(NULL, out_len * sizeof(double), PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
+    const size_t len = out_len + (size_t)nblocks;
+    double *shared = mmap(NULL, len * sizeof(double), PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
     if (shared == MAP_FAILED) return -1;
-    mr_job job = {nblocks, blk, neigh, trans, tfm, in, nrhs, nsteps, shared, out_off, division, swap};
+    mr_job job = {nblocks, blk, neigh, trans, tfm, in, nrhs, nsteps, shared, out_off, division, swap,
+                  shared + out_len};
     int rc = shm_run(nblocks, slot_bytes, mr_body, &job);
     memcpy(out, shared, out_len * sizeof(double));
-    munmap(shared, out_len * sizeof(double));
+    if (comm_time) memcpy(comm_time, shared + out_len, (size_t)nblocks * sizeof(double));
+    munmap(shared, len * sizeof(double));
     return rc;
 }
 #endif

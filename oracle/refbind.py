@@ -363,11 +363,12 @@ def _multirank_worker(division, nsteps, rhs, extended, full=False, division_file
     face = max(max(s[0] * s[1], s[1] * s[2], s[0] * s[2]) for s in shapes)
     slot = 13 * (g2 // 2) * face * 16       # long double in the 80-bit build
     path = None if division_file is None else os.fsencode(str(division_file))
+    comm = np.zeros(nb)
     rc = lib.refmpi_run_file(C.c_int(nb), params, neigh.ctypes.data_as(C.POINTER(C.c_int)),
                              trans.ctypes.data_as(C.POINTER(C.c_float)), tfm.ctypes.data_as(C.POINTER(C.c_int)), ptrs,
                              C.c_int(int(rhs)), C.c_int(nsteps),
                              _ptr(out), off.ctypes.data_as(C.POINTER(C.c_size_t)), C.c_size_t(total),
-                             C.c_size_t(slot), C.c_char_p(path), C.c_int(swap))
+                             C.c_size_t(slot), C.c_char_p(path), C.c_int(swap), _ptr(comm))
     if rc != 0:
         raise RuntimeError(f"multi-rank reference run failed ({rc})")
     res = []
@@ -375,7 +376,8 @@ def _multirank_worker(division, nsteps, rhs, extended, full=False, division_file
         o, n = int(off[b]), ng[b]
         res.append({"geometry": out[o:o + 13 * n].reshape((13,) + shapes[b]),
                     "rhs": out[o + 13 * n:o + 18 * n].reshape((5,) + shapes[b]),
-                    "state": out[o + 18 * n:o + 27 * n].reshape((9,) + shapes[b])})
+                    "state": out[o + 18 * n:o + 27 * n].reshape((9,) + shapes[b]),
+                    "comm_time": float(comm[b])})
     return res
 
 
@@ -383,7 +385,9 @@ def run_multirank(division, nsteps: int, rhs: bool = False, extended: bool = Fal
                   division_file=None, swap: int = 0):
     """Per block: geometry (13, ghosted), one right-hand side at the initial
     state (5, when rhs) and the state after nsteps steps (9: rho,u,v,w,e,p,
-    T,c,mue) of SHOCK's own multi-rank run of the division (extended: the
+    T,c,mue) of SHOCK's own multi-rank run of the division, and the seconds
+    SHOCK counted in its halo exchange during the steps (comm_time, waits
+    for the neighbours included) (extended: the
     80-bit build; full: the build with the full 3D metric).  With
     division_file, each rank reads its interfaces from that .sddc file with
     SHOCK's own loadDivision (src/Load.c:191-250; swap: its SwapDivFile
