@@ -216,7 +216,7 @@ def test_mixed_precision_l2(order, n, nsteps, parity):
     b.steps(nsteps)
     sa, sb = real(c, a.state()), real(c, b.state())
     err = _conserved_l2(sb, sa)
-    # rho*w is identically zero for this flow; judge it against |rho u|
+    # rho*w is identically zero for this flow; measure it against |rho u|
     scale = np.sqrt(np.mean((sa[0] * sa[1]) ** 2))
     err[3] = np.sqrt(np.mean((sb[0] * sb[3] - sa[0] * sa[3]) ** 2)) / scale
     parity("mixed_tgv", c.name, f"mixed vs FP64 L2, {nsteps} steps", err, 1e-6)
