@@ -51,3 +51,18 @@ int ref_load_division(struct strct_configuration *pc, const char *path, int rank
         }
     return ni;
 }
+
+/* The same for a caller without a configuration: one rank's row, SHOCK's
+ * SwapDivFile option as swap (0 auto, 1 never, 2 always).  Returns the
+ * number of interfaces.  (loadDivision ends the process when the file's
+ * size is not nranks rows.) */
+int ref_load_division_row(const char *path, int rank, int nranks, int swap, long long corners[6],
+                          ref_iface faces[6])
+{
+    struct strct_configuration *pc = calloc(1, sizeof *pc);
+    if (!pc) return -1;
+    pc->flag_swapDivisionFile = swap;
+    const int ni = ref_load_division(pc, path, rank, nranks, corners, faces);
+    free(pc);
+    return ni;
+}

@@ -398,3 +398,34 @@ def run_multirank(division, nsteps: int, rhs: bool = False, extended: bool = Fal
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
         return pool.apply(_multirank_worker, (division, nsteps, rhs, extended, full, division_file, swap))
+
+
+class RefIface(C.Structure):
+    """One face's interface as SHOCK's loadDivision reads it
+    (ref_harness/load_division.c)."""
+    _fields_ = [("neighbour", C.c_int), ("transform", C.c_int * 3), ("range", C.c_longlong * 6),
+                ("drange", C.c_longlong * 6), ("rc", C.c_float * 3), ("ra", C.c_float * 3), ("tr", C.c_float * 3)]
+
+
+def load_division_row(path, dim: int, rank: int, nranks: int, swap: int = 0):
+    """One rank's row of a .sddc file as SHOCK's own loadDivision reads it
+    (src/Load.c:191-250; swap: its SwapDivFile option): (corners (6,),
+    per face (neighbour 1-based or 0, transform (3,), range (2*dim,), drange
+    (2*dim,), translation (3,))).  In process: the file's size must be nranks rows,
+    which the caller checks first (loadDivision ends the process otherwise)."""
+    lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockmpi_w5_{dim}d.so"), mode=os.RTLD_LOCAL)
+    lib.ref_load_division_row.restype = C.c_int
+    corners = (C.c_longlong * 6)()
+    faces = (RefIface * 6)()
+    ni = lib.ref_load_division_row(os.fsencode(str(path)), C.c_int(rank), C.c_int(nranks), C.c_int(swap), corners,
+                                   faces)
+    if ni < 0:
+        raise RuntimeError("ref_load_division_row failed")
+    out = []
+    for f in range(2 * dim):
+        x = faces[f]
+        # ranges as SHOCK holds them: the first point per axis, then the last
+        rng = np.array(x.range[:dim] + x.range[3:3 + dim])
+        drng = np.array(x.drange[:dim] + x.drange[3:3 + dim])
+        out.append((x.neighbour, np.array(x.transform[:]), rng, drng, np.array(x.tr[:], dtype=np.float32)))
+    return np.array(corners[:]), out

@@ -563,6 +563,39 @@ def write_division(division: "Division", path: str, zone: str = "zone"):
         fh.write(b"".join(rows))
 
 
+def load_division(case: Case, path: str, nranks: int, swap: bool = False) -> "Division":
+    """The division a SHOCK .sddc file describes over the one zone ``case``
+    holds (its grid and fields, all rows naming that zone), as SHOCK's ranks
+    take it (src/Load.c:191-250, 355-400): rank r's block is the case's real
+    points between the row's corners, its neighbours, Translations and
+    Transforms are the row's (read by the library's shock_read_division), and
+    a face without a neighbour keeps the case's face type.  The zone's axes
+    must be every block's axes (Transforms of +-1, +-2, +-3 in place, as
+    TOOLS/generatedivfile writes them)."""
+    from . import read_division
+    nb, tr, tf, co, sz = read_division(path, case.dim, nranks, swap=swap)
+    n = (case.ni, case.nj, case.nk if case.dim == 3 else 1)
+    lo = co[:, :3] - 1
+    blocks = []
+    for r in range(nranks):
+        sl = tuple(slice(int(lo[r, a]), int(co[r, 3 + a])) for a in range(3))
+        if any(sl[a].start < 0 or sl[a].stop > n[a] for a in range(3)):
+            raise ValueError(f"rank {r}: corners {co[r].tolist()} outside the {n} zone")
+        bc = [0] * 6
+        for f in range(2 * case.dim):
+            if nb[r, f] < 0:
+                bc[f] = case.bc[f]
+            elif any(abs(int(tf[r, f, c])) != c + 1 for c in range(case.dim)):
+                raise ValueError(f"rank {r} face {f}: Transform {tf[r, f, :case.dim].tolist()} re-orders the "
+                                 "zone's axes; a rotated block needs its own orientation (rotate_block)")
+        blocks.append(case.replace(ni=int(sz[r, 0]), nj=int(sz[r, 1]), nk=int(sz[r, 2]) if case.dim == 3 else 1,
+                                   x=case.x[sl], y=case.y[sl], z=case.z[sl], rho=case.rho[sl], u=case.u[sl],
+                                   v=case.v[sl], w=case.w[sl], p=case.p[sl], periodic=(False, False, False),
+                                   bc=tuple(bc), name=f"{case.name}_b{r}"))
+    parts = tuple(len(np.unique(lo[:, a])) for a in range(3))
+    return Division(case=case, parts=parts, blocks=blocks, neighbour=nb, translation=tr, lo=lo, transform=tf)
+
+
 def _transforms(neigh, axes, flips, dim):
     """The .sddc Transform of every interface from the blocks' orientations:
     entry c of face f of block b is +-(1 + the axis of the neighbour that b's

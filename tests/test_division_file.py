@@ -6,13 +6,14 @@ the byte-swapped form (SwapDivFile) and a wrong rank count; and the same
 files read by SHOCK itself: its ranks load their rows with its own
 loadDivision, take them in as loadFile does and set up their geometry, bit
 for bit the geometry the library sets up from its reading of the file."""
+import os
 import struct
 
 import numpy as np
 import pytest
 
 import shock_b200
-from refbind import multirank_available, run_multirank
+from refbind import load_division_row, multirank_available, run_multirank
 from shock_b200 import cases
 from test_multiblock_host import DIVISIONS, division as named_division
 
@@ -160,6 +161,110 @@ def test_shock_reads_the_same_division(tmp_path, name, form):
     ref = run_multirank(d, 0, full=full, division_file=path, swap=2 if swap else 0)
     for b in range(len(d.blocks)):
         assert np.array_equal(got[b], ref[b]["geometry"]), (name, form, b)
+
+
+# the division files SHOCK ships with its test cases, in the reference tree
+# beside this repository (the same place oracle/Makefile compiles from)
+SHIPPED = os.path.join(os.path.dirname(os.path.abspath(__file__)), "..", "..", "reference", "testcases")
+
+
+def _shipped():
+    try:
+        return sorted(f for f in os.listdir(SHIPPED) if f.endswith(".sddc"))
+    except OSError:
+        return []
+
+
+@pytest.mark.parametrize("name", _shipped() or ["(none)"])
+def test_shipped_division_files(name):
+    """SHOCK's own division files (2D 2x2, 3D 2x4x1 and 2x2x2 divisions of
+    its cube test cases) read by the library as SHOCK's loadDivision reads them:
+    every rank's corners, neighbours, Transforms (with the face-axis sign
+    check_TransformationMatrix takes from the point ranges) and
+    Translations."""
+    if name == "(none)":
+        pytest.skip("SHOCK's test cases are not beside this repository")
+    if not multirank_available(5, 2) or not multirank_available(5, 3):
+        pytest.skip("multi-rank reference build absent (make -C oracle with the reference sources)")
+    dim = 2 if name.startswith("2d") else 3
+    path = os.path.join(SHIPPED, name)
+    row = 32 + 16 * dim + 2 * dim * (4 + 4 * dim + 32 * dim + 36)
+    size = os.path.getsize(path)
+    assert size % row == 0
+    nranks = size // row
+    nb, tr, tf, co, sz = shock_b200.read_division(path, dim, nranks)
+    interfaces = 0
+    for r in range(nranks):
+        corners, faces = load_division_row(path, dim, r, nranks)
+        assert np.array_equal(co[r], corners)
+        assert np.array_equal(sz[r][:dim], corners[3:3 + dim] - corners[:dim] + 1)
+        for f, (n, t, rng, drng, trans) in enumerate(faces):
+            assert nb[r, f] == (n - 1 if n else -1)
+            if not n:
+                continue
+            interfaces += 1
+            a = f // 2
+            me = next(x for x in range(dim) if rng[x] == rng[dim + x])
+            do = next(x for x in range(dim) if drng[x] == drng[dim + x])
+            want = t[:dim].copy()
+            want[a] = (1 if rng[me] != 1 else -1) * (1 if drng[do] == 1 else -1) * abs(t[a])
+            assert np.array_equal(tf[r, f, :dim], want)
+            assert np.array_equal(tr[r, f], trans)
+            # every neighbour names this rank back across its matching face
+            assert nb[n - 1, f ^ 1] == r
+    assert interfaces == {2: 8, 3: 20 if "16x16x16" in name else 24}[dim]
+
+
+def _zone_case(name, dim, size):
+    """A zone of the shipped division's size with a face type on every outer
+    face (the cube's CGNS grid is not readable here): walls, stretched grid."""
+    if dim == 2:
+        return cases.channel(2, 5, (size[0], size[1], 1), walls_i=True, stretch=1.2)
+    c = cases.smooth_random(3, 5, tuple(size), seed=9, stretch=0.05, inviscid=True)
+    return c.replace(periodic=(False, False, False), bc=(cases.BC_NAMES["wall_inviscid"],) * 6)
+
+
+@pytest.mark.parametrize("name", _shipped() or ["(none)"])
+def test_shipped_division_geometry(name):
+    """A grid divided by SHOCK's own division file: the library's division
+    (cases.load_division over its reader) sets up, on every ghosted point of
+    every block, the geometry SHOCK's ranks set up reading the same file with
+    loadDivision and exchanging their mesh halos."""
+    if name == "(none)":
+        pytest.skip("SHOCK's test cases are not beside this repository")
+    dim = 2 if name.startswith("2d") else 3
+    if not multirank_available(5, dim):
+        pytest.skip("multi-rank reference build absent (make -C oracle with the reference sources)")
+    path = os.path.join(SHIPPED, name)
+    nranks = 4 if dim == 2 else 8
+    _, _, _, co, _ = shock_b200.read_division(path, dim, nranks)
+    size = [int(co[:, 3 + a].max()) for a in range(dim)]
+    case = _zone_case(name, dim, size + [1] * (3 - dim))
+    d = cases.load_division(case, path, nranks)
+    assert sum(b.real_points for b in d.blocks) == case.real_points
+    got = shock_b200.host_multi_geometry(d)
+    ref = run_multirank(d, 0, division_file=path)
+    for b in range(nranks):
+        assert np.array_equal(got[b], ref[b]["geometry"]), (name, b)
+
+
+def test_load_division(tmp_path):
+    """cases.load_division gives back the division a file was written from
+    (blocks, neighbours, Translations, face types), and refuses a file whose
+    blocks are meshed in other orientations than the zone."""
+    c = cases.channel(3, 5, (16, 14, 12))
+    d = cases.split(c, (2, 2, 1))
+    path = tmp_path / "div.sddc"
+    cases.write_division(d, str(path))
+    e = cases.load_division(c, str(path), len(d.blocks))
+    assert np.array_equal(e.neighbour, d.neighbour) and np.array_equal(e.translation, d.translation)
+    assert np.array_equal(e.lo, d.lo) and tuple(e.parts) == tuple(d.parts)
+    for a, b in zip(d.blocks, e.blocks):
+        assert (a.ni, a.nj, a.nk, a.bc) == (b.ni, b.nj, b.nk, b.bc)
+        assert np.array_equal(a.x, b.x) and np.array_equal(a.p, b.p)
+    cases.write_division(_division(True), str(path))
+    with pytest.raises(ValueError):
+        cases.load_division(cases.taylor_green(12, order=5), str(path), 8)
 
 
 def test_division_file_size_checked(tmp_path):
