@@ -96,13 +96,17 @@ typedef struct shock_params {
 
 typedef struct shock_ctx shock_ctx;
 
-/* Fill the config.ini keys of *p from a SHOCK config.ini (src/Import.c:36-238,
- * iniparser's rules): [Numerics] TimeOrder, Tau; [FluidProperties] Mach,
- * Reynolds, Prandtl, Gamma, R, T, L; [Options] Inviscid,
- * ManufacturedSolution; [BoundaryConditions] T_wall, rho_inflow, p_inflow,
- * p_outflow, and AoA with [InitializeValues] u0 for u_inflow.  Keys that are absent
- * and all other fields (grid sizes, dim, order, periodicity, face types,
- * precision) are left as they were. */
+/* Fill the config.ini keys of *p from a SHOCK config.ini (src/Import.c:17-275,
+ * with the rules of the iniparser SHOCK ships, src/iniparser.c:555-720:
+ * quotes, ';'/'#' comments, backslash continuation, case-free names, atof
+ * for doubles, strtol base 0 for TimeOrder): [Numerics] TimeOrder, Tau;
+ * [FluidProperties] Mach, Reynolds, Prandtl, Gamma, R, T, L; [Options]
+ * Inviscid, ManufacturedSolution; [BoundaryConditions] T_wall, rho_inflow,
+ * p_inflow, p_outflow, and AoA with [InitializeValues] u0 for u_inflow.
+ * Keys that are absent and all other fields (grid sizes, dim, order,
+ * periodicity, face types, precision) are left as they were.  SHOCK_EINVAL
+ * for a file iniparser rejects (a line of 1024 characters or more, a last
+ * line without a newline). */
 int shock_params_from_ini(const char *path, shock_params *p);
 
 const char *shock_last_error(void);

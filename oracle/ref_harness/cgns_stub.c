@@ -1,12 +1,17 @@
 /*
- * Failing definitions of the CGNS calls SHOCK's Load.c makes in loadFile
- * (its mesh and solution reading), so that Load.c links into the multi-rank
- * oracle for its division-file reader alone.  loadFile is never called
- * there; if it were, the first call would fail and cg_error_exit would end
- * the rank.  Test infrastructure for the reference build under oracle/_ref.
+ * Failing definitions of the CGNS calls SHOCK's Load.c and Import.c make in
+ * their mesh and solution reading, so that they link into the oracle for
+ * their division-file and config.ini readers alone.  Those paths are never
+ * called there; if one were, its first call would fail and cg_error_exit
+ * would end the process.  Test infrastructure for the reference build under
+ * oracle/_ref.
  */
 #include <stdio.h>
 #include <stdlib.h>
+
+const char *BCTypeName[] = {"Null", "UserDefined", "BCFarfield", "BCInflow", "BCInflowSubsonic",
+                            "BCInflowSupersonic", "BCOutflow", "BCOutflowSubsonic", "BCWallInviscid",
+                            "BCWallViscous", "BCWallViscousIsothermal", "FamilySpecified"};
 
 #define CG_FAIL(name) \
     int name() { return 1; }
@@ -17,6 +22,8 @@ CG_FAIL(cg_base_read)
 CG_FAIL(cg_biter_read)
 CG_FAIL(cg_boco_info)
 CG_FAIL(cg_boco_read)
+CG_FAIL(cg_close)
+CG_FAIL(cg_coord_read)
 CG_FAIL(cg_coord_info)
 CG_FAIL(cg_descriptor_read)
 CG_FAIL(cg_fambc_read)
@@ -33,6 +40,7 @@ CG_FAIL(cg_nfamilies)
 CG_FAIL(cg_nfields)
 CG_FAIL(cg_nsols)
 CG_FAIL(cg_nzones)
+CG_FAIL(cg_open)
 CG_FAIL(cg_sol_info)
 CG_FAIL(cg_ziter_read)
 CG_FAIL(cg_zone_read)

@@ -429,3 +429,44 @@ def load_division_row(path, dim: int, rank: int, nranks: int, swap: int = 0):
         drng = np.array(x.drange[:dim] + x.drange[3:3 + dim])
         out.append((x.neighbour, np.array(x.transform[:]), rng, drng, np.array(x.tr[:], dtype=np.float32)))
     return np.array(corners[:]), out
+
+
+CONFIG_DOUBLES = ("time_order", "tau", "mach", "reynolds", "prandtl", "gamma", "gas_r", "t0", "l0", "t_wall",
+                  "rho_inflow", "p_inflow", "p_outflow", "u_inflow", "v_inflow", "w_inflow")
+CONFIG_FLAGS = ("inviscid", "mms", "swap_div_file", "inflow_normal_subsonic", "inflow_riemann_subsonic",
+                "inflow_isentrop_subsonic", "inflow_normal_supersonic", "outflow_normal_subsonic",
+                "outflow_riemann_subsonic", "outflow_rudy_subsonic")
+
+
+def config_available() -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", "libshockini_3d.so"))
+
+
+def _config_import_child(path):
+    lib = C.CDLL(os.path.join(HERE, "_ref", "libshockini_3d.so"), mode=os.RTLD_LOCAL)
+    d = (C.c_double * 16)()
+    i = (C.c_int * 10)()
+    if lib.ref_config_import(os.fsencode(str(path)), d, i) != 0:
+        raise RuntimeError("ref_config_import failed")
+    out = dict(zip(CONFIG_DOUBLES, d[:]))
+    out.update(zip(CONFIG_FLAGS, i[:]))
+    return out
+
+
+def config_import(path) -> dict:
+    """SHOCK's own reading of a config.ini (ConfigImport, src/Import.c:17-275,
+    with its iniparser): the fields the library's shock_params_from_ini
+    fills, and SHOCK's inflow/outflow option flags.  Runs in a child process,
+    since SHOCK ends the process on a file iniparser rejects or on an
+    inflow/outflow choice that does not name exactly one option each; then
+    RuntimeError carries the end of its output."""
+    import json
+    import subprocess
+    import sys
+    code = ("import json, sys; sys.path.insert(0, sys.argv[1]); import refbind; "
+            "print('CONFIG ' + json.dumps(refbind._config_import_child(sys.argv[2])))")
+    r = subprocess.run([sys.executable, "-c", code, HERE, str(path)], capture_output=True, text=True, timeout=120)
+    for line in r.stdout.splitlines():
+        if r.returncode == 0 and line.startswith("CONFIG "):
+            return json.loads(line[7:])
+    raise RuntimeError(f"SHOCK's ConfigImport ended with {r.returncode}: {(r.stdout + r.stderr)[-400:]}")

@@ -1,12 +1,28 @@
 // shock_params_from_ini: the config.ini keys of SHOCK's hot path.
 //
-// SHOCK reads its configuration with iniparser (src/Import.c:36-238):
-// sections in brackets, "key = value" lines, ';' or '#' starting a comment,
-// section and key names matched without regard to case, booleans true when
-// the value starts with y/Y/t/T/1.  This reader follows the same rules for
-// the keys the path consumes and leaves every other field of *p unchanged
-// (grid sizes, dimension and order come from the mesh and the build in
-// SHOCK, so the caller sets them).
+// SHOCK reads its configuration with the iniparser it ships
+// (src/iniparser.c:555-720, called from src/Import.c:17-275), and this reader
+// follows the same rules for the keys the path consumes:
+//   - a physical line loses its trailing white space; one that then ends in
+//     a backslash continues on the next line (the backslash dropped);
+//   - a line longer than 1023 characters, or a last line without a newline,
+//     makes iniparser reject the whole file (SHOCK then stops), and this
+//     reader too;
+//   - after stripping: empty lines and lines starting with ';' or '#' are
+//     skipped; "[name]" (first '[' and last ']') opens section name (up to
+//     the first ']', stripped, lower case);
+//   - "key = value": the key is everything before the first '=', stripped
+//     and lower case; a value starting with '"' or '\'' runs to the next
+//     such quote, any other value to the first ';' or '#', stripped; an
+//     empty or missing value is the empty string; a later line with the
+//     same key replaces the earlier one; other lines are ignored;
+//   - numbers are read as iniparser's getters read them: doubles with
+//     atof (an empty value is 0), integers with strtol in base 0
+//     (TimeOrder), booleans true when the value starts with y/Y/t/T/1 and
+//     false with n/N/f/F/0 (otherwise the field keeps its value).
+// Keys missing from the file leave their fields unchanged, as do all other
+// fields of *p (grid sizes, dimension and order come from the mesh and the
+// build in SHOCK, so the caller sets them).
 #include <cctype>
 #include <cmath>
 #include <cstdio>
@@ -43,6 +59,21 @@ int to_bool(const std::string &v, int def)
     return def;
 }
 
+// iniparser's value of one "key = value" line (the part after the first
+// '='): quoted up to the next quote of the same kind, else up to the first
+// comment character, stripped
+std::string ini_value(const std::string &rest)
+{
+    std::string v = trim(rest);
+    if (!v.empty() && (v[0] == '"' || v[0] == '\'')) {
+        const size_t e = v.find(v[0], 1);
+        if (e == 1) return "";                                 // "" or ''
+        if (e != std::string::npos || v.size() > 1) return trim(v.substr(1, e == std::string::npos ? e : e - 1));
+    }
+    const size_t c = v.find_first_of(";#");
+    return trim(c == std::string::npos ? v : v.substr(0, c));
+}
+
 }  // namespace
 
 extern "C" int shock_params_from_ini(const char *path, shock_params *p)
@@ -51,37 +82,55 @@ extern "C" int shock_params_from_ini(const char *path, shock_params *p)
     FILE *f = std::fopen(path, "r");
     if (!f) return shock::report_error(SHOCK_EINVAL, "cannot open %s", path);
     std::map<std::string, std::string> kv;   // "section:key" -> value
-    std::string section;
-    char line[4096];
-    while (std::fgets(line, sizeof line, f)) {
-        std::string s = trim(line);
-        if (s.empty() || s[0] == ';' || s[0] == '#') continue;
-        if (s[0] == '[') {
-            size_t e = s.find(']');
-            section = lower(trim(s.substr(1, e == std::string::npos ? std::string::npos : e - 1)));
+    std::string section, logical;
+    char buf[1025];
+    int lineno = 0;
+    bool ok = true;
+    while (std::fgets(buf, sizeof buf, f)) {
+        lineno++;
+        std::string raw(buf);
+        if (raw.size() <= 1 && logical.empty()) continue;      // a bare newline
+        if (raw.back() != '\n' || raw.size() + logical.size() > 1024) {
+            ok = false;                                        // too long, or no newline at the end
+            break;
+        }
+        size_t end = raw.size();
+        while (end > 0 && std::isspace((unsigned char)raw[end - 1])) end--;
+        raw.resize(end);
+        if (!raw.empty() && raw.back() == '\\') {              // continued on the next line
+            raw.pop_back();
+            logical += raw;
             continue;
         }
-        size_t eq = s.find('=');
-        if (eq == std::string::npos) continue;
-        std::string key = lower(trim(s.substr(0, eq)));
-        std::string val = s.substr(eq + 1);
-        size_t c = val.find_first_of(";#");
-        if (c != std::string::npos) val = val.substr(0, c);
-        kv[section + ":" + key] = trim(val);
+        std::string s = trim(logical + raw);
+        logical.clear();
+        if (s.empty() || s[0] == ';' || s[0] == '#') continue;
+        if (s[0] == '[' && s.back() == ']') {
+            const std::string name = s.substr(1, s.find(']') - 1);
+            if (!name.empty()) section = lower(trim(name));    // "[]" leaves the section as it was
+            continue;
+        }
+        const size_t eq = s.find('=');
+        if (eq == std::string::npos || eq == 0) continue;      // iniparser: syntax error, line ignored
+        kv[section + ":" + lower(trim(s.substr(0, eq)))] = ini_value(s.substr(eq + 1));
     }
     std::fclose(f);
+    if (!ok)
+        return shock::report_error(SHOCK_EINVAL,
+                                   "%s line %d: longer than 1023 characters or without a newline at the end of the "
+                                   "file; SHOCK's iniparser rejects the file",
+                                   path, lineno);
 
     auto num = [&](const char *k, double &dst) {
         auto it = kv.find(k);
-        if (it != kv.end() && !it->second.empty()) dst = std::strtod(it->second.c_str(), nullptr);
+        if (it != kv.end()) dst = std::atof(it->second.c_str());
     };
     auto boolean = [&](const char *k, int &dst) {
         auto it = kv.find(k);
         if (it != kv.end()) dst = to_bool(it->second, dst);
     };
-    double t = p->time_order;
-    num("numerics:timeorder", t);
-    p->time_order = (int)t;
+    auto it = kv.find("numerics:timeorder");
+    if (it != kv.end()) p->time_order = (int)std::strtol(it->second.c_str(), nullptr, 0);
     num("numerics:tau", p->tau);
     num("fluidproperties:mach", p->mach);
     num("fluidproperties:reynolds", p->reynolds);
