@@ -272,7 +272,7 @@ REF_SAMPLES = {
 # split in two or more (SHOCK's self-periodic exchange takes one axis per
 # rank at most) and each block keeps nj <= nk (its j-centred zeta stencil).
 MPI_SAMPLES = {
-    "w9": ("decaying_turbulence", {"n": 96, "order": 9}),
+    "w9": ("decaying_turbulence", {"n": 128, "order": 9}),
     "w5": ("taylor_green", {"n": 128, "order": 5}),
 }
 MPI_PARTS = {16: (4, 2, 2), 8: (2, 2, 2), 4: (2, 2, 1)}
