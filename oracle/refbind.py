@@ -407,14 +407,30 @@ class RefIface(C.Structure):
                 ("drange", C.c_longlong * 6), ("rc", C.c_float * 3), ("ra", C.c_float * 3), ("tr", C.c_float * 3)]
 
 
+_ROW_READERS = {}
+
+
+def _row_reader(dim):
+    if dim not in _ROW_READERS:
+        lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockmpi_w5_{dim}d.so"), mode=os.RTLD_LOCAL)
+        lib.ref_load_division_row.restype = C.c_int
+        _ROW_READERS[dim] = lib
+    return _ROW_READERS[dim]
+
+
+def generator_path():
+    """SHOCK's division-file generator built from its sources, or None."""
+    p = os.path.join(HERE, "_ref", "generatedivfile_3")
+    return p if os.path.exists(p) else None
+
+
 def load_division_row(path, dim: int, rank: int, nranks: int, swap: int = 0):
     """One rank's row of a .sddc file as SHOCK's own loadDivision reads it
     (src/Load.c:191-250; swap: its SwapDivFile option): (corners (6,),
     per face (neighbour 1-based or 0, transform (3,), range (2*dim,), drange
     (2*dim,), translation (3,))).  In process: the file's size must be nranks rows,
     which the caller checks first (loadDivision ends the process otherwise)."""
-    lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockmpi_w5_{dim}d.so"), mode=os.RTLD_LOCAL)
-    lib.ref_load_division_row.restype = C.c_int
+    lib = _row_reader(dim)
     corners = (C.c_longlong * 6)()
     faces = (RefIface * 6)()
     ni = lib.ref_load_division_row(os.fsencode(str(path)), C.c_int(rank), C.c_int(nranks), C.c_int(swap), corners,

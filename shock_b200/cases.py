@@ -168,6 +168,74 @@ def smooth_random(dim: int, order: int, n: Tuple[int, int, int], seed: int = 0,
     return c
 
 
+def parabolic_cgrid(dim: int, order: int, n: Tuple[int, int, int], half_width: float = 1.5, height: float = 1.2,
+                    span: float = 0.4, seed: int = 0, mach: float = 0.5, reynolds: float = 500.0,
+                    inviscid: bool = False) -> Case:
+    """A C-grid in parabolic coordinates, x = (xi^2 - eta^2)/2, y = xi eta
+    (z = the span in 3D, periodic): xi runs over ni points across
+    (-half_width, half_width), eta over nj points in (0, height), both at
+    half-cell offsets, so the grid wraps around the focus and the row below
+    j = 0 is the row j = 0 read from the other end of i (the ghost point
+    (xi, -eta) is the point (-xi, eta)).  That cut is the wake cut of a
+    C-grid (division_file generators join it bottom to bottom with
+    Transform (-1,-2,3), see wake_cut); the other faces are farfield.  A
+    seeded smooth state on a uniform stream along x."""
+    rng = np.random.default_rng(seed)
+    ni, nj, nk = n[0], n[1], (n[2] if dim == 3 else 1)
+    xi = -half_width + (np.arange(ni) + 0.5) * (2 * half_width / ni)
+    eta = (np.arange(nj) + 0.5) * (height / nj)
+    zs = span * np.arange(nk) / nk if dim == 3 else np.zeros(1)
+    X, E, Z = np.meshgrid(xi, eta, zs, indexing="ij")
+    x = 0.5 * (X * X - E * E)
+    y = X * E
+    z = Z
+
+    def smooth():
+        return sum(rng.normal() * np.sin(rng.integers(1, 3) * x + rng.uniform(0, 2 * math.pi))
+                   * np.cos(rng.integers(1, 3) * y) for _ in range(2))
+
+    amp = 0.02
+    u = 1.0 + amp * smooth()
+    v = amp * smooth()
+    w = amp * smooth() if dim == 3 else np.zeros_like(x)
+    rho = 1.0 + amp * smooth()
+    p = 1.0 / (1.4 * mach * mach) * (1.0 + amp * smooth())
+    far = 3   # BC_NAMES["farfield"]
+    c = Case(dim=dim, order=order, ni=ni, nj=nj, nk=nk, x=x, y=y, z=z, rho=rho, u=u, v=v, w=w, p=p,
+             mach=mach, reynolds=reynolds, inviscid=inviscid, periodic=(False, False, dim == 3),
+             period=(1.0, 1.0, span), bc=(far, far, 0, far, 0, 0), u_inflow=(1.0, 0.0, 0.0),
+             name=f"cgrid{dim}d_w{order}")
+    c.tau = cfl_tau(c)
+    return c
+
+
+def wake_cut(division: "Division") -> "Division":
+    """The division of a C-grid (parabolic_cgrid) with its wake cut: the
+    bottom face of block (i, 0, k) joins the bottom face of block
+    (parts[0]-1-i, 0, k) with Transform (-1,-2,3) -- i runs the other way
+    across the cut, and both normals point out of the zone -- as SHOCK's own
+    division generator writes it (TOOLS/generatedivfile/generatedivfile_3.c,
+    its case 2).  The blocks along i must mirror one another in size."""
+    P = division.parts
+    nb = division.neighbour.copy()
+    tf = division.transform.copy()
+    blocks = list(division.blocks)
+    for k in range(P[2]):
+        for i in range(P[0]):
+            r = (k * P[1]) * P[0] + i
+            m = (k * P[1]) * P[0] + (P[0] - 1 - i)
+            if blocks[r].ni != blocks[m].ni:
+                raise ValueError("the blocks along i do not mirror one another")
+            nb[r, 2] = m
+            tf[r, 2] = (-1, -2, 3)
+            bc = list(blocks[r].bc)
+            bc[2] = 0
+            blocks[r] = blocks[r].replace(bc=tuple(bc))
+    return Division(case=division.case, parts=division.parts, blocks=blocks, neighbour=nb,
+                    translation=division.translation.copy(), lo=division.lo, transform=tf,
+                    axes=division.axes, flips=division.flips)
+
+
 BC_NAMES = {"wall_viscous": 1, "wall_inviscid": 2, "farfield": 3, "wall_isothermal": 4,
             "inflow_subsonic": 5, "inflow_supersonic": 6, "outflow_subsonic": 7,
             "inflow_riemann": 8, "inflow_isentropic": 9, "outflow_riemann": 10, "outflow_rudy": 11}

@@ -13,9 +13,9 @@ import numpy as np
 import pytest
 
 import shock_b200
-from refbind import load_division_row, multirank_available, run_multirank
+from refbind import generator_path, load_division_row, multirank_available, run_multirank
 from shock_b200 import cases
-from test_multiblock_host import DIVISIONS, division as named_division
+from test_multiblock_host import CGRIDS, DIVISIONS, cgrid_division, division as named_division
 
 
 def _division(rotated):
@@ -213,6 +213,63 @@ def test_shipped_division_files(name):
     assert interfaces == {2: 8, 3: 20 if "16x16x16" in name else 24}[dim]
 
 
+def _check_rows_as_shock_reads_them(path, dim, nranks):
+    """Every rank's row of a division file: the library's reading against
+    SHOCK's loadDivision with the face-axis sign of
+    check_TransformationMatrix; returns the library's tables."""
+    nb, tr, tf, co, sz = shock_b200.read_division(path, dim, nranks)
+    for r in range(nranks):
+        corners, faces = load_division_row(path, dim, r, nranks)
+        assert np.array_equal(co[r], corners), r
+        for f, (n, t, rng, drng, trans) in enumerate(faces):
+            assert nb[r, f] == (n - 1 if n else -1), (r, f)
+            if not n:
+                continue
+            a = f // 2
+            me = next(x for x in range(dim) if rng[x] == rng[dim + x])
+            do = next(x for x in range(dim) if drng[x] == drng[dim + x])
+            want = t[:dim].copy()
+            want[a] = (1 if rng[me] != 1 else -1) * (1 if drng[do] == 1 else -1) * abs(t[a])
+            assert np.array_equal(tf[r, f, :dim], want), (r, f)
+            assert np.array_equal(tr[r, f], trans), (r, f)
+    return nb, tr, tf, co, sz
+
+
+def test_generated_cgrid_division(tmp_path):
+    """The division SHOCK's own generator writes (TOOLS/generatedivfile/
+    generatedivfile_3.c, run unmodified: a 2048x256x256 C-grid in 4096
+    blocks of 32^3, the wake cut joining mirrored blocks bottom to bottom
+    with Transform (-1,-2,3), a periodic span with a float32 Translation)
+    read by the library as SHOCK reads it, every rank; and every interface
+    named back from the other side with the inverse Transform, which is what
+    the library's division set-up requires."""
+    import subprocess
+    gen = generator_path()
+    if gen is None or not multirank_available(5, 3):
+        pytest.skip("SHOCK's generator or the multi-rank reference build absent (make -C oracle)")
+    subprocess.run([gen], cwd=tmp_path, check=True, capture_output=True)
+    (path,) = list(tmp_path.glob("*.sddc"))
+    nb, tr, tf, co, sz = _check_rows_as_shock_reads_them(path, 3, 4096)
+    assert (sz == 32).all()
+    wake = 0
+    for r in range(4096):
+        for f in range(6):
+            n = nb[r, f]
+            if n < 0:
+                continue
+            t = tf[r, f]
+            a, hi = f // 2, f % 2
+            fd = 2 * (abs(t[a]) - 1) + (hi ^ int(t[a] > 0))
+            assert nb[n, fd] == r, (r, f)
+            back = tf[n, fd]
+            for ax in range(3):
+                assert back[abs(t[ax]) - 1] == np.sign(t[ax]) * (ax + 1), (r, f)
+            assert np.array_equal(tr[n, fd], -tr[r, f]), (r, f)
+            wake += fd == f
+    # the wake cut: 8 blocks at each end of the 64 along i, 8 spans in k
+    assert wake == 2 * 8 * 8
+
+
 def _zone_case(name, dim, size):
     """A zone of the shipped division's size with a face type on every outer
     face (the cube's CGNS grid is not readable here): walls, stretched grid."""
@@ -243,6 +300,24 @@ def test_shipped_division_geometry(name):
     got = shock_b200.host_multi_geometry(d)
     ref = run_multirank(d, 0, division_file=path)
     for b in range(nranks):
+        assert np.array_equal(got[b], ref[b]["geometry"]), (name, b)
+
+
+@pytest.mark.parametrize("name", sorted(CGRIDS))
+def test_shock_reads_the_same_cgrid_division(tmp_path, name):
+    """A C-grid's division with its wake cut (bottom-to-bottom interfaces,
+    Transform (-1,-2,3)) written as a .sddc file: SHOCK's ranks read it with
+    loadDivision and set up, bit for bit, the geometry the library sets up
+    from its own reading of the file."""
+    case, d, full = cgrid_division(name)
+    if not multirank_available(case.order, case.dim, full=full):
+        pytest.skip("multi-rank reference build absent (make -C oracle with the reference sources)")
+    path = tmp_path / "cgrid.sddc"
+    cases.write_division(d, str(path))
+    _check_rows_as_shock_reads_them(path, case.dim, len(d.blocks))
+    got = shock_b200.host_multi_geometry(_read_back(d, path), full_metric=full)
+    ref = run_multirank(d, 0, full=full, division_file=path)
+    for b in range(len(d.blocks)):
         assert np.array_equal(got[b], ref[b]["geometry"]), (name, b)
 
 

@@ -5,7 +5,8 @@ libshockmpi_*: SHOCK's TransferMeshParameter between ranks over the forked
 shared-memory stand-in for MPI), bit for bit on every ghosted point of
 every block, also for divisions whose zones are meshed in other
 orientations (.sddc Transforms other than 1,2,3); and the division
-bookkeeping."""
+bookkeeping; and C-grids whose wake cut joins mirrored blocks bottom to
+bottom."""
 import numpy as np
 import pytest
 
@@ -57,6 +58,51 @@ def test_division_geometry_matches_shock_multirank(name):
     ref = run_multirank(d, 0, full=full)
     for b in range(len(d.blocks)):
         assert np.array_equal(got[b], ref[b]["geometry"]), (name, b)
+
+
+# C-grids (cases.parabolic_cgrid) divided with their wake cut (cases.wake_cut):
+# the bottom faces of mirrored blocks joined with Transform (-1,-2,3), the
+# topology of SHOCK's own division generator; (dim, order, points, parts,
+# full metric -- 3D C-grids have their metric in the cross terms)
+CGRIDS = {
+    "cgrid2d_w5_4x2": (2, 5, (24, 12, 1), (4, 2, 1), False),
+    "cgrid2d_w9_2x1": (2, 9, (20, 14, 1), (2, 1, 1), False),
+    "cgrid3d_w5_4x2x2_full": (3, 5, (16, 10, 12), (4, 2, 2), True),
+}
+
+
+def cgrid_division(name):
+    dim, order, n, parts, full = CGRIDS[name]
+    case = cases.parabolic_cgrid(dim, order, n, seed=3)
+    return case, cases.wake_cut(cases.split(case, parts)), full
+
+
+@pytest.mark.parametrize("name", sorted(CGRIDS))
+def test_cgrid_geometry_matches_shock_multirank(name):
+    case, d, full = cgrid_division(name)
+    if not multirank_available(case.order, case.dim, full=full):
+        pytest.skip("multi-rank reference build absent (make -C oracle with the reference sources)")
+    got = shock_b200.host_multi_geometry(d, full_metric=full)
+    ref = run_multirank(d, 0, full=full)
+    for b in range(len(d.blocks)):
+        assert np.array_equal(got[b], ref[b]["geometry"]), (name, b)
+
+
+def test_wake_cut_bookkeeping():
+    """Across the cut i runs the other way and both sides are bottom faces:
+    the ghost row below block b's j = 0 is its mirror block's row j = 0,
+    point for point (x(xi, -eta) = x(-xi, eta) in parabolic coordinates)."""
+    case, d, _ = cgrid_division("cgrid2d_w5_4x2")
+    for b in range(4):
+        m = 3 - b
+        assert d.neighbour[b, 2] == m and d.neighbour[m, 2] == b
+        assert tuple(d.transform[b, 2]) == (-1, -2, 3)
+    xi = -1.5 + (np.arange(24) + 0.5) * (3.0 / 24)
+    eta0 = 0.5 * 1.2 / 12
+    ghost_x = 0.5 * (xi ** 2 - eta0 ** 2)
+    assert np.array_equal(ghost_x, case.x[::-1, 0, 0])
+    with pytest.raises(ValueError):
+        cases.wake_cut(cases.split(cases.parabolic_cgrid(2, 5, (25, 12, 1)), (2, 1, 1)))
 
 
 def test_split_bookkeeping():
