@@ -218,6 +218,16 @@ int shock_post(shock_ctx *ctx, double *out3);
  * capacity: steps the device history holds.  n = 0 removes the probes.
  * The step graphs are captured again. */
 int shock_set_probes(shock_ctx *ctx, int n, const int *ijk3, int capacity);
+/* The points SHOCK records n probe locations xyz (n x 3: its config.ini
+ * PressureHistory / VelocityHistory P<p>_x/y/z-Location) at, chosen as
+ * preparePressureHistoryValues chooses them (src/Functions.c:5114-5188)
+ * from the block's ghosted coordinates x, y, z ((ni+2g) x (nj+2g) x
+ * (nk+2g or 1), i slowest, as shock_geometry writes them; z unused in
+ * 2D): the nearest point in SHOCK's visiting order, the probe this
+ * block's (found[p] = 1) when that point is a real point.  ijk3 receives
+ * the ghosted (i,j,k) to pass to shock_set_probes.  Host only. */
+int shock_locate_probes(int dim, int ni, int nj, int nk, int ghosts, const double *x, const double *y,
+                        const double *z, int n, const double *xyz, int *ijk3, int *found);
 /* The history since the last call: out4 receives steps x n x (p, u, v, w)
  * of U_lastStep after each step (p: the pressure the step's last stage
  * formed, which SHOCK copies into U_lastStep); *steps the number of steps

@@ -361,6 +361,42 @@ void ref_post(double *out3)
         for (int o = 0; o < n; o++) out3[(size_t)a * n + o] = (double)f[a][o];
 }
 
+/* SHOCK's placement of PressureHistory probes (preparePressureHistoryValues,
+ * src/Functions.c:5114-5188, called by setOptions after the set-up): n
+ * locations xyz (n x 3); ijk[p] receives SHOCK's ghosted linear index of the
+ * chosen point and flag[p] whether this block records the probe. */
+void ref_probe_points(int n, const double *xyz, int *ijk, int *flag)
+{
+    cfg.PressureHistory_No = n;
+    FLT *c[6];
+    for (int a = 0; a < 6; a++) c[a] = calloc((size_t)n, sizeof(FLT));
+    cfg.PressureHistory_x_P = c[0];
+    cfg.PressureHistory_y_P = c[1];
+    cfg.PressureHistory_z_P = c[2];
+    cfg.PressureHistory_x_P_real = c[3];
+    cfg.PressureHistory_y_P_real = c[4];
+    cfg.PressureHistory_z_P_real = c[5];
+    cfg.ijk_PressureHistory_P = calloc((size_t)n, sizeof(int));
+    cfg.flag_PressureHistory_P = calloc((size_t)n, sizeof(int));
+    for (int p = 0; p < n; p++) {
+        c[0][p] = xyz[3 * p];
+        c[1][p] = xyz[3 * p + 1];
+        c[2][p] = xyz[3 * p + 2];
+        cfg.ijk_PressureHistory_P[p] = -1;
+    }
+    preparePressureHistoryValues(&cfg, &msh);
+    for (int p = 0; p < n; p++) {
+        ijk[p] = cfg.ijk_PressureHistory_P[p];
+        flag[p] = cfg.flag_PressureHistory_P[p];
+    }
+    for (int a = 0; a < 6; a++) free(c[a]);
+    free(cfg.ijk_PressureHistory_P);
+    free(cfg.flag_PressureHistory_P);
+    cfg.ijk_PressureHistory_P = NULL;
+    cfg.flag_PressureHistory_P = NULL;
+    cfg.PressureHistory_No = 0;
+}
+
 void ref_free(void)
 {
     if (!live) return;

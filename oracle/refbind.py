@@ -171,6 +171,18 @@ class RefSolver:
         self.lib.ref_post(_ptr(q))
         return q.reshape((3,) + self.shape)
 
+    def probe_points(self, xyz):
+        """SHOCK's placement of PressureHistory probes at the n x 3
+        locations xyz (preparePressureHistoryValues): (ghosted linear index
+        of the chosen point, whether this block records the probe) each."""
+        xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+        n = len(xyz)
+        ijk = np.zeros(n, np.int32)
+        flag = np.zeros(n, np.int32)
+        self.lib.ref_probe_points(C.c_int(n), _ptr(xyz), ijk.ctypes.data_as(C.POINTER(C.c_int)),
+                                  flag.ctypes.data_as(C.POINTER(C.c_int)))
+        return ijk, flag
+
     def mms_source(self) -> np.ndarray:
         """J*S of the reference manufactured-solution source (5 fields)."""
         q = np.zeros(5 * self.n)

@@ -423,6 +423,25 @@ def _division_blocks(division):
     return arr, keep
 
 
+def locate_probes(case, geometry13, xyz):
+    """The grid points SHOCK records probes at (shock_locate_probes): for
+    the n x 3 locations xyz on the block of case with ghosted geometry
+    geometry13 (13 x ghosted shape, as Solver.geometry or host_geometry give
+    it), the ghosted (i, j, k) of each probe's point and whether the block
+    records it."""
+    g = np.ascontiguousarray(geometry13, np.float64)
+    xyz = np.ascontiguousarray(xyz, np.float64).reshape(-1, 3)
+    n = len(xyz)
+    ijk = np.zeros((n, 3), np.int32)
+    found = np.zeros(n, np.int32)
+    x, y, z = (np.ascontiguousarray(g[a]) for a in range(3))
+    ip = C.POINTER(C.c_int)
+    _check(lib().shock_locate_probes(case.dim, case.ni, case.nj, case.nk if case.dim == 3 else 1, case.ghosts,
+                                     _ptr(x), _ptr(y), _ptr(z), n, _ptr(xyz), ijk.ctypes.data_as(ip),
+                                     found.ctypes.data_as(ip)))
+    return ijk, found.astype(bool)
+
+
 def read_division(path, dim, nranks, swap=False):
     """Every rank's row of a SHOCK .sddc division file (shock_read_division):
     (neighbour (n,6), translation (n,6,3), transform (n,6,3), corners (n,6),
