@@ -105,7 +105,7 @@ typedef struct shock_ctx shock_ctx;
  * p_inflow, p_outflow, and AoA with [InitializeValues] u0 for u_inflow.
  * Keys that are absent and all other fields (grid sizes, dim, order,
  * periodicity, face types, precision) are left as they were.  SHOCK_EINVAL
- * for a file iniparser rejects (a line of 1024 characters or more, a last
+ * for a file iniparser rejects (a line of more than 1022 characters, a last
  * line without a newline). */
 int shock_params_from_ini(const char *path, shock_params *p);
 

@@ -5,9 +5,9 @@
 // follows the same rules for the keys the path consumes:
 //   - a physical line loses its trailing white space; one that then ends in
 //     a backslash continues on the next line (the backslash dropped);
-//   - a line longer than 1023 characters, or a last line without a newline,
-//     makes iniparser reject the whole file (SHOCK then stops), and this
-//     reader too;
+//   - a line of more than 1022 characters (a continued line counted from
+//     its start), or a last line without a newline, makes iniparser reject
+//     the whole file (SHOCK then stops), and this reader too;
 //   - after stripping: empty lines and lines starting with ';' or '#' are
 //     skipped; "[name]" (first '[' and last ']') opens section name (up to
 //     the first ']', stripped, lower case);
@@ -90,7 +90,9 @@ extern "C" int shock_params_from_ini(const char *path, shock_params *p)
         lineno++;
         std::string raw(buf);
         if (raw.size() <= 1 && logical.empty()) continue;      // a bare newline
-        if (raw.back() != '\n' || raw.size() + logical.size() > 1024) {
+        // iniparser reads a line into 1023 characters after what the previous
+        // lines of a continued line left, its newline included
+        if (raw.back() != '\n' || raw.size() + logical.size() > 1023) {
             ok = false;                                        // too long, or no newline at the end
             break;
         }
@@ -117,7 +119,7 @@ extern "C" int shock_params_from_ini(const char *path, shock_params *p)
     std::fclose(f);
     if (!ok)
         return shock::report_error(SHOCK_EINVAL,
-                                   "%s line %d: longer than 1023 characters or without a newline at the end of the "
+                                   "%s line %d: longer than 1022 characters or without a newline at the end of the "
                                    "file; SHOCK's iniparser rejects the file",
                                    path, lineno);
 

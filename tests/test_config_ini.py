@@ -4,9 +4,9 @@ iniparser SHOCK ships, built unmodified into oracle/_ref/libshockini_3d.so
 and run in a child process.  Every field the library fills must come out
 equal, bit for bit, for SHOCK's own config.ini and for files that exercise
 iniparser's rules (quotes, comments, continuation lines, case, duplicate
-keys, sections, integer bases, booleans, empty values); files iniparser
-rejects (a line of 1024 characters or more, a last line without a newline)
-must be rejected by both."""
+keys, sections, integer bases, booleans, empty values, the longest line it
+takes); files iniparser rejects (a line of more than 1022 characters, a
+last line without a newline) must be rejected by both."""
 import math
 import os
 
@@ -97,11 +97,14 @@ VARIANTS = {
     "missing_keys": lambda s: s.replace("u0\t\t\t=1.3", "").replace("Prandtl\t\t\t=0.72", ""),
     "missing_inflow_velocity": lambda s: s.replace("u0\t\t\t=1.3", "").replace("AoA\t\t\t=12.5\t;degrees", ""),
     "last_line_a_comment_without_newline": lambda s: s + ";",
+    "longest_line": lambda s: s.replace("[Numerics]", "[Numerics]\n; " + "x" * 1020),
+    "longest_continued_line": lambda s: s.replace("Tau\t\t\t=0.001", "Tau = 0.002 ;" + "y" * 500 + "\\\n" + "z" * 500),
 }
 
 REJECTED = {
     "last_line_without_newline": lambda s: s + "L = 2.0",
-    "line_too_long": lambda s: s.replace("[Numerics]", "[Numerics]\n; " + "x" * 1100),
+    "line_too_long": lambda s: s.replace("[Numerics]", "[Numerics]\n; " + "x" * 1021),
+    "continued_line_too_long": lambda s: s.replace("Tau\t\t\t=0.001", "Tau = 0.002 ;" + "y" * 500 + "\\\n" + "z" * 510),
 }
 
 
