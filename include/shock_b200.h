@@ -466,6 +466,11 @@ int shock_multi_rhs(shock_multi *m, int block, double *q5);
 /* A block's rho,u,v,w,e (5*NG, ghosted). */
 int shock_multi_download_state(shock_multi *m, int block, double *prim5);
 int shock_multi_upload_state(shock_multi *m, int block, const double *prim5);
+/* A block's U_RK pressure after the last step, and the U_lastStep pressure
+ * that goes with an uploaded state (NG doubles each, as
+ * shock_download_pressure / shock_upload_last_pressure). */
+int shock_multi_download_pressure(shock_multi *m, int block, double *p);
+int shock_multi_upload_last_pressure(shock_multi *m, int block, const double *p);
 /* The time step of the following steps (as shock_set_tau). */
 int shock_multi_set_tau(shock_multi *m, double tau);
 /* checkNAN over every block; SHOCK_ENAN when any density is non-finite. */

@@ -1,0 +1,185 @@
+/*
+ * A host-memory test double of libshock_b200 for the drop-in's division
+ * mode (shock_b200/dropin/GPU.c with several ranks), so that its MPI
+ * plumbing runs on CPU inside SHOCK's own multi-rank set-up: the blocks
+ * rank 0 hands to shock_multi_create go through the real library's host
+ * set-up (shock_host_multi_geometry, loaded from $SHOCK_B200_LIB), which
+ * checks the division and whose geometry is kept for the test to compare
+ * with SHOCK's; a "step" adds (block + 1) * 1e-3 to every density and
+ * remembers tau; $SHOCK_MOCK_NAN = "step block" plants a non-finite
+ * density.  Test infrastructure for the reference build under oracle/_ref;
+ * the single-block entry points the binding also links are stubs that fail.
+ */
+#include <dlfcn.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "shock_b200.h"
+
+struct shock_multi {
+    int nblocks, dim, g, steps;
+    size_t *ng;
+    double **state;   /* per block 6*NG: rho,u,v,w,e, then p */
+    double **plast;   /* per block NG: U_lastStep's p as uploaded */
+    double **geo;     /* per block 13*NG from the real library */
+    int dims[64][3];
+};
+
+static struct shock_multi *g_last;
+static double g_taus[256];
+static int g_ntau;
+
+const char *shock_last_error(void) { return "mock"; }
+
+#define MOCK_FAIL(name, ...) \
+    int name(__VA_ARGS__) { return SHOCK_EINVAL; }
+MOCK_FAIL(shock_create, const shock_params *p, const double *x, const double *y, const double *z, const double *u,
+          const double *v, const double *w, const double *pr, const double *rho, int device, shock_ctx **out)
+MOCK_FAIL(shock_set_dirichlet, shock_ctx *c, const double *e)
+MOCK_FAIL(shock_set_source, shock_ctx *c, const double *s)
+MOCK_FAIL(shock_upload_state, shock_ctx *c, const double *s)
+MOCK_FAIL(shock_upload_last_pressure, shock_ctx *c, const double *p)
+MOCK_FAIL(shock_set_tau, shock_ctx *c, double t)
+MOCK_FAIL(shock_step, shock_ctx *c, int n)
+MOCK_FAIL(shock_check_nan, shock_ctx *c, int *b)
+MOCK_FAIL(shock_download_state, shock_ctx *c, double *s, int w)
+MOCK_FAIL(shock_download_pressure, shock_ctx *c, double *p)
+MOCK_FAIL(shock_destroy, shock_ctx *c)
+
+int shock_multi_create(const shock_params *p, int nblocks, const shock_block *blocks, int device, shock_multi **out)
+{
+    (void)device;
+    const char *path = getenv("SHOCK_B200_LIB");
+    void *lib = path ? dlopen(path, RTLD_NOW | RTLD_LOCAL) : NULL;
+    if (!lib || nblocks > 64) return SHOCK_EINVAL;
+    int (*geom)(const shock_params *, int, const shock_block *, double *const *) =
+        (int (*)(const shock_params *, int, const shock_block *, double *const *))dlsym(lib, "shock_host_multi_geometry");
+    if (!geom) return SHOCK_EINVAL;
+    struct shock_multi *m = calloc(1, sizeof *m);
+    m->nblocks = nblocks;
+    m->dim = p->dim;
+    m->g = (p->order + 1) / 2;
+    m->ng = calloc((size_t)nblocks, sizeof(size_t));
+    m->state = calloc((size_t)nblocks, sizeof(double *));
+    m->plast = calloc((size_t)nblocks, sizeof(double *));
+    m->geo = calloc((size_t)nblocks, sizeof(double *));
+    for (int b = 0; b < nblocks; b++) {
+        const int n[3] = {blocks[b].ni, blocks[b].nj, blocks[b].nk};
+        size_t ng = 1;
+        for (int a = 0; a < 3; a++) {
+            m->dims[b][a] = a < p->dim ? n[a] + 2 * m->g : 1;
+            ng *= (size_t)m->dims[b][a];
+        }
+        m->ng[b] = ng;
+        m->state[b] = calloc(6 * ng, sizeof(double));
+        m->plast[b] = calloc(ng, sizeof(double));
+        m->geo[b] = calloc(13 * ng, sizeof(double));
+    }
+    const int rc = geom(p, nblocks, blocks, m->geo);
+    if (rc) return rc;
+    g_last = m;
+    g_ntau = 0;
+    g_taus[g_ntau++] = p->tau;
+    *out = m;
+    return SHOCK_OK;
+}
+
+int shock_multi_destroy(shock_multi *m)
+{
+    (void)m;   /* kept for the test to read */
+    return SHOCK_OK;
+}
+
+static int bad_block(const shock_multi *m, int b) { return !m || b < 0 || b >= m->nblocks; }
+
+int shock_multi_upload_state(shock_multi *m, int b, const double *s)
+{
+    if (bad_block(m, b)) return SHOCK_EINVAL;
+    memcpy(m->state[b], s, 5 * m->ng[b] * sizeof(double));
+    return SHOCK_OK;
+}
+
+int shock_multi_upload_last_pressure(shock_multi *m, int b, const double *p)
+{
+    if (bad_block(m, b)) return SHOCK_EINVAL;
+    memcpy(m->plast[b], p, m->ng[b] * sizeof(double));
+    /* the U_RK pressure the next download returns until a step forms one */
+    memcpy(m->state[b] + 5 * m->ng[b], p, m->ng[b] * sizeof(double));
+    return SHOCK_OK;
+}
+
+int shock_multi_download_state(shock_multi *m, int b, double *s)
+{
+    if (bad_block(m, b)) return SHOCK_EINVAL;
+    memcpy(s, m->state[b], 5 * m->ng[b] * sizeof(double));
+    return SHOCK_OK;
+}
+
+int shock_multi_download_pressure(shock_multi *m, int b, double *p)
+{
+    if (bad_block(m, b)) return SHOCK_EINVAL;
+    memcpy(p, m->state[b] + 5 * m->ng[b], m->ng[b] * sizeof(double));
+    return SHOCK_OK;
+}
+
+int shock_multi_set_tau(shock_multi *m, double tau)
+{
+    if (!m || g_ntau >= 256) return SHOCK_EINVAL;
+    g_taus[g_ntau++] = tau;
+    return SHOCK_OK;
+}
+
+int shock_multi_step(shock_multi *m, int n)
+{
+    if (!m) return SHOCK_EINVAL;
+    int nan_step = -1, nan_block = -1;
+    const char *e = getenv("SHOCK_MOCK_NAN");
+    if (e) sscanf(e, "%d %d", &nan_step, &nan_block);
+    for (int s = 0; s < n; s++) {
+        m->steps++;
+        for (int b = 0; b < m->nblocks; b++) {
+            for (size_t o = 0; o < m->ng[b]; o++) {
+                m->state[b][o] += 1e-3 * (b + 1);                              /* rho */
+                m->state[b][5 * m->ng[b] + o] = 2.0 + b + 0.5 * m->steps;      /* p */
+            }
+            if (m->steps == nan_step && b == nan_block) {
+                /* a real point: the first one past the ghost layers */
+                const int g = m->g, *d = m->dims[b];
+                const size_t o = ((size_t)g * d[1] + g) * d[2] + (m->dim == 3 ? g : 0);
+                m->state[b][o] = NAN;
+            }
+        }
+    }
+    return SHOCK_OK;
+}
+
+int shock_multi_check_nan(shock_multi *m, int *bad)
+{
+    if (!m || !bad) return SHOCK_EINVAL;
+    int n = 0;
+    for (int b = 0; b < m->nblocks; b++)
+        for (size_t o = 0; o < m->ng[b]; o++) n += !isfinite(m->state[b][o]);
+    *bad = n;
+    return n ? SHOCK_ENAN : SHOCK_OK;
+}
+
+/* For the harness: block b's geometry from the real library's host set-up,
+ * the number of steps, and the time steps the binding set (the first is
+ * shock_multi_create's). */
+int mock_block_geometry(int b, double *out13)
+{
+    if (!g_last || b < 0 || b >= g_last->nblocks) return -1;
+    memcpy(out13, g_last->geo[b], 13 * g_last->ng[b] * sizeof(double));
+    return 0;
+}
+
+int mock_steps(void) { return g_last ? g_last->steps : -1; }
+
+int mock_taus(double *out, int max)
+{
+    const int n = g_ntau < max ? g_ntau : max;
+    for (int i = 0; i < n; i++) out[i] = g_taus[i];
+    return g_ntau;
+}

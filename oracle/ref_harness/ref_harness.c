@@ -603,6 +603,7 @@ typedef struct {
     const char *division;         /* a .sddc file to read the interfaces from, or NULL */
     int swap;                     /* SHOCK's SwapDivFile for that file: 0 auto, 1 never, 2 always */
     double *comm;                 /* shared: per rank SHOCK's comm_time after the steps */
+    const size_t *out_off_ng;     /* [nblocks] ghosted points of each block (the drop-in run) */
 } mr_job;
 
 static const mr_job *g_job;
@@ -726,10 +727,8 @@ static void mr_interfaces(void)
     for (int c = 0; c < MESHDIMENSIONS; c++) cfg.offset[c] = 0;
 }
 
-static int mr_body(int rank, void *arg)
+static void mr_alloc(void)
 {
-    g_job = (const mr_job *)arg;
-    g_rank_blk = rank;
     for (int i = 0; i < 6; i++) {
         mr_tf[i] = calloc(3, sizeof(int));
         mr_rng[i] = calloc(6, sizeof(cgsize_t));
@@ -738,6 +737,13 @@ static int mr_body(int rank, void *arg)
         mr_rc[i] = calloc(3, sizeof(float));
         mr_ra[i] = calloc(3, sizeof(float));
     }
+}
+
+static int mr_body(int rank, void *arg)
+{
+    g_job = (const mr_job *)arg;
+    g_rank_blk = rank;
+    mr_alloc();
     if (g_job->division) {
         /* the row's block must be the block this rank is given */
         const ref_params *p = &g_job->blk[rank];
@@ -792,11 +798,102 @@ int refmpi_run_file(int nblocks, const ref_params *blk, const int *neigh, const 
     double *shared = mmap(NULL, len * sizeof(double), PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
     if (shared == MAP_FAILED) return -1;
     mr_job job = {nblocks, blk, neigh, trans, tfm, in, nrhs, nsteps, shared, out_off, division, swap,
-                  shared + out_len};
+                  shared + out_len, NULL};
     int rc = shm_run(nblocks, slot_bytes, mr_body, &job);
     memcpy(out, shared, out_len * sizeof(double));
     if (comm_time) memcpy(comm_time, shared + out_len, (size_t)nblocks * sizeof(double));
     munmap(shared, len * sizeof(double));
     return rc;
 }
+
+#ifdef SHOCK_DROPIN
+/*
+ * The drop-in's division mode (shock_b200/dropin/GPU.c with several ranks)
+ * inside SHOCK's own multi-rank set-up, over the library's host test double
+ * (ref_harness/mock_shock.c): each rank runs SHOCK's set-up of its block,
+ * then GPU_Create, nsteps of GPU_CalcRungeKutta + GPU_CheckNAN (tau times
+ * tau_factor before step tau_at), GPU_SyncHost; then changes its U_RK by
+ * (rank + 1) / 4 in rho, GPU_UploadState, one more step, GPU_SyncHost.
+ * Per block at out_off[b]: SHOCK's geometry (13*NG), U_lastStep before
+ * GPU_Create (6*NG: rho,u,v,w,e,p), U_RK after the loop (6*NG), U_RK after
+ * the upload and step (6*NG), the double's geometry of the block from the
+ * library's host set-up (13*NG, written by rank 0).  extra: per rank the
+ * number of steps GPU_CheckNAN reported (nblocks), then the double's step
+ * count and up to 16 time steps it was given.
+ */
+int mock_block_geometry(int b, double *out13);
+int mock_steps(void);
+int mock_taus(double *out, int max);
+
+typedef struct {
+    const mr_job *job;
+    int nsteps, tau_at;
+    double tau_factor;
+    double *extra;
+} dj_job;
+
+static void dj_state(const struct strct_U *U, double *o)
+{
+    const int n = NG;
+    const FLT *f6[6] = {U->rho, U->u, U->v, U->w, U->e, U->p};
+    for (int a = 0; a < 6; a++)
+        for (int q = 0; q < n; q++) o[(size_t)a * n + q] = (double)f6[a][q];
+}
+
+static int dj_body(int rank, void *arg)
+{
+    const dj_job *dj = (const dj_job *)arg;
+    g_job = dj->job;
+    g_rank_blk = rank;
+    mr_alloc();
+    g_iface_hook = mr_interfaces;
+    const double *const *in = g_job->in + 8 * rank;
+    if (ref_init(&g_job->blk[rank], in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7])) return 1;
+    const int n = NG;
+    double *o = g_job->out + g_job->out_off[rank];
+    ref_get_geom(o);
+    dj_state(&U_last, o + 13 * (size_t)n);
+    if (GPU_Create(&cfg, &msh, &U_last, &Qf, 0)) return 2;
+    int nans = 0;
+    for (int it = 0; it < dj->nsteps; it++) {
+        if (it == dj->tau_at) cfg.numericalTau *= dj->tau_factor;
+        GPU_CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh);
+        nans += GPU_CheckNAN(&cfg, &U_rk, &msh);
+    }
+    GPU_SyncHost(&cfg, &U_rk);
+    dj_state(&U_rk, o + 19 * (size_t)n);
+    for (int q = 0; q < n; q++) U_rk.rho[q] += 0.25 * (rank + 1);
+    GPU_UploadState(&cfg, &U_rk);
+    GPU_CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh);
+    GPU_SyncHost(&cfg, &U_rk);
+    dj_state(&U_rk, o + 25 * (size_t)n);
+    dj->extra[rank] = nans;
+    if (rank == 0) {
+        for (int b = 0; b < g_job->nblocks; b++) {
+            const size_t ngb = g_job->out_off_ng[b];
+            if (mock_block_geometry(b, g_job->out + g_job->out_off[b] + 31 * ngb)) return 3;
+        }
+        dj->extra[g_job->nblocks] = mock_steps();
+        mock_taus(dj->extra + g_job->nblocks + 1, 16);
+    }
+    GPU_Destroy();
+    return 0;
+}
+
+int refmpi_dropin_run(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const int *tfm,
+                      const double *const *in, int nsteps, int tau_at, double tau_factor, double *out,
+                      const size_t *out_off, const size_t *ng, size_t out_len, double *extra, size_t slot_bytes)
+{
+    const size_t len = out_len + (size_t)nblocks + 17;
+    double *shared = mmap(NULL, len * sizeof(double), PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
+    if (shared == MAP_FAILED) return -1;
+    mr_job job = {nblocks, blk, neigh, trans, tfm, in, 0, nsteps, shared, out_off, NULL, 0, shared + out_len, ng};
+    dj_job dj = {&job, nsteps, tau_at, tau_factor, shared + out_len};
+    int rc = shm_run(nblocks, slot_bytes, dj_body, &dj);
+    memcpy(out, shared, out_len * sizeof(double));
+    memcpy(extra, shared + out_len, ((size_t)nblocks + 17) * sizeof(double));
+    munmap(shared, len * sizeof(double));
+    return rc;
+}
+#endif
 #endif

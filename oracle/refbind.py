@@ -498,3 +498,68 @@ def config_import(path) -> dict:
         if r.returncode == 0 and line.startswith("CONFIG "):
             return json.loads(line[7:])
     raise RuntimeError(f"SHOCK's ConfigImport ended with {r.returncode}: {(r.stdout + r.stderr)[-400:]}")
+
+
+def dropin_multirank_available(order: int, dim: int) -> bool:
+    return os.path.exists(os.path.join(HERE, "_ref", f"libshockdropinmpi_w{order}_{dim}d.so"))
+
+
+def _dropin_multirank_worker(division, nsteps, tau_at, tau_factor, nan):
+    case = division.case
+    os.environ["SHOCK_B200_LIB"] = os.path.join(os.path.dirname(HERE), "shock_b200", "libshock_b200.so")
+    if nan is not None:
+        os.environ["SHOCK_MOCK_NAN"] = f"{nan[0]} {nan[1]}"
+    lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockdropinmpi_w{case.order}_{case.dim}d.so"), mode=os.RTLD_LOCAL)
+    lib.refmpi_dropin_run.restype = C.c_int
+    nb = len(division.blocks)
+    g2 = case.order + 1
+    shapes = [(b.ni + g2, b.nj + g2, (b.nk + g2) if case.dim == 3 else 1) for b in division.blocks]
+    ng = np.array([s[0] * s[1] * s[2] for s in shapes], dtype=np.uint64)
+    off = np.zeros(nb, dtype=np.uint64)
+    for b in range(1, nb):
+        off[b] = off[b - 1] + 44 * ng[b - 1]
+    total = int(off[-1] + 44 * ng[-1])
+    params = (RefParams * nb)(*[_ref_params(b) for b in division.blocks])
+    f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
+    keep = [[f(a) for a in b.real_fields()] for b in division.blocks]
+    ptrs = (C.POINTER(C.c_double) * (8 * nb))(*[_ptr(a) for fl in keep for a in fl])
+    neigh = np.ascontiguousarray(division.neighbour, dtype=np.int32)
+    trans = np.ascontiguousarray(division.translation, dtype=np.float32)
+    tfm = np.ascontiguousarray(division.transform, dtype=np.int32)
+    out = np.zeros(total)
+    extra = np.zeros(nb + 17)
+    face = max(max(s[0] * s[1], s[1] * s[2], s[0] * s[2]) for s in shapes)
+    nr = [b.real_points for b in division.blocks]
+    slot = max(13 * (g2 // 2) * face * 8, max(8 * (8 * r + 6 * int(n)) for r, n in zip(nr, ng)))
+    rc = lib.refmpi_dropin_run(C.c_int(nb), params, neigh.ctypes.data_as(C.POINTER(C.c_int)),
+                               trans.ctypes.data_as(C.POINTER(C.c_float)), tfm.ctypes.data_as(C.POINTER(C.c_int)),
+                               ptrs, C.c_int(nsteps), C.c_int(tau_at), C.c_double(tau_factor), _ptr(out),
+                               off.ctypes.data_as(C.POINTER(C.c_size_t)), ng.ctypes.data_as(C.POINTER(C.c_size_t)),
+                               C.c_size_t(total), _ptr(extra), C.c_size_t(slot))
+    if rc != 0:
+        raise RuntimeError(f"drop-in multi-rank run failed ({rc})")
+    res = []
+    for b in range(nb):
+        o, n = int(off[b]), int(ng[b])
+        blk = out[o:o + 44 * n]
+        res.append({"shock_geometry": blk[:13 * n].reshape((13,) + shapes[b]),
+                    "initial": blk[13 * n:19 * n].reshape((6,) + shapes[b]),
+                    "after_steps": blk[19 * n:25 * n].reshape((6,) + shapes[b]),
+                    "after_upload_step": blk[25 * n:31 * n].reshape((6,) + shapes[b]),
+                    "library_geometry": blk[31 * n:44 * n].reshape((13,) + shapes[b]),
+                    "nan_steps": int(extra[b])})
+    steps = int(extra[nb])
+    taus = [float(t) for t in extra[nb + 1:nb + 17] if t != 0.0]
+    return res, steps, taus
+
+
+def run_dropin_multirank(division, nsteps: int, tau_at: int = -1, tau_factor: float = 1.0, nan=None):
+    """The drop-in binding (shock_b200/dropin/GPU.c) in its division mode,
+    inside SHOCK's own multi-rank set-up of the division, over the library's
+    host test double (ref_harness/mock_shock.c); see refmpi_dropin_run.
+    nan = (step, block) plants a non-finite density in the double.  Returns
+    (per block dict, the double's step count, the time steps it was given)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        return pool.apply(_dropin_multirank_worker, (division, nsteps, tau_at, tau_factor, nan))

@@ -1326,6 +1326,18 @@ int shock_multi_upload_state(shock_multi *m, int block, const double *prim5)
     return shock_upload_state(m->blk[block], prim5);
 }
 
+int shock_multi_download_pressure(shock_multi *m, int block, double *p)
+{
+    if (!m || block < 0 || block >= (int)m->blk.size()) return fail(SHOCK_EINVAL, "bad block");
+    return shock_download_pressure(m->blk[block], p);
+}
+
+int shock_multi_upload_last_pressure(shock_multi *m, int block, const double *p)
+{
+    if (!m || block < 0 || block >= (int)m->blk.size()) return fail(SHOCK_EINVAL, "bad block");
+    return shock_upload_last_pressure(m->blk[block], p);
+}
+
 int shock_multi_set_tau(shock_multi *m, double tau)
 {
     if (!m) return fail(SHOCK_EINVAL, "null argument");

@@ -27,6 +27,20 @@
  *     rho_inflow, p_inflow, p_outflow and the inflow velocity.
  * Faces of any other kind (moving walls) are rejected by the library with
  * SHOCK_EINVAL.
+ *
+ * With more than one rank (config->MPI_size > 1) the ranks' blocks are the
+ * division of SHOCK's .sddc file, and rank 0 runs all of them on its device
+ * (shock_multi_*: the interfaces exchanged on the device before every
+ * stage, as TransferFlowParameterWithGhosts exchanges them between ranks).
+ * Each rank describes its block as loadFile and SHOCK's set-up left it
+ * (src/Load.c:355-400, check_TransformationMatrix): per face the rank
+ * across it, the Transform and the float32 Translation, or the face type.
+ * Every GPU_* call is then collective: GPU_Create sends each block's
+ * description, real-point fields and U_lastStep state to rank 0,
+ * GPU_CalcRungeKutta steps the division on rank 0, GPU_CheckNAN shares its
+ * count, GPU_SyncHost sends each block's U_RK (and p) back to its rank and
+ * GPU_UploadState each rank's to rank 0.  Only rank 0 uses a GPU.  Not
+ * with the manufactured solution (single-block in the library).
  */
 #include <stdio.h>
 #include <stdlib.h>
@@ -42,6 +56,10 @@
 #endif
 
 static shock_ctx *g_ctx;
+static shock_multi *g_multi;   /* division mode, rank 0 */
+static int g_division;         /* MPI_size > 1: every GPU_* call is collective */
+static size_t *g_block_ng;     /* rank 0: ghosted points of every rank's block */
+static double *g_block_buf;    /* rank 0: 6*NG doubles of the largest block */
 static int g_host_behind;   /* the device state is newer than the host U_RK */
 static double *g_buf;       /* 5*NG doubles */
 static double g_tau;        /* the numericalTau the device steps with */
@@ -78,9 +96,66 @@ static void real_fortran(const struct strct_configuration *c, const FLT *src, do
                 dst[n++] = (double)src[(size_t)i * nj * nk + (size_t)j * nk + k];
 }
 
+/* The SHOCK_BC_* type of face f (Left, Right, Bottom, Top, Behind, InFront)
+ * from the BC name src/Load.c:46-97 assigned and the inflow/outflow option
+ * of config.ini: -1 for an inflow or outflow face without an option the
+ * library has, SHOCK_BC_AUTO for any other name (a manufactured-solution
+ * face; the library rejects it on a run without one). */
+static int face_type(const struct strct_configuration *c, int f)
+{
+    const char *face[6] = {c->BC_Left, c->BC_Right, c->BC_Bottom, c->BC_Top, c->BC_Behind, c->BC_InFront};
+    if (strcmp(face[f], c->BCWallViscous) == 0) return SHOCK_BC_WALL_VISCOUS;
+    if (strcmp(face[f], c->BCWallInviscid) == 0) return SHOCK_BC_WALL_INVISCID;
+    if (strcmp(face[f], c->BCFarfield) == 0) return SHOCK_BC_FARFIELD;
+    if (strcmp(face[f], c->BCWallViscousIsothermal) == 0) return SHOCK_BC_WALL_ISOTHERMAL;
+    if (strncmp(face[f], c->BCInflow, strlen(c->BCInflow)) == 0)   /* BCInflow, -Subsonic, -Supersonic */
+        return c->flag_BC_option_inflow_normal_super == 1 ? SHOCK_BC_INFLOW_SUPERSONIC
+             : c->flag_BC_option_inflow_normal_sub == 1 ? SHOCK_BC_INFLOW_SUBSONIC
+             : c->flag_BC_option_inflow_riemann_sub == 1 ? SHOCK_BC_INFLOW_RIEMANN
+             : c->flag_BC_option_inflow_isentrop_sub == 1 ? SHOCK_BC_INFLOW_ISENTROPIC : -1;
+    if (strncmp(face[f], c->BCOutflow, strlen(c->BCOutflow)) == 0)   /* BCOutflow, -Subsonic */
+        return c->flag_BC_option_outflow_normal_sub == 1 ? SHOCK_BC_OUTFLOW_SUBSONIC
+             : c->flag_BC_option_outflow_riemann_sub == 1 ? SHOCK_BC_OUTFLOW_RIEMANN
+             : c->flag_BC_option_outflow_rudy_sub == 1 ? SHOCK_BC_OUTFLOW_RUDY : -1;
+    return SHOCK_BC_AUTO;
+}
+
+/* The parameters every block shares, from the configuration. */
+static void common_params(const struct strct_configuration *c, shock_params *sp)
+{
+    memset(sp, 0, sizeof *sp);
+    sp->dim = MESHDIMENSIONS;
+    sp->order = SPACEORDER;
+    sp->time_order = c->int_TimeOrder;
+    sp->tau = c->numericalTau;
+    sp->mach = c->machNumber;
+    sp->reynolds = c->reynoldsNumber;
+    sp->prandtl = c->prandtlNumber;
+    sp->gamma = c->gammaNumber;
+    sp->gas_r = c->gasConstantNumber;
+    sp->t0 = c->T0_dim;
+    sp->l0 = c->L0_dim;
+    sp->inviscid = c->flag_Inviscid == 1;
+    sp->mms = c->flag_ManufacturedSolution == 1;
+    sp->t_wall = c->T_wall;
+    sp->rho_inflow = c->rho_inflow;
+    sp->p_inflow = c->p_inflow;
+    sp->p_outflow = c->p_out;
+    sp->u_inflow[0] = c->u_inflow;
+    sp->u_inflow[1] = c->v_inflow;
+    sp->u_inflow[2] = c->w_inflow;
+    const char *prec = getenv("SHOCK_B200_PRECISION");
+    sp->precision = (prec && strcmp(prec, "mixed") == 0) ? SHOCK_MIXED : SHOCK_FP64;
+    sp->zeta_fix = 0;
+}
+
+static int create_division(struct strct_configuration *c, struct strct_mesh *m, struct strct_U *U_lastStep,
+                           int device);
+
 int GPU_Create(struct strct_configuration *c, struct strct_mesh *m, struct strct_U *U_lastStep,
                struct strct_Flux *Q, int device)
 {
+    if (c->MPI_size > 1) return create_division(c, m, U_lastStep, device);
     shock_params sp;
     memset(&sp, 0, sizeof sp);
     sp.dim = MESHDIMENSIONS;
@@ -103,24 +178,8 @@ int GPU_Create(struct strct_configuration *c, struct strct_mesh *m, struct strct
     sp.periodic[1] = self_periodic(c, c->InterfaceNeighbourBottom, c->InterfaceNeighbourTop, 1, &sp.period[1]);
     if (MESHDIMENSIONS == 3)
         sp.periodic[2] = self_periodic(c, c->InterfaceNeighbourBehind, c->InterfaceNeighbourInFront, 2, &sp.period[2]);
-    /* faces that are not interfaces: the BC names src/Load.c:46-97 assigned */
-    const char *face[6] = {c->BC_Left, c->BC_Right, c->BC_Bottom, c->BC_Top, c->BC_Behind, c->BC_InFront};
-    for (int f = 0; f < 2 * MESHDIMENSIONS; f++) {
-        if (sp.periodic[f / 2]) continue;
-        if (strcmp(face[f], c->BCWallViscous) == 0) sp.bc[f] = SHOCK_BC_WALL_VISCOUS;
-        else if (strcmp(face[f], c->BCWallInviscid) == 0) sp.bc[f] = SHOCK_BC_WALL_INVISCID;
-        else if (strcmp(face[f], c->BCFarfield) == 0) sp.bc[f] = SHOCK_BC_FARFIELD;
-        else if (strcmp(face[f], c->BCWallViscousIsothermal) == 0) sp.bc[f] = SHOCK_BC_WALL_ISOTHERMAL;
-        else if (strncmp(face[f], c->BCInflow, strlen(c->BCInflow)) == 0)   /* BCInflow, -Subsonic, -Supersonic */
-            sp.bc[f] = c->flag_BC_option_inflow_normal_super == 1 ? SHOCK_BC_INFLOW_SUPERSONIC
-                     : c->flag_BC_option_inflow_normal_sub == 1 ? SHOCK_BC_INFLOW_SUBSONIC
-                     : c->flag_BC_option_inflow_riemann_sub == 1 ? SHOCK_BC_INFLOW_RIEMANN
-                     : c->flag_BC_option_inflow_isentrop_sub == 1 ? SHOCK_BC_INFLOW_ISENTROPIC : -1;
-        else if (strncmp(face[f], c->BCOutflow, strlen(c->BCOutflow)) == 0)   /* BCOutflow, -Subsonic */
-            sp.bc[f] = c->flag_BC_option_outflow_normal_sub == 1 ? SHOCK_BC_OUTFLOW_SUBSONIC
-                     : c->flag_BC_option_outflow_riemann_sub == 1 ? SHOCK_BC_OUTFLOW_RIEMANN
-                     : c->flag_BC_option_outflow_rudy_sub == 1 ? SHOCK_BC_OUTFLOW_RUDY : -1;
-    }
+    for (int f = 0; f < 2 * MESHDIMENSIONS; f++)
+        if (!sp.periodic[f / 2]) sp.bc[f] = face_type(c, f);
     sp.t_wall = c->T_wall;
     sp.rho_inflow = c->rho_inflow;
     sp.p_inflow = c->p_inflow;
@@ -170,11 +229,241 @@ int GPU_Create(struct strct_configuration *c, struct strct_mesh *m, struct strct
     return shock_upload_state(g_ctx, g_buf);
 }
 
+/* ---- division mode: every rank's block on rank 0's device ---- */
+
+enum { TAG_DESC = 29101, TAG_FIELDS, TAG_STATE_UP, TAG_STATE_DOWN };
+#define DESC_INTS (3 + 6 + 6 + 18)
+
+static void wait_all(int n, MPI_Request *r)
+{
+    MPI_Status st[4];
+    MPI_Waitall(n, r, st);
+}
+
+/* rank 0 sends 6*ng doubles to rank r, or receives them from it */
+static void exchange_block(struct strct_configuration *c, int r, double *buf, size_t ng, int tag, int send)
+{
+    MPI_Request q;
+    if (send)
+        MPI_Isend(buf, (int)(6 * ng), MPI_DOUBLE, r, tag, c->MPI_comm, &q);
+    else
+        MPI_Irecv(buf, (int)(6 * ng), MPI_DOUBLE, r, tag, c->MPI_comm, &q);
+    wait_all(1, &q);
+}
+
+/* U_RK (or U_lastStep) of this rank as 6*NG doubles: rho,u,v,w,e, then p */
+static void pack_state(const struct strct_configuration *c, const struct strct_U *U, double *buf)
+{
+    const size_t ng = ghosted_points(c);
+    const FLT *s6[6] = {U->rho, U->u, U->v, U->w, U->e, U->p};
+    for (int f = 0; f < 6; f++)
+        for (size_t o = 0; o < ng; o++) buf[f * ng + o] = (double)s6[f][o];
+}
+
+static void unpack_state(const struct strct_configuration *c, const double *buf, struct strct_U *U)
+{
+    const size_t ng = ghosted_points(c);
+    FLT *d6[6] = {U->rho, U->u, U->v, U->w, U->e, U->p};
+    for (int f = 0; f < 6; f++)
+        for (size_t o = 0; o < ng; o++) d6[f][o] = (FLT)buf[f * ng + o];
+}
+
+/* This rank's block as loadFile and the set-up left it: sizes, then per face
+ * the rank across it (-1: none), the face type (interfaces: SHOCK_BC_AUTO),
+ * the Transform; and the Translations. */
+static void describe_block(const struct strct_configuration *c, int desc[DESC_INTS], float tr[18])
+{
+    const int side[6] = {c->InterfaceNeighbourLeft, c->InterfaceNeighbourRight, c->InterfaceNeighbourBottom,
+                         c->InterfaceNeighbourTop, c->InterfaceNeighbourBehind, c->InterfaceNeighbourInFront};
+    memset(desc, 0, DESC_INTS * sizeof(int));
+    memset(tr, 0, 18 * sizeof(float));
+    desc[0] = c->int_iEndReal - c->int_iStartReal + 1;
+    desc[1] = c->int_jEndReal - c->int_jStartReal + 1;
+    desc[2] = c->int_kEndReal - c->int_kStartReal + 1;
+    for (int f = 0; f < 6; f++) {
+        int *nb = desc + 3 + f, *bc = desc + 9 + f, *T = desc + 15 + 3 * f;
+        *nb = -1;
+        if (f >= 2 * MESHDIMENSIONS) continue;
+        const int ii = side[f];
+        if (ii == NO_NEIGHBOUR) {
+            *bc = face_type(c, f);
+            continue;
+        }
+        *nb = c->MPI_rankNeighbours[ii];
+        for (int a = 0; a < MESHDIMENSIONS; a++) T[a] = c->TransformMatrixOfInterface[ii][a];
+        for (int a = 0; a < 3; a++) tr[3 * f + a] = c->Translation[ii][a];
+    }
+}
+
+static int create_division(struct strct_configuration *c, struct strct_mesh *m, struct strct_U *U_lastStep,
+                           int device)
+{
+    const int P = c->MPI_size, me = c->MPI_rank;
+    const size_t ng = ghosted_points(c);
+    int desc[DESC_INTS];
+    float tr[18];
+    describe_block(c, desc, tr);
+    const size_t nr = (size_t)desc[0] * desc[1] * desc[2];
+    /* fields: x,y,z,u,v,w,p,rho real points (Fortran order), then the
+       U_lastStep state (6*NG) SHOCK's set-up left */
+    double *mine = malloc((8 * nr + 6 * ng) * sizeof(double));
+    const FLT *src[8] = {m->x, m->y, m->z, U_lastStep->u, U_lastStep->v, U_lastStep->w, U_lastStep->p,
+                         U_lastStep->rho};
+    for (int f = 0; f < 8; f++) real_fortran(c, src[f], mine + f * nr);
+    pack_state(c, U_lastStep, mine + 8 * nr);
+    g_division = 1;
+    g_tau = c->numericalTau;
+    g_host_behind = 0;
+    g_buf = malloc(6 * ng * sizeof(double));
+    int rc = 0;
+    if (me != 0) {
+        MPI_Request q[3];
+        MPI_Isend(desc, DESC_INTS, MPI_INT, 0, TAG_DESC, c->MPI_comm, &q[0]);
+        MPI_Isend(tr, 18, MPI_FLOAT, 0, TAG_DESC, c->MPI_comm, &q[1]);
+        MPI_Isend(mine, (int)(8 * nr + 6 * ng), MPI_DOUBLE, 0, TAG_FIELDS, c->MPI_comm, &q[2]);
+        wait_all(3, q);
+    } else {
+        const int g = (SPACEORDER + 1) / 2;
+        shock_params sp;
+        common_params(c, &sp);
+        shock_block *blk = calloc((size_t)P, sizeof(shock_block));
+        double **data = calloc((size_t)P, sizeof(double *));
+        g_block_ng = calloc((size_t)P, sizeof(size_t));
+        size_t most = 0;
+        for (int r = 0; r < P; r++) {
+            int d[DESC_INTS];
+            float t[18];
+            if (r == 0) {
+                memcpy(d, desc, sizeof d);
+                memcpy(t, tr, sizeof t);
+            } else {
+                MPI_Request q[2];
+                MPI_Irecv(d, DESC_INTS, MPI_INT, r, TAG_DESC, c->MPI_comm, &q[0]);
+                MPI_Irecv(t, 18, MPI_FLOAT, r, TAG_DESC, c->MPI_comm, &q[1]);
+                wait_all(2, q);
+            }
+            const size_t n = (size_t)d[0] * d[1] * d[2];
+            const size_t gn = (size_t)(d[0] + 2 * g) * (d[1] + 2 * g) * (MESHDIMENSIONS == 3 ? d[2] + 2 * g : 1);
+            g_block_ng[r] = gn;
+            if (gn > most) most = gn;
+            if (r == 0) {
+                data[r] = mine;
+            } else {
+                data[r] = malloc((8 * n + 6 * gn) * sizeof(double));
+                MPI_Request q;
+                MPI_Irecv(data[r], (int)(8 * n + 6 * gn), MPI_DOUBLE, r, TAG_FIELDS, c->MPI_comm, &q);
+                wait_all(1, &q);
+            }
+            shock_block *B = &blk[r];
+            B->ni = d[0];
+            B->nj = d[1];
+            B->nk = d[2];
+            double *a = data[r];
+            B->x = a; B->y = a + n; B->z = a + 2 * n; B->u = a + 3 * n; B->v = a + 4 * n; B->w = a + 5 * n;
+            B->p = a + 6 * n; B->rho = a + 7 * n;
+            for (int f = 0; f < 6; f++) {
+                B->neighbour[f] = d[3 + f];
+                B->bc[f] = d[9 + f];
+                for (int a3 = 0; a3 < 3; a3++) {
+                    B->transform[f][a3] = d[15 + 3 * f + a3];
+                    B->translation[f][a3] = t[3 * f + a3];
+                }
+            }
+        }
+        rc = shock_multi_create(&sp, P, blk, device, &g_multi);
+        /* start every block from the state SHOCK's set-up left (e as it
+           formed it), and with U_lastStep's p for the Rudy faces */
+        for (int r = 0; r < P && !rc; r++) {
+            const size_t n = (size_t)blk[r].ni * blk[r].nj * blk[r].nk, gn = g_block_ng[r];
+            const double *s6 = data[r] + 8 * n;
+            rc = shock_multi_upload_state(g_multi, r, s6);
+            if (!rc) rc = shock_multi_upload_last_pressure(g_multi, r, s6 + 5 * gn);
+        }
+        g_block_buf = malloc(6 * most * sizeof(double));
+        for (int r = 1; r < P; r++) free(data[r]);
+        free(data);
+        free(blk);
+    }
+    free(mine);
+    /* every rank returns rank 0's verdict */
+    MPI_Bcast(&rc, 1, MPI_INT, 0, c->MPI_comm);
+    return rc;
+}
+
+static void division_step(struct strct_configuration *c)
+{
+    if (c->MPI_rank == 0) {
+        if ((double)c->numericalTau != g_tau) {
+            int rt = shock_multi_set_tau(g_multi, (double)c->numericalTau);
+            if (rt) fail("shock_multi_set_tau", rt);
+        }
+        int rc = shock_multi_step(g_multi, 1);
+        if (rc) fail("shock_multi_step", rc);
+    }
+    g_tau = (double)c->numericalTau;
+    g_host_behind = 1;
+}
+
+static int division_nan(struct strct_configuration *c)
+{
+    int bad = 0;
+    if (c->MPI_rank == 0) {
+        int rc = shock_multi_check_nan(g_multi, &bad);
+        if (rc && rc != SHOCK_ENAN) fail("shock_multi_check_nan", rc);
+    }
+    MPI_Bcast(&bad, 1, MPI_INT, 0, c->MPI_comm);
+    return bad;
+}
+
+static void division_sync(struct strct_configuration *c, struct strct_U *U_RK)
+{
+    if (c->MPI_rank != 0) {
+        exchange_block(c, 0, g_buf, ghosted_points(c), TAG_STATE_DOWN, 0);
+        unpack_state(c, g_buf, U_RK);
+        return;
+    }
+    for (int r = 0; r < c->MPI_size; r++) {
+        const size_t gn = g_block_ng[r];
+        double *b = r == 0 ? g_buf : g_block_buf;
+        int rc = shock_multi_download_state(g_multi, r, b);
+        if (!rc) rc = shock_multi_download_pressure(g_multi, r, b + 5 * gn);
+        if (rc) fail("shock_multi_download_state", rc);
+        if (r == 0)
+            unpack_state(c, b, U_RK);
+        else
+            exchange_block(c, r, b, gn, TAG_STATE_DOWN, 1);
+    }
+}
+
+static void division_upload(struct strct_configuration *c, struct strct_U *U_RK)
+{
+    if (c->MPI_rank != 0) {
+        pack_state(c, U_RK, g_buf);
+        exchange_block(c, 0, g_buf, ghosted_points(c), TAG_STATE_UP, 1);
+        return;
+    }
+    for (int r = 0; r < c->MPI_size; r++) {
+        const size_t gn = g_block_ng[r];
+        double *b = r == 0 ? g_buf : g_block_buf;
+        if (r == 0)
+            pack_state(c, U_RK, b);
+        else
+            exchange_block(c, r, b, gn, TAG_STATE_UP, 0);
+        int rc = shock_multi_upload_state(g_multi, r, b);
+        if (!rc) rc = shock_multi_upload_last_pressure(g_multi, r, b + 5 * gn);
+        if (rc) fail("shock_multi_upload_state", rc);
+    }
+}
+
 void GPU_CalcRungeKutta(struct strct_configuration *c, struct strct_mesh *m, struct strct_U *U_lastStep,
                         struct strct_U *U_RK, struct strct_Flux *Q, struct strct_Flux *Q_sum,
                         struct strct_Flux *Flux, struct strct_Flux *Flux_PlusHalf)
 {
     (void)m; (void)U_lastStep; (void)U_RK; (void)Q; (void)Q_sum; (void)Flux; (void)Flux_PlusHalf;
+    if (g_division) {
+        division_step(c);
+        return;
+    }
     /* SHOCK's time loop changes numericalTau after a NaN reset and in its
      * accelerator (src/SHOCK.c:590,638,654); CalcRungeKutta reads it every
      * step */
@@ -191,6 +480,11 @@ void GPU_CalcRungeKutta(struct strct_configuration *c, struct strct_mesh *m, str
 int GPU_CheckNAN(struct strct_configuration *c, struct strct_U *U_RK, struct strct_mesh *m)
 {
     int bad = 0;
+    if (g_division) {
+        if (!division_nan(c)) return 0;
+        GPU_SyncHost(c, U_RK);
+        return checkNAN(c, U_RK, m);
+    }
     int rc = shock_check_nan(g_ctx, &bad);
     if (rc && rc != SHOCK_ENAN) fail("shock_check_nan", rc);
     /* every rank learns whether any rank saw one, as checkNAN's own
@@ -209,6 +503,11 @@ int GPU_CheckNAN(struct strct_configuration *c, struct strct_U *U_RK, struct str
 void GPU_SyncHost(struct strct_configuration *c, struct strct_U *U_RK)
 {
     if (!g_host_behind) return;
+    if (g_division) {
+        division_sync(c, U_RK);
+        g_host_behind = 0;
+        return;
+    }
     const size_t ng = ghosted_points(c);
     int rc = shock_download_state(g_ctx, g_buf, 0);
     if (rc) fail("shock_download_state", rc);
@@ -225,6 +524,11 @@ void GPU_SyncHost(struct strct_configuration *c, struct strct_U *U_RK)
 
 void GPU_UploadState(struct strct_configuration *c, struct strct_U *U_RK)
 {
+    if (g_division) {
+        division_upload(c, U_RK);
+        g_host_behind = 0;
+        return;
+    }
     const size_t ng = ghosted_points(c);
     const FLT *srcf[5] = {U_RK->rho, U_RK->u, U_RK->v, U_RK->w, U_RK->e};
     for (int f = 0; f < 5; f++)
@@ -243,6 +547,13 @@ void GPU_Destroy(void)
 {
     if (g_ctx) shock_destroy(g_ctx);
     g_ctx = NULL;
+    if (g_multi) shock_multi_destroy(g_multi);
+    g_multi = NULL;
+    g_division = 0;
     free(g_buf);
     g_buf = NULL;
+    free(g_block_ng);
+    g_block_ng = NULL;
+    free(g_block_buf);
+    g_block_buf = NULL;
 }

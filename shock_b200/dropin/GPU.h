@@ -15,6 +15,12 @@
  *   - before the host reads U_RK or U_lastStep (backups, sampling, export:
  *     src/SHOCK.c:663-717): GPU_SyncHost(&config, &U_RK);
  * and calls GPU_Destroy() at the end of the run.
+ *
+ * Run on several MPI ranks (a .sddc division), every GPU_* call is
+ * collective: rank 0 runs all ranks' blocks on its device (the interfaces
+ * exchanged on the device), and the other ranks send and receive their
+ * blocks' data through MPI; only rank 0 uses a GPU.  The manufactured
+ * solution is single-rank.
  */
 #ifndef SHOCK_GPU_H
 #define SHOCK_GPU_H
