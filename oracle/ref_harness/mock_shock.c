@@ -7,8 +7,9 @@
  * checks the division and whose geometry is kept for the test to compare
  * with SHOCK's; a "step" adds (block + 1) * 1e-3 to every density and
  * remembers tau; $SHOCK_MOCK_NAN = "step block" plants a non-finite
- * density.  Test infrastructure for the reference build under oracle/_ref;
- * the single-block entry points the binding also links are stubs that fail.
+ * density.  The single-block entry points record what shock_create is
+ * given (mock_params) and accept the rest.  Test infrastructure for the
+ * reference build under oracle/_ref.
  */
 #include <dlfcn.h>
 #include <math.h>
@@ -33,20 +34,38 @@ static int g_ntau;
 
 const char *shock_last_error(void) { return "mock"; }
 
-#define MOCK_FAIL(name, ...) \
-    int name(__VA_ARGS__) { return SHOCK_EINVAL; }
-MOCK_FAIL(shock_create, const shock_params *p, const double *x, const double *y, const double *z, const double *u,
-          const double *v, const double *w, const double *pr, const double *rho, int device, shock_ctx **out)
-MOCK_FAIL(shock_set_dirichlet, shock_ctx *c, const double *e)
-MOCK_FAIL(shock_set_source, shock_ctx *c, const double *s)
-MOCK_FAIL(shock_upload_state, shock_ctx *c, const double *s)
-MOCK_FAIL(shock_upload_last_pressure, shock_ctx *c, const double *p)
-MOCK_FAIL(shock_set_tau, shock_ctx *c, double t)
-MOCK_FAIL(shock_step, shock_ctx *c, int n)
-MOCK_FAIL(shock_check_nan, shock_ctx *c, int *b)
-MOCK_FAIL(shock_download_state, shock_ctx *c, double *s, int w)
-MOCK_FAIL(shock_download_pressure, shock_ctx *c, double *p)
-MOCK_FAIL(shock_destroy, shock_ctx *c)
+static shock_params g_single;
+static int g_single_created;
+
+int shock_create(const shock_params *p, const double *x, const double *y, const double *z, const double *u,
+                 const double *v, const double *w, const double *pr, const double *rho, int device, shock_ctx **out)
+{
+    (void)x; (void)y; (void)z; (void)u; (void)v; (void)w; (void)pr; (void)rho; (void)device;
+    g_single = *p;
+    g_single_created = 1;
+    *out = (shock_ctx *)&g_single;   /* never dereferenced */
+    return SHOCK_OK;
+}
+
+/* what the binding gave shock_create; 0 when it was called */
+int mock_params(shock_params *out)
+{
+    *out = g_single;
+    return g_single_created ? 0 : -1;
+}
+
+#define MOCK_OK(name, ...) \
+    int name(__VA_ARGS__) { return SHOCK_OK; }
+MOCK_OK(shock_set_dirichlet, shock_ctx *c, const double *e)
+MOCK_OK(shock_set_source, shock_ctx *c, const double *s)
+MOCK_OK(shock_upload_state, shock_ctx *c, const double *s)
+MOCK_OK(shock_upload_last_pressure, shock_ctx *c, const double *p)
+MOCK_OK(shock_set_tau, shock_ctx *c, double t)
+MOCK_OK(shock_step, shock_ctx *c, int n)
+MOCK_OK(shock_check_nan, shock_ctx *c, int *b)
+MOCK_OK(shock_download_state, shock_ctx *c, double *s, int w)
+MOCK_OK(shock_download_pressure, shock_ctx *c, double *p)
+MOCK_OK(shock_destroy, shock_ctx *c)
 
 int shock_multi_create(const shock_params *p, int nblocks, const shock_block *blocks, int device, shock_multi **out)
 {

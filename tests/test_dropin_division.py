@@ -70,3 +70,47 @@ def test_dropin_division_nan_on_every_rank():
     # marked the point (1e6, src/Functions.c:5443); the others stay finite
     assert (res[6]["after_steps"][0] == 1e6).sum() == 1
     assert all(np.isfinite(r["after_steps"][0]).all() for r in res)
+
+
+# One rank: the block GPU_Create describes to shock_create from SHOCK's
+# set-up (its BC names and config.ini options, its periodic interfaces, its
+# parameters), over the same test double.
+SINGLE = {
+    "tgv16_w5_periodic": lambda: cases.taylor_green(16, order=5),
+    "channel3d_w5_viscous_walls": lambda: cases.channel(3, 5, (12, 10, 12)),
+    "channel2d_w9_isothermal": lambda: cases.channel(2, 9, (16, 14, 1), bc="wall_isothermal", t_wall=1.3),
+    "channel2d_w5_slip_box": lambda: cases.channel(2, 5, (16, 14, 1), bc="wall_inviscid", walls_i=True),
+    "channel2d_w5_farfield": lambda: cases.channel(2, 5, (16, 14, 1), bc="farfield"),
+    "duct2d_w5_riemann_rudy": lambda: cases.duct(2, 5, (20, 12, 1), inflow="inflow_riemann", outflow="outflow_rudy",
+                                                 walls="wall_viscous"),
+    "duct2d_w9_isentropic_riemann": lambda: cases.duct(2, 9, (20, 14, 1), inflow="inflow_isentropic",
+                                                       outflow="outflow_riemann"),
+    "duct3d_w5_supersonic_subsonic": lambda: cases.duct(3, 5, (14, 10, 10), inflow="inflow_supersonic",
+                                                        outflow="outflow_subsonic", mach=1.5),
+}
+
+
+@pytest.mark.parametrize("name", sorted(SINGLE))
+def test_dropin_single_block_description(name):
+    import ctypes as C
+
+    import shock_b200
+    from refbind import RefSolver
+    case = SINGLE[name]()
+    try:
+        ref = RefSolver(case, _lib="libshockdropinmock")
+    except FileNotFoundError:
+        pytest.skip("drop-in test double build absent (make -C oracle with the reference sources)")
+    assert ref.lib.ref_dropin_create(0) == 0
+    p = shock_b200.Params()
+    assert ref.lib.mock_params(C.byref(p)) == 0
+    want = shock_b200.params_from_case(case)
+    for k in ("dim", "order", "ni", "nj", "nk", "time_order", "tau", "mach", "reynolds", "prandtl", "gamma", "gas_r",
+              "t0", "l0", "inviscid", "mms", "t_wall", "rho_inflow", "p_inflow", "p_outflow"):
+        assert getattr(p, k) == getattr(want, k), (name, k, getattr(p, k), getattr(want, k))
+    assert list(p.bc) == list(want.bc), (name, list(p.bc), list(want.bc))
+    assert list(p.periodic) == list(want.periodic), name
+    # the period travels as the float32 Translation of the .sddc row
+    assert [p.period[a] for a in range(3) if want.periodic[a]] == \
+        [float(np.float32(want.period[a])) for a in range(3) if want.periodic[a]], name
+    assert list(p.u_inflow) == list(want.u_inflow), name
