@@ -8,7 +8,8 @@
  * with SHOCK's; a "step" adds (block + 1) * 1e-3 to every density and
  * remembers tau; $SHOCK_MOCK_NAN = "step block" plants a non-finite
  * density.  The single-block entry points record what shock_create is
- * given (mock_params) and accept the rest.  Test infrastructure for the
+ * given (mock_params), record probe values mock_value forms after every
+ * step, and accept the rest.  Test infrastructure for the
  * reference build under oracle/_ref.
  */
 #include <dlfcn.h>
@@ -35,7 +36,11 @@ static int g_ntau;
 const char *shock_last_error(void) { return "mock"; }
 
 static shock_params g_single;
-static int g_single_created;
+static int g_single_created, g_single_steps, g_nprobe;
+static long long g_probe_idx[256];
+static double g_hist[256 * 256 * 4];
+static int g_hist_rows;
+static int g_single_dims[3];
 
 int shock_create(const shock_params *p, const double *x, const double *y, const double *z, const double *u,
                  const double *v, const double *w, const double *pr, const double *rho, int device, shock_ctx **out)
@@ -43,6 +48,11 @@ int shock_create(const shock_params *p, const double *x, const double *y, const 
     (void)x; (void)y; (void)z; (void)u; (void)v; (void)w; (void)pr; (void)rho; (void)device;
     g_single = *p;
     g_single_created = 1;
+    g_single_steps = 0;
+    g_nprobe = 0;
+    g_hist_rows = 0;
+    const int g = (p->order + 1) / 2, n[3] = {p->ni, p->nj, p->nk};
+    for (int a = 0; a < 3; a++) g_single_dims[a] = a < p->dim ? n[a] + 2 * g : 1;
     *out = (shock_ctx *)&g_single;   /* never dereferenced */
     return SHOCK_OK;
 }
@@ -54,6 +64,50 @@ int mock_params(shock_params *out)
     return g_single_created ? 0 : -1;
 }
 
+/* the double's U_lastStep after s steps at ghosted point o: p, u, v, w */
+static double mock_value(int field, long long o, int s) { return 1.0 + field + 0.01 * s + 1e-7 * (double)o; }
+
+int shock_set_probes(shock_ctx *c, int n, const int *ijk3, int capacity)
+{
+    (void)c; (void)capacity;
+    if (n < 0 || n > 256) return SHOCK_EINVAL;
+    for (int q = 0; q < n; q++)
+        g_probe_idx[q] = ((long long)ijk3[3 * q] * g_single_dims[1] + ijk3[3 * q + 1]) * g_single_dims[2] +
+                         ijk3[3 * q + 2];
+    g_nprobe = n;
+    g_hist_rows = 0;
+    return SHOCK_OK;
+}
+
+int shock_step(shock_ctx *c, int n)
+{
+    (void)c;
+    for (int s = 0; s < n; s++) {
+        g_single_steps++;
+        if (g_nprobe && g_hist_rows < 256) {
+            for (int q = 0; q < g_nprobe; q++)
+                for (int f = 0; f < 4; f++)
+                    g_hist[((size_t)g_hist_rows * g_nprobe + q) * 4 + f] = mock_value(f, g_probe_idx[q], g_single_steps);
+            g_hist_rows++;
+        }
+    }
+    return SHOCK_OK;
+}
+
+int shock_probe_history(shock_ctx *c, double *out4, int max_steps, int *steps)
+{
+    (void)c;
+    const int n = g_hist_rows < max_steps ? g_hist_rows : max_steps;
+    memcpy(out4, g_hist, (size_t)n * g_nprobe * 4 * sizeof(double));
+    *steps = n;
+    g_hist_rows = 0;
+    return SHOCK_OK;
+}
+
+/* the double's value of field (0 p, 1 u, 2 v, 3 w) at ghosted point o after
+ * step s, for the test */
+double mock_probe_value(int field, long long o, int s) { return mock_value(field, o, s); }
+
 #define MOCK_OK(name, ...) \
     int name(__VA_ARGS__) { return SHOCK_OK; }
 MOCK_OK(shock_set_dirichlet, shock_ctx *c, const double *e)
@@ -61,7 +115,6 @@ MOCK_OK(shock_set_source, shock_ctx *c, const double *s)
 MOCK_OK(shock_upload_state, shock_ctx *c, const double *s)
 MOCK_OK(shock_upload_last_pressure, shock_ctx *c, const double *p)
 MOCK_OK(shock_set_tau, shock_ctx *c, double t)
-MOCK_OK(shock_step, shock_ctx *c, int n)
 MOCK_OK(shock_check_nan, shock_ctx *c, int *b)
 MOCK_OK(shock_download_state, shock_ctx *c, double *s, int w)
 MOCK_OK(shock_download_pressure, shock_ctx *c, double *p)

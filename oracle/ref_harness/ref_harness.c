@@ -531,6 +531,79 @@ int ref_dropin_create(int device)
     return GPU_Create(&cfg, &msh, &U_last, &Qf, device);
 }
 
+/* Probe histories through the binding (GPU_EnableHistories and its two
+ * writers): PressureHistory at np and VelocityHistory at nv locations
+ * (xyz, (np + nv) x 3) placed by SHOCK's own prepare*HistoryValues, then
+ * nsteps of startSimulation's order (the step, time_dim advanced by tau,
+ * the writers at int_actualIteration).  out: per pressure point its ijk,
+ * its flag and nsteps pressures; per velocity point ijk, flag and 3 x
+ * nsteps velocities; then the nsteps pressure-history times. */
+int ref_dropin_histories(int np, int nv, const double *xyz, int nsteps, int device, double *out)
+{
+    cfg.flag_PressureHistory = np > 0;
+    cfg.flag_VelocityHistory = nv > 0;
+    cfg.PressureHistory_No = np;
+    cfg.VelocityHistory_No = nv;
+    FLT **pc[6] = {&cfg.PressureHistory_x_P, &cfg.PressureHistory_y_P, &cfg.PressureHistory_z_P,
+                   &cfg.PressureHistory_x_P_real, &cfg.PressureHistory_y_P_real, &cfg.PressureHistory_z_P_real};
+    FLT **vc[6] = {&cfg.VelocityHistory_x_P, &cfg.VelocityHistory_y_P, &cfg.VelocityHistory_z_P,
+                   &cfg.VelocityHistory_x_P_real, &cfg.VelocityHistory_y_P_real, &cfg.VelocityHistory_z_P_real};
+    for (int a = 0; a < 6; a++) {
+        *pc[a] = calloc((size_t)np + 1, sizeof(FLT));
+        *vc[a] = calloc((size_t)nv + 1, sizeof(FLT));
+    }
+    for (int q = 0; q < np; q++)
+        for (int a = 0; a < 3; a++) (*pc[a])[q] = xyz[3 * q + a];
+    for (int q = 0; q < nv; q++)
+        for (int a = 0; a < 3; a++) (*vc[a])[q] = xyz[3 * (np + q) + a];
+    cfg.ijk_PressureHistory_P = calloc((size_t)np + 1, sizeof(int));
+    cfg.flag_PressureHistory_P = calloc((size_t)np + 1, sizeof(int));
+    cfg.ijk_VelocityHistory_P = calloc((size_t)nv + 1, sizeof(int));
+    cfg.flag_VelocityHistory_P = calloc((size_t)nv + 1, sizeof(int));
+    cfg.PressureHistory_time = calloc((size_t)nsteps, sizeof(FLT));
+    cfg.VelocityHistory_time = calloc((size_t)nsteps, sizeof(FLT));
+    cfg.PressureHistory_pressure = calloc((size_t)np + 1, sizeof(FLT *));
+    cfg.VelocityHistory_VelocityX = calloc((size_t)nv + 1, sizeof(FLT *));
+    cfg.VelocityHistory_VelocityY = calloc((size_t)nv + 1, sizeof(FLT *));
+    cfg.VelocityHistory_VelocityZ = calloc((size_t)nv + 1, sizeof(FLT *));
+    for (int q = 0; q < np; q++) cfg.PressureHistory_pressure[q] = calloc((size_t)nsteps, sizeof(FLT));
+    for (int q = 0; q < nv; q++) {
+        cfg.VelocityHistory_VelocityX[q] = calloc((size_t)nsteps, sizeof(FLT));
+        cfg.VelocityHistory_VelocityY[q] = calloc((size_t)nsteps, sizeof(FLT));
+        cfg.VelocityHistory_VelocityZ[q] = calloc((size_t)nsteps, sizeof(FLT));
+    }
+    if (np) preparePressureHistoryValues(&cfg, &msh);
+    if (nv) prepareVelocityHistoryValues(&cfg, &msh);
+    int rc = ref_dropin_create(device);
+    if (!rc) rc = GPU_EnableHistories(&cfg);
+    if (rc) return rc;
+    cfg.int_StartIteration = 0;
+    cfg.time_dim = 0.0;
+    for (int it = 1; it <= nsteps; it++) {
+        cfg.int_actualIteration = it;
+        GPU_CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh);
+        cfg.time_dim += cfg.numericalTau;
+        if (np) GPU_WriteValuesForPressureHistory(&cfg, &U_last);
+        if (nv) GPU_WriteValuesForVelocityHistory(&cfg, &U_last);
+    }
+    double *o = out;
+    for (int q = 0; q < np; q++) {
+        *o++ = cfg.ijk_PressureHistory_P[q];
+        *o++ = cfg.flag_PressureHistory_P[q];
+        for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.PressureHistory_pressure[q][t];
+    }
+    for (int q = 0; q < nv; q++) {
+        *o++ = cfg.ijk_VelocityHistory_P[q];
+        *o++ = cfg.flag_VelocityHistory_P[q];
+        for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.VelocityHistory_VelocityX[q][t];
+        for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.VelocityHistory_VelocityY[q][t];
+        for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.VelocityHistory_VelocityZ[q][t];
+    }
+    for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.PressureHistory_time[t];
+    GPU_Destroy();
+    return 0;
+}
+
 void ref_dropin_steps(int n)
 {
     for (int s = 0; s < n; s++) {

@@ -63,6 +63,10 @@ static double *g_block_buf;    /* rank 0: 6*NG doubles of the largest block */
 static int g_host_behind;   /* the device state is newer than the host U_RK */
 static double *g_buf;       /* 5*NG doubles */
 static double g_tau;        /* the numericalTau the device steps with */
+static int g_np, g_nv;      /* probe points registered for the pressure / velocity histories */
+static double *g_probe_rows, *g_probe_last;   /* fetched history rows; the latest step's (p,u,v,w) */
+static int g_probe_pending; /* a step ran since the history was last fetched */
+#define PROBE_CAPACITY 256
 
 static size_t ghosted_points(const struct strct_configuration *c)
 {
@@ -475,6 +479,7 @@ void GPU_CalcRungeKutta(struct strct_configuration *c, struct strct_mesh *m, str
     int rc = shock_step(g_ctx, 1);
     if (rc) fail("shock_step", rc);
     g_host_behind = 1;
+    g_probe_pending = 1;
 }
 
 int GPU_CheckNAN(struct strct_configuration *c, struct strct_U *U_RK, struct strct_mesh *m)
@@ -543,6 +548,89 @@ void GPU_UploadState(struct strct_configuration *c, struct strct_U *U_RK)
     g_host_behind = 0;
 }
 
+/* ---- probe histories on the device (single rank) ---- */
+
+int GPU_EnableHistories(struct strct_configuration *c)
+{
+    if (g_division) return 0;   /* several ranks: GPU_SyncHost and SHOCK's own writers */
+    const int nj = c->int_jMeshPointsGhostCells, nk = c->int_kMeshPointsGhostCells;
+    const int np = c->flag_PressureHistory == 1 ? c->PressureHistory_No : 0;
+    const int nv = c->flag_VelocityHistory == 1 ? c->VelocityHistory_No : 0;
+    int *ijk3 = malloc(3 * (size_t)(np + nv + 1) * sizeof(int)), n = 0;
+    g_np = g_nv = 0;
+    for (int p = 0; p < np; p++)
+        if (c->flag_PressureHistory_P[p] == 1) {
+            const int o = c->ijk_PressureHistory_P[p];
+            ijk3[3 * n] = o / (nj * nk);
+            ijk3[3 * n + 1] = (o / nk) % nj;
+            ijk3[3 * n + 2] = o % nk;
+            n++;
+            g_np++;
+        }
+    for (int p = 0; p < nv; p++)
+        if (c->flag_VelocityHistory_P[p] == 1) {
+            const int o = c->ijk_VelocityHistory_P[p];
+            ijk3[3 * n] = o / (nj * nk);
+            ijk3[3 * n + 1] = (o / nk) % nj;
+            ijk3[3 * n + 2] = o % nk;
+            n++;
+            g_nv++;
+        }
+    int rc = shock_set_probes(g_ctx, n, ijk3, PROBE_CAPACITY);
+    free(ijk3);
+    free(g_probe_rows);
+    free(g_probe_last);
+    g_probe_rows = n ? malloc((size_t)PROBE_CAPACITY * n * 4 * sizeof(double)) : NULL;
+    g_probe_last = n ? calloc((size_t)n * 4, sizeof(double)) : NULL;
+    g_probe_pending = 0;
+    return rc;
+}
+
+/* the latest step's (p,u,v,w) of every registered point */
+static void fetch_probes(void)
+{
+    if (!g_probe_pending || !g_probe_rows) return;
+    int steps = 0;
+    int rc = shock_probe_history(g_ctx, g_probe_rows, PROBE_CAPACITY, &steps);
+    if (rc) fail("shock_probe_history", rc);
+    const int n = g_np + g_nv;
+    if (steps > 0) memcpy(g_probe_last, g_probe_rows + (size_t)(steps - 1) * n * 4, (size_t)n * 4 * sizeof(double));
+    g_probe_pending = 0;
+}
+
+void GPU_WriteValuesForPressureHistory(struct strct_configuration *c, struct strct_U *U_lastStep)
+{
+    if (g_division || !g_probe_last) {
+        WriteValuesForPressureHistory(c, U_lastStep);
+        return;
+    }
+    fetch_probes();
+    const int it = c->int_actualIteration - (c->int_StartIteration + 1);
+    c->PressureHistory_time[it] = c->time_dim;
+    int q = 0;
+    for (int p = 0; p < c->PressureHistory_No; p++)
+        if (c->flag_PressureHistory_P[p] == 1) c->PressureHistory_pressure[p][it] = (FLT)g_probe_last[4 * q++];
+}
+
+void GPU_WriteValuesForVelocityHistory(struct strct_configuration *c, struct strct_U *U_lastStep)
+{
+    if (g_division || !g_probe_last) {
+        WriteValuesForVelocityHistory(c, U_lastStep);
+        return;
+    }
+    fetch_probes();
+    const int it = c->int_actualIteration - (c->int_StartIteration + 1);
+    c->VelocityHistory_time[it] = c->time_dim;
+    int q = g_np;
+    for (int p = 0; p < c->VelocityHistory_No; p++)
+        if (c->flag_VelocityHistory_P[p] == 1) {
+            const double *v = g_probe_last + 4 * q++;
+            c->VelocityHistory_VelocityX[p][it] = (FLT)v[1];
+            c->VelocityHistory_VelocityY[p][it] = (FLT)v[2];
+            c->VelocityHistory_VelocityZ[p][it] = (FLT)v[3];
+        }
+}
+
 void GPU_Destroy(void)
 {
     if (g_ctx) shock_destroy(g_ctx);
@@ -556,4 +644,8 @@ void GPU_Destroy(void)
     g_block_ng = NULL;
     free(g_block_buf);
     g_block_buf = NULL;
+    free(g_probe_rows);
+    free(g_probe_last);
+    g_probe_rows = g_probe_last = NULL;
+    g_np = g_nv = 0;
 }

@@ -58,6 +58,21 @@ void GPU_SyncHost(struct strct_configuration *config, struct strct_U *U_RK);
 /* Pushes a host-modified U_RK (e.g. after a NaN reset) to the device. */
 void GPU_UploadState(struct strct_configuration *config, struct strct_U *U_RK);
 
+/* Probe histories recorded on the device (PressureHistory /
+ * VelocityHistory, src/SHOCK.c:722-734), so that they need no download of
+ * the state: call once after SHOCK's preparePressureHistoryValues /
+ * prepareVelocityHistoryValues and GPU_Create; it registers this rank's
+ * flagged points with shock_set_probes.  Then call
+ * GPU_WriteValuesForPressureHistory / GPU_WriteValuesForVelocityHistory in
+ * place of WriteValuesForPressureHistory / WriteValuesForVelocityHistory
+ * (src/Functions.c:5381-5417): they write the last step's device values
+ * (U_lastStep's p, u, v, w at the points) and time_dim at the current
+ * iteration.  With several ranks they are SHOCK's own writers (the host
+ * state must then be synced first, as before). */
+int GPU_EnableHistories(struct strct_configuration *config);
+void GPU_WriteValuesForPressureHistory(struct strct_configuration *config, struct strct_U *U_lastStep);
+void GPU_WriteValuesForVelocityHistory(struct strct_configuration *config, struct strct_U *U_lastStep);
+
 void GPU_Destroy(void);
 
 #endif

@@ -17,7 +17,8 @@ def test_dropin_binding_exports():
     header = open(os.path.join(ROOT, "shock_b200", "dropin", "GPU.h")).read()
     names = re.findall(r"\b(GPU_\w+)\s*\(", header)
     assert set(names) == {"GPU_Create", "GPU_CalcRungeKutta", "GPU_CheckNAN", "GPU_SyncHost", "GPU_UploadState",
-                          "GPU_Destroy"}
+                          "GPU_Destroy", "GPU_EnableHistories", "GPU_WriteValuesForPressureHistory",
+                          "GPU_WriteValuesForVelocityHistory"}
     lib = ctypes.CDLL(LIB, mode=os.RTLD_LOCAL)
     for n in names:
         assert hasattr(lib, n), n

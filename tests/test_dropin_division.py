@@ -114,3 +114,51 @@ def test_dropin_single_block_description(name):
     assert [p.period[a] for a in range(3) if want.periodic[a]] == \
         [float(np.float32(want.period[a])) for a in range(3) if want.periodic[a]], name
     assert list(p.u_inflow) == list(want.u_inflow), name
+
+
+@pytest.mark.parametrize("name", ["tgv16_w5_periodic", "channel2d_w9_isothermal"])
+def test_dropin_probe_histories(name):
+    """GPU_EnableHistories registers the points SHOCK's own
+    prepare*HistoryValues chose (flagged ones only), and the binding's
+    writers put the last step's device values of each point (U_lastStep's p,
+    u, v, w) and time_dim at the current iteration of SHOCK's history arrays
+    (over the test double, whose values name the point and the step)."""
+    import ctypes as C
+
+    from refbind import RefSolver
+    case = SINGLE[name]()
+    try:
+        ref = RefSolver(case, _lib="libshockdropinmock")
+    except FileNotFoundError:
+        pytest.skip("drop-in test double build absent (make -C oracle with the reference sources)")
+    rng = np.random.default_rng(11)
+    lo = np.array([case.x.min(), case.y.min(), case.z.min()])
+    hi = np.array([case.x.max(), case.y.max(), case.z.max()])
+    np_, nv, nsteps = 5, 4, 6
+    xyz = lo - 0.2 * (hi - lo) + rng.random((np_ + nv, 3)) * 1.4 * (hi - lo)
+    if case.dim == 2:
+        xyz[:, 2] = 0.0
+    xyz = np.ascontiguousarray(xyz)
+    out = np.zeros(np_ * (2 + nsteps) + nv * (2 + 3 * nsteps) + nsteps)
+    dp = C.POINTER(C.c_double)
+    assert ref.lib.ref_dropin_histories(np_, nv, xyz.ctypes.data_as(dp), nsteps, 0, out.ctypes.data_as(dp)) == 0
+    val = ref.lib.mock_probe_value
+    val.restype = C.c_double
+    o, flagged = 0, 0
+    for q in range(np_):
+        ijk, flag, hist = int(out[o]), int(out[o + 1]), out[o + 2:o + 2 + nsteps]
+        o += 2 + nsteps
+        want = [val(0, C.c_longlong(ijk), s) if flag else 0.0 for s in range(1, nsteps + 1)]
+        assert list(hist) == want, (name, q)
+        flagged += flag
+    for q in range(nv):
+        ijk, flag = int(out[o]), int(out[o + 1])
+        for f in range(3):
+            hist = out[o + 2 + f * nsteps:o + 2 + (f + 1) * nsteps]
+            want = [val(1 + f, C.c_longlong(ijk), s) if flag else 0.0 for s in range(1, nsteps + 1)]
+            assert list(hist) == want, (name, q, f)
+        o += 2 + 3 * nsteps
+        flagged += flag
+    # time_dim, advanced by tau after every step
+    assert np.allclose(out[o:o + nsteps], [case.tau * s for s in range(1, nsteps + 1)], rtol=1e-14, atol=0)
+    assert 0 < flagged < np_ + nv
