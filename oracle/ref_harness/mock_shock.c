@@ -104,6 +104,39 @@ int shock_probe_history(shock_ctx *c, double *out4, int max_steps, int *steps)
     return SHOCK_OK;
 }
 
+static int g_film_cap, g_film_frames;
+
+int shock_film_reserve(shock_ctx *c, int max_frames)
+{
+    (void)c;
+    g_film_cap = max_frames;
+    g_film_frames = 0;
+    return SHOCK_OK;
+}
+
+int shock_film_sample(shock_ctx *c)
+{
+    (void)c;
+    if (g_film_frames >= g_film_cap) return SHOCK_ENOMEM;
+    g_film_frames++;
+    return SHOCK_OK;
+}
+
+/* frame f, field q (rho, u, v, w, p, |grad rho|, Mach, lambda2), real point t */
+double mock_film_value(int f, int q, long long t) { return 10.0 * q + 0.001 * f + 1e-7 * (double)t; }
+
+int shock_film_download(shock_ctx *c, double *out, int max_frames, int *frames)
+{
+    (void)c;
+    const long long nr = (long long)g_single.ni * g_single.nj * (g_single.dim == 3 ? g_single.nk : 1);
+    const int n = g_film_frames < max_frames ? g_film_frames : max_frames;
+    for (int f = 0; f < n; f++)
+        for (int q = 0; q < 8; q++)
+            for (long long t = 0; t < nr; t++) out[((size_t)f * 8 + q) * nr + t] = mock_film_value(f, q, t);
+    *frames = n;
+    return SHOCK_OK;
+}
+
 /* the double's value of field (0 p, 1 u, 2 v, 3 w) at ghosted point o after
  * step s, for the test */
 double mock_probe_value(int field, long long o, int s) { return mock_value(field, o, s); }

@@ -531,6 +531,43 @@ int ref_dropin_create(int device)
     return GPU_Create(&cfg, &msh, &U_last, &Qf, device);
 }
 
+/* Film samples through the binding (GPU_EnableFilm, GPU_SampleFilm,
+ * GPU_SyncFilm): nsamples samples, one after every step, except that after
+ * sample `again` the sample index goes back one (a NaN reset that takes
+ * that sample again).  out: the eight Film arrays (rho, u, v, w, p,
+ * gradRho, MachNumber, Lambda2; nsamples x real points each), then the
+ * nsamples sample times. */
+int ref_dropin_film(int nsamples, int again, int device, double *out)
+{
+    const size_t nr = (size_t)cfg.int_iMeshPoints * cfg.int_jMeshPoints * cfg.int_kMeshPoints;
+    struct strct_Film F;
+    FLT **f8[8] = {&F.rho, &F.u, &F.v, &F.w, &F.p, &F.gradRho, &F.MachNumber, &F.Lambda2};
+    for (int q = 0; q < 8; q++) *f8[q] = calloc(nr * (size_t)nsamples, sizeof(FLT));
+    F.time_dim = calloc((size_t)nsamples, sizeof(FLT));
+    cfg.int_Samples = nsamples;
+    cfg.int_actualSample = 0;
+    cfg.time_dim = 0.0;
+    int rc = ref_dropin_create(device);
+    if (!rc) rc = GPU_EnableFilm(&cfg);
+    if (rc) return rc;
+    int taken = 0;
+    while (cfg.int_actualSample < nsamples) {
+        GPU_CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh);
+        cfg.time_dim += cfg.numericalTau;
+        GPU_SampleFilm(&cfg, &msh, &U_last, &F);
+        cfg.int_actualSample++;
+        if (++taken == again) cfg.int_actualSample--;
+    }
+    GPU_SyncFilm(&cfg, &F);
+    for (int q = 0; q < 8; q++)
+        for (size_t t = 0; t < nr * (size_t)nsamples; t++) out[q * nr * (size_t)nsamples + t] = (double)(*f8[q])[t];
+    for (int s2 = 0; s2 < nsamples; s2++) out[8 * nr * (size_t)nsamples + s2] = (double)F.time_dim[s2];
+    for (int q = 0; q < 8; q++) free(*f8[q]);
+    free(F.time_dim);
+    GPU_Destroy();
+    return 0;
+}
+
 /* Probe histories through the binding (GPU_EnableHistories and its two
  * writers): PressureHistory at np and VelocityHistory at nv locations
  * (xyz, (np + nv) x 3) placed by SHOCK's own prepare*HistoryValues, then

@@ -67,6 +67,8 @@ static int g_np, g_nv;      /* probe points registered for the pressure / veloci
 static double *g_probe_rows, *g_probe_last;   /* fetched history rows; the latest step's (p,u,v,w) */
 static int g_probe_pending; /* a step ran since the history was last fetched */
 #define PROBE_CAPACITY 256
+static int *g_film_sample;  /* the sample index of every device frame */
+static int g_film_frames, g_film_cap;
 
 static size_t ghosted_points(const struct strct_configuration *c)
 {
@@ -631,6 +633,57 @@ void GPU_WriteValuesForVelocityHistory(struct strct_configuration *c, struct str
         }
 }
 
+/* ---- Film samples on the device (single rank) ---- */
+
+int GPU_EnableFilm(struct strct_configuration *c)
+{
+    if (g_division) return 0;   /* several ranks: GPU_SyncHost and SHOCK's own sampling */
+    /* a NaN reset takes samples again, so leave room for every sample twice */
+    g_film_cap = 2 * c->int_Samples + 4;
+    int rc = shock_film_reserve(g_ctx, g_film_cap);
+    if (rc) return rc;
+    free(g_film_sample);
+    g_film_sample = malloc((size_t)g_film_cap * sizeof(int));
+    g_film_frames = 0;
+    return 0;
+}
+
+void GPU_SampleFilm(struct strct_configuration *c, struct strct_mesh *m, struct strct_U *U_lastStep,
+                    struct strct_Film *Film)
+{
+    if (g_division || !g_film_sample) {
+        CalcValuesForPost(c, m, U_lastStep);
+        WriteValuesFromUToFilm(c, U_lastStep, Film, m);
+        return;
+    }
+    Film->time_dim[c->int_actualSample] = c->time_dim;
+    if (g_film_frames >= g_film_cap) fail("GPU_SampleFilm", SHOCK_ENOMEM);
+    int rc = shock_film_sample(g_ctx);
+    if (rc) fail("shock_film_sample", rc);
+    g_film_sample[g_film_frames++] = c->int_actualSample;
+}
+
+void GPU_SyncFilm(struct strct_configuration *c, struct strct_Film *Film)
+{
+    if (g_division || !g_film_sample || !g_film_frames) return;
+    const size_t nr = (size_t)c->int_iMeshPoints * c->int_jMeshPoints * c->int_kMeshPoints;
+    double *buf = malloc(8 * nr * (size_t)g_film_frames * sizeof(double));
+    int got = 0;
+    int rc = shock_film_download(g_ctx, buf, g_film_frames, &got);
+    if (rc) fail("shock_film_download", rc);
+    /* device frame fields: rho, u, v, w, p, |grad rho|, Mach, lambda2; a
+       sample taken again after a reset overwrites the earlier frame */
+    FLT *dst[8] = {Film->rho, Film->u, Film->v, Film->w, Film->p, Film->gradRho, Film->MachNumber, Film->Lambda2};
+    for (int f = 0; f < got; f++) {
+        const size_t s0 = (size_t)g_film_sample[f] * nr;
+        for (int q = 0; q < 8; q++) {
+            const double *src = buf + ((size_t)f * 8 + q) * nr;
+            for (size_t t = 0; t < nr; t++) dst[q][s0 + t] = (FLT)src[t];
+        }
+    }
+    free(buf);
+}
+
 void GPU_Destroy(void)
 {
     if (g_ctx) shock_destroy(g_ctx);
@@ -648,4 +701,7 @@ void GPU_Destroy(void)
     free(g_probe_last);
     g_probe_rows = g_probe_last = NULL;
     g_np = g_nv = 0;
+    free(g_film_sample);
+    g_film_sample = NULL;
+    g_film_frames = g_film_cap = 0;
 }

@@ -73,6 +73,20 @@ int GPU_EnableHistories(struct strct_configuration *config);
 void GPU_WriteValuesForPressureHistory(struct strct_configuration *config, struct strct_U *U_lastStep);
 void GPU_WriteValuesForVelocityHistory(struct strct_configuration *config, struct strct_U *U_lastStep);
 
+/* Film samples taken on the device (src/SHOCK.c:698-717), so that sampling
+ * needs no download of the state: GPU_EnableFilm once after GPU_Create
+ * (room for int_Samples frames, twice over for samples a NaN reset takes
+ * again); GPU_SampleFilm in place of CalcValuesForPost +
+ * WriteValuesFromUToFilm at a sample (it sets Film->time_dim of
+ * int_actualSample; the caller still counts int_actualSample up);
+ * GPU_SyncFilm before the Film is written (saveFile): every frame into its
+ * sample's place in the Film arrays.  With several ranks they are SHOCK's
+ * own calls (the host state must then be synced first). */
+int GPU_EnableFilm(struct strct_configuration *config);
+void GPU_SampleFilm(struct strct_configuration *config, struct strct_mesh *mesh, struct strct_U *U_lastStep,
+                    struct strct_Film *Film);
+void GPU_SyncFilm(struct strct_configuration *config, struct strct_Film *Film);
+
 void GPU_Destroy(void);
 
 #endif

@@ -18,7 +18,7 @@ def test_dropin_binding_exports():
     names = re.findall(r"\b(GPU_\w+)\s*\(", header)
     assert set(names) == {"GPU_Create", "GPU_CalcRungeKutta", "GPU_CheckNAN", "GPU_SyncHost", "GPU_UploadState",
                           "GPU_Destroy", "GPU_EnableHistories", "GPU_WriteValuesForPressureHistory",
-                          "GPU_WriteValuesForVelocityHistory"}
+                          "GPU_WriteValuesForVelocityHistory", "GPU_EnableFilm", "GPU_SampleFilm", "GPU_SyncFilm"}
     lib = ctypes.CDLL(LIB, mode=os.RTLD_LOCAL)
     for n in names:
         assert hasattr(lib, n), n

@@ -162,3 +162,37 @@ def test_dropin_probe_histories(name):
     # time_dim, advanced by tau after every step
     assert np.allclose(out[o:o + nsteps], [case.tau * s for s in range(1, nsteps + 1)], rtol=1e-14, atol=0)
     assert 0 < flagged < np_ + nv
+
+
+@pytest.mark.parametrize("name", ["tgv16_w5_periodic", "duct2d_w9_isentropic_riemann"])
+def test_dropin_film(name):
+    """GPU_SampleFilm takes each sample on the device and GPU_SyncFilm puts
+    every frame at its sample's place in SHOCK's Film arrays, a sample taken
+    again after a NaN reset overwriting the earlier one; the sample times are
+    SHOCK's time_dim at each sample (over the test double, whose frames name
+    the frame, the field and the point)."""
+    import ctypes as C
+
+    from refbind import RefSolver
+    case = SINGLE[name]()
+    try:
+        ref = RefSolver(case, _lib="libshockdropinmock")
+    except FileNotFoundError:
+        pytest.skip("drop-in test double build absent (make -C oracle with the reference sources)")
+    nsamples, again = 4, 3
+    nr = case.real_points
+    out = np.zeros(8 * nsamples * nr + nsamples)
+    dp = C.POINTER(C.c_double)
+    assert ref.lib.ref_dropin_film(nsamples, again, 0, out.ctypes.data_as(dp)) == 0
+    val = ref.lib.mock_film_value
+    val.restype = C.c_double
+    frame_of = [0, 1, 3, 4]               # sample 2 taken again by frame 3
+    t = np.arange(nr)
+    for q in range(8):
+        film = out[q * nsamples * nr:(q + 1) * nsamples * nr].reshape(nsamples, nr)
+        for s, f in enumerate(frame_of):
+            want = 10.0 * q + 0.001 * f + 1e-7 * t
+            assert np.array_equal(film[s], want), (name, q, s)
+            assert val(f, q, C.c_longlong(5)) == want[5]
+    times = out[8 * nsamples * nr:]
+    assert np.allclose(times, [case.tau * (f + 1) for f in frame_of], rtol=1e-14, atol=0)
