@@ -531,6 +531,8 @@ int ref_dropin_create(int device)
     return GPU_Create(&cfg, &msh, &U_last, &Qf, device);
 }
 
+void ref_dropin_destroy(void);
+
 /* Film samples through the binding (GPU_EnableFilm, GPU_SampleFilm,
  * GPU_SyncFilm): nsamples samples, one after every step, except that after
  * sample `again` the sample index goes back one (a NaN reset that takes
@@ -564,7 +566,7 @@ int ref_dropin_film(int nsamples, int again, int device, double *out)
     for (int s2 = 0; s2 < nsamples; s2++) out[8 * nr * (size_t)nsamples + s2] = (double)F.time_dim[s2];
     for (int q = 0; q < 8; q++) free(*f8[q]);
     free(F.time_dim);
-    GPU_Destroy();
+    ref_dropin_destroy();
     return 0;
 }
 
@@ -637,7 +639,7 @@ int ref_dropin_histories(int np, int nv, const double *xyz, int nsteps, int devi
         for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.VelocityHistory_VelocityZ[q][t];
     }
     for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.PressureHistory_time[t];
-    GPU_Destroy();
+    ref_dropin_destroy();
     return 0;
 }
 

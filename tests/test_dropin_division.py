@@ -104,6 +104,7 @@ def test_dropin_single_block_description(name):
     assert ref.lib.ref_dropin_create(0) == 0
     p = shock_b200.Params()
     assert ref.lib.mock_params(C.byref(p)) == 0
+    ref.lib.ref_dropin_destroy()
     want = shock_b200.params_from_case(case)
     for k in ("dim", "order", "ni", "nj", "nk", "time_order", "tau", "mach", "reynolds", "prandtl", "gamma", "gas_r",
               "t0", "l0", "inviscid", "mms", "t_wall", "rho_inflow", "p_inflow", "p_outflow"):
