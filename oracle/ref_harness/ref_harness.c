@@ -922,20 +922,23 @@ int refmpi_run_file(int nblocks, const ref_params *blk, const int *neigh, const 
 /*
  * The drop-in's division mode (shock_b200/dropin/GPU.c with several ranks)
  * inside SHOCK's own multi-rank set-up, over the library's host test double
- * (ref_harness/mock_shock.c): each rank runs SHOCK's set-up of its block,
+ * (ref_harness/mock_shock.c, SHOCK_MOCK) or the library itself on rank 0's
+ * GPU: each rank runs SHOCK's set-up of its block,
  * then GPU_Create, nsteps of GPU_CalcRungeKutta + GPU_CheckNAN (tau times
  * tau_factor before step tau_at), GPU_SyncHost; then changes its U_RK by
  * (rank + 1) / 4 in rho, GPU_UploadState, one more step, GPU_SyncHost.
  * Per block at out_off[b]: SHOCK's geometry (13*NG), U_lastStep before
  * GPU_Create (6*NG: rho,u,v,w,e,p), U_RK after the loop (6*NG), U_RK after
  * the upload and step (6*NG), the double's geometry of the block from the
- * library's host set-up (13*NG, written by rank 0).  extra: per rank the
- * number of steps GPU_CheckNAN reported (nblocks), then the double's step
- * count and up to 16 time steps it was given.
+ * library's host set-up (13*NG, written by rank 0 over the double).  extra:
+ * per rank the number of steps GPU_CheckNAN reported (nblocks), then (over
+ * the double) its step count and up to 16 time steps it was given.
  */
+#ifdef SHOCK_MOCK
 int mock_block_geometry(int b, double *out13);
 int mock_steps(void);
 int mock_taus(double *out, int max);
+#endif
 
 typedef struct {
     const mr_job *job;
@@ -980,6 +983,7 @@ static int dj_body(int rank, void *arg)
     GPU_SyncHost(&cfg, &U_rk);
     dj_state(&U_rk, o + 25 * (size_t)n);
     dj->extra[rank] = nans;
+#ifdef SHOCK_MOCK
     if (rank == 0) {
         for (int b = 0; b < g_job->nblocks; b++) {
             const size_t ngb = g_job->out_off_ng[b];
@@ -988,6 +992,7 @@ static int dj_body(int rank, void *arg)
         dj->extra[g_job->nblocks] = mock_steps();
         mock_taus(dj->extra + g_job->nblocks + 1, 16);
     }
+#endif
     GPU_Destroy();
     return 0;
 }

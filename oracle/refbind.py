@@ -500,16 +500,19 @@ def config_import(path) -> dict:
     raise RuntimeError(f"SHOCK's ConfigImport ended with {r.returncode}: {(r.stdout + r.stderr)[-400:]}")
 
 
-def dropin_multirank_available(order: int, dim: int) -> bool:
-    return os.path.exists(os.path.join(HERE, "_ref", f"libshockdropinmpi_w{order}_{dim}d.so"))
+def dropin_multirank_available(order: int, dim: int, real: bool = False) -> bool:
+    tag = "real" if real else ""
+    return os.path.exists(os.path.join(HERE, "_ref", f"libshockdropinmpi{tag}_w{order}_{dim}d.so"))
 
 
-def _dropin_multirank_worker(division, nsteps, tau_at, tau_factor, nan):
+def _dropin_multirank_worker(division, nsteps, tau_at, tau_factor, nan, real=False):
     case = division.case
     os.environ["SHOCK_B200_LIB"] = os.path.join(os.path.dirname(HERE), "shock_b200", "libshock_b200.so")
     if nan is not None:
         os.environ["SHOCK_MOCK_NAN"] = f"{nan[0]} {nan[1]}"
-    lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockdropinmpi_w{case.order}_{case.dim}d.so"), mode=os.RTLD_LOCAL)
+    tag = "real" if real else ""
+    lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockdropinmpi{tag}_w{case.order}_{case.dim}d.so"),
+                 mode=os.RTLD_LOCAL)
     lib.refmpi_dropin_run.restype = C.c_int
     nb = len(division.blocks)
     g2 = case.order + 1
@@ -553,13 +556,15 @@ def _dropin_multirank_worker(division, nsteps, tau_at, tau_factor, nan):
     return res, steps, taus
 
 
-def run_dropin_multirank(division, nsteps: int, tau_at: int = -1, tau_factor: float = 1.0, nan=None):
+def run_dropin_multirank(division, nsteps: int, tau_at: int = -1, tau_factor: float = 1.0, nan=None,
+                         real: bool = False):
     """The drop-in binding (shock_b200/dropin/GPU.c) in its division mode,
     inside SHOCK's own multi-rank set-up of the division, over the library's
-    host test double (ref_harness/mock_shock.c); see refmpi_dropin_run.
-    nan = (step, block) plants a non-finite density in the double.  Returns
-    (per block dict, the double's step count, the time steps it was given)."""
+    host test double (ref_harness/mock_shock.c), or with real=True over the
+    library itself on rank 0's GPU; see refmpi_dropin_run.  nan = (step,
+    block) plants a non-finite density in the double.  Returns (per block
+    dict, the double's step count, the time steps it was given)."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
-        return pool.apply(_dropin_multirank_worker, (division, nsteps, tau_at, tau_factor, nan))
+        return pool.apply(_dropin_multirank_worker, (division, nsteps, tau_at, tau_factor, nan, real))

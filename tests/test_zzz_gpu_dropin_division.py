@@ -1,0 +1,35 @@
+"""The drop-in binding's division mode end to end on a GPU: SHOCK's own
+multi-rank set-up of a division on forked ranks, then GPU_Create,
+GPU_CalcRungeKutta + GPU_CheckNAN and GPU_SyncHost of
+shock_b200/dropin/GPU.c, rank 0 running every rank's block on its device
+(oracle/_ref/libshockdropinmpireal_*), against SHOCK's own multi-rank run
+of the same division on the CPU: 1e-10 relative L2 per variable after the
+steps, on every rank's U_RK as GPU_SyncHost hands it back.  (Named to run
+after the other GPU tests.)"""
+import numpy as np
+import pytest
+
+from _util import l2_rel
+from refbind import dropin_multirank_available, multirank_available, run_dropin_multirank, run_multirank
+from test_dropin_division import DIVISIONS
+from test_gpu_multiblock import _assemble
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("name", ["tgv12_w5_2x2x2", "smooth2d_w5_2x2_rotated", "channel3d_w5_walls_2x2x1"])
+def test_dropin_division_on_gpu(name):
+    d = DIVISIONS[name]()
+    case = d.case
+    if not dropin_multirank_available(case.order, case.dim, real=True) or not multirank_available(case.order,
+                                                                                                 case.dim):
+        pytest.skip("drop-in multi-rank builds absent (make -C oracle with the reference sources)")
+    nsteps = 10
+    res, _, _ = run_dropin_multirank(d, nsteps, real=True)
+    ref = run_multirank(d, nsteps)
+    got = _assemble(d, [r["after_steps"][:5] for r in res])
+    want = _assemble(d, [r["state"][:5] for r in ref])
+    idx = [0, 1, 2, 3, 4] if case.dim == 3 else [0, 1, 2, 4]
+    e = l2_rel(got, want)[idx]
+    assert (e <= 1e-10).all(), (name, e)
+    assert all(r["nan_steps"] == 0 for r in res)
