@@ -474,6 +474,155 @@ int ref_control_loop(int nsteps, int nan_at, double decel, int accel_every, doub
 
 double ref_tau(void) { return (double)cfg.numericalTau; }
 
+/*
+ * Sampling in startSimulation's order (SHOCK.c:557-734) with SHOCK's own
+ * calls or the drop-in binding's: after each step U_RK -> U_lastStep, then
+ * the Film sample and the probe histories of U_lastStep.  The ops differ
+ * only in where the steps and samples are taken.
+ */
+typedef struct {
+    int (*create)(int device, int film, int histories);
+    void (*step)(void);
+    void (*sample)(struct strct_Film *F);
+    void (*sync_film)(struct strct_Film *F);
+    void (*histories)(int np, int nv);
+    void (*destroy)(void);
+} sample_ops;
+
+/* Film: nsamples samples, one after every step, except that after sample
+ * `again` the sample index goes back one (a NaN reset that takes that
+ * sample again).  out: the eight Film arrays (rho, u, v, w, p, gradRho,
+ * MachNumber, Lambda2; nsamples x real points each), then the sample
+ * times. */
+static int film_run(const sample_ops *ops, int nsamples, int again, int device, double *out)
+{
+    const size_t nr = (size_t)cfg.int_iMeshPoints * cfg.int_jMeshPoints * cfg.int_kMeshPoints;
+    struct strct_Film F;
+    FLT **f8[8] = {&F.rho, &F.u, &F.v, &F.w, &F.p, &F.gradRho, &F.MachNumber, &F.Lambda2};
+    for (int q = 0; q < 8; q++) *f8[q] = calloc(nr * (size_t)nsamples, sizeof(FLT));
+    F.time_dim = calloc((size_t)nsamples, sizeof(FLT));
+    cfg.int_Samples = nsamples;
+    cfg.int_actualSample = 0;
+    cfg.time_dim = 0.0;
+    int rc = ops->create(device, 1, 0);
+    if (rc) return rc;
+    int taken = 0;
+    while (cfg.int_actualSample < nsamples) {
+        ops->step();
+        cfg.time_dim += cfg.numericalTau;
+        ops->sample(&F);
+        cfg.int_actualSample++;
+        if (++taken == again) cfg.int_actualSample--;
+    }
+    ops->sync_film(&F);
+    for (int q = 0; q < 8; q++)
+        for (size_t t = 0; t < nr * (size_t)nsamples; t++) out[q * nr * (size_t)nsamples + t] = (double)(*f8[q])[t];
+    for (int s2 = 0; s2 < nsamples; s2++) out[8 * nr * (size_t)nsamples + s2] = (double)F.time_dim[s2];
+    for (int q = 0; q < 8; q++) free(*f8[q]);
+    free(F.time_dim);
+    ops->destroy();
+    return 0;
+}
+
+/* Probe histories: PressureHistory at np and VelocityHistory at nv
+ * locations (xyz, (np + nv) x 3) placed by SHOCK's own
+ * prepare*HistoryValues, then nsteps steps (time_dim advanced by tau, the
+ * histories written at int_actualIteration).  out: per pressure point its
+ * ijk, its flag and nsteps pressures; per velocity point ijk, flag and 3 x
+ * nsteps velocities; then the nsteps pressure-history times. */
+static int histories_run(const sample_ops *ops, int np, int nv, const double *xyz, int nsteps, int device,
+                         double *out)
+{
+    cfg.flag_PressureHistory = np > 0;
+    cfg.flag_VelocityHistory = nv > 0;
+    cfg.PressureHistory_No = np;
+    cfg.VelocityHistory_No = nv;
+    FLT **pc[6] = {&cfg.PressureHistory_x_P, &cfg.PressureHistory_y_P, &cfg.PressureHistory_z_P,
+                   &cfg.PressureHistory_x_P_real, &cfg.PressureHistory_y_P_real, &cfg.PressureHistory_z_P_real};
+    FLT **vc[6] = {&cfg.VelocityHistory_x_P, &cfg.VelocityHistory_y_P, &cfg.VelocityHistory_z_P,
+                   &cfg.VelocityHistory_x_P_real, &cfg.VelocityHistory_y_P_real, &cfg.VelocityHistory_z_P_real};
+    for (int a = 0; a < 6; a++) {
+        *pc[a] = calloc((size_t)np + 1, sizeof(FLT));
+        *vc[a] = calloc((size_t)nv + 1, sizeof(FLT));
+    }
+    for (int q = 0; q < np; q++)
+        for (int a = 0; a < 3; a++) (*pc[a])[q] = xyz[3 * q + a];
+    for (int q = 0; q < nv; q++)
+        for (int a = 0; a < 3; a++) (*vc[a])[q] = xyz[3 * (np + q) + a];
+    cfg.ijk_PressureHistory_P = calloc((size_t)np + 1, sizeof(int));
+    cfg.flag_PressureHistory_P = calloc((size_t)np + 1, sizeof(int));
+    cfg.ijk_VelocityHistory_P = calloc((size_t)nv + 1, sizeof(int));
+    cfg.flag_VelocityHistory_P = calloc((size_t)nv + 1, sizeof(int));
+    cfg.PressureHistory_time = calloc((size_t)nsteps, sizeof(FLT));
+    cfg.VelocityHistory_time = calloc((size_t)nsteps, sizeof(FLT));
+    cfg.PressureHistory_pressure = calloc((size_t)np + 1, sizeof(FLT *));
+    cfg.VelocityHistory_VelocityX = calloc((size_t)nv + 1, sizeof(FLT *));
+    cfg.VelocityHistory_VelocityY = calloc((size_t)nv + 1, sizeof(FLT *));
+    cfg.VelocityHistory_VelocityZ = calloc((size_t)nv + 1, sizeof(FLT *));
+    for (int q = 0; q < np; q++) cfg.PressureHistory_pressure[q] = calloc((size_t)nsteps, sizeof(FLT));
+    for (int q = 0; q < nv; q++) {
+        cfg.VelocityHistory_VelocityX[q] = calloc((size_t)nsteps, sizeof(FLT));
+        cfg.VelocityHistory_VelocityY[q] = calloc((size_t)nsteps, sizeof(FLT));
+        cfg.VelocityHistory_VelocityZ[q] = calloc((size_t)nsteps, sizeof(FLT));
+    }
+    if (np) preparePressureHistoryValues(&cfg, &msh);
+    if (nv) prepareVelocityHistoryValues(&cfg, &msh);
+    int rc = ops->create(device, 0, 1);
+    if (rc) return rc;
+    cfg.int_StartIteration = 0;
+    cfg.time_dim = 0.0;
+    for (int it = 1; it <= nsteps; it++) {
+        cfg.int_actualIteration = it;
+        ops->step();
+        cfg.time_dim += cfg.numericalTau;
+        ops->histories(np, nv);
+    }
+    double *o = out;
+    for (int q = 0; q < np; q++) {
+        *o++ = cfg.ijk_PressureHistory_P[q];
+        *o++ = cfg.flag_PressureHistory_P[q];
+        for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.PressureHistory_pressure[q][t];
+    }
+    for (int q = 0; q < nv; q++) {
+        *o++ = cfg.ijk_VelocityHistory_P[q];
+        *o++ = cfg.flag_VelocityHistory_P[q];
+        for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.VelocityHistory_VelocityX[q][t];
+        for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.VelocityHistory_VelocityY[q][t];
+        for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.VelocityHistory_VelocityZ[q][t];
+    }
+    for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.PressureHistory_time[t];
+    ops->destroy();
+    return 0;
+}
+
+static int cpu_create(int device, int film, int histories) { (void)device; (void)film; (void)histories; return 0; }
+static void cpu_sample_step(void)
+{
+    CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh);
+    WriteValuesFromU1ToU2(&cfg, &U_rk, &U_last);
+}
+static void cpu_sample(struct strct_Film *F)
+{
+    CalcValuesForPost(&cfg, &msh, &U_last);
+    WriteValuesFromUToFilm(&cfg, &U_last, F, &msh);
+}
+static void cpu_sync_film(struct strct_Film *F) { (void)F; }
+static void cpu_histories(int np, int nv)
+{
+    if (np) WriteValuesForPressureHistory(&cfg, &U_last);
+    if (nv) WriteValuesForVelocityHistory(&cfg, &U_last);
+}
+
+static const sample_ops cpu_sample_ops = {cpu_create, cpu_sample_step, cpu_sample, cpu_sync_film, cpu_histories,
+                                          nothing};
+
+/* The two runs with SHOCK's own calls. */
+int ref_film(int nsamples, int again, double *out) { return film_run(&cpu_sample_ops, nsamples, again, 0, out); }
+int ref_histories(int np, int nv, const double *xyz, int nsteps, double *out)
+{
+    return histories_run(&cpu_sample_ops, np, nv, xyz, nsteps, 0, out);
+}
+
 #ifdef SHOCK_DROPIN
 /*
  * The drop-in path (shock_b200/dropin/GPU.c): SHOCK's own set-up (ref_init
@@ -533,115 +682,39 @@ int ref_dropin_create(int device)
 
 void ref_dropin_destroy(void);
 
-/* Film samples through the binding (GPU_EnableFilm, GPU_SampleFilm,
- * GPU_SyncFilm): nsamples samples, one after every step, except that after
- * sample `again` the sample index goes back one (a NaN reset that takes
- * that sample again).  out: the eight Film arrays (rho, u, v, w, p,
- * gradRho, MachNumber, Lambda2; nsamples x real points each), then the
- * nsamples sample times. */
-int ref_dropin_film(int nsamples, int again, int device, double *out)
+static int gpu_sample_create(int device, int film, int histories)
 {
-    const size_t nr = (size_t)cfg.int_iMeshPoints * cfg.int_jMeshPoints * cfg.int_kMeshPoints;
-    struct strct_Film F;
-    FLT **f8[8] = {&F.rho, &F.u, &F.v, &F.w, &F.p, &F.gradRho, &F.MachNumber, &F.Lambda2};
-    for (int q = 0; q < 8; q++) *f8[q] = calloc(nr * (size_t)nsamples, sizeof(FLT));
-    F.time_dim = calloc((size_t)nsamples, sizeof(FLT));
-    cfg.int_Samples = nsamples;
-    cfg.int_actualSample = 0;
-    cfg.time_dim = 0.0;
     int rc = ref_dropin_create(device);
-    if (!rc) rc = GPU_EnableFilm(&cfg);
-    if (rc) return rc;
-    int taken = 0;
-    while (cfg.int_actualSample < nsamples) {
-        GPU_CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh);
-        cfg.time_dim += cfg.numericalTau;
-        GPU_SampleFilm(&cfg, &msh, &U_last, &F);
-        cfg.int_actualSample++;
-        if (++taken == again) cfg.int_actualSample--;
-    }
-    GPU_SyncFilm(&cfg, &F);
-    for (int q = 0; q < 8; q++)
-        for (size_t t = 0; t < nr * (size_t)nsamples; t++) out[q * nr * (size_t)nsamples + t] = (double)(*f8[q])[t];
-    for (int s2 = 0; s2 < nsamples; s2++) out[8 * nr * (size_t)nsamples + s2] = (double)F.time_dim[s2];
-    for (int q = 0; q < 8; q++) free(*f8[q]);
-    free(F.time_dim);
-    ref_dropin_destroy();
-    return 0;
+    if (!rc && film) rc = GPU_EnableFilm(&cfg);
+    if (!rc && histories) rc = GPU_EnableHistories(&cfg);
+    return rc;
+}
+static void gpu_sample_step(void)
+{
+    GPU_CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh);
+    WriteValuesFromU1ToU2(&cfg, &U_rk, &U_last);
+}
+static void gpu_sample(struct strct_Film *F) { GPU_SampleFilm(&cfg, &msh, &U_last, F); }
+static void gpu_sync_film(struct strct_Film *F) { GPU_SyncFilm(&cfg, F); }
+static void gpu_histories(int np, int nv)
+{
+    if (np) GPU_WriteValuesForPressureHistory(&cfg, &U_last);
+    if (nv) GPU_WriteValuesForVelocityHistory(&cfg, &U_last);
 }
 
-/* Probe histories through the binding (GPU_EnableHistories and its two
- * writers): PressureHistory at np and VelocityHistory at nv locations
- * (xyz, (np + nv) x 3) placed by SHOCK's own prepare*HistoryValues, then
- * nsteps of startSimulation's order (the step, time_dim advanced by tau,
- * the writers at int_actualIteration).  out: per pressure point its ijk,
- * its flag and nsteps pressures; per velocity point ijk, flag and 3 x
- * nsteps velocities; then the nsteps pressure-history times. */
+static const sample_ops gpu_sample_ops = {gpu_sample_create, gpu_sample_step, gpu_sample, gpu_sync_film,
+                                          gpu_histories, ref_dropin_destroy};
+
+/* The two runs through the drop-in binding (device Film and histories). */
+int ref_dropin_film(int nsamples, int again, int device, double *out)
+{
+    return film_run(&gpu_sample_ops, nsamples, again, device, out);
+}
 int ref_dropin_histories(int np, int nv, const double *xyz, int nsteps, int device, double *out)
 {
-    cfg.flag_PressureHistory = np > 0;
-    cfg.flag_VelocityHistory = nv > 0;
-    cfg.PressureHistory_No = np;
-    cfg.VelocityHistory_No = nv;
-    FLT **pc[6] = {&cfg.PressureHistory_x_P, &cfg.PressureHistory_y_P, &cfg.PressureHistory_z_P,
-                   &cfg.PressureHistory_x_P_real, &cfg.PressureHistory_y_P_real, &cfg.PressureHistory_z_P_real};
-    FLT **vc[6] = {&cfg.VelocityHistory_x_P, &cfg.VelocityHistory_y_P, &cfg.VelocityHistory_z_P,
-                   &cfg.VelocityHistory_x_P_real, &cfg.VelocityHistory_y_P_real, &cfg.VelocityHistory_z_P_real};
-    for (int a = 0; a < 6; a++) {
-        *pc[a] = calloc((size_t)np + 1, sizeof(FLT));
-        *vc[a] = calloc((size_t)nv + 1, sizeof(FLT));
-    }
-    for (int q = 0; q < np; q++)
-        for (int a = 0; a < 3; a++) (*pc[a])[q] = xyz[3 * q + a];
-    for (int q = 0; q < nv; q++)
-        for (int a = 0; a < 3; a++) (*vc[a])[q] = xyz[3 * (np + q) + a];
-    cfg.ijk_PressureHistory_P = calloc((size_t)np + 1, sizeof(int));
-    cfg.flag_PressureHistory_P = calloc((size_t)np + 1, sizeof(int));
-    cfg.ijk_VelocityHistory_P = calloc((size_t)nv + 1, sizeof(int));
-    cfg.flag_VelocityHistory_P = calloc((size_t)nv + 1, sizeof(int));
-    cfg.PressureHistory_time = calloc((size_t)nsteps, sizeof(FLT));
-    cfg.VelocityHistory_time = calloc((size_t)nsteps, sizeof(FLT));
-    cfg.PressureHistory_pressure = calloc((size_t)np + 1, sizeof(FLT *));
-    cfg.VelocityHistory_VelocityX = calloc((size_t)nv + 1, sizeof(FLT *));
-    cfg.VelocityHistory_VelocityY = calloc((size_t)nv + 1, sizeof(FLT *));
-    cfg.VelocityHistory_VelocityZ = calloc((size_t)nv + 1, sizeof(FLT *));
-    for (int q = 0; q < np; q++) cfg.PressureHistory_pressure[q] = calloc((size_t)nsteps, sizeof(FLT));
-    for (int q = 0; q < nv; q++) {
-        cfg.VelocityHistory_VelocityX[q] = calloc((size_t)nsteps, sizeof(FLT));
-        cfg.VelocityHistory_VelocityY[q] = calloc((size_t)nsteps, sizeof(FLT));
-        cfg.VelocityHistory_VelocityZ[q] = calloc((size_t)nsteps, sizeof(FLT));
-    }
-    if (np) preparePressureHistoryValues(&cfg, &msh);
-    if (nv) prepareVelocityHistoryValues(&cfg, &msh);
-    int rc = ref_dropin_create(device);
-    if (!rc) rc = GPU_EnableHistories(&cfg);
-    if (rc) return rc;
-    cfg.int_StartIteration = 0;
-    cfg.time_dim = 0.0;
-    for (int it = 1; it <= nsteps; it++) {
-        cfg.int_actualIteration = it;
-        GPU_CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh);
-        cfg.time_dim += cfg.numericalTau;
-        if (np) GPU_WriteValuesForPressureHistory(&cfg, &U_last);
-        if (nv) GPU_WriteValuesForVelocityHistory(&cfg, &U_last);
-    }
-    double *o = out;
-    for (int q = 0; q < np; q++) {
-        *o++ = cfg.ijk_PressureHistory_P[q];
-        *o++ = cfg.flag_PressureHistory_P[q];
-        for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.PressureHistory_pressure[q][t];
-    }
-    for (int q = 0; q < nv; q++) {
-        *o++ = cfg.ijk_VelocityHistory_P[q];
-        *o++ = cfg.flag_VelocityHistory_P[q];
-        for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.VelocityHistory_VelocityX[q][t];
-        for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.VelocityHistory_VelocityY[q][t];
-        for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.VelocityHistory_VelocityZ[q][t];
-    }
-    for (int t = 0; t < nsteps; t++) *o++ = (double)cfg.PressureHistory_time[t];
-    ref_dropin_destroy();
-    return 0;
+    return histories_run(&gpu_sample_ops, np, nv, xyz, nsteps, device, out);
 }
+
 
 void ref_dropin_steps(int n)
 {
