@@ -471,6 +471,10 @@ int shock_multi_upload_state(shock_multi *m, int block, const double *prim5);
  * shock_download_pressure / shock_upload_last_pressure). */
 int shock_multi_download_pressure(shock_multi *m, int block, double *p);
 int shock_multi_upload_last_pressure(shock_multi *m, int block, const double *p);
+/* A block's probes and their history (as shock_set_probes /
+ * shock_probe_history), recorded by the division's step graph. */
+int shock_multi_set_probes(shock_multi *m, int block, int n, const int *ijk3, int capacity);
+int shock_multi_probe_history(shock_multi *m, int block, double *out4, int max_steps, int *steps);
 /* The time step of the following steps (as shock_set_tau). */
 int shock_multi_set_tau(shock_multi *m, double tau);
 /* checkNAN over every block; SHOCK_ENAN when any density is non-finite. */

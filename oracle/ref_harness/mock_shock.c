@@ -22,6 +22,9 @@
 
 struct shock_multi {
     int nblocks, dim, g, steps;
+    int nprobe[64], rows[64];
+    long long probe_idx[64][64];
+    double hist[64][64 * 4 * 8];
     size_t *ng;
     double **state;   /* per block 6*NG: rho,u,v,w,e, then p */
     double **plast;   /* per block NG: U_lastStep's p as uploaded */
@@ -30,6 +33,7 @@ struct shock_multi {
 };
 
 static struct shock_multi *g_last;
+double mock_div_probe_value(int b, int f, long long o, int s);
 static double g_taus[256];
 static int g_ntau;
 
@@ -249,6 +253,13 @@ int shock_multi_step(shock_multi *m, int n)
                 m->state[b][o] += 1e-3 * (b + 1);                              /* rho */
                 m->state[b][5 * m->ng[b] + o] = 2.0 + b + 0.5 * m->steps;      /* p */
             }
+            if (m->nprobe[b] && m->rows[b] < 8) {
+                for (int q = 0; q < m->nprobe[b]; q++)
+                    for (int f = 0; f < 4; f++)
+                        m->hist[b][((size_t)m->rows[b] * m->nprobe[b] + q) * 4 + f] =
+                            mock_div_probe_value(b, f, m->probe_idx[b][q], m->steps);
+                m->rows[b]++;
+            }
             if (m->steps == nan_step && b == nan_block) {
                 /* a real point: the first one past the ghost layers */
                 const int g = m->g, *d = m->dims[b];
@@ -257,6 +268,32 @@ int shock_multi_step(shock_multi *m, int n)
             }
         }
     }
+    return SHOCK_OK;
+}
+
+/* block b's probe value of field f (p, u, v, w) at ghosted point o after
+ * step s */
+double mock_div_probe_value(int b, int f, long long o, int s) { return 100.0 * b + 1.0 + f + 0.01 * s + 1e-7 * (double)o; }
+
+int shock_multi_set_probes(shock_multi *m, int b, int n, const int *ijk3, int capacity)
+{
+    (void)capacity;
+    if (bad_block(m, b) || n < 0 || n > 64) return SHOCK_EINVAL;
+    const int *d = m->dims[b];
+    for (int q = 0; q < n; q++)
+        m->probe_idx[b][q] = ((long long)ijk3[3 * q] * d[1] + ijk3[3 * q + 1]) * d[2] + ijk3[3 * q + 2];
+    m->nprobe[b] = n;
+    m->rows[b] = 0;
+    return SHOCK_OK;
+}
+
+int shock_multi_probe_history(shock_multi *m, int b, double *out4, int max_steps, int *steps)
+{
+    if (bad_block(m, b)) return SHOCK_EINVAL;
+    const int n = m->rows[b] < max_steps ? m->rows[b] : max_steps;
+    memcpy(out4, m->hist[b], (size_t)n * m->nprobe[b] * 4 * sizeof(double));
+    *steps = n;
+    m->rows[b] = 0;
     return SHOCK_OK;
 }
 

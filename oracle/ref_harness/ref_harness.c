@@ -1070,6 +1070,62 @@ static int dj_body(int rank, void *arg)
     return 0;
 }
 
+/* The division mode's device histories: every rank places the same
+ * locations with SHOCK's prepare*HistoryValues and runs histories_run over
+ * the binding; out at out_off[rank]: histories_run's output of the rank. */
+typedef struct {
+    const mr_job *job;
+    int np, nv, nsteps;
+    const double *xyz;
+} dh_job;
+
+static int div_hist_create(int device, int film, int histories)
+{
+    (void)film;
+    int rc = GPU_Create(&cfg, &msh, &U_last, &Qf, device);
+    if (!rc && histories) rc = GPU_EnableHistories(&cfg);
+    return rc;
+}
+static void div_hist_step(void)
+{
+    GPU_CalcRungeKutta(&cfg, &msh, &U_last, &U_rk, &Qf, &Qsum, &Fl, &Flh);
+    WriteValuesFromU1ToU2(&cfg, &U_rk, &U_last);
+}
+static void div_hist_write(int np, int nv)
+{
+    if (np) GPU_WriteValuesForPressureHistory(&cfg, &U_last);
+    if (nv) GPU_WriteValuesForVelocityHistory(&cfg, &U_last);
+}
+static void div_no_film(struct strct_Film *F) { (void)F; }
+
+static int dh_body(int rank, void *arg)
+{
+    const dh_job *dh = (const dh_job *)arg;
+    static const sample_ops ops = {div_hist_create, div_hist_step, div_no_film, div_no_film, div_hist_write,
+                                   GPU_Destroy};
+    g_job = dh->job;
+    g_rank_blk = rank;
+    mr_alloc();
+    g_iface_hook = mr_interfaces;
+    const double *const *in = g_job->in + 8 * rank;
+    if (ref_init(&g_job->blk[rank], in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7])) return 1;
+    return histories_run(&ops, dh->np, dh->nv, dh->xyz, dh->nsteps, 0, g_job->out + g_job->out_off[rank]) ? 2 : 0;
+}
+
+int refmpi_dropin_histories(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const int *tfm,
+                            const double *const *in, int np, int nv, const double *xyz, int nsteps, double *out,
+                            const size_t *out_off, size_t out_len, size_t slot_bytes)
+{
+    double *shared = mmap(NULL, out_len * sizeof(double), PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
+    if (shared == MAP_FAILED) return -1;
+    mr_job job = {nblocks, blk, neigh, trans, tfm, in, 0, nsteps, shared, out_off, NULL, 0, NULL, NULL};
+    dh_job dh = {&job, np, nv, nsteps, xyz};
+    int rc = shm_run(nblocks, slot_bytes, dh_body, &dh);
+    memcpy(out, shared, out_len * sizeof(double));
+    munmap(shared, out_len * sizeof(double));
+    return rc;
+}
+
 int refmpi_dropin_run(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const int *tfm,
                       const double *const *in, int nsteps, int tau_at, double tau_factor, double *out,
                       const size_t *out_off, const size_t *ng, size_t out_len, double *extra, size_t slot_bytes)

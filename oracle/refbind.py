@@ -568,3 +568,55 @@ def run_dropin_multirank(division, nsteps: int, tau_at: int = -1, tau_factor: fl
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
         return pool.apply(_dropin_multirank_worker, (division, nsteps, tau_at, tau_factor, nan, real))
+
+
+def _dropin_multirank_histories_worker(division, np_, nv, xyz, nsteps):
+    case = division.case
+    os.environ["SHOCK_B200_LIB"] = os.path.join(os.path.dirname(HERE), "shock_b200", "libshock_b200.so")
+    lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockdropinmpi_w{case.order}_{case.dim}d.so"), mode=os.RTLD_LOCAL)
+    lib.refmpi_dropin_histories.restype = C.c_int
+    nb = len(division.blocks)
+    per = np_ * (2 + nsteps) + nv * (2 + 3 * nsteps) + nsteps
+    off = np.arange(nb, dtype=np.uint64) * np.uint64(per)
+    params = (RefParams * nb)(*[_ref_params(b) for b in division.blocks])
+    f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
+    keep = [[f(a) for a in b.real_fields()] for b in division.blocks]
+    ptrs = (C.POINTER(C.c_double) * (8 * nb))(*[_ptr(a) for fl in keep for a in fl])
+    neigh = np.ascontiguousarray(division.neighbour, dtype=np.int32)
+    trans = np.ascontiguousarray(division.translation, dtype=np.float32)
+    tfm = np.ascontiguousarray(division.transform, dtype=np.int32)
+    xyz = np.ascontiguousarray(xyz, np.float64)
+    out = np.zeros(nb * per)
+    g2 = case.order + 1
+    shapes = [(b.ni + g2, b.nj + g2, (b.nk + g2) if case.dim == 3 else 1) for b in division.blocks]
+    face = max(max(s[0] * s[1], s[1] * s[2], s[0] * s[2]) for s in shapes)
+    ng = [s[0] * s[1] * s[2] for s in shapes]
+    slot = max(13 * (g2 // 2) * face * 8, max(8 * (8 * b.real_points + 6 * n) for b, n in zip(division.blocks, ng)))
+    rc = lib.refmpi_dropin_histories(C.c_int(nb), params, neigh.ctypes.data_as(C.POINTER(C.c_int)),
+                                     trans.ctypes.data_as(C.POINTER(C.c_float)),
+                                     tfm.ctypes.data_as(C.POINTER(C.c_int)), ptrs, C.c_int(np_), C.c_int(nv),
+                                     _ptr(xyz), C.c_int(nsteps), _ptr(out),
+                                     off.ctypes.data_as(C.POINTER(C.c_size_t)), C.c_size_t(out.size),
+                                     C.c_size_t(slot))
+    if rc != 0:
+        raise RuntimeError(f"drop-in multi-rank histories failed ({rc})")
+    return out.reshape(nb, per)
+
+
+def run_dropin_multirank_histories(division, np_: int, nv: int, xyz, nsteps: int):
+    """The drop-in's division mode with device probe histories (over the
+    test double): every rank places the locations xyz ((np_ + nv) x 3) with
+    SHOCK's own prepare*HistoryValues and runs nsteps steps writing its
+    histories through the binding.  Per rank: per pressure point its ijk,
+    flag and nsteps pressures; per velocity point ijk, flag, 3 x nsteps
+    velocities; then the nsteps times."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        return pool.apply(_dropin_multirank_histories_worker, (division, np_, nv, xyz, nsteps))
+
+
+def mock_div_probe_value(b, f, o, s):
+    """The test double's probe value of block b, field f (p, u, v, w) at
+    ghosted point o after step s (ref_harness/mock_shock.c)."""
+    return 100.0 * b + 1.0 + f + 0.01 * s + 1e-7 * float(o)

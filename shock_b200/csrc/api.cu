@@ -1047,6 +1047,13 @@ static void multi_enqueue_step(shock_multi *m, int un, int &nk)
             launch_bc_save(c->G, c->F.p, c->plast, m->stream);
             nk++;
         }
+    // each block's pressure and velocity histories of U_lastStep
+    for (shock_ctx *c : m->blk)
+        if (c->n_probes) {
+            launch_probe_record(c->probe_idx, c->n_probes, c->F.p, c->buf[cur], c->probe_hist, c->probe_cap,
+                                c->probe_count, m->stream);
+            nk++;
+        }
 }
 
 extern "C" {
@@ -1324,6 +1331,22 @@ int shock_multi_upload_state(shock_multi *m, int block, const double *prim5)
         m->un = 0;
     }
     return shock_upload_state(m->blk[block], prim5);
+}
+
+int shock_multi_set_probes(shock_multi *m, int block, int n, const int *ijk3, int capacity)
+{
+    if (!m || block < 0 || block >= (int)m->blk.size()) return fail(SHOCK_EINVAL, "bad block");
+    if (int rc = shock_set_probes(m->blk[block], n, ijk3, capacity)) return rc;
+    // the division's step graphs are captured again with (or without) it
+    for (int i = 0; i < 3; i++)
+        if (m->step_graph[i]) { cudaGraphExecDestroy(m->step_graph[i]); m->step_graph[i] = nullptr; }
+    return SHOCK_OK;
+}
+
+int shock_multi_probe_history(shock_multi *m, int block, double *out4, int max_steps, int *steps)
+{
+    if (!m || block < 0 || block >= (int)m->blk.size()) return fail(SHOCK_EINVAL, "bad block");
+    return shock_probe_history(m->blk[block], out4, max_steps, steps);
 }
 
 int shock_multi_download_pressure(shock_multi *m, int block, double *p)

@@ -67,6 +67,8 @@ static int g_np, g_nv;      /* probe points registered for the pressure / veloci
 static double *g_probe_rows, *g_probe_last;   /* fetched history rows; the latest step's (p,u,v,w) */
 static int g_probe_pending; /* a step ran since the history was last fetched */
 #define PROBE_CAPACITY 256
+static int g_div_hist;      /* division mode: some rank has probe points on the device */
+static int *g_probe_n;      /* rank 0, division mode: every rank's number of probe points */
 static int *g_film_sample;  /* the sample index of every device frame */
 static int g_film_frames, g_film_cap;
 
@@ -237,7 +239,7 @@ int GPU_Create(struct strct_configuration *c, struct strct_mesh *m, struct strct
 
 /* ---- division mode: every rank's block on rank 0's device ---- */
 
-enum { TAG_DESC = 29101, TAG_FIELDS, TAG_STATE_UP, TAG_STATE_DOWN };
+enum { TAG_DESC = 29101, TAG_FIELDS, TAG_STATE_UP, TAG_STATE_DOWN, TAG_PROBES };
 #define DESC_INTS (3 + 6 + 6 + 18)
 
 static void wait_all(int n, MPI_Request *r)
@@ -254,6 +256,18 @@ static void exchange_block(struct strct_configuration *c, int r, double *buf, si
         MPI_Isend(buf, (int)(6 * ng), MPI_DOUBLE, r, tag, c->MPI_comm, &q);
     else
         MPI_Irecv(buf, (int)(6 * ng), MPI_DOUBLE, r, tag, c->MPI_comm, &q);
+    wait_all(1, &q);
+}
+
+/* a row of n probe points (4 doubles each): rank 0 sends it to rank r, or
+ * another rank (r = 0) receives its own */
+static void exchange_row(struct strct_configuration *c, double *row, int n, int r)
+{
+    MPI_Request q;
+    if (c->MPI_rank == 0)
+        MPI_Isend(row, 4 * n, MPI_DOUBLE, r, TAG_PROBES, c->MPI_comm, &q);
+    else
+        MPI_Irecv(row, 4 * n, MPI_DOUBLE, 0, TAG_PROBES, c->MPI_comm, &q);
     wait_all(1, &q);
 }
 
@@ -408,6 +422,7 @@ static void division_step(struct strct_configuration *c)
     }
     g_tau = (double)c->numericalTau;
     g_host_behind = 1;
+    g_probe_pending = 1;
 }
 
 static int division_nan(struct strct_configuration *c)
@@ -552,9 +567,10 @@ void GPU_UploadState(struct strct_configuration *c, struct strct_U *U_RK)
 
 /* ---- probe histories on the device (single rank) ---- */
 
+static int enable_division_histories(struct strct_configuration *c, const int *ijk3, int n);
+
 int GPU_EnableHistories(struct strct_configuration *c)
 {
-    if (g_division) return 0;   /* several ranks: GPU_SyncHost and SHOCK's own writers */
     const int nj = c->int_jMeshPointsGhostCells, nk = c->int_kMeshPointsGhostCells;
     const int np = c->flag_PressureHistory == 1 ? c->PressureHistory_No : 0;
     const int nv = c->flag_VelocityHistory == 1 ? c->VelocityHistory_No : 0;
@@ -578,14 +594,86 @@ int GPU_EnableHistories(struct strct_configuration *c)
             n++;
             g_nv++;
         }
-    int rc = shock_set_probes(g_ctx, n, ijk3, PROBE_CAPACITY);
-    free(ijk3);
     free(g_probe_rows);
     free(g_probe_last);
-    g_probe_rows = n ? malloc((size_t)PROBE_CAPACITY * n * 4 * sizeof(double)) : NULL;
+    g_probe_rows = NULL;
     g_probe_last = n ? calloc((size_t)n * 4, sizeof(double)) : NULL;
     g_probe_pending = 0;
+    int rc;
+    if (g_division) {
+        rc = enable_division_histories(c, ijk3, n);
+    } else {
+        rc = shock_set_probes(g_ctx, n, ijk3, PROBE_CAPACITY);
+        g_probe_rows = n ? malloc((size_t)PROBE_CAPACITY * n * 4 * sizeof(double)) : NULL;
+    }
+    free(ijk3);
     return rc;
+}
+
+/* Division mode: every rank's probe points go to its block on rank 0 (a
+ * count, then the points), and every rank learns whether any rank has
+ * some, so that the writers take the same steps everywhere. */
+static int enable_division_histories(struct strct_configuration *c, const int *ijk3, int n)
+{
+    const int P = c->MPI_size;
+    int rc = 0, total = 0;
+    if (c->MPI_rank != 0) {
+        MPI_Request q[2];
+        MPI_Isend(&n, 1, MPI_INT, 0, TAG_PROBES, c->MPI_comm, &q[0]);
+        MPI_Isend((void *)ijk3, 3 * n + 1, MPI_INT, 0, TAG_PROBES, c->MPI_comm, &q[1]);
+        wait_all(2, q);
+    } else {
+        free(g_probe_n);
+        g_probe_n = calloc((size_t)P, sizeof(int));
+        size_t most = (size_t)n;
+        for (int r = 0; r < P; r++) {
+            int nr = n, *pts = (int *)ijk3;
+            if (r) {
+                MPI_Request q;
+                MPI_Irecv(&nr, 1, MPI_INT, r, TAG_PROBES, c->MPI_comm, &q);
+                wait_all(1, &q);
+                pts = malloc((3 * (size_t)nr + 1) * sizeof(int));
+                MPI_Irecv(pts, 3 * nr + 1, MPI_INT, r, TAG_PROBES, c->MPI_comm, &q);
+                wait_all(1, &q);
+            }
+            g_probe_n[r] = nr;
+            total += nr;
+            if ((size_t)nr > most) most = (size_t)nr;
+            const int e = shock_multi_set_probes(g_multi, r, nr, pts, PROBE_CAPACITY);
+            if (e && !rc) rc = e;
+            if (r) free(pts);
+        }
+        g_probe_rows = malloc((size_t)PROBE_CAPACITY * (most + 1) * 4 * sizeof(double));
+    }
+    MPI_Bcast(&rc, 1, MPI_INT, 0, c->MPI_comm);
+    MPI_Bcast(&total, 1, MPI_INT, 0, c->MPI_comm);
+    g_div_hist = !rc && total > 0;
+    return rc;
+}
+
+/* Division mode, collective: rank 0 fetches every block's history and
+ * sends each rank the last step's row of its points. */
+static void fetch_division_probes(struct strct_configuration *c)
+{
+    if (!g_probe_pending) return;
+    const int n = g_np + g_nv;
+    if (c->MPI_rank != 0) {
+        if (n) exchange_row(c, g_probe_last, n, 0);
+    } else {
+        for (int r = 0; r < c->MPI_size; r++) {
+            const int nr = g_probe_n[r];
+            if (!nr) continue;
+            int steps = 0;
+            int rc = shock_multi_probe_history(g_multi, r, g_probe_rows, PROBE_CAPACITY, &steps);
+            if (rc) fail("shock_multi_probe_history", rc);
+            double *row = g_probe_rows + (size_t)(steps > 0 ? steps - 1 : 0) * nr * 4;
+            if (r == 0)
+                memcpy(g_probe_last, row, (size_t)nr * 4 * sizeof(double));
+            else
+                exchange_row(c, row, nr, r);
+        }
+    }
+    g_probe_pending = 0;
 }
 
 /* the latest step's (p,u,v,w) of every registered point */
@@ -602,11 +690,14 @@ static void fetch_probes(void)
 
 void GPU_WriteValuesForPressureHistory(struct strct_configuration *c, struct strct_U *U_lastStep)
 {
-    if (g_division || !g_probe_last) {
+    if (g_division ? !g_div_hist : !g_probe_last) {
         WriteValuesForPressureHistory(c, U_lastStep);
         return;
     }
-    fetch_probes();
+    if (g_division)
+        fetch_division_probes(c);
+    else
+        fetch_probes();
     const int it = c->int_actualIteration - (c->int_StartIteration + 1);
     c->PressureHistory_time[it] = c->time_dim;
     int q = 0;
@@ -616,11 +707,14 @@ void GPU_WriteValuesForPressureHistory(struct strct_configuration *c, struct str
 
 void GPU_WriteValuesForVelocityHistory(struct strct_configuration *c, struct strct_U *U_lastStep)
 {
-    if (g_division || !g_probe_last) {
+    if (g_division ? !g_div_hist : !g_probe_last) {
         WriteValuesForVelocityHistory(c, U_lastStep);
         return;
     }
-    fetch_probes();
+    if (g_division)
+        fetch_division_probes(c);
+    else
+        fetch_probes();
     const int it = c->int_actualIteration - (c->int_StartIteration + 1);
     c->VelocityHistory_time[it] = c->time_dim;
     int q = g_np;
@@ -704,4 +798,7 @@ void GPU_Destroy(void)
     free(g_film_sample);
     g_film_sample = NULL;
     g_film_frames = g_film_cap = 0;
+    free(g_probe_n);
+    g_probe_n = NULL;
+    g_div_hist = 0;
 }

@@ -197,3 +197,38 @@ def test_dropin_film(name):
             assert val(f, q, C.c_longlong(5)) == want[5]
     times = out[8 * nsamples * nr:]
     assert np.allclose(times, [case.tau * (f + 1) for f in frame_of], rtol=1e-14, atol=0)
+
+
+def test_dropin_division_histories():
+    """In the division mode GPU_EnableHistories sends every rank's flagged
+    probe points to its block on rank 0, and the writers give every rank the
+    last step's device values of its own points (over the test double, whose
+    values name the block, the point and the step); each location inside
+    the zone is some rank's, and only that rank's, probe."""
+    from refbind import mock_div_probe_value, run_dropin_multirank_histories
+    d = DIVISIONS["tgv12_w5_2x2x2"]()
+    if not _available(d):
+        pytest.skip("drop-in multi-rank harness absent (make -C oracle with the reference sources)")
+    c = d.case
+    rng = np.random.default_rng(5)
+    lo = np.array([c.x.min(), c.y.min(), c.z.min()])
+    hi = np.array([c.x.max(), c.y.max(), c.z.max()])
+    np_, nv, nsteps = 5, 4, 5
+    xyz = lo + 0.05 * (hi - lo) + rng.random((np_ + nv, 3)) * 0.9 * (hi - lo)
+    out = run_dropin_multirank_histories(d, np_, nv, xyz, nsteps)
+    owners = np.zeros(np_ + nv, dtype=int)
+    for b in range(len(d.blocks)):
+        o = 0
+        for q in range(np_ + nv):
+            width = nsteps if q < np_ else 3 * nsteps
+            ijk, flag, hist = int(out[b, o]), int(out[b, o + 1]), out[b, o + 2:o + 2 + width]
+            owners[q] += flag
+            if q < np_:
+                want = [mock_div_probe_value(b, 0, ijk, s) if flag else 0.0 for s in range(1, nsteps + 1)]
+            else:
+                want = [mock_div_probe_value(b, f, ijk, s) if flag else 0.0
+                        for f in (1, 2, 3) for s in range(1, nsteps + 1)]
+            assert list(hist) == want, (b, q)
+            o += 2 + width
+        assert np.allclose(out[b, o:], [c.tau * s for s in range(1, nsteps + 1)], rtol=1e-14, atol=0)
+    assert (owners == 1).all(), owners
