@@ -67,8 +67,9 @@ void GPU_UploadState(struct strct_configuration *config, struct strct_U *U_RK);
  * place of WriteValuesForPressureHistory / WriteValuesForVelocityHistory
  * (src/Functions.c:5381-5417): they write the last step's device values
  * (U_lastStep's p, u, v, w at the points) and time_dim at the current
- * iteration.  With several ranks they are SHOCK's own writers (the host
- * state must then be synced first, as before). */
+ * iteration.  With several ranks every rank's points are its block's on
+ * rank 0's device and the calls are collective (rank 0 sends each rank the
+ * last step's values of its points). */
 int GPU_EnableHistories(struct strct_configuration *config);
 void GPU_WriteValuesForPressureHistory(struct strct_configuration *config, struct strct_U *U_lastStep);
 void GPU_WriteValuesForVelocityHistory(struct strct_configuration *config, struct strct_U *U_lastStep);
