@@ -1075,7 +1075,7 @@ static int dj_body(int rank, void *arg)
  * the binding; out at out_off[rank]: histories_run's output of the rank. */
 typedef struct {
     const mr_job *job;
-    int np, nv, nsteps;
+    int np, nv, nsteps, cpu;
     const double *xyz;
 } dh_job;
 
@@ -1103,23 +1103,26 @@ static int dh_body(int rank, void *arg)
     const dh_job *dh = (const dh_job *)arg;
     static const sample_ops ops = {div_hist_create, div_hist_step, div_no_film, div_no_film, div_hist_write,
                                    GPU_Destroy};
+    const sample_ops *use = dh->cpu ? &cpu_sample_ops : &ops;
     g_job = dh->job;
     g_rank_blk = rank;
     mr_alloc();
     g_iface_hook = mr_interfaces;
     const double *const *in = g_job->in + 8 * rank;
     if (ref_init(&g_job->blk[rank], in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7])) return 1;
-    return histories_run(&ops, dh->np, dh->nv, dh->xyz, dh->nsteps, 0, g_job->out + g_job->out_off[rank]) ? 2 : 0;
+    return histories_run(use, dh->np, dh->nv, dh->xyz, dh->nsteps, 0, g_job->out + g_job->out_off[rank]) ? 2 : 0;
 }
 
+/* cpu = 1: the same loop with SHOCK's own CalcRungeKutta and writers on
+ * every rank (the reference of the binding's run). */
 int refmpi_dropin_histories(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const int *tfm,
                             const double *const *in, int np, int nv, const double *xyz, int nsteps, double *out,
-                            const size_t *out_off, size_t out_len, size_t slot_bytes)
+                            const size_t *out_off, size_t out_len, size_t slot_bytes, int cpu)
 {
     double *shared = mmap(NULL, out_len * sizeof(double), PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
     if (shared == MAP_FAILED) return -1;
     mr_job job = {nblocks, blk, neigh, trans, tfm, in, 0, nsteps, shared, out_off, NULL, 0, NULL, NULL};
-    dh_job dh = {&job, np, nv, nsteps, xyz};
+    dh_job dh = {&job, np, nv, nsteps, cpu, xyz};
     int rc = shm_run(nblocks, slot_bytes, dh_body, &dh);
     memcpy(out, shared, out_len * sizeof(double));
     munmap(shared, out_len * sizeof(double));

@@ -570,10 +570,12 @@ def run_dropin_multirank(division, nsteps: int, tau_at: int = -1, tau_factor: fl
         return pool.apply(_dropin_multirank_worker, (division, nsteps, tau_at, tau_factor, nan, real))
 
 
-def _dropin_multirank_histories_worker(division, np_, nv, xyz, nsteps):
+def _dropin_multirank_histories_worker(division, np_, nv, xyz, nsteps, real=False, cpu=False):
     case = division.case
     os.environ["SHOCK_B200_LIB"] = os.path.join(os.path.dirname(HERE), "shock_b200", "libshock_b200.so")
-    lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockdropinmpi_w{case.order}_{case.dim}d.so"), mode=os.RTLD_LOCAL)
+    tag = "real" if real else ""
+    lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockdropinmpi{tag}_w{case.order}_{case.dim}d.so"),
+                 mode=os.RTLD_LOCAL)
     lib.refmpi_dropin_histories.restype = C.c_int
     nb = len(division.blocks)
     per = np_ * (2 + nsteps) + nv * (2 + 3 * nsteps) + nsteps
@@ -597,23 +599,25 @@ def _dropin_multirank_histories_worker(division, np_, nv, xyz, nsteps):
                                      tfm.ctypes.data_as(C.POINTER(C.c_int)), ptrs, C.c_int(np_), C.c_int(nv),
                                      _ptr(xyz), C.c_int(nsteps), _ptr(out),
                                      off.ctypes.data_as(C.POINTER(C.c_size_t)), C.c_size_t(out.size),
-                                     C.c_size_t(slot))
+                                     C.c_size_t(slot), C.c_int(int(cpu)))
     if rc != 0:
         raise RuntimeError(f"drop-in multi-rank histories failed ({rc})")
     return out.reshape(nb, per)
 
 
-def run_dropin_multirank_histories(division, np_: int, nv: int, xyz, nsteps: int):
+def run_dropin_multirank_histories(division, np_: int, nv: int, xyz, nsteps: int, real: bool = False,
+                                   cpu: bool = False):
     """The drop-in's division mode with device probe histories (over the
-    test double): every rank places the locations xyz ((np_ + nv) x 3) with
-    SHOCK's own prepare*HistoryValues and runs nsteps steps writing its
-    histories through the binding.  Per rank: per pressure point its ijk,
-    flag and nsteps pressures; per velocity point ijk, flag, 3 x nsteps
-    velocities; then the nsteps times."""
+    test double, or with real=True over the library on rank 0's GPU; cpu=True:
+    the same loop with SHOCK's own steps and writers): every rank places the
+    locations xyz ((np_ + nv) x 3) with SHOCK's own prepare*HistoryValues and
+    runs nsteps steps writing its histories.  Per rank: per pressure point
+    its ijk, flag and nsteps pressures; per velocity point ijk, flag, 3 x
+    nsteps velocities; then the nsteps times."""
     import multiprocessing as mp
     ctx = mp.get_context("spawn")
     with ctx.Pool(1) as pool:
-        return pool.apply(_dropin_multirank_histories_worker, (division, np_, nv, xyz, nsteps))
+        return pool.apply(_dropin_multirank_histories_worker, (division, np_, nv, xyz, nsteps, real, cpu))
 
 
 def mock_div_probe_value(b, f, o, s):

@@ -33,3 +33,32 @@ def test_dropin_division_on_gpu(name):
     e = l2_rel(got, want)[idx]
     assert (e <= 1e-10).all(), (name, e)
     assert all(r["nan_steps"] == 0 for r in res)
+
+
+def test_dropin_division_histories_on_gpu():
+    """The division mode's device probe histories over the library on rank
+    0's GPU against the same loop with SHOCK's own steps and writers on
+    every rank: the same flagged points on the same ranks, values within
+    1e-12 of SHOCK's, the same times."""
+    from refbind import run_dropin_multirank_histories
+    d = DIVISIONS["tgv12_w5_2x2x2"]()
+    c = d.case
+    if not dropin_multirank_available(c.order, c.dim, real=True):
+        pytest.skip("drop-in multi-rank builds absent (make -C oracle with the reference sources)")
+    rng = np.random.default_rng(5)
+    lo = np.array([c.x.min(), c.y.min(), c.z.min()])
+    hi = np.array([c.x.max(), c.y.max(), c.z.max()])
+    np_, nv, nsteps = 4, 3, 6
+    xyz = lo + 0.05 * (hi - lo) + rng.random((np_ + nv, 3)) * 0.9 * (hi - lo)
+    got = run_dropin_multirank_histories(d, np_, nv, xyz, nsteps, real=True)
+    want = run_dropin_multirank_histories(d, np_, nv, xyz, nsteps, real=True, cpu=True)
+    for b in range(len(d.blocks)):
+        o = 0
+        for q in range(np_ + nv):
+            width = nsteps if q < np_ else 3 * nsteps
+            assert got[b, o] == want[b, o] and got[b, o + 1] == want[b, o + 1], (b, q)
+            a, r = got[b, o + 2:o + 2 + width], want[b, o + 2:o + 2 + width]
+            scale = max(np.abs(r).max(), 1e-300)
+            assert np.abs(a - r).max() <= 1e-12 * scale, (b, q)
+            o += 2 + width
+        assert np.array_equal(got[b, o:], want[b, o:])
