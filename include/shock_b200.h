@@ -475,6 +475,11 @@ int shock_multi_upload_last_pressure(shock_multi *m, int block, const double *p)
  * shock_probe_history), recorded by the division's step graph. */
 int shock_multi_set_probes(shock_multi *m, int block, int n, const int *ijk3, int capacity);
 int shock_multi_probe_history(shock_multi *m, int block, double *out4, int max_steps, int *steps);
+/* Film frames of every block (as shock_film_reserve / shock_film_sample),
+ * and one block's frames (as shock_film_download). */
+int shock_multi_film_reserve(shock_multi *m, int max_frames);
+int shock_multi_film_sample(shock_multi *m);
+int shock_multi_film_download(shock_multi *m, int block, double *out, int max_frames, int *frames);
 /* The time step of the following steps (as shock_set_tau). */
 int shock_multi_set_tau(shock_multi *m, double tau);
 /* checkNAN over every block; SHOCK_ENAN when any density is non-finite. */

@@ -297,6 +297,39 @@ int shock_multi_probe_history(shock_multi *m, int b, double *out4, int max_steps
     return SHOCK_OK;
 }
 
+static int g_div_film_cap, g_div_film_frames;
+
+int shock_multi_film_reserve(shock_multi *m, int max_frames)
+{
+    if (!m) return SHOCK_EINVAL;
+    g_div_film_cap = max_frames;
+    g_div_film_frames = 0;
+    return SHOCK_OK;
+}
+
+int shock_multi_film_sample(shock_multi *m)
+{
+    if (!m || g_div_film_frames >= g_div_film_cap) return SHOCK_ENOMEM;
+    g_div_film_frames++;
+    return SHOCK_OK;
+}
+
+/* block b's frame f, field q, real point t */
+double mock_div_film_value(int b, int f, int q, long long t) { return 1000.0 * b + 10.0 * q + 0.001 * f + 1e-7 * (double)t; }
+
+int shock_multi_film_download(shock_multi *m, int b, double *out, int max_frames, int *frames)
+{
+    if (bad_block(m, b)) return SHOCK_EINVAL;
+    long long nr = 1;
+    for (int a = 0; a < m->dim; a++) nr *= m->dims[b][a] - 2 * m->g;
+    const int n = g_div_film_frames < max_frames ? g_div_film_frames : max_frames;
+    for (int f = 0; f < n; f++)
+        for (int q = 0; q < 8; q++)
+            for (long long t = 0; t < nr; t++) out[((size_t)f * 8 + q) * nr + t] = mock_div_film_value(b, f, q, t);
+    *frames = n;
+    return SHOCK_OK;
+}
+
 int shock_multi_check_nan(shock_multi *m, int *bad)
 {
     if (!m || !bad) return SHOCK_EINVAL;

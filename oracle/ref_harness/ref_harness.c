@@ -1129,6 +1129,54 @@ int refmpi_dropin_histories(int nblocks, const ref_params *blk, const int *neigh
     return rc;
 }
 
+/* The division mode's device Film: every rank runs film_run over the
+ * binding (or, cpu = 1, with SHOCK's own steps and sampling); out at
+ * out_off[rank]: film_run's output of the rank. */
+typedef struct {
+    const mr_job *job;
+    int nsamples, again, cpu;
+} df_job;
+
+static int div_film_create(int device, int film, int histories)
+{
+    (void)histories;
+    int rc = GPU_Create(&cfg, &msh, &U_last, &Qf, device);
+    if (!rc && film) rc = GPU_EnableFilm(&cfg);
+    return rc;
+}
+static void div_film_sample(struct strct_Film *F) { GPU_SampleFilm(&cfg, &msh, &U_last, F); }
+static void div_film_sync(struct strct_Film *F) { GPU_SyncFilm(&cfg, F); }
+static void div_no_hist(int np, int nv) { (void)np; (void)nv; }
+
+static int df_body(int rank, void *arg)
+{
+    const df_job *df = (const df_job *)arg;
+    static const sample_ops ops = {div_film_create, div_hist_step, div_film_sample, div_film_sync, div_no_hist,
+                                   GPU_Destroy};
+    g_job = df->job;
+    g_rank_blk = rank;
+    mr_alloc();
+    g_iface_hook = mr_interfaces;
+    const double *const *in = g_job->in + 8 * rank;
+    if (ref_init(&g_job->blk[rank], in[0], in[1], in[2], in[3], in[4], in[5], in[6], in[7])) return 1;
+    return film_run(df->cpu ? &cpu_sample_ops : &ops, df->nsamples, df->again, 0,
+                    g_job->out + g_job->out_off[rank]) ? 2 : 0;
+}
+
+int refmpi_dropin_film(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const int *tfm,
+                       const double *const *in, int nsamples, int again, double *out, const size_t *out_off,
+                       size_t out_len, size_t slot_bytes, int cpu)
+{
+    double *shared = mmap(NULL, out_len * sizeof(double), PROT_READ | PROT_WRITE, MAP_SHARED | MAP_ANONYMOUS, -1, 0);
+    if (shared == MAP_FAILED) return -1;
+    mr_job job = {nblocks, blk, neigh, trans, tfm, in, 0, 0, shared, out_off, NULL, 0, NULL, NULL};
+    df_job df = {&job, nsamples, again, cpu};
+    int rc = shm_run(nblocks, slot_bytes, df_body, &df);
+    memcpy(out, shared, out_len * sizeof(double));
+    munmap(shared, out_len * sizeof(double));
+    return rc;
+}
+
 int refmpi_dropin_run(int nblocks, const ref_params *blk, const int *neigh, const float *trans, const int *tfm,
                       const double *const *in, int nsteps, int tau_at, double tau_factor, double *out,
                       const size_t *out_off, const size_t *ng, size_t out_len, double *extra, size_t slot_bytes)

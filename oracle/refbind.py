@@ -624,3 +624,52 @@ def mock_div_probe_value(b, f, o, s):
     """The test double's probe value of block b, field f (p, u, v, w) at
     ghosted point o after step s (ref_harness/mock_shock.c)."""
     return 100.0 * b + 1.0 + f + 0.01 * s + 1e-7 * float(o)
+
+
+def _dropin_multirank_film_worker(division, nsamples, again, real, cpu):
+    case = division.case
+    os.environ["SHOCK_B200_LIB"] = os.path.join(os.path.dirname(HERE), "shock_b200", "libshock_b200.so")
+    tag = "real" if real else ""
+    lib = C.CDLL(os.path.join(HERE, "_ref", f"libshockdropinmpi{tag}_w{case.order}_{case.dim}d.so"),
+                 mode=os.RTLD_LOCAL)
+    lib.refmpi_dropin_film.restype = C.c_int
+    nb = len(division.blocks)
+    nr = [b.real_points for b in division.blocks]
+    per = [8 * nsamples * n + nsamples for n in nr]
+    off = np.zeros(nb, dtype=np.uint64)
+    for b in range(1, nb):
+        off[b] = off[b - 1] + per[b - 1]
+    params = (RefParams * nb)(*[_ref_params(b) for b in division.blocks])
+    f = lambda a: np.ascontiguousarray(np.asarray(a, np.float64).transpose(2, 1, 0)).ravel()
+    keep = [[f(a) for a in b.real_fields()] for b in division.blocks]
+    ptrs = (C.POINTER(C.c_double) * (8 * nb))(*[_ptr(a) for fl in keep for a in fl])
+    neigh = np.ascontiguousarray(division.neighbour, dtype=np.int32)
+    trans = np.ascontiguousarray(division.translation, dtype=np.float32)
+    tfm = np.ascontiguousarray(division.transform, dtype=np.int32)
+    out = np.zeros(int(off[-1]) + per[-1])
+    g2 = case.order + 1
+    shapes = [(b.ni + g2, b.nj + g2, (b.nk + g2) if case.dim == 3 else 1) for b in division.blocks]
+    face = max(max(s[0] * s[1], s[1] * s[2], s[0] * s[2]) for s in shapes)
+    ng = [s[0] * s[1] * s[2] for s in shapes]
+    slot = max(13 * (g2 // 2) * face * 8, max(8 * (8 * r + 6 * n) for r, n in zip(nr, ng)),
+               max(8 * 8 * r * (2 * nsamples + 4) for r in nr))
+    rc = lib.refmpi_dropin_film(C.c_int(nb), params, neigh.ctypes.data_as(C.POINTER(C.c_int)),
+                                trans.ctypes.data_as(C.POINTER(C.c_float)), tfm.ctypes.data_as(C.POINTER(C.c_int)),
+                                ptrs, C.c_int(nsamples), C.c_int(again), _ptr(out),
+                                off.ctypes.data_as(C.POINTER(C.c_size_t)), C.c_size_t(out.size), C.c_size_t(slot),
+                                C.c_int(int(cpu)))
+    if rc != 0:
+        raise RuntimeError(f"drop-in multi-rank film failed ({rc})")
+    return [out[int(off[b]):int(off[b]) + per[b]] for b in range(nb)]
+
+
+def run_dropin_multirank_film(division, nsamples: int, again: int, real: bool = False, cpu: bool = False):
+    """The drop-in's division mode with device Film (over the test double,
+    or with real=True over the library on rank 0's GPU; cpu=True: SHOCK's
+    own steps and sampling on every rank): per rank the eight Film arrays
+    (nsamples x its real points each) and the sample times; after sample
+    `again` the sample index goes back one (a NaN reset)."""
+    import multiprocessing as mp
+    ctx = mp.get_context("spawn")
+    with ctx.Pool(1) as pool:
+        return pool.apply(_dropin_multirank_film_worker, (division, nsamples, again, real, cpu))

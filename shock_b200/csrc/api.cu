@@ -1349,6 +1349,28 @@ int shock_multi_probe_history(shock_multi *m, int block, double *out4, int max_s
     return shock_probe_history(m->blk[block], out4, max_steps, steps);
 }
 
+int shock_multi_film_reserve(shock_multi *m, int max_frames)
+{
+    if (!m) return fail(SHOCK_EINVAL, "null argument");
+    for (shock_ctx *c : m->blk)
+        if (int rc = shock_film_reserve(c, max_frames)) return rc;
+    return SHOCK_OK;
+}
+
+int shock_multi_film_sample(shock_multi *m)
+{
+    if (!m) return fail(SHOCK_EINVAL, "null argument");
+    for (shock_ctx *c : m->blk)
+        if (int rc = shock_film_sample(c)) return rc;
+    return SHOCK_OK;
+}
+
+int shock_multi_film_download(shock_multi *m, int block, double *out, int max_frames, int *frames)
+{
+    if (!m || block < 0 || block >= (int)m->blk.size()) return fail(SHOCK_EINVAL, "bad block");
+    return shock_film_download(m->blk[block], out, max_frames, frames);
+}
+
 int shock_multi_download_pressure(shock_multi *m, int block, double *p)
 {
     if (!m || block < 0 || block >= (int)m->blk.size()) return fail(SHOCK_EINVAL, "bad block");

@@ -59,6 +59,7 @@ static shock_ctx *g_ctx;
 static shock_multi *g_multi;   /* division mode, rank 0 */
 static int g_division;         /* MPI_size > 1: every GPU_* call is collective */
 static size_t *g_block_ng;     /* rank 0: ghosted points of every rank's block */
+static size_t *g_block_nr;     /* rank 0: real points of every rank's block */
 static double *g_block_buf;    /* rank 0: 6*NG doubles of the largest block */
 static int g_host_behind;   /* the device state is newer than the host U_RK */
 static double *g_buf;       /* 5*NG doubles */
@@ -239,7 +240,7 @@ int GPU_Create(struct strct_configuration *c, struct strct_mesh *m, struct strct
 
 /* ---- division mode: every rank's block on rank 0's device ---- */
 
-enum { TAG_DESC = 29101, TAG_FIELDS, TAG_STATE_UP, TAG_STATE_DOWN, TAG_PROBES };
+enum { TAG_DESC = 29101, TAG_FIELDS, TAG_STATE_UP, TAG_STATE_DOWN, TAG_PROBES, TAG_FILM };
 #define DESC_INTS (3 + 6 + 6 + 18)
 
 static void wait_all(int n, MPI_Request *r)
@@ -349,6 +350,7 @@ static int create_division(struct strct_configuration *c, struct strct_mesh *m, 
         shock_block *blk = calloc((size_t)P, sizeof(shock_block));
         double **data = calloc((size_t)P, sizeof(double *));
         g_block_ng = calloc((size_t)P, sizeof(size_t));
+        g_block_nr = calloc((size_t)P, sizeof(size_t));
         size_t most = 0;
         for (int r = 0; r < P; r++) {
             int d[DESC_INTS];
@@ -365,6 +367,7 @@ static int create_division(struct strct_configuration *c, struct strct_mesh *m, 
             const size_t n = (size_t)d[0] * d[1] * d[2];
             const size_t gn = (size_t)(d[0] + 2 * g) * (d[1] + 2 * g) * (MESHDIMENSIONS == 3 ? d[2] + 2 * g : 1);
             g_block_ng[r] = gn;
+            g_block_nr[r] = n;
             if (gn > most) most = gn;
             if (r == 0) {
                 data[r] = mine;
@@ -731,10 +734,14 @@ void GPU_WriteValuesForVelocityHistory(struct strct_configuration *c, struct str
 
 int GPU_EnableFilm(struct strct_configuration *c)
 {
-    if (g_division) return 0;   /* several ranks: GPU_SyncHost and SHOCK's own sampling */
     /* a NaN reset takes samples again, so leave room for every sample twice */
     g_film_cap = 2 * c->int_Samples + 4;
-    int rc = shock_film_reserve(g_ctx, g_film_cap);
+    int rc = 0;
+    if (!g_division)
+        rc = shock_film_reserve(g_ctx, g_film_cap);
+    else if (c->MPI_rank == 0)
+        rc = shock_multi_film_reserve(g_multi, g_film_cap);
+    if (g_division) MPI_Bcast(&rc, 1, MPI_INT, 0, c->MPI_comm);
     if (rc) return rc;
     free(g_film_sample);
     g_film_sample = malloc((size_t)g_film_cap * sizeof(int));
@@ -745,26 +752,51 @@ int GPU_EnableFilm(struct strct_configuration *c)
 void GPU_SampleFilm(struct strct_configuration *c, struct strct_mesh *m, struct strct_U *U_lastStep,
                     struct strct_Film *Film)
 {
-    if (g_division || !g_film_sample) {
+    if (!g_film_sample) {
         CalcValuesForPost(c, m, U_lastStep);
         WriteValuesFromUToFilm(c, U_lastStep, Film, m);
         return;
     }
     Film->time_dim[c->int_actualSample] = c->time_dim;
     if (g_film_frames >= g_film_cap) fail("GPU_SampleFilm", SHOCK_ENOMEM);
-    int rc = shock_film_sample(g_ctx);
-    if (rc) fail("shock_film_sample", rc);
+    if (!g_division || c->MPI_rank == 0) {
+        /* several ranks: rank 0 takes every block's frame */
+        int rc = g_division ? shock_multi_film_sample(g_multi) : shock_film_sample(g_ctx);
+        if (rc) fail("shock_film_sample", rc);
+    }
     g_film_sample[g_film_frames++] = c->int_actualSample;
 }
 
 void GPU_SyncFilm(struct strct_configuration *c, struct strct_Film *Film)
 {
-    if (g_division || !g_film_sample || !g_film_frames) return;
+    if (!g_film_sample || !g_film_frames) return;
     const size_t nr = (size_t)c->int_iMeshPoints * c->int_jMeshPoints * c->int_kMeshPoints;
     double *buf = malloc(8 * nr * (size_t)g_film_frames * sizeof(double));
-    int got = 0;
-    int rc = shock_film_download(g_ctx, buf, g_film_frames, &got);
-    if (rc) fail("shock_film_download", rc);
+    int got = g_film_frames;
+    if (!g_division) {
+        int rc = shock_film_download(g_ctx, buf, g_film_frames, &got);
+        if (rc) fail("shock_film_download", rc);
+    } else if (c->MPI_rank != 0) {
+        /* several ranks: rank 0 downloads every block's frames and sends
+           each rank its own */
+        MPI_Request q;
+        MPI_Irecv(buf, (int)(8 * nr * (size_t)g_film_frames), MPI_DOUBLE, 0, TAG_FILM, c->MPI_comm, &q);
+        wait_all(1, &q);
+    } else {
+        for (int r = c->MPI_size - 1; r >= 0; r--) {   /* rank 0's own frames last, into buf */
+            int frames = 0;
+            double *b = r == 0 ? buf : malloc(8 * g_block_nr[r] * (size_t)g_film_frames * sizeof(double));
+            int rc = shock_multi_film_download(g_multi, r, b, g_film_frames, &frames);
+            if (rc) fail("shock_multi_film_download", rc);
+            if (r) {
+                MPI_Request q;
+                MPI_Isend(b, (int)(8 * g_block_nr[r] * (size_t)g_film_frames), MPI_DOUBLE, r, TAG_FILM, c->MPI_comm,
+                          &q);
+                wait_all(1, &q);
+                free(b);
+            }
+        }
+    }
     /* device frame fields: rho, u, v, w, p, |grad rho|, Mach, lambda2; a
        sample taken again after a reset overwrites the earlier frame */
     FLT *dst[8] = {Film->rho, Film->u, Film->v, Film->w, Film->p, Film->gradRho, Film->MachNumber, Film->Lambda2};
@@ -789,6 +821,8 @@ void GPU_Destroy(void)
     g_buf = NULL;
     free(g_block_ng);
     g_block_ng = NULL;
+    free(g_block_nr);
+    g_block_nr = NULL;
     free(g_block_buf);
     g_block_buf = NULL;
     free(g_probe_rows);

@@ -81,8 +81,9 @@ void GPU_WriteValuesForVelocityHistory(struct strct_configuration *config, struc
  * WriteValuesFromUToFilm at a sample (it sets Film->time_dim of
  * int_actualSample; the caller still counts int_actualSample up);
  * GPU_SyncFilm before the Film is written (saveFile): every frame into its
- * sample's place in the Film arrays.  With several ranks they are SHOCK's
- * own calls (the host state must then be synced first). */
+ * sample's place in the Film arrays.  With several ranks the calls are
+ * collective: rank 0 takes every block's frame and sends each rank its own
+ * block's frames at GPU_SyncFilm. */
 int GPU_EnableFilm(struct strct_configuration *config);
 void GPU_SampleFilm(struct strct_configuration *config, struct strct_mesh *mesh, struct strct_U *U_lastStep,
                     struct strct_Film *Film);

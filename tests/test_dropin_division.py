@@ -232,3 +232,27 @@ def test_dropin_division_histories():
             o += 2 + width
         assert np.allclose(out[b, o:], [c.tau * s for s in range(1, nsteps + 1)], rtol=1e-14, atol=0)
     assert (owners == 1).all(), owners
+
+
+def test_dropin_division_film():
+    """In the division mode GPU_SampleFilm has rank 0 take every block's
+    frame and GPU_SyncFilm sends every rank its own block's frames, each at
+    its sample's place (a re-taken sample overwriting its frame), over the
+    test double whose frames name the block, the frame, the field and the
+    point."""
+    from refbind import run_dropin_multirank_film
+    d = DIVISIONS["tgv12_w5_2x2x2"]()
+    if not _available(d):
+        pytest.skip("drop-in multi-rank harness absent (make -C oracle with the reference sources)")
+    nsamples, again = 4, 3
+    res = run_dropin_multirank_film(d, nsamples, again)
+    frame_of = [0, 1, 3, 4]
+    for b, r in enumerate(res):
+        nr = d.blocks[b].real_points
+        film = r[:8 * nsamples * nr].reshape(8, nsamples, nr)
+        t = np.arange(nr)
+        for q in range(8):
+            for s, f in enumerate(frame_of):
+                want = 1000.0 * b + 10.0 * q + 0.001 * f + 1e-7 * t
+                assert np.array_equal(film[q, s], want), (b, q, s)
+        assert np.allclose(r[8 * nsamples * nr:], [d.case.tau * (f + 1) for f in frame_of], rtol=1e-14, atol=0)

@@ -62,3 +62,28 @@ def test_dropin_division_histories_on_gpu():
             assert np.abs(a - r).max() <= 1e-12 * scale, (b, q)
             o += 2 + width
         assert np.array_equal(got[b, o:], want[b, o:])
+
+
+def test_dropin_division_film_on_gpu():
+    """The division mode's device Film over the library on rank 0's GPU
+    against the same loop with SHOCK's own steps, CalcValuesForPost and
+    WriteValuesFromUToFilm on every rank: frames within 1e-12 (lambda2
+    1e-9), a re-taken sample in its place, the same times."""
+    from _util import rel_err
+    from refbind import run_dropin_multirank_film
+    d = DIVISIONS["tgv12_w5_2x2x2"]()
+    c = d.case
+    if not dropin_multirank_available(c.order, c.dim, real=True):
+        pytest.skip("drop-in multi-rank builds absent (make -C oracle with the reference sources)")
+    nsamples, again = 4, 3
+    got = run_dropin_multirank_film(d, nsamples, again, real=True)
+    want = run_dropin_multirank_film(d, nsamples, again, real=True, cpu=True)
+    for b in range(len(d.blocks)):
+        nr = d.blocks[b].real_points
+        fg = got[b][:8 * nsamples * nr].reshape(8, nsamples, nr)
+        fw = want[b][:8 * nsamples * nr].reshape(8, nsamples, nr)
+        for s in range(nsamples):
+            err = rel_err(fg[:, s], fw[:, s])
+            assert (err[:7] <= 1e-12).all(), (b, s, err)
+            assert err[7] <= 1e-9, (b, s, err)
+        assert np.array_equal(got[b][8 * nsamples * nr:], want[b][8 * nsamples * nr:])
